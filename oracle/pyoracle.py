@@ -1,0 +1,280 @@
+"""ctypes binding of the oracle restatement (oracle/xtoracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline leg of bench.py, as the checker.  The product library never
+imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libxtoracle.so")
+REF_BIN = os.path.join(HERE, "_ref", "xtref")
+
+XO_ACCEL_OCTREE, XO_ACCEL_BVH = 0, 1
+STENCIL, DEPTH, AO, PATHTRACER = 0, 1, 2, 3
+INTEGRATOR_NAMES = {STENCIL: "stencil", DEPTH: "depth", AO: "ao", PATHTRACER: "pathtracer"}
+
+
+class XoMaterial(C.Structure):
+    _fields_ = [("type", C.c_int32), ("diffuse", C.c_float * 3), ("specular", C.c_float * 3),
+                ("emissive", C.c_float * 3), ("reflectance", C.c_float), ("exponent", C.c_float),
+                ("ior", C.c_float)]
+
+
+class XoSceneDesc(C.Structure):
+    _fields_ = [("n_objects", C.c_int32), ("obj_kind", C.c_void_p), ("obj_first", C.c_void_p),
+                ("obj_count", C.c_void_p), ("obj_material", C.c_void_p),
+                ("n_spheres", C.c_int32), ("spheres", C.c_void_p),
+                ("n_planes", C.c_int32), ("planes", C.c_void_p),
+                ("n_tris", C.c_int32), ("tris", C.c_void_p), ("tri_normals", C.c_void_p),
+                ("n_materials", C.c_int32), ("materials", C.c_void_p),
+                ("env_type", C.c_int32), ("env_a", C.c_float * 3), ("env_b", C.c_float * 3),
+                ("cam_pos", C.c_float * 3), ("cam_target", C.c_float * 3), ("cam_up", C.c_float * 3),
+                ("cam_fov", C.c_float)]
+
+
+class XoRenderParams(C.Structure):
+    _fields_ = [("integrator", C.c_int32), ("width", C.c_int32), ("height", C.c_int32),
+                ("spp", C.c_int32), ("rdepth", C.c_int32), ("ao_max_distance", C.c_float),
+                ("seed", C.c_uint64)]
+
+
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["sh", os.path.join(HERE, "build_oracle.sh")], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        L.xo_scene_create.argtypes = [C.POINTER(XoSceneDesc), C.c_int, C.POINTER(C.c_void_p)]
+        L.xo_scene_destroy.argtypes = [C.c_void_p]
+        L.xo_trace.argtypes = [C.c_void_p, C.c_int64] + [C.c_void_p] * 8
+        L.xo_camera_ray.argtypes = [C.c_void_p] * 3 + [C.c_float] * 5 + [C.c_void_p] * 2
+        L.xo_render.argtypes = [C.c_void_p, C.POINTER(XoRenderParams), C.c_int64, C.c_void_p,
+                                C.c_void_p, C.POINTER(C.c_uint64)]
+        for n in ("xo_kat_sphere", "xo_kat_plane"):
+            getattr(L, n).argtypes = [C.c_void_p] * 4
+        L.xo_kat_triangle.argtypes = [C.c_void_p] * 5
+        L.xo_kat_aabb.argtypes = [C.c_void_p] * 4
+        L.xo_kat_hemisphere.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
+        L.xo_kat_diffuse.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
+        L.xo_kat_lobe.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]
+        L.xo_kat_material.argtypes = [C.POINTER(XoMaterial), C.c_void_p, C.c_int32] + [C.c_void_p] * 4
+        L.xo_kat_gradient.argtypes = [C.c_void_p] * 4
+        L.xo_stream_uniform.argtypes = [C.c_uint64, C.c_uint32]
+        L.xo_stream_uniform.restype = C.c_double
+        L.xo_path_key.argtypes = [C.c_uint64, C.c_uint64]
+        L.xo_path_key.restype = C.c_uint64
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+class OracleScene:
+    """The restated reference scene (Scene + ISurface objects + Octree/BVH)."""
+
+    def __init__(self, spec, accel: int = XO_ACCEL_BVH):
+        self.spec = spec
+        self._keep = []
+
+        def arr(a, dt):
+            a = np.ascontiguousarray(a, dtype=dt)
+            self._keep.append(a)
+            return a
+
+        d = XoSceneDesc()
+        d.n_objects = len(spec.obj_kind)
+        d.obj_kind = _ptr(arr(spec.obj_kind, np.int32))
+        d.obj_first = _ptr(arr(spec.obj_first, np.int32))
+        d.obj_count = _ptr(arr(spec.obj_count, np.int32))
+        d.obj_material = _ptr(arr(spec.obj_material, np.int32))
+        d.n_spheres = spec.spheres.shape[0]
+        d.spheres = _ptr(arr(spec.spheres.reshape(-1), np.float32))
+        d.n_planes = spec.planes.shape[0]
+        d.planes = _ptr(arr(spec.planes.reshape(-1), np.float32))
+        d.n_tris = spec.tris.shape[0]
+        d.tris = _ptr(arr(spec.tris.reshape(-1), np.float32))
+        d.tri_normals = _ptr(arr(spec.tri_normals.reshape(-1), np.float32)) if spec.tri_normals is not None else None
+        mats = (XoMaterial * max(1, len(spec.materials)))()
+        for i, m in enumerate(spec.materials):
+            mats[i].type = m.type
+            mats[i].diffuse[:] = list(m.diffuse)
+            mats[i].specular[:] = list(m.specular)
+            mats[i].emissive[:] = list(m.emissive)
+            mats[i].reflectance = m.reflectance
+            mats[i].exponent = m.exponent
+            mats[i].ior = m.ior
+        self._keep.append(mats)
+        d.n_materials = len(spec.materials)
+        d.materials = C.cast(mats, C.c_void_p)
+        d.env_type = spec.env_type
+        d.env_a[:] = list(spec.env_a)
+        d.env_b[:] = list(spec.env_b)
+        d.cam_pos[:] = list(spec.camera.position)
+        d.cam_target[:] = list(spec.camera.target)
+        d.cam_up[:] = list(spec.camera.up)
+        d.cam_fov = spec.camera.fov
+        self._desc = d
+        h = C.c_void_p()
+        if lib().xo_scene_create(C.byref(d), accel, C.byref(h)) != 0:
+            raise RuntimeError("xo_scene_create failed")
+        self.handle = h
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                lib().xo_scene_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+    def trace(self, org: np.ndarray, dirs: np.ndarray):
+        org = np.ascontiguousarray(org, np.float64).reshape(-1, 3)
+        dirs = np.ascontiguousarray(dirs, np.float64).reshape(-1, 3)
+        n = org.shape[0]
+        hit = np.zeros(n, np.int32); t = np.zeros(n); obj = np.zeros(n, np.int32); prim = np.zeros(n, np.int32)
+        pt = np.zeros((n, 3)); nr = np.zeros((n, 3))
+        lib().xo_trace(self.handle, n, _ptr(org), _ptr(dirs), _ptr(hit), _ptr(t), _ptr(obj), _ptr(prim),
+                       _ptr(pt), _ptr(nr))
+        return dict(hit=hit, t=t, obj=obj, prim=prim, point=pt, normal=nr)
+
+    def render(self, integrator: int, width: int, height: int, spp: int = 1, rdepth: int = 4,
+               ao_max_distance: float = 100.0, seed: int = 1, pixels: np.ndarray = None):
+        if pixels is None:
+            ys, xs = np.mgrid[0:height, 0:width]
+            pixels = np.stack([xs.ravel(), ys.ravel()], axis=1)
+        pixels = np.ascontiguousarray(pixels, np.int32).reshape(-1, 2)
+        p = XoRenderParams(integrator, width, height, spp, rdepth, ao_max_distance, seed)
+        out = np.zeros((pixels.shape[0], 4), np.float32)
+        rays = C.c_uint64(0)
+        lib().xo_render(self.handle, C.byref(p), pixels.shape[0], _ptr(pixels), _ptr(out), C.byref(rays))
+        return out, int(rays.value)
+
+
+def camera_rays(spec, width: int, height: int, pixels: np.ndarray):
+    """Pixel-centre primary rays (x+0.5, y+0.5) in FP64."""
+    pixels = np.asarray(pixels).reshape(-1, 2)
+    n = pixels.shape[0]
+    org = np.zeros((n, 3)); dirs = np.zeros((n, 3))
+    cam = spec.camera
+    pos = (C.c_float * 3)(*cam.position); tgt = (C.c_float * 3)(*cam.target); up = (C.c_float * 3)(*cam.up)
+    o = np.zeros(3); d = np.zeros(3)
+    L = lib()
+    for i in range(n):
+        L.xo_camera_ray(C.cast(pos, C.c_void_p), C.cast(tgt, C.c_void_p), C.cast(up, C.c_void_p), cam.fov,
+                        float(pixels[i, 0]) + 0.5, float(pixels[i, 1]) + 0.5, float(width), float(height),
+                        _ptr(o), _ptr(d))
+        org[i] = o; dirs[i] = d
+    return org, dirs
+
+
+def path_key(seed: int, path: int) -> int:
+    return int(lib().xo_path_key(seed, path))
+
+
+def stream_uniform(key: int, counter: int) -> float:
+    return float(lib().xo_stream_uniform(key, counter))
+
+
+# ----------------------------------------------------------------------
+# The reference itself (oracle/_ref/xtref, built from the XTracer sources).
+def ref_available() -> bool:
+    return os.path.exists(REF_BIN)
+
+
+def ref_render(scn: str, integrator: str, width: int, height: int, spp: int = 1, aa: int = 1, rdepth: int = 4,
+               threads: int = 1, seed: int = 1, tiles=None, ao_max_distance: float = None, workdir: str = "/tmp"):
+    """Runs the reference integrator through IIntegrator::render on the given tiles
+    ((x0,y0,x1,y1) list, or None for the full frame).  Returns (pixels xy, rgba,
+    stats dict with render_s / rays / threads)."""
+    import json
+    import tempfile
+    fd, out = tempfile.mkstemp(suffix=".bin", dir=workdir)
+    os.close(fd)
+    tfile = "-"
+    if tiles is not None:
+        fd, tfile = tempfile.mkstemp(suffix=".txt", dir=workdir)
+        with os.fdopen(fd, "w") as fh:
+            fh.write("".join("%d %d %d %d\n" % tuple(t) for t in tiles))
+    cmd = [REF_BIN, "render", scn, integrator, str(width), str(height), str(spp), str(aa), str(rdepth),
+           str(threads), str(seed), tfile, out]
+    if ao_max_distance is not None:
+        cmd.append(repr(float(ao_max_distance)))
+    env = dict(os.environ)
+    if threads:
+        env["OMP_NUM_THREADS"] = str(threads)
+    r = subprocess.run(cmd, capture_output=True, text=True, env=env)
+    if r.returncode != 0:
+        raise RuntimeError("xtref render failed: %s %s" % (r.stdout, r.stderr))
+    stats = json.loads(r.stdout.strip().splitlines()[-1])
+    raw = open(out, "rb").read()
+    os.unlink(out)
+    if tfile != "-":
+        os.unlink(tfile)
+    n = int(np.frombuffer(raw[:8], np.int64)[0])
+    rec = np.frombuffer(raw[8:], dtype=np.dtype([("xy", np.int32, 2), ("rgba", np.float32, 4)]), count=n)
+    return rec["xy"].copy(), rec["rgba"].copy(), stats
+
+
+def ref_hits(scn: str, width: int, height: int, tiles=None, obj_path: str = None, workdir: str = "/tmp"):
+    """Primary-ray closest hits through the reference's Scene::intersection, plus
+    the triangle index from an Octree<Triangle> replica of the mesh."""
+    import tempfile
+    fd, out = tempfile.mkstemp(suffix=".bin", dir=workdir)
+    os.close(fd)
+    tfile = "-"
+    if tiles is not None:
+        fd, tfile = tempfile.mkstemp(suffix=".txt", dir=workdir)
+        with os.fdopen(fd, "w") as fh:
+            fh.write("".join("%d %d %d %d\n" % tuple(t) for t in tiles))
+    cmd = [REF_BIN, "hits", scn, str(width), str(height), tfile, out] + ([obj_path] if obj_path else [])
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("xtref hits failed: %s %s" % (r.stdout, r.stderr))
+    raw = open(out, "rb").read()
+    os.unlink(out)
+    if tfile != "-":
+        os.unlink(tfile)
+    n = int(np.frombuffer(raw[:8], np.int64)[0])
+    nobj = int(np.frombuffer(raw[8:12], np.int32)[0])
+    names = [raw[12 + 64 * i:12 + 64 * (i + 1)].split(b"\0")[0].decode() for i in range(nobj)]
+    off = 12 + 64 * nobj
+    dt = np.dtype([("xy", np.int32, 2), ("hi", np.int32, 3), ("rec", np.float64, 14)])
+    rec = np.frombuffer(raw[off:], dtype=dt, count=n)
+    r = rec["rec"]
+    return dict(xy=rec["xy"].copy(), hit=rec["hi"][:, 0].copy(), obj=rec["hi"][:, 1].copy(),
+                prim=rec["hi"][:, 2].copy(), org=r[:, 0:3].copy(), dir=r[:, 3:6].copy(), t=r[:, 6].copy(),
+                point=r[:, 7:10].copy(), normal=r[:, 10:13].copy(), t_replica=r[:, 13].copy(), names=names)
+
+
+def ref_kat(lines, workdir: str = "/tmp"):
+    """Runs known-answer lines ("kind a b c ...", numbers as hex floats) through
+    the reference functions; returns the output lines split into tokens."""
+    import tempfile
+    fd, fin = tempfile.mkstemp(suffix=".txt", dir=workdir)
+    with os.fdopen(fd, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+    fd, fout = tempfile.mkstemp(suffix=".txt", dir=workdir)
+    os.close(fd)
+    r = subprocess.run([REF_BIN, "kat", fin, fout], capture_output=True, text=True)
+    os.unlink(fin)
+    if r.returncode != 0:
+        raise RuntimeError("xtref kat failed: %s" % r.stderr)
+    res = [ln.split() for ln in open(fout).read().splitlines()]
+    os.unlink(fout)
+    return res

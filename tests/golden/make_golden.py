@@ -1,0 +1,255 @@
+"""Generates the golden fixtures in tests/golden/ by running the REFERENCE
+renderer's own code (XTracer's xtcore compiled from its sources by
+oracle/ref.mk, driven by oracle/ref_driver.cc).
+
+The reference ships no unit tests, golden images or known-answer vectors, so
+these fixtures are what pins the oracle restatement (oracle/xtoracle.c):
+
+* kat.npz     single reference functions on seeded and edge-case inputs
+              (camera, sphere, plane, triangle, AABB, hemisphere, diffuse, lobe,
+              Lambert/Phong/Blinn-Phong/Emissive sample_path, gradient sky),
+              with the libc rand() values each sampling call consumed;
+* hits_*.npz  primary-ray closest hits (object, triangle index from an
+              Octree<Triangle> replica, t, point, normal) on small scenes;
+* render_*.npz stencil/depth frames (deterministic) and AO/pathtracer frames at
+              several seeds (single thread, time() fixed by the driver) for the
+              statistical checks.
+
+Run here (needs the reference sources and oracle/_ref/xtref):
+    make -f oracle/ref.mk REF=<xtracer source tree> -j8
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import pyoracle as po  # noqa: E402
+from xtracer_b200 import scenes  # noqa: E402
+
+H = float.hex
+
+
+def _line(kind, *vals):
+    return " ".join([kind] + [H(float(v)) for v in vals])
+
+
+def _unit(rng, n):
+    v = rng.normal(size=(n, 3))
+    return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+
+def make_kat(rng):
+    out = {}
+    # --- camera (perspective.cc:38-98)
+    cam_in = []
+    for i in range(64):
+        pos = rng.uniform(-20, 20, 3).astype(np.float32)
+        tgt = (pos + rng.uniform(-10, 10, 3)).astype(np.float32)
+        up = np.array([0, 1, 0], np.float32) if i % 4 else rng.uniform(-1, 1, 3).astype(np.float32)
+        fov = np.float32(rng.choice([30.0, 45.0, 60.0, 90.0, 37.5]))
+        w, h = [(256, 256), (1920, 1080), (64, 48), (1024, 1024)][i % 4]
+        x, y = np.float32(rng.integers(0, w) + 0.5), np.float32(rng.integers(0, h) + 0.5)
+        cam_in.append(np.concatenate([pos, tgt, up, [fov, w, h, x, y]]).astype(np.float64))
+    cam_in = np.array(cam_in)
+    res = po.ref_kat([_line("camera", *r) for r in cam_in])
+    out["camera_in"] = cam_in
+    out["camera_out"] = np.array([[float.fromhex(t) for t in r[1:]] for r in res])
+
+    # --- sphere (sphere.cc:35-62)
+    sph = []
+    for i in range(200):
+        c = rng.uniform(-5, 5, 3); r = rng.uniform(0.1, 2.0)
+        if i % 5 == 0:
+            o = c + _unit(rng, 1)[0] * r * 0.5            # origin inside -> miss
+        else:
+            o = c + _unit(rng, 1)[0] * rng.uniform(r * 1.5, 10)
+        if i % 3 == 0:
+            d = c + _unit(rng, 1)[0] * r * 0.7 - o          # towards the sphere
+        else:
+            d = _unit(rng, 1)[0]
+        d = d / np.linalg.norm(d)
+        sph.append(np.concatenate([c, [r], o, d]))
+    sph += [np.array([0, 0, 0, 1, -5, 1, 0, 1, 0, 0.0]),   # tangent: discriminant 0
+            np.array([0, 0, 0, 0, -5, 0, 0, 1, 0, 0.0]),   # radius 0 (point light)
+            np.array([0, 0, 5, 1, 0, 0, 0, 0, 0, 1.0]),    # axis ray
+            np.array([0, 0, -5, 1, 0, 0, 0, 0, 0, 1.0])]   # sphere behind
+    sph = np.array(sph)
+    res = po.ref_kat([_line("sphere", *r) for r in sph])
+    out["sphere_in"] = sph
+    out["sphere_out"] = np.array([[int(r[1])] + [float.fromhex(t) for t in r[2:]] for r in res])
+
+    # --- plane (plane.cc:19-61)
+    pl = []
+    for i in range(100):
+        n = _unit(rng, 1)[0] if i % 4 else np.array([0, 1, 0.0])
+        off = rng.uniform(-3, 3)
+        o = rng.uniform(-5, 5, 3)
+        d = _unit(rng, 1)[0]
+        pl.append(np.concatenate([n, [off], o, d]))
+    pl += [np.array([0, 1, 0, 0, 0, 1, 0, 1, 0, 0.0]),     # parallel
+           np.array([0, 1, 0, 0, 0, -1, 0, 0, 1, 0.0]),    # from below (two-sided)
+           np.array([0, 1, 0, 2, 0, 5, 0, 0, -1, 0.0])]    # offset plane
+    pl = np.array(pl)
+    res = po.ref_kat([_line("plane", *r) for r in pl])
+    out["plane_in"] = pl
+    out["plane_out"] = np.array([[int(r[1])] + [float.fromhex(t) for t in r[2:]] for r in res])
+
+    # --- triangle (triangle.cc:82-184)
+    tri = []
+    for i in range(300):
+        v = rng.uniform(-3, 3, (3, 3))
+        nrm = np.zeros((3, 3)) if i % 3 else _unit(rng, 3)
+        bc = rng.dirichlet([1, 1, 1])
+        if i % 7 == 0:
+            bc = np.array([0.5, 0.5, 0.0])                  # on an edge
+        if i % 11 == 0:
+            bc = np.array([1.0, 0.0, 0.0])                  # on a vertex
+        if i % 13 == 0:
+            bc = np.array([1.2, -0.1, -0.1])                # outside
+        p = bc @ v
+        o = p + _unit(rng, 1)[0] * rng.uniform(0.5, 8)
+        d = (p - o) / np.linalg.norm(p - o)
+        if i % 17 == 0:
+            d = -d                                          # pointing away
+        tri.append(np.concatenate([v.ravel(), nrm.ravel(), o, d]))
+    v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0.0]])
+    tri += [np.concatenate([v.ravel(), np.zeros(9), [0.2, 0.2, -1], [1, 0, 0]]),      # parallel
+            np.concatenate([np.zeros(9), np.zeros(9), [0, 0, -1], [0, 0, 1]])]          # degenerate
+    tri = np.array(tri)
+    res = po.ref_kat([_line("triangle", *r) for r in tri])
+    out["triangle_in"] = tri
+    out["triangle_out"] = np.array([[int(r[1])] + [float.fromhex(t) for t in r[2:]] for r in res])
+
+    # --- AABB slab test (aabb.cc:32-71)
+    bb = []
+    for i in range(300):
+        a = rng.uniform(-3, 3, 3); b = a + rng.uniform(0.01, 3, 3)
+        o = rng.uniform(-6, 6, 3)
+        d = _unit(rng, 1)[0]
+        if i % 5 == 0:
+            d[rng.integers(0, 3)] = 0.0
+            d /= np.linalg.norm(d)
+        if i % 9 == 0:
+            o = (a + b) / 2                                 # inside
+        bb.append(np.concatenate([a, b, o, d]))
+    bb = np.array(bb)
+    res = po.ref_kat([_line("aabb", *r) for r in bb])
+    out["aabb_in"] = bb
+    out["aabb_out"] = np.array([int(r[1]) for r in res])
+
+    # --- sampling with the rand() values they consume
+    seeds = np.arange(1, 97, dtype=np.int64) * 7919
+    res = po.ref_kat(["rand %d 64" % s for s in seeds])
+    out["rand_seeds"] = seeds
+    out["rand_table"] = np.array([[int(t) for t in r[1:65]] for r in res], np.int64)
+    out["rand_max"] = np.int64(int(res[0][65]))
+    nrm = _unit(rng, 96)
+    nrm[0] = [0, 1, 0]; nrm[1] = [0, 0, 1]; nrm[2] = [1, 0, 0]
+    res = po.ref_kat(["hemisphere %d %s %s %s" % (s, H(n[0]), H(n[1]), H(n[2])) for s, n in zip(seeds, nrm)])
+    out["hemisphere_n"] = nrm
+    out["hemisphere_out"] = np.array([[float.fromhex(t) for t in r[1:]] for r in res])
+    res = po.ref_kat(["diffuse %d %s %s %s" % (s, H(n[0]), H(n[1]), H(n[2])) for s, n in zip(seeds, nrm)])
+    out["diffuse_out"] = np.array([[float.fromhex(t) for t in r[1:]] for r in res])
+    dirs = _unit(rng, 96)
+    dirs = np.where((np.sum(dirs * nrm, axis=1) < 0)[:, None], -dirs, dirs)
+    exps = rng.uniform(1, 256, 96)
+    res = po.ref_kat(["lobe %d %s %s %s %s %s %s %s" % ((s,) + tuple(H(x) for x in n) + tuple(H(x) for x in d) + (H(e),))
+                      for s, n, d, e in zip(seeds, nrm, dirs, exps)])
+    out["lobe_d"] = dirs
+    out["lobe_e"] = exps
+    out["lobe_out"] = np.array([[float.fromhex(t) for t in r[1:]] for r in res])
+
+    # --- materials (lambert.cc:30-40, phong.cc:35-55, blinnphong.cc:34-61, emissive.cc:20-27)
+    mat_in = []
+    for i, s in enumerate(seeds):
+        mtype = i % 4
+        cols = rng.uniform(0, 1, 9).astype(np.float32)
+        refl = np.float32(rng.choice([0.0, 0.25, 0.5, 0.75, 1.0]))
+        ex = np.float32(rng.uniform(8, 256))
+        p = rng.uniform(-5, 5, 3)
+        n = nrm[i]
+        inc = -dirs[i]
+        mat_in.append(np.concatenate([[mtype, s], cols, [refl, ex], p, n, inc]))
+    mat_in = np.array(mat_in)
+    res = po.ref_kat([" ".join(["material", str(int(r[0])), str(int(r[1]))] + [H(float(x)) for x in r[2:]])
+                      for r in mat_in])
+    out["material_in"] = mat_in
+    out["material_out"] = np.array([[int(r[1])] + [float.fromhex(t) for t in r[2:]] for r in res])
+
+    # --- gradient environment (sampler_gradient.cc:11-17)
+    g_in = np.concatenate([rng.uniform(0, 1, (64, 6)).astype(np.float32).astype(np.float64), _unit(rng, 64)], axis=1)
+    res = po.ref_kat([_line("gradient", *r) for r in g_in])
+    out["gradient_in"] = g_in
+    out["gradient_out"] = np.array([[float.fromhex(t) for t in r[1:]] for r in res])
+    return out
+
+
+def small_scenes():
+    """Small scenes for the fixtures (names double as fixture names)."""
+    sp = scenes.spheres_scene(64, seed=1, name="spheres64")
+    te = scenes.terrain_scene(20_000, seed=2, name="terrain20k")
+    hb = scenes.hairball_scene(20_000, seed=3, name="hairball20k")
+    return {"spheres64": (sp, 64, 64), "terrain20k": (te, 96, 54), "hairball20k": (hb, 64, 64)}
+
+
+def main():
+    if not po.ref_available():
+        raise SystemExit("oracle/_ref/xtref missing: make -f oracle/ref.mk REF=<xtracer sources>")
+    rng = np.random.default_rng(20261203)
+    kat = make_kat(rng)
+    np.savez_compressed(os.path.join(HERE, "kat.npz"), **kat)
+    print("kat.npz", {k: v.shape for k, v in kat.items()})
+    if "--kat-only" in sys.argv:
+        return
+
+    work = tempfile.mkdtemp(prefix="xtgold")
+    for name, (spec, w, h) in small_scenes().items():
+        scn = spec.write_scn(work)
+        objp = spec.mesh_obj_path(work, 0) if spec.n_tris else None
+        hits = po.ref_hits(scn, w, h, None, objp, workdir=work)
+        names = np.array(hits.pop("names"))
+        np.savez_compressed(os.path.join(HERE, "hits_%s.npz" % name), names=names, width=w, height=h, **hits)
+        print("hits", name, int(hits["hit"].sum()), "hits of", hits["hit"].size)
+        rend = {}
+        for integ, spp in (("stencil", 2), ("depth", 2)):
+            xy, rgba, st = po.ref_render(scn, integ, w, h, spp=spp, threads=1, seed=1, workdir=work)
+            rend["%s_xy" % integ] = xy
+            rend["%s_rgba" % integ] = rgba
+            rend["%s_spp" % integ] = spp
+        # AO: the shipped distance (100) and the hairball workload's 0.2;
+        # four seeds each so the reference's own noise can be estimated.
+        for md in (100.0, 0.2):
+            tag = "ao%g" % md
+            imgs = []
+            for seed in (11, 12, 13, 14):
+                xy, rgba, st = po.ref_render(scn, "ao", w, h, spp=16, threads=1, seed=seed,
+                                             ao_max_distance=md, workdir=work)
+                imgs.append(rgba)
+            rend["%s_xy" % tag] = xy
+            rend["%s_rgba" % tag] = np.stack(imgs)
+            rend["%s_spp" % tag] = 16
+        if name == "spheres64":
+            imgs = []
+            for seed in (21, 22, 23, 24):
+                xy, rgba, st = po.ref_render(scn, "pathtracer", w, h, spp=16, rdepth=4, threads=1, seed=seed,
+                                             workdir=work)
+                imgs.append(rgba)
+                rend["pt_rays_seed%d" % seed] = st["rays"]
+            rend["pt_xy"] = xy
+            rend["pt_rgba"] = np.stack(imgs)
+            rend["pt_spp"] = 16
+            rend["pt_depth"] = 4
+        np.savez_compressed(os.path.join(HERE, "render_%s.npz" % name), width=w, height=h, **rend)
+        print("render", name, sorted(rend))
+
+
+if __name__ == "__main__":
+    main()

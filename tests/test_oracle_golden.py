@@ -1,0 +1,195 @@
+"""Pins the oracle restatement (oracle/xtoracle.c) against fixtures made by the
+reference renderer's own code (tests/golden/make_golden.py).
+
+Deterministic functions must match bit for bit; AO and pathtracer frames use a
+different random source than the reference's libc rand(), so they must agree
+within the reference's own sampling noise at equal spp.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+from xtracer_b200 import scenes
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def P(a):
+    return np.ascontiguousarray(a).ctypes.data_as(C.c_void_p)
+
+
+@pytest.fixture(scope="module")
+def kat():
+    return np.load(os.path.join(GOLD, "kat.npz"))
+
+
+def small_scenes():
+    return {"spheres64": (scenes.spheres_scene(64, seed=1, name="spheres64"), 64, 64),
+            "terrain20k": (scenes.terrain_scene(20_000, seed=2, name="terrain20k"), 96, 54),
+            "hairball20k": (scenes.hairball_scene(20_000, seed=3, name="hairball20k"), 64, 64)}
+
+
+def test_camera_kat(kat):
+    L = po.lib()
+    for r, o in zip(kat["camera_in"], kat["camera_out"]):
+        pos, tgt, up = [(C.c_float * 3)(*r[i:i + 3]) for i in (0, 3, 6)]
+        org = np.zeros(3); d = np.zeros(3)
+        L.xo_camera_ray(C.cast(pos, C.c_void_p), C.cast(tgt, C.c_void_p), C.cast(up, C.c_void_p), r[9],
+                        r[12], r[13], r[10], r[11], P(org), P(d))
+        assert np.array_equal(org, o[:3]) and np.array_equal(d, o[3:])
+
+
+@pytest.mark.parametrize("kind", ["sphere", "plane"])
+def test_sphere_plane_kat(kat, kind):
+    fn = getattr(po.lib(), "xo_kat_" + kind)
+    for r, o in zip(kat[kind + "_in"], kat[kind + "_out"]):
+        out = np.zeros(7)
+        h = fn(P(r[:4]), P(r[4:7]), P(r[7:10]), P(out))
+        assert h == o[0]
+        if h:
+            assert np.array_equal(out, o[1:])
+
+
+def test_triangle_kat(kat):
+    L = po.lib()
+    for r, o in zip(kat["triangle_in"], kat["triangle_out"]):
+        out = np.zeros(7)
+        h = L.xo_kat_triangle(P(r[:9]), P(r[9:18]), P(r[18:21]), P(r[21:24]), P(out))
+        assert h == o[0]
+        if h:
+            assert np.array_equal(out, o[1:])
+
+
+def test_aabb_kat(kat):
+    L = po.lib()
+    got = [L.xo_kat_aabb(P(r[0:3]), P(r[3:6]), P(r[6:9]), P(r[9:12])) for r in kat["aabb_in"]]
+    assert np.array_equal(np.array(got), kat["aabb_out"])
+
+
+def test_sampling_kat(kat):
+    """hemisphere / diffuse / lobe consume the same libc rand() values as the
+    reference and return the same bits (sample.inl:28-107)."""
+    L = po.lib()
+    tab = kat["rand_table"].astype(np.int32)
+    rm = int(kat["rand_max"])
+    for i in range(tab.shape[0]):
+        out = np.zeros(3)
+        L.xo_kat_hemisphere(P(tab[i]), rm, P(kat["hemisphere_n"][i]), P(out))
+        assert np.array_equal(out, kat["hemisphere_out"][i])
+        L.xo_kat_diffuse(P(tab[i]), rm, P(kat["hemisphere_n"][i]), P(out))
+        assert np.array_equal(out, kat["diffuse_out"][i])
+        L.xo_kat_lobe(P(tab[i]), rm, P(kat["hemisphere_n"][i]), P(kat["lobe_d"][i]), kat["lobe_e"][i], P(out))
+        assert np.array_equal(out, kat["lobe_out"][i])
+
+
+def test_material_kat(kat):
+    L = po.lib()
+    tab = kat["rand_table"].astype(np.int32)
+    rm = int(kat["rand_max"])
+    for i, (r, o) in enumerate(zip(kat["material_in"], kat["material_out"])):
+        m = po.XoMaterial()
+        m.type = int(r[0]); m.diffuse[:] = list(r[2:5]); m.specular[:] = list(r[5:8])
+        m.emissive[:] = list(r[8:11]); m.reflectance = r[11]; m.exponent = r[12]
+        out = np.zeros(9)
+        cont = L.xo_kat_material(C.byref(m), P(tab[i]), rm, P(r[13:16]), P(r[16:19]), P(r[19:22]), P(out))
+        assert cont == o[0]
+        assert np.array_equal(out[6:], o[7:])
+        if cont:
+            assert np.array_equal(out[:6], o[1:7])
+
+
+def test_gradient_kat(kat):
+    L = po.lib()
+    for r, o in zip(kat["gradient_in"], kat["gradient_out"]):
+        a = (C.c_float * 3)(*r[0:3]); b = (C.c_float * 3)(*r[3:6]); out = np.zeros(3, np.float32)
+        L.xo_kat_gradient(C.cast(a, C.c_void_p), C.cast(b, C.c_void_p), P(r[6:9]), P(out))
+        assert np.array_equal(out.astype(np.float64), o)
+
+
+@pytest.mark.parametrize("name", ["spheres64", "terrain20k", "hairball20k"])
+@pytest.mark.parametrize("accel", [po.XO_ACCEL_OCTREE, po.XO_ACCEL_BVH])
+def test_primary_hits_golden(name, accel):
+    """Closest hit, object, triangle index (octree item), t, point and normal of
+    every primary ray equal the reference's (scene.cc:191-216, octree.tml:206-249)."""
+    spec, w, h = small_scenes()[name]
+    g = np.load(os.path.join(GOLD, "hits_%s.npz" % name))
+    assert list(g["names"]) == ["o%05d" % i for i in range(len(spec.obj_kind))]
+    sc = po.OracleScene(spec, accel)
+    org, d = po.camera_rays(spec, w, h, g["xy"])
+    assert np.array_equal(org, g["org"]) and np.array_equal(d, g["dir"])
+    r = sc.trace(org, d)
+    m = g["hit"] == 1
+    assert np.array_equal(r["hit"], g["hit"])
+    assert np.array_equal(r["t"][m], g["t"][m])
+    assert np.array_equal(r["obj"][m], g["obj"][m])
+    assert np.array_equal(r["point"][m], g["point"][m])
+    assert np.array_equal(r["normal"][m], g["normal"][m])
+    if spec.n_tris:
+        pm = m & (g["prim"] >= 0)
+        assert np.array_equal(r["prim"][pm] - spec.obj_first[r["obj"][pm]], g["prim"][pm])
+
+
+@pytest.mark.parametrize("name", ["spheres64", "terrain20k", "hairball20k"])
+@pytest.mark.parametrize("integ", ["stencil", "depth"])
+def test_deterministic_frames_golden(name, integ):
+    spec, w, h = small_scenes()[name]
+    g = np.load(os.path.join(GOLD, "render_%s.npz" % name))
+    sc = po.OracleScene(spec, po.XO_ACCEL_OCTREE)
+    kind = po.STENCIL if integ == "stencil" else po.DEPTH
+    img, rays = sc.render(kind, w, h, spp=int(g[integ + "_spp"]), pixels=g[integ + "_xy"])
+    assert np.array_equal(img, g[integ + "_rgba"])
+    assert rays == w * h * int(g[integ + "_spp"])
+
+
+def _rmse(a, b):
+    return float(np.sqrt(np.mean((a[:, :3] - b[:, :3]) ** 2)))
+
+
+def stochastic_agreement(O, R):
+    """Leave-one-out comparison: the oracle frame against the mean of 3 reference
+    frames, next to each reference frame against the mean of the other 3."""
+    n = R.shape[0]
+    ref = np.mean([_rmse(R[i], R[[j for j in range(n) if j != i]].mean(0)) for i in range(n)])
+    got = np.mean([_rmse(O, R[[j for j in range(n) if j != i]].mean(0)) for i in range(n)])
+    return got, ref
+
+
+@pytest.mark.parametrize("name,key,integ,md", [
+    ("spheres64", "ao100", po.AO, 100.0), ("spheres64", "ao0.2", po.AO, 0.2),
+    ("terrain20k", "ao100", po.AO, 100.0), ("terrain20k", "ao0.2", po.AO, 0.2),
+    ("hairball20k", "ao100", po.AO, 100.0), ("hairball20k", "ao0.2", po.AO, 0.2),
+    ("spheres64", "pt", po.PATHTRACER, 100.0)])
+def test_stochastic_frames_within_reference_noise(name, key, integ, md):
+    spec, w, h = small_scenes()[name]
+    g = np.load(os.path.join(GOLD, "render_%s.npz" % name))
+    sc = po.OracleScene(spec, po.XO_ACCEL_BVH)
+    O, rays = sc.render(integ, w, h, spp=int(g[key + "_spp"]), rdepth=4, ao_max_distance=md, seed=777,
+                        pixels=g[key + "_xy"])
+    R = g[key + "_rgba"]
+    got, ref = stochastic_agreement(O, R)
+    assert got <= 1.25 * ref + 1e-6, (got, ref)
+    # No bias in the frame mean beyond 4.5 standard errors.  The standard error
+    # comes from the per-pixel variance between the reference frames (one
+    # channel: AO writes the same value to r, g and b); O - mean(R) has variance
+    # se^2 (1 + 1/n).
+    n = R.shape[0]
+    for ch in range(3):
+        diff = O[:, ch] - R[:, :, ch].mean(0)
+        se = np.sqrt(R[:, :, ch].var(0, ddof=1).mean() / diff.size * (1 + 1.0 / n))
+        assert abs(diff.mean()) < 4.5 * se + 1e-5, (ch, diff.mean(), se)
+    if key == "pt":
+        ref_rays = [int(g["pt_rays_seed%d" % s]) for s in (21, 22, 23, 24)]
+        assert abs(rays - np.mean(ref_rays)) < 5 * np.std(ref_rays) + 0.005 * np.mean(ref_rays)
+
+
+def test_stream_rng_is_uniform():
+    """The counter stream (SplitMix64 finaliser) shared with the GPU path."""
+    k = po.path_key(1234, 99)
+    u = np.array([po.stream_uniform(k, i) for i in range(20000)])
+    assert u.min() >= 0.0 and u.max() < 1.0
+    assert abs(u.mean() - 0.5) < 0.01
+    assert abs(u.var() - 1 / 12) < 0.005
+    assert np.all(u * 16777216.0 == np.floor(u * 16777216.0))

@@ -1,0 +1,381 @@
+"""Seeded synthetic scenes and job streams for the ray-intersection hot path.
+
+Every scene is produced from a seed and held as flat float32 arrays (the layout
+the C ABI takes, include/xtgpu.h).  The same scene can be written as an XTracer
+``.scn`` file (+ ``.obj`` for meshes) so the reference renderer loads exactly the
+same numbers:
+
+* all coordinates are rounded to dyadic grids (2^-16 for |x| < 128, 2^-22 inside
+  the unit ball), so each value is an exact float32 whose shortest decimal form
+  parses back to the same float in the reference's ``sscanf("%f")`` /
+  ``strtod`` / tinyobj readers;
+* object names are zero-padded (``o00000``...), so the reference's std::map
+  iteration order (src/xtcore/scene.cc:191-216) is the order used here.
+
+No public dataset is used; the reference's own sample meshes (scene/data/) are
+absent from its repository anyway.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import os
+from typing import List, Optional
+
+import numpy as np
+
+SPHERE, PLANE, MESH = 0, 1, 2
+LAMBERT, PHONG, BLINNPHONG, EMISSIVE, DIELECTRIC = 0, 1, 2, 3, 4
+ENV_NONE, ENV_COLOR, ENV_GRADIENT = 0, 1, 2
+MATERIAL_NAMES = {LAMBERT: "lambert", PHONG: "phong", BLINNPHONG: "blinn_phong",
+                  EMISSIVE: "emissive", DIELECTRIC: "dielectric"}
+
+
+@dataclasses.dataclass
+class Material:
+    type: int = LAMBERT
+    diffuse: tuple = (0.0, 0.0, 0.0)
+    specular: tuple = (0.0, 0.0, 0.0)
+    emissive: tuple = (0.0, 0.0, 0.0)
+    reflectance: float = 0.0
+    exponent: float = 0.0
+    ior: float = 1.0
+
+
+@dataclasses.dataclass
+class Camera:
+    position: tuple = (0.0, 0.0, -10.0)
+    target: tuple = (0.0, 0.0, 0.0)
+    up: tuple = (0.0, 1.0, 0.0)
+    fov: float = 60.0
+
+
+@dataclasses.dataclass
+class SceneSpec:
+    """Flat scene: objects in intersection order, each a sphere, a plane or a
+    mesh (a contiguous range of triangles)."""
+    name: str
+    spheres: np.ndarray            # (S, 4) float32: cx cy cz r
+    planes: np.ndarray             # (P, 4) float32: nx ny nz offset
+    tris: np.ndarray               # (T, 3, 3) float32, OBJ face order per mesh
+    obj_kind: np.ndarray           # (O,) int32
+    obj_first: np.ndarray          # (O,) int32
+    obj_count: np.ndarray          # (O,) int32
+    obj_material: np.ndarray       # (O,) int32
+    materials: List[Material]
+    camera: Camera
+    env_type: int = ENV_NONE
+    env_a: tuple = (0.0, 0.0, 0.0)
+    env_b: tuple = (0.0, 0.0, 0.0)
+    tri_normals: Optional[np.ndarray] = None
+    # mesh vertex/index form for writing OBJ (per mesh object): list of (verts, faces)
+    mesh_obj: Optional[list] = None
+
+    @property
+    def n_tris(self) -> int:
+        return int(self.tris.shape[0])
+
+    @property
+    def n_prims(self) -> int:
+        return int(self.tris.shape[0] + self.spheres.shape[0] + self.planes.shape[0])
+
+    # ------------------------------------------------------------------
+    def write_scn(self, directory: str) -> str:
+        """Writes ``<name>.scn`` (+ one OBJ per mesh) in the reference's NCF
+        format (src/xtcore/proto.h, parseutil.cc:697-822).  Returns the path."""
+        os.makedirs(directory, exist_ok=True)
+        f = lambda v: repr(float(v))
+        v3 = lambda v: "vec3(%s,%s,%s)" % (f(v[0]), f(v[1]), f(v[2]))
+        c3 = lambda v: "col3(%s,%s,%s)" % (f(v[0]), f(v[1]), f(v[2]))
+        out = ["title = %s" % self.name, "version = 1.0", ""]
+        if self.env_type == ENV_GRADIENT:
+            out += ["environment = {", "  type = gradient", "  config = {",
+                    "    a = %s" % c3(self.env_a), "    b = %s" % c3(self.env_b), "  }", "}"]
+        elif self.env_type == ENV_COLOR:
+            out += ["environment = {", "  type = color", "  config = {",
+                    "    value = %s" % c3(self.env_a), "  }", "}"]
+        cam = self.camera
+        out += ["camera = {", "  default = {", "    type = thin-lens",
+                "    position = %s" % v3(cam.position), "    target = %s" % v3(cam.target),
+                "    up = %s" % v3(cam.up), "    fov = %s" % f(cam.fov), "  }", "}"]
+        out.append("geometry = {")
+        mesh_i = 0
+        for oi in range(len(self.obj_kind)):
+            k, first = int(self.obj_kind[oi]), int(self.obj_first[oi])
+            gname = "g%05d" % oi
+            if k == SPHERE:
+                s = self.spheres[first]
+                out += ["  %s = {" % gname, "    type = sphere", "    position = %s" % v3(s[:3]),
+                        "    radius = %s" % f(s[3]), "  }"]
+            elif k == PLANE:
+                p = self.planes[first]
+                out += ["  %s = {" % gname, "    type = plane", "    normal = %s" % v3(p[:3]),
+                        "    distance = %s" % f(p[3]), "  }"]
+            else:
+                objname = "%s_m%02d.obj" % (self.name, mesh_i)
+                self._write_obj(os.path.join(directory, objname), mesh_i, first, int(self.obj_count[oi]))
+                mesh_i += 1
+                out += ["  %s = {" % gname, "    type = mesh", "    source = %s" % objname, "  }"]
+        out.append("}")
+        out.append("material = {")
+        for mi, m in enumerate(self.materials):
+            out += ["  m%05d = {" % mi, "    type = %s" % MATERIAL_NAMES[m.type], "    properties = {",
+                    "      samplers = {"]
+            for key in ("diffuse", "specular", "emissive"):
+                out += ["        %s = {" % key, "          type = color",
+                        "          value = %s" % c3(getattr(m, key)), "        }"]
+            out += ["      }", "      scalars = {", "        reflectance = %s" % f(m.reflectance),
+                    "        exponent = %s" % f(m.exponent), "        ior = %s" % f(m.ior),
+                    "      }", "    }", "  }"]
+        out.append("}")
+        out.append("object = {")
+        for oi in range(len(self.obj_kind)):
+            out += ["  o%05d = {" % oi, "    geometry = g%05d" % oi,
+                    "    material = m%05d" % int(self.obj_material[oi]), "  }"]
+        out.append("}")
+        path = os.path.join(directory, self.name + ".scn")
+        with open(path, "w") as fh:
+            fh.write("\n".join(out) + "\n")
+        return path
+
+    def mesh_obj_path(self, directory: str, mesh_index: int = 0) -> str:
+        return os.path.join(directory, "%s_m%02d.obj" % (self.name, mesh_index))
+
+    def _write_obj(self, path: str, mesh_i: int, first: int, count: int) -> None:
+        if self.mesh_obj is not None and mesh_i < len(self.mesh_obj) and self.mesh_obj[mesh_i] is not None:
+            verts, faces = self.mesh_obj[mesh_i]
+        else:
+            verts = self.tris[first:first + count].reshape(-1, 3)
+            faces = np.arange(count * 3, dtype=np.int64).reshape(-1, 3)
+        with open(path, "w") as fh:
+            fh.write("".join("v %r %r %r\n" % (float(a), float(b), float(c)) for a, b, c in verts.tolist()))
+            fh.write("".join("f %d %d %d\n" % (a + 1, b + 1, c + 1) for a, b, c in faces.tolist()))
+
+
+# ----------------------------------------------------------------------
+def _q(x, step_log2: int) -> np.ndarray:
+    """Round to a dyadic grid so the value is an exact float32."""
+    s = float(2.0 ** step_log2)
+    return (np.round(np.asarray(x, dtype=np.float64) * s) / s).astype(np.float32)
+
+
+def _qs(x, step_log2: int = 16) -> float:
+    return float(_q(np.array([x]), step_log2)[0])
+
+
+def _objects(kinds, firsts, counts, mats):
+    return (np.asarray(kinds, np.int32), np.asarray(firsts, np.int32),
+            np.asarray(counts, np.int32), np.asarray(mats, np.int32))
+
+
+def spheres_scene(n_spheres: int = 64, seed: int = 1, extent: float = 5.0, name: str = None,
+                  with_light: bool = True, camera: Camera = None) -> SceneSpec:
+    """Ground plane y=0 plus `n_spheres` Lambert spheres: centres uniform in
+    [-e,e]x[0.5,4]x[-e,e], radii uniform in [0.2,0.8], albedo uniform in
+    [0.1,0.9]^3; a point light at (0,10,0) of intensity 100 (loaded by the
+    reference as a radius-0 sphere, parseutil.cc:379-383) and a gradient sky."""
+    rng = np.random.default_rng(seed)
+    c = np.stack([rng.uniform(-extent, extent, n_spheres), rng.uniform(0.5, 4.0, n_spheres),
+                  rng.uniform(-extent, extent, n_spheres)], axis=1)
+    r = rng.uniform(0.2, 0.8, n_spheres)
+    alb = rng.uniform(0.1, 0.9, (n_spheres, 3))
+    sph = np.concatenate([_q(c, 16), _q(r[:, None], 16)], axis=1).astype(np.float32)
+    mats = [Material(LAMBERT, diffuse=(0.5, 0.5, 0.5))]
+    for i in range(n_spheres):
+        a = _q(alb[i], 16)
+        mats.append(Material(LAMBERT, diffuse=(float(a[0]), float(a[1]), float(a[2]))))
+    kinds, firsts, counts, omat = [PLANE], [0], [1], [0]
+    for i in range(n_spheres):
+        kinds.append(SPHERE); firsts.append(i); counts.append(1); omat.append(i + 1)
+    if with_light:
+        sph = np.concatenate([sph, np.array([[0.0, 10.0, 0.0, 0.0]], np.float32)], axis=0)
+        mats.append(Material(EMISSIVE, emissive=(100.0, 100.0, 100.0)))
+        kinds.append(SPHERE); firsts.append(n_spheres); counts.append(1); omat.append(len(mats) - 1)
+    planes = np.array([[0.0, 1.0, 0.0, 0.0]], np.float32)
+    k, f, cnt, om = _objects(kinds, firsts, counts, omat)
+    cam = camera or Camera((0.0, 6.0, -14.0), (0.0, 1.0, 0.0), (0.0, 1.0, 0.0), 60.0)
+    if camera is None and extent > 5.0:
+        cam = Camera((0.0, 2.5 * extent, -3.0 * extent), (0.0, 1.0, 0.0), (0.0, 1.0, 0.0), 60.0)
+    return SceneSpec(name or ("spheres%d" % n_spheres), sph, planes, np.zeros((0, 3, 3), np.float32),
+                     k, f, cnt, om, mats, cam, ENV_GRADIENT, (1.0, 1.0, 1.0), (0.5, 0.7, 1.0))
+
+
+def _value_noise(x: np.ndarray, z: np.ndarray, lattice: np.ndarray) -> np.ndarray:
+    """Value noise with smoothstep interpolation on a periodic random lattice."""
+    L = lattice.shape[0]
+    xi = np.floor(x); zi = np.floor(z)
+    fx = x - xi; fz = z - zi
+    sx = fx * fx * (3 - 2 * fx); sz = fz * fz * (3 - 2 * fz)
+    i0 = xi.astype(np.int64) % L; j0 = zi.astype(np.int64) % L
+    i1 = (i0 + 1) % L; j1 = (j0 + 1) % L
+    a = lattice[i0, j0]; b = lattice[i1, j0]; c = lattice[i0, j1]; d = lattice[i1, j1]
+    return (a * (1 - sx) + b * sx) * (1 - sz) + (c * (1 - sx) + d * sx) * sz
+
+
+def terrain_mesh(grid: int = 708, seed: int = 2, half: float = 50.0, amplitude: float = 8.0,
+                 octaves: int = 6, base_freq: float = 1.0 / 16.0, offset=(0.0, 0.0)):
+    """Height field over [-half,half]^2 on a grid x grid vertex lattice:
+    height = sum_{o<octaves} amplitude * 2^-o * valuenoise(2^o * base_freq * (x,z)).
+    Returns (verts (V,3) float32, faces (F,3) int64) with 2 triangles per quad in
+    row-major order."""
+    rng = np.random.default_rng(seed)
+    lattices = [rng.uniform(-1.0, 1.0, (64, 64)) for _ in range(octaves)]
+    lin = np.linspace(-half, half, grid)
+    X, Z = np.meshgrid(lin + offset[0], lin + offset[1], indexing="xy")
+    H = np.zeros_like(X)
+    for o in range(octaves):
+        fq = (2.0 ** o) * base_freq
+        H += amplitude * (2.0 ** -o) * _value_noise(X * fq, Z * fq, lattices[o])
+    verts = np.stack([_q(X, 16), _q(H, 16), _q(Z, 16)], axis=-1).reshape(-1, 3).astype(np.float32)
+    idx = np.arange(grid * grid, dtype=np.int64).reshape(grid, grid)
+    a = idx[:-1, :-1].ravel(); b = idx[:-1, 1:].ravel(); c = idx[1:, :-1].ravel(); d = idx[1:, 1:].ravel()
+    faces = np.empty((a.size * 2, 3), np.int64)
+    faces[0::2] = np.stack([a, b, c], axis=1)
+    faces[1::2] = np.stack([b, d, c], axis=1)
+    return verts, faces
+
+
+def grid_for_tris(n_tris: int) -> int:
+    return 1 + int(round(math.sqrt(n_tris / 2.0)))
+
+
+def terrain_scene(n_tris: int = 999_698, seed: int = 2, name: str = None) -> SceneSpec:
+    """Config-2 terrain: ~n_tris triangles (708^2 grid gives 999,698) of 6-octave
+    value noise, amplitude 8, over [-50,50]^2, one Lambert mesh, gradient sky."""
+    grid = grid_for_tris(n_tris)
+    verts, faces = terrain_mesh(grid, seed)
+    tris = verts[faces]
+    k, f, cnt, om = _objects([MESH], [0], [tris.shape[0]], [0])
+    cam = Camera((0.0, 30.0, -75.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 60.0)
+    return SceneSpec(name or ("terrain%d" % tris.shape[0]), np.zeros((0, 4), np.float32),
+                     np.zeros((0, 4), np.float32), tris.astype(np.float32), k, f, cnt, om,
+                     [Material(LAMBERT, diffuse=(0.6, 0.5, 0.4))], cam, ENV_GRADIENT,
+                     (1.0, 1.0, 1.0), (0.5, 0.7, 1.0), mesh_obj=[(verts, faces)])
+
+
+def hairball_tris(n_tris: int = 2_000_000, seed: int = 3, edge: float = 0.01, radius: float = 1.0,
+                  center=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """Equilateral triangles of the given edge, centroids uniform in a ball,
+    orientations from uniform random quaternions (Shoemake 1992)."""
+    rng = np.random.default_rng(seed)
+    u = rng.normal(size=(n_tris, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    rad = radius * rng.uniform(0.0, 1.0, n_tris) ** (1.0 / 3.0)
+    cen = u * rad[:, None] + np.asarray(center)[None, :]
+    r1, r2, r3 = rng.uniform(0, 1, (3, n_tris))
+    q = np.stack([np.sqrt(1 - r1) * np.sin(2 * np.pi * r2), np.sqrt(1 - r1) * np.cos(2 * np.pi * r2),
+                  np.sqrt(r1) * np.sin(2 * np.pi * r3), np.sqrt(r1) * np.cos(2 * np.pi * r3)], axis=1)
+    x, y, z, w = q.T
+    R = np.stack([np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+                  np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+                  np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1)], axis=1)
+    cr = edge / math.sqrt(3.0)
+    ang = np.array([0.0, 2 * np.pi / 3, 4 * np.pi / 3])
+    local = np.stack([cr * np.cos(ang), cr * np.sin(ang), np.zeros(3)], axis=1)   # (3,3)
+    v = cen[:, None, :] + np.einsum("nij,kj->nki", R, local)
+    scale_log2 = 22 if (radius + abs(max(center, key=abs)) + edge) < 2.0 else 16
+    return _q(v, scale_log2).astype(np.float32)
+
+
+def hairball_scene(n_tris: int = 2_000_000, seed: int = 3, name: str = None) -> SceneSpec:
+    """Config-3 hairball: n_tris equilateral triangles (edge 0.01) with centroids
+    uniform in the unit ball, one Lambert mesh, gradient sky."""
+    tris = hairball_tris(n_tris, seed)
+    k, f, cnt, om = _objects([MESH], [0], [tris.shape[0]], [0])
+    cam = Camera((0.0, 0.0, -3.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 45.0)
+    return SceneSpec(name or ("hairball%d" % n_tris), np.zeros((0, 4), np.float32),
+                     np.zeros((0, 4), np.float32), tris, k, f, cnt, om,
+                     [Material(LAMBERT, diffuse=(0.8, 0.8, 0.8))], cam, ENV_GRADIENT,
+                     (1.0, 1.0, 1.0), (0.5, 0.7, 1.0))
+
+
+def precision_scene(scale: float = 1.0, seed: int = 5) -> SceneSpec:
+    """Config-5 scene: 8 displaced terrain tiles + 4 hairballs (8M triangles at
+    scale 1), Phong / Blinn-Phong materials with exponent uniform in [8,256] and
+    reflectance 0.5, one emissive sphere and one 200-triangle emissive mesh."""
+    rng = np.random.default_rng(seed)
+    tile_tris = max(2, int(500_000 * scale))
+    hb_tris = max(1, int(1_000_000 * scale))
+    chunks, kinds, firsts, counts, omat, mats = [], [], [], [], [], []
+    first = 0
+    for t in range(8):
+        ox, oz = (t % 4) * 100.0 - 150.0, (t // 4) * 100.0 - 50.0
+        verts, faces = terrain_mesh(grid_for_tris(tile_tris), seed * 100 + t, offset=(ox, oz))
+        tri = verts[faces]
+        chunks.append(tri); kinds.append(MESH); firsts.append(first); counts.append(tri.shape[0])
+        mats.append(Material(PHONG if t % 2 == 0 else BLINNPHONG, diffuse=(0.6, 0.55, 0.5),
+                             specular=(0.9, 0.9, 0.9), reflectance=0.5,
+                             exponent=_qs(rng.uniform(8, 256), 8)))
+        omat.append(len(mats) - 1); first += tri.shape[0]
+    for h in range(4):
+        c = ((h % 2) * 100.0 - 50.0, 12.0, (h // 2) * 60.0 - 30.0)
+        tri = hairball_tris(hb_tris, seed * 1000 + h, edge=0.1, radius=8.0, center=c)
+        chunks.append(tri); kinds.append(MESH); firsts.append(first); counts.append(tri.shape[0])
+        mats.append(Material(BLINNPHONG if h % 2 == 0 else PHONG, diffuse=(0.7, 0.7, 0.7),
+                             specular=(1.0, 1.0, 1.0), reflectance=0.5,
+                             exponent=_qs(rng.uniform(8, 256), 8)))
+        omat.append(len(mats) - 1); first += tri.shape[0]
+    # 200-triangle emissive mesh: a 10x10 quad grid above the scene
+    g = np.linspace(-20.0, 20.0, 11)
+    X, Z = np.meshgrid(g, g, indexing="xy")
+    lv = np.stack([X, np.full_like(X, 60.0), Z], -1).reshape(-1, 3)
+    idx = np.arange(121).reshape(11, 11)
+    a = idx[:-1, :-1].ravel(); b = idx[:-1, 1:].ravel(); cc = idx[1:, :-1].ravel(); d = idx[1:, 1:].ravel()
+    lf = np.empty((200, 3), np.int64); lf[0::2] = np.stack([a, b, cc], 1); lf[1::2] = np.stack([b, d, cc], 1)
+    ltri = _q(lv, 16)[lf]
+    chunks.append(ltri); kinds.append(MESH); firsts.append(first); counts.append(200)
+    mats.append(Material(EMISSIVE, emissive=(20.0, 20.0, 20.0))); omat.append(len(mats) - 1)
+    first += 200
+    sph = np.array([[30.0, 40.0, 0.0, 6.0]], np.float32)
+    kinds.append(SPHERE); firsts.append(0); counts.append(1)
+    mats.append(Material(EMISSIVE, emissive=(40.0, 38.0, 30.0))); omat.append(len(mats) - 1)
+    tris = np.concatenate(chunks, axis=0).astype(np.float32)
+    k, f, cnt, om = _objects(kinds, firsts, counts, omat)
+    cam = Camera((0.0, 60.0, -160.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), 60.0)
+    return SceneSpec("precision8m" if scale == 1.0 else "precision_s%g" % scale, sph,
+                     np.zeros((0, 4), np.float32), tris, k, f, cnt, om, mats, cam, ENV_NONE)
+
+
+# ----------------------------------------------------------------------
+JOBSTREAM_SCENES = [("terrain10k", 10_000), ("terrain50k", 50_000), ("terrain200k", 200_000),
+                    ("terrain500k", 500_000), ("terrain1m", 1_000_000), ("hairball2m", 2_000_000),
+                    ("spheres64", 64), ("spheres4096", 4096)]
+
+
+def jobstream_scene(name: str, scale: float = 1.0) -> SceneSpec:
+    """The 8 resident scenes of the served job stream (terrain and hairball
+    generators at 10k..2M triangles, plus 64- and 4096-sphere scenes)."""
+    n = dict(JOBSTREAM_SCENES)[name]
+    if name.startswith("terrain"):
+        return terrain_scene(max(8, int(n * scale)), seed=40 + int(math.log2(n)), name=name)
+    if name.startswith("hairball"):
+        return hairball_scene(max(8, int(n * scale)), seed=43, name=name)
+    if n == 64:
+        return spheres_scene(64, seed=44, name=name)
+    return spheres_scene(n, seed=45, extent=40.0, name=name)
+
+
+@dataclasses.dataclass
+class Job:
+    job_id: int
+    scene: int          # index into the resident scene list
+    width: int
+    height: int
+    spp: int
+    depth: int
+    arrival_s: float
+    seed: int
+
+
+def job_stream(n_jobs: int = 512, seed: int = 4, rate_hz: float = 50.0, n_scenes: int = 8,
+               resolutions=(128, 256, 512, 1024), spps=(1, 4, 16, 64), depth: int = 4) -> List[Job]:
+    """Poisson arrivals at `rate_hz`; resolution and spp uniform over the given
+    sets, scene uniform over the resident scenes, pathtracer depth 4."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate_hz, n_jobs)
+    t = np.cumsum(gaps) - gaps[0]
+    jobs = []
+    for i in range(n_jobs):
+        r = int(rng.choice(resolutions)); s = int(rng.choice(spps)); sc = int(rng.integers(0, n_scenes))
+        jobs.append(Job(i, sc, r, r, s, depth, float(t[i]), int(rng.integers(1, 2 ** 62))))
+    return jobs
