@@ -1,0 +1,429 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 ray-intersection / integrator backend on the served
+job stream: 8 resident scenes (terrain 10k..1M triangles, a 2M-triangle
+hairball, 64 and 4096 spheres), 512 seeded jobs with resolution in
+{128,256,512,1024}^2, spp in {1,4,16,64}, pathtracer depth 4.
+
+A step is one slice of 64 jobs of that stream, all submitted at once and run
+to completion through the render service (merged waves, 8-bit quantised BVH,
+CUDA graphs).  Reported beside it, on the same jobs: the plain path (one job per
+launch, FP32 BVH, no graphs), an end-to-end pass with every frame copied back
+to host memory, open-loop p50/p99 latency under Poisson arrivals, the extend
+kernel's roofline and the reference CPU renderer on the host cores.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python -m torch.distributed.run --nproc-per-node N ... bench.py --gpus N
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = ("jobstream-512: 8 resident scenes (terrain 10k/50k/200k/500k/1M tris, hairball 2M tris, "
+            "64 and 4096 spheres), jobs res {128,256,512,1024}^2 x spp {1,4,16,64}, pathtracer depth 4")
+METRIC = "Mrays/s of the served job stream (merged waves, q8 BVH, CUDA graphs); p50/p99 job latency"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="xtgpu", choices=["xtgpu", "reference"])
+    ap.add_argument("--jobs-per-step", type=int, default=64)
+    ap.add_argument("--scale", type=float, default=1.0, help="scene size scale (1.0 = the workload)")
+    ap.add_argument("--stream-jobs", type=int, default=512)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-latency", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Dist:
+    def __init__(self, world, use_cuda):
+        self.world = world
+        self.pg = None
+        if world > 1:
+            import datetime
+            import torch.distributed as dist
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            dist.init_process_group("nccl" if use_cuda else "gloo", timeout=datetime.timedelta(seconds=120))
+            self.dist = dist
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, x):
+        if self.world == 1:
+            return x
+        import torch
+        t = torch.tensor([float(x)], device="cuda" if torch.cuda.is_available() else "cpu")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x):
+        if self.world == 1:
+            return x
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+def build_scenes(scale):
+    from xtracer_b200 import scenes, xtgpu
+    out, specs = [], []
+    for name, _ in scenes.JOBSTREAM_SCENES:
+        spec = scenes.jobstream_scene(name, scale)
+        specs.append(spec)
+        out.append(xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8)))
+    return specs, out
+
+
+def run_slice(svc, jobs, record=None, per_scene=None):
+    """Submits the jobs at once, runs the service to completion; returns
+    (rays, latencies in s).  per_scene (array) accumulates rays by scene."""
+    from xtracer_b200 import xtgpu
+    ids = [svc.submit(j.scene, xtgpu.PATHTRACER, j.width, j.height, j.spp, j.depth, 100.0, j.seed) for j in jobs]
+    svc.run()
+    rays, lat = 0, []
+    for j, i in zip(jobs, ids):
+        st = svc.poll(i)
+        if st.state != 2:
+            raise RuntimeError("job %d did not finish (state %d)" % (i, st.state))
+        rays += st.rays
+        if per_scene is not None:
+            per_scene[j.scene] += st.rays
+        lat.append(st.finish_s - st.submit_s)
+        if record is not None:
+            record.append(svc.result(i))
+        svc.release(i)
+    return rays, lat
+
+
+def pct(v, q):
+    return float(np.percentile(np.asarray(v), q)) if len(v) else None
+
+
+def roofline_bytes_per_ray(specs, gpu_scenes, node_format):
+    """Algorithmic bytes per ray of the extend kernel, per scene:
+    32 (ray) + 16 (hit) + nodes_visited * node_bytes + prims_tested * 48, with
+    the visit counts measured once per scene by a counting traversal over a
+    pathtracer job of that scene (128^2 x 4 spp, depth 4)."""
+    from xtracer_b200 import xtgpu
+    from xtracer_b200.service import Service
+    node_bytes = 32 if node_format == xtgpu.NODES_Q8 else 64
+    out = []
+    for k, sc in enumerate(gpu_scenes):
+        svc = Service(gpu_scenes, node_format=node_format, count_visits=True)
+        jid = svc.submit(k, xtgpu.PATHTRACER, 128, 128, 4, 4, 100.0, 12345)
+        svc.run()
+        st = svc.stats()
+        svc.release(jid)
+        svc.close()
+        vn = st.node_visits / max(st.rays, 1)
+        vp = st.prim_tests / max(st.rays, 1)
+        out.append({"scene": specs[k].name, "nodes_per_ray": vn, "prims_per_ray": vp,
+                    "bytes_per_ray": 32 + 16 + vn * node_bytes + vp * 48})
+    return out
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_sample(scale, threads, budget_s=20.0):
+    """The reference renderer (oracle/_ref/xtref, XTracer's xtcore built from its
+    sources) on the host cores: pathtracer depth 4 over crops of stream jobs on
+    the scenes it loads quickly (spheres64, spheres4096, terrain10k,
+    terrain50k).  The octree build of the larger meshes alone takes minutes, so
+    they are left out of the sample."""
+    from oracle import pyoracle as po
+    from xtracer_b200 import scenes
+    if not po.ref_available():
+        return None
+    work = tempfile.mkdtemp(prefix="xtref")
+    total_rays, total_s, parts = 0, 0.0, []
+    plan = [("spheres64", 256, 16, 64), ("spheres4096", 256, 4, 32), ("terrain10k", 256, 16, 64),
+            ("terrain50k", 256, 16, 64)]
+    for name, res, spp, crop in plan:
+        spec = scenes.jobstream_scene(name, scale)
+        scn = spec.write_scn(work)
+        x0 = (res - crop) // 2
+        tiles = [(x0, x0, x0 + crop, x0 + crop)]
+        t0 = time.time()
+        xy, rgba, st = po.ref_render(scn, "pathtracer", res, res, spp=spp, rdepth=4, threads=threads, seed=7,
+                                     tiles=tiles, workdir=work)
+        total_rays += st["rays"]
+        total_s += st["render_s"]
+        parts.append("%s %dx%d crop of %d^2 x %d spp" % (name, crop, crop, res, spp))
+        if time.time() - t0 > budget_s:
+            break
+    return {"value": total_rays / total_s / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "reference",
+            "sample": "; ".join(parts) + " (pathtracer depth 4, IIntegrator::render timed, rays counted at "
+                                        "Scene::intersection)", "rays": total_rays, "seconds": total_s}
+
+
+def reference_arm(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    vals = []
+    for _ in range(args.warmup):
+        cpu_reference_sample(args.scale, threads, budget_s=5.0)
+    t_all, r_all = 0.0, 0
+    for _ in range(args.steps):
+        r = cpu_reference_sample(args.scale, threads, budget_s=5.0)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/xtref was not built"}))
+            return 0
+        t_all += r["seconds"]
+        r_all += r["rays"]
+        vals.append(r)
+    value = r_all / t_all / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_all / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded scenes and job stream)",
+            "config": {"workload": WORKLOAD, "sample": vals[-1]["sample"]},
+            "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": "reference",
+                             "sample": vals[-1]["sample"]},
+            "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    import torch
+    rank, world, local = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    D = Dist(world, True)
+    from xtracer_b200 import scenes, xtgpu
+    from xtracer_b200.service import Service
+
+    specs, gscenes = build_scenes(args.scale)
+    jobs = scenes.job_stream(args.stream_jobs, seed=4 + rank)
+    nslices = max(1, len(jobs) // args.jobs_per_step)
+    slices = [jobs[i * args.jobs_per_step:(i + 1) * args.jobs_per_step] for i in range(nslices)]
+    budget = 48 << 30
+
+    served = Service(gscenes, node_format=xtgpu.NODES_Q8, use_graphs=True, merge_jobs=True, memory_budget=budget,
+                     time_kernels=True)
+    # warm-up steps (untimed): graphs captured, allocator pools primed
+    for w in range(args.warmup):
+        run_slice(served, slices[w % nslices])
+    served.reset_stats()
+    timed = [slices[(args.warmup + k) % nslices] for k in range(args.steps)]
+
+    clocks = ClockSampler(local)
+    D.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    rays, lat = 0, []
+    per_scene = np.zeros(len(gscenes))
+    for sl in timed:
+        r, l = run_slice(served, sl, per_scene=per_scene)
+        rays += r
+        lat += l
+    e1.record()
+    torch.cuda.synchronize()
+    D.barrier()
+    clk = clocks.stop()
+    dev_s = e0.elapsed_time(e1) / 1000.0
+    st = served.stats()
+    t_max = D.max(dev_s)
+    rays_all = D.sum(rays)
+    value = rays_all / t_max / 1e6
+
+    # roofline of the extend kernel over the timed region
+    bpr = roofline_bytes_per_ray(specs, gscenes, xtgpu.NODES_Q8)
+    scene_bpr = [b["bytes_per_ray"] for b in bpr]
+    # rays of each scene in the timed steps times that scene's bytes per ray
+    alg_bytes = float(np.dot(per_scene, scene_bpr))
+    ext_s = st.extend_ms / 1000.0
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / ext_s / 1e9 if ext_s > 0 else None
+
+    # end to end: same steps, every frame copied to host memory by the service
+    e2e_svc = Service(gscenes, node_format=xtgpu.NODES_Q8, use_graphs=True, merge_jobs=True, memory_budget=budget,
+                      host_results=True)
+    run_slice(e2e_svc, slices[0])
+    D.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e_rays = 0
+    d2h = 0
+    for sl in timed:
+        r, _ = run_slice(e2e_svc, sl, record=[])
+        e_rays += r
+        d2h += sum(j.width * j.height * 16 for j in sl)
+    torch.cuda.synchronize()
+    e2e_s = D.max(time.perf_counter() - t0)
+    e2e_value = D.sum(e_rays) / e2e_s / 1e6
+    e2e_svc.close()
+
+    # plain path: one job per launch, FP32 BVH, no graphs, on the first timed step
+    plain = None
+    if not args.no_plain:
+        psvc = Service(gscenes, node_format=xtgpu.NODES_FP32, use_graphs=False, merge_jobs=False,
+                       memory_budget=budget)
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record()
+        pr, pl = run_slice(psvc, timed[0])
+        p1.record()
+        torch.cuda.synchronize()
+        ps = p0.elapsed_time(p1) / 1000.0
+        psvc.close()
+        # the served path on exactly that step, for a like-for-like ratio
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        sr, sl_ = run_slice(served, timed[0])
+        s1.record()
+        torch.cuda.synchronize()
+        ss = s0.elapsed_time(s1) / 1000.0
+        plain = {"value": pr / ps / 1e6, "unit": "Mrays/s", "step_jobs": len(timed[0]),
+                 "p50_ms": 1000 * pct(pl, 50), "p99_ms": 1000 * pct(pl, 99),
+                 "served_same_step_mrays": sr / ss / 1e6, "speedup": (sr / ss) / (pr / ps),
+                 "form": "one job per launch, FP32 BVH, no CUDA graphs"}
+
+    # open-loop latency: Poisson arrivals at 1.5x the plain path's job rate
+    latency = None
+    if not args.no_latency:
+        rate = 1.5 * len(timed[0]) / ps if plain is not None else 50.0
+        lsvc = Service(gscenes, node_format=xtgpu.NODES_Q8, use_graphs=True, merge_jobs=True, memory_budget=budget)
+        arr = np.cumsum(np.random.default_rng(4).exponential(1.0 / rate, len(timed[0])))
+        ids = [lsvc.submit(j.scene, xtgpu.PATHTRACER, j.width, j.height, j.spp, j.depth, 100.0, j.seed,
+                           submit_s=0.05 + float(a)) for j, a in zip(timed[0], arr)]
+        lsvc.run()
+        lats = [lsvc.poll(i).finish_s - lsvc.poll(i).submit_s for i in ids]
+        lsvc.close()
+        latency = {"arrivals": "Poisson, %.2f jobs/s (1.5x the plain path's job rate)" % rate,
+                   "jobs": len(ids), "p50_ms": 1000 * pct(lats, 50), "p99_ms": 1000 * pct(lats, 99)}
+
+    cpu = None
+    if not args.no_cpu and rank == 0:
+        cpu = cpu_reference_sample(args.scale, os.cpu_count() or 1)
+    served.close()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes and job stream)",
+            "config": {"workload": WORKLOAD, "jobs_per_step": args.jobs_per_step, "scale": args.scale,
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "cache": "inputs larger than L2 (resident scenes ~%.0f MB)" %
+                                (sum(s.device_bytes() for s in gscenes) / 1e6),
+                       "wave_paths": 1 << 22, "node_format": "q8", "cuda_graphs": True},
+            "p50_ms": 1000 * pct(lat, 50), "p99_ms": 1000 * pct(lat, 99),
+            "latency_open_loop": latency, "plain": plain,
+            "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 64 * len(timed[0]),
+                    "d2h_bytes_per_step": d2h // max(1, len(timed))},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "kernel": "k_extend (closest-hit traversal)", "peak_kind": peak_kind,
+                         "extend_ms": st.extend_ms, "extend_launches": st.extend_launches,
+                         "bytes_per_ray": {b["scene"]: round(b["bytes_per_ray"], 1) for b in bpr}},
+            "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(st.kernel_launches),
+            "rays": rays_all,
+        }
+        print(json.dumps(line))
+    D.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,246 @@
+/*
+ * xtgpu.h — C ABI of the B200 ray-scene intersection and integrator backend for
+ * XTracer (4rknova/xtracer).
+ *
+ * XTracer's C++ host (the .scn loader, Scene, IIntegrator, tiles, image output)
+ * stays as it is.  A GPU integrator flattens the loaded
+ * Scene into an xtgpu_scene_desc and calls the entry points below.  Plain
+ * pointers and sizes only; every call returns an xtgpu_status and never throws;
+ * xtgpu_last_error() gives the text of the last failure on the calling thread.
+ *
+ * Reference interfaces replaced (paths relative to the XTracer source tree):
+ *   xtgpu_scene_create     the Scene built by io::scn::load
+ *                          (src/xtcore/parseutil.cc:697-822, scene.h:35-86):
+ *                          objects, surfaces, materials, environment, camera
+ *   xtgpu_bvh_build        Mesh::build_octree / Octree<Triangle>::build
+ *                          (src/xtcore/mesh.cc:70-113, octree.tml:118-198)
+ *   xtgpu_trace            Scene::intersection (src/xtcore/scene.cc:191-216)
+ *                          over a batch of rays, including the per-mesh
+ *                          Octree::r_intersection (octree.tml:206-249)
+ *   xtgpu_render           IIntegrator::render + render_tile of the stencil,
+ *                          depth, ao and pathtracer integrators
+ *                          (src/xtcore/integrator.cc:29-53,
+ *                          integrator/{stencil,depth,ao,pathtracer}/integrator.cc)
+ *   xtgpu_service_*        no reference counterpart: a persistent render
+ *                          service (resident scenes, memory-budget admission,
+ *                          merged wavefront launches in CUDA graphs)
+ *
+ * Device pointers are CUDA global-memory pointers on the current device;
+ * `stream` is a cudaStream_t (NULL = legacy default stream).
+ */
+#ifndef XTGPU_H
+#define XTGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define XTGPU_API __attribute__((visibility("default")))
+#else
+#define XTGPU_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    XTGPU_OK = 0,
+    XTGPU_ERR_INVALID = 1,   /* bad argument: NULL handle, size out of range, bad enum */
+    XTGPU_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+    XTGPU_ERR_NOMEM = 3,     /* device allocation failed or a memory budget is exceeded */
+    XTGPU_ERR_LIMIT = 4,     /* a fixed capacity was exceeded (traversal stack, queue) */
+    XTGPU_ERR_TIMEOUT = 5,   /* a bounded wait expired */
+    XTGPU_ERR_NOT_FOUND = 6, /* unknown job or scene id */
+    XTGPU_ERR_STATE = 7      /* call not valid in the object's current state */
+} xtgpu_status;
+
+/* Surface kinds (src/xtcore/math/{sphere,plane}.cc, mesh.cc). */
+enum { XTGPU_SPHERE = 0, XTGPU_PLANE = 1, XTGPU_MESH = 2 };
+/* Materials (src/xtcore/material/, names in matdefs.h:4-12). */
+enum { XTGPU_LAMBERT = 0, XTGPU_PHONG = 1, XTGPU_BLINNPHONG = 2, XTGPU_EMISSIVE = 3, XTGPU_DIELECTRIC = 4 };
+/* Environment samplers (sampler_col.cc, sampler_gradient.cc); none = black. */
+enum { XTGPU_ENV_NONE = 0, XTGPU_ENV_COLOR = 1, XTGPU_ENV_GRADIENT = 2 };
+/* Integrators. */
+enum { XTGPU_STENCIL = 0, XTGPU_DEPTH = 1, XTGPU_AO = 2, XTGPU_PATHTRACER = 3 };
+/* BVH node formats: 64-byte FP32 child boxes, or 32-byte boxes quantised to
+ * 8 bits per bound with outward rounding. */
+enum { XTGPU_NODES_FP32 = 0, XTGPU_NODES_Q8 = 1 };
+
+typedef struct {
+    int32_t type;                  /* XTGPU_LAMBERT ... */
+    float diffuse[3], specular[3], emissive[3];
+    float reflectance, exponent, ior;
+} xtgpu_material;
+
+typedef struct {
+    float position[3], target[3], up[3];
+    float fov;                     /* degrees, horizontal (perspective.cc:48-50) */
+} xtgpu_camera;
+
+/* A flattened Scene.  Objects are listed in the order Scene::intersection
+ * visits them (the std::map order of their ids).  Host pointers; copied. */
+typedef struct {
+    int32_t n_objects;
+    const int32_t *obj_kind;       /* XTGPU_SPHERE / XTGPU_PLANE / XTGPU_MESH */
+    const int32_t *obj_first;      /* sphere index, plane index, or first triangle */
+    const int32_t *obj_count;      /* triangle count of a mesh, 1 otherwise */
+    const int32_t *obj_material;   /* index into materials */
+    int32_t n_spheres;
+    const float *spheres;          /* 4 floats each: centre xyz, radius */
+    int32_t n_planes;
+    const float *planes;           /* 4 floats each: normal xyz, offset */
+    int32_t n_tris;
+    const float *tris;             /* 9 floats each: v0 v1 v2 */
+    const float *tri_normals;      /* 9 floats each, or NULL (face normals) */
+    int32_t n_materials;
+    const xtgpu_material *materials;
+    int32_t env_type;
+    float env_a[3], env_b[3];
+    xtgpu_camera camera;
+} xtgpu_scene_desc;
+
+typedef struct xtgpu_scene xtgpu_scene;
+
+typedef struct {
+    int32_t node_format;           /* XTGPU_NODES_FP32 or XTGPU_NODES_Q8 */
+    int32_t leaf_size;             /* primitives per leaf, 1..4 (0 = default 2) */
+} xtgpu_bvh_opts;
+
+/* Uploads the scene (geometry, materials, camera) to the current device. */
+XTGPU_API xtgpu_status xtgpu_scene_create(const xtgpu_scene_desc *desc, void *stream, xtgpu_scene **out);
+/* Builds the scene's LBVH on the device: 30-bit Morton codes, in-house radix
+ * sort, Karras hierarchy, bottom-up refit, optional 8-bit quantisation.  Both
+ * node formats can be built and kept; the last one built is used by default. */
+XTGPU_API xtgpu_status xtgpu_bvh_build(xtgpu_scene *scene, const xtgpu_bvh_opts *opts, void *stream);
+/* Frees every device buffer of the scene. */
+XTGPU_API xtgpu_status xtgpu_scene_destroy(xtgpu_scene *scene);
+/* Bytes of device memory the scene holds (geometry + built BVHs). */
+XTGPU_API xtgpu_status xtgpu_scene_device_bytes(const xtgpu_scene *scene, uint64_t *bytes);
+
+/* BVH statistics and intermediate build arrays, copied to host memory (any
+ * pointer may be NULL).  morton/order: n_prims each (sorted codes, sorted
+ * primitive ids); left/right: n_prims-1 each, Karras child references
+ * (>= 0 internal node, < 0 leaf ~index); depth: maximum root-to-leaf depth. */
+typedef struct {
+    int64_t n_prims;               /* triangles + spheres (planes are tested apart) */
+    int32_t depth;
+    int32_t leaf_size;
+    uint64_t node_bytes_fp32, node_bytes_q8;
+} xtgpu_bvh_info;
+XTGPU_API xtgpu_status xtgpu_bvh_export(const xtgpu_scene *scene, xtgpu_bvh_info *info, uint32_t *morton,
+                              uint32_t *order, int32_t *left, int32_t *right, void *stream);
+
+/* Ray batch in device memory, structure of arrays of float4:
+ *   org_tmin[i] = (origin.xyz, tmin), dir_tmax[i] = (direction.xyz, tmax)
+ * Hit output per ray: t (inf on a miss), primitive id (triangles 0..T-1, then
+ * spheres T..T+S-1, then planes), barycentric u, v of the hit triangle.
+ * Primitive ids follow the desc arrays, so the object of a hit is found from
+ * obj_first/obj_count. */
+typedef struct {
+    float t;
+    uint32_t prim;
+    float u, v;
+} xtgpu_hit;
+
+/* Closest hit of n rays: Scene::intersection semantics (nearest hit over every
+ * object; spheres hit only from outside, planes from both sides).  node_format
+ * picks the BVH to traverse (it must have been built). */
+XTGPU_API xtgpu_status xtgpu_trace(xtgpu_scene *scene, int64_t n, const void *org_tmin_dev, const void *dir_tmax_dev,
+                         xtgpu_hit *hits_dev, int32_t node_format, void *stream);
+/* The same with host buffers (pinned or pageable), copies included. */
+XTGPU_API xtgpu_status xtgpu_trace_host(xtgpu_scene *scene, int64_t n, const float *org_tmin, const float *dir_tmax,
+                              xtgpu_hit *hits, int32_t node_format, void *stream);
+
+typedef struct {
+    int32_t integrator;            /* XTGPU_STENCIL .. XTGPU_PATHTRACER */
+    int32_t width, height;         /* frame size (params_t, context.h:18-34) */
+    int32_t spp;                   /* samples per pixel, weight 1/spp each (aa.cc:66-74) */
+    int32_t rdepth;                /* pathtracer recursion depth */
+    float ao_max_distance;         /* AO: 100 in the shipped integrator (ao/integrator.cc:10) */
+    uint64_t seed;                 /* random stream key: results depend only on (seed, pixel, sample) */
+    int32_t node_format;           /* BVH to traverse */
+    int32_t x0, y0, x1, y1;        /* pixel rectangle to render; x1 = y1 = 0 means the whole frame */
+} xtgpu_render_params;
+
+/* Renders the rectangle with aa = 1 (one pixel-centre ray per sample,
+ * aa.cc:11-18) and writes RGBA float per pixel of the rectangle (row-major)
+ * into rgba_dev (device memory).  rays_traced (optional, host) receives the
+ * number of rays traced. */
+XTGPU_API xtgpu_status xtgpu_render(xtgpu_scene *scene, const xtgpu_render_params *params, float *rgba_dev,
+                          uint64_t *rays_traced, void *stream);
+/* The same into host memory (copy included). */
+XTGPU_API xtgpu_status xtgpu_render_host(xtgpu_scene *scene, const xtgpu_render_params *params, float *rgba_host,
+                               uint64_t *rays_traced, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Render service.  Scenes stay resident; jobs are admitted while their
+ * accumulation buffers fit the memory budget and a job slot is free; the rays of
+ * all admitted jobs are merged into shared wavefront launches (camera, extend,
+ * shade, accumulate) replayed as CUDA graphs.  Results depend only on the job
+ * (seed, pixel, sample), never on what else is in flight.                   */
+typedef struct xtgpu_service xtgpu_service;
+
+typedef struct {
+    uint64_t memory_budget_bytes;  /* for job accumulation buffers and queues */
+    int32_t max_jobs;              /* concurrent job slots (<= 1024) */
+    int64_t wave_paths;            /* paths per merged wavefront (0 = autotuned) */
+    int32_t node_format;           /* BVH format used by the service */
+    int32_t use_graphs;            /* 1 = replay each wave as a CUDA graph */
+    int32_t merge_jobs;            /* 0 = one job per launch (the plain path) */
+    int32_t host_results;          /* 1 = copy each finished frame to host memory and free
+                                      its device buffer at once (frees budget early) */
+    int32_t time_kernels;          /* 1 = time every extend launch with CUDA events */
+    int32_t count_visits;          /* 1 = count BVH nodes visited / primitives tested */
+} xtgpu_service_opts;
+
+typedef struct {
+    int32_t scene;                 /* id from xtgpu_service_add_scene */
+    int32_t integrator;
+    int32_t width, height, spp, rdepth;
+    float ao_max_distance;
+    uint64_t seed;
+} xtgpu_job_desc;
+
+typedef struct {
+    int32_t state;                 /* 0 queued, 1 running, 2 done, 3 failed */
+    uint64_t rays;                 /* rays traced for the job */
+    double submit_s, start_s, finish_s;   /* service clock (seconds) */
+} xtgpu_job_status;
+
+XTGPU_API xtgpu_status xtgpu_service_create(const xtgpu_service_opts *opts, void *stream, xtgpu_service **out);
+XTGPU_API xtgpu_status xtgpu_service_add_scene(xtgpu_service *svc, xtgpu_scene *scene, int32_t *scene_id);
+/* Queues a job; submit_s is the arrival time on the service clock (seconds
+ * since xtgpu_service_create), or a negative value for "now". */
+XTGPU_API xtgpu_status xtgpu_service_submit(xtgpu_service *svc, const xtgpu_job_desc *job, double submit_s, int64_t *job_id);
+/* Runs admission + waves until every queued job whose arrival time has passed
+ * is done, or max_seconds of service clock elapsed (0 = no limit). */
+XTGPU_API xtgpu_status xtgpu_service_run(xtgpu_service *svc, double max_seconds);
+XTGPU_API xtgpu_status xtgpu_service_poll(xtgpu_service *svc, int64_t job_id, xtgpu_job_status *status);
+/* Copies a finished job's RGBA frame (width*height*4 floats) to host memory. */
+XTGPU_API xtgpu_status xtgpu_service_result(xtgpu_service *svc, int64_t job_id, float *rgba_host);
+/* Releases a finished job's frame buffer. */
+XTGPU_API xtgpu_status xtgpu_service_release(xtgpu_service *svc, int64_t job_id);
+XTGPU_API xtgpu_status xtgpu_service_destroy(xtgpu_service *svc);
+
+typedef struct {
+    uint64_t rays;                 /* rays traced since the last reset */
+    uint64_t waves;                /* merged wavefront launches */
+    uint64_t kernel_launches;      /* camera + extend + shade + accumulate kernels */
+    double extend_ms;              /* device time of the extend launches (time_kernels) */
+    uint64_t extend_launches;
+    uint64_t node_visits, prim_tests;   /* count_visits */
+} xtgpu_service_stats;
+/* Counters of the service since creation or the last reset. */
+XTGPU_API xtgpu_status xtgpu_service_get_stats(xtgpu_service *svc, xtgpu_service_stats *stats);
+XTGPU_API xtgpu_status xtgpu_service_reset_stats(xtgpu_service *svc);
+
+/* Text of the last error on this thread ("" if none). */
+XTGPU_API const char *xtgpu_last_error(void);
+/* Library version string. */
+XTGPU_API const char *xtgpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XTGPU_H */

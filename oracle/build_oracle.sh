@@ -5,4 +5,4 @@ set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
 mkdir -p "$HERE/_build"
 /usr/bin/gcc -O2 -std=c99 -D_GNU_SOURCE -fPIC -shared -Wall -Wextra -Wno-unused-parameter -Wno-maybe-uninitialized -Wno-alloc-size-larger-than \
-    "$HERE/xtoracle.c" -o "$HERE/_build/libxtoracle.so" -lm
+    "$HERE/xtoracle.c" "$HERE/lbvh_cpu.c" -o "$HERE/_build/libxtoracle.so" -lm

@@ -1,0 +1,106 @@
+"""Helpers shared by the parity tests: primitive bookkeeping and the FP64
+classification of GPU/reference disagreements (tie, grazing, or GPU error)."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from oracle import pyoracle as po
+from xtracer_b200 import scenes
+
+
+def P(a):
+    return np.ascontiguousarray(a, np.float64).ctypes.data_as(C.c_void_p)
+
+
+def global_prim(spec, obj, prim_in_obj_or_global, is_mesh_local=True):
+    """Global primitive id (triangles, then spheres, then planes) of an object hit."""
+    kind = spec.obj_kind[obj]
+    first = spec.obj_first[obj]
+    if kind == scenes.MESH:
+        return int(first + prim_in_obj_or_global) if is_mesh_local else int(prim_in_obj_or_global)
+    if kind == scenes.SPHERE:
+        return spec.n_tris + int(first)
+    return spec.n_tris + spec.spheres.shape[0] + int(first)
+
+
+def oracle_global_prim(spec, obj, prim):
+    """xo_trace returns prim = triangle index (global) for meshes, sphere/plane
+    index otherwise; convert to the GPU's global id."""
+    out = np.full(obj.shape, -1, np.int64)
+    for i in range(obj.size):
+        o = obj[i]
+        if o < 0:
+            continue
+        k = spec.obj_kind[o]
+        if k == scenes.MESH:
+            out[i] = prim[i]
+        elif k == scenes.SPHERE:
+            out[i] = spec.n_tris + prim[i]
+        else:
+            out[i] = spec.n_tris + spec.spheres.shape[0] + prim[i]
+    return out
+
+
+def ref_t_of(spec, gid, o, d):
+    """(hit, t, margin) of the reference's FP64 test of primitive gid; margin is
+    the smallest barycentric (triangles) or relative discriminant (spheres)."""
+    L = po.lib()
+    out = np.zeros(7)
+    nt, ns = spec.n_tris, spec.spheres.shape[0]
+    if gid < nt:
+        v = spec.tris[gid].astype(np.float64).ravel()
+        n = np.zeros(9) if spec.tri_normals is None else spec.tri_normals[gid].astype(np.float64).ravel()
+        h = L.xo_kat_triangle(P(v), P(n), P(o), P(d), P(out))
+        # watertight FP64 barycentric margin at the ray's crossing of the plane
+        V = v.reshape(3, 3)
+        e1, e2 = V[1] - V[0], V[2] - V[0]
+        pv = np.cross(d, e2)
+        det = e1 @ pv
+        if abs(det) < 1e-300:
+            return h, out[0], 0.0
+        tv = o - V[0]
+        u = (tv @ pv) / det
+        qv = np.cross(tv, e1)
+        w = (d @ qv) / det
+        margin = min(u, w, 1 - u - w)
+        return h, out[0], margin
+    if gid < nt + ns:
+        s = spec.spheres[gid - nt].astype(np.float64)
+        h = L.xo_kat_sphere(P(s), P(o), P(d), P(out))
+        f = o - s[:3]
+        b = f @ d
+        disc = b * b - (f @ f - s[3] ** 2)
+        return h, out[0], disc / max(s[3] ** 2, 1e-300)
+    pl = spec.planes[gid - nt - ns].astype(np.float64)
+    h = L.xo_kat_plane(P(pl), P(o), P(d), P(out))
+    return h, out[0], abs(pl[:3] @ d)
+
+
+def classify(spec, org, dirs, g_hit, g_gid, g_t, r_hit, r_gid, r_t, tie_rel=1e-5, graze=1e-5):
+    """Returns (n_agree, n_tie, n_graze, unexplained_indices) over all rays."""
+    agree = (g_hit == r_hit) & ((g_hit == 0) | (g_gid == r_gid))
+    tie = graze_n = 0
+    bad = []
+    for i in np.nonzero(~agree)[0]:
+        o, d = org[i], dirs[i]
+        if g_hit[i] and r_hit[i]:
+            h, t_alt, m = ref_t_of(spec, int(g_gid[i]), o, d)
+            if h and abs(t_alt - r_t[i]) <= tie_rel * r_t[i]:
+                tie += 1
+                continue
+            _, _, mg = ref_t_of(spec, int(g_gid[i]), o, d)
+            _, _, mr = ref_t_of(spec, int(r_gid[i]), o, d)
+            if abs(mg) < graze or abs(mr) < graze:
+                graze_n += 1
+                continue
+            bad.append(i)
+        else:
+            gid = int(g_gid[i]) if g_hit[i] else int(r_gid[i])
+            _, _, m = ref_t_of(spec, gid, o, d)
+            if abs(m) < graze:
+                graze_n += 1
+            else:
+                bad.append(i)
+    return int(agree.sum()), tie, graze_n, bad

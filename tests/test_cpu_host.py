@@ -1,0 +1,120 @@
+"""Host-side checks that need no GPU: the C ABI library loads and exports
+every entry point include/xtgpu.h declares, argument checks reject bad input
+before any device work, the scene generators produce exact float32 inputs, and
+the CPU LBVH replica builds a valid Karras hierarchy."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+from xtracer_b200 import scenes, xtgpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "xtgpu.h")).read()
+    return sorted(set(re.findall(r"XTGPU_API\s+[\w\s\*]+?\b(xtgpu_\w+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    names = header_functions()
+    assert len(names) >= 19
+    out = subprocess.run(["nm", "-D", "--defined-only", xtgpu.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (xtgpu_\w+)", out))
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+    L = xtgpu.lib()
+    for n in names:
+        assert getattr(L, n) is not None
+    assert set(xtgpu.SIGNATURES) | {"xtgpu_last_error", "xtgpu_version"} == set(names)
+
+
+def test_library_is_sm100a():
+    out = subprocess.run(["strings", xtgpu.LIB_PATH], capture_output=True, text=True).stdout
+    assert "sm_100a" in out or "compute_100a" in out or xtgpu.lib().xtgpu_version().decode().endswith("(sm_100a)")
+
+
+def test_invalid_arguments_are_rejected_without_device_work():
+    L = xtgpu.lib()
+    out = C.c_void_p()
+    assert L.xtgpu_scene_create(None, None, C.byref(out)) == 1
+    d = xtgpu.SceneDesc()
+    d.n_tris = 3            # triangles without an array
+    assert L.xtgpu_scene_create(C.byref(d), None, C.byref(out)) == 1
+    assert b"NULL arrays" in L.xtgpu_last_error()
+    d = xtgpu.SceneDesc()   # a sphere that belongs to no object
+    sph = np.zeros(4, np.float32)
+    d.n_spheres = 1
+    d.spheres = sph.ctypes.data_as(C.c_void_p)
+    assert L.xtgpu_scene_create(C.byref(d), None, C.byref(out)) == 1
+    assert b"no object" in L.xtgpu_last_error()
+    assert L.xtgpu_bvh_build(None, None, None) == 1
+    assert L.xtgpu_render(None, None, None, None, None) == 1
+    assert L.xtgpu_trace(None, 4, None, None, None, 0, None) == 1
+    assert L.xtgpu_service_create(None, None, C.byref(out)) == 1
+    o = xtgpu.ServiceOpts(1 << 20, 0, 0, 0, 1, 1, 0, 0, 0)   # max_jobs 0
+    assert L.xtgpu_service_create(C.byref(o), None, C.byref(out)) == 1
+    assert L.xtgpu_scene_destroy(None) == 0
+
+
+def test_generated_scenes_are_exact_float32():
+    for spec in (scenes.spheres_scene(64, seed=1), scenes.terrain_scene(5_000, seed=2),
+                 scenes.hairball_scene(5_000, seed=3)):
+        for a in (spec.spheres, spec.planes, spec.tris):
+            a64 = a.astype(np.float64)
+            # dyadic grid: every value round-trips through its shortest repr
+            for v in a64.ravel()[:2000]:
+                assert float(repr(float(v))) == v and np.float32(v) == v
+        assert spec.obj_kind.size == spec.obj_first.size == spec.obj_count.size == spec.obj_material.size
+
+
+def test_terrain_sizes_and_orientation():
+    spec = scenes.terrain_scene(999_698, seed=2)
+    assert spec.n_tris == 999_698
+    t = spec.tris[:1000].astype(np.float64)
+    n = np.cross(t[:, 1] - t[:, 0], t[:, 2] - t[:, 0])
+    assert np.all(n[:, 1] > 0), "terrain faces wound counter-clockwise seen from above"
+    assert spec.tris[:, :, 0].min() == -50.0 and spec.tris[:, :, 0].max() == 50.0
+
+
+def test_hairball_geometry():
+    t = scenes.hairball_tris(20_000, seed=3).astype(np.float64)
+    e = np.linalg.norm(t[:, 1] - t[:, 0], axis=1)
+    assert np.allclose(e, 0.01, atol=1e-5)
+    c = t.mean(axis=1)
+    assert np.linalg.norm(c, axis=1).max() <= 1.0 + 1e-5
+
+
+def test_job_stream_is_seeded():
+    a = scenes.job_stream(512, seed=4)
+    b = scenes.job_stream(512, seed=4)
+    assert [(j.scene, j.width, j.spp, j.arrival_s) for j in a] == [(j.scene, j.width, j.spp, j.arrival_s) for j in b]
+    assert {j.width for j in a} == {128, 256, 512, 1024} and {j.spp for j in a} == {1, 4, 16, 64}
+    assert all(j.depth == 4 for j in a)
+    assert all(x.arrival_s <= y.arrival_s for x, y in zip(a, a[1:]))
+
+
+@pytest.mark.parametrize("n_sph", [1, 2, 3, 64, 4096])
+def test_cpu_lbvh_replica_is_a_valid_karras_tree(n_sph):
+    spec = scenes.spheres_scene(n_sph, seed=5, with_light=False)
+    L = po.lib()
+    L.xo_lbvh_build.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p] + [C.c_void_p] * 4
+    n = n_sph
+    keys = np.zeros(n, np.uint32); order = np.zeros(n, np.uint32)
+    left = np.zeros(max(n - 1, 1), np.int32); right = np.zeros(max(n - 1, 1), np.int32)
+    sph = np.ascontiguousarray(spec.spheres.reshape(-1), np.float32)
+    L.xo_lbvh_build(0, None, n, sph.ctypes.data_as(C.c_void_p), *[a.ctypes.data_as(C.c_void_p)
+                                                                  for a in (keys, order, left, right)])
+    assert np.all(np.diff(keys.astype(np.int64)) >= 0)
+    assert np.array_equal(np.sort(order), np.arange(n))
+    if n > 1:
+        left, right = left[:n - 1], right[:n - 1]
+        inner = np.concatenate([left[left >= 0], right[right >= 0]])
+        leaves = np.concatenate([~left[left < 0], ~right[right < 0]])
+        assert np.array_equal(np.sort(inner), np.arange(1, n - 1))
+        assert np.array_equal(np.sort(leaves), np.arange(n))

@@ -1,0 +1,257 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle restatement
+and the reference's own golden fixtures.
+
+Bars (from the hot-path contract):
+* LBVH integer steps (Morton codes, sort order, Karras topology): bit-exact
+  against the CPU re-implementation (oracle/lbvh_cpu.c).
+* Primary hits: primitive agreement >= 99.99% of pixels, every disagreement
+  explained as a tie (|dt|/t <= 1e-5 between the two primitives in FP64) or a
+  grazing hit (barycentric margin or sphere discriminant below 1e-5); relative
+  depth error <= 1e-5 where the primitives agree.
+* Stencil frames identical where hits agree; depth frames within 1e-5 relative.
+* AO / pathtracer: per-pixel RMSE against the reference's frames within the
+  reference's own sampling noise at equal spp.
+* 8-bit quantised BVH: the same hits as the FP32 BVH.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+from tests import parity
+from xtracer_b200 import scenes, xtgpu
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def cuda_device():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    torch.cuda.set_device(0)
+    xtgpu.lib()
+    yield
+
+
+def small_scenes():
+    return {"spheres64": (scenes.spheres_scene(64, seed=1, name="spheres64"), 64, 64),
+            "terrain20k": (scenes.terrain_scene(20_000, seed=2, name="terrain20k"), 96, 54),
+            "hairball20k": (scenes.hairball_scene(20_000, seed=3, name="hairball20k"), 64, 64)}
+
+
+def lbvh_cpu(spec):
+    L = po.lib()
+    L.xo_lbvh_build.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p] + [C.c_void_p] * 4
+    n = spec.n_tris + spec.spheres.shape[0]
+    keys = np.zeros(max(n, 1), np.uint32); order = np.zeros(max(n, 1), np.uint32)
+    left = np.zeros(max(n - 1, 1), np.int32); right = np.zeros(max(n - 1, 1), np.int32)
+    tris = np.ascontiguousarray(spec.tris.reshape(-1), np.float32)
+    sph = np.ascontiguousarray(spec.spheres.reshape(-1), np.float32)
+    L.xo_lbvh_build(spec.n_tris, tris.ctypes.data_as(C.c_void_p), spec.spheres.shape[0],
+                    sph.ctypes.data_as(C.c_void_p), *[a.ctypes.data_as(C.c_void_p) for a in (keys, order, left, right)])
+    return keys[:n], order[:n], left[:max(n - 1, 0)], right[:max(n - 1, 0)]
+
+
+def duplicate_scene():
+    """Many triangles with identical centroids: equal Morton codes everywhere."""
+    t = np.array([[[0, 0, 0], [1, 0, 0], [0, 1, 0]]], np.float32)
+    tris = np.repeat(t, 1000, axis=0)
+    tris[500:] += np.float32(4.0)
+    spec = scenes.terrain_scene(8, seed=1, name="dup")
+    spec.tris = tris
+    spec.obj_count = np.array([tris.shape[0]], np.int32)
+    spec.mesh_obj = None
+    return spec
+
+
+def tiny_scene(n_spheres):
+    return scenes.spheres_scene(n_spheres, seed=9, name="tiny%d" % n_spheres, with_light=False)
+
+
+@pytest.mark.parametrize("name", ["spheres64", "terrain20k", "hairball20k", "dup", "tiny1", "tiny2", "tiny3",
+                                  "hairball300k"])
+def test_lbvh_bit_exact_vs_cpu(name):
+    if name in small_scenes():
+        spec = small_scenes()[name][0]
+    elif name == "dup":
+        spec = duplicate_scene()
+    elif name == "hairball300k":
+        spec = scenes.hairball_scene(300_000, seed=5)
+    else:
+        spec = tiny_scene(int(name[-1]))
+    sc = xtgpu.Scene(spec)
+    ex = sc.bvh_export()
+    keys, order, left, right = lbvh_cpu(spec)
+    assert np.array_equal(ex["morton"], keys)
+    assert np.array_equal(ex["order"], order)
+    assert np.array_equal(ex["left"], left)
+    assert np.array_equal(ex["right"], right)
+    n = keys.size
+    assert np.all(np.diff(keys.astype(np.int64)) >= 0)
+    if n > 1:
+        # every node but the root has exactly one parent
+        inner = np.concatenate([left[left >= 0], right[right >= 0]])
+        leaves = np.concatenate([~left[left < 0], ~right[right < 0]])
+        assert np.array_equal(np.sort(inner), np.arange(1, n - 1))
+        assert np.array_equal(np.sort(leaves), np.arange(n))
+    sc.close()
+
+
+def gpu_primary(spec, w, h, fmt=xtgpu.NODES_FP32, sc=None):
+    """Primary rays through the GPU: the FP64 reference camera rays rounded to
+    FP32, traced by xtgpu_trace_host."""
+    ys, xs = np.mgrid[0:h, 0:w]
+    px = np.stack([xs.ravel(), ys.ravel()], 1)
+    org, dirs = po.camera_rays(spec, w, h, px)
+    own = sc is None
+    if own:
+        sc = xtgpu.Scene(spec, node_formats=(fmt,))
+    hits = sc.intersection(org.astype(np.float32), dirs.astype(np.float32), node_format=fmt)
+    if own:
+        sc.close()
+    return org, dirs, hits
+
+
+@pytest.mark.parametrize("name", ["spheres64", "terrain20k", "hairball20k"])
+@pytest.mark.parametrize("fmt", [xtgpu.NODES_FP32, xtgpu.NODES_Q8])
+def test_primary_hits_vs_reference_golden(name, fmt):
+    spec, w, h = small_scenes()[name]
+    g = np.load(os.path.join(GOLD, "hits_%s.npz" % name))
+    org, dirs, hits = gpu_primary(spec, w, h, fmt)
+    g_hit = (hits["prim"] != 0xffffffff).astype(np.int32)
+    g_gid = hits["prim"].astype(np.int64)
+    r_hit = g["hit"].astype(np.int32)
+    r_gid = np.array([parity.global_prim(spec, o, p) if o >= 0 else -1 for o, p in zip(g["obj"], g["prim"])])
+    n_agree, tie, graze, bad = parity.classify(spec, org, dirs, g_hit, g_gid, hits["t"].astype(np.float64),
+                                               r_hit, r_gid, g["t"])
+    assert not bad, "unexplained disagreements at %s" % bad[:10]
+    assert n_agree >= 0.999 * g_hit.size
+    m = (g_hit == 1) & (r_hit == 1) & (g_gid == r_gid)
+    rel = np.abs(hits["t"][m].astype(np.float64) - g["t"][m]) / g["t"][m]
+    assert rel.max() <= 1e-5, rel.max()
+
+
+def test_primary_hits_terrain_200k_vs_oracle():
+    """A larger mesh than the fixtures, checked against the oracle restatement."""
+    spec = scenes.terrain_scene(200_000, seed=11)
+    w, h = 480, 270
+    org, dirs, hits = gpu_primary(spec, w, h)
+    orc = po.OracleScene(spec, po.XO_ACCEL_BVH)
+    r = orc.trace(org, dirs)
+    r_gid = parity.oracle_global_prim(spec, r["obj"], r["prim"])
+    g_hit = (hits["prim"] != 0xffffffff).astype(np.int32)
+    g_gid = hits["prim"].astype(np.int64)
+    n_agree, tie, graze, bad = parity.classify(spec, org, dirs, g_hit, g_gid, hits["t"].astype(np.float64),
+                                               r["hit"], r_gid, r["t"])
+    assert not bad, "unexplained disagreements: %d" % len(bad)
+    assert n_agree >= 0.9999 * g_hit.size
+    m = (g_hit == 1) & (r["hit"] == 1) & (g_gid == r_gid)
+    rel = np.abs(hits["t"][m].astype(np.float64) - r["t"][m]) / r["t"][m]
+    assert rel.max() <= 1e-5, rel.max()
+
+
+@pytest.mark.parametrize("name", ["spheres64", "terrain20k", "hairball20k"])
+def test_q8_hits_equal_fp32(name):
+    spec, w, h = small_scenes()[name]
+    sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8))
+    _, _, a = gpu_primary(spec, w, h, xtgpu.NODES_FP32, sc)
+    _, _, b = gpu_primary(spec, w, h, xtgpu.NODES_Q8, sc)
+    same = (a["prim"] == b["prim"]) & ((a["t"] == b["t"]) | (a["prim"] == 0xffffffff))
+    assert same.mean() >= 0.9999
+    sc.close()
+
+
+@pytest.mark.parametrize("name", ["spheres64", "terrain20k", "hairball20k"])
+def test_stencil_depth_frames_vs_reference_golden(name):
+    spec, w, h = small_scenes()[name]
+    g = np.load(os.path.join(GOLD, "render_%s.npz" % name))
+    sc = xtgpu.Scene(spec)
+    for key, integ in (("stencil", xtgpu.STENCIL), ("depth", xtgpu.DEPTH)):
+        spp = int(g[key + "_spp"])
+        img, rays = sc.render(integ, w, h, spp=spp)
+        xy = g[key + "_xy"]
+        got = img[xy[:, 1], xy[:, 0]]
+        ref = g[key + "_rgba"]
+        if integ == xtgpu.STENCIL:
+            assert (got == ref).all(axis=1).mean() >= 0.999
+        else:
+            both = (ref[:, 3] > 0)
+            rel = np.abs(got[:, 0] - ref[:, 0]) / np.maximum(np.abs(ref[:, 0]), 1e-6)
+            assert np.mean(rel[both] <= 1e-5) >= 0.999, np.sort(rel)[-5:]
+        assert rays == w * h * spp
+    sc.close()
+
+
+def _rmse(a, b):
+    return float(np.sqrt(np.mean((a[:, :3] - b[:, :3]) ** 2)))
+
+
+@pytest.mark.parametrize("name,key,integ,md", [
+    ("spheres64", "ao100", xtgpu.AO, 100.0), ("spheres64", "ao0.2", xtgpu.AO, 0.2),
+    ("terrain20k", "ao100", xtgpu.AO, 100.0), ("terrain20k", "ao0.2", xtgpu.AO, 0.2),
+    ("hairball20k", "ao100", xtgpu.AO, 100.0), ("hairball20k", "ao0.2", xtgpu.AO, 0.2),
+    ("spheres64", "pt", xtgpu.PATHTRACER, 100.0)])
+def test_stochastic_frames_within_reference_noise(name, key, integ, md):
+    spec, w, h = small_scenes()[name]
+    g = np.load(os.path.join(GOLD, "render_%s.npz" % name))
+    sc = xtgpu.Scene(spec)
+    img, rays = sc.render(integ, w, h, spp=int(g[key + "_spp"]), rdepth=4, ao_max_distance=md, seed=777)
+    xy = g[key + "_xy"]
+    O = img[xy[:, 1], xy[:, 0]]
+    R = g[key + "_rgba"]
+    n = R.shape[0]
+    ref = np.mean([_rmse(R[i], R[[j for j in range(n) if j != i]].mean(0)) for i in range(n)])
+    got = np.mean([_rmse(O, R[[j for j in range(n) if j != i]].mean(0)) for i in range(n)])
+    assert got <= 1.25 * ref + 1e-6, (got, ref)
+    for ch in range(3):
+        diff = O[:, ch] - R[:, :, ch].mean(0)
+        se = np.sqrt(R[:, :, ch].var(0, ddof=1).mean() / diff.size * (1 + 1.0 / n))
+        assert abs(diff.mean()) < 4.5 * se + 1e-5, (ch, diff.mean(), se)
+    sc.close()
+
+
+@pytest.mark.parametrize("integ,md", [(xtgpu.AO, 0.5), (xtgpu.PATHTRACER, 100.0)])
+def test_stochastic_same_stream_as_oracle(integ, md):
+    """With the same random stream, GPU (FP32) and oracle (FP64) frames differ
+    only where a rounding difference sends a path another way."""
+    spec, w, h = small_scenes()["spheres64"]
+    sc = xtgpu.Scene(spec)
+    img, rays = sc.render(integ, w, h, spp=16, rdepth=4, ao_max_distance=md, seed=99)
+    orc = po.OracleScene(spec, po.XO_ACCEL_BVH)
+    ys, xs = np.mgrid[0:h, 0:w]
+    o, orays = orc.render(po.AO if integ == xtgpu.AO else po.PATHTRACER, w, h, spp=16, rdepth=4,
+                          ao_max_distance=md, seed=99, pixels=np.stack([xs.ravel(), ys.ravel()], 1))
+    d = np.abs(img.reshape(-1, 4)[:, :3] - o[:, :3]).max(axis=1)
+    assert np.mean(d < 1e-3) >= 0.97, np.mean(d < 1e-3)
+    assert abs(rays - orays) <= 0.01 * orays
+    sc.close()
+
+
+def test_render_is_deterministic_and_rect_consistent():
+    spec, w, h = small_scenes()["terrain20k"]
+    sc = xtgpu.Scene(spec)
+    a, _ = sc.render(xtgpu.PATHTRACER, w, h, spp=8, rdepth=4, seed=5)
+    b, _ = sc.render(xtgpu.PATHTRACER, w, h, spp=8, rdepth=4, seed=5)
+    assert np.array_equal(a, b)
+    c, _ = sc.render(xtgpu.PATHTRACER, w, h, spp=8, rdepth=4, seed=5, rect=(10, 7, 50, 31))
+    assert np.array_equal(c, a[7:31, 10:50])
+    sc.close()
+
+
+def test_bad_arguments_return_invalid():
+    spec, w, h = small_scenes()["spheres64"]
+    sc = xtgpu.Scene(spec)
+    with pytest.raises(xtgpu.XtgpuError) as e:
+        sc.render(xtgpu.STENCIL, 0, 10)
+    assert e.value.status == 1
+    with pytest.raises(xtgpu.XtgpuError) as e:
+        sc.render(xtgpu.AO, 8, 8, ao_max_distance=0.0)
+    assert e.value.status == 1
+    with pytest.raises(xtgpu.XtgpuError) as e:
+        sc.render(xtgpu.STENCIL, 8, 8, node_format=xtgpu.NODES_Q8)   # not built
+    assert e.value.status == 7
+    sc.close()

@@ -1,0 +1,97 @@
+"""Render service on the GPU: a job's frame is the same alone and in the mix,
+whatever the wave size, merging and graph replay; admission respects the
+memory budget; latency bookkeeping is consistent."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from xtracer_b200 import scenes, xtgpu
+from xtracer_b200.service import Service
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def cuda_device():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    torch.cuda.set_device(0)
+    xtgpu.lib()
+    yield
+
+
+@pytest.fixture(scope="module")
+def resident():
+    fm = (xtgpu.NODES_FP32, xtgpu.NODES_Q8)
+    return [xtgpu.Scene(scenes.spheres_scene(64, seed=1, name="s64"), node_formats=fm),
+            xtgpu.Scene(scenes.terrain_scene(20_000, seed=2, name="t20k"), node_formats=fm),
+            xtgpu.Scene(scenes.hairball_scene(20_000, seed=3, name="h20k"), node_formats=fm)]
+
+
+JOBS = [(0, xtgpu.PATHTRACER, 64, 48, 8, 4, 100.0, 11), (1, xtgpu.PATHTRACER, 40, 40, 16, 4, 100.0, 12),
+        (2, xtgpu.AO, 32, 32, 8, 4, 0.2, 13), (1, xtgpu.DEPTH, 50, 30, 2, 1, 100.0, 14),
+        (0, xtgpu.STENCIL, 33, 17, 3, 1, 100.0, 15), (2, xtgpu.PATHTRACER, 24, 24, 4, 4, 100.0, 16)]
+
+
+@pytest.mark.parametrize("fmt", [xtgpu.NODES_FP32, xtgpu.NODES_Q8])
+def test_job_alone_equals_job_in_mix(resident, fmt):
+    alone = []
+    for (s, integ, w, h, spp, d, md, seed) in JOBS:
+        img, _ = resident[s].render(integ, w, h, spp=spp, rdepth=d, ao_max_distance=md, seed=seed, node_format=fmt)
+        alone.append(img)
+    for wave, graphs in ((1 << 22, True), (777, True), (5000, False)):
+        svc = Service(resident, node_format=fmt, wave_paths=wave, use_graphs=graphs, merge_jobs=True,
+                      memory_budget=1 << 30)
+        ids = [svc.submit(s, integ, w, h, spp, d, md, seed) for (s, integ, w, h, spp, d, md, seed) in JOBS]
+        svc.run()
+        for jid, ref in zip(ids, alone):
+            st = svc.poll(jid)
+            assert st.state == 2
+            out = svc.result(jid)
+            assert np.array_equal(out, ref), "job %d differs in the mix (wave=%d)" % (jid, wave)
+            svc.release(jid)
+        svc.close()
+
+
+def test_plain_path_equals_served(resident):
+    plain = Service(resident, node_format=xtgpu.NODES_FP32, use_graphs=False, merge_jobs=False)
+    served = Service(resident, node_format=xtgpu.NODES_FP32, use_graphs=True, merge_jobs=True)
+    a = [plain.submit(*j) for j in JOBS]
+    b = [served.submit(*j) for j in JOBS]
+    plain.run()
+    served.run()
+    for x, y in zip(a, b):
+        assert np.array_equal(plain.result(x), served.result(y))
+        assert plain.poll(x).rays == served.poll(y).rays
+    plain.close()
+    served.close()
+
+
+def test_memory_budget_limits_concurrency(resident):
+    # budget for exactly one 64x64 frame: jobs run one after another
+    svc = Service(resident, memory_budget=64 * 64 * 16, merge_jobs=True, host_results=True)
+    ids = [svc.submit(0, xtgpu.STENCIL, 64, 64, 1, 1, 100.0, k) for k in range(4)]
+    big = svc.submit(0, xtgpu.STENCIL, 128, 128, 1, 1, 100.0, 9)   # never fits
+    svc.run()
+    sts = [svc.poll(i) for i in ids]
+    assert all(s.state == 2 for s in sts)
+    for s0, s1 in zip(sts, sts[1:]):
+        assert s1.start_s >= s0.finish_s - 1e-6
+    assert svc.poll(big).state == 3
+    svc.close()
+
+
+def test_arrivals_and_latency_bookkeeping(resident):
+    svc = Service(resident, merge_jobs=True)
+    ids = [svc.submit(0, xtgpu.PATHTRACER, 32, 32, 4, 4, 100.0, k, submit_s=0.05 * k) for k in range(5)]
+    svc.run()
+    for k, i in enumerate(ids):
+        st = svc.poll(i)
+        assert st.state == 2
+        assert st.submit_s == pytest.approx(0.05 * k)
+        assert st.start_s >= st.submit_s - 1e-6
+        assert st.finish_s >= st.start_s
+        assert st.rays > 0
+    svc.close()

@@ -1,0 +1,478 @@
+// C ABI entry points (include/xtgpu.h): scene upload, BVH build/export, batched
+// closest-hit tracing and single-job frame rendering.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "render.h"
+
+namespace xtg {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string &msg) { g_err = msg; }
+
+xtgpu_status cuda_fail(cudaError_t e, const char *what, const char *file, int line)
+{
+    char buf[512];
+    snprintf(buf, sizeof(buf), "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+    g_err = buf;
+    return e == cudaErrorMemoryAllocation ? XTGPU_ERR_NOMEM : XTGPU_ERR_CUDA;
+}
+
+xtgpu_status dalloc(HostBuf &b, size_t bytes, cudaStream_t s)
+{
+    (void)s;
+    dfree(b);
+    cudaError_t e = cudaMalloc(&b.p, bytes ? bytes : 16);
+    if (e != cudaSuccess) {
+        b.p = nullptr;
+        return cuda_fail(e, "cudaMalloc", __FILE__, __LINE__);
+    }
+    b.bytes = bytes;
+    return XTGPU_OK;
+}
+
+void dfree(HostBuf &b)
+{
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+// Perspective::calculate_transform (camera/perspective.cc:26-36) in FP64.
+struct d3 {
+    double x, y, z;
+};
+static d3 dsub(d3 a, d3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+static d3 dcross(d3 a, d3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+static d3 dnorm(d3 a)
+{
+    double l = std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
+    return l != 0 ? d3{a.x / l, a.y / l, a.z / l} : a;
+}
+
+DevCamera make_camera(const xtgpu_camera &c)
+{
+    DevCamera k;
+    d3 pos{c.position[0], c.position[1], c.position[2]};
+    d3 tgt{c.target[0], c.target[1], c.target[2]};
+    d3 up{c.up[0], c.up[1], c.up[2]};
+    d3 rz = dnorm(dsub(tgt, pos));
+    d3 rx = dnorm(dcross(up, rz));
+    d3 ry = dnorm(dcross(rx, rz));
+    k.pos[0] = pos.x; k.pos[1] = pos.y; k.pos[2] = pos.z;
+    k.rx[0] = rx.x; k.rx[1] = rx.y; k.rx[2] = rx.z;
+    k.ry[0] = ry.x; k.ry[1] = ry.y; k.ry[2] = ry.z;
+    k.rz[0] = rz.x; k.rz[1] = rz.y; k.rz[2] = rz.z;
+    const double RADIAN = 0.017453292519943;   // lib/nmath/precision.h:111
+    k.dz = 1.0 / std::tan(c.fov * RADIAN / 2.0);
+    return k;
+}
+
+// One wave runner per process, shared by xtgpu_render calls.
+static std::mutex g_runner_mu;
+static WaveRunner *g_runner = nullptr;
+static int64_t g_runner_cap = 0;
+
+static xtgpu_status get_runner(int64_t cap, cudaStream_t s, WaveRunner **out)
+{
+    if (!g_runner || g_runner_cap < cap) {
+        if (g_runner) {
+            cudaStreamSynchronize(s);
+            g_runner->release();
+            delete g_runner;
+            g_runner = nullptr;
+        }
+        g_runner = new WaveRunner();
+        xtgpu_status st = g_runner->init(cap, 4, 1, s);
+        if (st != XTGPU_OK) {
+            g_runner->release();
+            delete g_runner;
+            g_runner = nullptr;
+            return st;
+        }
+        g_runner_cap = cap;
+    }
+    *out = g_runner;
+    return XTGPU_OK;
+}
+
+}  // namespace xtg
+
+using namespace xtg;
+
+extern "C" {
+
+const char *xtgpu_last_error(void) { return g_err.c_str(); }
+const char *xtgpu_version(void) { return "xtgpu 0.1 (sm_100a)"; }
+
+xtgpu_status xtgpu_scene_create(const xtgpu_scene_desc *d, void *stream, xtgpu_scene **out)
+{
+    if (!d || !out) {
+        set_error("xtgpu_scene_create: NULL argument");
+        return XTGPU_ERR_INVALID;
+    }
+    *out = nullptr;
+    if (d->n_tris < 0 || d->n_spheres < 0 || d->n_planes < 0 || d->n_objects < 0 || d->n_materials < 0 ||
+        (d->n_tris && !d->tris) || (d->n_spheres && !d->spheres) || (d->n_planes && !d->planes) ||
+        (d->n_objects && (!d->obj_kind || !d->obj_first || !d->obj_count || !d->obj_material)) ||
+        (d->n_materials && !d->materials)) {
+        set_error("xtgpu_scene_create: inconsistent sizes or NULL arrays");
+        return XTGPU_ERR_INVALID;
+    }
+    const int64_t nprim = (int64_t)d->n_tris + d->n_spheres + d->n_planes;
+    // every primitive must belong to exactly one object with a valid material
+    std::vector<int32_t> prim_obj((size_t)std::max<int64_t>(1, nprim), -1);
+    for (int32_t o = 0; o < d->n_objects; ++o) {
+        int32_t k = d->obj_kind[o], f = d->obj_first[o], c = d->obj_count[o], m = d->obj_material[o];
+        if (m < 0 || m >= d->n_materials) {
+            set_error("xtgpu_scene_create: object material out of range");
+            return XTGPU_ERR_INVALID;
+        }
+        int64_t base, lim;
+        if (k == XTGPU_MESH) { base = 0; lim = d->n_tris; }
+        else if (k == XTGPU_SPHERE) { base = d->n_tris; lim = d->n_spheres; c = 1; }
+        else if (k == XTGPU_PLANE) { base = (int64_t)d->n_tris + d->n_spheres; lim = d->n_planes; c = 1; }
+        else {
+            set_error("xtgpu_scene_create: bad object kind");
+            return XTGPU_ERR_INVALID;
+        }
+        if (f < 0 || c < 0 || (int64_t)f + c > lim) {
+            set_error("xtgpu_scene_create: object range out of bounds");
+            return XTGPU_ERR_INVALID;
+        }
+        for (int64_t i = 0; i < c; ++i) prim_obj[(size_t)(base + f + i)] = o;
+    }
+    for (int64_t i = 0; i < nprim; ++i)
+        if (prim_obj[(size_t)i] < 0) {
+            set_error("xtgpu_scene_create: a primitive belongs to no object");
+            return XTGPU_ERR_INVALID;
+        }
+    if (d->env_type < XTGPU_ENV_NONE || d->env_type > XTGPU_ENV_GRADIENT) {
+        set_error("xtgpu_scene_create: bad environment type");
+        return XTGPU_ERR_INVALID;
+    }
+
+    cudaStream_t s = (cudaStream_t)stream;
+    xtgpu_scene *sc = new xtgpu_scene();
+    cudaGetDevice(&sc->device);
+    auto fail = [&](xtgpu_status st) {
+        xtgpu_scene_destroy(sc);
+        return st;
+    };
+    // triangles as 3 x float4 per triangle
+    std::vector<float4> tv((size_t)std::max(1, 3 * d->n_tris));
+    for (int32_t i = 0; i < d->n_tris; ++i)
+        for (int k = 0; k < 3; ++k)
+            tv[3 * i + k] = make_float4(d->tris[9 * (size_t)i + 3 * k], d->tris[9 * (size_t)i + 3 * k + 1],
+                                        d->tris[9 * (size_t)i + 3 * k + 2], 0.f);
+    xtgpu_status st;
+    if ((st = dalloc(sc->tri_v, sizeof(float4) * tv.size(), s)) != XTGPU_OK) return fail(st);
+    if (cudaMemcpy(sc->tri_v.p, tv.data(), sizeof(float4) * tv.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(cuda_fail(cudaGetLastError(), "cudaMemcpy", __FILE__, __LINE__));
+    if (d->tri_normals && d->n_tris) {
+        for (int32_t i = 0; i < d->n_tris; ++i)
+            for (int k = 0; k < 3; ++k)
+                tv[3 * i + k] = make_float4(d->tri_normals[9 * (size_t)i + 3 * k], d->tri_normals[9 * (size_t)i + 3 * k + 1],
+                                            d->tri_normals[9 * (size_t)i + 3 * k + 2], 0.f);
+        if ((st = dalloc(sc->tri_n, sizeof(float4) * tv.size(), s)) != XTGPU_OK) return fail(st);
+        cudaMemcpy(sc->tri_n.p, tv.data(), sizeof(float4) * tv.size(), cudaMemcpyHostToDevice);
+    }
+    std::vector<float4> sp((size_t)std::max(1, d->n_spheres)), pl((size_t)std::max(1, d->n_planes));
+    for (int32_t i = 0; i < d->n_spheres; ++i)
+        sp[i] = make_float4(d->spheres[4 * i], d->spheres[4 * i + 1], d->spheres[4 * i + 2], d->spheres[4 * i + 3]);
+    for (int32_t i = 0; i < d->n_planes; ++i)
+        pl[i] = make_float4(d->planes[4 * i], d->planes[4 * i + 1], d->planes[4 * i + 2], d->planes[4 * i + 3]);
+    if ((st = dalloc(sc->spheres, sizeof(float4) * sp.size(), s)) != XTGPU_OK) return fail(st);
+    if ((st = dalloc(sc->planes, sizeof(float4) * pl.size(), s)) != XTGPU_OK) return fail(st);
+    if ((st = dalloc(sc->prim_obj, sizeof(int32_t) * prim_obj.size(), s)) != XTGPU_OK) return fail(st);
+    std::vector<DevMaterial> mats((size_t)std::max(1, d->n_materials));
+    for (int32_t i = 0; i < d->n_materials; ++i) {
+        const xtgpu_material &m = d->materials[i];
+        mats[i].type = m.type;
+        mats[i].diffuse = make_float3(m.diffuse[0], m.diffuse[1], m.diffuse[2]);
+        mats[i].specular = make_float3(m.specular[0], m.specular[1], m.specular[2]);
+        mats[i].emissive = make_float3(m.emissive[0], m.emissive[1], m.emissive[2]);
+        mats[i].reflectance = m.reflectance;
+        mats[i].exponent = m.exponent;
+        mats[i].ior = m.ior;
+    }
+    std::vector<int32_t> om((size_t)std::max(1, d->n_objects));
+    for (int32_t i = 0; i < d->n_objects; ++i) om[i] = d->obj_material[i];
+    if ((st = dalloc(sc->materials, sizeof(DevMaterial) * mats.size(), s)) != XTGPU_OK) return fail(st);
+    if ((st = dalloc(sc->obj_material, sizeof(int32_t) * om.size(), s)) != XTGPU_OK) return fail(st);
+    cudaMemcpy(sc->spheres.p, sp.data(), sizeof(float4) * sp.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(sc->planes.p, pl.data(), sizeof(float4) * pl.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(sc->prim_obj.p, prim_obj.data(), sizeof(int32_t) * prim_obj.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(sc->materials.p, mats.data(), sizeof(DevMaterial) * mats.size(), cudaMemcpyHostToDevice);
+    if (cudaMemcpy(sc->obj_material.p, om.data(), sizeof(int32_t) * om.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(cuda_fail(cudaGetLastError(), "cudaMemcpy", __FILE__, __LINE__));
+
+    DevScene &S = sc->dev;
+    S.tri_v = (const float4 *)sc->tri_v.p;
+    S.tri_n = (const float4 *)sc->tri_n.p;
+    S.spheres = (const float4 *)sc->spheres.p;
+    S.planes = (const float4 *)sc->planes.p;
+    S.prim_obj = (const int32_t *)sc->prim_obj.p;
+    S.obj_material = (const int32_t *)sc->obj_material.p;
+    S.materials = (const DevMaterial *)sc->materials.p;
+    S.n_tris = d->n_tris;
+    S.n_spheres = d->n_spheres;
+    S.n_planes = d->n_planes;
+    S.root = EMPTY_REF;
+    S.env_type = d->env_type;
+    S.env_a = make_float3(d->env_a[0], d->env_a[1], d->env_a[2]);
+    S.env_b = make_float3(d->env_b[0], d->env_b[1], d->env_b[2]);
+    S.cam = make_camera(d->camera);
+    sc->n_objects = d->n_objects;
+    *out = sc;
+    return XTGPU_OK;
+}
+
+xtgpu_status xtgpu_bvh_build(xtgpu_scene *sc, const xtgpu_bvh_opts *opts, void *stream)
+{
+    if (!sc) {
+        set_error("xtgpu_bvh_build: NULL scene");
+        return XTGPU_ERR_INVALID;
+    }
+    int fmt = opts ? opts->node_format : XTGPU_NODES_FP32;
+    int leaf = opts && opts->leaf_size > 0 ? opts->leaf_size : 2;
+    if (fmt != XTGPU_NODES_FP32 && fmt != XTGPU_NODES_Q8) {
+        set_error("xtgpu_bvh_build: bad node format");
+        return XTGPU_ERR_INVALID;
+    }
+    if (leaf < 1 || leaf > MAX_LEAF) {
+        set_error("xtgpu_bvh_build: leaf_size out of range");
+        return XTGPU_ERR_INVALID;
+    }
+    return build_bvh(sc, fmt, leaf, (cudaStream_t)stream);
+}
+
+xtgpu_status xtgpu_scene_destroy(xtgpu_scene *sc)
+{
+    if (!sc) return XTGPU_OK;
+    for (HostBuf *b : {&sc->tri_v, &sc->tri_n, &sc->spheres, &sc->planes, &sc->prim_obj, &sc->obj_material,
+                       &sc->materials, &sc->leaf_prims, &sc->nodes32, &sc->nodes8, &sc->morton, &sc->order,
+                       &sc->left, &sc->right})
+        dfree(*b);
+    delete sc;
+    return XTGPU_OK;
+}
+
+xtgpu_status xtgpu_scene_device_bytes(const xtgpu_scene *sc, uint64_t *bytes)
+{
+    if (!sc || !bytes) {
+        set_error("xtgpu_scene_device_bytes: NULL argument");
+        return XTGPU_ERR_INVALID;
+    }
+    uint64_t b = 0;
+    for (const HostBuf *h : {&sc->tri_v, &sc->tri_n, &sc->spheres, &sc->planes, &sc->prim_obj, &sc->obj_material,
+                             &sc->materials, &sc->leaf_prims, &sc->nodes32, &sc->nodes8, &sc->morton, &sc->order,
+                             &sc->left, &sc->right})
+        b += h->bytes;
+    *bytes = b;
+    return XTGPU_OK;
+}
+
+xtgpu_status xtgpu_bvh_export(const xtgpu_scene *sc, xtgpu_bvh_info *info, uint32_t *morton, uint32_t *order,
+                              int32_t *left, int32_t *right, void *stream)
+{
+    if (!sc) {
+        set_error("xtgpu_bvh_export: NULL scene");
+        return XTGPU_ERR_INVALID;
+    }
+    if (!sc->built32) {
+        set_error("xtgpu_bvh_export: BVH not built");
+        return XTGPU_ERR_STATE;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    XTG_CUDA(cudaStreamSynchronize(s));
+    int64_t n = sc->n_prims;
+    if (info) {
+        info->n_prims = n;
+        info->depth = sc->depth;
+        info->leaf_size = sc->leaf_size;
+        info->node_bytes_fp32 = sc->nodes32.bytes;
+        info->node_bytes_q8 = sc->nodes8.bytes;
+    }
+    if (n > 0) {
+        if (morton) XTG_CUDA(cudaMemcpy(morton, sc->morton.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+        if (order) XTG_CUDA(cudaMemcpy(order, sc->order.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+        if (n > 1 && left) XTG_CUDA(cudaMemcpy(left, sc->left.p, sizeof(int32_t) * (n - 1), cudaMemcpyDeviceToHost));
+        if (n > 1 && right) XTG_CUDA(cudaMemcpy(right, sc->right.p, sizeof(int32_t) * (n - 1), cudaMemcpyDeviceToHost));
+    }
+    return XTGPU_OK;
+}
+
+static xtgpu_status check_format(const xtgpu_scene *sc, int32_t fmt)
+{
+    if (fmt == XTGPU_NODES_FP32 && sc->built32) return XTGPU_OK;
+    if (fmt == XTGPU_NODES_Q8 && sc->built8) return XTGPU_OK;
+    set_error("node format not built for this scene");
+    return XTGPU_ERR_STATE;
+}
+
+xtgpu_status xtgpu_trace(xtgpu_scene *sc, int64_t n, const void *org, const void *dir, xtgpu_hit *hits, int32_t fmt,
+                         void *stream)
+{
+    if (!sc || n < 0 || (n && (!org || !dir || !hits))) {
+        set_error("xtgpu_trace: bad argument");
+        return XTGPU_ERR_INVALID;
+    }
+    XTG_TRY(check_format(sc, fmt));
+    if (n == 0) return XTGPU_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    int32_t *ctl = nullptr;
+    XTG_CUDA(cudaMallocAsync((void **)&ctl, 64, s));
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int32_t overflow = 0;
+    for (int64_t base = 0; base < n; base += (1ll << 30)) {
+        int32_t cnt = (int32_t)std::min<int64_t>(n - base, 1ll << 30);
+        WaveQueues q{};
+        q.org[0] = (float4 *)((const float4 *)org + base);
+        q.dir[0] = (float4 *)((const float4 *)dir + base);
+        q.hit = hits + base;
+        q.ctl = ctl;
+        q.rays = (unsigned long long *)((char *)ctl + 32);
+        int32_t init[4] = {cnt, 0, 0, 0};
+        XTG_CUDA(cudaMemcpyAsync(ctl, init, sizeof(init), cudaMemcpyHostToDevice, s));
+        launch_extend(fmt, sc->dev, q, 0, sms * 12, s);
+        XTG_CUDA(cudaGetLastError());
+        int32_t back[4];
+        XTG_CUDA(cudaMemcpyAsync(back, ctl, sizeof(back), cudaMemcpyDeviceToHost, s));
+        XTG_CUDA(cudaStreamSynchronize(s));
+        overflow |= back[3];
+    }
+    cudaFreeAsync(ctl, s);
+    if (overflow) {
+        set_error("xtgpu_trace: traversal stack overflow");
+        return XTGPU_ERR_LIMIT;
+    }
+    return XTGPU_OK;
+}
+
+xtgpu_status xtgpu_trace_host(xtgpu_scene *sc, int64_t n, const float *org, const float *dir, xtgpu_hit *hits,
+                              int32_t fmt, void *stream)
+{
+    if (!sc || n < 0 || (n && (!org || !dir || !hits))) {
+        set_error("xtgpu_trace_host: bad argument");
+        return XTGPU_ERR_INVALID;
+    }
+    if (n == 0) return XTGPU_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    float4 *dorg = nullptr, *ddir = nullptr;
+    xtgpu_hit *dhit = nullptr;
+    XTG_CUDA(cudaMallocAsync((void **)&dorg, sizeof(float4) * n, s));
+    XTG_CUDA(cudaMallocAsync((void **)&ddir, sizeof(float4) * n, s));
+    XTG_CUDA(cudaMallocAsync((void **)&dhit, sizeof(xtgpu_hit) * n, s));
+    XTG_CUDA(cudaMemcpyAsync(dorg, org, sizeof(float4) * n, cudaMemcpyHostToDevice, s));
+    XTG_CUDA(cudaMemcpyAsync(ddir, dir, sizeof(float4) * n, cudaMemcpyHostToDevice, s));
+    xtgpu_status st = xtgpu_trace(sc, n, dorg, ddir, dhit, fmt, stream);
+    if (st == XTGPU_OK) {
+        cudaError_t e = cudaMemcpyAsync(hits, dhit, sizeof(xtgpu_hit) * n, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = cuda_fail(e, "cudaMemcpyAsync", __FILE__, __LINE__);
+    }
+    cudaFreeAsync(dorg, s);
+    cudaFreeAsync(ddir, s);
+    cudaFreeAsync(dhit, s);
+    return st;
+}
+
+xtgpu_status xtgpu_render(xtgpu_scene *sc, const xtgpu_render_params *p, float *rgba, uint64_t *rays, void *stream)
+{
+    if (!sc || !p || !rgba) {
+        set_error("xtgpu_render: NULL argument");
+        return XTGPU_ERR_INVALID;
+    }
+    if (p->integrator < XTGPU_STENCIL || p->integrator > XTGPU_PATHTRACER || p->width <= 0 || p->height <= 0 ||
+        p->spp <= 0 || p->rdepth < 0 || (p->integrator == XTGPU_AO && !(p->ao_max_distance > 0.f))) {
+        set_error("xtgpu_render: bad parameters");
+        return XTGPU_ERR_INVALID;
+    }
+    int x0 = p->x0, y0 = p->y0, x1 = p->x1, y1 = p->y1;
+    if (x1 == 0 && y1 == 0) {
+        x0 = y0 = 0;
+        x1 = p->width;
+        y1 = p->height;
+    }
+    if (x0 < 0 || y0 < 0 || x1 > p->width || y1 > p->height || x0 >= x1 || y0 >= y1) {
+        set_error("xtgpu_render: bad rectangle");
+        return XTGPU_ERR_INVALID;
+    }
+    XTG_TRY(check_format(sc, p->node_format));
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t npix = (int64_t)(x1 - x0) * (y1 - y0);
+    const int64_t paths = npix * p->spp;
+    const int64_t cap = std::min<int64_t>(paths, 1ll << 22);
+    std::lock_guard<std::mutex> lock(g_runner_mu);
+    WaveRunner *R = nullptr;
+    XTG_TRY(get_runner(std::max<int64_t>(cap, 1 << 16), s, &R));
+    XTG_TRY(R->set_scenes(&sc->dev, 1, s));
+    XTG_CUDA(cudaMemsetAsync(R->q.ctl, 0, 64, s));
+    XTG_CUDA(cudaMemsetAsync(rgba, 0, sizeof(float4) * npix, s));
+    DevJob J{};
+    J.integrator = p->integrator;
+    J.width = p->width;
+    J.height = p->height;
+    J.spp = p->spp;
+    J.rdepth = p->rdepth;
+    J.ao_maxd = p->ao_max_distance;
+    J.seed = p->seed;
+    J.x0 = x0;
+    J.y0 = y0;
+    J.rw = x1 - x0;
+    J.rh = y1 - y0;
+    J.scene = 0;
+    J.bounces = bounces_of(p->integrator, p->rdepth);
+    J.frame = (float4 *)rgba;
+    std::vector<DevJob> jobs(1, J);
+    for (int64_t first = 0; first < paths; first += R->cap) {
+        jobs[0].first = first;
+        jobs[0].count = std::min<int64_t>(R->cap, paths - first);
+        XTG_TRY(R->run_wave(jobs, J.bounces, p->node_format, false, s));
+    }
+    int32_t overflow = 0;
+    unsigned long long nr = 0;
+    XTG_TRY(R->read_ctl(&overflow, &nr, s));
+    if (rays) *rays = nr;
+    if (overflow) {
+        set_error("xtgpu_render: traversal stack overflow");
+        return XTGPU_ERR_LIMIT;
+    }
+    return XTGPU_OK;
+}
+
+xtgpu_status xtgpu_render_host(xtgpu_scene *sc, const xtgpu_render_params *p, float *rgba_host, uint64_t *rays,
+                               void *stream)
+{
+    if (!sc || !p || !rgba_host) {
+        set_error("xtgpu_render_host: NULL argument");
+        return XTGPU_ERR_INVALID;
+    }
+    int64_t w = (p->x1 == 0 && p->y1 == 0) ? p->width : p->x1 - p->x0;
+    int64_t h = (p->x1 == 0 && p->y1 == 0) ? p->height : p->y1 - p->y0;
+    if (w <= 0 || h <= 0) {
+        set_error("xtgpu_render_host: bad rectangle");
+        return XTGPU_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    float *d = nullptr;
+    XTG_CUDA(cudaMallocAsync((void **)&d, sizeof(float4) * w * h, s));
+    xtgpu_status st = xtgpu_render(sc, p, d, rays, stream);
+    if (st == XTGPU_OK) {
+        cudaError_t e = cudaMemcpyAsync(rgba_host, d, sizeof(float4) * w * h, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = cuda_fail(e, "cudaMemcpyAsync", __FILE__, __LINE__);
+    }
+    cudaFreeAsync(d, s);
+    return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,676 @@
+// Wavefront kernels and the wave runner shared by xtgpu_render (one job) and
+// the render service (many jobs merged per wave).
+//
+// Per-sample semantics restated from the reference (paths relative to the
+// XTracer source tree):
+//   camera      Perspective::get_primary_ray, camera/perspective.cc:38-98, in
+//               FP64 with every operation rounded as the reference rounds it
+//   stencil     integrator/stencil/integrator.cc:13-33
+//   depth       integrator/depth/integrator.cc:15-54
+//   ao          integrator/ao/integrator.cc:14-52 (maximum distance a parameter)
+//   pathtracer  integrator/pathtracer/integrator.cc:21-74 and the materials'
+//               sample_path (material/lambert.cc:30-40, phong.cc:35-55,
+//               blinnphong.cc:34-61, emissive.cc:20-27, dielectric.cc:22-31)
+//   sampling    lib/nmath/sample.inl:28-107, in FP32
+#include <algorithm>
+#include <vector>
+
+#include "render.h"
+
+namespace xtg {
+
+// ---------------------------------------------------------------------------
+// random stream: SplitMix64 finaliser of (path key + counter)
+__device__ __forceinline__ uint64_t mix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ uint64_t path_key(uint64_t seed, uint64_t path)
+{
+    return mix64(seed ^ mix64(path + 0x9E3779B97F4A7C15ull));
+}
+__device__ __forceinline__ float uniform(uint64_t key, uint32_t &ctr)
+{
+    uint64_t x = mix64(key + (uint64_t)(ctr + 1u) * 0x9E3779B97F4A7C15ull);
+    ++ctr;
+    return (float)(uint32_t)(x >> 40) * (1.0f / 16777216.0f);
+}
+
+__device__ __forceinline__ float3 f3(float4 v) { return make_float3(v.x, v.y, v.z); }
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator*(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross3(float3 a, float3 b)
+{
+    return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float3 normalized(float3 a)
+{
+    float l = sqrtf(dot3(a, a));
+    return l != 0.f ? make_float3(a.x / l, a.y / l, a.z / l) : a;
+}
+// colour channels are clamped at 0 by every operation (lib/nimg/color.inl:48-61)
+__device__ __forceinline__ float c0(float v) { return v < 0.f ? 0.f : v; }
+__device__ __forceinline__ float3 cmul(float3 a, float3 b) { return make_float3(c0(a.x * b.x), c0(a.y * b.y), c0(a.z * b.z)); }
+__device__ __forceinline__ float3 cmuls(float3 a, float s) { return make_float3(c0(a.x * s), c0(a.y * s), c0(a.z * s)); }
+
+// Perspective::get_primary_ray (camera/perspective.cc:38-98), FP64, no contraction.
+__device__ __forceinline__ void camera_ray(const DevCamera &c, float x, float y, float w, float h, float3 &o,
+                                           float3 &d)
+{
+    double aspect = __ddiv_rn((double)w, (double)h);
+    double dx = __dsub_rn(__ddiv_rn(__dmul_rn(2.0, (double)x), (double)w), 1.0);
+    double dy = __ddiv_rn(__dsub_rn(__ddiv_rn(__dmul_rn(2.0, (double)y), (double)h), 1.0), aspect);
+    double dz = c.dz;
+    double t[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        t[k] = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(c.rx[k], dx), __dmul_rn(c.ry[k], dy)), __dmul_rn(c.rz[k], dz)),
+                         0.0);
+    double len = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(t[0], t[0]), __dmul_rn(t[1], t[1])), __dmul_rn(t[2], t[2])));
+    if (len != 0.0) {
+        t[0] = __ddiv_rn(t[0], len);
+        t[1] = __ddiv_rn(t[1], len);
+        t[2] = __ddiv_rn(t[2], len);
+    }
+    o = make_float3((float)c.pos[0], (float)c.pos[1], (float)c.pos[2]);
+    d = make_float3((float)t[0], (float)t[1], (float)t[2]);
+}
+
+// Origin moved off the surface along n by a few ulps (Waechter and Binder, "A
+// Fast and Robust Method for Avoiding Self-Intersection", Ray Tracing Gems
+// 2019); the reference moves it by n * 1e-8, which FP32 cannot resolve.
+__device__ __forceinline__ float3 offset_ray(float3 p, float3 n)
+{
+    const float origin = 1.0f / 32.0f, fscale = 1.0f / 65536.0f, iscale = 256.0f;
+    int ix = (int)(iscale * n.x), iy = (int)(iscale * n.y), iz = (int)(iscale * n.z);
+    float px = __int_as_float(__float_as_int(p.x) + (p.x < 0.f ? -ix : ix));
+    float py = __int_as_float(__float_as_int(p.y) + (p.y < 0.f ? -iy : iy));
+    float pz = __int_as_float(__float_as_int(p.z) + (p.z < 0.f ? -iz : iz));
+    return make_float3(fabsf(p.x) < origin ? p.x + fscale * n.x : px, fabsf(p.y) < origin ? p.y + fscale * n.y : py,
+                       fabsf(p.z) < origin ? p.z + fscale * n.z : pz);
+}
+
+// sample::hemisphere (sample.inl:28-59).  cross(n + eps, n) = eps * cross((1,1,1), n).
+__device__ float3 s_hemisphere(float3 n, uint64_t key, uint32_t &ctr)
+{
+    float u = uniform(key, ctr), v = uniform(key, ctr);
+    float phi = acosf(sqrtf(u));
+    float theta = 6.283185307179586f * v;
+    float sp, cp, st, ct;
+    sincosf(phi, &sp, &cp);
+    sincosf(theta, &st, &ct);
+    float3 d = make_float3(ct * sp, cp, st * sp);
+    float3 nn = normalized(n);
+    float3 xv = normalized(cross3(make_float3(1.f, 1.f, 1.f), nn));
+    float3 zv = normalized(cross3(xv, nn));
+    return normalized(xv * d.x + nn * d.y + zv * d.z);
+}
+
+// sample::diffuse (sample.inl:92-107): rejection on x^4 + y^4 + z^4 < 1; the
+// first value drawn is z, as the reference build evaluates the three draws.
+__device__ float3 s_diffuse(float3 n, uint64_t key, uint32_t &ctr)
+{
+    float3 p = make_float3(0.f, 0.f, 0.f);
+    for (int it = 0; it < 256; ++it) {
+        float c = uniform(key, ctr), b = uniform(key, ctr), a = uniform(key, ctr);
+        p = make_float3(2.f * a - 1.f, 2.f * b - 1.f, 2.f * c - 1.f);
+        float x2 = p.x * p.x, y2 = p.y * p.y, z2 = p.z * p.z;
+        if (x2 * x2 + y2 * y2 + z2 * z2 < 1.0f) break;
+    }
+    return normalized(p + n);
+}
+
+// sample::lobe (sample.inl:61-90).  vc * pow(vdotr, e) normalised is vc (or 0).
+__device__ float3 s_lobe(float3 n, float3 dir, float e, uint64_t key, uint32_t &ctr)
+{
+    float3 i = normalized(dir), nn = normalized(n);
+    float3 refl = nn * (2.f * dot3(i, nn)) - i;
+    float3 cx = make_float3(1.f, 0.f, 0.f), cy = make_float3(0.f, 1.f, 0.f), cz = make_float3(0.f, 0.f, 1.f);
+    if (1.0f - dot3(dir, n) > 1e-8f) {
+        cx = normalized(cross3(dir, refl));
+        cy = refl;
+        cz = cross3(refl, cx);
+    }
+    float u = uniform(key, ctr), v = uniform(key, ctr);
+    float theta = 6.283185307179586f * u;
+    float phi = acosf(powf(v, 1.0f / (e + 1.0f)));
+    float sp, cp, st, ct;
+    sincosf(phi, &sp, &cp);
+    sincosf(theta, &st, &ct);
+    float3 vc = cx * (ct * sp) + cy * cp + cz * (st * sp);
+    float vdotr = dot3(refl, vc);
+    return vdotr > 0.f ? normalized(vc) : make_float3(0.f, 0.f, 0.f);
+}
+
+__device__ __forceinline__ float3 environment(const DevScene &S, float3 dir)
+{
+    if (S.env_type == XTGPU_ENV_COLOR) return S.env_a;
+    if (S.env_type == XTGPU_ENV_GRADIENT) {   // sampler_gradient.cc:11-17
+        float3 d = normalized(dir);
+        float t = 0.5f * d.y + 1.0f;
+        float3 a = cmuls(S.env_a, 1.0f - t), b = cmuls(S.env_b, t);
+        return make_float3(c0(a.x + b.x), c0(a.y + b.y), c0(a.z + b.z));
+    }
+    return make_float3(0.f, 0.f, 0.f);
+}
+
+// Hit record normal as the reference forms it: triangles the face normal (or the
+// barycentric blend of vertex normals when given, not renormalised), spheres
+// (p - c) / r, planes the stored normal.
+__device__ __forceinline__ float3 hit_normal(const DevScene &S, uint32_t prim, float3 p, float bu, float bv)
+{
+    if ((int)prim < S.n_tris) {
+        float3 a = f3(S.tri_v[3 * prim]), b = f3(S.tri_v[3 * prim + 1]), c = f3(S.tri_v[3 * prim + 2]);
+        float3 fn = normalized(cross3(b - a, c - a));
+        if (S.tri_n) {
+            float bw = 1.f - bu - bv;
+            float3 na = f3(S.tri_n[3 * prim]), nb = f3(S.tri_n[3 * prim + 1]), nc = f3(S.tri_n[3 * prim + 2]);
+            float3 pn = na * bw + nb * bu + nc * bv;
+            if (dot3(pn, pn) != 0.f) return pn;
+        }
+        return fn;
+    }
+    if ((int)prim < S.n_tris + S.n_spheres) {
+        float4 s = S.spheres[prim - S.n_tris];
+        return make_float3((p.x - s.x) / s.w, (p.y - s.y) / s.w, (p.z - s.z) / s.w);
+    }
+    return f3(S.planes[prim - S.n_tris - S.n_spheres]);
+}
+
+__device__ __forceinline__ int find_job(const DevJob *jobs, int njobs, int64_t i)
+{
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].offset <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int warp_append(int32_t *counter, bool pred)
+{
+    unsigned act = __activemask();
+    unsigned m = __ballot_sync(act, pred);
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(act) - 1;
+    int base = 0;
+    if (lane == leader && m) base = atomicAdd(counter, __popc(m));
+    base = __shfl_sync(act, base, leader);
+    return base + __popc(m & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ const DevScene &scene_of(const DevScene *scenes, const DevJob &j) { return scenes[j.scene]; }
+
+// ---------------------------------------------------------------------------
+__global__ void k_camera(const DevJob *__restrict__ jobs, const DevScene *__restrict__ scenes, WaveQueues q)
+{
+    const int njobs = q.ctl[4];
+    const int64_t total = q.ctl[5];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        int jn = find_job(jobs, njobs, i);
+        const DevJob &J = jobs[jn];
+        int64_t p = J.first + (i - J.offset);
+        int64_t npix = (int64_t)J.rw * J.rh;
+        int64_t s = p / npix, pix = p - s * npix;
+        int x = J.x0 + (int)(pix % J.rw), y = J.y0 + (int)(pix / J.rw);
+        float3 o, d;
+        camera_ray(scenes[J.scene].cam, (float)x + 0.5f, (float)y + 0.5f, (float)J.width, (float)J.height, o, d);
+        q.org[0][i] = make_float4(o.x, o.y, o.z, 0.f);
+        q.dir[0][i] = make_float4(d.x, d.y, d.z, INFINITY);
+        q.meta[0][i] = make_uint2((uint32_t)i, (uint32_t)jn);
+        q.P[0][i] = make_float4(1.f, 1.f, 1.f, __uint_as_float(0u));
+        q.I[0][i] = make_float4(1.f, 1.f, 1.f, __int_as_float(J.bounces));
+        q.contrib[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+
+// Persistent extend: each warp takes 32 queued rays at a time from a global
+// counter until the queue is drained.
+template <int FMT, bool MULTI>
+__global__ void __launch_bounds__(128) k_extend(DevScene S1, const DevScene *__restrict__ scenes,
+                                                const DevJob *__restrict__ jobs, WaveQueues q, int side)
+{
+    const int n = q.ctl[side];
+    const int lane = threadIdx.x & 31;
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(q.rays, (unsigned long long)n);
+    const bool per_job = q.job_rays != nullptr;
+    const float4 *org = q.org[side], *dir = q.dir[side];
+    while (true) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(&q.ctl[2], 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        int i = base + lane;
+        if (i < n) {
+            float4 a = org[i], b = dir[i];
+            RayPre r;
+            ray_pre(make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z), r);
+            HitRec h;
+            uint32_t nv = 0, np = 0;
+            uint32_t *pv = q.stats ? &nv : nullptr, *pp = q.stats ? &np : nullptr;
+            if (MULTI) {
+                const DevScene &S = scenes[jobs[q.meta[side][i].y].scene];
+                trace_closest<FMT>(S, r, a.w, b.w, h, &q.ctl[3], pv, pp);
+            } else {
+                trace_closest<FMT>(S1, r, a.w, b.w, h, &q.ctl[3], pv, pp);
+            }
+            if (q.stats) {
+                atomicAdd(&q.stats[0], (unsigned long long)nv);
+                atomicAdd(&q.stats[1], (unsigned long long)np);
+            }
+            xtgpu_hit o;
+            o.t = h.t;
+            o.prim = h.prim;
+            o.u = h.u;
+            o.v = h.v;
+            q.hit[i] = o;
+        }
+        if (per_job) {
+            // rays per job: one atomic per group of lanes of the same job
+            uint32_t jb = i < n ? q.meta[side][i].y : 0xffffffffu;
+            unsigned peers = __match_any_sync(0xffffffffu, jb);
+            if (i < n && (peers & ((1u << lane) - 1u)) == 0u)
+                atomicAdd(&q.job_rays[jb], (unsigned long long)__popc(peers));
+        }
+    }
+}
+
+__global__ void k_shade(const DevJob *__restrict__ jobs, const DevScene *__restrict__ scenes, WaveQueues q, int side)
+{
+    const int n = q.ctl[side];
+    const int out = side ^ 1;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        int i = base + threadIdx.x;
+        bool valid = i < n;
+        bool cont = false;
+        float4 no = make_float4(0.f, 0.f, 0.f, 0.f), nd = no, nP = no, nI = no;
+        uint2 meta = make_uint2(0u, 0u);
+        if (valid) {
+            meta = q.meta[side][i];
+            const DevJob &J = jobs[meta.y];
+            const DevScene &S = scenes[J.scene];
+            xtgpu_hit h = q.hit[i];
+            float4 a = q.org[side][i], b = q.dir[side][i];
+            float3 o = f3(a), d = f3(b);
+            bool hit = h.prim != 0xffffffffu;
+            int64_t lp = meta.x;   // wave-local path index
+            float4 P = q.P[side][i], I = q.I[side][i];
+            uint32_t ctr = __float_as_uint(P.w);
+            int depth_left = __float_as_int(I.w);
+            int64_t path = J.first + (lp - J.offset);
+            int64_t npix = (int64_t)J.rw * J.rh;
+            int64_t smp = path / npix, pix = path - smp * npix;
+            int64_t fx = J.x0 + pix % J.rw, fy = J.y0 + pix / J.rw;
+            uint64_t key = path_key(J.seed, (uint64_t)smp * (uint64_t)J.width * (uint64_t)J.height +
+                                                (uint64_t)fy * (uint64_t)J.width + (uint64_t)fx);
+            switch (J.integrator) {
+            case XTGPU_STENCIL:
+                q.contrib[lp] = make_float4(0.f, 0.f, 0.f, hit ? 1.f : 0.f);
+                break;
+            case XTGPU_DEPTH: {
+                // 1 / log(|o - p|), computed in double as the reference does
+                float dv = hit ? (float)(1.0 / log((double)h.t)) : 0.f;
+                q.contrib[lp] = make_float4(dv, 0.f, 0.f, hit ? 1.f : 0.f);
+                break;
+            }
+            case XTGPU_AO: {
+                if (depth_left == J.bounces) {
+                    // primary ray: a miss scores 1; a hit spawns the AO ray
+                    if (!hit) {
+                        q.contrib[lp] = make_float4(1.f, 0.f, 0.f, 1.f);
+                    } else {
+                        float3 p = o + d * h.t;
+                        float3 nrm = hit_normal(S, h.prim, p, h.u, h.v);
+                        float3 ad = s_hemisphere(nrm, key, ctr);
+                        float3 org = offset_ray(p, normalized(nrm));
+                        no = make_float4(org.x, org.y, org.z, 0.f);
+                        nd = make_float4(ad.x, ad.y, ad.z, J.ao_maxd);
+                        nP = make_float4(0.f, 0.f, 0.f, __uint_as_float(ctr));
+                        nI = make_float4(0.f, 0.f, 0.f, __int_as_float(depth_left - 1));
+                        cont = true;
+                    }
+                } else {
+                    float w = hit ? fminf(h.t, J.ao_maxd) / J.ao_maxd : 1.f;
+                    q.contrib[lp] = make_float4(w, 0.f, 0.f, 1.f);
+                }
+                break;
+            }
+            default: {   // pathtracer
+                float3 Pp = f3(P), Ii = f3(I);
+                if (!hit) {
+                    float3 L = cmul(Pp, environment(S, d));
+                    q.contrib[lp] = make_float4(L.x, L.y, L.z, 1.f);
+                    break;
+                }
+                float3 p = o + d * h.t;
+                float3 nrm = hit_normal(S, h.prim, p, h.u, h.v);
+                const DevMaterial &M = S.materials[S.obj_material[S.prim_obj[h.prim]]];
+                float3 f, nd3;
+                bool go = true;
+                if (M.type == XTGPU_LAMBERT) {
+                    nd3 = normalized(s_diffuse(nrm, key, ctr));
+                    f = cmuls(M.diffuse, dot3(nrm, nd3));
+                } else if (M.type == XTGPU_PHONG || M.type == XTGPU_BLINNPHONG) {
+                    float k = uniform(key, ctr);
+                    if (k > M.reflectance) {
+                        f = M.diffuse;
+                        nd3 = s_diffuse(nrm, key, ctr);
+                    } else {
+                        f = M.specular;
+                        nd3 = s_lobe(nrm, make_float3(-d.x, -d.y, -d.z), M.exponent, key, ctr);
+                    }
+                } else if (M.type == XTGPU_EMISSIVE) {
+                    float3 L = cmul(Pp, cmul(Ii, M.emissive));
+                    q.contrib[lp] = make_float4(L.x, L.y, L.z, 1.f);
+                    go = false;
+                } else {
+                    // dielectric: its intensity stays 0 (dielectric.cc:22-31),
+                    // so the path's value is 0 whatever follows
+                    q.contrib[lp] = make_float4(0.f, 0.f, 0.f, 1.f);
+                    go = false;
+                }
+                if (go) {
+                    float3 np = cmul(Pp, cmul(Ii, f));
+                    // eval(0) returns black (pathtracer/integrator.cc:23), and a
+                    // zero prefix stays zero: both end the path at value 0
+                    if (depth_left - 1 <= 0 || (np.x == 0.f && np.y == 0.f && np.z == 0.f)) {
+                        q.contrib[lp] = make_float4(0.f, 0.f, 0.f, 1.f);
+                    } else {
+                        float3 org = offset_ray(p, normalized(nrm));
+                        no = make_float4(org.x, org.y, org.z, 0.f);
+                        nd = make_float4(nd3.x, nd3.y, nd3.z, INFINITY);
+                        nP = make_float4(np.x, np.y, np.z, __uint_as_float(ctr));
+                        nI = make_float4(f.x, f.y, f.z, __int_as_float(depth_left - 1));
+                        cont = true;
+                    }
+                }
+            }
+            }
+        }
+        int slot = warp_append(&q.ctl[out], cont);
+        if (cont) {
+            q.org[out][slot] = no;
+            q.dir[out][slot] = nd;
+            q.meta[out][slot] = meta;
+            q.P[out][slot] = nP;
+            q.I[out][slot] = nI;
+        }
+    }
+}
+
+// One thread per pixel touched by the wave; its samples folded in order.
+__global__ void k_accumulate(const DevJob *__restrict__ jobs, const int32_t *__restrict__ ctl,
+                             const int64_t *__restrict__ pix_prefix, const float4 *__restrict__ contrib)
+{
+    const int njobs = ctl[4];
+    const int64_t total = pix_prefix[njobs];
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < total; g += (int64_t)gridDim.x * blockDim.x) {
+        int lo = 0, hi = njobs - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (pix_prefix[mid] <= g) lo = mid;
+            else hi = mid - 1;
+        }
+        const DevJob &J = jobs[lo];
+        int64_t npix = (int64_t)J.rw * J.rh;
+        int64_t k = g - pix_prefix[lo];
+        // pixels touched: those of paths [first, first+count), sample-major
+        int64_t pix = (J.first + k) % npix;
+        int64_t a = J.first, e = J.first + J.count;   // path range
+        int64_t s_lo = (a - pix + npix - 1) / npix;
+        if (a - pix <= 0) s_lo = 0;
+        int64_t s_hi = (e - 1 - pix) / npix;
+        if (e - 1 - pix < 0) continue;
+        float4 c = J.frame[pix];
+        double w = 1.f;
+        w *= 1.0 / (double)J.spp;
+        for (int64_t s = s_lo; s <= s_hi; ++s) {
+            float4 v = contrib[J.offset + (s * npix + pix - a)];
+            switch (J.integrator) {
+            case XTGPU_STENCIL:
+                if (v.w != 0.f) {
+                    float al = (float)((double)c.w + w);
+                    c = make_float4(1.f, 1.f, 1.f, al < 0.f ? 0.f : (al > 1.f ? 1.f : al));
+                }
+                break;
+            case XTGPU_DEPTH:
+                if (v.w != 0.f) {
+                    float dv = c0((float)((double)c.x + (double)v.x * w));
+                    c = make_float4(dv, dv, dv, 1.f);
+                }
+                c.w = 1.f;
+                break;
+            case XTGPU_AO: {
+                float r = c0((float)((double)c.x + (double)v.x * w));
+                float gg = c0((float)((double)c.y + (double)v.x * w));
+                float b = c0((float)((double)c.z + (double)v.x * w));
+                c = make_float4(r, gg, b, 1.f);
+                break;
+            }
+            default: {
+                float wf = (float)w;
+                c = make_float4(c0(c.x + c0(v.x * wf)), c0(c.y + c0(v.y * wf)), c0(c.z + c0(v.z * wf)), 1.f);
+            }
+            }
+        }
+        J.frame[pix] = c;
+    }
+}
+
+// ---------------------------------------------------------------------------
+xtgpu_status WaveRunner::init(int64_t capacity, int max_jobs, int max_scenes, cudaStream_t s)
+{
+    cap = capacity;
+    for (int k = 0; k < 2; ++k) {
+        XTG_TRY(dalloc(bufs[5 * k + 0], sizeof(float4) * cap, s));
+        XTG_TRY(dalloc(bufs[5 * k + 1], sizeof(float4) * cap, s));
+        XTG_TRY(dalloc(bufs[5 * k + 2], sizeof(uint2) * cap, s));
+        XTG_TRY(dalloc(bufs[5 * k + 3], sizeof(float4) * cap, s));
+        XTG_TRY(dalloc(bufs[5 * k + 4], sizeof(float4) * cap, s));
+        q.org[k] = (float4 *)bufs[5 * k + 0].p;
+        q.dir[k] = (float4 *)bufs[5 * k + 1].p;
+        q.meta[k] = (uint2 *)bufs[5 * k + 2].p;
+        q.P[k] = (float4 *)bufs[5 * k + 3].p;
+        q.I[k] = (float4 *)bufs[5 * k + 4].p;
+    }
+    XTG_TRY(dalloc(hitbuf, sizeof(xtgpu_hit) * cap, s));
+    XTG_TRY(dalloc(contribbuf, sizeof(float4) * cap, s));
+    XTG_TRY(dalloc(ctlbuf, 64, s));
+    XTG_TRY(dalloc(jobbuf, sizeof(DevJob) * (size_t)max_jobs, s));
+    XTG_TRY(dalloc(prefixbuf, sizeof(int64_t) * (size_t)(max_jobs + 1), s));
+    XTG_TRY(dalloc(scenebuf, sizeof(DevScene) * (size_t)max_scenes, s));
+    XTG_TRY(dalloc(jobraysbuf, sizeof(unsigned long long) * (size_t)max_jobs, s));
+    q.hit = (xtgpu_hit *)hitbuf.p;
+    q.contrib = (float4 *)contribbuf.p;
+    q.ctl = (int32_t *)ctlbuf.p;
+    q.rays = (unsigned long long *)((char *)ctlbuf.p + 32);
+    q.capacity = cap;
+    this->max_jobs = max_jobs;
+    this->max_scenes = max_scenes;
+    XTG_CUDA(cudaMemsetAsync(ctlbuf.p, 0, 64, s));
+    XTG_CUDA(cudaMallocHost(&host_jobs, sizeof(DevJob) * (size_t)max_jobs));
+    XTG_CUDA(cudaMallocHost(&host_prefix, sizeof(int64_t) * (size_t)(max_jobs + 1)));
+    XTG_CUDA(cudaMallocHost(&host_ctl, 64));
+    int dev = 0;
+    XTG_CUDA(cudaGetDevice(&dev));
+    XTG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    for (int k = 0; k < 2 * MAX_TIMED; ++k) XTG_CUDA(cudaEventCreate(&ev[k]));
+    XTG_TRY(dalloc(statsbuf, 16, s));
+    XTG_CUDA(cudaMemsetAsync(statsbuf.p, 0, 16, s));
+    return XTGPU_OK;
+}
+
+void WaveRunner::release()
+{
+    for (auto &b : bufs) dfree(b);
+    dfree(hitbuf);
+    dfree(contribbuf);
+    dfree(ctlbuf);
+    dfree(jobbuf);
+    dfree(prefixbuf);
+    dfree(scenebuf);
+    dfree(jobraysbuf);
+    dfree(statsbuf);
+    for (int k = 0; k < 2 * MAX_TIMED; ++k)
+        if (ev[k]) cudaEventDestroy(ev[k]);
+    for (auto &e : ev) e = nullptr;
+    if (host_jobs) cudaFreeHost(host_jobs);
+    if (host_prefix) cudaFreeHost(host_prefix);
+    if (host_ctl) cudaFreeHost(host_ctl);
+    host_jobs = nullptr;
+    host_prefix = nullptr;
+    host_ctl = nullptr;
+    for (auto &g : graphs)
+        if (g.second) cudaGraphExecDestroy(g.second);
+    graphs.clear();
+}
+
+xtgpu_status WaveRunner::set_scenes(const DevScene *scenes, int n, cudaStream_t s)
+{
+    if (n > max_scenes) {
+        set_error("too many scenes for the wave runner");
+        return XTGPU_ERR_LIMIT;
+    }
+    XTG_CUDA(cudaMemcpyAsync(scenebuf.p, scenes, sizeof(DevScene) * (size_t)n, cudaMemcpyHostToDevice, s));
+    nscenes = n;
+    single = scenes[0];
+    return XTGPU_OK;
+}
+
+// Enqueues the kernels of one wave (no host synchronisation inside).
+void WaveRunner::enqueue(int njobs, int64_t total, int bounces, int fmt, bool multi, cudaStream_t s)
+{
+    (void)njobs;
+    (void)total;
+    const DevJob *jobs = (const DevJob *)jobbuf.p;
+    const DevScene *scenes = (const DevScene *)scenebuf.p;
+    int gb = sms * 8;
+    k_camera<<<gb, 256, 0, s>>>(jobs, scenes, q);
+    int side = 0;
+    for (int b = 0; b < bounces; ++b) {
+        cudaMemsetAsync(q.ctl + 2, 0, sizeof(int32_t), s);
+        int eb = sms * extend_blocks_per_sm;
+        if (time_extend && b < MAX_TIMED) cudaEventRecord(ev[2 * b], s);
+        if (fmt == XTGPU_NODES_Q8) {
+            if (multi) k_extend<XTGPU_NODES_Q8, true><<<eb, 128, 0, s>>>(single, scenes, jobs, q, side);
+            else k_extend<XTGPU_NODES_Q8, false><<<eb, 128, 0, s>>>(single, scenes, jobs, q, side);
+        } else {
+            if (multi) k_extend<XTGPU_NODES_FP32, true><<<eb, 128, 0, s>>>(single, scenes, jobs, q, side);
+            else k_extend<XTGPU_NODES_FP32, false><<<eb, 128, 0, s>>>(single, scenes, jobs, q, side);
+        }
+        if (time_extend && b < MAX_TIMED) cudaEventRecord(ev[2 * b + 1], s);
+        cudaMemsetAsync(q.ctl + (side ^ 1), 0, sizeof(int32_t), s);
+        k_shade<<<gb, 256, 0, s>>>(jobs, scenes, q, side);
+        side ^= 1;
+    }
+    k_accumulate<<<gb, 256, 0, s>>>(jobs, q.ctl, (const int64_t *)prefixbuf.p, q.contrib);
+}
+
+xtgpu_status WaveRunner::collect_times(cudaStream_t s)
+{
+    if (!time_extend) return XTGPU_OK;
+    XTG_CUDA(cudaStreamSynchronize(s));
+    for (int b = 0; b < std::min(last_bounces, MAX_TIMED); ++b) {
+        float ms = 0.f;
+        XTG_CUDA(cudaEventElapsedTime(&ms, ev[2 * b], ev[2 * b + 1]));
+        extend_ms += ms;
+        extend_launches += 1;
+    }
+    return XTGPU_OK;
+}
+
+xtgpu_status WaveRunner::run_wave(const std::vector<DevJob> &jobs, int bounces, int fmt, bool use_graph,
+                                  cudaStream_t s)
+{
+    int nj = (int)jobs.size();
+    if (nj == 0) return XTGPU_OK;
+    if (nj > max_jobs) {
+        set_error("too many jobs in one wave");
+        return XTGPU_ERR_LIMIT;
+    }
+    int64_t total = 0;
+    host_prefix[0] = 0;
+    for (int j = 0; j < nj; ++j) {
+        host_jobs[j] = jobs[j];
+        host_jobs[j].offset = total;
+        total += jobs[j].count;
+        int64_t npix = (int64_t)jobs[j].rw * jobs[j].rh;
+        host_prefix[j + 1] = host_prefix[j] + std::min<int64_t>(npix, jobs[j].count);
+    }
+    if (total > cap) {
+        set_error("wave larger than the queue capacity");
+        return XTGPU_ERR_LIMIT;
+    }
+    bool multi = nscenes > 1;
+    XTG_CUDA(cudaMemcpyAsync(jobbuf.p, host_jobs, sizeof(DevJob) * nj, cudaMemcpyHostToDevice, s));
+    XTG_CUDA(cudaMemcpyAsync(prefixbuf.p, host_prefix, sizeof(int64_t) * (nj + 1), cudaMemcpyHostToDevice, s));
+    // queue A holds the wave's primary rays; its count is the wave size.  The
+    // kernels read the counts from device memory, so the launch sequence does
+    // not depend on the wave's contents.
+    host_ctl[0] = (int32_t)total;
+    host_ctl[1] = 0;
+    host_ctl[2] = 0;
+    host_ctl[3] = overflow_seen;
+    host_ctl[4] = nj;
+    host_ctl[5] = (int32_t)total;
+    XTG_CUDA(cudaMemcpyAsync(q.ctl, host_ctl, 24, cudaMemcpyHostToDevice, s));
+    if (job_rays_enabled) XTG_CUDA(cudaMemsetAsync(q.job_rays, 0, sizeof(unsigned long long) * nj, s));
+    if (use_graph) {
+        // One graph per (bounces, format, scene count) shape; kernel arguments
+        // point at fixed buffers, so a graph replays any wave of that shape.
+        uint64_t key = ((uint64_t)bounces << 4) ^ (uint64_t)fmt ^ (multi ? 2ull : 0ull) ^ (time_extend ? 4ull : 0ull) ^
+                       (q.stats ? 8ull : 0ull);
+        auto it = graphs.find(key);
+        if (it == graphs.end()) {
+            cudaGraph_t g;
+            XTG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            enqueue(nj, total, bounces, fmt, multi, s);
+            XTG_CUDA(cudaStreamEndCapture(s, &g));
+            cudaGraphExec_t ex;
+            XTG_CUDA(cudaGraphInstantiate(&ex, g, 0));
+            cudaGraphDestroy(g);
+            if (graphs.size() > 256) {
+                for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+                graphs.clear();
+            }
+            it = graphs.emplace(key, ex).first;
+        }
+        XTG_CUDA(cudaGraphLaunch(it->second, s));
+    } else {
+        enqueue(nj, total, bounces, fmt, multi, s);
+    }
+    launches += 2 + 2 * bounces;   // camera, bounces x (extend, shade), accumulate
+    last_bounces = bounces;
+    XTG_CUDA(cudaGetLastError());
+    return XTGPU_OK;
+}
+
+xtgpu_status WaveRunner::read_ctl(int32_t *overflow, unsigned long long *rays, cudaStream_t s)
+{
+    XTG_CUDA(cudaMemcpyAsync(host_ctl, q.ctl, 64, cudaMemcpyDeviceToHost, s));
+    XTG_CUDA(cudaStreamSynchronize(s));
+    if (overflow) *overflow = host_ctl[3];
+    overflow_seen = host_ctl[3];
+    if (rays) *rays = *(unsigned long long *)((char *)host_ctl + 32);
+    return XTGPU_OK;
+}
+
+void launch_extend(int fmt, const DevScene &S, const WaveQueues &q, int side, int blocks, cudaStream_t s)
+{
+    if (fmt == XTGPU_NODES_Q8) k_extend<XTGPU_NODES_Q8, false><<<blocks, 128, 0, s>>>(S, nullptr, nullptr, q, side);
+    else k_extend<XTGPU_NODES_FP32, false><<<blocks, 128, 0, s>>>(S, nullptr, nullptr, q, side);
+}
+
+int bounces_of(int integrator, int rdepth)
+{
+    if (integrator == XTGPU_AO) return 2;
+    if (integrator == XTGPU_PATHTRACER) return std::max(0, rdepth);
+    return 1;
+}
+
+}  // namespace xtg

@@ -1,0 +1,53 @@
+// Host side of the wavefront: queue buffers, job table, CUDA-graph cache.
+#pragma once
+
+#include <unordered_map>
+#include <vector>
+
+#include "wavefront.cuh"
+
+namespace xtg {
+
+struct WaveRunner {
+    WaveQueues q{};
+    HostBuf bufs[10], hitbuf, contribbuf, ctlbuf, jobbuf, prefixbuf, scenebuf, jobraysbuf;
+    bool job_rays_enabled = false;
+    int32_t overflow_seen = 0;
+    // live timing of the extend kernel (CUDA events around each launch, also
+    // inside captured graphs) and launch counting
+    static constexpr int MAX_TIMED = 16;
+    bool time_extend = false;
+    cudaEvent_t ev[2 * MAX_TIMED] = {};
+    double extend_ms = 0.0;
+    int64_t extend_launches = 0;
+    int64_t launches = 0;
+    int last_bounces = 0;
+    HostBuf statsbuf;
+    xtgpu_status collect_times(cudaStream_t s);
+    void enable_stats(bool on) { q.stats = on ? (unsigned long long *)statsbuf.p : nullptr; }
+    DevJob *host_jobs = nullptr;      // pinned
+    int64_t *host_prefix = nullptr;   // pinned
+    int32_t *host_ctl = nullptr;      // pinned, 64 bytes
+    int64_t cap = 0;
+    int max_jobs = 0, max_scenes = 0, nscenes = 0;
+    int sms = 148;
+    int extend_blocks_per_sm = 12;
+    DevScene single{};
+    std::unordered_map<uint64_t, cudaGraphExec_t> graphs;
+
+    xtgpu_status init(int64_t capacity, int max_jobs, int max_scenes, cudaStream_t s);
+    void release();
+    xtgpu_status set_scenes(const DevScene *scenes, int n, cudaStream_t s);
+    // jobs[j].first/count select the job's paths in this wave; offset is filled in.
+    xtgpu_status run_wave(const std::vector<DevJob> &jobs, int bounces, int fmt, bool use_graph, cudaStream_t s);
+    xtgpu_status read_ctl(int32_t *overflow, unsigned long long *rays, cudaStream_t s);
+    // per-job ray counts of the last wave (requires enable_job_rays)
+    void enable_job_rays(bool on) { job_rays_enabled = on; q.job_rays = on ? (unsigned long long *)jobraysbuf.p : nullptr; }
+    void enqueue(int njobs, int64_t total, int bounces, int fmt, bool multi, cudaStream_t s);
+};
+
+int bounces_of(int integrator, int rdepth);
+// Closest hit of the q.ctl[side] rays of queue `side` (no job table needed).
+void launch_extend(int fmt, const DevScene &S, const WaveQueues &q, int side, int blocks, cudaStream_t s);
+
+}  // namespace xtg

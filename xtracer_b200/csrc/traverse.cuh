@@ -1,0 +1,280 @@
+// Ray traversal device code: closest hit over the scene's BVH (triangles and
+// spheres) plus the scene's infinite planes, which no BVH can bound.
+//
+// Semantics follow Scene::intersection (src/xtcore/scene.cc:191-216): the
+// nearest hit over every surface; spheres are hit only from outside
+// (t = min(t1, t2) must be positive, math/sphere.cc:35-62), planes and
+// triangles from both sides (math/plane.cc:19-61, math/triangle.cc:82-123).
+//
+// Triangles use the watertight test of Woop, Benthin and Wald ("Watertight
+// Ray/Triangle Intersection", JCGT 2013) in FP32: shear into ray space, 2D
+// edge functions with the products rounded separately (no FMA contraction, so
+// a shared edge gives exactly opposite values in both triangles) and an FP64
+// re-evaluation when an edge function is exactly zero.  Box tests are the slab
+// test with the far distance scaled up by 1 + 2*gamma(3) (Ize, "Robust BVH Ray
+// Traversal", JCGT 2013) so rounding never culls a box the ray touches.
+#pragma once
+
+#include "xtgpu_internal.cuh"
+
+namespace xtg {
+
+struct RayPre {
+    float3 o, d, inv, oinv;
+    int kx, ky, kz;
+    float Sx, Sy, Sz;
+};
+
+__device__ __forceinline__ float comp(const float3 &v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+__device__ __forceinline__ void ray_pre(float3 o, float3 d, RayPre &r)
+{
+    r.o = o;
+    r.d = d;
+    const float tiny = 1e-20f;
+    float dx = fabsf(d.x) < tiny ? copysignf(tiny, d.x) : d.x;
+    float dy = fabsf(d.y) < tiny ? copysignf(tiny, d.y) : d.y;
+    float dz = fabsf(d.z) < tiny ? copysignf(tiny, d.z) : d.z;
+    r.inv = make_float3(1.0f / dx, 1.0f / dy, 1.0f / dz);
+    r.oinv = make_float3(o.x * r.inv.x, o.y * r.inv.y, o.z * r.inv.z);
+    float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    int kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    int kx = kz == 2 ? 0 : kz + 1;
+    int ky = kx == 2 ? 0 : kx + 1;
+    float dk = comp(d, kz);
+    if (dk < 0.f) {
+        int t = kx;
+        kx = ky;
+        ky = t;
+    }
+    r.kx = kx;
+    r.ky = ky;
+    r.kz = kz;
+    r.Sx = comp(d, kx) / dk;
+    r.Sy = comp(d, ky) / dk;
+    r.Sz = 1.0f / dk;
+}
+
+// 1 + 2*gamma(3) rounded up
+#define XTG_TFAR_SCALE 1.00000072f
+
+__device__ __forceinline__ bool slab(const RayPre &r, float lx, float hx, float ly, float hy, float lz, float hz,
+                                     float tmin, float tmax, float &tnear)
+{
+    float tx0 = fmaf(lx, r.inv.x, -r.oinv.x), tx1 = fmaf(hx, r.inv.x, -r.oinv.x);
+    float ty0 = fmaf(ly, r.inv.y, -r.oinv.y), ty1 = fmaf(hy, r.inv.y, -r.oinv.y);
+    float tz0 = fmaf(lz, r.inv.z, -r.oinv.z), tz1 = fmaf(hz, r.inv.z, -r.oinv.z);
+    float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
+    float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
+    tnear = tn;
+    return tn <= tf * XTG_TFAR_SCALE;
+}
+
+// FP64 re-evaluation of the edge functions (the paper's fallback).
+static __device__ __noinline__ void edges_fp64(float Ax, float Ay, float Bx, float By, float Cx, float Cy, float &U,
+                                        float &V, float &W)
+{
+    U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+    V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+    W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+}
+
+// Two-sided watertight triangle test.  On a hit inside (tmin, tmax) updates
+// tmax and the barycentrics of v1 (u) and v2 (v).
+__device__ __forceinline__ bool hit_triangle(const RayPre &r, float3 v0, float3 v1, float3 v2, float tmin,
+                                             float &tmax, float &bu, float &bv)
+{
+    float3 A = make_float3(v0.x - r.o.x, v0.y - r.o.y, v0.z - r.o.z);
+    float3 B = make_float3(v1.x - r.o.x, v1.y - r.o.y, v1.z - r.o.z);
+    float3 C = make_float3(v2.x - r.o.x, v2.y - r.o.y, v2.z - r.o.z);
+    float Akz = comp(A, r.kz), Bkz = comp(B, r.kz), Ckz = comp(C, r.kz);
+    float Ax = __fsub_rn(comp(A, r.kx), __fmul_rn(r.Sx, Akz));
+    float Ay = __fsub_rn(comp(A, r.ky), __fmul_rn(r.Sy, Akz));
+    float Bx = __fsub_rn(comp(B, r.kx), __fmul_rn(r.Sx, Bkz));
+    float By = __fsub_rn(comp(B, r.ky), __fmul_rn(r.Sy, Bkz));
+    float Cx = __fsub_rn(comp(C, r.kx), __fmul_rn(r.Sx, Ckz));
+    float Cy = __fsub_rn(comp(C, r.ky), __fmul_rn(r.Sy, Ckz));
+    float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+    float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+    float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+    if (U == 0.f || V == 0.f || W == 0.f) edges_fp64(Ax, Ay, Bx, By, Cx, Cy, U, V, W);
+    if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) return false;
+    float det = U + V + W;
+    if (det == 0.f) return false;
+    float Az = r.Sz * Akz, Bz = r.Sz * Bkz, Cz = r.Sz * Ckz;
+    float T = U * Az + V * Bz + W * Cz;
+    float rcp = 1.0f / det;
+    float t = T * rcp;
+    if (!(t > tmin && t < tmax)) return false;
+    tmax = t;
+    bu = V * rcp;
+    bv = W * rcp;
+    return true;
+}
+
+// Sphere hit only from outside: the nearer root must lie in (tmin, tmax).
+// Discriminant in the form of Haines et al., "Precision Improvements for
+// Ray/Sphere Intersection" (Ray Tracing Gems, 2019); unit direction assumed.
+__device__ __forceinline__ bool hit_sphere(const RayPre &r, float3 c, float rad, float tmin, float &tmax)
+{
+    float3 f = make_float3(r.o.x - c.x, r.o.y - c.y, r.o.z - c.z);
+    float b = f.x * r.d.x + f.y * r.d.y + f.z * r.d.z;
+    float3 h = make_float3(f.x - b * r.d.x, f.y - b * r.d.y, f.z - b * r.d.z);
+    float r2 = rad * rad;
+    float disc = r2 - (h.x * h.x + h.y * h.y + h.z * h.z);
+    if (!(disc > 0.f)) return false;
+    float cc = (f.x * f.x + f.y * f.y + f.z * f.z) - r2;
+    float q = -b - copysignf(sqrtf(disc), b);
+    float t0 = cc / q, t1 = q;
+    float tn = fminf(t0, t1);
+    if (!(tn > tmin && tn < tmax)) return false;
+    tmax = tn;
+    return true;
+}
+
+// Infinite plane through |n| * offset (plane.cc:33-41), two-sided.
+__device__ __forceinline__ bool hit_plane(const RayPre &r, float4 pl, float tmin, float &tmax)
+{
+    float ndd = pl.x * r.d.x + pl.y * r.d.y + pl.z * r.d.z;
+    if (fabsf(ndd) < 1e-8f) return false;
+    float3 v = make_float3(fabsf(pl.x) * pl.w - r.o.x, fabsf(pl.y) * pl.w - r.o.y, fabsf(pl.z) * pl.w - r.o.z);
+    float t = (v.x * pl.x + v.y * pl.y + v.z * pl.z) / ndd;
+    if (!(t > tmin && t < tmax)) return false;
+    tmax = t;
+    return true;
+}
+
+struct Node2 {
+    float lx[2], hx[2], ly[2], hy[2], lz[2], hz[2];
+    int32_t ref[2];
+};
+
+template <int FMT>
+__device__ __forceinline__ void load_node(const DevScene &S, int32_t i, Node2 &n);
+
+template <>
+__device__ __forceinline__ void load_node<XTGPU_NODES_FP32>(const DevScene &S, int32_t i, Node2 &n)
+{
+    const float4 *p = S.nodes32 + 4 * (size_t)i;
+    float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
+    n.lx[0] = a.x; n.hx[0] = a.y; n.ly[0] = a.z; n.hy[0] = a.w;
+    n.lx[1] = b.x; n.hx[1] = b.y; n.ly[1] = b.z; n.hy[1] = b.w;
+    n.lz[0] = c.x; n.hz[0] = c.y; n.lz[1] = c.z; n.hz[1] = c.w;
+    n.ref[0] = __float_as_int(d.x);
+    n.ref[1] = __float_as_int(d.y);
+}
+
+// 32-byte node: origin xyz with the biased power-of-two scale exponent in each
+// low byte, 12 child bounds of 8 bits, two child refs.
+template <>
+__device__ __forceinline__ void load_node<XTGPU_NODES_Q8>(const DevScene &S, int32_t i, Node2 &n)
+{
+    const uint4 *p = S.nodes8 + 2 * (size_t)i;
+    uint4 a = __ldg(p), b = __ldg(p + 1);
+    float ox = __uint_as_float(a.x & ~0xFFu), oy = __uint_as_float(a.y & ~0xFFu), oz = __uint_as_float(a.z & ~0xFFu);
+    float sx = __uint_as_float((a.x & 0xFFu) << 23), sy = __uint_as_float((a.y & 0xFFu) << 23),
+          sz = __uint_as_float((a.z & 0xFFu) << 23);
+    uint32_t q0 = a.w, q1 = b.x, q2 = b.y;
+#define XTG_Q(w, k) ((float)(((w) >> (8 * (k))) & 0xFFu))
+    n.lx[0] = __fmaf_rn(XTG_Q(q0, 0), sx, ox);
+    n.ly[0] = __fmaf_rn(XTG_Q(q0, 1), sy, oy);
+    n.lz[0] = __fmaf_rn(XTG_Q(q0, 2), sz, oz);
+    n.hx[0] = __fmaf_rn(XTG_Q(q0, 3), sx, ox);
+    n.hy[0] = __fmaf_rn(XTG_Q(q1, 0), sy, oy);
+    n.hz[0] = __fmaf_rn(XTG_Q(q1, 1), sz, oz);
+    n.lx[1] = __fmaf_rn(XTG_Q(q1, 2), sx, ox);
+    n.ly[1] = __fmaf_rn(XTG_Q(q1, 3), sy, oy);
+    n.lz[1] = __fmaf_rn(XTG_Q(q2, 0), sz, oz);
+    n.hx[1] = __fmaf_rn(XTG_Q(q2, 1), sx, ox);
+    n.hy[1] = __fmaf_rn(XTG_Q(q2, 2), sy, oy);
+    n.hz[1] = __fmaf_rn(XTG_Q(q2, 3), sz, oz);
+#undef XTG_Q
+    n.ref[0] = (int32_t)b.z;
+    n.ref[1] = (int32_t)b.w;
+}
+
+struct HitRec {
+    float t;
+    uint32_t prim;
+    float u, v;
+};
+
+// Closest hit in (tmin, tmax).  Returns false (and sets *overflow) only if the
+// traversal stack would overflow, which the builder's depth check excludes.
+template <int FMT>
+__device__ __forceinline__ void trace_closest(const DevScene &S, const RayPre &r, float tmin, float tmax,
+                                              HitRec &h, int *overflow, uint32_t *visits = nullptr,
+                                              uint32_t *tests = nullptr)
+{
+    h.t = INFINITY;
+    h.prim = 0xffffffffu;
+    h.u = h.v = 0.f;
+    int32_t stack[STACK_MAX];
+    int sp = 0;
+    int32_t ref = S.root;
+    uint32_t nv = 0, np = 0;
+    // A valid tree visits each node at most once per ray; the bound only turns
+    // a corrupted tree into an error instead of an endless loop.
+    for (uint32_t guard = 0;; ++guard) {
+        if (guard >= (1u << 22)) {
+            *overflow = 1;
+            break;
+        }
+        if (ref >= 0) {
+            Node2 n;
+            load_node<FMT>(S, ref, n);
+            ++nv;
+            float t0, t1;
+            bool h0 = slab(r, n.lx[0], n.hx[0], n.ly[0], n.hy[0], n.lz[0], n.hz[0], tmin, tmax, t0);
+            bool h1 = slab(r, n.lx[1], n.hx[1], n.ly[1], n.hy[1], n.lz[1], n.hz[1], tmin, tmax, t1);
+            if (h0 && h1) {
+                bool sw = t1 < t0;
+                if (sp >= STACK_MAX) {
+                    *overflow = 1;
+                    break;
+                }
+                stack[sp++] = sw ? n.ref[0] : n.ref[1];
+                ref = sw ? n.ref[1] : n.ref[0];
+                continue;
+            }
+            if (h0) { ref = n.ref[0]; continue; }
+            if (h1) { ref = n.ref[1]; continue; }
+        } else if (ref != EMPTY_REF) {
+            uint32_t first = leaf_first(ref), cnt = leaf_count(ref);
+            np += cnt;
+            for (uint32_t k = 0; k < cnt; ++k) {
+                const float4 *lp = S.leaf_prims + 3 * (size_t)(first + k);
+                float4 a = __ldg(lp), b = __ldg(lp + 1);
+                uint32_t id = __float_as_uint(a.w);
+                if (id & SPHERE_BIT) {
+                    if (hit_sphere(r, make_float3(a.x, a.y, a.z), b.x, tmin, tmax)) {
+                        h.prim = id & ~SPHERE_BIT;
+                        h.u = h.v = 0.f;
+                    }
+                } else {
+                    float4 c = __ldg(lp + 2);
+                    float bu, bv;
+                    if (hit_triangle(r, make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z),
+                                     make_float3(c.x, c.y, c.z), tmin, tmax, bu, bv)) {
+                        h.prim = id;
+                        h.u = bu;
+                        h.v = bv;
+                    }
+                }
+            }
+        }
+        if (sp == 0) break;
+        ref = stack[--sp];
+    }
+    for (int p = 0; p < S.n_planes; ++p) {
+        if (hit_plane(r, __ldg(S.planes + p), tmin, tmax)) {
+            h.prim = (uint32_t)(S.n_tris + S.n_spheres + p);
+            h.u = h.v = 0.f;
+        }
+    }
+    if (h.prim != 0xffffffffu) h.t = tmax;
+    if (visits) *visits = nv;
+    if (tests) *tests = np + (uint32_t)S.n_planes;
+}
+
+}  // namespace xtg

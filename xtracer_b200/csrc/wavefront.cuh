@@ -1,0 +1,51 @@
+// Wavefront integrators: the per-sample logic of the reference's stencil,
+// depth, ao and pathtracer render_tile methods, split into queue stages.
+//
+//   camera     one ray per (pixel, sample) of every job in the wave
+//   extend     closest hit of every queued ray (traverse.cuh)
+//   shade      integrator step: contribution of finished paths, next rays of the
+//              others appended to the next queue (warp-aggregated atomics)
+//   accumulate per pixel, the samples of the wave folded in sample order into
+//              the job's frame exactly as the reference folds them (float
+//              colour channels clamped at 0, alpha clamped to [0, 1])
+//
+// A path's result depends only on (job seed, pixel, sample): the random stream is
+// keyed by them, never by a queue slot, and the fold runs in sample order.  So a
+// job renders to the same bits alone, split over any number of waves, or merged
+// with other jobs.
+#pragma once
+
+#include "traverse.cuh"
+
+namespace xtg {
+
+// One job's share of a wave.
+struct DevJob {
+    int32_t integrator, width, height, spp, rdepth;
+    float ao_maxd;
+    uint64_t seed;
+    int32_t x0, y0, rw, rh;          // rectangle rendered
+    int32_t scene;                   // index in the scene table
+    int32_t bounces;                 // extend passes this job needs
+    float4 *frame;                   // rw*rh RGBA accumulation buffer
+    int64_t first;                   // first path id of the job in this wave
+    int64_t count;                   // paths of the job in this wave
+    int64_t offset;                  // wave-local index of the job's first path
+};
+
+struct WaveQueues {
+    float4 *org[2], *dir[2];         // (org, tmin), (dir, tmax)
+    uint2 *meta[2];                  // (wave-local path index, job slot)
+    float4 *P[2];                    // (prefix throughput rgb, rng counter)
+    float4 *I[2];                    // (incoming intensity rgb, depth left)
+    xtgpu_hit *hit;
+    float4 *contrib;                 // per wave-local path: result of the sample
+    int32_t *ctl;                    // [0],[1] queue counts, [2] fetch counter, [3] overflow flag,
+                                     // [4] jobs in the wave, [5] paths in the wave
+    unsigned long long *rays;        // rays traced (extend inputs)
+    unsigned long long *job_rays;    // per job of the wave, or nullptr
+    unsigned long long *stats;       // [0] nodes visited, [1] primitives tested, or nullptr
+    int64_t capacity;
+};
+
+}  // namespace xtg

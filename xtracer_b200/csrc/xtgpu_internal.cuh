@@ -1,0 +1,129 @@
+// Internal device/host structures of the xtgpu library (sm_100a).
+//
+// Data layout in HBM (all structure-of-arrays, 16-byte aligned):
+//   leaf primitives, in Morton order   3 x float4 (48 B) per primitive
+//       triangle: (v0.xyz, id) (v1.xyz, 0) (v2.xyz, 0)
+//       sphere:   (c.xyz, id | SPHERE_BIT) (r, 0, 0, 0) (0)
+//   FP32 BVH node                      4 x float4 (64 B): both child boxes + refs
+//   Q8 BVH node                        2 x uint4 (32 B): origin+exponents, 8-bit
+//                                      child bounds rounded outward, refs
+//   rays                               float4 (org, tmin) + float4 (dir, tmax)
+//   hits                               (t, prim, u, v) 16 B
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/xtgpu.h"
+
+namespace xtg {
+
+constexpr uint32_t SPHERE_BIT = 0x80000000u;
+constexpr int LEAF_BITS = 3;                  // leaf ref: ~((first << 3) | count)
+constexpr int MAX_LEAF = (1 << LEAF_BITS) - 1;
+constexpr int32_t EMPTY_REF = ~0;             // leaf of 0 primitives
+constexpr int STACK_MAX = 64;
+
+__host__ __device__ inline int32_t leaf_ref(uint32_t first, uint32_t count)
+{
+    return ~(int32_t)((first << LEAF_BITS) | count);
+}
+__host__ __device__ inline uint32_t leaf_first(int32_t ref) { return ((uint32_t)~ref) >> LEAF_BITS; }
+__host__ __device__ inline uint32_t leaf_count(int32_t ref) { return ((uint32_t)~ref) & MAX_LEAF; }
+
+struct DevMaterial {
+    int type;
+    float3 diffuse, specular, emissive;
+    float reflectance, exponent, ior;
+};
+
+// Camera basis precomputed on the host in FP64 exactly as
+// Perspective::calculate_transform (camera/perspective.cc:26-36).
+struct DevCamera {
+    double pos[3];
+    double rx[3], ry[3], rz[3];
+    double dz;            // 1 / tan(fov * RADIAN / 2)
+};
+
+// Everything a kernel needs to intersect and shade one scene.
+struct DevScene {
+    // geometry in the desc order (shading)
+    const float4 *tri_v;       // 3 per triangle
+    const float4 *tri_n;       // 3 per triangle, or nullptr
+    const float4 *spheres;     // (c, r)
+    const float4 *planes;      // (n, offset)
+    const int32_t *prim_obj;   // object of each primitive id (tris, spheres, planes)
+    const int32_t *obj_material;
+    const DevMaterial *materials;
+    int32_t n_tris, n_spheres, n_planes;
+    // BVH
+    const float4 *leaf_prims;  // 3 per primitive, Morton order
+    const float4 *nodes32;     // 4 per node
+    const uint4 *nodes8;       // 2 per node
+    int32_t root;              // ref of the root (>= 0 node, < 0 leaf)
+    int32_t env_type;
+    float3 env_a, env_b;
+    DevCamera cam;
+};
+
+// Host-side scene object behind the C handle.
+struct HostBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace xtg
+
+struct xtgpu_scene {
+    xtg::DevScene dev{};
+    xtg::HostBuf tri_v, tri_n, spheres, planes, prim_obj, obj_material, materials;
+    xtg::HostBuf leaf_prims, nodes32, nodes8;
+    xtg::HostBuf morton, order, left, right;   // kept for xtgpu_bvh_export
+    int64_t n_prims = 0;
+    int32_t depth = 0;
+    int32_t leaf_size = 2;
+    int32_t last_format = XTGPU_NODES_FP32;
+    bool built32 = false, built8 = false;
+    int device = 0;
+    // host copies used by the service and the tests
+    int32_t n_objects = 0;
+};
+
+namespace xtg {
+
+// error plumbing -----------------------------------------------------------
+void set_error(const std::string &msg);
+xtgpu_status cuda_fail(cudaError_t e, const char *what, const char *file, int line);
+
+#define XTG_CUDA(call)                                                              \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess) return xtg::cuda_fail(e_, #call, __FILE__, __LINE__); \
+    } while (0)
+
+#define XTG_TRY(call)                          \
+    do {                                       \
+        xtgpu_status s_ = (call);              \
+        if (s_ != XTGPU_OK) return s_;         \
+    } while (0)
+
+xtgpu_status dalloc(HostBuf &b, size_t bytes, cudaStream_t s);
+void dfree(HostBuf &b);
+
+// BVH build (bvh.cu)
+xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, cudaStream_t s);
+
+// Ray/primitive batches (trace.cu)
+struct RayQueue {
+    const float4 *org;    // (org, tmin)
+    const float4 *dir;    // (dir, tmax)
+    xtgpu_hit *hit;
+};
+xtgpu_status launch_trace(const DevScene &S, int fmt, int64_t n, const float4 *org, const float4 *dir,
+                          xtgpu_hit *hits, const int32_t *count_dev, int32_t *fetch_dev, cudaStream_t s);
+int trace_grid_blocks();
+int trace_block_threads();
+
+}  // namespace xtg

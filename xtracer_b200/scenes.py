@@ -230,8 +230,9 @@ def terrain_mesh(grid: int = 708, seed: int = 2, half: float = 50.0, amplitude: 
     idx = np.arange(grid * grid, dtype=np.int64).reshape(grid, grid)
     a = idx[:-1, :-1].ravel(); b = idx[:-1, 1:].ravel(); c = idx[1:, :-1].ravel(); d = idx[1:, 1:].ravel()
     faces = np.empty((a.size * 2, 3), np.int64)
-    faces[0::2] = np.stack([a, b, c], axis=1)
-    faces[1::2] = np.stack([b, d, c], axis=1)
+    # counter-clockwise seen from above: face normals point up (+y)
+    faces[0::2] = np.stack([a, c, b], axis=1)
+    faces[1::2] = np.stack([b, c, d], axis=1)
     return verts, faces
 
 
@@ -321,7 +322,7 @@ def precision_scene(scale: float = 1.0, seed: int = 5) -> SceneSpec:
     lv = np.stack([X, np.full_like(X, 60.0), Z], -1).reshape(-1, 3)
     idx = np.arange(121).reshape(11, 11)
     a = idx[:-1, :-1].ravel(); b = idx[:-1, 1:].ravel(); cc = idx[1:, :-1].ravel(); d = idx[1:, 1:].ravel()
-    lf = np.empty((200, 3), np.int64); lf[0::2] = np.stack([a, b, cc], 1); lf[1::2] = np.stack([b, d, cc], 1)
+    lf = np.empty((200, 3), np.int64); lf[0::2] = np.stack([a, cc, b], 1); lf[1::2] = np.stack([b, cc, d], 1)
     ltri = _q(lv, 16)[lf]
     chunks.append(ltri); kinds.append(MESH); firsts.append(first); counts.append(200)
     mats.append(Material(EMISSIVE, emissive=(20.0, 20.0, 20.0))); omat.append(len(mats) - 1)

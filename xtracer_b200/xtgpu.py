@@ -1,0 +1,320 @@
+"""ctypes binding of libxtgpu.so (include/xtgpu.h) and a thin Python mirror of
+XTracer's renderer interface for the hot path:
+
+* ``Scene``            a flattened, resident xtcore Scene (scene.h:35-86) with its
+                       LBVH; ``Scene.intersection`` is Scene::intersection
+                       (scene.cc:191-216) over a batch of rays.
+* ``Params``           params_t (context.h:18-34): width, height, samples, rdepth.
+* ``StencilIntegrator``, ``DepthIntegrator``, ``AOIntegrator``,
+  ``PathtracerIntegrator``: IIntegrator (integrator.h:10-24) with setup() and
+  render(); render() returns the RGBA frame the reference assembles from its
+  tiles (context.cc:38-52).
+
+The CUDA library is required: nothing here falls back to a CPU path.  Errors
+raise XtgpuError with the library's message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libxtgpu.so")
+
+STENCIL, DEPTH, AO, PATHTRACER = 0, 1, 2, 3
+NODES_FP32, NODES_Q8 = 0, 1
+STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "NOMEM", 4: "LIMIT", 5: "TIMEOUT", 6: "NOT_FOUND", 7: "STATE"}
+
+
+class XtgpuError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__("%s: %s" % (STATUS.get(status, status), msg))
+        self.status = status
+
+
+class Material(C.Structure):
+    _fields_ = [("type", C.c_int32), ("diffuse", C.c_float * 3), ("specular", C.c_float * 3),
+                ("emissive", C.c_float * 3), ("reflectance", C.c_float), ("exponent", C.c_float),
+                ("ior", C.c_float)]
+
+
+class CameraDesc(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("target", C.c_float * 3), ("up", C.c_float * 3), ("fov", C.c_float)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("n_objects", C.c_int32), ("obj_kind", C.c_void_p), ("obj_first", C.c_void_p),
+                ("obj_count", C.c_void_p), ("obj_material", C.c_void_p),
+                ("n_spheres", C.c_int32), ("spheres", C.c_void_p),
+                ("n_planes", C.c_int32), ("planes", C.c_void_p),
+                ("n_tris", C.c_int32), ("tris", C.c_void_p), ("tri_normals", C.c_void_p),
+                ("n_materials", C.c_int32), ("materials", C.c_void_p),
+                ("env_type", C.c_int32), ("env_a", C.c_float * 3), ("env_b", C.c_float * 3),
+                ("camera", CameraDesc)]
+
+
+class BvhOpts(C.Structure):
+    _fields_ = [("node_format", C.c_int32), ("leaf_size", C.c_int32)]
+
+
+class BvhInfo(C.Structure):
+    _fields_ = [("n_prims", C.c_int64), ("depth", C.c_int32), ("leaf_size", C.c_int32),
+                ("node_bytes_fp32", C.c_uint64), ("node_bytes_q8", C.c_uint64)]
+
+
+class Hit(C.Structure):
+    _fields_ = [("t", C.c_float), ("prim", C.c_uint32), ("u", C.c_float), ("v", C.c_float)]
+
+
+HIT_DTYPE = np.dtype([("t", np.float32), ("prim", np.uint32), ("u", np.float32), ("v", np.float32)])
+
+
+class RenderParams(C.Structure):
+    _fields_ = [("integrator", C.c_int32), ("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32),
+                ("rdepth", C.c_int32), ("ao_max_distance", C.c_float), ("seed", C.c_uint64),
+                ("node_format", C.c_int32), ("x0", C.c_int32), ("y0", C.c_int32), ("x1", C.c_int32),
+                ("y1", C.c_int32)]
+
+
+class ServiceOpts(C.Structure):
+    _fields_ = [("memory_budget_bytes", C.c_uint64), ("max_jobs", C.c_int32), ("wave_paths", C.c_int64),
+                ("node_format", C.c_int32), ("use_graphs", C.c_int32), ("merge_jobs", C.c_int32),
+                ("host_results", C.c_int32), ("time_kernels", C.c_int32), ("count_visits", C.c_int32)]
+
+
+class ServiceStats(C.Structure):
+    _fields_ = [("rays", C.c_uint64), ("waves", C.c_uint64), ("kernel_launches", C.c_uint64),
+                ("extend_ms", C.c_double), ("extend_launches", C.c_uint64), ("node_visits", C.c_uint64),
+                ("prim_tests", C.c_uint64)]
+
+
+class JobDesc(C.Structure):
+    _fields_ = [("scene", C.c_int32), ("integrator", C.c_int32), ("width", C.c_int32), ("height", C.c_int32),
+                ("spp", C.c_int32), ("rdepth", C.c_int32), ("ao_max_distance", C.c_float), ("seed", C.c_uint64)]
+
+
+class JobStatus(C.Structure):
+    _fields_ = [("state", C.c_int32), ("rays", C.c_uint64), ("submit_s", C.c_double), ("start_s", C.c_double),
+                ("finish_s", C.c_double)]
+
+
+# Every entry point of include/xtgpu.h with its argument types.
+SIGNATURES = {
+    "xtgpu_scene_create": [C.POINTER(SceneDesc), C.c_void_p, C.POINTER(C.c_void_p)],
+    "xtgpu_bvh_build": [C.c_void_p, C.POINTER(BvhOpts), C.c_void_p],
+    "xtgpu_scene_destroy": [C.c_void_p],
+    "xtgpu_scene_device_bytes": [C.c_void_p, C.POINTER(C.c_uint64)],
+    "xtgpu_bvh_export": [C.c_void_p, C.POINTER(BvhInfo), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+    "xtgpu_trace": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p],
+    "xtgpu_trace_host": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p],
+    "xtgpu_render": [C.c_void_p, C.POINTER(RenderParams), C.c_void_p, C.POINTER(C.c_uint64), C.c_void_p],
+    "xtgpu_render_host": [C.c_void_p, C.POINTER(RenderParams), C.c_void_p, C.POINTER(C.c_uint64), C.c_void_p],
+    "xtgpu_service_create": [C.POINTER(ServiceOpts), C.c_void_p, C.POINTER(C.c_void_p)],
+    "xtgpu_service_add_scene": [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)],
+    "xtgpu_service_submit": [C.c_void_p, C.POINTER(JobDesc), C.c_double, C.POINTER(C.c_int64)],
+    "xtgpu_service_run": [C.c_void_p, C.c_double],
+    "xtgpu_service_poll": [C.c_void_p, C.c_int64, C.POINTER(JobStatus)],
+    "xtgpu_service_result": [C.c_void_p, C.c_int64, C.c_void_p],
+    "xtgpu_service_release": [C.c_void_p, C.c_int64],
+    "xtgpu_service_destroy": [C.c_void_p],
+    "xtgpu_service_get_stats": [C.c_void_p, C.POINTER(ServiceStats)],
+    "xtgpu_service_reset_stats": [C.c_void_p],
+}
+
+_lib = None
+
+
+def lib():
+    """Loads libxtgpu.so (building it first if it is missing).  Raises if it
+    cannot be built or loaded: there is no CPU fallback."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            from . import build as _b
+            _b.build()
+        L = C.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = C.c_int
+        L.xtgpu_last_error.restype = C.c_char_p
+        L.xtgpu_version.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != 0:
+        raise XtgpuError(status, lib().xtgpu_last_error().decode())
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def stream_handle(stream=None) -> Optional[int]:
+    """cudaStream_t of a torch.cuda.Stream (or None for the default stream)."""
+    if stream is None:
+        return None
+    return int(getattr(stream, "cuda_stream", stream))
+
+
+class Scene:
+    """A flattened xtcore Scene resident on the current CUDA device."""
+
+    def __init__(self, spec, node_formats=(NODES_FP32,), leaf_size: int = 2, stream=None):
+        self.spec = spec
+        keep = []
+
+        def arr(a, dt):
+            a = np.ascontiguousarray(a, dtype=dt)
+            keep.append(a)
+            return _ptr(a)
+
+        d = SceneDesc()
+        d.n_objects = len(spec.obj_kind)
+        d.obj_kind = arr(spec.obj_kind, np.int32)
+        d.obj_first = arr(spec.obj_first, np.int32)
+        d.obj_count = arr(spec.obj_count, np.int32)
+        d.obj_material = arr(spec.obj_material, np.int32)
+        d.n_spheres = spec.spheres.shape[0]
+        d.spheres = arr(spec.spheres.reshape(-1), np.float32)
+        d.n_planes = spec.planes.shape[0]
+        d.planes = arr(spec.planes.reshape(-1), np.float32)
+        d.n_tris = spec.tris.shape[0]
+        d.tris = arr(spec.tris.reshape(-1), np.float32)
+        d.tri_normals = arr(spec.tri_normals.reshape(-1), np.float32) if spec.tri_normals is not None else None
+        mats = (Material * max(1, len(spec.materials)))()
+        for i, m in enumerate(spec.materials):
+            mats[i].type = m.type
+            mats[i].diffuse[:] = list(m.diffuse)
+            mats[i].specular[:] = list(m.specular)
+            mats[i].emissive[:] = list(m.emissive)
+            mats[i].reflectance, mats[i].exponent, mats[i].ior = m.reflectance, m.exponent, m.ior
+        keep.append(mats)
+        d.n_materials = len(spec.materials)
+        d.materials = C.cast(mats, C.c_void_p)
+        d.env_type = spec.env_type
+        d.env_a[:] = list(spec.env_a)
+        d.env_b[:] = list(spec.env_b)
+        cam = spec.camera
+        d.camera.position[:] = list(cam.position)
+        d.camera.target[:] = list(cam.target)
+        d.camera.up[:] = list(cam.up)
+        d.camera.fov = cam.fov
+        h = C.c_void_p()
+        check(lib().xtgpu_scene_create(C.byref(d), stream_handle(stream), C.byref(h)))
+        self.handle = h
+        self.formats = set()
+        for f in node_formats:
+            self.build_bvh(f, leaf_size, stream)
+
+    def build_bvh(self, node_format: int = NODES_FP32, leaf_size: int = 2, stream=None) -> None:
+        o = BvhOpts(node_format, leaf_size)
+        check(lib().xtgpu_bvh_build(self.handle, C.byref(o), stream_handle(stream)))
+        self.formats.add(node_format)
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().xtgpu_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def device_bytes(self) -> int:
+        b = C.c_uint64()
+        check(lib().xtgpu_scene_device_bytes(self.handle, C.byref(b)))
+        return int(b.value)
+
+    def bvh_export(self):
+        info = BvhInfo()
+        check(lib().xtgpu_bvh_export(self.handle, C.byref(info), None, None, None, None, None))
+        n = int(info.n_prims)
+        mort = np.zeros(max(n, 1), np.uint32); order = np.zeros(max(n, 1), np.uint32)
+        left = np.zeros(max(n - 1, 1), np.int32); right = np.zeros(max(n - 1, 1), np.int32)
+        check(lib().xtgpu_bvh_export(self.handle, C.byref(info), _ptr(mort), _ptr(order), _ptr(left), _ptr(right),
+                                     None))
+        return dict(info=info, morton=mort[:n], order=order[:n], left=left[:max(n - 1, 0)], right=right[:max(n - 1, 0)])
+
+    def intersection(self, org: np.ndarray, dirs: np.ndarray, tmin: float = 0.0, tmax: float = np.inf,
+                     node_format: int = NODES_FP32):
+        """Closest hits of a batch of rays (host arrays; copies included)."""
+        org = np.asarray(org, np.float32).reshape(-1, 3)
+        dirs = np.asarray(dirs, np.float32).reshape(-1, 3)
+        n = org.shape[0]
+        o4 = np.empty((n, 4), np.float32); d4 = np.empty((n, 4), np.float32)
+        o4[:, :3] = org; o4[:, 3] = tmin
+        d4[:, :3] = dirs; d4[:, 3] = tmax
+        hits = np.zeros(n, HIT_DTYPE)
+        check(lib().xtgpu_trace_host(self.handle, n, _ptr(o4), _ptr(d4), _ptr(hits), node_format, None))
+        return hits
+
+    def render(self, integrator: int, width: int, height: int, spp: int = 1, rdepth: int = 4,
+               ao_max_distance: float = 100.0, seed: int = 1, node_format: int = NODES_FP32, rect=None):
+        x0, y0, x1, y1 = rect if rect is not None else (0, 0, 0, 0)
+        p = RenderParams(integrator, width, height, spp, rdepth, ao_max_distance, seed, node_format, x0, y0, x1, y1)
+        rw, rh = (x1 - x0, y1 - y0) if rect is not None else (width, height)
+        out = np.zeros((rh, rw, 4), np.float32)
+        rays = C.c_uint64()
+        check(lib().xtgpu_render_host(self.handle, C.byref(p), _ptr(out), C.byref(rays), None))
+        return out, int(rays.value)
+
+
+class Params:
+    """params_t (context.h:18-34) for the GPU integrators; aa is fixed at 1."""
+
+    def __init__(self, width=500, height=500, samples=1, rdepth=100, seed=1, node_format=NODES_FP32,
+                 ao_max_distance=100.0):
+        self.width, self.height, self.samples, self.rdepth = width, height, samples, rdepth
+        self.seed, self.node_format, self.ao_max_distance = seed, node_format, ao_max_distance
+
+
+class Context:
+    """context_t (context.h:36-51): a scene plus render parameters."""
+
+    def __init__(self, scene: Scene, params: Params):
+        self.scene, self.params = scene, params
+
+
+class _Integrator:
+    kind = None
+
+    def __init__(self):
+        self.ctx = None
+        self.rays = 0
+
+    def setup(self, context: Context) -> None:   # IIntegrator::setup, integrator.cc:14-17
+        self.ctx = context
+
+    def render(self):
+        """IIntegrator::render (integrator.cc:29-53) for the whole frame.  Like
+        the reference it does nothing without a context."""
+        if self.ctx is None:
+            return None
+        p = self.ctx.params
+        img, self.rays = self.ctx.scene.render(self.kind, p.width, p.height, p.samples, p.rdepth,
+                                               p.ao_max_distance, p.seed, p.node_format)
+        return img
+
+
+class StencilIntegrator(_Integrator):
+    kind = STENCIL
+
+
+class DepthIntegrator(_Integrator):
+    kind = DEPTH
+
+
+class AOIntegrator(_Integrator):
+    kind = AO
+
+
+class PathtracerIntegrator(_Integrator):
+    kind = PATHTRACER
