@@ -287,6 +287,10 @@ def main():
     if not torch.cuda.is_available():
         raise SystemExit("bench.py needs a CUDA device")
     torch.cuda.set_device(local)
+    # the services launch on this stream and the step events are recorded on it
+    # (the legacy default stream cannot be captured into CUDA graphs)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     D = Dist(world, True)
     from xtracer_b200 import scenes, xtgpu
     from xtracer_b200.service import Service
@@ -298,7 +302,7 @@ def main():
     budget = 48 << 30
 
     served = Service(gscenes, node_format=xtgpu.NODES_Q8, use_graphs=True, merge_jobs=True, memory_budget=budget,
-                     time_kernels=True)
+                     time_kernels=True, stream=stream)
     # warm-up steps (untimed): graphs captured, allocator pools primed
     for w in range(args.warmup):
         run_slice(served, slices[w % nslices])
@@ -338,7 +342,7 @@ def main():
 
     # end to end: same steps, every frame copied to host memory by the service
     e2e_svc = Service(gscenes, node_format=xtgpu.NODES_Q8, use_graphs=True, merge_jobs=True, memory_budget=budget,
-                      host_results=True)
+                      host_results=True, stream=stream)
     run_slice(e2e_svc, slices[0])
     D.barrier()
     torch.cuda.synchronize()
@@ -358,7 +362,7 @@ def main():
     plain = None
     if not args.no_plain:
         psvc = Service(gscenes, node_format=xtgpu.NODES_FP32, use_graphs=False, merge_jobs=False,
-                       memory_budget=budget)
+                       memory_budget=budget, stream=stream)
         torch.cuda.synchronize()
         p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         p0.record()
@@ -383,7 +387,8 @@ def main():
     latency = None
     if not args.no_latency:
         rate = 1.5 * len(timed[0]) / ps if plain is not None else 50.0
-        lsvc = Service(gscenes, node_format=xtgpu.NODES_Q8, use_graphs=True, merge_jobs=True, memory_budget=budget)
+        lsvc = Service(gscenes, node_format=xtgpu.NODES_Q8, use_graphs=True, merge_jobs=True, memory_budget=budget,
+                       stream=stream)
         arr = np.cumsum(np.random.default_rng(4).exponential(1.0 / rate, len(timed[0])))
         ids = [lsvc.submit(j.scene, xtgpu.PATHTRACER, j.width, j.height, j.spp, j.depth, 100.0, j.seed,
                            submit_s=0.05 + float(a)) for j, a in zip(timed[0], arr)]

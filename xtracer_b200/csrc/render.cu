@@ -555,7 +555,7 @@ void WaveRunner::enqueue(int njobs, int64_t total, int bounces, int fmt, bool mu
     for (int b = 0; b < bounces; ++b) {
         cudaMemsetAsync(q.ctl + 2, 0, sizeof(int32_t), s);
         int eb = sms * extend_blocks_per_sm;
-        if (time_extend && b < MAX_TIMED) cudaEventRecord(ev[2 * b], s);
+        if (time_extend && b < MAX_TIMED) cudaEventRecordWithFlags(ev[2 * b], s, cudaEventRecordExternal);
         if (fmt == XTGPU_NODES_Q8) {
             if (multi) k_extend<XTGPU_NODES_Q8, true><<<eb, 128, 0, s>>>(single, scenes, jobs, q, side);
             else k_extend<XTGPU_NODES_Q8, false><<<eb, 128, 0, s>>>(single, scenes, jobs, q, side);
@@ -563,7 +563,7 @@ void WaveRunner::enqueue(int njobs, int64_t total, int bounces, int fmt, bool mu
             if (multi) k_extend<XTGPU_NODES_FP32, true><<<eb, 128, 0, s>>>(single, scenes, jobs, q, side);
             else k_extend<XTGPU_NODES_FP32, false><<<eb, 128, 0, s>>>(single, scenes, jobs, q, side);
         }
-        if (time_extend && b < MAX_TIMED) cudaEventRecord(ev[2 * b + 1], s);
+        if (time_extend && b < MAX_TIMED) cudaEventRecordWithFlags(ev[2 * b + 1], s, cudaEventRecordExternal);
         cudaMemsetAsync(q.ctl + (side ^ 1), 0, sizeof(int32_t), s);
         k_shade<<<gb, 256, 0, s>>>(jobs, scenes, q, side);
         side ^= 1;

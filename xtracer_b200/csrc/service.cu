@@ -38,6 +38,7 @@ struct SvcJob {
 struct xtgpu_service {
     xtgpu_service_opts o{};
     cudaStream_t s = nullptr;
+    bool own_stream = false;   // created here: the legacy default stream cannot be captured
     xtg::WaveRunner R;
     std::vector<xtgpu_scene *> scenes;
     std::vector<xtg::DevScene> dev;
@@ -92,10 +93,19 @@ xtgpu_status xtgpu_service_create(const xtgpu_service_opts *opts, void *stream, 
     xtgpu_service *v = new xtgpu_service();
     v->o = *opts;
     v->s = (cudaStream_t)stream;
+    if (!v->s) {
+        if (cudaStreamCreateWithFlags(&v->s, cudaStreamNonBlocking) != cudaSuccess) {
+            delete v;
+            set_error("xtgpu_service_create: cudaStreamCreate failed");
+            return XTGPU_ERR_CUDA;
+        }
+        v->own_stream = true;
+    }
     int64_t cap = opts->wave_paths > 0 ? opts->wave_paths : (1ll << 22);
     xtgpu_status st = v->R.init(cap, opts->max_jobs, 64, v->s);
     if (st != XTGPU_OK) {
         v->R.release();
+        if (v->own_stream) cudaStreamDestroy(v->s);
         delete v;
         return st;
     }
@@ -379,6 +389,7 @@ xtgpu_status xtgpu_service_destroy(xtgpu_service *v)
         if (kv.second.frame) cudaFreeAsync(kv.second.frame, v->s);
     cudaStreamSynchronize(v->s);
     v->R.release();
+    if (v->own_stream) cudaStreamDestroy(v->s);
     delete v;
     return XTGPU_OK;
 }
