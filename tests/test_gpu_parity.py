@@ -101,11 +101,13 @@ def test_lbvh_bit_exact_vs_cpu(name):
     sc.close()
 
 
-def gpu_primary(spec, w, h, fmt=xtgpu.NODES_FP32, sc=None):
+def gpu_primary(spec, w, h, fmt=xtgpu.NODES_FP32, sc=None, px=None):
     """Primary rays through the GPU: the FP64 reference camera rays rounded to
-    FP32, traced by xtgpu_trace_host."""
-    ys, xs = np.mgrid[0:h, 0:w]
-    px = np.stack([xs.ravel(), ys.ravel()], 1)
+    FP32, traced by xtgpu_trace_host.  px: (x, y) pixel list (default: the
+    frame in row-major order)."""
+    if px is None:
+        ys, xs = np.mgrid[0:h, 0:w]
+        px = np.stack([xs.ravel(), ys.ravel()], 1)
     org, dirs = po.camera_rays(spec, w, h, px)
     own = sc is None
     if own:
@@ -121,7 +123,9 @@ def gpu_primary(spec, w, h, fmt=xtgpu.NODES_FP32, sc=None):
 def test_primary_hits_vs_reference_golden(name, fmt):
     spec, w, h = small_scenes()[name]
     g = np.load(os.path.join(GOLD, "hits_%s.npz" % name))
-    org, dirs, hits = gpu_primary(spec, w, h, fmt)
+    # fixture records are in the reference driver's tile order
+    org, dirs, hits = gpu_primary(spec, w, h, fmt, px=g["xy"])
+    assert np.array_equal(org, g["org"]) and np.array_equal(dirs, g["dir"])
     g_hit = (hits["prim"] != 0xffffffff).astype(np.int32)
     g_gid = hits["prim"].astype(np.int64)
     r_hit = g["hit"].astype(np.int32)

@@ -521,8 +521,8 @@ xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, cudaStre
             int32_t *left = (int32_t *)sc->left.p, *right = (int32_t *)sc->right.p;
             k_gather<<<blocks(n, 256), 256, 0, s>>>(n, S.n_tris, vals, S.tri_v, S.spheres, (float4 *)sc->leaf_prims.p);
             S.leaf_prims = (const float4 *)sc->leaf_prims.p;
-            if (n <= leaf_size) {
-                S.root = leaf_ref(0, (uint32_t)n);
+            if (n == 1) {
+                S.root = leaf_ref(0, 1u);
                 sc->depth = 0;
                 // a single dummy node keeps the node pointers valid
                 XTG_TRY(dalloc(sc->nodes32, sizeof(float4) * 4, s));
@@ -561,7 +561,8 @@ xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, cudaStre
                     return XTGPU_ERR_CUDA;
                 }
                 sc->depth = h;
-                S.root = 0;
+                // a scene no larger than one leaf is traversed as that leaf
+                S.root = n <= leaf_size ? leaf_ref(0, (uint32_t)n) : 0;
             }
             XTG_CUDA(cudaGetLastError());
         }
