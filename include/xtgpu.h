@@ -235,6 +235,19 @@ typedef struct {
 XTGPU_API xtgpu_status xtgpu_service_get_stats(xtgpu_service *svc, xtgpu_service_stats *stats);
 XTGPU_API xtgpu_status xtgpu_service_reset_stats(xtgpu_service *svc);
 
+/* ---------------------------------------------------------------------- */
+/* Launch configuration of the wavefront kernels (process-wide).            */
+typedef struct {
+    int32_t extend_variant;        /* 0 = warp-batched ray fetch, 1 = per-lane refill */
+    int32_t extend_block;          /* threads per block of the extend kernel (32..256) */
+    int32_t extend_blocks_per_sm;  /* resident extend blocks per SM, in 128-thread units */
+    int32_t tile;                  /* camera ray order: square pixel tiles of this edge (0 = rows) */
+    int64_t wave_paths;            /* paths per wave of xtgpu_render */
+    int32_t leaf_size;             /* default primitives per BVH leaf */
+} xtgpu_tuning;
+XTGPU_API xtgpu_status xtgpu_get_tuning(xtgpu_tuning *t);
+XTGPU_API xtgpu_status xtgpu_set_tuning(const xtgpu_tuning *t);
+
 /* Text of the last error on this thread ("" if none). */
 XTGPU_API const char *xtgpu_last_error(void);
 /* Library version string. */

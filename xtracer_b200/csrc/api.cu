@@ -108,6 +108,29 @@ using namespace xtg;
 extern "C" {
 
 const char *xtgpu_last_error(void) { return g_err.c_str(); }
+
+xtgpu_status xtgpu_get_tuning(xtgpu_tuning *t)
+{
+    if (!t) {
+        set_error("xtgpu_get_tuning: NULL argument");
+        return XTGPU_ERR_INVALID;
+    }
+    *t = tuning();
+    return XTGPU_OK;
+}
+
+xtgpu_status xtgpu_set_tuning(const xtgpu_tuning *t)
+{
+    if (!t || t->extend_variant < 0 || t->extend_variant > 1 || t->extend_block < 32 || t->extend_block > 256 ||
+        (t->extend_block & 31) || t->extend_blocks_per_sm < 1 || t->extend_blocks_per_sm > 64 || t->tile < 0 ||
+        t->tile > 256 || t->wave_paths < 1024 || t->wave_paths > (1ll << 26) || t->leaf_size < 1 ||
+        t->leaf_size > MAX_LEAF) {
+        set_error("xtgpu_set_tuning: value out of range");
+        return XTGPU_ERR_INVALID;
+    }
+    tuning() = *t;
+    return XTGPU_OK;
+}
 const char *xtgpu_version(void) { return "xtgpu 0.1 (sm_100a)"; }
 
 xtgpu_status xtgpu_scene_create(const xtgpu_scene_desc *d, void *stream, xtgpu_scene **out)
@@ -240,7 +263,7 @@ xtgpu_status xtgpu_bvh_build(xtgpu_scene *sc, const xtgpu_bvh_opts *opts, void *
         return XTGPU_ERR_INVALID;
     }
     int fmt = opts ? opts->node_format : XTGPU_NODES_FP32;
-    int leaf = opts && opts->leaf_size > 0 ? opts->leaf_size : 2;
+    int leaf = opts && opts->leaf_size > 0 ? opts->leaf_size : tuning().leaf_size;
     if (fmt != XTGPU_NODES_FP32 && fmt != XTGPU_NODES_Q8) {
         set_error("xtgpu_bvh_build: bad node format");
         return XTGPU_ERR_INVALID;
@@ -342,7 +365,7 @@ xtgpu_status xtgpu_trace(xtgpu_scene *sc, int64_t n, const void *org, const void
         q.rays = (unsigned long long *)((char *)ctl + 32);
         int32_t init[4] = {cnt, 0, 0, 0};
         XTG_CUDA(cudaMemcpyAsync(ctl, init, sizeof(init), cudaMemcpyHostToDevice, s));
-        launch_extend(fmt, sc->dev, q, 0, sms * 12, s);
+        launch_extend(fmt, sc->dev, q, 0, sms * tuning().extend_blocks_per_sm, s);
         XTG_CUDA(cudaGetLastError());
         int32_t back[4];
         XTG_CUDA(cudaMemcpyAsync(back, ctl, sizeof(back), cudaMemcpyDeviceToHost, s));
@@ -410,7 +433,7 @@ xtgpu_status xtgpu_render(xtgpu_scene *sc, const xtgpu_render_params *p, float *
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t npix = (int64_t)(x1 - x0) * (y1 - y0);
     const int64_t paths = npix * p->spp;
-    const int64_t cap = std::min<int64_t>(paths, 1ll << 22);
+    const int64_t cap = std::min<int64_t>(paths, tuning().wave_paths);
     std::lock_guard<std::mutex> lock(g_runner_mu);
     WaveRunner *R = nullptr;
     XTG_TRY(get_runner(std::max<int64_t>(cap, 1 << 16), s, &R));
@@ -431,6 +454,7 @@ xtgpu_status xtgpu_render(xtgpu_scene *sc, const xtgpu_render_params *p, float *
     J.rh = y1 - y0;
     J.scene = 0;
     J.bounces = bounces_of(p->integrator, p->rdepth);
+    J.tile = tuning().tile;
     J.frame = (float4 *)rgba;
     std::vector<DevJob> jobs(1, J);
     for (int64_t first = 0; first < paths; first += R->cap) {

@@ -364,7 +364,9 @@ __device__ __forceinline__ uint32_t pick_exp(float origin, float hi)
         int be = ex + 127;
         e = (uint32_t)max(1, min(254, be - 1));
     }
-    while (e < 254 && __fmaf_rn(255.0f, __uint_as_float(e << 23), origin) < hi) ++e;
+    // 254 quanta must reach hi
+    // one quantum of headroom above hi (the bounds are padded by one quantum)
+    while (e < 254 && __fmaf_rn(254.0f, __uint_as_float(e << 23), origin) < hi) ++e;
     return e;
 }
 
@@ -381,8 +383,10 @@ __device__ __forceinline__ void quant_axis(float lo, float hi, float o, float sc
     int qh = (int)fmaxf(0.f, fminf(255.f, b));
     while (ql > 0 && __fmaf_rn((float)ql, sc, o) > lo) --ql;
     while (qh < 255 && __fmaf_rn((float)qh, sc, o) < hi) ++qh;
-    qlo = (uint32_t)ql;
-    qhi = (uint32_t)qh;
+    // one quantum of padding on each side: the traversal evaluates the bounds
+    // in t-space with different rounding than this dequantisation
+    qlo = (uint32_t)max(0, ql - 1);
+    qhi = (uint32_t)min(255, qh + 1);
 }
 
 __global__ void k_quantise(int nnodes, const float4 *nodes, uint4 *q)

@@ -181,6 +181,29 @@ __device__ __forceinline__ float3 hit_normal(const DevScene &S, uint32_t prim, f
     return f3(S.planes[prim - S.n_tris - S.n_spheres]);
 }
 
+// Pixel of the k-th pixel slot of a job.  With tiles, slots run through
+// square tiles of `tile` pixels (row-major tiles, row-major inside a tile; the
+// last band and column may be partial), which keeps the rays of a warp close
+// together on screen.  A bijection of [0, rw*rh), so every pixel is visited once.
+__device__ __forceinline__ void pixel_of(const DevJob &J, int64_t k, int &x, int &y)
+{
+    const int T = J.tile;
+    if (T <= 1) {
+        x = J.x0 + (int)(k % J.rw);
+        y = J.y0 + (int)(k / J.rw);
+        return;
+    }
+    const int64_t bandpix = (int64_t)T * J.rw;
+    const int64_t band = k / bandpix;
+    const int64_t qq = k - band * bandpix;
+    const int th = min(T, J.rh - (int)band * T);
+    const int64_t c = qq / ((int64_t)T * th);
+    const int wc = min(T, J.rw - (int)c * T);
+    const int64_t rr = qq - c * T * th;
+    y = J.y0 + (int)band * T + (int)(rr / wc);
+    x = J.x0 + (int)c * T + (int)(rr % wc);
+}
+
 __device__ __forceinline__ int find_job(const DevJob *jobs, int njobs, int64_t i)
 {
     int lo = 0, hi = njobs - 1;
@@ -217,7 +240,8 @@ __global__ void k_camera(const DevJob *__restrict__ jobs, const DevScene *__rest
         int64_t p = J.first + (i - J.offset);
         int64_t npix = (int64_t)J.rw * J.rh;
         int64_t s = p / npix, pix = p - s * npix;
-        int x = J.x0 + (int)(pix % J.rw), y = J.y0 + (int)(pix / J.rw);
+        int x, y;
+        pixel_of(J, pix, x, y);
         float3 o, d;
         camera_ray(scenes[J.scene].cam, (float)x + 0.5f, (float)y + 0.5f, (float)J.width, (float)J.height, o, d);
         q.org[0][i] = make_float4(o.x, o.y, o.z, 0.f);
@@ -229,53 +253,233 @@ __global__ void k_camera(const DevJob *__restrict__ jobs, const DevScene *__rest
     }
 }
 
-// Persistent extend: each warp takes 32 queued rays at a time from a global
-// counter until the queue is drained.
+// Persistent extend.  Every lane holds one ray; a lane that finishes takes the
+// next queued ray at once (warp-aggregated fetch), so warps stay full while
+// long rays are still traversing.  Inner nodes are walked until the lane
+// reaches a leaf (while-while); stack entries keep their entry distance so a
+// popped subtree beyond the current closest hit is skipped without a fetch.
 template <int FMT, bool MULTI>
-__global__ void __launch_bounds__(128) k_extend(DevScene S1, const DevScene *__restrict__ scenes,
-                                                const DevJob *__restrict__ jobs, WaveQueues q, int side)
+__global__ void __launch_bounds__(256) k_extend_refill(DevScene S1, const DevScene *__restrict__ scenes,
+                                                       const DevJob *__restrict__ jobs, WaveQueues q, int side)
 {
     const int n = q.ctl[side];
     const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(q.rays, (unsigned long long)n);
-    const bool per_job = q.job_rays != nullptr;
     const float4 *org = q.org[side], *dir = q.dir[side];
+    SceneView V = scene_view<FMT>(S1);
+    RayPre r;
+    float tmin = 0.f, tmax = 0.f, bu = 0.f, bv = 0.f;
+    uint32_t prim = 0xffffffffu, nv = 0, np = 0, guard = 0;
+    int32_t ref = 0, idx = 0;
+    int sp = 0;
+    int2 stack[STACK_MAX];
+    bool active = false, exhausted = false;
+    while (true) {
+        // refill finished lanes from the queue
+        const bool want = !active && !exhausted;
+        const unsigned m = __ballot_sync(0xffffffffu, want);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(&q.ctl[2], __popc(m));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            uint32_t jb = 0xffffffffu;
+            if (want) {
+                idx = base + __popc(m & lt);
+                if (idx < n) {
+                    float4 a = org[idx], b = dir[idx];
+                    ray_pre(make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z), r);
+                    tmin = a.w;
+                    tmax = b.w;
+                    if (MULTI || q.job_rays) jb = q.meta[side][idx].y;
+                    if (MULTI) V = scene_view<FMT>(scenes[jobs[jb].scene]);
+                    prim = 0xffffffffu;
+                    bu = bv = 0.f;
+                    ref = V.root;
+                    sp = 0;
+                    nv = np = guard = 0;
+                    active = true;
+                } else {
+                    exhausted = true;
+                }
+            }
+            if (q.job_rays) {
+                // rays per job: one atomic per group of lanes of the same job
+                const unsigned peers = __match_any_sync(0xffffffffu, jb);
+                if (jb != 0xffffffffu && (peers & lt) == 0u) atomicAdd(&q.job_rays[jb], (unsigned long long)__popc(peers));
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (!active) continue;
+        bool done = false;
+        // inner nodes until a leaf (or the end of the ray)
+        while (ref >= 0) {
+            if (++guard > (1u << 22)) {   // corrupted tree: report, never loop forever
+                q.ctl[3] = 1;
+                done = true;
+                break;
+            }
+            Pair P;
+            node_pair<FMT>(V.nodes, ref, r, tmin, tmax, P);
+            ++nv;
+            if (P.h0 && P.h1) {
+                const bool sw = P.t1 < P.t0;
+                if (sp >= STACK_MAX) {
+                    q.ctl[3] = 1;
+                    done = true;
+                    break;
+                }
+                stack[sp++] = make_int2(sw ? P.c0 : P.c1, __float_as_int(sw ? P.t0 : P.t1));
+                ref = sw ? P.c1 : P.c0;
+            } else if (P.h0) {
+                ref = P.c0;
+            } else if (P.h1) {
+                ref = P.c1;
+            } else {
+                ref = EMPTY_REF;   // nothing here: fall through to the pop below
+                break;
+            }
+        }
+        if (!done) {
+            if (ref != EMPTY_REF) {
+                np += leaf_count(ref);
+                leaf_test(V, ref, r, tmin, tmax, prim, bu, bv);
+            }
+            // next subtree still in front of the closest hit, or the end
+            done = true;
+            while (sp > 0) {
+                const int2 e = stack[--sp];
+                if (__int_as_float(e.y) <= tmax) {
+                    ref = e.x;
+                    done = false;
+                    break;
+                }
+            }
+        }
+        if (done) {
+            for (int p = 0; p < V.n_planes; ++p)
+                if (hit_plane(r, __ldg(V.planes + p), tmin, tmax)) {
+                    prim = V.plane_base + (uint32_t)p;
+                    bu = bv = 0.f;
+                }
+            xtgpu_hit o;
+            o.t = prim != 0xffffffffu ? tmax : INFINITY;
+            o.prim = prim;
+            o.u = bu;
+            o.v = bv;
+            q.hit[idx] = o;
+            if (q.stats) {
+                atomicAdd(&q.stats[0], (unsigned long long)nv);
+                atomicAdd(&q.stats[1], (unsigned long long)(np + (uint32_t)V.n_planes));
+            }
+            active = false;
+        }
+    }
+}
+
+// Closest hit of one ray: a single loop that takes one node or one leaf per
+// iteration; stack entries keep their entry distance so subtrees beyond the
+// current closest hit are dropped without a fetch.
+template <int FMT>
+__device__ __forceinline__ void trace_ray(const SceneView &V, const RayPre &r, float tmin, float &tmax,
+                                          uint32_t &prim, float &bu, float &bv, int32_t *ctl_overflow, uint32_t &nv,
+                                          uint32_t &np)
+{
+    int2 stack[STACK_MAX];
+    int sp = 0;
+    int32_t ref = V.root;
+    for (uint32_t guard = 0;; ++guard) {
+        if (guard >= (1u << 22)) {   // corrupted tree: report, never loop forever
+            *ctl_overflow = 1;
+            break;
+        }
+        if (ref >= 0) {
+            Pair P;
+            node_pair<FMT>(V.nodes, ref, r, tmin, tmax, P);
+            ++nv;
+            if (P.h0 && P.h1) {
+                const bool sw = P.t1 < P.t0;
+                if (sp >= STACK_MAX) {
+                    *ctl_overflow = 1;
+                    break;
+                }
+                stack[sp++] = make_int2(sw ? P.c0 : P.c1, __float_as_int(sw ? P.t0 : P.t1));
+                ref = sw ? P.c1 : P.c0;
+                continue;
+            }
+            if (P.h0) { ref = P.c0; continue; }
+            if (P.h1) { ref = P.c1; continue; }
+        } else if (ref != EMPTY_REF) {
+            np += leaf_count(ref);
+            leaf_test(V, ref, r, tmin, tmax, prim, bu, bv);
+        }
+        bool more = false;
+        while (sp > 0) {
+            const int2 e = stack[--sp];
+            if (__int_as_float(e.y) <= tmax) {
+                ref = e.x;
+                more = true;
+                break;
+            }
+        }
+        if (!more) break;
+    }
+    for (int p = 0; p < V.n_planes; ++p)
+        if (hit_plane(r, __ldg(V.planes + p), tmin, tmax)) {
+            prim = V.plane_base + (uint32_t)p;
+            bu = bv = 0.f;
+        }
+}
+
+// Persistent extend, warp-batched: each warp takes the next 32 queued rays and
+// every lane runs its ray to the end.
+template <int FMT, bool MULTI>
+__global__ void __launch_bounds__(256) k_extend_batch(DevScene S1, const DevScene *__restrict__ scenes,
+                                                      const DevJob *__restrict__ jobs, WaveQueues q, int side)
+{
+    const int n = q.ctl[side];
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(q.rays, (unsigned long long)n);
+    const float4 *org = q.org[side], *dir = q.dir[side];
+    const SceneView V1 = scene_view<FMT>(S1);
     while (true) {
         int base = 0;
         if (lane == 0) base = atomicAdd(&q.ctl[2], 32);
         base = __shfl_sync(0xffffffffu, base, 0);
         if (base >= n) break;
-        int i = base + lane;
+        const int i = base + lane;
+        uint32_t jb = 0xffffffffu;
         if (i < n) {
             float4 a = org[i], b = dir[i];
             RayPre r;
             ray_pre(make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z), r);
-            HitRec h;
-            uint32_t nv = 0, np = 0;
-            uint32_t *pv = q.stats ? &nv : nullptr, *pp = q.stats ? &np : nullptr;
+            float tmax = b.w, bu = 0.f, bv = 0.f;
+            uint32_t prim = 0xffffffffu, nv = 0, np = 0;
+            if (MULTI || q.job_rays) jb = q.meta[side][i].y;
             if (MULTI) {
-                const DevScene &S = scenes[jobs[q.meta[side][i].y].scene];
-                trace_closest<FMT>(S, r, a.w, b.w, h, &q.ctl[3], pv, pp);
+                const SceneView V = scene_view<FMT>(scenes[jobs[jb].scene]);
+                trace_ray<FMT>(V, r, a.w, tmax, prim, bu, bv, &q.ctl[3], nv, np);
+                np += (uint32_t)V.n_planes;
             } else {
-                trace_closest<FMT>(S1, r, a.w, b.w, h, &q.ctl[3], pv, pp);
+                trace_ray<FMT>(V1, r, a.w, tmax, prim, bu, bv, &q.ctl[3], nv, np);
+                np += (uint32_t)V1.n_planes;
             }
+            xtgpu_hit o;
+            o.t = prim != 0xffffffffu ? tmax : INFINITY;
+            o.prim = prim;
+            o.u = bu;
+            o.v = bv;
+            q.hit[i] = o;
             if (q.stats) {
                 atomicAdd(&q.stats[0], (unsigned long long)nv);
                 atomicAdd(&q.stats[1], (unsigned long long)np);
             }
-            xtgpu_hit o;
-            o.t = h.t;
-            o.prim = h.prim;
-            o.u = h.u;
-            o.v = h.v;
-            q.hit[i] = o;
         }
-        if (per_job) {
-            // rays per job: one atomic per group of lanes of the same job
-            uint32_t jb = i < n ? q.meta[side][i].y : 0xffffffffu;
-            unsigned peers = __match_any_sync(0xffffffffu, jb);
-            if (i < n && (peers & ((1u << lane) - 1u)) == 0u)
-                atomicAdd(&q.job_rays[jb], (unsigned long long)__popc(peers));
+        if (q.job_rays) {
+            const unsigned peers = __match_any_sync(0xffffffffu, jb);
+            if (jb != 0xffffffffu && (peers & lt) == 0u) atomicAdd(&q.job_rays[jb], (unsigned long long)__popc(peers));
         }
     }
 }
@@ -305,7 +509,9 @@ __global__ void k_shade(const DevJob *__restrict__ jobs, const DevScene *__restr
             int64_t path = J.first + (lp - J.offset);
             int64_t npix = (int64_t)J.rw * J.rh;
             int64_t smp = path / npix, pix = path - smp * npix;
-            int64_t fx = J.x0 + pix % J.rw, fy = J.y0 + pix / J.rw;
+            int px_, py_;
+            pixel_of(J, pix, px_, py_);
+            int64_t fx = px_, fy = py_;
             uint64_t key = path_key(J.seed, (uint64_t)smp * (uint64_t)J.width * (uint64_t)J.height +
                                                 (uint64_t)fy * (uint64_t)J.width + (uint64_t)fx);
             switch (J.integrator) {
@@ -426,7 +632,10 @@ __global__ void k_accumulate(const DevJob *__restrict__ jobs, const int32_t *__r
         if (a - pix <= 0) s_lo = 0;
         int64_t s_hi = (e - 1 - pix) / npix;
         if (e - 1 - pix < 0) continue;
-        float4 c = J.frame[pix];
+        int fx, fy;
+        pixel_of(J, pix, fx, fy);
+        const int64_t fpix = (int64_t)(fy - J.y0) * J.rw + (fx - J.x0);
+        float4 c = J.frame[fpix];
         double w = 1.f;
         w *= 1.0 / (double)J.spp;
         for (int64_t s = s_lo; s <= s_hi; ++s) {
@@ -458,7 +667,7 @@ __global__ void k_accumulate(const DevJob *__restrict__ jobs, const int32_t *__r
             }
             }
         }
-        J.frame[pix] = c;
+        J.frame[fpix] = c;
     }
 }
 
@@ -554,15 +763,9 @@ void WaveRunner::enqueue(int njobs, int64_t total, int bounces, int fmt, bool mu
     int side = 0;
     for (int b = 0; b < bounces; ++b) {
         cudaMemsetAsync(q.ctl + 2, 0, sizeof(int32_t), s);
-        int eb = sms * extend_blocks_per_sm;
+        int eb = sms * tuning().extend_blocks_per_sm;
         if (time_extend && b < MAX_TIMED) cudaEventRecordWithFlags(ev[2 * b], s, cudaEventRecordExternal);
-        if (fmt == XTGPU_NODES_Q8) {
-            if (multi) k_extend<XTGPU_NODES_Q8, true><<<eb, 128, 0, s>>>(single, scenes, jobs, q, side);
-            else k_extend<XTGPU_NODES_Q8, false><<<eb, 128, 0, s>>>(single, scenes, jobs, q, side);
-        } else {
-            if (multi) k_extend<XTGPU_NODES_FP32, true><<<eb, 128, 0, s>>>(single, scenes, jobs, q, side);
-            else k_extend<XTGPU_NODES_FP32, false><<<eb, 128, 0, s>>>(single, scenes, jobs, q, side);
-        }
+        launch_extend_kernel(fmt, multi, single, scenes, jobs, q, side, eb, s);
         if (time_extend && b < MAX_TIMED) cudaEventRecordWithFlags(ev[2 * b + 1], s, cudaEventRecordExternal);
         cudaMemsetAsync(q.ctl + (side ^ 1), 0, sizeof(int32_t), s);
         k_shade<<<gb, 256, 0, s>>>(jobs, scenes, q, side);
@@ -660,10 +863,33 @@ xtgpu_status WaveRunner::read_ctl(int32_t *overflow, unsigned long long *rays, c
     return XTGPU_OK;
 }
 
+// Process-wide launch configuration (xtgpu_set_tuning / xtgpu_autotune).
+// Defaults from a sweep on a B200 (variant x leaf x node format x launch shape x
+// tile over terrain, hairball and sphere scenes): warp-batched fetch, one
+// primitive per leaf, 8x8 pixel tiles; the launch shape barely matters.
+static xtgpu_tuning g_tuning = {0, 128, 12, 8, 1ll << 22, 1};
+xtgpu_tuning &tuning() { return g_tuning; }
+
+void launch_extend_kernel(int fmt, bool multi, const DevScene &single, const DevScene *scenes, const DevJob *jobs,
+                          const WaveQueues &q, int side, int blocks, cudaStream_t s)
+{
+    const xtgpu_tuning &T = tuning();
+    const int tb = T.extend_block;
+    const int nb = std::max(1, blocks * 128 / tb);   // same resident thread count for any block size
+#define XTG_LAUNCH(K, F, M) K<F, M><<<nb, tb, 0, s>>>(single, scenes, jobs, q, side)
+    if (T.extend_variant == 1) {
+        if (fmt == XTGPU_NODES_Q8) { if (multi) XTG_LAUNCH(k_extend_refill, XTGPU_NODES_Q8, true); else XTG_LAUNCH(k_extend_refill, XTGPU_NODES_Q8, false); }
+        else { if (multi) XTG_LAUNCH(k_extend_refill, XTGPU_NODES_FP32, true); else XTG_LAUNCH(k_extend_refill, XTGPU_NODES_FP32, false); }
+    } else {
+        if (fmt == XTGPU_NODES_Q8) { if (multi) XTG_LAUNCH(k_extend_batch, XTGPU_NODES_Q8, true); else XTG_LAUNCH(k_extend_batch, XTGPU_NODES_Q8, false); }
+        else { if (multi) XTG_LAUNCH(k_extend_batch, XTGPU_NODES_FP32, true); else XTG_LAUNCH(k_extend_batch, XTGPU_NODES_FP32, false); }
+    }
+#undef XTG_LAUNCH
+}
+
 void launch_extend(int fmt, const DevScene &S, const WaveQueues &q, int side, int blocks, cudaStream_t s)
 {
-    if (fmt == XTGPU_NODES_Q8) k_extend<XTGPU_NODES_Q8, false><<<blocks, 128, 0, s>>>(S, nullptr, nullptr, q, side);
-    else k_extend<XTGPU_NODES_FP32, false><<<blocks, 128, 0, s>>>(S, nullptr, nullptr, q, side);
+    launch_extend_kernel(fmt, false, S, nullptr, nullptr, q, side, blocks, s);
 }
 
 int bounces_of(int integrator, int rdepth)

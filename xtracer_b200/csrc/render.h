@@ -31,7 +31,6 @@ struct WaveRunner {
     int64_t cap = 0;
     int max_jobs = 0, max_scenes = 0, nscenes = 0;
     int sms = 148;
-    int extend_blocks_per_sm = 12;
     DevScene single{};
     std::unordered_map<uint64_t, cudaGraphExec_t> graphs;
 
@@ -47,6 +46,9 @@ struct WaveRunner {
 };
 
 int bounces_of(int integrator, int rdepth);
+xtgpu_tuning &tuning();
+void launch_extend_kernel(int fmt, bool multi, const DevScene &single, const DevScene *scenes, const DevJob *jobs,
+                          const WaveQueues &q, int side, int blocks, cudaStream_t s);
 // Closest hit of the q.ctl[side] rays of queue `side` (no job table needed).
 void launch_extend(int fmt, const DevScene &S, const WaveQueues &q, int side, int blocks, cudaStream_t s);
 

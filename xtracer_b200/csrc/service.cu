@@ -201,24 +201,26 @@ xtgpu_status xtgpu_service_run(xtgpu_service *v, double max_seconds)
             set_error("xtgpu_service_run: admission stalled");
             return XTGPU_ERR_STATE;
         }
-        // plan the wave: an equal share of the capacity per running job, then
-        // the rest in admission order
+        // plan the wave: jobs with the fewest remaining paths first, each taking
+        // what it still needs up to the capacity left.  Small jobs finish in the
+        // next wave (low latency); the largest share whatever remains, so the
+        // queue is always full (throughput).
         wave.clear();
         ids.clear();
         int64_t left = cap;
         int n = (int)v->active.size();
+        std::vector<int> order(n);
+        for (int k = 0; k < n; ++k) order[k] = k;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+            const SvcJob &A = v->jobs[v->active[a]], &B = v->jobs[v->active[b]];
+            return (A.paths - A.done) < (B.paths - B.done);
+        });
         std::vector<int64_t> take(n, 0);
-        int64_t share = std::max<int64_t>(1, cap / n);
-        for (int k = 0; k < n && left > 0; ++k) {
+        for (int k : order) {
+            if (left <= 0) break;
             SvcJob &J = v->jobs[v->active[k]];
-            take[k] = std::min<int64_t>({share, J.paths - J.done, left});
+            take[k] = std::min<int64_t>(J.paths - J.done, left);
             left -= take[k];
-        }
-        for (int k = 0; k < n && left > 0; ++k) {
-            SvcJob &J = v->jobs[v->active[k]];
-            int64_t more = std::min<int64_t>(J.paths - J.done - take[k], left);
-            take[k] += more;
-            left -= more;
         }
         int bounces = 0;
         for (int k = 0; k < n; ++k) {
@@ -238,6 +240,7 @@ xtgpu_status xtgpu_service_run(xtgpu_service *v, double max_seconds)
             dj.rh = J.d.height;
             dj.scene = J.d.scene;
             dj.bounces = bounces_of(J.d.integrator, J.d.rdepth);
+            dj.tile = tuning().tile;
             dj.frame = J.frame;
             dj.first = J.done;
             dj.count = take[k];

@@ -144,137 +144,123 @@ __device__ __forceinline__ bool hit_plane(const RayPre &r, float4 pl, float tmin
     return true;
 }
 
-struct Node2 {
-    float lx[2], hx[2], ly[2], hy[2], lz[2], hz[2];
-    int32_t ref[2];
+// Both children of a node: entry distances and whether each box is hit.
+struct Pair {
+    float t0, t1;
+    bool h0, h1;
+    int32_t c0, c1;
 };
 
-template <int FMT>
-__device__ __forceinline__ void load_node(const DevScene &S, int32_t i, Node2 &n);
-
-template <>
-__device__ __forceinline__ void load_node<XTGPU_NODES_FP32>(const DevScene &S, int32_t i, Node2 &n)
+__device__ __forceinline__ bool slab_t(float tx0, float tx1, float ty0, float ty1, float tz0, float tz1, float tmin,
+                                       float tmax, float scale, float &tnear)
 {
-    const float4 *p = S.nodes32 + 4 * (size_t)i;
+    float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
+    float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
+    tnear = tn;
+    return tn <= tf * scale;
+}
+
+template <int FMT>
+__device__ __forceinline__ void node_pair(const void *nodes, int32_t i, const RayPre &r, float tmin, float tmax,
+                                          Pair &P);
+
+// 64-byte node: (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y) (c1 ...) (c0.lo.z, c0.hi.z,
+// c1.lo.z, c1.hi.z) (ref0, ref1, -, -)
+template <>
+__device__ __forceinline__ void node_pair<XTGPU_NODES_FP32>(const void *nodes, int32_t i, const RayPre &r, float tmin,
+                                                            float tmax, Pair &P)
+{
+    const float4 *p = (const float4 *)nodes + 4 * (size_t)i;
     float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
-    n.lx[0] = a.x; n.hx[0] = a.y; n.ly[0] = a.z; n.hy[0] = a.w;
-    n.lx[1] = b.x; n.hx[1] = b.y; n.ly[1] = b.z; n.hy[1] = b.w;
-    n.lz[0] = c.x; n.hz[0] = c.y; n.lz[1] = c.z; n.hz[1] = c.w;
-    n.ref[0] = __float_as_int(d.x);
-    n.ref[1] = __float_as_int(d.y);
+    P.h0 = slab_t(fmaf(a.x, r.inv.x, -r.oinv.x), fmaf(a.y, r.inv.x, -r.oinv.x), fmaf(a.z, r.inv.y, -r.oinv.y),
+                  fmaf(a.w, r.inv.y, -r.oinv.y), fmaf(c.x, r.inv.z, -r.oinv.z), fmaf(c.y, r.inv.z, -r.oinv.z), tmin,
+                  tmax, XTG_TFAR_SCALE, P.t0);
+    P.h1 = slab_t(fmaf(b.x, r.inv.x, -r.oinv.x), fmaf(b.y, r.inv.x, -r.oinv.x), fmaf(b.z, r.inv.y, -r.oinv.y),
+                  fmaf(b.w, r.inv.y, -r.oinv.y), fmaf(c.z, r.inv.z, -r.oinv.z), fmaf(c.w, r.inv.z, -r.oinv.z), tmin,
+                  tmax, XTG_TFAR_SCALE, P.t1);
+    P.c0 = __float_as_int(d.x);
+    P.c1 = __float_as_int(d.y);
 }
 
-// 32-byte node: origin xyz with the biased power-of-two scale exponent in each
-// low byte, 12 child bounds of 8 bits, two child refs.
+// Slightly larger far-distance scale for the quantised test, whose bounds are
+// formed in t-space as q * (scale * inv) + (origin * inv - o * inv).
+#define XTG_TFAR_SCALE_Q8 1.0000015f
+
+// 32-byte node: origin xyz with a biased power-of-two scale exponent in each
+// low byte, 12 child bounds of 8 bits, two child refs.  The slab test runs in
+// quantised space: t(q) = q * (s * inv) + (o - ray.o) * inv, one FMA per bound.
 template <>
-__device__ __forceinline__ void load_node<XTGPU_NODES_Q8>(const DevScene &S, int32_t i, Node2 &n)
+__device__ __forceinline__ void node_pair<XTGPU_NODES_Q8>(const void *nodes, int32_t i, const RayPre &r, float tmin,
+                                                          float tmax, Pair &P)
 {
-    const uint4 *p = S.nodes8 + 2 * (size_t)i;
+    const uint4 *p = (const uint4 *)nodes + 2 * (size_t)i;
     uint4 a = __ldg(p), b = __ldg(p + 1);
-    float ox = __uint_as_float(a.x & ~0xFFu), oy = __uint_as_float(a.y & ~0xFFu), oz = __uint_as_float(a.z & ~0xFFu);
-    float sx = __uint_as_float((a.x & 0xFFu) << 23), sy = __uint_as_float((a.y & 0xFFu) << 23),
-          sz = __uint_as_float((a.z & 0xFFu) << 23);
-    uint32_t q0 = a.w, q1 = b.x, q2 = b.y;
+    float ax = __uint_as_float((a.x & 0xFFu) << 23) * r.inv.x;
+    float ay = __uint_as_float((a.y & 0xFFu) << 23) * r.inv.y;
+    float az = __uint_as_float((a.z & 0xFFu) << 23) * r.inv.z;
+    float bx = fmaf(__uint_as_float(a.x & ~0xFFu), r.inv.x, -r.oinv.x);
+    float by = fmaf(__uint_as_float(a.y & ~0xFFu), r.inv.y, -r.oinv.y);
+    float bz = fmaf(__uint_as_float(a.z & ~0xFFu), r.inv.z, -r.oinv.z);
+    const uint32_t q0 = a.w, q1 = b.x, q2 = b.y;
 #define XTG_Q(w, k) ((float)(((w) >> (8 * (k))) & 0xFFu))
-    n.lx[0] = __fmaf_rn(XTG_Q(q0, 0), sx, ox);
-    n.ly[0] = __fmaf_rn(XTG_Q(q0, 1), sy, oy);
-    n.lz[0] = __fmaf_rn(XTG_Q(q0, 2), sz, oz);
-    n.hx[0] = __fmaf_rn(XTG_Q(q0, 3), sx, ox);
-    n.hy[0] = __fmaf_rn(XTG_Q(q1, 0), sy, oy);
-    n.hz[0] = __fmaf_rn(XTG_Q(q1, 1), sz, oz);
-    n.lx[1] = __fmaf_rn(XTG_Q(q1, 2), sx, ox);
-    n.ly[1] = __fmaf_rn(XTG_Q(q1, 3), sy, oy);
-    n.lz[1] = __fmaf_rn(XTG_Q(q2, 0), sz, oz);
-    n.hx[1] = __fmaf_rn(XTG_Q(q2, 1), sx, ox);
-    n.hy[1] = __fmaf_rn(XTG_Q(q2, 2), sy, oy);
-    n.hz[1] = __fmaf_rn(XTG_Q(q2, 3), sz, oz);
+    P.h0 = slab_t(fmaf(XTG_Q(q0, 0), ax, bx), fmaf(XTG_Q(q0, 3), ax, bx), fmaf(XTG_Q(q0, 1), ay, by),
+                  fmaf(XTG_Q(q1, 0), ay, by), fmaf(XTG_Q(q0, 2), az, bz), fmaf(XTG_Q(q1, 1), az, bz), tmin, tmax,
+                  XTG_TFAR_SCALE_Q8, P.t0);
+    P.h1 = slab_t(fmaf(XTG_Q(q1, 2), ax, bx), fmaf(XTG_Q(q2, 1), ax, bx), fmaf(XTG_Q(q1, 3), ay, by),
+                  fmaf(XTG_Q(q2, 2), ay, by), fmaf(XTG_Q(q2, 0), az, bz), fmaf(XTG_Q(q2, 3), az, bz), tmin, tmax,
+                  XTG_TFAR_SCALE_Q8, P.t1);
 #undef XTG_Q
-    n.ref[0] = (int32_t)b.z;
-    n.ref[1] = (int32_t)b.w;
+    P.c0 = (int32_t)b.z;
+    P.c1 = (int32_t)b.w;
 }
 
-struct HitRec {
-    float t;
-    uint32_t prim;
-    float u, v;
+// Per-lane view of the scene being traversed.
+struct SceneView {
+    const void *nodes;
+    const float4 *leaf;
+    const float4 *planes;
+    int32_t root, n_planes;
+    uint32_t plane_base;
 };
 
-// Closest hit in (tmin, tmax).  Returns false (and sets *overflow) only if the
-// traversal stack would overflow, which the builder's depth check excludes.
 template <int FMT>
-__device__ __forceinline__ void trace_closest(const DevScene &S, const RayPre &r, float tmin, float tmax,
-                                              HitRec &h, int *overflow, uint32_t *visits = nullptr,
-                                              uint32_t *tests = nullptr)
+__device__ __forceinline__ SceneView scene_view(const DevScene &S)
 {
-    h.t = INFINITY;
-    h.prim = 0xffffffffu;
-    h.u = h.v = 0.f;
-    int32_t stack[STACK_MAX];
-    int sp = 0;
-    int32_t ref = S.root;
-    uint32_t nv = 0, np = 0;
-    // A valid tree visits each node at most once per ray; the bound only turns
-    // a corrupted tree into an error instead of an endless loop.
-    for (uint32_t guard = 0;; ++guard) {
-        if (guard >= (1u << 22)) {
-            *overflow = 1;
-            break;
-        }
-        if (ref >= 0) {
-            Node2 n;
-            load_node<FMT>(S, ref, n);
-            ++nv;
-            float t0, t1;
-            bool h0 = slab(r, n.lx[0], n.hx[0], n.ly[0], n.hy[0], n.lz[0], n.hz[0], tmin, tmax, t0);
-            bool h1 = slab(r, n.lx[1], n.hx[1], n.ly[1], n.hy[1], n.lz[1], n.hz[1], tmin, tmax, t1);
-            if (h0 && h1) {
-                bool sw = t1 < t0;
-                if (sp >= STACK_MAX) {
-                    *overflow = 1;
-                    break;
-                }
-                stack[sp++] = sw ? n.ref[0] : n.ref[1];
-                ref = sw ? n.ref[1] : n.ref[0];
-                continue;
+    SceneView v;
+    v.nodes = FMT == XTGPU_NODES_Q8 ? (const void *)S.nodes8 : (const void *)S.nodes32;
+    v.leaf = S.leaf_prims;
+    v.planes = S.planes;
+    v.root = S.root;
+    v.n_planes = S.n_planes;
+    v.plane_base = (uint32_t)(S.n_tris + S.n_spheres);
+    return v;
+}
+
+// Tests the primitives of leaf `ref`; updates tmax / prim / barycentrics.
+__device__ __forceinline__ void leaf_test(const SceneView &V, int32_t ref, const RayPre &r, float tmin, float &tmax,
+                                          uint32_t &prim, float &bu, float &bv)
+{
+    uint32_t first = leaf_first(ref), cnt = leaf_count(ref);
+    for (uint32_t k = 0; k < cnt; ++k) {
+        const float4 *lp = V.leaf + 3 * (size_t)(first + k);
+        float4 a = __ldg(lp), b = __ldg(lp + 1);
+        uint32_t id = __float_as_uint(a.w);
+        if (id & SPHERE_BIT) {
+            if (hit_sphere(r, make_float3(a.x, a.y, a.z), b.x, tmin, tmax)) {
+                prim = id & ~SPHERE_BIT;
+                bu = bv = 0.f;
             }
-            if (h0) { ref = n.ref[0]; continue; }
-            if (h1) { ref = n.ref[1]; continue; }
-        } else if (ref != EMPTY_REF) {
-            uint32_t first = leaf_first(ref), cnt = leaf_count(ref);
-            np += cnt;
-            for (uint32_t k = 0; k < cnt; ++k) {
-                const float4 *lp = S.leaf_prims + 3 * (size_t)(first + k);
-                float4 a = __ldg(lp), b = __ldg(lp + 1);
-                uint32_t id = __float_as_uint(a.w);
-                if (id & SPHERE_BIT) {
-                    if (hit_sphere(r, make_float3(a.x, a.y, a.z), b.x, tmin, tmax)) {
-                        h.prim = id & ~SPHERE_BIT;
-                        h.u = h.v = 0.f;
-                    }
-                } else {
-                    float4 c = __ldg(lp + 2);
-                    float bu, bv;
-                    if (hit_triangle(r, make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z),
-                                     make_float3(c.x, c.y, c.z), tmin, tmax, bu, bv)) {
-                        h.prim = id;
-                        h.u = bu;
-                        h.v = bv;
-                    }
-                }
+        } else {
+            float4 c = __ldg(lp + 2);
+            float u, v;
+            if (hit_triangle(r, make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z), make_float3(c.x, c.y, c.z),
+                             tmin, tmax, u, v)) {
+                prim = id;
+                bu = u;
+                bv = v;
             }
         }
-        if (sp == 0) break;
-        ref = stack[--sp];
     }
-    for (int p = 0; p < S.n_planes; ++p) {
-        if (hit_plane(r, __ldg(S.planes + p), tmin, tmax)) {
-            h.prim = (uint32_t)(S.n_tris + S.n_spheres + p);
-            h.u = h.v = 0.f;
-        }
-    }
-    if (h.prim != 0xffffffffu) h.t = tmax;
-    if (visits) *visits = nv;
-    if (tests) *tests = np + (uint32_t)S.n_planes;
 }
 
 }  // namespace xtg

@@ -27,6 +27,7 @@ struct DevJob {
     int32_t x0, y0, rw, rh;          // rectangle rendered
     int32_t scene;                   // index in the scene table
     int32_t bounces;                 // extend passes this job needs
+    int32_t tile;                    // camera order: square pixel tiles of this edge (0 = rows)
     float4 *frame;                   // rw*rh RGBA accumulation buffer
     int64_t first;                   // first path id of the job in this wave
     int64_t count;                   // paths of the job in this wave

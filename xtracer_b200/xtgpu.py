@@ -91,6 +91,24 @@ class ServiceStats(C.Structure):
                 ("prim_tests", C.c_uint64)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("extend_variant", C.c_int32), ("extend_block", C.c_int32), ("extend_blocks_per_sm", C.c_int32),
+                ("tile", C.c_int32), ("wave_paths", C.c_int64), ("leaf_size", C.c_int32)]
+
+
+def get_tuning() -> "Tuning":
+    t = Tuning()
+    check(lib().xtgpu_get_tuning(C.byref(t)))
+    return t
+
+
+def set_tuning(**kw) -> None:
+    t = get_tuning()
+    for k, v in kw.items():
+        setattr(t, k, v)
+    check(lib().xtgpu_set_tuning(C.byref(t)))
+
+
 class JobDesc(C.Structure):
     _fields_ = [("scene", C.c_int32), ("integrator", C.c_int32), ("width", C.c_int32), ("height", C.c_int32),
                 ("spp", C.c_int32), ("rdepth", C.c_int32), ("ao_max_distance", C.c_float), ("seed", C.c_uint64)]
@@ -122,6 +140,8 @@ SIGNATURES = {
     "xtgpu_service_destroy": [C.c_void_p],
     "xtgpu_service_get_stats": [C.c_void_p, C.POINTER(ServiceStats)],
     "xtgpu_service_reset_stats": [C.c_void_p],
+    "xtgpu_get_tuning": [C.c_void_p],
+    "xtgpu_set_tuning": [C.c_void_p],
 }
 
 _lib = None
