@@ -173,6 +173,22 @@ XTGPU_API xtgpu_status xtgpu_render(xtgpu_scene *scene, const xtgpu_render_param
 XTGPU_API xtgpu_status xtgpu_render_host(xtgpu_scene *scene, const xtgpu_render_params *params, float *rgba_host,
                                uint64_t *rays_traced, void *stream);
 
+/* xtgpu_render for one rectangle without allocating any memory.  No
+ * counterpart in the reference.  For callers that cannot allocate device
+ * memory at render time: a render_tile on XTracer's OpenMP tile threads, where
+ * a cudaMalloc would synchronise the device and stall every other tile; a
+ * process that reserved its device memory at start-up under a fixed budget (or
+ * leaves it to another allocator); a render loop that must not meet an
+ * allocation failure mid-frame.  Scratch is one static device array of about
+ * 11.5 MB held by every GPU that loads the library; a call renders at most
+ * XTGPU_NOALLOC_MAX_PATHS paths (rectangle pixels x spp) and larger requests
+ * return XTGPU_ERR_LIMIT.  Calls that overlap on the GPU race on the shared
+ * array.  The first call on a device looks up the array's address; make it
+ * before any stream capture.  Output: rgba_dev as in xtgpu_render. */
+#define XTGPU_NOALLOC_MAX_PATHS 65536
+XTGPU_API xtgpu_status xtgpu_render_tile_noalloc(xtgpu_scene *scene, const xtgpu_render_params *params,
+                                                 float *rgba_dev, uint64_t *rays_traced, void *stream);
+
 /* ---------------------------------------------------------------------- */
 /* Render service.  Scenes stay resident; jobs are admitted while their
  * accumulation buffers fit the memory budget and a job slot is free; the rays of

@@ -887,6 +887,22 @@ void launch_extend_kernel(int fmt, bool multi, const DevScene &single, const Dev
 #undef XTG_LAUNCH
 }
 
+void enqueue_wave_raw(const WaveQueues &q, const DevJob *jobs, const DevScene *scenes, const DevScene &single,
+                      const int64_t *prefix, int bounces, int fmt, int sms, cudaStream_t s)
+{
+    const int gb = sms * 8;
+    k_camera<<<gb, 256, 0, s>>>(jobs, scenes, q);
+    int side = 0;
+    for (int b = 0; b < bounces; ++b) {
+        cudaMemsetAsync(q.ctl + 2, 0, sizeof(int32_t), s);
+        launch_extend_kernel(fmt, false, single, scenes, jobs, q, side, sms * tuning().extend_blocks_per_sm, s);
+        cudaMemsetAsync(q.ctl + (side ^ 1), 0, sizeof(int32_t), s);
+        k_shade<<<gb, 256, 0, s>>>(jobs, scenes, q, side);
+        side ^= 1;
+    }
+    k_accumulate<<<gb, 256, 0, s>>>(jobs, q.ctl, prefix, q.contrib);
+}
+
 void launch_extend(int fmt, const DevScene &S, const WaveQueues &q, int side, int blocks, cudaStream_t s)
 {
     launch_extend_kernel(fmt, false, S, nullptr, nullptr, q, side, blocks, s);

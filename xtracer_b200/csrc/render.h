@@ -49,6 +49,11 @@ int bounces_of(int integrator, int rdepth);
 xtgpu_tuning &tuning();
 void launch_extend_kernel(int fmt, bool multi, const DevScene &single, const DevScene *scenes, const DevJob *jobs,
                           const WaveQueues &q, int side, int blocks, cudaStream_t s);
+// One single-scene wave over caller-provided device buffers: no allocation and
+// no host synchronisation.  jobs/scenes/prefix and q.ctl must already hold the
+// wave (ctl[0] = ctl[5] = paths, ctl[4] = jobs, other counters zero).
+void enqueue_wave_raw(const WaveQueues &q, const DevJob *jobs, const DevScene *scenes, const DevScene &single,
+                      const int64_t *prefix, int bounces, int fmt, int sms, cudaStream_t s);
 // Closest hit of the q.ctl[side] rays of queue `side` (no job table needed).
 void launch_extend(int fmt, const DevScene &S, const WaveQueues &q, int side, int blocks, cudaStream_t s);
 

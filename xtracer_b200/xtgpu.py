@@ -130,6 +130,8 @@ SIGNATURES = {
     "xtgpu_trace_host": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p],
     "xtgpu_render": [C.c_void_p, C.POINTER(RenderParams), C.c_void_p, C.POINTER(C.c_uint64), C.c_void_p],
     "xtgpu_render_host": [C.c_void_p, C.POINTER(RenderParams), C.c_void_p, C.POINTER(C.c_uint64), C.c_void_p],
+    "xtgpu_render_tile_noalloc": [C.c_void_p, C.POINTER(RenderParams), C.c_void_p, C.POINTER(C.c_uint64),
+                                  C.c_void_p],
     "xtgpu_service_create": [C.POINTER(ServiceOpts), C.c_void_p, C.POINTER(C.c_void_p)],
     "xtgpu_service_add_scene": [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)],
     "xtgpu_service_submit": [C.c_void_p, C.POINTER(JobDesc), C.c_double, C.POINTER(C.c_int64)],
