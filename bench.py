@@ -52,48 +52,9 @@ def parse():
     return ap.parse_args()
 
 
-# ---------------------------------------------------------------------------
 def dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
-
-
-class Dist:
-    def __init__(self, world, use_cuda):
-        self.world = world
-        self.pg = None
-        if world > 1:
-            import datetime
-            import torch.distributed as dist
-            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-            dist.init_process_group("nccl" if use_cuda else "gloo", timeout=datetime.timedelta(seconds=120))
-            self.dist = dist
-
-    def barrier(self):
-        if self.world > 1:
-            self.dist.barrier()
-
-    def max(self, x):
-        if self.world == 1:
-            return x
-        import torch
-        t = torch.tensor([float(x)], device="cuda" if torch.cuda.is_available() else "cpu")
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum(self, x):
-        if self.world == 1:
-            return x
-        import torch
-        t = torch.tensor([float(x)], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
-        return float(t.item())
-
-    def close(self):
-        if self.world > 1:
-            self.dist.destroy_process_group()
+    from xtracer_b200 import replicas
+    return replicas.env()
 
 
 # ---------------------------------------------------------------------------
@@ -227,8 +188,8 @@ def cpu_reference_sample(scale, threads, budget_s=20.0):
         return None
     work = tempfile.mkdtemp(prefix="xtref")
     total_rays, total_s, parts = 0, 0.0, []
-    plan = [("spheres64", 256, 16, 64), ("spheres4096", 256, 4, 32), ("terrain10k", 256, 16, 64),
-            ("terrain50k", 256, 16, 64)]
+    plan = [("spheres64", 256, 16, 48), ("terrain10k", 256, 16, 48), ("terrain50k", 256, 16, 32),
+            ("spheres4096", 256, 4, 12)]
     for name, res, spp, crop in plan:
         spec = scenes.jobstream_scene(name, scale)
         scn = spec.write_scn(work)
@@ -240,7 +201,8 @@ def cpu_reference_sample(scale, threads, budget_s=20.0):
         total_rays += st["rays"]
         total_s += st["render_s"]
         parts.append("%s %dx%d crop of %d^2 x %d spp" % (name, crop, crop, res, spp))
-        if time.time() - t0 > budget_s:
+        budget_s -= time.time() - t0
+        if budget_s <= 0:
             break
     return {"value": total_rays / total_s / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "reference",
             "sample": "; ".join(parts) + " (pathtracer depth 4, IIntegrator::render timed, rays counted at "
@@ -291,12 +253,12 @@ def main():
     # (the legacy default stream cannot be captured into CUDA graphs)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    D = Dist(world, True)
-    from xtracer_b200 import scenes, xtgpu
+    from xtracer_b200 import replicas, scenes, xtgpu
     from xtracer_b200.service import Service
+    D = replicas.Group(world, "nccl")
 
     specs, gscenes = build_scenes(args.scale)
-    jobs = scenes.job_stream(args.stream_jobs, seed=4 + rank)
+    jobs = replicas.rank_stream(rank, args.stream_jobs)
     nslices = max(1, len(jobs) // args.jobs_per_step)
     slices = [jobs[i * args.jobs_per_step:(i + 1) * args.jobs_per_step] for i in range(nslices)]
     budget = 48 << 30
@@ -330,6 +292,7 @@ def main():
     t_max = D.max(dev_s)
     rays_all = D.sum(rays)
     value = rays_all / t_max / 1e6
+    lat_all = D.gather(lat)
 
     # roofline of the extend kernel over the timed region
     bpr = roofline_bytes_per_ray(specs, gscenes, xtgpu.NODES_Q8)
@@ -413,7 +376,7 @@ def main():
                        "cache": "inputs larger than L2 (resident scenes ~%.0f MB)" %
                                 (sum(s.device_bytes() for s in gscenes) / 1e6),
                        "wave_paths": 1 << 22, "node_format": "q8", "cuda_graphs": True},
-            "p50_ms": 1000 * pct(lat, 50), "p99_ms": 1000 * pct(lat, 99),
+            "p50_ms": 1000 * pct(lat_all, 50), "p99_ms": 1000 * pct(lat_all, 99),
             "latency_open_loop": latency, "plain": plain,
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 64 * len(timed[0]),
                     "d2h_bytes_per_step": d2h // max(1, len(timed))},
@@ -421,7 +384,9 @@ def main():
                          "frac": (achieved / peak) if achieved else None, "traffic": None,
                          "kernel": "k_extend (closest-hit traversal)", "peak_kind": peak_kind,
                          "extend_ms": st.extend_ms, "extend_launches": st.extend_launches,
-                         "bytes_per_ray": {b["scene"]: round(b["bytes_per_ray"], 1) for b in bpr}},
+                         "bytes_per_ray": {b["scene"]: round(b["bytes_per_ray"], 1) for b in bpr},
+                         "nodes_per_ray": {b["scene"]: round(b["nodes_per_ray"], 2) for b in bpr},
+                         "prims_per_ray": {b["scene"]: round(b["prims_per_ray"], 2) for b in bpr}},
             "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(st.kernel_launches),
             "rays": rays_all,
         }

@@ -148,6 +148,12 @@ typedef struct {
  * picks the BVH to traverse (it must have been built). */
 XTGPU_API xtgpu_status xtgpu_trace(xtgpu_scene *scene, int64_t n, const void *org_tmin_dev, const void *dir_tmax_dev,
                          xtgpu_hit *hits_dev, int32_t node_format, void *stream);
+/* xtgpu_trace with a counting traversal: also returns the BVH nodes visited
+ * (counts[0]) and primitives tested (counts[1]) summed over the batch, the
+ * per-ray figures behind the extend kernel's algorithmic bytes. */
+XTGPU_API xtgpu_status xtgpu_trace_counts(xtgpu_scene *scene, int64_t n, const void *org_tmin_dev,
+                                          const void *dir_tmax_dev, xtgpu_hit *hits_dev, int32_t node_format,
+                                          uint64_t counts[2], void *stream);
 /* The same with host buffers (pinned or pageable), copies included. */
 XTGPU_API xtgpu_status xtgpu_trace_host(xtgpu_scene *scene, int64_t n, const float *org_tmin, const float *dir_tmax,
                               xtgpu_hit *hits, int32_t node_format, void *stream);
@@ -208,6 +214,8 @@ typedef struct {
                                       its device buffer at once (frees budget early) */
     int32_t time_kernels;          /* 1 = time every extend launch with CUDA events */
     int32_t count_visits;          /* 1 = count BVH nodes visited / primitives tested */
+    int32_t policy;                /* wave planning: 0 = fewest remaining paths first,
+                                      1 = equal share per running job */
 } xtgpu_service_opts;
 
 typedef struct {
@@ -254,12 +262,17 @@ XTGPU_API xtgpu_status xtgpu_service_reset_stats(xtgpu_service *svc);
 /* ---------------------------------------------------------------------- */
 /* Launch configuration of the wavefront kernels (process-wide).            */
 typedef struct {
-    int32_t extend_variant;        /* 0 = warp-batched ray fetch, 1 = per-lane refill */
+    int32_t extend_variant;        /* 0 = warp-batched ray fetch, 1 = lanes refilled when
+                                      refill_threshold of them are idle */
     int32_t extend_block;          /* threads per block of the extend kernel (32..256) */
     int32_t extend_blocks_per_sm;  /* resident extend blocks per SM, in 128-thread units */
     int32_t tile;                  /* camera ray order: square pixel tiles of this edge (0 = rows) */
     int64_t wave_paths;            /* paths per wave of xtgpu_render */
     int32_t leaf_size;             /* default primitives per BVH leaf */
+    int32_t node_layout;           /* BVH node order: 0 = Karras index, 1 = depth-first */
+    int32_t refill_threshold;      /* variant 1: idle lanes (1..32) that trigger a refill */
+    int32_t extend_min_blocks;     /* variant 0: 0, or 8/10/12/16 resident 128-thread blocks per SM
+                                      requested from the compiler (caps registers) */
 } xtgpu_tuning;
 XTGPU_API xtgpu_status xtgpu_get_tuning(xtgpu_tuning *t);
 XTGPU_API xtgpu_status xtgpu_set_tuning(const xtgpu_tuning *t);

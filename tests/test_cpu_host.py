@@ -57,7 +57,7 @@ def test_invalid_arguments_are_rejected_without_device_work():
     assert L.xtgpu_render(None, None, None, None, None) == 1
     assert L.xtgpu_trace(None, 4, None, None, None, 0, None) == 1
     assert L.xtgpu_service_create(None, None, C.byref(out)) == 1
-    o = xtgpu.ServiceOpts(1 << 20, 0, 0, 0, 1, 1, 0, 0, 0)   # max_jobs 0
+    o = xtgpu.ServiceOpts(1 << 20, 0, 0, 0, 1, 1, 0, 0, 0, 0)   # max_jobs 0
     assert L.xtgpu_service_create(C.byref(o), None, C.byref(out)) == 1
     assert L.xtgpu_scene_destroy(None) == 0
 

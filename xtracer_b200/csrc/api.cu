@@ -124,7 +124,10 @@ xtgpu_status xtgpu_set_tuning(const xtgpu_tuning *t)
     if (!t || t->extend_variant < 0 || t->extend_variant > 1 || t->extend_block < 32 || t->extend_block > 256 ||
         (t->extend_block & 31) || t->extend_blocks_per_sm < 1 || t->extend_blocks_per_sm > 64 || t->tile < 0 ||
         t->tile > 256 || t->wave_paths < 1024 || t->wave_paths > (1ll << 26) || t->leaf_size < 1 ||
-        t->leaf_size > MAX_LEAF) {
+        t->leaf_size > MAX_LEAF || t->node_layout < 0 || t->node_layout > 1 || t->refill_threshold < 1 ||
+        t->refill_threshold > 32 ||
+        !(t->extend_min_blocks == 0 || t->extend_min_blocks == 8 || t->extend_min_blocks == 10 ||
+          t->extend_min_blocks == 12 || t->extend_min_blocks == 16)) {
         set_error("xtgpu_set_tuning: value out of range");
         return XTGPU_ERR_INVALID;
     }
@@ -272,7 +275,7 @@ xtgpu_status xtgpu_bvh_build(xtgpu_scene *sc, const xtgpu_bvh_opts *opts, void *
         set_error("xtgpu_bvh_build: leaf_size out of range");
         return XTGPU_ERR_INVALID;
     }
-    return build_bvh(sc, fmt, leaf, (cudaStream_t)stream);
+    return build_bvh(sc, fmt, leaf, tuning().node_layout, (cudaStream_t)stream);
 }
 
 xtgpu_status xtgpu_scene_destroy(xtgpu_scene *sc)
@@ -339,8 +342,27 @@ static xtgpu_status check_format(const xtgpu_scene *sc, int32_t fmt)
     return XTGPU_ERR_STATE;
 }
 
+static xtgpu_status trace_impl(xtgpu_scene *sc, int64_t n, const void *org, const void *dir, xtgpu_hit *hits,
+                               int32_t fmt, uint64_t *counts, void *stream);
+
 xtgpu_status xtgpu_trace(xtgpu_scene *sc, int64_t n, const void *org, const void *dir, xtgpu_hit *hits, int32_t fmt,
                          void *stream)
+{
+    return trace_impl(sc, n, org, dir, hits, fmt, nullptr, stream);
+}
+
+xtgpu_status xtgpu_trace_counts(xtgpu_scene *sc, int64_t n, const void *org, const void *dir, xtgpu_hit *hits,
+                                int32_t fmt, uint64_t counts[2], void *stream)
+{
+    if (!counts) {
+        set_error("xtgpu_trace_counts: NULL counts");
+        return XTGPU_ERR_INVALID;
+    }
+    return trace_impl(sc, n, org, dir, hits, fmt, counts, stream);
+}
+
+static xtgpu_status trace_impl(xtgpu_scene *sc, int64_t n, const void *org, const void *dir, xtgpu_hit *hits,
+                               int32_t fmt, uint64_t *counts, void *stream)
 {
     if (!sc || n < 0 || (n && (!org || !dir || !hits))) {
         set_error("xtgpu_trace: bad argument");
@@ -350,7 +372,9 @@ xtgpu_status xtgpu_trace(xtgpu_scene *sc, int64_t n, const void *org, const void
     if (n == 0) return XTGPU_OK;
     cudaStream_t s = (cudaStream_t)stream;
     int32_t *ctl = nullptr;
-    XTG_CUDA(cudaMallocAsync((void **)&ctl, 64, s));
+    XTG_CUDA(cudaMallocAsync((void **)&ctl, 64 + 16, s));
+    unsigned long long *stats = counts ? (unsigned long long *)((char *)ctl + 64) : nullptr;
+    if (stats) XTG_CUDA(cudaMemsetAsync(stats, 0, 16, s));
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -363,6 +387,7 @@ xtgpu_status xtgpu_trace(xtgpu_scene *sc, int64_t n, const void *org, const void
         q.hit = hits + base;
         q.ctl = ctl;
         q.rays = (unsigned long long *)((char *)ctl + 32);
+        q.stats = stats;
         int32_t init[4] = {cnt, 0, 0, 0};
         XTG_CUDA(cudaMemcpyAsync(ctl, init, sizeof(init), cudaMemcpyHostToDevice, s));
         launch_extend(fmt, sc->dev, q, 0, sms * tuning().extend_blocks_per_sm, s);
@@ -371,6 +396,12 @@ xtgpu_status xtgpu_trace(xtgpu_scene *sc, int64_t n, const void *org, const void
         XTG_CUDA(cudaMemcpyAsync(back, ctl, sizeof(back), cudaMemcpyDeviceToHost, s));
         XTG_CUDA(cudaStreamSynchronize(s));
         overflow |= back[3];
+    }
+    if (stats) {
+        unsigned long long c[2];
+        XTG_CUDA(cudaMemcpy(c, stats, 16, cudaMemcpyDeviceToHost));
+        counts[0] = c[0];
+        counts[1] = c[1];
     }
     cudaFreeAsync(ctl, s);
     if (overflow) {

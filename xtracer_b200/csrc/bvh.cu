@@ -300,24 +300,46 @@ __global__ void k_refit(int n, const int32_t *left, const int32_t *right, const 
     }
 }
 
+// Depth-first position of every inner node: the left child follows its parent,
+// the right child follows the parent's whole left subtree (g - lo inner nodes).
+// Each node climbs to the root summing those offsets.
+__global__ void k_dfs_pos(int n, const int32_t *left, const int32_t *rlo, const int32_t *gam,
+                          const int32_t *parent_int, int32_t *pos, uint32_t *err)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int32_t p = 0, x = i;
+    for (int guard = 0; x != 0; ++guard) {
+        int32_t par = parent_int[x];
+        if (guard > 256 || par < 0 || par >= n - 1) {
+            atomicOr(err, 4u);
+            return;
+        }
+        p += left[par] == x ? 1 : 1 + (gam[par] - rlo[par]);
+        x = par;
+    }
+    pos[i] = p;
+}
+
 __global__ void k_emit(int n, int leaf_size, const int32_t *left, const int32_t *right, const int32_t *rlo,
                        const int32_t *rhi, const int32_t *gam, const float4 *nlo, const float4 *nhi,
-                       const float4 *plo, const float4 *phi, const uint32_t *order, float4 *nodes)
+                       const float4 *plo, const float4 *phi, const uint32_t *order, const int32_t *pos, float4 *nodes)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
     int g = gam[i];
     int32_t l = left[i], r = right[i];
     int nl = g - rlo[i] + 1, nr = rhi[i] - g;
-    int32_t refl = nl <= leaf_size ? leaf_ref((uint32_t)rlo[i], (uint32_t)nl) : l;
-    int32_t refr = nr <= leaf_size ? leaf_ref((uint32_t)(g + 1), (uint32_t)nr) : r;
+    int32_t refl = nl <= leaf_size ? leaf_ref((uint32_t)rlo[i], (uint32_t)nl) : (pos ? pos[l] : l);
+    int32_t refr = nr <= leaf_size ? leaf_ref((uint32_t)(g + 1), (uint32_t)nr) : (pos ? pos[r] : r);
+    const int o = pos ? pos[i] : i;
     float4 alo, ahi, blo, bhi;
     child_box(l, nlo, nhi, plo, phi, order, alo, ahi);
     child_box(r, nlo, nhi, plo, phi, order, blo, bhi);
-    nodes[4 * i + 0] = make_float4(alo.x, ahi.x, alo.y, ahi.y);
-    nodes[4 * i + 1] = make_float4(blo.x, bhi.x, blo.y, bhi.y);
-    nodes[4 * i + 2] = make_float4(alo.z, ahi.z, blo.z, bhi.z);
-    nodes[4 * i + 3] = make_float4(__int_as_float(refl), __int_as_float(refr), 0.f, 0.f);
+    nodes[4 * o + 0] = make_float4(alo.x, ahi.x, alo.y, ahi.y);
+    nodes[4 * o + 1] = make_float4(blo.x, bhi.x, blo.y, bhi.y);
+    nodes[4 * o + 2] = make_float4(alo.z, ahi.z, blo.z, bhi.z);
+    nodes[4 * o + 3] = make_float4(__int_as_float(refl), __int_as_float(refr), 0.f, 0.f);
 }
 
 // Every child reference in range and every leaf range inside the primitive
@@ -465,7 +487,7 @@ inline int blocks(int64_t n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
 
-xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, cudaStream_t s)
+xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, int layout, cudaStream_t s)
 {
     DevScene &S = sc->dev;
     const int n = S.n_tris + S.n_spheres;
@@ -478,7 +500,7 @@ xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, cudaStre
 
     // Morton order, keys and topology are the same for both node formats: build
     // them once and keep them.
-    bool need_topology = !(sc->built32 || sc->built8) || sc->leaf_size != leaf_size;
+    bool need_topology = !(sc->built32 || sc->built8) || sc->leaf_size != leaf_size || sc->layout != layout;
     if (need_topology) {
         sc->built32 = sc->built8 = false;
         dfree(sc->nodes32);
@@ -489,6 +511,7 @@ xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, cudaStre
         dfree(sc->left);
         dfree(sc->right);
         sc->leaf_size = leaf_size;
+        sc->layout = layout;
         if (n == 0) {
             S.root = EMPTY_REF;
             sc->depth = 0;
@@ -551,8 +574,13 @@ xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, cudaStre
                 k_refit<<<blocks(n, 256), 256, 0, s>>>(n, left, right, pint, pleaf, plo, phi, vals, nlo, nhi, height,
                                                        flags);
                 XTG_TRY(dalloc(sc->nodes32, sizeof(float4) * 4 * (size_t)ni, s));
+                int32_t *pos = nullptr;
+                if (layout == 1) {
+                    XTG_CUDA(tmp.get(&pos, ni));
+                    k_dfs_pos<<<blocks(ni, 256), 256, 0, s>>>(n, left, rlo, gam, pint, pos, flags + ni + 1);
+                }
                 k_emit<<<blocks(ni, 256), 256, 0, s>>>(n, leaf_size, left, right, rlo, rhi, gam, nlo, nhi, plo, phi,
-                                                       vals, (float4 *)sc->nodes32.p);
+                                                       vals, pos, (float4 *)sc->nodes32.p);
                 k_validate<<<blocks(ni, 256), 256, 0, s>>>(n, (const float4 *)sc->nodes32.p, flags + ni + 1);
                 int32_t h = 0;
                 uint32_t errs[2] = {0, 0};

@@ -253,14 +253,18 @@ __global__ void k_camera(const DevJob *__restrict__ jobs, const DevScene *__rest
     }
 }
 
-// Persistent extend.  Every lane holds one ray; a lane that finishes takes the
-// next queued ray at once (warp-aggregated fetch), so warps stay full while
-// long rays are still traversing.  Inner nodes are walked until the lane
-// reaches a leaf (while-while); stack entries keep their entry distance so a
-// popped subtree beyond the current closest hit is skipped without a fetch.
+// Persistent extend with refill: one node or one leaf per lane per iteration;
+// when at least `refill` lanes of the warp have finished their rays they take
+// new ones from the queue together (Aila and Laine, "Understanding the
+// Efficiency of Ray Traversal on GPUs", HPG 2009: dynamic ray fetch), so long
+// rays do not hold a mostly idle warp.
+// "pop the next stack entry": a leaf ref of count 0 that no build produces
+constexpr int32_t POP_REF = ~(1 << LEAF_BITS);
+
 template <int FMT, bool MULTI>
 __global__ void __launch_bounds__(256) k_extend_refill(DevScene S1, const DevScene *__restrict__ scenes,
-                                                       const DevJob *__restrict__ jobs, WaveQueues q, int side)
+                                                       const DevJob *__restrict__ jobs, WaveQueues q, int side,
+                                                       int refill)
 {
     const int n = q.ctl[side];
     const int lane = threadIdx.x & 31;
@@ -276,10 +280,10 @@ __global__ void __launch_bounds__(256) k_extend_refill(DevScene S1, const DevSce
     int2 stack[STACK_MAX];
     bool active = false, exhausted = false;
     while (true) {
-        // refill finished lanes from the queue
         const bool want = !active && !exhausted;
         const unsigned m = __ballot_sync(0xffffffffu, want);
-        if (m) {
+        const unsigned busy = __ballot_sync(0xffffffffu, active);
+        if (m && (__popc(m) >= refill || busy == 0u)) {
             const int leader = __ffs(m) - 1;
             int base = 0;
             if (lane == leader) base = atomicAdd(&q.ctl[2], __popc(m));
@@ -305,21 +309,17 @@ __global__ void __launch_bounds__(256) k_extend_refill(DevScene S1, const DevSce
                 }
             }
             if (q.job_rays) {
-                // rays per job: one atomic per group of lanes of the same job
                 const unsigned peers = __match_any_sync(0xffffffffu, jb);
                 if (jb != 0xffffffffu && (peers & lt) == 0u) atomicAdd(&q.job_rays[jb], (unsigned long long)__popc(peers));
             }
         }
-        if (!__any_sync(0xffffffffu, active)) break;
+        if (!__any_sync(0xffffffffu, active || !exhausted)) break;
         if (!active) continue;
         bool done = false;
-        // inner nodes until a leaf (or the end of the ray)
-        while (ref >= 0) {
-            if (++guard > (1u << 22)) {   // corrupted tree: report, never loop forever
-                q.ctl[3] = 1;
-                done = true;
-                break;
-            }
+        if (++guard > (1u << 22)) {   // corrupted tree: report, never loop forever
+            q.ctl[3] = 1;
+            done = true;
+        } else if (ref >= 0) {
             Pair P;
             node_pair<FMT>(V.nodes, ref, r, tmin, tmax, P);
             ++nv;
@@ -328,25 +328,25 @@ __global__ void __launch_bounds__(256) k_extend_refill(DevScene S1, const DevSce
                 if (sp >= STACK_MAX) {
                     q.ctl[3] = 1;
                     done = true;
-                    break;
+                } else {
+                    stack[sp++] = make_int2(sw ? P.c0 : P.c1, __float_as_int(sw ? P.t0 : P.t1));
+                    ref = sw ? P.c1 : P.c0;
                 }
-                stack[sp++] = make_int2(sw ? P.c0 : P.c1, __float_as_int(sw ? P.t0 : P.t1));
-                ref = sw ? P.c1 : P.c0;
             } else if (P.h0) {
                 ref = P.c0;
             } else if (P.h1) {
                 ref = P.c1;
             } else {
-                ref = EMPTY_REF;   // nothing here: fall through to the pop below
-                break;
+                ref = POP_REF;
             }
-        }
-        if (!done) {
-            if (ref != EMPTY_REF) {
+        } else {
+            if (leaf_count(ref) > 0) {
                 np += leaf_count(ref);
                 leaf_test(V, ref, r, tmin, tmax, prim, bu, bv);
             }
-            // next subtree still in front of the closest hit, or the end
+            ref = POP_REF;
+        }
+        if (!done && ref == POP_REF) {
             done = true;
             while (sp > 0) {
                 const int2 e = stack[--sp];
@@ -433,10 +433,13 @@ __device__ __forceinline__ void trace_ray(const SceneView &V, const RayPre &r, f
 }
 
 // Persistent extend, warp-batched: each warp takes the next 32 queued rays and
-// every lane runs its ray to the end.
-template <int FMT, bool MULTI>
-__global__ void __launch_bounds__(256) k_extend_batch(DevScene S1, const DevScene *__restrict__ scenes,
-                                                      const DevJob *__restrict__ jobs, WaveQueues q, int side)
+// every lane runs its ray to the end.  MINB > 0 asks the compiler for at least
+// MINB resident 128-thread blocks per SM (fewer registers, more warps to hide
+// the latency of the dependent node loads).
+template <int FMT, bool MULTI, int MINB>
+__global__ void __launch_bounds__(MINB > 0 ? 128 : 256, MINB > 0 ? MINB : 1)
+    k_extend_batch(DevScene S1, const DevScene *__restrict__ scenes, const DevJob *__restrict__ jobs, WaveQueues q,
+                   int side)
 {
     const int n = q.ctl[side];
     const int lane = threadIdx.x & 31;
@@ -752,8 +755,14 @@ xtgpu_status WaveRunner::set_scenes(const DevScene *scenes, int n, cudaStream_t 
 }
 
 // Enqueues the kernels of one wave (no host synchronisation inside).
-void WaveRunner::enqueue(int njobs, int64_t total, int bounces, int fmt, bool multi, cudaStream_t s)
+void WaveRunner::enqueue(int njobs, int64_t total, int bounces, int fmt, bool multi, cudaStream_t s, bool capturing)
 {
+    // inside a capture the events become external event-record nodes that
+    // record on every replay; outside, plain records
+    auto rec = [&](cudaEvent_t e) {
+        if (capturing) cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+        else cudaEventRecord(e, s);
+    };
     (void)njobs;
     (void)total;
     const DevJob *jobs = (const DevJob *)jobbuf.p;
@@ -764,9 +773,9 @@ void WaveRunner::enqueue(int njobs, int64_t total, int bounces, int fmt, bool mu
     for (int b = 0; b < bounces; ++b) {
         cudaMemsetAsync(q.ctl + 2, 0, sizeof(int32_t), s);
         int eb = sms * tuning().extend_blocks_per_sm;
-        if (time_extend && b < MAX_TIMED) cudaEventRecordWithFlags(ev[2 * b], s, cudaEventRecordExternal);
+        if (time_extend && b < MAX_TIMED) rec(ev[2 * b]);
         launch_extend_kernel(fmt, multi, single, scenes, jobs, q, side, eb, s);
-        if (time_extend && b < MAX_TIMED) cudaEventRecordWithFlags(ev[2 * b + 1], s, cudaEventRecordExternal);
+        if (time_extend && b < MAX_TIMED) rec(ev[2 * b + 1]);
         cudaMemsetAsync(q.ctl + (side ^ 1), 0, sizeof(int32_t), s);
         k_shade<<<gb, 256, 0, s>>>(jobs, scenes, q, side);
         side ^= 1;
@@ -832,7 +841,7 @@ xtgpu_status WaveRunner::run_wave(const std::vector<DevJob> &jobs, int bounces, 
         if (it == graphs.end()) {
             cudaGraph_t g;
             XTG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-            enqueue(nj, total, bounces, fmt, multi, s);
+            enqueue(nj, total, bounces, fmt, multi, s, true);
             XTG_CUDA(cudaStreamEndCapture(s, &g));
             cudaGraphExec_t ex;
             XTG_CUDA(cudaGraphInstantiate(&ex, g, 0));
@@ -845,7 +854,7 @@ xtgpu_status WaveRunner::run_wave(const std::vector<DevJob> &jobs, int bounces, 
         }
         XTG_CUDA(cudaGraphLaunch(it->second, s));
     } else {
-        enqueue(nj, total, bounces, fmt, multi, s);
+        enqueue(nj, total, bounces, fmt, multi, s, false);
     }
     launches += 2 + 2 * bounces;   // camera, bounces x (extend, shade), accumulate
     last_bounces = bounces;
@@ -864,10 +873,11 @@ xtgpu_status WaveRunner::read_ctl(int32_t *overflow, unsigned long long *rays, c
 }
 
 // Process-wide launch configuration (xtgpu_set_tuning / xtgpu_autotune).
-// Defaults from a sweep on a B200 (variant x leaf x node format x launch shape x
-// tile over terrain, hairball and sphere scenes): warp-batched fetch, one
-// primitive per leaf, 8x8 pixel tiles; the launch shape barely matters.
-static xtgpu_tuning g_tuning = {0, 128, 12, 8, 1ll << 22, 1};
+// Defaults from sweeps on a B200 (variant x leaf x node format x launch shape x
+// tile x register cap over terrain, hairball and sphere scenes): warp-batched
+// fetch, one primitive per leaf, depth-first node order, 8x8 pixel tiles, and
+// 64 registers (8 resident 128-thread blocks per SM).
+static xtgpu_tuning g_tuning = {0, 128, 8, 8, 1ll << 22, 1, 1, 8, 8};
 xtgpu_tuning &tuning() { return g_tuning; }
 
 void launch_extend_kernel(int fmt, bool multi, const DevScene &single, const DevScene *scenes, const DevJob *jobs,
@@ -877,14 +887,34 @@ void launch_extend_kernel(int fmt, bool multi, const DevScene &single, const Dev
     const int tb = T.extend_block;
     const int nb = std::max(1, blocks * 128 / tb);   // same resident thread count for any block size
 #define XTG_LAUNCH(K, F, M) K<F, M><<<nb, tb, 0, s>>>(single, scenes, jobs, q, side)
+#define XTG_LAUNCH_R(K, F, M) K<F, M><<<nb, tb, 0, s>>>(single, scenes, jobs, q, side, T.refill_threshold)
     if (T.extend_variant == 1) {
-        if (fmt == XTGPU_NODES_Q8) { if (multi) XTG_LAUNCH(k_extend_refill, XTGPU_NODES_Q8, true); else XTG_LAUNCH(k_extend_refill, XTGPU_NODES_Q8, false); }
-        else { if (multi) XTG_LAUNCH(k_extend_refill, XTGPU_NODES_FP32, true); else XTG_LAUNCH(k_extend_refill, XTGPU_NODES_FP32, false); }
-    } else {
-        if (fmt == XTGPU_NODES_Q8) { if (multi) XTG_LAUNCH(k_extend_batch, XTGPU_NODES_Q8, true); else XTG_LAUNCH(k_extend_batch, XTGPU_NODES_Q8, false); }
-        else { if (multi) XTG_LAUNCH(k_extend_batch, XTGPU_NODES_FP32, true); else XTG_LAUNCH(k_extend_batch, XTGPU_NODES_FP32, false); }
+        if (fmt == XTGPU_NODES_Q8) { if (multi) XTG_LAUNCH_R(k_extend_refill, XTGPU_NODES_Q8, true); else XTG_LAUNCH_R(k_extend_refill, XTGPU_NODES_Q8, false); }
+        else { if (multi) XTG_LAUNCH_R(k_extend_refill, XTGPU_NODES_FP32, true); else XTG_LAUNCH_R(k_extend_refill, XTGPU_NODES_FP32, false); }
+        return;
     }
+    // register-capped instantiations run with 128-thread blocks
+#define XTG_B(MB)                                                                                      \
+    do {                                                                                               \
+        const int tbb = MB > 0 ? 128 : tb, nbb = MB > 0 ? std::max(1, blocks) : nb;                 \
+        if (fmt == XTGPU_NODES_Q8) {                                                                   \
+            if (multi) k_extend_batch<XTGPU_NODES_Q8, true, MB><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side);   \
+            else k_extend_batch<XTGPU_NODES_Q8, false, MB><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side);       \
+        } else {                                                                                       \
+            if (multi) k_extend_batch<XTGPU_NODES_FP32, true, MB><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side); \
+            else k_extend_batch<XTGPU_NODES_FP32, false, MB><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side);     \
+        }                                                                                              \
+    } while (0)
+    switch (T.extend_min_blocks) {
+    case 8: XTG_B(8); break;
+    case 10: XTG_B(10); break;
+    case 12: XTG_B(12); break;
+    case 16: XTG_B(16); break;
+    default: XTG_B(0); break;
+    }
+#undef XTG_B
 #undef XTG_LAUNCH
+#undef XTG_LAUNCH_R
 }
 
 void enqueue_wave_raw(const WaveQueues &q, const DevJob *jobs, const DevScene *scenes, const DevScene &single,

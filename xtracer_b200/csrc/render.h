@@ -42,7 +42,7 @@ struct WaveRunner {
     xtgpu_status read_ctl(int32_t *overflow, unsigned long long *rays, cudaStream_t s);
     // per-job ray counts of the last wave (requires enable_job_rays)
     void enable_job_rays(bool on) { job_rays_enabled = on; q.job_rays = on ? (unsigned long long *)jobraysbuf.p : nullptr; }
-    void enqueue(int njobs, int64_t total, int bounces, int fmt, bool multi, cudaStream_t s);
+    void enqueue(int njobs, int64_t total, int bounces, int fmt, bool multi, cudaStream_t s, bool capturing);
 };
 
 int bounces_of(int integrator, int rdepth);

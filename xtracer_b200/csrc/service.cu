@@ -90,6 +90,17 @@ xtgpu_status xtgpu_service_create(const xtgpu_service_opts *opts, void *stream, 
         set_error("xtgpu_service_create: bad options");
         return XTGPU_ERR_INVALID;
     }
+    // Frames come and go with every job: keep freed pool memory cached instead
+    // of returning it to the driver at each synchronisation (the default), so
+    // admission does not remap memory for every job.
+    {
+        int dev = 0;
+        cudaMemPool_t pool;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     xtgpu_service *v = new xtgpu_service();
     v->o = *opts;
     v->s = (cudaStream_t)stream;
@@ -211,16 +222,27 @@ xtgpu_status xtgpu_service_run(xtgpu_service *v, double max_seconds)
         int n = (int)v->active.size();
         std::vector<int> order(n);
         for (int k = 0; k < n; ++k) order[k] = k;
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-            const SvcJob &A = v->jobs[v->active[a]], &B = v->jobs[v->active[b]];
-            return (A.paths - A.done) < (B.paths - B.done);
-        });
         std::vector<int64_t> take(n, 0);
+        if (v->o.policy == 1) {
+            // equal share per running job, then the rest in admission order
+            const int64_t share = std::max<int64_t>(1, cap / n);
+            for (int k = 0; k < n && left > 0; ++k) {
+                SvcJob &J = v->jobs[v->active[k]];
+                take[k] = std::min<int64_t>({share, J.paths - J.done, left});
+                left -= take[k];
+            }
+        } else {
+            std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+                const SvcJob &A = v->jobs[v->active[a]], &B = v->jobs[v->active[b]];
+                return (A.paths - A.done) < (B.paths - B.done);
+            });
+        }
         for (int k : order) {
             if (left <= 0) break;
             SvcJob &J = v->jobs[v->active[k]];
-            take[k] = std::min<int64_t>(J.paths - J.done, left);
-            left -= take[k];
+            int64_t more = std::min<int64_t>(J.paths - J.done - take[k], left);
+            take[k] += more;
+            left -= more;
         }
         int bounces = 0;
         for (int k = 0; k < n; ++k) {

@@ -84,6 +84,7 @@ struct xtgpu_scene {
     int64_t n_prims = 0;
     int32_t depth = 0;
     int32_t leaf_size = 2;
+    int32_t layout = 0;
     int32_t last_format = XTGPU_NODES_FP32;
     bool built32 = false, built8 = false;
     int device = 0;
@@ -113,7 +114,7 @@ xtgpu_status dalloc(HostBuf &b, size_t bytes, cudaStream_t s);
 void dfree(HostBuf &b);
 
 // BVH build (bvh.cu)
-xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, cudaStream_t s);
+xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, int layout, cudaStream_t s);
 
 // Ray/primitive batches (trace.cu)
 struct RayQueue {

@@ -15,9 +15,9 @@ class Service:
     def __init__(self, scenes, node_format: int = xtgpu.NODES_FP32, wave_paths: int = 0, use_graphs: bool = True,
                  merge_jobs: bool = True, memory_budget: int = 48 << 30, max_jobs: int = 512,
                  host_results: bool = False, time_kernels: bool = False, count_visits: bool = False,
-                 stream=None):
+                 policy: int = 0, stream=None):
         o = xtgpu.ServiceOpts(memory_budget, max_jobs, wave_paths, node_format, int(use_graphs), int(merge_jobs),
-                              int(host_results), int(time_kernels), int(count_visits))
+                              int(host_results), int(time_kernels), int(count_visits), policy)
         h = C.c_void_p()
         check(lib().xtgpu_service_create(C.byref(o), xtgpu.stream_handle(stream), C.byref(h)))
         self.handle = h

@@ -82,7 +82,8 @@ class RenderParams(C.Structure):
 class ServiceOpts(C.Structure):
     _fields_ = [("memory_budget_bytes", C.c_uint64), ("max_jobs", C.c_int32), ("wave_paths", C.c_int64),
                 ("node_format", C.c_int32), ("use_graphs", C.c_int32), ("merge_jobs", C.c_int32),
-                ("host_results", C.c_int32), ("time_kernels", C.c_int32), ("count_visits", C.c_int32)]
+                ("host_results", C.c_int32), ("time_kernels", C.c_int32), ("count_visits", C.c_int32),
+                ("policy", C.c_int32)]
 
 
 class ServiceStats(C.Structure):
@@ -93,7 +94,8 @@ class ServiceStats(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("extend_variant", C.c_int32), ("extend_block", C.c_int32), ("extend_blocks_per_sm", C.c_int32),
-                ("tile", C.c_int32), ("wave_paths", C.c_int64), ("leaf_size", C.c_int32)]
+                ("tile", C.c_int32), ("wave_paths", C.c_int64), ("leaf_size", C.c_int32),
+                ("node_layout", C.c_int32), ("refill_threshold", C.c_int32), ("extend_min_blocks", C.c_int32)]
 
 
 def get_tuning() -> "Tuning":
@@ -128,6 +130,8 @@ SIGNATURES = {
     "xtgpu_bvh_export": [C.c_void_p, C.POINTER(BvhInfo), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
     "xtgpu_trace": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p],
     "xtgpu_trace_host": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p],
+    "xtgpu_trace_counts": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                           C.c_void_p],
     "xtgpu_render": [C.c_void_p, C.POINTER(RenderParams), C.c_void_p, C.POINTER(C.c_uint64), C.c_void_p],
     "xtgpu_render_host": [C.c_void_p, C.POINTER(RenderParams), C.c_void_p, C.POINTER(C.c_uint64), C.c_void_p],
     "xtgpu_render_tile_noalloc": [C.c_void_p, C.POINTER(RenderParams), C.c_void_p, C.POINTER(C.c_uint64),
