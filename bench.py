@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-latency", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     return ap.parse_args()
 
 
@@ -117,14 +118,22 @@ def measured_peaks():
 
 
 # ---------------------------------------------------------------------------
-def build_scenes(scale):
+def build_scenes(scale, autotune=False):
+    """The resident scenes; with autotune, each scene's leaf size, stack, tile,
+    register cap and wave size are picked by xtgpu_autotune (Q8 nodes)."""
     from xtracer_b200 import scenes, xtgpu
-    out, specs = [], []
+    out, specs, tunes = [], [], {}
     for name, _ in scenes.JOBSTREAM_SCENES:
         spec = scenes.jobstream_scene(name, scale)
         specs.append(spec)
-        out.append(xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8)))
-    return specs, out
+        sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8))
+        if autotune:
+            t = sc.autotune(xtgpu.NODES_Q8, budget_ms=2000)
+            sc.build_bvh(xtgpu.NODES_FP32, t.leaf_size)
+            tunes[name] = {k: getattr(t, k) for k in ("leaf_size", "stack_entries", "tile", "extend_min_blocks",
+                                                       "wave_paths")}
+        out.append(sc)
+    return specs, out, tunes
 
 
 def run_slice(svc, jobs, record=None, per_scene=None):
@@ -257,7 +266,7 @@ def main():
     from xtracer_b200.service import Service
     D = replicas.Group(world, "nccl")
 
-    specs, gscenes = build_scenes(args.scale)
+    specs, gscenes, tunes = build_scenes(args.scale, autotune=not args.no_autotune)
     jobs = replicas.rank_stream(rank, args.stream_jobs)
     nslices = max(1, len(jobs) // args.jobs_per_step)
     slices = [jobs[i * args.jobs_per_step:(i + 1) * args.jobs_per_step] for i in range(nslices)]
@@ -375,7 +384,8 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single",
                        "cache": "inputs larger than L2 (resident scenes ~%.0f MB)" %
                                 (sum(s.device_bytes() for s in gscenes) / 1e6),
-                       "wave_paths": 1 << 22, "node_format": "q8", "cuda_graphs": True},
+                       "wave_paths": 1 << 22, "node_format": "q8", "cuda_graphs": True,
+                       "autotuned": tunes},
             "p50_ms": 1000 * pct(lat_all, 50), "p99_ms": 1000 * pct(lat_all, 99),
             "latency_open_loop": latency, "plain": plain,
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 64 * len(timed[0]),

@@ -271,11 +271,24 @@ typedef struct {
     int32_t leaf_size;             /* default primitives per BVH leaf */
     int32_t node_layout;           /* BVH node order: 0 = Karras index, 1 = depth-first */
     int32_t refill_threshold;      /* variant 1: idle lanes (1..32) that trigger a refill */
-    int32_t extend_min_blocks;     /* variant 0: 0, or 8/10/12/16 resident 128-thread blocks per SM
+    int32_t extend_min_blocks;     /* variant 0: 0, 8 or 10 resident 128-thread blocks per SM
                                       requested from the compiler (caps registers) */
+    int32_t stack_entries;         /* traversal stack: 32 or 64 entries (0 = smallest that
+                                      holds the scene's BVH depth) */
 } xtgpu_tuning;
 XTGPU_API xtgpu_status xtgpu_get_tuning(xtgpu_tuning *t);
 XTGPU_API xtgpu_status xtgpu_set_tuning(const xtgpu_tuning *t);
+/* Autotuner.  Picks for one scene the primitives per BVH leaf, the traversal
+ * stack size, the camera tile, the extend kernel's register cap and the wave
+ * size, by timing a probe pathtracer job (512x512, 4 spp, depth 4) for every
+ * candidate of one knob at a time (coordinate descent from the process-wide
+ * tuning, within budget_ms of wall time).  The result stays with the scene: the
+ * BVH is rebuilt with the chosen leaf size, xtgpu_render uses it, and the service
+ * uses its tile for the scene's jobs.  *best receives it. */
+XTGPU_API xtgpu_status xtgpu_autotune(xtgpu_scene *scene, int32_t node_format, double budget_ms, xtgpu_tuning *best,
+                                      void *stream);
+/* Tuning stored with a scene (the process-wide one if it was never tuned). */
+XTGPU_API xtgpu_status xtgpu_scene_tuning(const xtgpu_scene *scene, xtgpu_tuning *t);
 
 /* Text of the last error on this thread ("" if none). */
 XTGPU_API const char *xtgpu_last_error(void);

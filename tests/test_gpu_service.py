@@ -95,3 +95,20 @@ def test_arrivals_and_latency_bookkeeping(resident):
         assert st.finish_s >= st.start_s
         assert st.rays > 0
     svc.close()
+
+
+def test_autotune_keeps_results(resident):
+    """The autotuner changes leaf size, stack, tile, register cap and wave size,
+    never the result: depth and stencil frames are the same before and after."""
+    from xtracer_b200 import scenes as sc_mod
+    s = xtgpu.Scene(sc_mod.terrain_scene(50_000, seed=21, name="tune"))
+    before = [s.render(k, 96, 64, spp=2)[0] for k in (xtgpu.STENCIL, xtgpu.DEPTH)]
+    t = s.autotune(xtgpu.NODES_FP32, budget_ms=5000)
+    assert t.leaf_size in (1, 2, 4) and t.tile in (0, 4, 8, 16) and t.extend_min_blocks in (0, 8, 10)
+    assert t.stack_entries in (0, 32, 64) and t.wave_paths in (1 << 16, 1 << 18, 1 << 22)
+    got = s.tuning()
+    assert (got.leaf_size, got.tile, got.wave_paths) == (t.leaf_size, t.tile, t.wave_paths)
+    after = [s.render(k, 96, 64, spp=2)[0] for k in (xtgpu.STENCIL, xtgpu.DEPTH)]
+    assert np.array_equal(before[0], after[0])
+    assert np.array_equal(before[1], after[1])
+    s.close()

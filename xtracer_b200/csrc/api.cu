@@ -73,6 +73,8 @@ DevCamera make_camera(const xtgpu_camera &c)
     return k;
 }
 
+const xtgpu_tuning &scene_tuning(const xtgpu_scene *sc) { return sc->tuned ? sc->tune : tuning(); }
+
 // One wave runner per process, shared by xtgpu_render calls.
 static std::mutex g_runner_mu;
 static WaveRunner *g_runner = nullptr;
@@ -119,6 +121,16 @@ xtgpu_status xtgpu_get_tuning(xtgpu_tuning *t)
     return XTGPU_OK;
 }
 
+xtgpu_status xtgpu_scene_tuning(const xtgpu_scene *sc, xtgpu_tuning *t)
+{
+    if (!sc || !t) {
+        set_error("xtgpu_scene_tuning: NULL argument");
+        return XTGPU_ERR_INVALID;
+    }
+    *t = scene_tuning(sc);
+    return XTGPU_OK;
+}
+
 xtgpu_status xtgpu_set_tuning(const xtgpu_tuning *t)
 {
     if (!t || t->extend_variant < 0 || t->extend_variant > 1 || t->extend_block < 32 || t->extend_block > 256 ||
@@ -126,8 +138,8 @@ xtgpu_status xtgpu_set_tuning(const xtgpu_tuning *t)
         t->tile > 256 || t->wave_paths < 1024 || t->wave_paths > (1ll << 26) || t->leaf_size < 1 ||
         t->leaf_size > MAX_LEAF || t->node_layout < 0 || t->node_layout > 1 || t->refill_threshold < 1 ||
         t->refill_threshold > 32 ||
-        !(t->extend_min_blocks == 0 || t->extend_min_blocks == 8 || t->extend_min_blocks == 10 ||
-          t->extend_min_blocks == 12 || t->extend_min_blocks == 16)) {
+        !(t->extend_min_blocks == 0 || t->extend_min_blocks == 8 || t->extend_min_blocks == 10) ||
+        !(t->stack_entries == 0 || t->stack_entries == 32 || t->stack_entries == 64)) {
         set_error("xtgpu_set_tuning: value out of range");
         return XTGPU_ERR_INVALID;
     }
@@ -266,7 +278,7 @@ xtgpu_status xtgpu_bvh_build(xtgpu_scene *sc, const xtgpu_bvh_opts *opts, void *
         return XTGPU_ERR_INVALID;
     }
     int fmt = opts ? opts->node_format : XTGPU_NODES_FP32;
-    int leaf = opts && opts->leaf_size > 0 ? opts->leaf_size : tuning().leaf_size;
+    int leaf = opts && opts->leaf_size > 0 ? opts->leaf_size : scene_tuning(sc).leaf_size;
     if (fmt != XTGPU_NODES_FP32 && fmt != XTGPU_NODES_Q8) {
         set_error("xtgpu_bvh_build: bad node format");
         return XTGPU_ERR_INVALID;
@@ -275,7 +287,7 @@ xtgpu_status xtgpu_bvh_build(xtgpu_scene *sc, const xtgpu_bvh_opts *opts, void *
         set_error("xtgpu_bvh_build: leaf_size out of range");
         return XTGPU_ERR_INVALID;
     }
-    return build_bvh(sc, fmt, leaf, tuning().node_layout, (cudaStream_t)stream);
+    return build_bvh(sc, fmt, leaf, scene_tuning(sc).node_layout, (cudaStream_t)stream);
 }
 
 xtgpu_status xtgpu_scene_destroy(xtgpu_scene *sc)
@@ -390,7 +402,8 @@ static xtgpu_status trace_impl(xtgpu_scene *sc, int64_t n, const void *org, cons
         q.stats = stats;
         int32_t init[4] = {cnt, 0, 0, 0};
         XTG_CUDA(cudaMemcpyAsync(ctl, init, sizeof(init), cudaMemcpyHostToDevice, s));
-        launch_extend(fmt, sc->dev, q, 0, sms * tuning().extend_blocks_per_sm, s);
+        const xtgpu_tuning &T = scene_tuning(sc);
+        launch_extend(T, fmt, sc->dev, q, 0, sms, stack_for_depth(sc->depth, T.stack_entries), s);
         XTG_CUDA(cudaGetLastError());
         int32_t back[4];
         XTG_CUDA(cudaMemcpyAsync(back, ctl, sizeof(back), cudaMemcpyDeviceToHost, s));
@@ -441,6 +454,18 @@ xtgpu_status xtgpu_trace_host(xtgpu_scene *sc, int64_t n, const float *org, cons
 
 xtgpu_status xtgpu_render(xtgpu_scene *sc, const xtgpu_render_params *p, float *rgba, uint64_t *rays, void *stream)
 {
+    if (!sc) {
+        set_error("xtgpu_render: NULL argument");
+        return XTGPU_ERR_INVALID;
+    }
+    return render_impl(sc, p, rgba, rays, (cudaStream_t)stream, scene_tuning(sc));
+}
+
+}  // extern "C"
+
+xtgpu_status xtg::render_impl(xtgpu_scene *sc, const xtgpu_render_params *p, float *rgba, uint64_t *rays,
+                              cudaStream_t stream, const xtgpu_tuning &T)
+{
     if (!sc || !p || !rgba) {
         set_error("xtgpu_render: NULL argument");
         return XTGPU_ERR_INVALID;
@@ -464,11 +489,13 @@ xtgpu_status xtgpu_render(xtgpu_scene *sc, const xtgpu_render_params *p, float *
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t npix = (int64_t)(x1 - x0) * (y1 - y0);
     const int64_t paths = npix * p->spp;
-    const int64_t cap = std::min<int64_t>(paths, tuning().wave_paths);
+    const int64_t cap = std::min<int64_t>(paths, T.wave_paths);
     std::lock_guard<std::mutex> lock(g_runner_mu);
     WaveRunner *R = nullptr;
     XTG_TRY(get_runner(std::max<int64_t>(cap, 1 << 16), s, &R));
     XTG_TRY(R->set_scenes(&sc->dev, 1, s));
+    R->T = T;
+    R->stack = stack_for_depth(sc->depth, T.stack_entries);
     XTG_CUDA(cudaMemsetAsync(R->q.ctl, 0, 64, s));
     XTG_CUDA(cudaMemsetAsync(rgba, 0, sizeof(float4) * npix, s));
     DevJob J{};
@@ -485,7 +512,7 @@ xtgpu_status xtgpu_render(xtgpu_scene *sc, const xtgpu_render_params *p, float *
     J.rh = y1 - y0;
     J.scene = 0;
     J.bounces = bounces_of(p->integrator, p->rdepth);
-    J.tile = tuning().tile;
+    J.tile = T.tile;
     J.frame = (float4 *)rgba;
     std::vector<DevJob> jobs(1, J);
     for (int64_t first = 0; first < paths; first += R->cap) {
@@ -503,6 +530,8 @@ xtgpu_status xtgpu_render(xtgpu_scene *sc, const xtgpu_render_params *p, float *
     }
     return XTGPU_OK;
 }
+
+extern "C" {
 
 xtgpu_status xtgpu_render_host(xtgpu_scene *sc, const xtgpu_render_params *p, float *rgba_host, uint64_t *rays,
                                void *stream)

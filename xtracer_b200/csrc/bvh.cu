@@ -611,7 +611,7 @@ xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, int layo
         S.nodes8 = (const uint4 *)sc->nodes8.p;
         sc->built8 = true;
     }
-    if (sc->depth > STACK_MAX - 2) {
+    if (sc->depth > STACK_MAX - 2) {   // the 64-entry stack variant must hold the tree
         set_error("xtgpu_bvh_build: BVH depth exceeds the traversal stack");
         return XTGPU_ERR_LIMIT;
     }

@@ -150,7 +150,8 @@ extern "C" xtgpu_status xtgpu_render_tile_noalloc(xtgpu_scene *sc, const xtgpu_r
     J.rh = y1 - y0;
     J.scene = 0;
     J.bounces = bounces_of(p->integrator, p->rdepth);
-    J.tile = tuning().tile;
+    const xtgpu_tuning &T = scene_tuning(sc);
+    J.tile = T.tile;
     J.frame = (float4 *)rgba;
     J.first = 0;
     J.count = paths;
@@ -170,7 +171,8 @@ extern "C" xtgpu_status xtgpu_render_tile_noalloc(xtgpu_scene *sc, const xtgpu_r
     int dev = 0, sms = 148;
     XTG_CUDA(cudaGetDevice(&dev));
     XTG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    enqueue_wave_raw(q, jobs_dev, scene_dev, sc->dev, prefix_dev, J.bounces, p->node_format, sms, s);
+    enqueue_wave_raw(T, q, jobs_dev, scene_dev, sc->dev, prefix_dev, J.bounces, p->node_format, sms,
+                     stack_for_depth(sc->depth, T.stack_entries), s);
     XTG_CUDA(cudaGetLastError());
     int32_t back[16];
     XTG_CUDA(cudaMemcpyAsync(back, q.ctl, sizeof(back), cudaMemcpyDeviceToHost, s));

@@ -381,12 +381,12 @@ __global__ void __launch_bounds__(256) k_extend_refill(DevScene S1, const DevSce
 // Closest hit of one ray: a single loop that takes one node or one leaf per
 // iteration; stack entries keep their entry distance so subtrees beyond the
 // current closest hit are dropped without a fetch.
-template <int FMT>
+template <int FMT, int STACK>
 __device__ __forceinline__ void trace_ray(const SceneView &V, const RayPre &r, float tmin, float &tmax,
                                           uint32_t &prim, float &bu, float &bv, int32_t *ctl_overflow, uint32_t &nv,
                                           uint32_t &np)
 {
-    int2 stack[STACK_MAX];
+    int2 stack[STACK];
     int sp = 0;
     int32_t ref = V.root;
     for (uint32_t guard = 0;; ++guard) {
@@ -400,7 +400,7 @@ __device__ __forceinline__ void trace_ray(const SceneView &V, const RayPre &r, f
             ++nv;
             if (P.h0 && P.h1) {
                 const bool sw = P.t1 < P.t0;
-                if (sp >= STACK_MAX) {
+                if (sp >= STACK) {
                     *ctl_overflow = 1;
                     break;
                 }
@@ -436,7 +436,7 @@ __device__ __forceinline__ void trace_ray(const SceneView &V, const RayPre &r, f
 // every lane runs its ray to the end.  MINB > 0 asks the compiler for at least
 // MINB resident 128-thread blocks per SM (fewer registers, more warps to hide
 // the latency of the dependent node loads).
-template <int FMT, bool MULTI, int MINB>
+template <int FMT, bool MULTI, int MINB, int STACK>
 __global__ void __launch_bounds__(MINB > 0 ? 128 : 256, MINB > 0 ? MINB : 1)
     k_extend_batch(DevScene S1, const DevScene *__restrict__ scenes, const DevJob *__restrict__ jobs, WaveQueues q,
                    int side)
@@ -463,10 +463,10 @@ __global__ void __launch_bounds__(MINB > 0 ? 128 : 256, MINB > 0 ? MINB : 1)
             if (MULTI || q.job_rays) jb = q.meta[side][i].y;
             if (MULTI) {
                 const SceneView V = scene_view<FMT>(scenes[jobs[jb].scene]);
-                trace_ray<FMT>(V, r, a.w, tmax, prim, bu, bv, &q.ctl[3], nv, np);
+                trace_ray<FMT, STACK>(V, r, a.w, tmax, prim, bu, bv, &q.ctl[3], nv, np);
                 np += (uint32_t)V.n_planes;
             } else {
-                trace_ray<FMT>(V1, r, a.w, tmax, prim, bu, bv, &q.ctl[3], nv, np);
+                trace_ray<FMT, STACK>(V1, r, a.w, tmax, prim, bu, bv, &q.ctl[3], nv, np);
                 np += (uint32_t)V1.n_planes;
             }
             xtgpu_hit o;
@@ -712,6 +712,7 @@ xtgpu_status WaveRunner::init(int64_t capacity, int max_jobs, int max_scenes, cu
     XTG_CUDA(cudaGetDevice(&dev));
     XTG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     for (int k = 0; k < 2 * MAX_TIMED; ++k) XTG_CUDA(cudaEventCreate(&ev[k]));
+    XTG_CUDA(cudaEventCreateWithFlags(&acc_done, cudaEventDisableTiming));
     XTG_TRY(dalloc(statsbuf, 16, s));
     XTG_CUDA(cudaMemsetAsync(statsbuf.p, 0, 16, s));
     return XTGPU_OK;
@@ -731,6 +732,8 @@ void WaveRunner::release()
     for (int k = 0; k < 2 * MAX_TIMED; ++k)
         if (ev[k]) cudaEventDestroy(ev[k]);
     for (auto &e : ev) e = nullptr;
+    if (acc_done) cudaEventDestroy(acc_done);
+    acc_done = nullptr;
     if (host_jobs) cudaFreeHost(host_jobs);
     if (host_prefix) cudaFreeHost(host_prefix);
     if (host_ctl) cudaFreeHost(host_ctl);
@@ -772,15 +775,15 @@ void WaveRunner::enqueue(int njobs, int64_t total, int bounces, int fmt, bool mu
     int side = 0;
     for (int b = 0; b < bounces; ++b) {
         cudaMemsetAsync(q.ctl + 2, 0, sizeof(int32_t), s);
-        int eb = sms * tuning().extend_blocks_per_sm;
+
         if (time_extend && b < MAX_TIMED) rec(ev[2 * b]);
-        launch_extend_kernel(fmt, multi, single, scenes, jobs, q, side, eb, s);
+        launch_extend_kernel(T, fmt, multi, single, scenes, jobs, q, side, sms, stack, s);
         if (time_extend && b < MAX_TIMED) rec(ev[2 * b + 1]);
         cudaMemsetAsync(q.ctl + (side ^ 1), 0, sizeof(int32_t), s);
         k_shade<<<gb, 256, 0, s>>>(jobs, scenes, q, side);
         side ^= 1;
     }
-    k_accumulate<<<gb, 256, 0, s>>>(jobs, q.ctl, (const int64_t *)prefixbuf.p, q.contrib);
+    if (!defer_acc) k_accumulate<<<gb, 256, 0, s>>>(jobs, q.ctl, (const int64_t *)prefixbuf.p, q.contrib);
 }
 
 xtgpu_status WaveRunner::collect_times(cudaStream_t s)
@@ -836,7 +839,10 @@ xtgpu_status WaveRunner::run_wave(const std::vector<DevJob> &jobs, int bounces, 
         // One graph per (bounces, format, scene count) shape; kernel arguments
         // point at fixed buffers, so a graph replays any wave of that shape.
         uint64_t key = ((uint64_t)bounces << 4) ^ (uint64_t)fmt ^ (multi ? 2ull : 0ull) ^ (time_extend ? 4ull : 0ull) ^
-                       (q.stats ? 8ull : 0ull);
+                       (defer_acc ? (1ull << 48) : 0ull) ^
+                       (q.stats ? 8ull : 0ull) ^ ((uint64_t)stack << 12) ^ ((uint64_t)T.extend_min_blocks << 20) ^
+                       ((uint64_t)T.extend_variant << 28) ^ ((uint64_t)T.extend_blocks_per_sm << 32) ^
+                       ((uint64_t)T.extend_block << 40);
         auto it = graphs.find(key);
         if (it == graphs.end()) {
             cudaGraph_t g;
@@ -855,6 +861,14 @@ xtgpu_status WaveRunner::run_wave(const std::vector<DevJob> &jobs, int bounces, 
         XTG_CUDA(cudaGraphLaunch(it->second, s));
     } else {
         enqueue(nj, total, bounces, fmt, multi, s, false);
+    }
+    if (defer_acc) {
+        // waves of two runners overlap; a job's samples are still folded in
+        // order because each accumulate waits for the one before it
+        if (prev_acc) XTG_CUDA(cudaStreamWaitEvent(s, prev_acc, 0));
+        k_accumulate<<<sms * 8, 256, 0, s>>>((const DevJob *)jobbuf.p, q.ctl, (const int64_t *)prefixbuf.p,
+                                             q.contrib);
+        XTG_CUDA(cudaEventRecord(acc_done, s));
     }
     launches += 2 + 2 * bounces;   // camera, bounces x (extend, shade), accumulate
     last_bounces = bounces;
@@ -877,16 +891,16 @@ xtgpu_status WaveRunner::read_ctl(int32_t *overflow, unsigned long long *rays, c
 // tile x register cap over terrain, hairball and sphere scenes): warp-batched
 // fetch, one primitive per leaf, depth-first node order, 8x8 pixel tiles, and
 // 64 registers (8 resident 128-thread blocks per SM).
-static xtgpu_tuning g_tuning = {0, 128, 8, 8, 1ll << 22, 1, 1, 8, 8};
+static xtgpu_tuning g_tuning = {0, 128, 8, 8, 1ll << 22, 1, 1, 8, 8, 0};
 xtgpu_tuning &tuning() { return g_tuning; }
 
-void launch_extend_kernel(int fmt, bool multi, const DevScene &single, const DevScene *scenes, const DevJob *jobs,
-                          const WaveQueues &q, int side, int blocks, cudaStream_t s)
+void launch_extend_kernel(const xtgpu_tuning &T, int fmt, bool multi, const DevScene &single,
+                          const DevScene *scenes, const DevJob *jobs, const WaveQueues &q, int side, int sms,
+                          int stack, cudaStream_t s)
 {
-    const xtgpu_tuning &T = tuning();
+    const int blocks = sms * T.extend_blocks_per_sm;
     const int tb = T.extend_block;
     const int nb = std::max(1, blocks * 128 / tb);   // same resident thread count for any block size
-#define XTG_LAUNCH(K, F, M) K<F, M><<<nb, tb, 0, s>>>(single, scenes, jobs, q, side)
 #define XTG_LAUNCH_R(K, F, M) K<F, M><<<nb, tb, 0, s>>>(single, scenes, jobs, q, side, T.refill_threshold)
     if (T.extend_variant == 1) {
         if (fmt == XTGPU_NODES_Q8) { if (multi) XTG_LAUNCH_R(k_extend_refill, XTGPU_NODES_Q8, true); else XTG_LAUNCH_R(k_extend_refill, XTGPU_NODES_Q8, false); }
@@ -894,38 +908,37 @@ void launch_extend_kernel(int fmt, bool multi, const DevScene &single, const Dev
         return;
     }
     // register-capped instantiations run with 128-thread blocks
-#define XTG_B(MB)                                                                                      \
-    do {                                                                                               \
-        const int tbb = MB > 0 ? 128 : tb, nbb = MB > 0 ? std::max(1, blocks) : nb;                 \
-        if (fmt == XTGPU_NODES_Q8) {                                                                   \
-            if (multi) k_extend_batch<XTGPU_NODES_Q8, true, MB><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side);   \
-            else k_extend_batch<XTGPU_NODES_Q8, false, MB><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side);       \
-        } else {                                                                                       \
-            if (multi) k_extend_batch<XTGPU_NODES_FP32, true, MB><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side); \
-            else k_extend_batch<XTGPU_NODES_FP32, false, MB><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side);     \
-        }                                                                                              \
+#define XTG_B(MB, ST)                                                                                   \
+    do {                                                                                                \
+        const int tbb = MB > 0 ? 128 : tb, nbb = MB > 0 ? std::max(1, blocks) : nb;                  \
+        if (fmt == XTGPU_NODES_Q8) {                                                                    \
+            if (multi) k_extend_batch<XTGPU_NODES_Q8, true, MB, ST><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side);   \
+            else k_extend_batch<XTGPU_NODES_Q8, false, MB, ST><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side);       \
+        } else {                                                                                        \
+            if (multi) k_extend_batch<XTGPU_NODES_FP32, true, MB, ST><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side); \
+            else k_extend_batch<XTGPU_NODES_FP32, false, MB, ST><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side);     \
+        }                                                                                               \
     } while (0)
+    const bool small = stack <= 32;
     switch (T.extend_min_blocks) {
-    case 8: XTG_B(8); break;
-    case 10: XTG_B(10); break;
-    case 12: XTG_B(12); break;
-    case 16: XTG_B(16); break;
-    default: XTG_B(0); break;
+    case 8: if (small) XTG_B(8, 32); else XTG_B(8, 64); break;
+    case 10: if (small) XTG_B(10, 32); else XTG_B(10, 64); break;
+    default: if (small) XTG_B(0, 32); else XTG_B(0, 64); break;
     }
 #undef XTG_B
-#undef XTG_LAUNCH
 #undef XTG_LAUNCH_R
 }
 
-void enqueue_wave_raw(const WaveQueues &q, const DevJob *jobs, const DevScene *scenes, const DevScene &single,
-                      const int64_t *prefix, int bounces, int fmt, int sms, cudaStream_t s)
+void enqueue_wave_raw(const xtgpu_tuning &T, const WaveQueues &q, const DevJob *jobs, const DevScene *scenes,
+                      const DevScene &single, const int64_t *prefix, int bounces, int fmt, int sms, int stack,
+                      cudaStream_t s)
 {
     const int gb = sms * 8;
     k_camera<<<gb, 256, 0, s>>>(jobs, scenes, q);
     int side = 0;
     for (int b = 0; b < bounces; ++b) {
         cudaMemsetAsync(q.ctl + 2, 0, sizeof(int32_t), s);
-        launch_extend_kernel(fmt, false, single, scenes, jobs, q, side, sms * tuning().extend_blocks_per_sm, s);
+        launch_extend_kernel(T, fmt, false, single, scenes, jobs, q, side, sms, stack, s);
         cudaMemsetAsync(q.ctl + (side ^ 1), 0, sizeof(int32_t), s);
         k_shade<<<gb, 256, 0, s>>>(jobs, scenes, q, side);
         side ^= 1;
@@ -933,9 +946,17 @@ void enqueue_wave_raw(const WaveQueues &q, const DevJob *jobs, const DevScene *s
     k_accumulate<<<gb, 256, 0, s>>>(jobs, q.ctl, prefix, q.contrib);
 }
 
-void launch_extend(int fmt, const DevScene &S, const WaveQueues &q, int side, int blocks, cudaStream_t s)
+void launch_extend(const xtgpu_tuning &T, int fmt, const DevScene &S, const WaveQueues &q, int side, int sms,
+                   int stack, cudaStream_t s)
 {
-    launch_extend_kernel(fmt, false, S, nullptr, nullptr, q, side, blocks, s);
+    launch_extend_kernel(T, fmt, false, S, nullptr, nullptr, q, side, sms, stack, s);
+}
+
+int stack_for_depth(int depth, int requested)
+{
+    if (requested == 32 && depth <= 30) return 32;
+    if (requested == 64) return 64;
+    return depth <= 30 ? 32 : 64;
 }
 
 int bounces_of(int integrator, int rdepth)

@@ -23,6 +23,11 @@ struct WaveRunner {
     int64_t launches = 0;
     int last_bounces = 0;
     HostBuf statsbuf;
+    // overlapped waves: accumulate launched after the wave's graph, ordered
+    // behind prev_acc (the previous wave's accumulate), signalling acc_done
+    bool defer_acc = false;
+    cudaEvent_t acc_done = nullptr;
+    cudaEvent_t prev_acc = nullptr;
     xtgpu_status collect_times(cudaStream_t s);
     void enable_stats(bool on) { q.stats = on ? (unsigned long long *)statsbuf.p : nullptr; }
     DevJob *host_jobs = nullptr;      // pinned
@@ -32,6 +37,8 @@ struct WaveRunner {
     int max_jobs = 0, max_scenes = 0, nscenes = 0;
     int sms = 148;
     DevScene single{};
+    xtgpu_tuning T{};   // launch configuration of the next waves
+    int stack = 64;     // traversal stack entries (32 or 64)
     std::unordered_map<uint64_t, cudaGraphExec_t> graphs;
 
     xtgpu_status init(int64_t capacity, int max_jobs, int max_scenes, cudaStream_t s);
@@ -47,14 +54,19 @@ struct WaveRunner {
 
 int bounces_of(int integrator, int rdepth);
 xtgpu_tuning &tuning();
-void launch_extend_kernel(int fmt, bool multi, const DevScene &single, const DevScene *scenes, const DevJob *jobs,
-                          const WaveQueues &q, int side, int blocks, cudaStream_t s);
+void launch_extend_kernel(const xtgpu_tuning &T, int fmt, bool multi, const DevScene &single,
+                          const DevScene *scenes, const DevJob *jobs, const WaveQueues &q, int side, int sms,
+                          int stack, cudaStream_t s);
+// smallest stack variant (32 or 64 entries) that holds a tree of this depth
+int stack_for_depth(int depth, int requested);
 // One single-scene wave over caller-provided device buffers: no allocation and
 // no host synchronisation.  jobs/scenes/prefix and q.ctl must already hold the
 // wave (ctl[0] = ctl[5] = paths, ctl[4] = jobs, other counters zero).
-void enqueue_wave_raw(const WaveQueues &q, const DevJob *jobs, const DevScene *scenes, const DevScene &single,
-                      const int64_t *prefix, int bounces, int fmt, int sms, cudaStream_t s);
+void enqueue_wave_raw(const xtgpu_tuning &T, const WaveQueues &q, const DevJob *jobs, const DevScene *scenes,
+                      const DevScene &single, const int64_t *prefix, int bounces, int fmt, int sms, int stack,
+                      cudaStream_t s);
 // Closest hit of the q.ctl[side] rays of queue `side` (no job table needed).
-void launch_extend(int fmt, const DevScene &S, const WaveQueues &q, int side, int blocks, cudaStream_t s);
+void launch_extend(const xtgpu_tuning &T, int fmt, const DevScene &S, const WaveQueues &q, int side, int sms,
+                   int stack, cudaStream_t s);
 
 }  // namespace xtg

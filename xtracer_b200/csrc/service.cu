@@ -262,13 +262,27 @@ xtgpu_status xtgpu_service_run(xtgpu_service *v, double max_seconds)
             dj.rh = J.d.height;
             dj.scene = J.d.scene;
             dj.bounces = bounces_of(J.d.integrator, J.d.rdepth);
-            dj.tile = tuning().tile;
+            dj.tile = scene_tuning(v->scenes[J.d.scene]).tile;
             dj.frame = J.frame;
             dj.first = J.done;
             dj.count = take[k];
             bounces = std::max(bounces, dj.bounces);
             wave.push_back(dj);
             ids.push_back(v->active[k]);
+        }
+        // launch configuration: the tuning of the scene with the most paths in
+        // the wave (its own if autotuned); the stack holds the deepest BVH the
+        // wave touches
+        {
+            std::vector<int64_t> per(v->scenes.size(), 0);
+            for (const DevJob &dj : wave) per[dj.scene] += dj.count;
+            int top = (int)(std::max_element(per.begin(), per.end()) - per.begin());
+            v->R.T = scene_tuning(v->scenes[top]);
+            int stack = 32;
+            for (size_t k = 0; k < per.size(); ++k)
+                if (per[k] > 0)
+                    stack = std::max(stack, stack_for_depth(v->scenes[k]->depth, scene_tuning(v->scenes[k]).stack_entries));
+            v->R.stack = stack;
         }
         XTG_TRY(v->R.run_wave(wave, bounces, v->o.node_format, v->o.use_graphs != 0, v->s));
         v->wave_rays.resize(wave.size());

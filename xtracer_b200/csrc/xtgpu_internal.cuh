@@ -90,6 +90,9 @@ struct xtgpu_scene {
     int device = 0;
     // host copies used by the service and the tests
     int32_t n_objects = 0;
+    // tuning picked by xtgpu_autotune for this scene
+    xtgpu_tuning tune{};
+    bool tuned = false;
 };
 
 namespace xtg {
@@ -116,15 +119,10 @@ void dfree(HostBuf &b);
 // BVH build (bvh.cu)
 xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, int layout, cudaStream_t s);
 
-// Ray/primitive batches (trace.cu)
-struct RayQueue {
-    const float4 *org;    // (org, tmin)
-    const float4 *dir;    // (dir, tmax)
-    xtgpu_hit *hit;
-};
-xtgpu_status launch_trace(const DevScene &S, int fmt, int64_t n, const float4 *org, const float4 *dir,
-                          xtgpu_hit *hits, const int32_t *count_dev, int32_t *fetch_dev, cudaStream_t s);
-int trace_grid_blocks();
-int trace_block_threads();
+// the tuning a scene renders with: its own if autotuned, else the process-wide one
+const xtgpu_tuning &scene_tuning(const xtgpu_scene *sc);
+// xtgpu_render with an explicit launch configuration (the autotuner's probe)
+xtgpu_status render_impl(xtgpu_scene *sc, const xtgpu_render_params *p, float *rgba, uint64_t *rays,
+                         cudaStream_t s, const xtgpu_tuning &T);
 
 }  // namespace xtg

@@ -95,7 +95,8 @@ class ServiceStats(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("extend_variant", C.c_int32), ("extend_block", C.c_int32), ("extend_blocks_per_sm", C.c_int32),
                 ("tile", C.c_int32), ("wave_paths", C.c_int64), ("leaf_size", C.c_int32),
-                ("node_layout", C.c_int32), ("refill_threshold", C.c_int32), ("extend_min_blocks", C.c_int32)]
+                ("node_layout", C.c_int32), ("refill_threshold", C.c_int32), ("extend_min_blocks", C.c_int32),
+                ("stack_entries", C.c_int32)]
 
 
 def get_tuning() -> "Tuning":
@@ -148,6 +149,8 @@ SIGNATURES = {
     "xtgpu_service_reset_stats": [C.c_void_p],
     "xtgpu_get_tuning": [C.c_void_p],
     "xtgpu_set_tuning": [C.c_void_p],
+    "xtgpu_autotune": [C.c_void_p, C.c_int32, C.c_double, C.c_void_p, C.c_void_p],
+    "xtgpu_scene_tuning": [C.c_void_p, C.c_void_p],
 }
 
 _lib = None
@@ -242,6 +245,19 @@ class Scene:
         o = BvhOpts(node_format, leaf_size)
         check(lib().xtgpu_bvh_build(self.handle, C.byref(o), stream_handle(stream)))
         self.formats.add(node_format)
+
+    def autotune(self, node_format: int = NODES_FP32, budget_ms: float = 3000.0, stream=None) -> "Tuning":
+        """Picks this scene's leaf size, stack size, tile, register cap and wave
+        size by timing a probe pathtracer job (xtgpu_autotune)."""
+        t = Tuning()
+        check(lib().xtgpu_autotune(self.handle, node_format, budget_ms, C.byref(t), stream_handle(stream)))
+        self.formats.add(node_format)
+        return t
+
+    def tuning(self) -> "Tuning":
+        t = Tuning()
+        check(lib().xtgpu_scene_tuning(self.handle, C.byref(t)))
+        return t
 
     def close(self) -> None:
         if getattr(self, "handle", None):
