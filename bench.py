@@ -5,8 +5,8 @@ hairball, 64 and 4096 spheres), 512 seeded jobs with resolution in
 {128,256,512,1024}^2, spp in {1,4,16,64}, pathtracer depth 4.
 
 A step is one slice of 64 jobs of that stream, all submitted at once and run
-to completion through the render service (merged waves, 8-bit quantised BVH,
-CUDA graphs).  Reported beside it, on the same jobs: the plain path (one job per
+to completion through the render service (merged waves, two in flight, 8-bit
+quantised BVH, CUDA graphs).  Reported beside it, on the same jobs: the plain path (one job per
 launch, FP32 BVH, no graphs), an end-to-end pass with every frame copied back
 to host memory, open-loop p50/p99 latency under Poisson arrivals, the extend
 kernel's roofline and the reference CPU renderer on the host cores.
@@ -136,9 +136,11 @@ def build_scenes(scale, autotune=False):
     return specs, out, tunes
 
 
-def run_slice(svc, jobs, record=None, per_scene=None):
+def run_slice(svc, jobs, record=None, per_scene=None, view=False):
     """Submits the jobs at once, runs the service to completion; returns
-    (rays, latencies in s).  per_scene (array) accumulates rays by scene."""
+    (rays, latencies in s).  per_scene (array) accumulates rays by scene.
+    record collects each frame (copied), or with view (host_results services)
+    the last pixel read from the frame's host copy in place."""
     from xtracer_b200 import xtgpu
     ids = [svc.submit(j.scene, xtgpu.PATHTRACER, j.width, j.height, j.spp, j.depth, 100.0, j.seed) for j in jobs]
     svc.run()
@@ -152,7 +154,7 @@ def run_slice(svc, jobs, record=None, per_scene=None):
             per_scene[j.scene] += st.rays
         lat.append(st.finish_s - st.submit_s)
         if record is not None:
-            record.append(svc.result(i))
+            record.append(float(svc.result_view(i)[-1, -1, 0]) if view else svc.result(i))
         svc.release(i)
     return rays, lat
 
@@ -273,7 +275,7 @@ def main():
     budget = 48 << 30
 
     served = Service(gscenes, node_format=xtgpu.NODES_Q8, use_graphs=True, merge_jobs=True, memory_budget=budget,
-                     time_kernels=True, stream=stream)
+                     waves_in_flight=2, stream=stream)
     # warm-up steps (untimed): graphs captured, allocator pools primed
     for w in range(args.warmup):
         run_slice(served, slices[w % nslices])
@@ -287,9 +289,8 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     rays, lat = 0, []
-    per_scene = np.zeros(len(gscenes))
     for sl in timed:
-        r, l = run_slice(served, sl, per_scene=per_scene)
+        r, l = run_slice(served, sl)
         rays += r
         lat += l
     e1.record()
@@ -303,12 +304,23 @@ def main():
     value = rays_all / t_max / 1e6
     lat_all = D.gather(lat)
 
-    # roofline of the extend kernel over the timed region
+    # roofline of the extend kernel: the same steps again, one wave at a time
+    # so that each extend launch's CUDA-event duration is its own (with two
+    # waves in flight, launches share the SMs with the other wave's kernels)
+    rsvc = Service(gscenes, node_format=xtgpu.NODES_Q8, use_graphs=True, merge_jobs=True, memory_budget=budget,
+                   time_kernels=True, waves_in_flight=1, stream=stream)
+    run_slice(rsvc, slices[0])
+    rsvc.reset_stats()
+    per_scene = np.zeros(len(gscenes))
+    for sl in timed:
+        run_slice(rsvc, sl, per_scene=per_scene)
+    rst = rsvc.stats()
+    rsvc.close()
     bpr = roofline_bytes_per_ray(specs, gscenes, xtgpu.NODES_Q8)
     scene_bpr = [b["bytes_per_ray"] for b in bpr]
     # rays of each scene in the timed steps times that scene's bytes per ray
     alg_bytes = float(np.dot(per_scene, scene_bpr))
-    ext_s = st.extend_ms / 1000.0
+    ext_s = rst.extend_ms / 1000.0
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / ext_s / 1e9 if ext_s > 0 else None
 
@@ -322,7 +334,7 @@ def main():
     e_rays = 0
     d2h = 0
     for sl in timed:
-        r, _ = run_slice(e2e_svc, sl, record=[])
+        r, _ = run_slice(e2e_svc, sl, record=[], view=True)
         e_rays += r
         d2h += sum(j.width * j.height * 16 for j in sl)
     torch.cuda.synchronize()
@@ -334,7 +346,7 @@ def main():
     plain = None
     if not args.no_plain:
         psvc = Service(gscenes, node_format=xtgpu.NODES_FP32, use_graphs=False, merge_jobs=False,
-                       memory_budget=budget, stream=stream)
+                       memory_budget=budget, waves_in_flight=1, stream=stream)
         torch.cuda.synchronize()
         p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         p0.record()
@@ -350,9 +362,22 @@ def main():
         s1.record()
         torch.cuda.synchronize()
         ss = s0.elapsed_time(s1) / 1000.0
+        # the served form with FP32 nodes on that step (node-format cost)
+        fsvc = Service(gscenes, node_format=xtgpu.NODES_FP32, use_graphs=True, merge_jobs=True,
+                       memory_budget=budget, waves_in_flight=2, stream=stream)
+        run_slice(fsvc, slices[0])
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        fr, _ = run_slice(fsvc, timed[0])
+        f1.record()
+        torch.cuda.synchronize()
+        fs = f0.elapsed_time(f1) / 1000.0
+        fsvc.close()
         plain = {"value": pr / ps / 1e6, "unit": "Mrays/s", "step_jobs": len(timed[0]),
                  "p50_ms": 1000 * pct(pl, 50), "p99_ms": 1000 * pct(pl, 99),
                  "served_same_step_mrays": sr / ss / 1e6, "speedup": (sr / ss) / (pr / ps),
+                 "served_fp32_same_step_mrays": fr / fs / 1e6,
                  "form": "one job per launch, FP32 BVH, no CUDA graphs"}
 
     # open-loop latency: Poisson arrivals at 1.5x the plain path's job rate
@@ -384,7 +409,7 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single",
                        "cache": "inputs larger than L2 (resident scenes ~%.0f MB)" %
                                 (sum(s.device_bytes() for s in gscenes) / 1e6),
-                       "wave_paths": 1 << 22, "node_format": "q8", "cuda_graphs": True,
+                       "wave_paths": 1 << 22, "node_format": "q8", "cuda_graphs": True, "waves_in_flight": 2,
                        "autotuned": tunes},
             "p50_ms": 1000 * pct(lat_all, 50), "p99_ms": 1000 * pct(lat_all, 99),
             "latency_open_loop": latency, "plain": plain,
@@ -393,7 +418,8 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": None,
                          "kernel": "k_extend (closest-hit traversal)", "peak_kind": peak_kind,
-                         "extend_ms": st.extend_ms, "extend_launches": st.extend_launches,
+                         "extend_ms": rst.extend_ms, "extend_launches": rst.extend_launches,
+                         "timing": "CUDA events around every extend launch, same steps, one wave in flight",
                          "bytes_per_ray": {b["scene"]: round(b["bytes_per_ray"], 1) for b in bpr},
                          "nodes_per_ray": {b["scene"]: round(b["nodes_per_ray"], 2) for b in bpr},
                          "prims_per_ray": {b["scene"]: round(b["prims_per_ray"], 2) for b in bpr}},

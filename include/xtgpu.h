@@ -210,12 +210,16 @@ typedef struct {
     int32_t node_format;           /* BVH format used by the service */
     int32_t use_graphs;            /* 1 = replay each wave as a CUDA graph */
     int32_t merge_jobs;            /* 0 = one job per launch (the plain path) */
-    int32_t host_results;          /* 1 = copy each finished frame to host memory and free
-                                      its device buffer at once (frees budget early) */
+    int32_t host_results;          /* 1 = copy each finished frame to pinned host memory
+                                      (asynchronously, reused between jobs) and free its
+                                      device buffer at once (frees budget early) */
     int32_t time_kernels;          /* 1 = time every extend launch with CUDA events */
     int32_t count_visits;          /* 1 = count BVH nodes visited / primitives tested */
     int32_t policy;                /* wave planning: 0 = fewest remaining paths first,
                                       1 = equal share per running job */
+    int32_t waves_in_flight;       /* 1 = one wave at a time; 2 (or 0) = the next wave is
+                                      launched on a second stream while the previous one
+                                      drains, so its kernels fill the previous tail */
 } xtgpu_service_opts;
 
 typedef struct {
@@ -229,7 +233,9 @@ typedef struct {
 typedef struct {
     int32_t state;                 /* 0 queued, 1 running, 2 done, 3 failed */
     uint64_t rays;                 /* rays traced for the job */
-    double submit_s, start_s, finish_s;   /* service clock (seconds) */
+    double submit_s, start_s, finish_s;   /* service clock (seconds): arrival, admission,
+                                             result available (on the host with host_results) */
+    double render_done_s;          /* the job's last wave retired (device work done) */
 } xtgpu_job_status;
 
 XTGPU_API xtgpu_status xtgpu_service_create(const xtgpu_service_opts *opts, void *stream, xtgpu_service **out);
@@ -243,6 +249,9 @@ XTGPU_API xtgpu_status xtgpu_service_run(xtgpu_service *svc, double max_seconds)
 XTGPU_API xtgpu_status xtgpu_service_poll(xtgpu_service *svc, int64_t job_id, xtgpu_job_status *status);
 /* Copies a finished job's RGBA frame (width*height*4 floats) to host memory. */
 XTGPU_API xtgpu_status xtgpu_service_result(xtgpu_service *svc, int64_t job_id, float *rgba_host);
+/* With host_results: the finished job's frame in the service's pinned host
+ * memory, without a copy; valid until xtgpu_service_release. */
+XTGPU_API xtgpu_status xtgpu_service_result_host(xtgpu_service *svc, int64_t job_id, const float **rgba_host);
 /* Releases a finished job's frame buffer. */
 XTGPU_API xtgpu_status xtgpu_service_release(xtgpu_service *svc, int64_t job_id);
 XTGPU_API xtgpu_status xtgpu_service_destroy(xtgpu_service *svc);

@@ -8,6 +8,10 @@
 // fixed kernel sequence (camera, [extend, shade] x bounces, accumulate) whose
 // sizes live in device memory, so it replays as a CUDA graph.
 //
+// Two waves are in flight at a time, on two streams with their own queues:
+// the next wave's camera, extend and shade kernels fill the SMs the previous
+// wave's tail leaves idle, and its accumulate waits for the previous one.
+//
 // Because paths are keyed by (seed, pixel, sample) and folded per pixel in
 // sample order, a job's frame is bit-identical whatever it is merged with.
 #include <algorithm>
@@ -25,21 +29,37 @@ namespace xtg {
 struct SvcJob {
     xtgpu_job_desc d{};
     int state = 0;   // 0 queued, 1 running, 2 done, 3 failed
-    double submit_s = 0, start_s = 0, finish_s = 0;
-    int64_t paths = 0, done = 0;
+    double submit_s = 0, start_s = 0, finish_s = 0, render_done_s = 0;
+    int64_t paths = 0;
+    int64_t planned = 0;   // paths given to launched waves
+    int64_t done = 0;      // paths of retired waves
     uint64_t rays = 0;
     uint64_t frame_bytes = 0;
     float4 *frame = nullptr;
-    std::vector<float4> host;   // host copy (host_results)
+    float4 *host = nullptr;          // pinned host copy (host_results)
+    cudaEvent_t copied = nullptr;    // set while the host copy is in flight
+};
+
+// One wave in flight: its runner (queues, job table, graphs), the stream it
+// runs on, and what the host needs when it retires.
+struct WaveSlot {
+    WaveRunner R;
+    cudaStream_t s = nullptr;
+    cudaEvent_t fin = nullptr;            // after the wave's accumulate and ray-count copy
+    unsigned long long *jrays = nullptr;  // pinned: rays per job of the wave
+    std::vector<DevJob> wave;
+    std::vector<int64_t> ids;
 };
 
 }  // namespace xtg
 
 struct xtgpu_service {
     xtgpu_service_opts o{};
-    cudaStream_t s = nullptr;
+    cudaStream_t s = nullptr;  // admission, frees, results
     bool own_stream = false;   // created here: the legacy default stream cannot be captured
-    xtg::WaveRunner R;
+    int nslots = 2;
+    xtg::WaveSlot slot[2];
+    cudaEvent_t admitted = nullptr;   // frames of admitted jobs allocated and zeroed
     std::vector<xtgpu_scene *> scenes;
     std::vector<xtg::DevScene> dev;
     std::map<int64_t, xtg::SvcJob> jobs;
@@ -48,8 +68,11 @@ struct xtgpu_service {
     int64_t next_id = 0;
     uint64_t mem_used = 0;
     std::chrono::steady_clock::time_point t0;
-    std::vector<unsigned long long> wave_rays;
     uint64_t waves = 0;
+    // host_results: pinned frames reused by size, events of copies in flight
+    std::multimap<uint64_t, float4 *> pinned_free;
+    std::vector<cudaEvent_t> events_free;
+    std::vector<int64_t> copying;    // finished on the GPU, host copy in flight
 
     double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
 };
@@ -81,6 +104,192 @@ static xtgpu_status admit(xtgpu_service *v, double now)
     return XTGPU_OK;
 }
 
+// Plans a wave over the admitted jobs' paths that no wave has taken yet and
+// launches it on slot W, its accumulate ordered behind prev_acc.
+//
+// Policy 0: jobs with the fewest remaining paths first, each taking what it
+// still needs up to the capacity left.  Small jobs finish in the next wave (low
+// latency); the largest share whatever remains, so the queue is always full
+// (throughput).  Policy 1: an equal share per running job, then the rest in
+// admission order.
+static xtgpu_status launch_wave(xtgpu_service *v, WaveSlot &W, cudaEvent_t prev_acc)
+{
+    const int64_t cap = W.R.cap;
+    W.wave.clear();
+    W.ids.clear();
+    int64_t left = cap;
+    const int n = (int)v->active.size();
+    std::vector<int> order(n);
+    for (int k = 0; k < n; ++k) order[k] = k;
+    std::vector<int64_t> take(n, 0);
+    if (v->o.policy == 1) {
+        const int64_t share = std::max<int64_t>(1, cap / n);
+        for (int k = 0; k < n && left > 0; ++k) {
+            SvcJob &J = v->jobs[v->active[k]];
+            take[k] = std::min<int64_t>({share, J.paths - J.planned, left});
+            left -= take[k];
+        }
+    } else {
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+            const SvcJob &A = v->jobs[v->active[a]], &B = v->jobs[v->active[b]];
+            return (A.paths - A.planned) < (B.paths - B.planned);
+        });
+    }
+    for (int k : order) {
+        if (left <= 0) break;
+        SvcJob &J = v->jobs[v->active[k]];
+        int64_t more = std::min<int64_t>(J.paths - J.planned - take[k], left);
+        take[k] += more;
+        left -= more;
+    }
+    int bounces = 0;
+    for (int k = 0; k < n; ++k) {
+        if (take[k] <= 0) continue;
+        SvcJob &J = v->jobs[v->active[k]];
+        DevJob dj{};
+        dj.integrator = J.d.integrator;
+        dj.width = J.d.width;
+        dj.height = J.d.height;
+        dj.spp = J.d.spp;
+        dj.rdepth = J.d.rdepth;
+        dj.ao_maxd = J.d.ao_max_distance;
+        dj.seed = J.d.seed;
+        dj.x0 = 0;
+        dj.y0 = 0;
+        dj.rw = J.d.width;
+        dj.rh = J.d.height;
+        dj.scene = J.d.scene;
+        dj.bounces = bounces_of(J.d.integrator, J.d.rdepth);
+        dj.tile = scene_tuning(v->scenes[J.d.scene]).tile;
+        dj.frame = J.frame;
+        dj.first = J.planned;
+        dj.count = take[k];
+        J.planned += take[k];
+        bounces = std::max(bounces, dj.bounces);
+        W.wave.push_back(dj);
+        W.ids.push_back(v->active[k]);
+    }
+    // launch configuration: the tuning of the scene with the most paths in the
+    // wave (its own if autotuned); the stack holds the deepest BVH the wave touches
+    {
+        std::vector<int64_t> per(v->scenes.size(), 0);
+        for (const DevJob &dj : W.wave) per[dj.scene] += dj.count;
+        int top = (int)(std::max_element(per.begin(), per.end()) - per.begin());
+        W.R.T = scene_tuning(v->scenes[top]);
+        int stack = 32;
+        for (size_t k = 0; k < per.size(); ++k)
+            if (per[k] > 0)
+                stack = std::max(stack, stack_for_depth(v->scenes[k]->depth, scene_tuning(v->scenes[k]).stack_entries));
+        W.R.stack = stack;
+    }
+    // frames of newly admitted jobs are allocated and zeroed on the service stream
+    XTG_CUDA(cudaEventRecord(v->admitted, v->s));
+    XTG_CUDA(cudaStreamWaitEvent(W.s, v->admitted, 0));
+    W.R.prev_acc = prev_acc;
+    XTG_TRY(W.R.run_wave(W.wave, bounces, v->o.node_format, v->o.use_graphs != 0, W.s));
+    XTG_CUDA(cudaMemcpyAsync(W.jrays, W.R.q.job_rays, sizeof(unsigned long long) * W.wave.size(),
+                             cudaMemcpyDeviceToHost, W.s));
+    XTG_CUDA(cudaEventRecord(W.fin, W.s));
+    ++v->waves;
+    return XTGPU_OK;
+}
+
+// Waits for the wave on slot W, credits its paths and rays to its jobs and
+// finishes the jobs it completed.  Waves retire in launch order, so a job is
+// complete once the wave that took its last paths retires.
+static xtgpu_status retire_wave(xtgpu_service *v, WaveSlot &W)
+{
+    XTG_CUDA(cudaEventSynchronize(W.fin));
+    XTG_TRY(W.R.collect_times(W.s));
+    double now = v->now();
+    for (size_t k = 0; k < W.ids.size(); ++k) {
+        SvcJob &J = v->jobs[W.ids[k]];
+        J.done += W.wave[k].count;
+        J.rays += W.jrays[k];
+        if (J.done < J.paths) continue;
+        J.render_done_s = now;
+        v->active.erase(std::find(v->active.begin(), v->active.end(), W.ids[k]));
+        if (v->o.host_results) {
+            // frame -> pinned host memory on the service stream; the device
+            // frame is freed behind the copy, so its budget is free at once
+            auto it = v->pinned_free.find(J.frame_bytes);
+            if (it != v->pinned_free.end()) {
+                J.host = it->second;
+                v->pinned_free.erase(it);
+            } else {
+                XTG_CUDA(cudaMallocHost((void **)&J.host, J.frame_bytes));
+            }
+            if (!v->events_free.empty()) {
+                J.copied = v->events_free.back();
+                v->events_free.pop_back();
+            } else {
+                XTG_CUDA(cudaEventCreateWithFlags(&J.copied, cudaEventDisableTiming));
+            }
+            XTG_CUDA(cudaMemcpyAsync(J.host, J.frame, J.frame_bytes, cudaMemcpyDeviceToHost, v->s));
+            XTG_CUDA(cudaFreeAsync(J.frame, v->s));
+            XTG_CUDA(cudaEventRecord(J.copied, v->s));
+            J.frame = nullptr;
+            v->mem_used -= J.frame_bytes;
+            v->copying.push_back(W.ids[k]);
+            continue;
+        }
+        J.state = 2;
+        J.finish_s = now;
+    }
+    W.wave.clear();
+    W.ids.clear();
+    return XTGPU_OK;
+}
+
+// Marks the jobs whose host copy has landed as done (all of them, waiting,
+// when wait is set); their finish time is when the copy was seen complete.
+static xtgpu_status finish_copies(xtgpu_service *v, bool wait)
+{
+    size_t keep = 0;
+    for (size_t k = 0; k < v->copying.size(); ++k) {
+        SvcJob &J = v->jobs[v->copying[k]];
+        cudaError_t e = wait ? cudaEventSynchronize(J.copied) : cudaEventQuery(J.copied);
+        if (e == cudaErrorNotReady) {
+            v->copying[keep++] = v->copying[k];
+            continue;
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "host copy of a finished frame", __FILE__, __LINE__);
+        v->events_free.push_back(J.copied);
+        J.copied = nullptr;
+        J.state = 2;
+        J.finish_s = v->now();
+    }
+    v->copying.resize(keep);
+    return XTGPU_OK;
+}
+
+// Waits for everything the service launched, frees its frames, runners,
+// streams and events, and deletes it.
+static void destroy_service(xtgpu_service *v)
+{
+    for (int k = 0; k < v->nslots; ++k)
+        if (v->slot[k].s) cudaStreamSynchronize(v->slot[k].s);
+    cudaStreamSynchronize(v->s);
+    for (auto &kv : v->jobs) {
+        if (kv.second.frame) cudaFreeAsync(kv.second.frame, v->s);
+        if (kv.second.host) cudaFreeHost(kv.second.host);
+        if (kv.second.copied) cudaEventDestroy(kv.second.copied);
+    }
+    cudaStreamSynchronize(v->s);
+    for (auto &kv : v->pinned_free) cudaFreeHost(kv.second);
+    for (cudaEvent_t e : v->events_free) cudaEventDestroy(e);
+    for (int k = 0; k < v->nslots; ++k) {
+        WaveSlot &W = v->slot[k];
+        W.R.release();
+        if (W.fin) cudaEventDestroy(W.fin);
+        if (W.jrays) cudaFreeHost(W.jrays);
+        if (W.s) cudaStreamDestroy(W.s);
+    }
+    if (v->admitted) cudaEventDestroy(v->admitted);
+    if (v->own_stream) cudaStreamDestroy(v->s);
+    delete v;
+}
+
 extern "C" {
 
 xtgpu_status xtgpu_service_create(const xtgpu_service_opts *opts, void *stream, xtgpu_service **out)
@@ -104,6 +313,12 @@ xtgpu_status xtgpu_service_create(const xtgpu_service_opts *opts, void *stream, 
     xtgpu_service *v = new xtgpu_service();
     v->o = *opts;
     v->s = (cudaStream_t)stream;
+    v->nslots = opts->waves_in_flight == 1 ? 1 : 2;
+    int64_t cap = opts->wave_paths > 0 ? opts->wave_paths : (1ll << 22);
+    auto fail = [&](xtgpu_status st) {
+        destroy_service(v);
+        return st;
+    };
     if (!v->s) {
         if (cudaStreamCreateWithFlags(&v->s, cudaStreamNonBlocking) != cudaSuccess) {
             delete v;
@@ -112,17 +327,24 @@ xtgpu_status xtgpu_service_create(const xtgpu_service_opts *opts, void *stream, 
         }
         v->own_stream = true;
     }
-    int64_t cap = opts->wave_paths > 0 ? opts->wave_paths : (1ll << 22);
-    xtgpu_status st = v->R.init(cap, opts->max_jobs, 64, v->s);
-    if (st != XTGPU_OK) {
-        v->R.release();
-        if (v->own_stream) cudaStreamDestroy(v->s);
-        delete v;
-        return st;
+    cudaError_t e0 = cudaEventCreateWithFlags(&v->admitted, cudaEventDisableTiming);
+    if (e0 != cudaSuccess) return fail(cuda_fail(e0, "xtgpu_service_create: cudaEventCreate", __FILE__, __LINE__));
+    for (int k = 0; k < v->nslots; ++k) {
+        WaveSlot &W = v->slot[k];
+        cudaError_t e = cudaStreamCreateWithFlags(&W.s, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&W.fin, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaMallocHost((void **)&W.jrays, sizeof(unsigned long long) * opts->max_jobs);
+        if (e != cudaSuccess) return fail(cuda_fail(e, "xtgpu_service_create: wave slot", __FILE__, __LINE__));
+        xtgpu_status st = W.R.init(cap, opts->max_jobs, 64, v->s);
+        if (st != XTGPU_OK) return fail(st);
+        W.R.enable_job_rays(true);
+        W.R.time_extend = opts->time_kernels != 0;
+        W.R.enable_stats(opts->count_visits != 0);
+        W.R.defer_acc = v->nslots > 1;
     }
-    v->R.enable_job_rays(true);
-    v->R.time_extend = opts->time_kernels != 0;
-    v->R.enable_stats(opts->count_visits != 0);
+    // queue buffers are zeroed on the service stream; waves run on the slots' streams
+    e0 = cudaStreamSynchronize(v->s);
+    if (e0 != cudaSuccess) return fail(cuda_fail(e0, "xtgpu_service_create: synchronize", __FILE__, __LINE__));
     v->t0 = std::chrono::steady_clock::now();
     *out = v;
     return XTGPU_OK;
@@ -144,7 +366,8 @@ xtgpu_status xtgpu_service_add_scene(xtgpu_service *v, xtgpu_scene *sc, int32_t 
     }
     v->scenes.push_back(sc);
     v->dev.push_back(sc->dev);
-    XTG_TRY(v->R.set_scenes(v->dev.data(), (int)v->dev.size(), v->s));
+    for (int k = 0; k < v->nslots; ++k) XTG_TRY(v->slot[k].R.set_scenes(v->dev.data(), (int)v->dev.size(), v->s));
+    XTG_CUDA(cudaStreamSynchronize(v->s));   // the slots' streams read the scene table
     *id = (int32_t)v->scenes.size() - 1;
     return XTGPU_OK;
 }
@@ -181,6 +404,75 @@ xtgpu_status xtgpu_service_submit(xtgpu_service *v, const xtgpu_job_desc *d, dou
     return XTGPU_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+static xtgpu_status run_loop(xtgpu_service *v, double max_seconds)
+{
+    const double t_end = max_seconds > 0 ? v->now() + max_seconds : 1e300;
+    // slots in flight, oldest first; `last` is the most recently launched one,
+    // whose accumulate the next wave's accumulate waits for
+    std::deque<int> flight;
+    int last = -1;
+    bool out_of_time = false;
+    while (true) {
+        double now = v->now();
+        if (!out_of_time) XTG_TRY(admit(v, now));
+        // 1. launch a wave if a slot is free and an admitted job has paths no
+        //    wave has taken yet
+        bool plannable = false;
+        if (!out_of_time && (int)flight.size() < v->nslots)
+            for (int64_t id : v->active) {
+                const SvcJob &J = v->jobs[id];
+                if (J.planned < J.paths) {
+                    plannable = true;
+                    break;
+                }
+            }
+        if (plannable) {
+            int k = 0;
+            while (k < v->nslots && std::find(flight.begin(), flight.end(), k) != flight.end()) ++k;
+            XTG_TRY(launch_wave(v, v->slot[k], last >= 0 ? v->slot[last].R.acc_done : nullptr));
+            flight.push_back(k);
+            last = k;
+            continue;
+        }
+        // 2. retire the oldest wave in flight
+        if (!flight.empty()) {
+            WaveSlot &W = v->slot[flight.front()];
+            flight.pop_front();
+            XTG_TRY(retire_wave(v, W));
+            XTG_TRY(finish_copies(v, false));
+            if (v->now() >= t_end) out_of_time = true;
+            continue;
+        }
+        if (out_of_time) return XTGPU_ERR_TIMEOUT;
+        // 3. nothing in flight and nothing to launch: wait for arrivals
+        if (!v->active.empty()) {
+            // every admitted job is fully planned and nothing is in flight
+            set_error("xtgpu_service_run: inconsistent job state");
+            return XTGPU_ERR_STATE;
+        }
+        if (v->pending.empty()) return XTGPU_OK;
+        double next = v->jobs[v->pending.front()].submit_s;
+        if (next > now) {
+            if (now >= t_end) return XTGPU_ERR_TIMEOUT;
+            double dt = std::min(next, t_end) - now;
+            std::this_thread::sleep_for(std::chrono::duration<double>(std::min(dt, 0.01)));
+            continue;
+        }
+        // the head job does not fit yet and nothing runs: cannot happen
+        // (admission only blocks on memory held by running jobs)
+        set_error("xtgpu_service_run: admission stalled");
+        return XTGPU_ERR_STATE;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
 xtgpu_status xtgpu_service_run(xtgpu_service *v, double max_seconds)
 {
     if (!v) {
@@ -191,128 +483,10 @@ xtgpu_status xtgpu_service_run(xtgpu_service *v, double max_seconds)
         set_error("xtgpu_service_run: no scene");
         return XTGPU_ERR_STATE;
     }
-    const double t_end = max_seconds > 0 ? v->now() + max_seconds : 1e300;
-    const int64_t cap = v->R.cap;
-    std::vector<DevJob> wave;
-    std::vector<int64_t> ids;
-    while (true) {
-        double now = v->now();
-        XTG_TRY(admit(v, now));
-        if (v->active.empty()) {
-            if (v->pending.empty()) return XTGPU_OK;
-            double next = v->jobs[v->pending.front()].submit_s;
-            if (next > now) {
-                if (now >= t_end) return XTGPU_ERR_TIMEOUT;
-                double dt = std::min(next, t_end) - now;
-                std::this_thread::sleep_for(std::chrono::duration<double>(std::min(dt, 0.01)));
-                continue;
-            }
-            // the head job does not fit yet and nothing runs: cannot happen
-            // (admission only blocks on memory held by running jobs)
-            set_error("xtgpu_service_run: admission stalled");
-            return XTGPU_ERR_STATE;
-        }
-        // plan the wave: jobs with the fewest remaining paths first, each taking
-        // what it still needs up to the capacity left.  Small jobs finish in the
-        // next wave (low latency); the largest share whatever remains, so the
-        // queue is always full (throughput).
-        wave.clear();
-        ids.clear();
-        int64_t left = cap;
-        int n = (int)v->active.size();
-        std::vector<int> order(n);
-        for (int k = 0; k < n; ++k) order[k] = k;
-        std::vector<int64_t> take(n, 0);
-        if (v->o.policy == 1) {
-            // equal share per running job, then the rest in admission order
-            const int64_t share = std::max<int64_t>(1, cap / n);
-            for (int k = 0; k < n && left > 0; ++k) {
-                SvcJob &J = v->jobs[v->active[k]];
-                take[k] = std::min<int64_t>({share, J.paths - J.done, left});
-                left -= take[k];
-            }
-        } else {
-            std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-                const SvcJob &A = v->jobs[v->active[a]], &B = v->jobs[v->active[b]];
-                return (A.paths - A.done) < (B.paths - B.done);
-            });
-        }
-        for (int k : order) {
-            if (left <= 0) break;
-            SvcJob &J = v->jobs[v->active[k]];
-            int64_t more = std::min<int64_t>(J.paths - J.done - take[k], left);
-            take[k] += more;
-            left -= more;
-        }
-        int bounces = 0;
-        for (int k = 0; k < n; ++k) {
-            if (take[k] <= 0) continue;
-            SvcJob &J = v->jobs[v->active[k]];
-            DevJob dj{};
-            dj.integrator = J.d.integrator;
-            dj.width = J.d.width;
-            dj.height = J.d.height;
-            dj.spp = J.d.spp;
-            dj.rdepth = J.d.rdepth;
-            dj.ao_maxd = J.d.ao_max_distance;
-            dj.seed = J.d.seed;
-            dj.x0 = 0;
-            dj.y0 = 0;
-            dj.rw = J.d.width;
-            dj.rh = J.d.height;
-            dj.scene = J.d.scene;
-            dj.bounces = bounces_of(J.d.integrator, J.d.rdepth);
-            dj.tile = scene_tuning(v->scenes[J.d.scene]).tile;
-            dj.frame = J.frame;
-            dj.first = J.done;
-            dj.count = take[k];
-            bounces = std::max(bounces, dj.bounces);
-            wave.push_back(dj);
-            ids.push_back(v->active[k]);
-        }
-        // launch configuration: the tuning of the scene with the most paths in
-        // the wave (its own if autotuned); the stack holds the deepest BVH the
-        // wave touches
-        {
-            std::vector<int64_t> per(v->scenes.size(), 0);
-            for (const DevJob &dj : wave) per[dj.scene] += dj.count;
-            int top = (int)(std::max_element(per.begin(), per.end()) - per.begin());
-            v->R.T = scene_tuning(v->scenes[top]);
-            int stack = 32;
-            for (size_t k = 0; k < per.size(); ++k)
-                if (per[k] > 0)
-                    stack = std::max(stack, stack_for_depth(v->scenes[k]->depth, scene_tuning(v->scenes[k]).stack_entries));
-            v->R.stack = stack;
-        }
-        XTG_TRY(v->R.run_wave(wave, bounces, v->o.node_format, v->o.use_graphs != 0, v->s));
-        v->wave_rays.resize(wave.size());
-        XTG_CUDA(cudaMemcpyAsync(v->wave_rays.data(), v->R.q.job_rays, sizeof(unsigned long long) * wave.size(),
-                                 cudaMemcpyDeviceToHost, v->s));
-        XTG_CUDA(cudaStreamSynchronize(v->s));
-        XTG_TRY(v->R.collect_times(v->s));
-        ++v->waves;
-        now = v->now();
-        for (size_t k = 0; k < ids.size(); ++k) {
-            SvcJob &J = v->jobs[ids[k]];
-            J.done += wave[k].count;
-            J.rays += v->wave_rays[k];
-            if (J.done >= J.paths) {
-                if (v->o.host_results) {
-                    J.host.resize((size_t)J.d.width * J.d.height);
-                    XTG_CUDA(cudaMemcpyAsync(J.host.data(), J.frame, J.frame_bytes, cudaMemcpyDeviceToHost, v->s));
-                    XTG_CUDA(cudaFreeAsync(J.frame, v->s));
-                    XTG_CUDA(cudaStreamSynchronize(v->s));
-                    J.frame = nullptr;
-                    v->mem_used -= J.frame_bytes;
-                    now = v->now();
-                }
-                J.state = 2;
-                J.finish_s = now;
-                v->active.erase(std::find(v->active.begin(), v->active.end(), ids[k]));
-            }
-        }
-        if (now >= t_end) return XTGPU_ERR_TIMEOUT;
-    }
+    xtgpu_status st = run_loop(v, max_seconds);
+    // host copies of finished frames still in flight land before returning
+    xtgpu_status cst = finish_copies(v, true);
+    return st != XTGPU_OK ? st : cst;
 }
 
 xtgpu_status xtgpu_service_poll(xtgpu_service *v, int64_t id, xtgpu_job_status *st)
@@ -332,6 +506,7 @@ xtgpu_status xtgpu_service_poll(xtgpu_service *v, int64_t id, xtgpu_job_status *
     st->submit_s = J.submit_s;
     st->start_s = J.start_s;
     st->finish_s = J.finish_s;
+    st->render_done_s = J.render_done_s;
     return XTGPU_OK;
 }
 
@@ -347,8 +522,8 @@ xtgpu_status xtgpu_service_result(xtgpu_service *v, int64_t id, float *rgba)
         return XTGPU_ERR_NOT_FOUND;
     }
     SvcJob &J = it->second;
-    if (J.state == 2 && !J.host.empty()) {
-        memcpy(rgba, J.host.data(), J.frame_bytes);
+    if (J.state == 2 && J.host) {
+        memcpy(rgba, J.host, J.frame_bytes);
         return XTGPU_OK;
     }
     if (J.state != 2 || !J.frame) {
@@ -357,6 +532,26 @@ xtgpu_status xtgpu_service_result(xtgpu_service *v, int64_t id, float *rgba)
     }
     XTG_CUDA(cudaMemcpyAsync(rgba, J.frame, J.frame_bytes, cudaMemcpyDeviceToHost, v->s));
     XTG_CUDA(cudaStreamSynchronize(v->s));
+    return XTGPU_OK;
+}
+
+xtgpu_status xtgpu_service_result_host(xtgpu_service *v, int64_t id, const float **rgba)
+{
+    if (!v || !rgba) {
+        set_error("xtgpu_service_result_host: NULL argument");
+        return XTGPU_ERR_INVALID;
+    }
+    auto it = v->jobs.find(id);
+    if (it == v->jobs.end()) {
+        set_error("xtgpu_service_result_host: unknown job");
+        return XTGPU_ERR_NOT_FOUND;
+    }
+    const SvcJob &J = it->second;
+    if (J.state != 2 || !J.host) {
+        set_error("xtgpu_service_result_host: no host copy (job not finished, released, or host_results off)");
+        return XTGPU_ERR_STATE;
+    }
+    *rgba = (const float *)J.host;
     return XTGPU_OK;
 }
 
@@ -381,7 +576,10 @@ xtgpu_status xtgpu_service_release(xtgpu_service *v, int64_t id)
         J.frame = nullptr;
         v->mem_used -= J.frame_bytes;
     }
-    std::vector<float4>().swap(J.host);
+    if (J.host) {
+        v->pinned_free.emplace(J.frame_bytes, J.host);
+        J.host = nullptr;
+    }
     return XTGPU_OK;
 }
 
@@ -391,16 +589,20 @@ xtgpu_status xtgpu_service_get_stats(xtgpu_service *v, xtgpu_service_stats *st)
         set_error("xtgpu_service_get_stats: NULL argument");
         return XTGPU_ERR_INVALID;
     }
-    unsigned long long rays = 0, sv[2] = {0, 0};
-    XTG_TRY(v->R.read_ctl(nullptr, &rays, v->s));
-    XTG_CUDA(cudaMemcpy(sv, v->R.statsbuf.p, 16, cudaMemcpyDeviceToHost));
-    st->rays = rays;
+    *st = xtgpu_service_stats{};
+    for (int k = 0; k < v->nslots; ++k) {
+        WaveRunner &R = v->slot[k].R;
+        unsigned long long rays = 0, sv[2] = {0, 0};
+        XTG_TRY(R.read_ctl(nullptr, &rays, v->slot[k].s));
+        XTG_CUDA(cudaMemcpy(sv, R.statsbuf.p, 16, cudaMemcpyDeviceToHost));
+        st->rays += rays;
+        st->kernel_launches += (uint64_t)R.launches;
+        st->extend_ms += R.extend_ms;
+        st->extend_launches += (uint64_t)R.extend_launches;
+        st->node_visits += sv[0];
+        st->prim_tests += sv[1];
+    }
     st->waves = v->waves;
-    st->kernel_launches = (uint64_t)v->R.launches;
-    st->extend_ms = v->R.extend_ms;
-    st->extend_launches = (uint64_t)v->R.extend_launches;
-    st->node_visits = sv[0];
-    st->prim_tests = sv[1];
     return XTGPU_OK;
 }
 
@@ -410,26 +612,22 @@ xtgpu_status xtgpu_service_reset_stats(xtgpu_service *v)
         set_error("xtgpu_service_reset_stats: NULL service");
         return XTGPU_ERR_INVALID;
     }
-    XTG_CUDA(cudaStreamSynchronize(v->s));
-    XTG_CUDA(cudaMemset((char *)v->R.ctlbuf.p + 32, 0, 8));
-    XTG_CUDA(cudaMemset(v->R.statsbuf.p, 0, 16));
+    for (int k = 0; k < v->nslots; ++k) {
+        WaveRunner &R = v->slot[k].R;
+        XTG_CUDA(cudaStreamSynchronize(v->slot[k].s));
+        XTG_CUDA(cudaMemset((char *)R.ctlbuf.p + 32, 0, 8));
+        XTG_CUDA(cudaMemset(R.statsbuf.p, 0, 16));
+        R.launches = 0;
+        R.extend_ms = 0.0;
+        R.extend_launches = 0;
+    }
     v->waves = 0;
-    v->R.launches = 0;
-    v->R.extend_ms = 0.0;
-    v->R.extend_launches = 0;
     return XTGPU_OK;
 }
 
 xtgpu_status xtgpu_service_destroy(xtgpu_service *v)
 {
-    if (!v) return XTGPU_OK;
-    cudaStreamSynchronize(v->s);
-    for (auto &kv : v->jobs)
-        if (kv.second.frame) cudaFreeAsync(kv.second.frame, v->s);
-    cudaStreamSynchronize(v->s);
-    v->R.release();
-    if (v->own_stream) cudaStreamDestroy(v->s);
-    delete v;
+    if (v) destroy_service(v);
     return XTGPU_OK;
 }
 

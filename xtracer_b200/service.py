@@ -15,9 +15,9 @@ class Service:
     def __init__(self, scenes, node_format: int = xtgpu.NODES_FP32, wave_paths: int = 0, use_graphs: bool = True,
                  merge_jobs: bool = True, memory_budget: int = 48 << 30, max_jobs: int = 512,
                  host_results: bool = False, time_kernels: bool = False, count_visits: bool = False,
-                 policy: int = 0, stream=None):
+                 policy: int = 0, waves_in_flight: int = 2, stream=None):
         o = xtgpu.ServiceOpts(memory_budget, max_jobs, wave_paths, node_format, int(use_graphs), int(merge_jobs),
-                              int(host_results), int(time_kernels), int(count_visits), policy)
+                              int(host_results), int(time_kernels), int(count_visits), policy, waves_in_flight)
         h = C.c_void_p()
         check(lib().xtgpu_service_create(C.byref(o), xtgpu.stream_handle(stream), C.byref(h)))
         self.handle = h
@@ -50,6 +50,16 @@ class Service:
             out = np.zeros((h, w, 4), np.float32)
         check(lib().xtgpu_service_result(self.handle, jid, out.ctypes.data_as(C.c_void_p)))
         return out
+
+    def result_view(self, jid: int) -> np.ndarray:
+        """The finished frame in the service's pinned host memory (host_results
+        services), as a read-only array without a copy; valid until release."""
+        h, w = self.shapes[jid]
+        p = C.POINTER(C.c_float)()
+        check(lib().xtgpu_service_result_host(self.handle, jid, C.byref(p)))
+        a = np.ctypeslib.as_array(p, shape=(h, w, 4))
+        a.flags.writeable = False
+        return a
 
     def release(self, jid: int) -> None:
         check(lib().xtgpu_service_release(self.handle, jid))

@@ -83,7 +83,7 @@ class ServiceOpts(C.Structure):
     _fields_ = [("memory_budget_bytes", C.c_uint64), ("max_jobs", C.c_int32), ("wave_paths", C.c_int64),
                 ("node_format", C.c_int32), ("use_graphs", C.c_int32), ("merge_jobs", C.c_int32),
                 ("host_results", C.c_int32), ("time_kernels", C.c_int32), ("count_visits", C.c_int32),
-                ("policy", C.c_int32)]
+                ("policy", C.c_int32), ("waves_in_flight", C.c_int32)]
 
 
 class ServiceStats(C.Structure):
@@ -119,7 +119,7 @@ class JobDesc(C.Structure):
 
 class JobStatus(C.Structure):
     _fields_ = [("state", C.c_int32), ("rays", C.c_uint64), ("submit_s", C.c_double), ("start_s", C.c_double),
-                ("finish_s", C.c_double)]
+                ("finish_s", C.c_double), ("render_done_s", C.c_double)]
 
 
 # Every entry point of include/xtgpu.h with its argument types.
@@ -143,6 +143,7 @@ SIGNATURES = {
     "xtgpu_service_run": [C.c_void_p, C.c_double],
     "xtgpu_service_poll": [C.c_void_p, C.c_int64, C.POINTER(JobStatus)],
     "xtgpu_service_result": [C.c_void_p, C.c_int64, C.c_void_p],
+    "xtgpu_service_result_host": [C.c_void_p, C.c_int64, C.POINTER(C.POINTER(C.c_float))],
     "xtgpu_service_release": [C.c_void_p, C.c_int64],
     "xtgpu_service_destroy": [C.c_void_p],
     "xtgpu_service_get_stats": [C.c_void_p, C.POINTER(ServiceStats)],
