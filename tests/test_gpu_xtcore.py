@@ -1,0 +1,74 @@
+"""The GPU integrator inside XTracer's own host: xtgpu-xtcore loads a .scn with
+io::scn::load, runs IIntegrator::render() (OpenMP tile loop, produce/pop
+contract) with xtcore::integrator::gpu::Integrator and assembles the tiles.
+
+* The frame equals, bit for bit, the C ABI's render of the generator's scene
+  (same seed): flattening and the tile plumbing lose nothing.
+* Depth and stencil agree with the reference's CPU integrators run by the same
+  binary on the same loaded Scene (primitive ties and grazing hits aside)."""
+import numpy as np
+import pytest
+
+from xtracer_b200 import scenes, xtgpu
+from tests import xtcore_host as xh
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not xh.available(), reason="xtgpu-xtcore not built (needs the XTracer sources)")]
+
+NAMES = {xtgpu.STENCIL: "stencil", xtgpu.DEPTH: "depth", xtgpu.AO: "ao", xtgpu.PATHTRACER: "pathtracer"}
+
+
+@pytest.fixture(scope="module", autouse=True)
+def cuda_device():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    torch.cuda.set_device(0)
+    xtgpu.lib()
+    yield
+
+
+@pytest.fixture(scope="module")
+def written(tmp_path_factory):
+    d = tmp_path_factory.mktemp("scn")
+    specs = [scenes.spheres_scene(64, seed=1, name="s64"), scenes.terrain_scene(5_000, seed=2, name="t5k"),
+             scenes.hairball_scene(3_000, seed=3, name="h3k")]
+    return [(s, s.write_scn(str(d))) for s in specs], d
+
+
+def render_host(scn, kind, w, h, spp, rdepth, out, *extra):
+    r = xh.run("render", scn, NAMES[kind], w, h, spp, rdepth, out, *extra)
+    assert r.returncode == 0, r.stdout + r.stderr
+    return xh.read_frame(out)
+
+
+@pytest.mark.parametrize("kind, spp, rdepth, extra", [
+    (xtgpu.STENCIL, 2, 1, ()), (xtgpu.DEPTH, 1, 1, ()), (xtgpu.AO, 4, 1, ()),
+    (xtgpu.AO, 4, 1, ("--ao-distance", "0.25")), (xtgpu.PATHTRACER, 4, 4, ()),
+    (xtgpu.PATHTRACER, 3, 4, ("--q8", "--seed", "7", "--tile", "16"))])
+def test_integrator_in_host_equals_c_abi(written, kind, spp, rdepth, extra):
+    specs, d = written
+    fmt = xtgpu.NODES_Q8 if "--q8" in extra else xtgpu.NODES_FP32
+    seed = int(extra[extra.index("--seed") + 1]) if "--seed" in extra else 1
+    aod = float(extra[extra.index("--ao-distance") + 1]) if "--ao-distance" in extra else 100.0
+    for spec, scn in specs:
+        got = render_host(scn, kind, 80, 56, spp, rdepth, d / ("%s.bin" % spec.name), *extra)
+        sc = xtgpu.Scene(spec, node_formats=(fmt,))
+        ref, _ = sc.render(kind, 80, 56, spp=spp, rdepth=rdepth, ao_max_distance=aod, seed=seed, node_format=fmt)
+        sc.close()
+        assert np.array_equal(got, ref), "%s %s differs through the xtcore host" % (spec.name, NAMES[kind])
+
+
+@pytest.mark.parametrize("kind", [xtgpu.STENCIL, xtgpu.DEPTH])
+def test_integrator_in_host_matches_reference_cpu_integrator(written, kind):
+    specs, d = written
+    for spec, scn in specs[:2]:
+        gpu = render_host(scn, kind, 64, 48, 1, 1, d / "g.bin")
+        cpu = render_host(scn, kind, 64, 48, 1, 1, d / "c.bin", "--cpu", "--threads", "4")
+        if kind == xtgpu.STENCIL:
+            bad = np.any(gpu != cpu, axis=2)
+        else:
+            bad = np.abs(gpu[..., 0] - cpu[..., 0]) > 1e-5 * np.maximum(np.abs(cpu[..., 0]), 1e-30)
+            bad |= gpu[..., 3] != cpu[..., 3]
+        # a mismatch is a hit/miss or primitive disagreement on a grazing ray
+        assert bad.sum() <= 2, "%s %s: %d pixels differ" % (spec.name, NAMES[kind], bad.sum())

@@ -1,0 +1,113 @@
+"""The xtcore-side Scene flattener (xtracer_b200/xtcore/gpu_integrator.cc) on
+scenes loaded by XTracer's own io::scn::load: the description it hands the C
+ABI equals the generator's, object by object, and what the GPU path cannot
+render is refused with a reason.  CPU only: flattening makes no CUDA call."""
+import os
+
+import numpy as np
+import pytest
+
+from xtracer_b200 import scenes
+from tests import xtcore_host as xh
+
+pytestmark = pytest.mark.skipif(not xh.available(), reason="xtgpu-xtcore not built (needs the XTracer sources)")
+
+
+def flatten(spec, tmp_path):
+    scn = spec.write_scn(str(tmp_path))
+    out = tmp_path / "flat.bin"
+    r = xh.run("flatten", scn, out)
+    assert r.returncode == 0, r.stderr
+    return xh.read_flat(out)
+
+
+@pytest.mark.parametrize("make", [lambda: scenes.spheres_scene(64, seed=1, name="s64"),
+                                  lambda: scenes.terrain_scene(5_000, seed=2, name="t5k"),
+                                  lambda: scenes.hairball_scene(3_000, seed=3, name="h3k"),
+                                  lambda: scenes.precision_scene(scale=0.002, seed=5)])
+def test_flattened_scene_equals_generator(make, tmp_path):
+    spec = make()
+    d = flatten(spec, tmp_path)
+    for key in ("obj_kind", "obj_first", "obj_count"):
+        assert np.array_equal(d[key], getattr(spec, key)), key
+    assert np.array_equal(d["spheres"], spec.spheres)
+    assert np.array_equal(d["planes"], spec.planes)
+    # mesh triangles come out of each Mesh's octree items, in OBJ face order
+    assert np.array_equal(d["tris"], spec.tris)
+    assert d["tri_normals"] is None
+    assert d["env_type"] == spec.env_type
+    assert np.array_equal(d["env_a"], np.float32(spec.env_a))
+    if spec.env_type == scenes.ENV_GRADIENT:
+        assert np.array_equal(d["env_b"], np.float32(spec.env_b))
+    cam = spec.camera
+    assert np.array_equal(d["camera"], np.float32(list(cam.position) + list(cam.target) + list(cam.up) + [cam.fov]))
+    for oi in range(len(spec.obj_kind)):
+        t, row = d["materials"][d["obj_material"][oi]]
+        m = spec.materials[spec.obj_material[oi]]
+        assert t == m.type, oi
+        assert np.array_equal(row, xh.material_row(m)), oi
+
+
+SCN_HEAD = """title = t
+version = 1.0
+camera = {
+  default = {
+    type = thin-lens
+    position = vec3(0,1,-5)
+    target = vec3(0,0,0)
+    up = vec3(0,1,0)
+    fov = 60
+%s  }
+}
+geometry = {
+  g0 = {
+    type = %s
+    position = vec3(0,0,0)
+    radius = 1
+  }
+}
+material = {
+  m0 = {
+    type = lambert
+    properties = {
+      samplers = {
+        diffuse = {
+%s
+        }
+      }
+    }
+  }
+}
+object = {
+  o0 = {
+    geometry = g0
+    material = m0
+  }
+}
+"""
+COLOUR = "          type = color\n          value = col3(0.5,0.5,0.5)"
+TEXTURE = "          type = texture\n          source = missing.png"
+
+
+@pytest.mark.parametrize("extra, geom, sampler, why", [
+    ("    flength = 2\n    aperture = 0.1\n", "sphere", COLOUR, "depth of field"),
+    ("", "sphere", TEXTURE, "not a solid colour"),
+])
+def test_unsupported_features_are_refused(tmp_path, extra, geom, sampler, why):
+    scn = tmp_path / "u.scn"
+    scn.write_text(SCN_HEAD % (extra, geom, sampler))
+    r = xh.run("flatten", scn, tmp_path / "f.bin")
+    assert r.returncode == 1
+    assert why in r.stderr
+
+
+def test_point_geometry_is_a_zero_radius_sphere(tmp_path):
+    """The loader makes `point` geometry a Sphere of radius 0
+    (parseutil.cc:379-383); the flattener passes it on as such."""
+    scn = tmp_path / "p.scn"
+    scn.write_text((SCN_HEAD % ("", "point", COLOUR)).replace("    radius = 1\n", ""))
+    r = xh.run("flatten", scn, tmp_path / "f.bin")
+    assert r.returncode == 0, r.stderr
+    d = xh.read_flat(tmp_path / "f.bin")
+    assert d["obj_kind"].tolist() == [scenes.SPHERE]
+    assert d["spheres"].tolist() == [[0.0, 0.0, 0.0, 0.0]]

@@ -1,0 +1,346 @@
+// GPU integrator for XTracer's xtcore and the Scene flattener behind it.
+#include "gpu_integrator.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <map>
+
+#include <xtcore/log.h>
+#include <xtcore/mesh.h>
+#include <xtcore/octree.h>
+#include <xtcore/material.h>
+#include <xtcore/sampler_col.h>
+#include <xtcore/sampler_gradient.h>
+#include <xtcore/camera/perspective.h>
+#include <xtcore/math/sphere.h>
+#include <xtcore/math/plane.h>
+#include <xtcore/math/triangle.h>
+#include <xtcore/matdefs.h>
+
+namespace {
+
+// The triangles of a Mesh live in its private Octree (src/xtcore/mesh.h:38,
+// octree.h:61-63), in OBJ face order: m_items is filled by Octree::add in the
+// loop of Mesh::build_octree (mesh.cc:70-113).  Inside the XTracer tree a
+// maintainer adds a public accessor to Mesh; built against an unmodified tree,
+// the members are reached through explicit template instantiation, for which
+// C++ does not apply access checks ([temp.explicit]).
+typedef xtcore::Octree<xtcore::surface::Triangle> TriOctree;
+typedef std::vector<xtcore::OctreeItem<xtcore::surface::Triangle> > TriItems;
+
+template <typename Tag, typename Tag::type Member>
+struct Expose {
+    friend typename Tag::type member_of(Tag) { return Member; }
+};
+struct MeshOctreeTag {
+    typedef TriOctree xtcore::surface::Mesh::*type;
+    friend type member_of(MeshOctreeTag);
+};
+struct OctreeItemsTag {
+    typedef TriItems TriOctree::*type;
+    friend type member_of(OctreeItemsTag);
+};
+template struct Expose<MeshOctreeTag, &xtcore::surface::Mesh::m_octree>;
+template struct Expose<OctreeItemsTag, &TriOctree::m_items>;
+
+const TriItems &mesh_triangles(const xtcore::surface::Mesh *m)
+{
+    const TriOctree &oct = m->*member_of(MeshOctreeTag());
+    return oct.*member_of(OctreeItemsTag());
+}
+
+void put3(std::vector<float> &v, const nmath::Vector3f &p)
+{
+    v.push_back((float)p.x);
+    v.push_back((float)p.y);
+    v.push_back((float)p.z);
+}
+
+// A material sampler as a constant colour: absent samplers are black, as in
+// IMaterial::get_sample (material.cc:65-70); only SolidColor samplers are
+// constant, any other kind (textures, cubemaps) fails the flattening.
+bool solid_colour(const xtcore::asset::IMaterial *m, const char *name, float out[3], std::string &err)
+{
+    out[0] = out[1] = out[2] = 0.f;
+    for (size_t i = 0; i < m->get_sampler_count(); ++i) {
+        std::string n;
+        xtcore::sampler::ISampler *s = const_cast<xtcore::asset::IMaterial *>(m)->get_sampler_by_index(i, &n);
+        if (n != name) continue;
+        if (!dynamic_cast<xtcore::sampler::SolidColor *>(s)) {
+            err = std::string("material sampler '") + name + "' is not a solid colour";
+            return false;
+        }
+        nimg::ColorRGBf c = s->sample(nmath::Vector3f(0, 0, 0));
+        out[0] = c.r();
+        out[1] = c.g();
+        out[2] = c.b();
+        return true;
+    }
+    return true;
+}
+
+bool material_of(const xtcore::asset::IMaterial *m, xtgpu_material &out, std::string &err)
+{
+    using namespace xtcore::asset::material;
+    out = xtgpu_material();
+    if (dynamic_cast<const BlinnPhong *>(m)) out.type = XTGPU_BLINNPHONG;
+    else if (dynamic_cast<const Phong *>(m)) out.type = XTGPU_PHONG;
+    else if (dynamic_cast<const Lambert *>(m)) out.type = XTGPU_LAMBERT;
+    else if (dynamic_cast<const Emissive *>(m)) out.type = XTGPU_EMISSIVE;
+    else if (dynamic_cast<const Dielectric *>(m)) out.type = XTGPU_DIELECTRIC;
+    else {
+        err = "unknown material class";
+        return false;
+    }
+    if (!solid_colour(m, MAT_SAMPLER_DIFFUSE, out.diffuse, err)) return false;
+    if (!solid_colour(m, MAT_SAMPLER_SPECULAR, out.specular, err)) return false;
+    if (!solid_colour(m, MAT_SAMPLER_EMISSIVE, out.emissive, err)) return false;
+    out.reflectance = m->get_scalar(MAT_SCALART_REFLECTANCE);
+    out.exponent = m->get_scalar(MAT_SCALART_EXPONENT);
+    out.ior = m->get_scalar(MAT_SCALART_IOR);
+    return true;
+}
+
+}  // namespace
+
+namespace xtcore {
+    namespace integrator {
+        namespace gpu {
+
+xtgpu_status flatten(xtcore::Scene &scene, HASH_UINT64 camera, FlatScene &F, std::string &err)
+{
+    F = FlatScene();
+    auto fail = [&](const std::string &why) {
+        err = why;
+        return XTGPU_ERR_INVALID;
+    };
+    // Geometry is grouped by kind in the description (spheres, planes and
+    // triangles each in one array) while the objects keep the map order.
+    std::map<HASH_UINT64, int32_t> mat_index;
+    for (auto it = scene.m_objects.begin(); it != scene.m_objects.end(); ++it) {
+        const xtcore::asset::Object *obj = it->second;
+        if (!obj) continue;
+        auto gs = scene.m_surface.find(obj->surface);
+        // Scene::intersection skips objects whose surface is missing
+        if (gs == scene.m_surface.end() || !gs->second) continue;
+        const xtcore::asset::ISurface *g = gs->second;
+        int32_t kind, first, count = 1;
+        if (const xtcore::surface::Sphere *s = dynamic_cast<const xtcore::surface::Sphere *>(g)) {
+            kind = XTGPU_SPHERE;
+            first = (int32_t)(F.spheres.size() / 4);
+            put3(F.spheres, s->origin);
+            F.spheres.push_back((float)s->radius);
+        } else if (const xtcore::surface::Plane *p = dynamic_cast<const xtcore::surface::Plane *>(g)) {
+            kind = XTGPU_PLANE;
+            first = (int32_t)(F.planes.size() / 4);
+            put3(F.planes, p->normal);
+            F.planes.push_back((float)p->offset);
+        } else if (const xtcore::surface::Triangle *t = dynamic_cast<const xtcore::surface::Triangle *>(g)) {
+            kind = XTGPU_MESH;
+            first = (int32_t)(F.tris.size() / 9);
+            for (int k = 0; k < 3; ++k) put3(F.tris, t->v[k]);
+            for (int k = 0; k < 3; ++k) {
+                put3(F.tri_normals, t->n[k]);
+                F.has_normals |= t->n[k].x != 0 || t->n[k].y != 0 || t->n[k].z != 0;
+            }
+        } else if (const xtcore::surface::Mesh *m = dynamic_cast<const xtcore::surface::Mesh *>(g)) {
+            kind = XTGPU_MESH;
+            first = (int32_t)(F.tris.size() / 9);
+            const TriItems &items = mesh_triangles(m);
+            count = (int32_t)items.size();
+            for (size_t i = 0; i < items.size(); ++i) {
+                const xtcore::surface::Triangle &t = items[i].data;
+                for (int k = 0; k < 3; ++k) put3(F.tris, t.v[k]);
+                for (int k = 0; k < 3; ++k) {
+                    put3(F.tri_normals, t.n[k]);
+                    F.has_normals |= t.n[k].x != 0 || t.n[k].y != 0 || t.n[k].z != 0;
+                }
+            }
+            if (count == 0) continue;   // an empty mesh is never hit
+        } else {
+            return fail("unsupported surface class");
+        }
+        // material: shared entries per material id; an object without one
+        // gets a black Lambert (the CPU pathtracer dereferences it unchecked)
+        int32_t mi;
+        auto known = mat_index.find(obj->material);
+        if (known != mat_index.end()) {
+            mi = known->second;
+        } else {
+            xtgpu_material gm = xtgpu_material();
+            gm.type = XTGPU_LAMBERT;
+            auto ms = scene.m_materials.find(obj->material);
+            if (ms != scene.m_materials.end() && ms->second && !material_of(ms->second, gm, err)) return XTGPU_ERR_INVALID;
+            mi = (int32_t)F.materials.size();
+            F.materials.push_back(gm);
+            mat_index[obj->material] = mi;
+        }
+        F.obj_kind.push_back(kind);
+        F.obj_first.push_back(first);
+        F.obj_count.push_back(count);
+        F.obj_material.push_back(mi);
+        F.obj_id.push_back(it->first);
+    }
+    if (F.tris.size() / 9 > (size_t)INT32_MAX / 4) return fail("too many triangles");
+
+    xtgpu_scene_desc &d = F.desc;
+    d = xtgpu_scene_desc();
+    d.n_objects = (int32_t)F.obj_kind.size();
+    d.obj_kind = F.obj_kind.data();
+    d.obj_first = F.obj_first.data();
+    d.obj_count = F.obj_count.data();
+    d.obj_material = F.obj_material.data();
+    d.n_spheres = (int32_t)(F.spheres.size() / 4);
+    d.spheres = F.spheres.data();
+    d.n_planes = (int32_t)(F.planes.size() / 4);
+    d.planes = F.planes.data();
+    d.n_tris = (int32_t)(F.tris.size() / 9);
+    d.tris = F.tris.data();
+    d.tri_normals = F.has_normals ? F.tri_normals.data() : 0;
+    d.n_materials = (int32_t)F.materials.size();
+    d.materials = F.materials.data();
+
+    // environment (Scene::sample_environment, scene.cc:142-145)
+    d.env_type = XTGPU_ENV_NONE;
+    if (scene.m_environment) {
+        if (xtcore::sampler::Gradient *gr = dynamic_cast<xtcore::sampler::Gradient *>(scene.m_environment)) {
+            d.env_type = XTGPU_ENV_GRADIENT;
+            d.env_a[0] = gr->a.r(); d.env_a[1] = gr->a.g(); d.env_a[2] = gr->a.b();
+            d.env_b[0] = gr->b.r(); d.env_b[1] = gr->b.g(); d.env_b[2] = gr->b.b();
+        } else if (dynamic_cast<xtcore::sampler::SolidColor *>(scene.m_environment)) {
+            d.env_type = XTGPU_ENV_COLOR;
+            nimg::ColorRGBf c = scene.m_environment->sample(nmath::Vector3f(0, 0, 0));
+            d.env_a[0] = c.r(); d.env_a[1] = c.g(); d.env_a[2] = c.b();
+        } else {
+            return fail("unsupported environment sampler");
+        }
+    }
+
+    // camera (Perspective::get_primary_ray, camera/perspective.cc:38-98)
+    xtcore::asset::ICamera *cam = scene.get_camera(camera);
+    if (!cam) return fail("no camera");
+    xtcore::camera::Perspective *pc = dynamic_cast<xtcore::camera::Perspective *>(cam);
+    if (!pc) return fail(std::string("unsupported camera type ") + cam->get_type());
+    if (pc->flength > 0) return fail("depth of field (flength > 0) is not supported");
+    auto set3 = [](float *o, const nmath::Vector3f &v) {
+        o[0] = (float)v.x;
+        o[1] = (float)v.y;
+        o[2] = (float)v.z;
+    };
+    set3(d.camera.position, pc->position);
+    set3(d.camera.target, pc->target);
+    set3(d.camera.up, pc->up);
+    d.camera.fov = pc->fov;
+    return XTGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+Integrator::Integrator(int kind, int node_format)
+    : ao_max_distance(100.f), seed(1), m_kind(kind), m_format(node_format), m_scene(0), m_uploaded(0),
+      m_x0(0), m_y0(0), m_w(0), m_h(0), m_served(0), m_ready(false), m_status(XTGPU_OK), m_rays(0)
+{}
+
+Integrator::~Integrator()
+{
+    if (m_scene) xtgpu_scene_destroy(m_scene);
+}
+
+void Integrator::invalidate_scene()
+{
+    std::lock_guard<std::mutex> lock(m_mutex);
+    m_uploaded = 0;
+}
+
+xtgpu_status Integrator::render_frame()
+{
+    xtcore::render::params_t &p = ctx->params;
+    if (p.aa != 1 || p.sample_distribution != xtcore::antialiasing::SAMPLE_DISTRIBUTION_GRID) {
+        m_error = "only aa = 1 with the grid sample distribution is supported";
+        return XTGPU_ERR_INVALID;
+    }
+    if (!m_scene || m_uploaded != &ctx->scene) {
+        FlatScene F;
+        xtgpu_status st = flatten(ctx->scene, p.camera, F, m_error);
+        if (st != XTGPU_OK) return st;
+        if (m_scene) xtgpu_scene_destroy(m_scene);
+        m_scene = 0;
+        if ((st = xtgpu_scene_create(&F.desc, 0, &m_scene)) != XTGPU_OK) {
+            m_error = xtgpu_last_error();
+            return st;
+        }
+        xtgpu_bvh_opts o = {m_format, 0};
+        if ((st = xtgpu_bvh_build(m_scene, &o, 0)) != XTGPU_OK) {
+            m_error = xtgpu_last_error();
+            return st;
+        }
+        m_uploaded = &ctx->scene;
+    }
+    // bounding rectangle of the context's tiles
+    size_t x0 = (size_t)-1, y0 = (size_t)-1, x1 = 0, y1 = 0;
+    for (size_t i = 0; i < ctx->tiles.size(); ++i) {
+        const xtcore::render::tile_t &t = ctx->tiles[i];
+        x0 = std::min(x0, t.x0());
+        y0 = std::min(y0, t.y0());
+        x1 = std::max(x1, t.x1());
+        y1 = std::max(y1, t.y1());
+    }
+    if (x1 <= x0 || y1 <= y0) {
+        m_error = "no tiles";
+        return XTGPU_ERR_INVALID;
+    }
+    xtgpu_render_params rp = xtgpu_render_params();
+    rp.integrator = m_kind;
+    rp.width = (int32_t)p.width;
+    rp.height = (int32_t)p.height;
+    rp.spp = (int32_t)p.samples;
+    rp.rdepth = (int32_t)p.rdepth;
+    rp.ao_max_distance = ao_max_distance;
+    rp.seed = seed;
+    rp.node_format = m_format;
+    rp.x0 = (int32_t)x0;
+    rp.y0 = (int32_t)y0;
+    rp.x1 = (int32_t)x1;
+    rp.y1 = (int32_t)y1;
+    m_x0 = x0;
+    m_y0 = y0;
+    m_w = x1 - x0;
+    m_h = y1 - y0;
+    m_frame.assign(4 * m_w * m_h, 0.f);
+    xtgpu_status st = xtgpu_render_host(m_scene, &rp, m_frame.data(), &m_rays, 0);
+    if (st != XTGPU_OK) m_error = xtgpu_last_error();
+    return st;
+}
+
+void Integrator::render_tile(xtcore::render::tile_t *tile)
+{
+    {
+        std::lock_guard<std::mutex> lock(m_mutex);
+        if (!m_ready) {
+            m_error.clear();
+            m_rays = 0;
+            m_status = render_frame();
+            if (m_status != XTGPU_OK)
+                xtcore::Log::handle().post_warning("gpu integrator: %s", m_error.c_str());
+            m_served = 0;
+            m_ready = true;
+        }
+    }
+    // the produce/pop contract: every sample the tile was given is consumed
+    while (tile->samples.count() > 0) {
+        xtcore::antialiasing::sample_rgba_t s;
+        tile->samples.pop(s);
+    }
+    if (m_status == XTGPU_OK) {
+        for (size_t y = tile->y0(); y < tile->y1(); ++y)
+            for (size_t x = tile->x0(); x < tile->x1(); ++x) {
+                const float *c = &m_frame[4 * ((y - m_y0) * m_w + (x - m_x0))];
+                tile->write(x, y, nimg::ColorRGBAf(c[0], c[1], c[2], c[3]));
+            }
+    }
+    std::lock_guard<std::mutex> lock(m_mutex);
+    if (++m_served >= ctx->tiles.size()) m_ready = false;
+}
+
+        } /* namespace gpu */
+    } /* namespace integrator */
+} /* namespace xtcore */

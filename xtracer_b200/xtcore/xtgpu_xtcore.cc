@@ -1,0 +1,223 @@
+// xtgpu-xtcore: a minimal XTracer front end that renders a .scn through the
+// reference host (io::scn::load, params, tiles, IIntegrator::render, assemble)
+// with the GPU integrator, or with one of the reference's CPU integrators for
+// comparison, as the GUI does it (src/frontend/gui/workspace.cc:55-81).
+//
+//   xtgpu-xtcore render <scn> <integrator> W H spp rdepth <out.bin> [options]
+//       integrator: stencil | depth | ao | pathtracer
+//       --cpu          the reference's CPU integrator instead of the GPU one
+//       --q8           8-bit quantised BVH nodes (GPU)
+//       --seed N       sample stream key (GPU), default 1
+//       --ao-distance D  AO occlusion distance (GPU), default 100
+//       --threads N    OpenMP threads of the tile loop, default all
+//       --tile N       tile size, default 32 (context.cc:5)
+//   xtgpu-xtcore flatten <scn> <out.bin>
+//       writes the flattened scene description (see write_flat)
+//
+// render writes int32 width, height, then width*height RGBA float32 pixels,
+// row-major (the assembled Pixmap), and prints one JSON line.
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <omp.h>
+
+#include <xtcore/xtcore.h>
+#include <xtcore/log.h>
+#include <xtcore/context.h>
+#include <xtcore/integrator.h>
+#include <xtcore/parseutil.h>
+
+#include "gpu_integrator.h"
+
+namespace {
+
+int load(xtcore::render::context_t &ctx, const char *scn)
+{
+    xtcore::Log::handle().echo(false);
+    if (xtcore::io::scn::load(&ctx.scene, scn, 0)) {
+        fprintf(stderr, "xtgpu-xtcore: failed to load %s\n", scn);
+        return 1;
+    }
+    if (ctx.scene.m_cameras.empty()) {
+        fprintf(stderr, "xtgpu-xtcore: no camera in %s\n", scn);
+        return 1;
+    }
+    // the GUI's fallback (gui/workspace.cc:33-39): the first camera
+    ctx.params.camera = ctx.scene.m_cameras.begin()->first;
+    return 0;
+}
+
+template <typename T>
+void put(FILE *f, const T *p, size_t n)
+{
+    if (n) fwrite(p, sizeof(T), n, f);
+}
+
+// int32 n_objects, n_spheres, n_planes, n_tris, n_materials, has_normals,
+// env_type; int32 obj_kind/first/count/material [n_objects each]; float32
+// spheres [4n], planes [4n], tris [9n], tri_normals [9n] when has_normals;
+// per material int32 type + float32 diffuse[3] specular[3] emissive[3]
+// reflectance exponent ior; float32 env_a[3] env_b[3]; float32 camera
+// position[3] target[3] up[3] fov.
+int write_flat(const xtcore::integrator::gpu::FlatScene &F, const char *out)
+{
+    const xtgpu_scene_desc &d = F.desc;
+    FILE *f = fopen(out, "wb");
+    if (!f) return 1;
+    int32_t head[7] = {d.n_objects, d.n_spheres, d.n_planes, d.n_tris, d.n_materials, d.tri_normals ? 1 : 0,
+                       d.env_type};
+    put(f, head, 7);
+    put(f, d.obj_kind, (size_t)d.n_objects);
+    put(f, d.obj_first, (size_t)d.n_objects);
+    put(f, d.obj_count, (size_t)d.n_objects);
+    put(f, d.obj_material, (size_t)d.n_objects);
+    put(f, d.spheres, 4 * (size_t)d.n_spheres);
+    put(f, d.planes, 4 * (size_t)d.n_planes);
+    put(f, d.tris, 9 * (size_t)d.n_tris);
+    if (d.tri_normals) put(f, d.tri_normals, 9 * (size_t)d.n_tris);
+    for (int32_t i = 0; i < d.n_materials; ++i) {
+        const xtgpu_material &m = d.materials[i];
+        put(f, &m.type, 1);
+        put(f, m.diffuse, 3);
+        put(f, m.specular, 3);
+        put(f, m.emissive, 3);
+        float sc[3] = {m.reflectance, m.exponent, m.ior};
+        put(f, sc, 3);
+    }
+    put(f, d.env_a, 3);
+    put(f, d.env_b, 3);
+    put(f, d.camera.position, 3);
+    put(f, d.camera.target, 3);
+    put(f, d.camera.up, 3);
+    put(f, &d.camera.fov, 1);
+    fclose(f);
+    return 0;
+}
+
+int mode_flatten(int argc, char **argv)
+{
+    if (argc < 4) return 2;
+    xtcore::init();
+    xtcore::render::context_t ctx;
+    if (load(ctx, argv[2])) return 1;
+    xtcore::integrator::gpu::FlatScene F;
+    std::string err;
+    if (xtcore::integrator::gpu::flatten(ctx.scene, ctx.params.camera, F, err) != XTGPU_OK) {
+        fprintf(stderr, "xtgpu-xtcore: %s\n", err.c_str());
+        return 1;
+    }
+    return write_flat(F, argv[3]);
+}
+
+int mode_render(int argc, char **argv)
+{
+    if (argc < 9) return 2;
+    const char *scn = argv[2];
+    std::string integ = argv[3];
+    size_t w = strtoul(argv[4], 0, 10), h = strtoul(argv[5], 0, 10);
+    size_t spp = strtoul(argv[6], 0, 10), rdepth = strtoul(argv[7], 0, 10);
+    const char *out = argv[8];
+    bool cpu = false, q8 = false;
+    unsigned long long seed = 1;
+    float aod = 100.f;
+    size_t threads = 0, tile = 32;
+    for (int i = 9; i < argc; ++i) {
+        std::string a = argv[i];
+        if (a == "--cpu") cpu = true;
+        else if (a == "--q8") q8 = true;
+        else if (a == "--seed" && i + 1 < argc) seed = strtoull(argv[++i], 0, 10);
+        else if (a == "--ao-distance" && i + 1 < argc) aod = (float)atof(argv[++i]);
+        else if (a == "--threads" && i + 1 < argc) threads = strtoul(argv[++i], 0, 10);
+        else if (a == "--tile" && i + 1 < argc) tile = strtoul(argv[++i], 0, 10);
+        else {
+            fprintf(stderr, "xtgpu-xtcore: unknown option %s\n", a.c_str());
+            return 2;
+        }
+    }
+    if (!w || !h || !spp || !tile) return 2;
+
+    xtcore::init();
+    xtcore::render::context_t ctx;
+    if (load(ctx, scn)) return 1;
+    ctx.params.width = w;
+    ctx.params.height = h;
+    ctx.params.samples = spp;
+    ctx.params.rdepth = rdepth;
+    ctx.params.threads = threads;
+    ctx.params.tile_size = tile;
+    ctx.init();   // segments the frame into tiles (context.cc)
+
+    xtcore::render::IIntegrator *ig = 0;
+    xtcore::integrator::gpu::Integrator *gi = 0;
+    int kind = integ == "stencil" ? XTGPU_STENCIL : integ == "depth" ? XTGPU_DEPTH : integ == "ao" ? XTGPU_AO
+             : integ == "pathtracer" ? XTGPU_PATHTRACER : -1;
+    if (kind < 0) {
+        fprintf(stderr, "xtgpu-xtcore: unknown integrator %s\n", integ.c_str());
+        return 2;
+    }
+    if (cpu) {
+        if (kind == XTGPU_STENCIL) ig = new xtcore::integrator::stencil::Integrator();
+        else if (kind == XTGPU_DEPTH) ig = new xtcore::integrator::depth::Integrator();
+        else if (kind == XTGPU_AO) ig = new xtcore::integrator::ao::Integrator();
+        else ig = new xtcore::integrator::pathtracer::Integrator();
+    } else {
+        gi = new xtcore::integrator::gpu::Integrator(kind, q8 ? XTGPU_NODES_Q8 : XTGPU_NODES_FP32);
+        gi->seed = seed;
+        gi->ao_max_distance = aod;
+        ig = gi;
+    }
+    ig->setup(ctx);
+    auto t0 = std::chrono::steady_clock::now();
+    ig->render();
+    auto t1 = std::chrono::steady_clock::now();
+    double secs = std::chrono::duration<double>(t1 - t0).count();
+
+    nimg::Pixmap pm;
+    xtcore::render::assemble(pm, ctx);
+    FILE *f = fopen(out, "wb");
+    if (!f) return 1;
+    int32_t wh[2] = {(int32_t)w, (int32_t)h};
+    put(f, wh, 2);
+    std::vector<float> row(4 * w);
+    for (size_t y = 0; y < h; ++y) {
+        for (size_t x = 0; x < w; ++x) {
+            const nimg::ColorRGBAf &c = pm.pixel_ro(x, y);
+            row[4 * x] = c.r();
+            row[4 * x + 1] = c.g();
+            row[4 * x + 2] = c.b();
+            row[4 * x + 3] = c.a();
+        }
+        put(f, row.data(), row.size());
+    }
+    fclose(f);
+    int rc = 0;
+    if (gi) {
+        printf("{\"integrator\": \"gpu:%s\", \"render_s\": %.9f, \"rays\": %llu, \"status\": %d, \"error\": \"%s\"}\n",
+               integ.c_str(), secs, (unsigned long long)gi->rays(), (int)gi->status(), gi->error().c_str());
+        rc = gi->status() == XTGPU_OK ? 0 : 1;
+    } else {
+        printf("{\"integrator\": \"cpu:%s\", \"render_s\": %.9f, \"threads\": %d}\n", integ.c_str(), secs,
+               threads ? (int)threads : omp_get_max_threads());
+    }
+    delete ig;
+    return rc;
+}
+
+}  // namespace
+
+int main(int argc, char **argv)
+{
+    if (argc < 2) {
+        fprintf(stderr, "usage: xtgpu-xtcore render|flatten ...\n");
+        return 2;
+    }
+    std::string m = argv[1];
+    int rc = 2;
+    if (m == "render") rc = mode_render(argc, argv);
+    else if (m == "flatten") rc = mode_flatten(argc, argv);
+    if (rc == 2) fprintf(stderr, "xtgpu-xtcore: bad arguments\n");
+    return rc;
+}
