@@ -1,0 +1,163 @@
+"""Parity at the full sizes of the benchmark configurations.
+
+* Pathtracer, 64 spheres + plane, 256x256, 16 spp, depth 4: per-pixel RMSE
+  against a converged 4096-spp frame equals the oracle's at equal spp (the
+  oracle restates the reference and is pinned to it by the golden fixtures).
+* Depth + stencil, 999,698-triangle terrain, 1920x1080, 1 spp: primary hits on
+  every 8th pixel in x and y against the FP64 oracle (every disagreement a tie
+  or a grazing hit), depth values within 1e-5, and the Q8 frames equal to the
+  FP32 frames.
+* AO, 2M-triangle hairball, 1024x1024, 64 spp, distance 0.2: against the
+  oracle on the same random stream, per ray (1 spp, every 4th pixel) and per
+  pixel (64 spp, a 32x32 lattice); Q8 frame equal to FP32.
+* Precision scene, 8M triangles, Phong/Blinn-Phong, sphere and mesh lights:
+  primary hits of FP32 and Q8 nodes against the FP64 oracle on every 8th pixel,
+  and the 1920x1080, 256-spp, depth-8 pathtracer frame with Q8 nodes equal to
+  the one with FP32 nodes (hence equal RMSE).
+"""
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+from tests import parity
+from xtracer_b200 import scenes, xtgpu
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def cuda_device():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    torch.cuda.set_device(0)
+    xtgpu.lib()
+    yield
+
+
+def lattice(w, h, step):
+    ys, xs = np.mgrid[step // 2:h:step, step // 2:w:step]
+    return np.stack([xs.ravel(), ys.ravel()], 1)
+
+
+def hits_vs_oracle(spec, sc, orc, w, h, px, fmt):
+    """Primary hits of the GPU (C ABI trace of the FP64 camera rays rounded to
+    FP32) against the oracle on the pixels px; returns (agreement fraction,
+    max relative t error where both hit the same primitive)."""
+    org, dirs = po.camera_rays(spec, w, h, px)
+    g = sc.intersection(org.astype(np.float32), dirs.astype(np.float32), node_format=fmt)
+    r = orc.trace(org, dirs)
+    r_gid = parity.oracle_global_prim(spec, r["obj"], r["prim"])
+    g_hit = (g["prim"] != 0xffffffff).astype(np.int32)
+    g_gid = g["prim"].astype(np.int64)
+    n_agree, tie, graze, bad = parity.classify(spec, org, dirs, g_hit, g_gid, g["t"].astype(np.float64),
+                                               r["hit"], r_gid, r["t"])
+    assert not bad, "unexplained disagreements at %s" % bad[:10]
+    m = (g_hit == 1) & (r["hit"] == 1) & (g_gid == r_gid)
+    rel = np.abs(g["t"][m].astype(np.float64) - r["t"][m]) / r["t"][m]
+    return n_agree / g_hit.size, float(rel.max()) if rel.size else 0.0
+
+
+def test_config_pathtracer_spheres_rmse_matches_oracle():
+    spec = scenes.spheres_scene(64, seed=1)
+    w = h = 256
+    sc = xtgpu.Scene(spec)
+    ref, _ = sc.render(xtgpu.PATHTRACER, w, h, spp=4096, rdepth=4, seed=1000)
+    gpu, rays = sc.render(xtgpu.PATHTRACER, w, h, spp=16, rdepth=4, seed=1)
+    sc.close()
+    orc = po.OracleScene(spec, po.XO_ACCEL_BVH)
+    o, orays = orc.render(po.PATHTRACER, w, h, spp=16, rdepth=4, seed=2)
+    R = ref.reshape(-1, 4)[:, :3].astype(np.float64)
+    G = gpu.reshape(-1, 4)[:, :3].astype(np.float64)
+    O = o[:, :3].astype(np.float64)
+    rmse_g = np.sqrt(np.mean((G - R) ** 2))
+    rmse_o = np.sqrt(np.mean((O - R) ** 2))
+    # 65,536 pixels: the RMSE of either estimate is known to well under 1 %
+    assert abs(rmse_g / rmse_o - 1.0) < 0.03, (rmse_g, rmse_o)
+    for ch in range(3):
+        d = G[:, ch] - O[:, ch]
+        assert abs(d.mean()) < 4.5 * d.std() / np.sqrt(d.size) + 1e-6, ch
+    assert abs(rays - orays) < 0.01 * orays
+
+
+def test_config_terrain_1m_depth_stencil_full_hd():
+    spec = scenes.terrain_scene(999_698, seed=2)
+    w, h = 1920, 1080
+    sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8))
+    orc = po.OracleScene(spec, po.XO_ACCEL_BVH)
+    px = lattice(w, h, 8)   # 240 x 135 = 32,400 rays
+    for fmt in (xtgpu.NODES_FP32, xtgpu.NODES_Q8):
+        agree, rel = hits_vs_oracle(spec, sc, orc, w, h, px, fmt)
+        assert agree >= 0.9999 and rel <= 1e-5, (fmt, agree, rel)
+    frames = {}
+    for fmt in (xtgpu.NODES_FP32, xtgpu.NODES_Q8):
+        for integ in (xtgpu.STENCIL, xtgpu.DEPTH):
+            img, rays = sc.render(integ, w, h, spp=1, node_format=fmt)
+            assert rays == w * h
+            frames[fmt, integ] = img
+    for integ in (xtgpu.STENCIL, xtgpu.DEPTH):
+        same = np.all(frames[xtgpu.NODES_FP32, integ] == frames[xtgpu.NODES_Q8, integ], axis=2)
+        assert same.mean() >= 0.9999, (integ, same.mean())
+    # depth values on the lattice against the oracle's depth integrator
+    od, _ = orc.render(po.DEPTH, w, h, spp=1, pixels=px)
+    gd = frames[xtgpu.NODES_FP32, xtgpu.DEPTH][px[:, 1], px[:, 0]]
+    both = (od[:, 3] > 0) & (gd[:, 3] > 0)
+    assert np.mean((od[:, 3] > 0) == (gd[:, 3] > 0)) >= 0.9999
+    rel = np.abs(gd[both, 0].astype(np.float64) - od[both, 0]) / np.maximum(np.abs(od[both, 0]), 1e-30)
+    assert np.mean(rel <= 1e-5) >= 0.9999, np.sort(rel)[-5:]
+    os_, _ = orc.render(po.STENCIL, w, h, spp=1, pixels=px)
+    gs = frames[xtgpu.NODES_FP32, xtgpu.STENCIL][px[:, 1], px[:, 0]]
+    assert np.all(gs == os_, axis=1).mean() >= 0.9999
+    sc.close()
+
+
+def test_config_hairball_2m_ao_same_stream_as_oracle():
+    """Same random stream on both sides, so rays differ only where FP32 and
+    FP64 part ways: AO origins leave the surface by a few hundred ulps on the
+    GPU (Waechter-Binder) and by n*1e-8 in the reference, and in a hairball of
+    crossing triangles a hit within that distance, or on an edge, changes."""
+    spec = scenes.hairball_scene(2_000_000, seed=3)
+    w = h = 1024
+    sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8))
+    img, rays = sc.render(xtgpu.AO, w, h, spp=64, ao_max_distance=0.2, seed=31)
+    img8, rays8 = sc.render(xtgpu.AO, w, h, spp=64, ao_max_distance=0.2, seed=31, node_format=xtgpu.NODES_Q8)
+    one, _ = sc.render(xtgpu.AO, w, h, spp=1, ao_max_distance=0.2, seed=31)
+    sc.close()
+    assert np.all(img == img8, axis=2).mean() >= 0.9999
+    assert rays == rays8
+    orc = po.OracleScene(spec, po.XO_ACCEL_BVH)
+    # per ray: one AO ray per pixel on a dense lattice
+    px1 = lattice(w, h, 4)
+    o1, _ = orc.render(po.AO, w, h, spp=1, ao_max_distance=0.2, seed=31, pixels=px1)
+    d1 = np.abs(one[px1[:, 1], px1[:, 0], 0].astype(np.float64) - o1[:, 0])
+    assert np.mean(d1 > 1e-3) <= 0.01, np.mean(d1 > 1e-3)
+    # per pixel at 64 spp on a 32x32 lattice
+    px = lattice(w, h, 32)
+    o, _ = orc.render(po.AO, w, h, spp=64, ao_max_distance=0.2, seed=31, pixels=px)
+    g = img[px[:, 1], px[:, 0], 0].astype(np.float64)
+    d = np.abs(g - o[:, 0])
+    assert np.mean(d < 1e-3) >= 0.75, np.mean(d < 1e-3)
+    assert abs(g.mean() - float(o[:, 0].mean())) < 1e-3
+
+
+def test_config_precision_8m_q8_vs_fp32_vs_fp64():
+    spec = scenes.precision_scene(1.0, seed=5)
+    assert spec.n_tris >= 8_000_000
+    w, h = 1920, 1080
+    sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8))
+    orc = po.OracleScene(spec, po.XO_ACCEL_BVH)
+    px = lattice(w, h, 8)
+    for fmt in (xtgpu.NODES_FP32, xtgpu.NODES_Q8):
+        agree, rel = hits_vs_oracle(spec, sc, orc, w, h, px, fmt)
+        assert agree >= 0.9999 and rel <= 1e-5, (fmt, agree, rel)
+    del orc
+    a, ra = sc.render(xtgpu.PATHTRACER, w, h, spp=256, rdepth=8, seed=5, node_format=xtgpu.NODES_FP32)
+    b, rb = sc.render(xtgpu.PATHTRACER, w, h, spp=256, rdepth=8, seed=5, node_format=xtgpu.NODES_Q8)
+    # the frame is 127 waves of 4 Mi paths; a tile of it rendered in one wave
+    # gives the same pixels
+    tile, _ = sc.render(xtgpu.PATHTRACER, w, h, spp=256, rdepth=8, seed=5, rect=(960, 512, 1024, 576))
+    sc.close()
+    assert np.array_equal(tile, a[512:576, 960:1024])
+    same = np.all(a == b, axis=2)
+    assert same.mean() >= 0.9999, same.mean()
+    assert abs(ra - rb) <= 1e-5 * ra

@@ -246,6 +246,26 @@ def test_render_is_deterministic_and_rect_consistent():
     sc.close()
 
 
+@pytest.mark.parametrize("integ", [xtgpu.AO, xtgpu.PATHTRACER])
+def test_frame_split_into_many_waves_equals_one_wave(integ):
+    """A frame rendered in 16 waves of 65,536 paths equals the frame rendered in
+    one wave.  The waves are queued back to back without host synchronisation,
+    so every wave must keep its own job table until its copies have run."""
+    spec, _, _ = small_scenes()["terrain20k"]
+    sc = xtgpu.Scene(spec)
+    keep = xtgpu.get_tuning().wave_paths
+    try:
+        xtgpu.set_tuning(wave_paths=1 << 22)
+        one, r1 = sc.render(integ, 256, 256, spp=16, rdepth=4, ao_max_distance=0.5, seed=3)
+        xtgpu.set_tuning(wave_paths=1 << 16)
+        many, r2 = sc.render(integ, 256, 256, spp=16, rdepth=4, ao_max_distance=0.5, seed=3)
+    finally:
+        xtgpu.set_tuning(wave_paths=keep)
+    sc.close()
+    assert r1 == r2
+    assert np.array_equal(one, many)
+
+
 def test_bad_arguments_return_invalid():
     spec, w, h = small_scenes()["spheres64"]
     sc = xtgpu.Scene(spec)

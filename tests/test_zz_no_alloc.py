@@ -61,3 +61,45 @@ def test_noalloc_rejects_requests_beyond_its_array():
     st, _ = _noalloc(sc, xtgpu.PATHTRACER, 64, 64, 16, (0, 0, 64, 64), out)   # exactly 65536 paths
     assert st == 0
     sc.close()
+
+
+def test_noalloc_concurrent_host_threads():
+    """Tiles rendered at once from several host threads (XTracer's OpenMP tile
+    loop), each on its own stream, equal the same tiles rendered one by one:
+    the calls take turns on the shared scratch array."""
+    import threading
+
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    torch.cuda.set_device(0)
+    sc = xtgpu.Scene(scenes.terrain_scene(20_000, seed=2, name="noalloc_mt"))
+    w, h = 128, 64
+    rects = [(x, y, x + 32, y + 32) for y in (0, 32) for x in (0, 32, 64, 96)]
+    refs = [sc.render(xtgpu.PATHTRACER, w, h, spp=8, rdepth=4, seed=5, rect=r)[0] for r in rects]
+    outs = [torch.empty((32, 32, 4), dtype=torch.float32, device="cuda") for _ in rects]
+    streams = [torch.cuda.Stream() for _ in rects]
+    status = [None] * len(rects)
+
+    def work(k):
+        torch.cuda.set_device(0)
+        x0, y0, x1, y1 = rects[k]
+        p = xtgpu.RenderParams(xtgpu.PATHTRACER, w, h, 8, 4, 2.0, 5, xtgpu.NODES_FP32, x0, y0, x1, y1)
+        rays = C.c_uint64()
+        status[k] = xtgpu.lib().xtgpu_render_tile_noalloc(sc.handle, C.byref(p), C.c_void_p(outs[k].data_ptr()),
+                                                          C.byref(rays), C.c_void_p(streams[k].cuda_stream))
+
+    for rep in range(3):
+        for o in outs:
+            o.fill_(-7.0)
+        torch.cuda.synchronize()
+        threads = [threading.Thread(target=work, args=(k,)) for k in range(len(rects))]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        torch.cuda.synchronize()
+        assert status == [0] * len(rects)
+        for k, ref in enumerate(refs):
+            assert np.array_equal(outs[k].cpu().numpy(), ref), "tile %d, repetition %d" % (k, rep)
+    sc.close()

@@ -84,7 +84,8 @@ static xtgpu_status get_runner(int64_t cap, cudaStream_t s, WaveRunner **out)
 {
     if (!g_runner || g_runner_cap < cap) {
         if (g_runner) {
-            cudaStreamSynchronize(s);
+            // every call ends synchronised (read_ctl), but a failed one may not have
+            cudaDeviceSynchronize();
             g_runner->release();
             delete g_runner;
             g_runner = nullptr;
@@ -515,9 +516,11 @@ xtgpu_status xtg::render_impl(xtgpu_scene *sc, const xtgpu_render_params *p, flo
     J.tile = T.tile;
     J.frame = (float4 *)rgba;
     std::vector<DevJob> jobs(1, J);
-    for (int64_t first = 0; first < paths; first += R->cap) {
+    // waves of the tuned size (the shared runner may be larger from an earlier call)
+    const int64_t wave = std::max<int64_t>(1, std::min<int64_t>(R->cap, cap));
+    for (int64_t first = 0; first < paths; first += wave) {
         jobs[0].first = first;
-        jobs[0].count = std::min<int64_t>(R->cap, paths - first);
+        jobs[0].count = std::min<int64_t>(wave, paths - first);
         XTG_TRY(R->run_wave(jobs, J.bounces, p->node_format, false, s));
     }
     int32_t overflow = 0;

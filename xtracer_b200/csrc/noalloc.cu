@@ -54,11 +54,15 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 // device memory, so it is never passed to a kernel directly.
 static std::mutex g_na_mu;
 static unsigned char *g_na_addr[64] = {};
+// One call at a time per device owns the scratch: tiles rendered concurrently
+// from several host threads take turns (each call ends synchronised).
+static std::mutex g_na_call_mu[64];
 
-static xtgpu_status noalloc_scratch(unsigned char **out)
+static xtgpu_status noalloc_scratch(unsigned char **out, int *device)
 {
     int dev = 0;
     XTG_CUDA(cudaGetDevice(&dev));
+    *device = dev;
     if (dev < 0 || dev >= 64) {
         set_error("xtgpu_render_tile_noalloc: device index out of range");
         return XTGPU_ERR_INVALID;
@@ -113,7 +117,9 @@ extern "C" xtgpu_status xtgpu_render_tile_noalloc(xtgpu_scene *sc, const xtgpu_r
         return XTGPU_ERR_STATE;
     }
     unsigned char *base = nullptr;
-    XTG_TRY(noalloc_scratch(&base));
+    int dev = 0;
+    XTG_TRY(noalloc_scratch(&base, &dev));
+    std::lock_guard<std::mutex> call_lock(g_na_call_mu[dev]);
     cudaStream_t s = (cudaStream_t)stream;
 
     WaveQueues q{};
@@ -168,8 +174,7 @@ extern "C" xtgpu_status xtgpu_render_tile_noalloc(xtgpu_scene *sc, const xtgpu_r
     XTG_CUDA(cudaMemcpyAsync(scene_dev, &sc->dev, sizeof(DevScene), cudaMemcpyHostToDevice, s));
     XTG_CUDA(cudaMemcpyAsync(q.ctl, ctl, sizeof(ctl), cudaMemcpyHostToDevice, s));
     XTG_CUDA(cudaMemsetAsync(rgba, 0, sizeof(float4) * npix, s));
-    int dev = 0, sms = 148;
-    XTG_CUDA(cudaGetDevice(&dev));
+    int sms = 148;
     XTG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     enqueue_wave_raw(T, q, jobs_dev, scene_dev, sc->dev, prefix_dev, J.bounces, p->node_format, sms,
                      stack_for_depth(sc->depth, T.stack_entries), s);

@@ -705,8 +705,12 @@ xtgpu_status WaveRunner::init(int64_t capacity, int max_jobs, int max_scenes, cu
     this->max_jobs = max_jobs;
     this->max_scenes = max_scenes;
     XTG_CUDA(cudaMemsetAsync(ctlbuf.p, 0, 64, s));
-    XTG_CUDA(cudaMallocHost(&host_jobs, sizeof(DevJob) * (size_t)max_jobs));
-    XTG_CUDA(cudaMallocHost(&host_prefix, sizeof(int64_t) * (size_t)(max_jobs + 1)));
+    for (Staging &S : stage) {
+        XTG_CUDA(cudaMallocHost(&S.jobs, sizeof(DevJob) * (size_t)max_jobs));
+        XTG_CUDA(cudaMallocHost(&S.prefix, sizeof(int64_t) * (size_t)(max_jobs + 1)));
+        XTG_CUDA(cudaMallocHost(&S.ctl, 64));
+        XTG_CUDA(cudaEventCreateWithFlags(&S.copied, cudaEventDisableTiming));
+    }
     XTG_CUDA(cudaMallocHost(&host_ctl, 64));
     int dev = 0;
     XTG_CUDA(cudaGetDevice(&dev));
@@ -734,11 +738,15 @@ void WaveRunner::release()
     for (auto &e : ev) e = nullptr;
     if (acc_done) cudaEventDestroy(acc_done);
     acc_done = nullptr;
-    if (host_jobs) cudaFreeHost(host_jobs);
-    if (host_prefix) cudaFreeHost(host_prefix);
+    for (Staging &S : stage) {
+        if (S.copied) cudaEventSynchronize(S.copied);
+        if (S.jobs) cudaFreeHost(S.jobs);
+        if (S.prefix) cudaFreeHost(S.prefix);
+        if (S.ctl) cudaFreeHost(S.ctl);
+        if (S.copied) cudaEventDestroy(S.copied);
+        S = Staging();
+    }
     if (host_ctl) cudaFreeHost(host_ctl);
-    host_jobs = nullptr;
-    host_prefix = nullptr;
     host_ctl = nullptr;
     for (auto &g : graphs)
         if (g.second) cudaGraphExecDestroy(g.second);
@@ -808,32 +816,37 @@ xtgpu_status WaveRunner::run_wave(const std::vector<DevJob> &jobs, int bounces, 
         set_error("too many jobs in one wave");
         return XTGPU_ERR_LIMIT;
     }
+    Staging &S = stage[stage_next];
+    stage_next ^= 1;
+    if (S.pending) XTG_CUDA(cudaEventSynchronize(S.copied));
     int64_t total = 0;
-    host_prefix[0] = 0;
+    S.prefix[0] = 0;
     for (int j = 0; j < nj; ++j) {
-        host_jobs[j] = jobs[j];
-        host_jobs[j].offset = total;
+        S.jobs[j] = jobs[j];
+        S.jobs[j].offset = total;
         total += jobs[j].count;
         int64_t npix = (int64_t)jobs[j].rw * jobs[j].rh;
-        host_prefix[j + 1] = host_prefix[j] + std::min<int64_t>(npix, jobs[j].count);
+        S.prefix[j + 1] = S.prefix[j] + std::min<int64_t>(npix, jobs[j].count);
     }
     if (total > cap) {
         set_error("wave larger than the queue capacity");
         return XTGPU_ERR_LIMIT;
     }
     bool multi = nscenes > 1;
-    XTG_CUDA(cudaMemcpyAsync(jobbuf.p, host_jobs, sizeof(DevJob) * nj, cudaMemcpyHostToDevice, s));
-    XTG_CUDA(cudaMemcpyAsync(prefixbuf.p, host_prefix, sizeof(int64_t) * (nj + 1), cudaMemcpyHostToDevice, s));
+    XTG_CUDA(cudaMemcpyAsync(jobbuf.p, S.jobs, sizeof(DevJob) * nj, cudaMemcpyHostToDevice, s));
+    XTG_CUDA(cudaMemcpyAsync(prefixbuf.p, S.prefix, sizeof(int64_t) * (nj + 1), cudaMemcpyHostToDevice, s));
     // queue A holds the wave's primary rays; its count is the wave size.  The
     // kernels read the counts from device memory, so the launch sequence does
     // not depend on the wave's contents.
-    host_ctl[0] = (int32_t)total;
-    host_ctl[1] = 0;
-    host_ctl[2] = 0;
-    host_ctl[3] = overflow_seen;
-    host_ctl[4] = nj;
-    host_ctl[5] = (int32_t)total;
-    XTG_CUDA(cudaMemcpyAsync(q.ctl, host_ctl, 24, cudaMemcpyHostToDevice, s));
+    S.ctl[0] = (int32_t)total;
+    S.ctl[1] = 0;
+    S.ctl[2] = 0;
+    S.ctl[3] = overflow_seen;
+    S.ctl[4] = nj;
+    S.ctl[5] = (int32_t)total;
+    XTG_CUDA(cudaMemcpyAsync(q.ctl, S.ctl, 24, cudaMemcpyHostToDevice, s));
+    XTG_CUDA(cudaEventRecord(S.copied, s));
+    S.pending = true;
     if (job_rays_enabled) XTG_CUDA(cudaMemsetAsync(q.job_rays, 0, sizeof(unsigned long long) * nj, s));
     if (use_graph) {
         // One graph per (bounces, format, scene count) shape; kernel arguments

@@ -30,9 +30,20 @@ struct WaveRunner {
     cudaEvent_t prev_acc = nullptr;
     xtgpu_status collect_times(cudaStream_t s);
     void enable_stats(bool on) { q.stats = on ? (unsigned long long *)statsbuf.p : nullptr; }
-    DevJob *host_jobs = nullptr;      // pinned
-    int64_t *host_prefix = nullptr;   // pinned
-    int32_t *host_ctl = nullptr;      // pinned, 64 bytes
+    // Pinned staging of a wave's job table, pixel prefix and counters.  The
+    // copies run when the stream reaches them, after the host may already have
+    // planned further waves, so two slots alternate and a slot is rewritten
+    // only once its previous copies have run.
+    struct Staging {
+        DevJob *jobs = nullptr;
+        int64_t *prefix = nullptr;
+        int32_t *ctl = nullptr;            // 24 bytes used
+        cudaEvent_t copied = nullptr;      // recorded after the slot's copies
+        bool pending = false;
+    };
+    Staging stage[2];
+    int stage_next = 0;
+    int32_t *host_ctl = nullptr;      // pinned, 64 bytes: read_ctl
     int64_t cap = 0;
     int max_jobs = 0, max_scenes = 0, nscenes = 0;
     int sms = 148;
