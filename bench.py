@@ -34,7 +34,8 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = ("jobstream-512: 8 resident scenes (terrain 10k/50k/200k/500k/1M tris, hairball 2M tris, "
             "64 and 4096 spheres), jobs res {128,256,512,1024}^2 x spp {1,4,16,64}, pathtracer depth 4")
-METRIC = "Mrays/s of the served job stream (merged waves, q8 BVH, CUDA graphs); p50/p99 job latency"
+METRIC = ("Mrays/s of the served job stream (merged waves, 8-wide BVH with 8-bit quantised child bounds, "
+          "CUDA graphs); p50/p99 job latency")
 
 
 def parse():
@@ -118,20 +119,25 @@ def measured_peaks():
 
 
 # ---------------------------------------------------------------------------
+SERVED_FORMAT = 2   # xtgpu.NODES_W8: 8-wide BVH, 8-bit quantised child bounds
+
+
 def build_scenes(scale, autotune=False):
-    """The resident scenes; with autotune, each scene's leaf size, stack, tile,
-    register cap and wave size are picked by xtgpu_autotune (Q8 nodes)."""
+    """The resident scenes with FP32, Q8 and W8 nodes; with autotune, each
+    scene's leaf size, extend kernel, stack, tile, register cap and wave size
+    are picked by xtgpu_autotune for the served format (W8)."""
     from xtracer_b200 import scenes, xtgpu
     out, specs, tunes = [], [], {}
     for name, _ in scenes.JOBSTREAM_SCENES:
         spec = scenes.jobstream_scene(name, scale)
         specs.append(spec)
-        sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8))
+        sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8), leaf_size=1)
         if autotune:
-            t = sc.autotune(xtgpu.NODES_Q8, budget_ms=2000)
-            sc.build_bvh(xtgpu.NODES_FP32, t.leaf_size)
-            tunes[name] = {k: getattr(t, k) for k in ("leaf_size", "stack_entries", "tile", "extend_min_blocks",
-                                                       "wave_paths")}
+            t = sc.autotune(SERVED_FORMAT, budget_ms=2000)
+            for f in (xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8):
+                sc.build_bvh(f, t.leaf_size)
+            tunes[name] = {k: getattr(t, k) for k in ("leaf_size", "extend_variant", "steps_per_vote",
+                                                       "stack_entries", "tile", "extend_min_blocks", "wave_paths")}
         out.append(sc)
     return specs, out, tunes
 
@@ -170,7 +176,7 @@ def roofline_bytes_per_ray(specs, gpu_scenes, node_format):
     pathtracer job of that scene (128^2 x 4 spp, depth 4)."""
     from xtracer_b200 import xtgpu
     from xtracer_b200.service import Service
-    node_bytes = 32 if node_format == xtgpu.NODES_Q8 else 64
+    node_bytes = xtgpu.NODE_BYTES[node_format]
     out = []
     for k, sc in enumerate(gpu_scenes):
         svc = Service(gpu_scenes, node_format=node_format, count_visits=True)
@@ -274,7 +280,7 @@ def main():
     slices = [jobs[i * args.jobs_per_step:(i + 1) * args.jobs_per_step] for i in range(nslices)]
     budget = 48 << 30
 
-    served = Service(gscenes, node_format=xtgpu.NODES_Q8, use_graphs=True, merge_jobs=True, memory_budget=budget,
+    served = Service(gscenes, node_format=SERVED_FORMAT, use_graphs=True, merge_jobs=True, memory_budget=budget,
                      waves_in_flight=2, stream=stream)
     # warm-up steps (untimed): graphs captured, allocator pools primed
     for w in range(args.warmup):
@@ -307,7 +313,7 @@ def main():
     # roofline of the extend kernel: the same steps again, one wave at a time
     # so that each extend launch's CUDA-event duration is its own (with two
     # waves in flight, launches share the SMs with the other wave's kernels)
-    rsvc = Service(gscenes, node_format=xtgpu.NODES_Q8, use_graphs=True, merge_jobs=True, memory_budget=budget,
+    rsvc = Service(gscenes, node_format=SERVED_FORMAT, use_graphs=True, merge_jobs=True, memory_budget=budget,
                    time_kernels=True, waves_in_flight=1, stream=stream)
     run_slice(rsvc, slices[0])
     rsvc.reset_stats()
@@ -316,7 +322,7 @@ def main():
         run_slice(rsvc, sl, per_scene=per_scene)
     rst = rsvc.stats()
     rsvc.close()
-    bpr = roofline_bytes_per_ray(specs, gscenes, xtgpu.NODES_Q8)
+    bpr = roofline_bytes_per_ray(specs, gscenes, SERVED_FORMAT)
     scene_bpr = [b["bytes_per_ray"] for b in bpr]
     # rays of each scene in the timed steps times that scene's bytes per ray
     alg_bytes = float(np.dot(per_scene, scene_bpr))
@@ -325,7 +331,7 @@ def main():
     achieved = alg_bytes / ext_s / 1e9 if ext_s > 0 else None
 
     # end to end: same steps, every frame copied to host memory by the service
-    e2e_svc = Service(gscenes, node_format=xtgpu.NODES_Q8, use_graphs=True, merge_jobs=True, memory_budget=budget,
+    e2e_svc = Service(gscenes, node_format=SERVED_FORMAT, use_graphs=True, merge_jobs=True, memory_budget=budget,
                       host_results=True, stream=stream)
     run_slice(e2e_svc, slices[0])
     D.barrier()
@@ -347,6 +353,7 @@ def main():
     if not args.no_plain:
         psvc = Service(gscenes, node_format=xtgpu.NODES_FP32, use_graphs=False, merge_jobs=False,
                        memory_budget=budget, waves_in_flight=1, stream=stream)
+        run_slice(psvc, slices[0])   # warm-up: allocator pools, modules
         torch.cuda.synchronize()
         p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         p0.record()
@@ -362,29 +369,31 @@ def main():
         s1.record()
         torch.cuda.synchronize()
         ss = s0.elapsed_time(s1) / 1000.0
-        # the served form with FP32 nodes on that step (node-format cost)
-        fsvc = Service(gscenes, node_format=xtgpu.NODES_FP32, use_graphs=True, merge_jobs=True,
-                       memory_budget=budget, waves_in_flight=2, stream=stream)
-        run_slice(fsvc, slices[0])
-        torch.cuda.synchronize()
-        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        f0.record()
-        fr, _ = run_slice(fsvc, timed[0])
-        f1.record()
-        torch.cuda.synchronize()
-        fs = f0.elapsed_time(f1) / 1000.0
-        fsvc.close()
+        # the served form with the other node formats on that step
+        other = {}
+        for fname, f in (("fp32", xtgpu.NODES_FP32), ("q8", xtgpu.NODES_Q8)):
+            fsvc = Service(gscenes, node_format=f, use_graphs=True, merge_jobs=True,
+                           memory_budget=budget, waves_in_flight=2, stream=stream)
+            run_slice(fsvc, slices[0])
+            torch.cuda.synchronize()
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            f0.record()
+            fr, _ = run_slice(fsvc, timed[0])
+            f1.record()
+            torch.cuda.synchronize()
+            other[fname] = fr / (f0.elapsed_time(f1) / 1000.0) / 1e6
+            fsvc.close()
         plain = {"value": pr / ps / 1e6, "unit": "Mrays/s", "step_jobs": len(timed[0]),
                  "p50_ms": 1000 * pct(pl, 50), "p99_ms": 1000 * pct(pl, 99),
                  "served_same_step_mrays": sr / ss / 1e6, "speedup": (sr / ss) / (pr / ps),
-                 "served_fp32_same_step_mrays": fr / fs / 1e6,
+                 "served_fp32_same_step_mrays": other["fp32"], "served_q8_same_step_mrays": other["q8"],
                  "form": "one job per launch, FP32 BVH, no CUDA graphs"}
 
     # open-loop latency: Poisson arrivals at 1.5x the plain path's job rate
     latency = None
     if not args.no_latency:
         rate = 1.5 * len(timed[0]) / ps if plain is not None else 50.0
-        lsvc = Service(gscenes, node_format=xtgpu.NODES_Q8, use_graphs=True, merge_jobs=True, memory_budget=budget,
+        lsvc = Service(gscenes, node_format=SERVED_FORMAT, use_graphs=True, merge_jobs=True, memory_budget=budget,
                        stream=stream)
         arr = np.cumsum(np.random.default_rng(4).exponential(1.0 / rate, len(timed[0])))
         ids = [lsvc.submit(j.scene, xtgpu.PATHTRACER, j.width, j.height, j.spp, j.depth, 100.0, j.seed,
@@ -409,7 +418,7 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single",
                        "cache": "inputs larger than L2 (resident scenes ~%.0f MB)" %
                                 (sum(s.device_bytes() for s in gscenes) / 1e6),
-                       "wave_paths": 1 << 22, "node_format": "q8", "cuda_graphs": True, "waves_in_flight": 2,
+                       "wave_paths": 1 << 22, "node_format": "w8 (8-wide, 8-bit quantised)", "cuda_graphs": True, "waves_in_flight": 2,
                        "autotuned": tunes},
             "p50_ms": 1000 * pct(lat_all, 50), "p99_ms": 1000 * pct(lat_all, 99),
             "latency_open_loop": latency, "plain": plain,

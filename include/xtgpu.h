@@ -63,9 +63,11 @@ enum { XTGPU_LAMBERT = 0, XTGPU_PHONG = 1, XTGPU_BLINNPHONG = 2, XTGPU_EMISSIVE 
 enum { XTGPU_ENV_NONE = 0, XTGPU_ENV_COLOR = 1, XTGPU_ENV_GRADIENT = 2 };
 /* Integrators. */
 enum { XTGPU_STENCIL = 0, XTGPU_DEPTH = 1, XTGPU_AO = 2, XTGPU_PATHTRACER = 3 };
-/* BVH node formats: 64-byte FP32 child boxes, or 32-byte boxes quantised to
- * 8 bits per bound with outward rounding. */
-enum { XTGPU_NODES_FP32 = 0, XTGPU_NODES_Q8 = 1 };
+/* BVH node formats: binary nodes with 64-byte FP32 child boxes or 32-byte
+ * boxes quantised to 8 bits per bound with outward rounding; or 8-wide nodes
+ * (80 bytes) with 8-bit quantised child boxes, collapsed from the binary tree
+ * (leaves of at most 3 primitives). */
+enum { XTGPU_NODES_FP32 = 0, XTGPU_NODES_Q8 = 1, XTGPU_NODES_W8 = 2 };
 
 typedef struct {
     int32_t type;                  /* XTGPU_LAMBERT ... */
@@ -127,6 +129,8 @@ typedef struct {
     int32_t depth;
     int32_t leaf_size;
     uint64_t node_bytes_fp32, node_bytes_q8;
+    uint64_t node_bytes_w8;        /* 8-wide nodes (0 if not built) */
+    int32_t depth_w8;              /* levels of the 8-wide tree */
 } xtgpu_bvh_info;
 XTGPU_API xtgpu_status xtgpu_bvh_export(const xtgpu_scene *scene, xtgpu_bvh_info *info, uint32_t *morton,
                               uint32_t *order, int32_t *left, int32_t *right, void *stream);
@@ -272,18 +276,20 @@ XTGPU_API xtgpu_status xtgpu_service_reset_stats(xtgpu_service *svc);
 /* Launch configuration of the wavefront kernels (process-wide).            */
 typedef struct {
     int32_t extend_variant;        /* 0 = warp-batched ray fetch, 1 = lanes refilled when
-                                      refill_threshold of them are idle */
+                                      refill_threshold of them are idle (binary nodes),
+                                      2 = the same, voting every steps_per_vote steps */
     int32_t extend_block;          /* threads per block of the extend kernel (32..256) */
     int32_t extend_blocks_per_sm;  /* resident extend blocks per SM, in 128-thread units */
     int32_t tile;                  /* camera ray order: square pixel tiles of this edge (0 = rows) */
     int64_t wave_paths;            /* paths per wave of xtgpu_render */
     int32_t leaf_size;             /* default primitives per BVH leaf */
     int32_t node_layout;           /* BVH node order: 0 = Karras index, 1 = depth-first */
-    int32_t refill_threshold;      /* variant 1: idle lanes (1..32) that trigger a refill */
+    int32_t refill_threshold;      /* variants 1, 2: idle lanes (1..32) that trigger a refill */
     int32_t extend_min_blocks;     /* variant 0: 0, 8 or 10 resident 128-thread blocks per SM
                                       requested from the compiler (caps registers) */
     int32_t stack_entries;         /* traversal stack: 32 or 64 entries (0 = smallest that
                                       holds the scene's BVH depth) */
+    int32_t steps_per_vote;        /* variant 2: traversal steps between refill votes (1..64) */
 } xtgpu_tuning;
 XTGPU_API xtgpu_status xtgpu_get_tuning(xtgpu_tuning *t);
 XTGPU_API xtgpu_status xtgpu_set_tuning(const xtgpu_tuning *t);

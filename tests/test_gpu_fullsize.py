@@ -83,21 +83,22 @@ def test_config_pathtracer_spheres_rmse_matches_oracle():
 def test_config_terrain_1m_depth_stencil_full_hd():
     spec = scenes.terrain_scene(999_698, seed=2)
     w, h = 1920, 1080
-    sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8))
+    sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8))
     orc = po.OracleScene(spec, po.XO_ACCEL_BVH)
     px = lattice(w, h, 8)   # 240 x 135 = 32,400 rays
-    for fmt in (xtgpu.NODES_FP32, xtgpu.NODES_Q8):
+    for fmt in (xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8):
         agree, rel = hits_vs_oracle(spec, sc, orc, w, h, px, fmt)
         assert agree >= 0.9999 and rel <= 1e-5, (fmt, agree, rel)
     frames = {}
-    for fmt in (xtgpu.NODES_FP32, xtgpu.NODES_Q8):
+    for fmt in (xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8):
         for integ in (xtgpu.STENCIL, xtgpu.DEPTH):
             img, rays = sc.render(integ, w, h, spp=1, node_format=fmt)
             assert rays == w * h
             frames[fmt, integ] = img
     for integ in (xtgpu.STENCIL, xtgpu.DEPTH):
-        same = np.all(frames[xtgpu.NODES_FP32, integ] == frames[xtgpu.NODES_Q8, integ], axis=2)
-        assert same.mean() >= 0.9999, (integ, same.mean())
+        for fmt in (xtgpu.NODES_Q8, xtgpu.NODES_W8):
+            same = np.all(frames[xtgpu.NODES_FP32, integ] == frames[fmt, integ], axis=2)
+            assert same.mean() >= 0.9999, (integ, fmt, same.mean())
     # depth values on the lattice against the oracle's depth integrator
     od, _ = orc.render(po.DEPTH, w, h, spp=1, pixels=px)
     gd = frames[xtgpu.NODES_FP32, xtgpu.DEPTH][px[:, 1], px[:, 0]]
@@ -118,9 +119,11 @@ def test_config_hairball_2m_ao_same_stream_as_oracle():
     crossing triangles a hit within that distance, or on an edge, changes."""
     spec = scenes.hairball_scene(2_000_000, seed=3)
     w = h = 1024
-    sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8))
+    sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8))
     img, rays = sc.render(xtgpu.AO, w, h, spp=64, ao_max_distance=0.2, seed=31)
     img8, rays8 = sc.render(xtgpu.AO, w, h, spp=64, ao_max_distance=0.2, seed=31, node_format=xtgpu.NODES_Q8)
+    imgw, raysw = sc.render(xtgpu.AO, w, h, spp=64, ao_max_distance=0.2, seed=31, node_format=xtgpu.NODES_W8)
+    assert np.array_equal(img, imgw) and rays == raysw
     one, _ = sc.render(xtgpu.AO, w, h, spp=1, ao_max_distance=0.2, seed=31)
     sc.close()
     assert np.all(img == img8, axis=2).mean() >= 0.9999
@@ -144,15 +147,17 @@ def test_config_precision_8m_q8_vs_fp32_vs_fp64():
     spec = scenes.precision_scene(1.0, seed=5)
     assert spec.n_tris >= 8_000_000
     w, h = 1920, 1080
-    sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8))
+    sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8))
     orc = po.OracleScene(spec, po.XO_ACCEL_BVH)
     px = lattice(w, h, 8)
-    for fmt in (xtgpu.NODES_FP32, xtgpu.NODES_Q8):
+    for fmt in (xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8):
         agree, rel = hits_vs_oracle(spec, sc, orc, w, h, px, fmt)
         assert agree >= 0.9999 and rel <= 1e-5, (fmt, agree, rel)
     del orc
     a, ra = sc.render(xtgpu.PATHTRACER, w, h, spp=256, rdepth=8, seed=5, node_format=xtgpu.NODES_FP32)
     b, rb = sc.render(xtgpu.PATHTRACER, w, h, spp=256, rdepth=8, seed=5, node_format=xtgpu.NODES_Q8)
+    c, rc = sc.render(xtgpu.PATHTRACER, w, h, spp=256, rdepth=8, seed=5, node_format=xtgpu.NODES_W8)
+    assert np.array_equal(a, c) and ra == rc
     # the frame is 127 waves of 4 Mi paths; a tile of it rendered in one wave
     # gives the same pixels
     tile, _ = sc.render(xtgpu.PATHTRACER, w, h, spp=256, rdepth=8, seed=5, rect=(960, 512, 1024, 576))

@@ -119,7 +119,7 @@ def gpu_primary(spec, w, h, fmt=xtgpu.NODES_FP32, sc=None, px=None):
 
 
 @pytest.mark.parametrize("name", ["spheres64", "terrain20k", "hairball20k"])
-@pytest.mark.parametrize("fmt", [xtgpu.NODES_FP32, xtgpu.NODES_Q8])
+@pytest.mark.parametrize("fmt", [xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8])
 def test_primary_hits_vs_reference_golden(name, fmt):
     spec, w, h = small_scenes()[name]
     g = np.load(os.path.join(GOLD, "hits_%s.npz" % name))
@@ -167,6 +167,72 @@ def test_q8_hits_equal_fp32(name):
     same = (a["prim"] == b["prim"]) & ((a["t"] == b["t"]) | (a["prim"] == 0xffffffff))
     assert same.mean() >= 0.9999
     sc.close()
+
+
+@pytest.mark.parametrize("name", ["spheres64", "terrain20k", "hairball20k", "dup", "tiny1", "tiny2", "tiny3"])
+@pytest.mark.parametrize("leaf", [1, 2, 3])
+def test_w8_hits_equal_fp32(name, leaf):
+    """The 8-wide quantised BVH finds the same closest hits as the binary FP32
+    BVH, bit for bit: conservative boxes, the same primitive tests, and ties
+    broken by primitive id whatever the visiting order."""
+    if name in small_scenes():
+        spec, w, h = small_scenes()[name]
+    else:
+        spec = duplicate_scene() if name == "dup" else tiny_scene(int(name[-1]))
+        w, h = 48, 32
+    sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_W8), leaf_size=leaf)
+    info = sc.bvh_export()["info"]
+    assert info.node_bytes_w8 > 0 and info.depth_w8 >= 1
+    org, dirs, a = gpu_primary(spec, w, h, xtgpu.NODES_FP32, sc)
+    _, _, b = gpu_primary(spec, w, h, xtgpu.NODES_W8, sc)
+    assert np.array_equal(a["prim"], b["prim"])
+    assert np.array_equal(a["t"], b["t"])
+    # secondary-like rays from inside the scene, in all directions
+    rng = np.random.default_rng(leaf)
+    lo = spec.tris.reshape(-1, 3).min(0) if spec.n_tris else spec.spheres[:, :3].min(0)
+    hi = spec.tris.reshape(-1, 3).max(0) if spec.n_tris else spec.spheres[:, :3].max(0)
+    o = (lo + (hi - lo) * rng.random((20000, 3))).astype(np.float32)
+    d = rng.normal(size=(20000, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    a = sc.intersection(o, d, node_format=xtgpu.NODES_FP32)
+    b = sc.intersection(o, d, node_format=xtgpu.NODES_W8)
+    assert np.array_equal(a["prim"], b["prim"])
+    assert np.array_equal(a["t"], b["t"])
+    sc.close()
+
+
+@pytest.mark.parametrize("variant,refill,steps", [(0, 8, 8), (1, 8, 8), (2, 8, 1), (2, 16, 8), (2, 32, 64)])
+@pytest.mark.parametrize("fmt", [xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8])
+def test_extend_variants_agree(variant, refill, steps, fmt):
+    """Every extend kernel (warp-batched, per-step refill, pooled lanes with a
+    vote every few steps) and node format returns the same hits."""
+    spec, w, h = small_scenes()["hairball20k"]
+    sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8), leaf_size=1)
+    rng = np.random.default_rng(7)
+    o = (rng.random((50000, 3)) * 2.4 - 1.2).astype(np.float32)
+    d = rng.normal(size=(50000, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    ref = sc.intersection(o, d, node_format=xtgpu.NODES_FP32)
+    keep = {k: getattr(xtgpu.get_tuning(), k) for k, _ in xtgpu.Tuning._fields_}
+    try:
+        xtgpu.set_tuning(extend_variant=variant, refill_threshold=refill, steps_per_vote=steps)
+        got = sc.intersection(o, d, node_format=fmt)
+    finally:
+        xtgpu.set_tuning(**keep)
+    sc.close()
+    assert np.array_equal(ref["prim"], got["prim"])
+    assert np.array_equal(ref["t"], got["t"])
+
+
+@pytest.mark.parametrize("integ", [xtgpu.STENCIL, xtgpu.DEPTH, xtgpu.AO, xtgpu.PATHTRACER])
+def test_w8_frames_equal_fp32(integ):
+    spec, w, h = small_scenes()["terrain20k"]
+    sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_W8), leaf_size=1)
+    a, ra = sc.render(integ, w, h, spp=8, rdepth=4, ao_max_distance=0.5, seed=4, node_format=xtgpu.NODES_FP32)
+    b, rb = sc.render(integ, w, h, spp=8, rdepth=4, ao_max_distance=0.5, seed=4, node_format=xtgpu.NODES_W8)
+    sc.close()
+    assert ra == rb
+    assert np.array_equal(a, b)
 
 
 @pytest.mark.parametrize("name", ["spheres64", "terrain20k", "hairball20k"])

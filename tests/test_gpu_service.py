@@ -24,7 +24,7 @@ def cuda_device():
 
 @pytest.fixture(scope="module")
 def resident():
-    fm = (xtgpu.NODES_FP32, xtgpu.NODES_Q8)
+    fm = (xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8)
     return [xtgpu.Scene(scenes.spheres_scene(64, seed=1, name="s64"), node_formats=fm),
             xtgpu.Scene(scenes.terrain_scene(20_000, seed=2, name="t20k"), node_formats=fm),
             xtgpu.Scene(scenes.hairball_scene(20_000, seed=3, name="h20k"), node_formats=fm)]
@@ -35,7 +35,7 @@ JOBS = [(0, xtgpu.PATHTRACER, 64, 48, 8, 4, 100.0, 11), (1, xtgpu.PATHTRACER, 40
         (0, xtgpu.STENCIL, 33, 17, 3, 1, 100.0, 15), (2, xtgpu.PATHTRACER, 24, 24, 4, 4, 100.0, 16)]
 
 
-@pytest.mark.parametrize("fmt", [xtgpu.NODES_FP32, xtgpu.NODES_Q8])
+@pytest.mark.parametrize("fmt", [xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8])
 def test_job_alone_equals_job_in_mix(resident, fmt):
     alone = []
     for (s, integ, w, h, spp, d, md, seed) in JOBS:

@@ -134,7 +134,7 @@ xtgpu_status xtgpu_scene_tuning(const xtgpu_scene *sc, xtgpu_tuning *t)
 
 xtgpu_status xtgpu_set_tuning(const xtgpu_tuning *t)
 {
-    if (!t || t->extend_variant < 0 || t->extend_variant > 1 || t->extend_block < 32 || t->extend_block > 256 ||
+    if (!t || t->extend_variant < 0 || t->extend_variant > 2 || t->steps_per_vote < 1 || t->steps_per_vote > 64 || t->extend_block < 32 || t->extend_block > 256 ||
         (t->extend_block & 31) || t->extend_blocks_per_sm < 1 || t->extend_blocks_per_sm > 64 || t->tile < 0 ||
         t->tile > 256 || t->wave_paths < 1024 || t->wave_paths > (1ll << 26) || t->leaf_size < 1 ||
         t->leaf_size > MAX_LEAF || t->node_layout < 0 || t->node_layout > 1 || t->refill_threshold < 1 ||
@@ -280,10 +280,11 @@ xtgpu_status xtgpu_bvh_build(xtgpu_scene *sc, const xtgpu_bvh_opts *opts, void *
     }
     int fmt = opts ? opts->node_format : XTGPU_NODES_FP32;
     int leaf = opts && opts->leaf_size > 0 ? opts->leaf_size : scene_tuning(sc).leaf_size;
-    if (fmt != XTGPU_NODES_FP32 && fmt != XTGPU_NODES_Q8) {
+    if (!format_valid(fmt)) {
         set_error("xtgpu_bvh_build: bad node format");
         return XTGPU_ERR_INVALID;
     }
+    if (fmt == XTGPU_NODES_W8 && !(opts && opts->leaf_size > 0)) leaf = std::min(leaf, 3);
     if (leaf < 1 || leaf > MAX_LEAF) {
         set_error("xtgpu_bvh_build: leaf_size out of range");
         return XTGPU_ERR_INVALID;
@@ -295,8 +296,8 @@ xtgpu_status xtgpu_scene_destroy(xtgpu_scene *sc)
 {
     if (!sc) return XTGPU_OK;
     for (HostBuf *b : {&sc->tri_v, &sc->tri_n, &sc->spheres, &sc->planes, &sc->prim_obj, &sc->obj_material,
-                       &sc->materials, &sc->leaf_prims, &sc->nodes32, &sc->nodes8, &sc->morton, &sc->order,
-                       &sc->left, &sc->right})
+                       &sc->materials, &sc->leaf_prims, &sc->nodes32, &sc->nodes8, &sc->nodesW, &sc->leafW,
+                       &sc->morton, &sc->order, &sc->left, &sc->right})
         dfree(*b);
     delete sc;
     return XTGPU_OK;
@@ -310,8 +311,8 @@ xtgpu_status xtgpu_scene_device_bytes(const xtgpu_scene *sc, uint64_t *bytes)
     }
     uint64_t b = 0;
     for (const HostBuf *h : {&sc->tri_v, &sc->tri_n, &sc->spheres, &sc->planes, &sc->prim_obj, &sc->obj_material,
-                             &sc->materials, &sc->leaf_prims, &sc->nodes32, &sc->nodes8, &sc->morton, &sc->order,
-                             &sc->left, &sc->right})
+                             &sc->materials, &sc->leaf_prims, &sc->nodes32, &sc->nodes8, &sc->nodesW, &sc->leafW,
+                             &sc->morton, &sc->order, &sc->left, &sc->right})
         b += h->bytes;
     *bytes = b;
     return XTGPU_OK;
@@ -337,6 +338,8 @@ xtgpu_status xtgpu_bvh_export(const xtgpu_scene *sc, xtgpu_bvh_info *info, uint3
         info->leaf_size = sc->leaf_size;
         info->node_bytes_fp32 = sc->nodes32.bytes;
         info->node_bytes_q8 = sc->nodes8.bytes;
+        info->node_bytes_w8 = sc->builtW ? (uint64_t)sc->n_wide * 80u : 0u;
+        info->depth_w8 = sc->depthW;
     }
     if (n > 0) {
         if (morton) XTG_CUDA(cudaMemcpy(morton, sc->morton.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
@@ -349,8 +352,7 @@ xtgpu_status xtgpu_bvh_export(const xtgpu_scene *sc, xtgpu_bvh_info *info, uint3
 
 static xtgpu_status check_format(const xtgpu_scene *sc, int32_t fmt)
 {
-    if (fmt == XTGPU_NODES_FP32 && sc->built32) return XTGPU_OK;
-    if (fmt == XTGPU_NODES_Q8 && sc->built8) return XTGPU_OK;
+    if (format_built(sc, fmt)) return XTGPU_OK;
     set_error("node format not built for this scene");
     return XTGPU_ERR_STATE;
 }
@@ -404,7 +406,7 @@ static xtgpu_status trace_impl(xtgpu_scene *sc, int64_t n, const void *org, cons
         int32_t init[4] = {cnt, 0, 0, 0};
         XTG_CUDA(cudaMemcpyAsync(ctl, init, sizeof(init), cudaMemcpyHostToDevice, s));
         const xtgpu_tuning &T = scene_tuning(sc);
-        launch_extend(T, fmt, sc->dev, q, 0, sms, stack_for_depth(sc->depth, T.stack_entries), s);
+        launch_extend(T, fmt, sc->dev, q, 0, sms, stack_for_scene(sc, fmt, T.stack_entries), s);
         XTG_CUDA(cudaGetLastError());
         int32_t back[4];
         XTG_CUDA(cudaMemcpyAsync(back, ctl, sizeof(back), cudaMemcpyDeviceToHost, s));
@@ -496,7 +498,7 @@ xtgpu_status xtg::render_impl(xtgpu_scene *sc, const xtgpu_render_params *p, flo
     XTG_TRY(get_runner(std::max<int64_t>(cap, 1 << 16), s, &R));
     XTG_TRY(R->set_scenes(&sc->dev, 1, s));
     R->T = T;
-    R->stack = stack_for_depth(sc->depth, T.stack_entries);
+    R->stack = stack_for_scene(sc, p->node_format, T.stack_entries);
     XTG_CUDA(cudaMemsetAsync(R->q.ctl, 0, 64, s));
     XTG_CUDA(cudaMemsetAsync(rgba, 0, sizeof(float4) * npix, s));
     DevJob J{};

@@ -1,5 +1,6 @@
 // Autotuner: per scene, the knobs that the best launch shape and data layout
-// depend on — primitives per BVH leaf, traversal stack size, camera tile,
+// depend on — primitives per BVH leaf, extend kernel (warp-batched or pooled
+// lanes, and how often the pool votes), traversal stack size, camera tile,
 // register cap of the extend kernel and wave size — picked by timing a probe
 // pathtracer job for each candidate of one knob at a time (coordinate descent
 // from the process-wide tuning).  No counterpart in the reference, which has
@@ -49,9 +50,9 @@ xtgpu_status probe_ms(Probe &P, const xtgpu_tuning &T, float *ms)
 
 xtgpu_status rebuild(xtgpu_scene *sc, int fmt, int leaf, int layout, cudaStream_t s)
 {
-    sc->built32 = sc->built8 = false;   // force a new topology
+    sc->built32 = sc->built8 = sc->builtW = false;   // force a new topology
     XTG_TRY(build_bvh(sc, XTGPU_NODES_FP32, leaf, layout, s));
-    if (fmt == XTGPU_NODES_Q8) XTG_TRY(build_bvh(sc, XTGPU_NODES_Q8, leaf, layout, s));
+    if (fmt != XTGPU_NODES_FP32) XTG_TRY(build_bvh(sc, fmt, leaf, layout, s));
     return XTGPU_OK;
 }
 
@@ -60,7 +61,7 @@ xtgpu_status rebuild(xtgpu_scene *sc, int fmt, int leaf, int layout, cudaStream_
 extern "C" xtgpu_status xtgpu_autotune(xtgpu_scene *sc, int32_t fmt, double budget_ms, xtgpu_tuning *best,
                                        void *stream)
 {
-    if (!sc || (fmt != XTGPU_NODES_FP32 && fmt != XTGPU_NODES_Q8) || !(budget_ms > 0)) {
+    if (!sc || !format_valid(fmt) || !(budget_ms > 0)) {
         set_error("xtgpu_autotune: bad argument");
         return XTGPU_ERR_INVALID;
     }
@@ -81,7 +82,7 @@ extern "C" xtgpu_status xtgpu_autotune(xtgpu_scene *sc, int32_t fmt, double budg
     xtgpu_tuning T = scene_tuning(sc);
     xtgpu_status st = XTGPU_OK;
     float cur = 0.f;
-    if (fmt == XTGPU_NODES_Q8 && !sc->built8) st = build_bvh(sc, XTGPU_NODES_Q8, sc->leaf_size, sc->layout, s);
+    if (fmt != XTGPU_NODES_FP32 && !format_built(sc, fmt)) st = build_bvh(sc, fmt, sc->leaf_size, sc->layout, s);
     if (st == XTGPU_OK) {
         T.leaf_size = sc->leaf_size;
         st = probe_ms(P, T, &cur);
@@ -89,7 +90,7 @@ extern "C" xtgpu_status xtgpu_autotune(xtgpu_scene *sc, int32_t fmt, double budg
     // 1. primitives per leaf (rebuilds the BVH)
     if (st == XTGPU_OK) {
         int best_leaf = T.leaf_size;
-        for (int leaf : {1, 2, 4}) {
+        for (int leaf : {1, 2, fmt == XTGPU_NODES_W8 ? 3 : 4}) {
             if (leaf == T.leaf_size || elapsed_ms() > budget_ms) continue;
             if ((st = rebuild(sc, fmt, leaf, T.node_layout, s)) != XTGPU_OK) break;
             xtgpu_tuning C = T;
@@ -120,7 +121,9 @@ extern "C" xtgpu_status xtgpu_autotune(xtgpu_scene *sc, int32_t fmt, double budg
             }
         }
     };
-    if (sc->depth <= 30) knob(&xtgpu_tuning::stack_entries, {32, 64});
+    knob(&xtgpu_tuning::extend_variant, {0, 2});
+    if (T.extend_variant == 2) knob(&xtgpu_tuning::steps_per_vote, {4, 8, 16});
+    if ((fmt == XTGPU_NODES_W8 ? sc->depthW : sc->depth) <= 30) knob(&xtgpu_tuning::stack_entries, {32, 64});
     knob(&xtgpu_tuning::extend_min_blocks, {0, 8, 10});
     knob(&xtgpu_tuning::tile, {0, 4, 8, 16});
     if (st == XTGPU_OK) {

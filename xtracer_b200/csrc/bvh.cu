@@ -502,9 +502,11 @@ xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, int layo
     // them once and keep them.
     bool need_topology = !(sc->built32 || sc->built8) || sc->leaf_size != leaf_size || sc->layout != layout;
     if (need_topology) {
-        sc->built32 = sc->built8 = false;
+        sc->built32 = sc->built8 = sc->builtW = false;
         dfree(sc->nodes32);
         dfree(sc->nodes8);
+        dfree(sc->nodesW);
+        dfree(sc->leafW);
         dfree(sc->leaf_prims);
         dfree(sc->morton);
         dfree(sc->order);
@@ -615,6 +617,7 @@ xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, int layo
         set_error("xtgpu_bvh_build: BVH depth exceeds the traversal stack");
         return XTGPU_ERR_LIMIT;
     }
+    if (node_format == XTGPU_NODES_W8 && !sc->builtW) XTG_TRY(build_wide(sc, s));
     sc->last_format = node_format;
     XTG_CUDA(cudaStreamSynchronize(s));
     return XTGPU_OK;

@@ -111,8 +111,7 @@ extern "C" xtgpu_status xtgpu_render_tile_noalloc(xtgpu_scene *sc, const xtgpu_r
                   "split the frame into smaller tiles");
         return XTGPU_ERR_LIMIT;
     }
-    if ((p->node_format == XTGPU_NODES_FP32 && !sc->built32) || (p->node_format == XTGPU_NODES_Q8 && !sc->built8) ||
-        (p->node_format != XTGPU_NODES_FP32 && p->node_format != XTGPU_NODES_Q8)) {
+    if (!format_valid(p->node_format) || !format_built(sc, p->node_format)) {
         set_error("xtgpu_render_tile_noalloc: node format not built for this scene");
         return XTGPU_ERR_STATE;
     }
@@ -177,7 +176,7 @@ extern "C" xtgpu_status xtgpu_render_tile_noalloc(xtgpu_scene *sc, const xtgpu_r
     int sms = 148;
     XTG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     enqueue_wave_raw(T, q, jobs_dev, scene_dev, sc->dev, prefix_dev, J.bounces, p->node_format, sms,
-                     stack_for_depth(sc->depth, T.stack_entries), s);
+                     stack_for_scene(sc, p->node_format, T.stack_entries), s);
     XTG_CUDA(cudaGetLastError());
     int32_t back[16];
     XTG_CUDA(cudaMemcpyAsync(back, q.ctl, sizeof(back), cudaMemcpyDeviceToHost, s));

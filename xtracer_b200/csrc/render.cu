@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "render.h"
+#include "wide.cuh"
 
 namespace xtg {
 
@@ -432,6 +433,160 @@ __device__ __forceinline__ void trace_ray(const SceneView &V, const RayPre &r, f
         }
 }
 
+// One step of the binary traversal: a node (descend, pushing the farther hit
+// child with its entry distance) or a leaf; then, if the ray has nowhere to go,
+// the next stack entry still nearer than the closest hit.  Returns true when
+// the traversal is over.
+template <int FMT, int STACK>
+__device__ __forceinline__ bool binary_step(const SceneView &V, const RayPre &r, float tmin, float &tmax,
+                                            uint32_t &prim, float &bu, float &bv, int32_t &ref, int &sp, uint2 *stack,
+                                            int32_t *ctl_overflow, uint32_t &nv, uint32_t &np)
+{
+    if (ref >= 0) {
+        Pair P;
+        node_pair<FMT>(V.nodes, ref, r, tmin, tmax, P);
+        ++nv;
+        if (P.h0 && P.h1) {
+            const bool sw = P.t1 < P.t0;
+            if (sp >= STACK) {
+                *ctl_overflow = 1;
+                return true;
+            }
+            stack[sp++] = make_uint2((uint32_t)(sw ? P.c0 : P.c1), __float_as_uint(sw ? P.t0 : P.t1));
+            ref = sw ? P.c1 : P.c0;
+            return false;
+        }
+        if (P.h0) {
+            ref = P.c0;
+            return false;
+        }
+        if (P.h1) {
+            ref = P.c1;
+            return false;
+        }
+    } else if (ref != EMPTY_REF) {
+        np += leaf_count(ref);
+        leaf_test(V, ref, r, tmin, tmax, prim, bu, bv);
+    }
+    while (sp > 0) {
+        const uint2 e = stack[--sp];
+        if (__uint_as_float(e.y) <= tmax) {
+            ref = (int32_t)e.x;
+            return false;
+        }
+    }
+    return true;
+}
+
+// Persistent extend with pooled lanes: every lane runs its own ray; a lane
+// whose ray is done idles until `refill` lanes of the warp are idle (or all
+// are), and then they take new rays together.  The warp votes on refills only
+// every `ksteps` traversal steps, so the vote costs little per step, while
+// long rays no longer hold a mostly idle warp (Aila and Laine, "Understanding
+// the Efficiency of Ray Traversal on GPUs", HPG 2009: persistent threads with
+// dynamic fetch).  Binary (FP32, Q8) or 8-wide nodes.
+template <int FMT, bool MULTI, int MINB, int STACK>
+__global__ void __launch_bounds__(MINB > 0 ? 128 : 256, MINB > 0 ? MINB : 1)
+    k_extend_pool(DevScene S1, const DevScene *__restrict__ scenes, const DevJob *__restrict__ jobs, WaveQueues q,
+                  int side, int refill, int ksteps)
+{
+    const int n = q.ctl[side];
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(q.rays, (unsigned long long)n);
+    const float4 *org = q.org[side], *dir = q.dir[side];
+    SceneView V = scene_view<FMT>(S1);
+    RayPre r;
+    float tmin = 0.f, tmax = 0.f, bu = 0.f, bv = 0.f;
+    uint32_t prim = 0xffffffffu, nv = 0, np = 0, guard = 0, oct = 0;
+    int32_t cur = 0;
+    int idx = 0, sp = 0;
+    uint2 stack[STACK];
+    bool active = false, exhausted = false;
+    while (true) {
+        const bool want = !active && !exhausted;
+        const unsigned m = __ballot_sync(0xffffffffu, want);
+        const unsigned busy = __ballot_sync(0xffffffffu, active);
+        if (m && (__popc(m) >= refill || busy == 0u)) {
+            const int leader = __ffs(m) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(&q.ctl[2], __popc(m));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            uint32_t jb = 0xffffffffu;
+            if (want) {
+                idx = base + __popc(m & lt);
+                if (idx < n) {
+                    float4 a = org[idx], b = dir[idx];
+                    ray_pre(make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z), r);
+                    tmin = a.w;
+                    tmax = b.w;
+                    if (MULTI || q.job_rays) jb = q.meta[side][idx].y;
+                    if (MULTI) V = scene_view<FMT>(scenes[jobs[jb].scene]);
+                    prim = 0xffffffffu;
+                    bu = bv = 0.f;
+                    cur = V.root;
+                    oct = ray_octant(r);
+                    sp = 0;
+                    nv = np = guard = 0;
+                    active = true;
+                    // an empty 8-wide tree has no root node
+                    if (FMT == XTGPU_NODES_W8 && cur < 0) cur = EMPTY_REF;
+                } else {
+                    exhausted = true;
+                }
+            }
+            if (q.job_rays) {
+                const unsigned peers = __match_any_sync(0xffffffffu, jb);
+                if (jb != 0xffffffffu && (peers & lt) == 0u) atomicAdd(&q.job_rays[jb], (unsigned long long)__popc(peers));
+            }
+        }
+        if (!__any_sync(0xffffffffu, active || !exhausted)) break;
+        if (!active) continue;
+        bool done = false;
+        for (int k = 0; k < ksteps && !done; ++k) {
+            if (++guard > (1u << 22)) {   // corrupted tree: report, never loop forever
+                q.ctl[3] = 1;
+                done = true;
+            } else if constexpr (FMT == XTGPU_NODES_W8) {
+                done = cur == EMPTY_REF ||
+                       wide_step<STACK>(V, r, oct, tmin, tmax, prim, bu, bv, cur, sp, stack, &q.ctl[3], nv, np);
+            } else {
+                done = binary_step<FMT, STACK>(V, r, tmin, tmax, prim, bu, bv, cur, sp, stack, &q.ctl[3], nv, np);
+            }
+        }
+        if (done) {
+            for (int p = 0; p < V.n_planes; ++p)
+                if (hit_plane(r, __ldg(V.planes + p), tmin, tmax)) {
+                    prim = V.plane_base + (uint32_t)p;
+                    bu = bv = 0.f;
+                }
+            xtgpu_hit o;
+            o.t = prim != 0xffffffffu ? tmax : INFINITY;
+            o.prim = prim;
+            o.u = bu;
+            o.v = bv;
+            q.hit[idx] = o;
+            if (q.stats) {
+                atomicAdd(&q.stats[0], (unsigned long long)nv);
+                atomicAdd(&q.stats[1], (unsigned long long)(np + (uint32_t)V.n_planes));
+            }
+            active = false;
+        }
+    }
+}
+
+// closest hit in the node format FMT
+template <int FMT, int STACK>
+__device__ __forceinline__ void trace_any(const SceneView &V, const RayPre &r, float tmin, float &tmax,
+                                          uint32_t &prim, float &bu, float &bv, int32_t *ctl_overflow, uint32_t &nv,
+                                          uint32_t &np)
+{
+    if constexpr (FMT == XTGPU_NODES_W8)
+        trace_wide<STACK>(V, r, tmin, tmax, prim, bu, bv, ctl_overflow, nv, np);
+    else
+        trace_ray<FMT, STACK>(V, r, tmin, tmax, prim, bu, bv, ctl_overflow, nv, np);
+}
+
 // Persistent extend, warp-batched: each warp takes the next 32 queued rays and
 // every lane runs its ray to the end.  MINB > 0 asks the compiler for at least
 // MINB resident 128-thread blocks per SM (fewer registers, more warps to hide
@@ -463,10 +618,10 @@ __global__ void __launch_bounds__(MINB > 0 ? 128 : 256, MINB > 0 ? MINB : 1)
             if (MULTI || q.job_rays) jb = q.meta[side][i].y;
             if (MULTI) {
                 const SceneView V = scene_view<FMT>(scenes[jobs[jb].scene]);
-                trace_ray<FMT, STACK>(V, r, a.w, tmax, prim, bu, bv, &q.ctl[3], nv, np);
+                trace_any<FMT, STACK>(V, r, a.w, tmax, prim, bu, bv, &q.ctl[3], nv, np);
                 np += (uint32_t)V.n_planes;
             } else {
-                trace_ray<FMT, STACK>(V1, r, a.w, tmax, prim, bu, bv, &q.ctl[3], nv, np);
+                trace_any<FMT, STACK>(V1, r, a.w, tmax, prim, bu, bv, &q.ctl[3], nv, np);
                 np += (uint32_t)V1.n_planes;
             }
             xtgpu_hit o;
@@ -901,10 +1056,11 @@ xtgpu_status WaveRunner::read_ctl(int32_t *overflow, unsigned long long *rays, c
 
 // Process-wide launch configuration (xtgpu_set_tuning / xtgpu_autotune).
 // Defaults from sweeps on a B200 (variant x leaf x node format x launch shape x
-// tile x register cap over terrain, hairball and sphere scenes): warp-batched
-// fetch, one primitive per leaf, depth-first node order, 8x8 pixel tiles, and
-// 64 registers (8 resident 128-thread blocks per SM).
-static xtgpu_tuning g_tuning = {0, 128, 8, 8, 1ll << 22, 1, 1, 8, 8, 0};
+// tile x register cap over terrain, hairball and sphere scenes, and the served
+// job stream): pooled lanes refilled when 8 are idle with a vote every 8 steps,
+// one primitive per leaf, depth-first node order, 8x8 pixel tiles, and 64
+// registers (8 resident 128-thread blocks per SM).
+static xtgpu_tuning g_tuning = {2, 128, 8, 8, 1ll << 22, 1, 1, 8, 8, 0, 8};
 xtgpu_tuning &tuning() { return g_tuning; }
 
 void launch_extend_kernel(const xtgpu_tuning &T, int fmt, bool multi, const DevScene &single,
@@ -915,16 +1071,44 @@ void launch_extend_kernel(const xtgpu_tuning &T, int fmt, bool multi, const DevS
     const int tb = T.extend_block;
     const int nb = std::max(1, blocks * 128 / tb);   // same resident thread count for any block size
 #define XTG_LAUNCH_R(K, F, M) K<F, M><<<nb, tb, 0, s>>>(single, scenes, jobs, q, side, T.refill_threshold)
-    if (T.extend_variant == 1) {
+    if (T.extend_variant == 1 && fmt != XTGPU_NODES_W8) {
         if (fmt == XTGPU_NODES_Q8) { if (multi) XTG_LAUNCH_R(k_extend_refill, XTGPU_NODES_Q8, true); else XTG_LAUNCH_R(k_extend_refill, XTGPU_NODES_Q8, false); }
         else { if (multi) XTG_LAUNCH_R(k_extend_refill, XTGPU_NODES_FP32, true); else XTG_LAUNCH_R(k_extend_refill, XTGPU_NODES_FP32, false); }
+        return;
+    }
+    if (T.extend_variant == 2) {
+        const int ks = std::max(1, T.steps_per_vote), rf = T.refill_threshold;
+#define XTG_P(MB, ST)                                                                                   \
+    do {                                                                                                \
+        const int tbb = MB > 0 ? 128 : tb, nbb = MB > 0 ? std::max(1, blocks) : nb;                  \
+        if (fmt == XTGPU_NODES_W8) {                                                                    \
+            if (multi) k_extend_pool<XTGPU_NODES_W8, true, MB, ST><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side, rf, ks);   \
+            else k_extend_pool<XTGPU_NODES_W8, false, MB, ST><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side, rf, ks);       \
+        } else if (fmt == XTGPU_NODES_Q8) {                                                             \
+            if (multi) k_extend_pool<XTGPU_NODES_Q8, true, MB, ST><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side, rf, ks);   \
+            else k_extend_pool<XTGPU_NODES_Q8, false, MB, ST><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side, rf, ks);       \
+        } else {                                                                                        \
+            if (multi) k_extend_pool<XTGPU_NODES_FP32, true, MB, ST><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side, rf, ks); \
+            else k_extend_pool<XTGPU_NODES_FP32, false, MB, ST><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side, rf, ks);     \
+        }                                                                                               \
+    } while (0)
+        const bool small = stack <= 32;
+        switch (T.extend_min_blocks) {
+        case 8: if (small) XTG_P(8, 32); else XTG_P(8, 64); break;
+        case 10: if (small) XTG_P(10, 32); else XTG_P(10, 64); break;
+        default: if (small) XTG_P(0, 32); else XTG_P(0, 64); break;
+        }
+#undef XTG_P
         return;
     }
     // register-capped instantiations run with 128-thread blocks
 #define XTG_B(MB, ST)                                                                                   \
     do {                                                                                                \
         const int tbb = MB > 0 ? 128 : tb, nbb = MB > 0 ? std::max(1, blocks) : nb;                  \
-        if (fmt == XTGPU_NODES_Q8) {                                                                    \
+        if (fmt == XTGPU_NODES_W8) {                                                                    \
+            if (multi) k_extend_batch<XTGPU_NODES_W8, true, MB, ST><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side);   \
+            else k_extend_batch<XTGPU_NODES_W8, false, MB, ST><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side);       \
+        } else if (fmt == XTGPU_NODES_Q8) {                                                             \
             if (multi) k_extend_batch<XTGPU_NODES_Q8, true, MB, ST><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side);   \
             else k_extend_batch<XTGPU_NODES_Q8, false, MB, ST><<<nbb, tbb, 0, s>>>(single, scenes, jobs, q, side);       \
         } else {                                                                                        \
@@ -970,6 +1154,11 @@ int stack_for_depth(int depth, int requested)
     if (requested == 32 && depth <= 30) return 32;
     if (requested == 64) return 64;
     return depth <= 30 ? 32 : 64;
+}
+
+int stack_for_scene(const xtgpu_scene *sc, int f, int requested)
+{
+    return stack_for_depth(f == XTGPU_NODES_W8 ? sc->depthW : sc->depth, requested);
 }
 
 int bounces_of(int integrator, int rdepth)

@@ -179,7 +179,8 @@ static xtgpu_status launch_wave(xtgpu_service *v, WaveSlot &W, cudaEvent_t prev_
         int stack = 32;
         for (size_t k = 0; k < per.size(); ++k)
             if (per[k] > 0)
-                stack = std::max(stack, stack_for_depth(v->scenes[k]->depth, scene_tuning(v->scenes[k]).stack_entries));
+                stack = std::max(stack, stack_for_scene(v->scenes[k], v->o.node_format,
+                                                        scene_tuning(v->scenes[k]).stack_entries));
         W.R.stack = stack;
     }
     // frames of newly admitted jobs are allocated and zeroed on the service stream
@@ -295,7 +296,7 @@ extern "C" {
 xtgpu_status xtgpu_service_create(const xtgpu_service_opts *opts, void *stream, xtgpu_service **out)
 {
     if (!opts || !out || opts->max_jobs <= 0 || opts->max_jobs > 1024 || opts->wave_paths < 0 ||
-        (opts->node_format != XTGPU_NODES_FP32 && opts->node_format != XTGPU_NODES_Q8)) {
+        !format_valid(opts->node_format)) {
         set_error("xtgpu_service_create: bad options");
         return XTGPU_ERR_INVALID;
     }
@@ -356,7 +357,7 @@ xtgpu_status xtgpu_service_add_scene(xtgpu_service *v, xtgpu_scene *sc, int32_t 
         set_error("xtgpu_service_add_scene: NULL argument");
         return XTGPU_ERR_INVALID;
     }
-    if ((v->o.node_format == XTGPU_NODES_FP32 && !sc->built32) || (v->o.node_format == XTGPU_NODES_Q8 && !sc->built8)) {
+    if (!format_built(sc, v->o.node_format)) {
         set_error("xtgpu_service_add_scene: the service's node format is not built for this scene");
         return XTGPU_ERR_STATE;
     }

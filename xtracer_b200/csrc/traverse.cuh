@@ -81,8 +81,16 @@ static __device__ __noinline__ void edges_fp64(float Ax, float Ay, float Bx, flo
 
 // Two-sided watertight triangle test.  On a hit inside (tmin, tmax) updates
 // tmax and the barycentrics of v1 (u) and v2 (v).
+// A hit replaces the current one if it is nearer, or as near and of a lower
+// primitive id: the closest hit then does not depend on the order in which a
+// traversal meets the primitives (binary or wide nodes, any child order).
+__device__ __forceinline__ bool nearer(float t, float tmax, uint32_t id, uint32_t cur)
+{
+    return t < tmax || (t == tmax && cur != 0xffffffffu && id < cur);
+}
+
 __device__ __forceinline__ bool hit_triangle(const RayPre &r, float3 v0, float3 v1, float3 v2, float tmin,
-                                             float &tmax, float &bu, float &bv)
+                                             float &tmax, float &bu, float &bv, uint32_t id, uint32_t cur)
 {
     float3 A = make_float3(v0.x - r.o.x, v0.y - r.o.y, v0.z - r.o.z);
     float3 B = make_float3(v1.x - r.o.x, v1.y - r.o.y, v1.z - r.o.z);
@@ -105,7 +113,7 @@ __device__ __forceinline__ bool hit_triangle(const RayPre &r, float3 v0, float3 
     float T = U * Az + V * Bz + W * Cz;
     float rcp = 1.0f / det;
     float t = T * rcp;
-    if (!(t > tmin && t < tmax)) return false;
+    if (!(t > tmin && nearer(t, tmax, id, cur))) return false;
     tmax = t;
     bu = V * rcp;
     bv = W * rcp;
@@ -115,7 +123,8 @@ __device__ __forceinline__ bool hit_triangle(const RayPre &r, float3 v0, float3 
 // Sphere hit only from outside: the nearer root must lie in (tmin, tmax).
 // Discriminant in the form of Haines et al., "Precision Improvements for
 // Ray/Sphere Intersection" (Ray Tracing Gems, 2019); unit direction assumed.
-__device__ __forceinline__ bool hit_sphere(const RayPre &r, float3 c, float rad, float tmin, float &tmax)
+__device__ __forceinline__ bool hit_sphere(const RayPre &r, float3 c, float rad, float tmin, float &tmax, uint32_t id,
+                                           uint32_t cur)
 {
     float3 f = make_float3(r.o.x - c.x, r.o.y - c.y, r.o.z - c.z);
     float b = f.x * r.d.x + f.y * r.d.y + f.z * r.d.z;
@@ -127,7 +136,7 @@ __device__ __forceinline__ bool hit_sphere(const RayPre &r, float3 c, float rad,
     float q = -b - copysignf(sqrtf(disc), b);
     float t0 = cc / q, t1 = q;
     float tn = fminf(t0, t1);
-    if (!(tn > tmin && tn < tmax)) return false;
+    if (!(tn > tmin && nearer(tn, tmax, id, cur))) return false;
     tmax = tn;
     return true;
 }
@@ -227,13 +236,45 @@ template <int FMT>
 __device__ __forceinline__ SceneView scene_view(const DevScene &S)
 {
     SceneView v;
-    v.nodes = FMT == XTGPU_NODES_Q8 ? (const void *)S.nodes8 : (const void *)S.nodes32;
-    v.leaf = S.leaf_prims;
+    if (FMT == XTGPU_NODES_W8) {
+        v.nodes = (const void *)S.nodesW;
+        v.leaf = S.leafW;
+        v.root = S.rootW;
+    } else {
+        v.nodes = FMT == XTGPU_NODES_Q8 ? (const void *)S.nodes8 : (const void *)S.nodes32;
+        v.leaf = S.leaf_prims;
+        v.root = S.root;
+    }
     v.planes = S.planes;
-    v.root = S.root;
     v.n_planes = S.n_planes;
     v.plane_base = (uint32_t)(S.n_tris + S.n_spheres);
     return v;
+}
+
+// Primitive i of the leaf array (3 float4: triangle vertices or sphere centre
+// and radius, the primitive id in the first w).
+__device__ __forceinline__ void prim_test(const float4 *leaf, uint32_t i, const RayPre &r, float tmin, float &tmax,
+                                          uint32_t &prim, float &bu, float &bv)
+{
+    const float4 *lp = leaf + 3 * (size_t)i;
+    float4 a = __ldg(lp), b = __ldg(lp + 1);
+    uint32_t id = __float_as_uint(a.w);
+    if (id & SPHERE_BIT) {
+        id &= ~SPHERE_BIT;
+        if (hit_sphere(r, make_float3(a.x, a.y, a.z), b.x, tmin, tmax, id, prim)) {
+            prim = id;
+            bu = bv = 0.f;
+        }
+    } else {
+        float4 c = __ldg(lp + 2);
+        float u, v;
+        if (hit_triangle(r, make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z), make_float3(c.x, c.y, c.z), tmin,
+                         tmax, u, v, id, prim)) {
+            prim = id;
+            bu = u;
+            bv = v;
+        }
+    }
 }
 
 // Tests the primitives of leaf `ref`; updates tmax / prim / barycentrics.
@@ -241,26 +282,7 @@ __device__ __forceinline__ void leaf_test(const SceneView &V, int32_t ref, const
                                           uint32_t &prim, float &bu, float &bv)
 {
     uint32_t first = leaf_first(ref), cnt = leaf_count(ref);
-    for (uint32_t k = 0; k < cnt; ++k) {
-        const float4 *lp = V.leaf + 3 * (size_t)(first + k);
-        float4 a = __ldg(lp), b = __ldg(lp + 1);
-        uint32_t id = __float_as_uint(a.w);
-        if (id & SPHERE_BIT) {
-            if (hit_sphere(r, make_float3(a.x, a.y, a.z), b.x, tmin, tmax)) {
-                prim = id & ~SPHERE_BIT;
-                bu = bv = 0.f;
-            }
-        } else {
-            float4 c = __ldg(lp + 2);
-            float u, v;
-            if (hit_triangle(r, make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z), make_float3(c.x, c.y, c.z),
-                             tmin, tmax, u, v)) {
-                prim = id;
-                bu = u;
-                bv = v;
-            }
-        }
-    }
+    for (uint32_t k = 0; k < cnt; ++k) prim_test(V.leaf, first + k, r, tmin, tmax, prim, bu, bv);
 }
 
 }  // namespace xtg

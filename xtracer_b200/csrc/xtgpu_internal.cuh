@@ -7,6 +7,8 @@
 //   FP32 BVH node                      4 x float4 (64 B): both child boxes + refs
 //   Q8 BVH node                        2 x uint4 (32 B): origin+exponents, 8-bit
 //                                      child bounds rounded outward, refs
+//   W8 BVH node (8-wide)               5 x uint4 (80 B): origin+exponents, child
+//                                      masks and bases, 48 8-bit child bounds
 //   rays                               float4 (org, tmin) + float4 (dir, tmax)
 //   hits                               (t, prim, u, v) 16 B
 #pragma once
@@ -63,6 +65,10 @@ struct DevScene {
     const float4 *nodes32;     // 4 per node
     const uint4 *nodes8;       // 2 per node
     int32_t root;              // ref of the root (>= 0 node, < 0 leaf)
+    // 8-wide BVH (wide.cu): 5 uint4 per node, its own copy of the primitives
+    const uint4 *nodesW;
+    const float4 *leafW;
+    int32_t rootW;             // 0, or -1 for an empty scene
     int32_t env_type;
     float3 env_a, env_b;
     DevCamera cam;
@@ -79,14 +85,16 @@ struct HostBuf {
 struct xtgpu_scene {
     xtg::DevScene dev{};
     xtg::HostBuf tri_v, tri_n, spheres, planes, prim_obj, obj_material, materials;
-    xtg::HostBuf leaf_prims, nodes32, nodes8;
+    xtg::HostBuf leaf_prims, nodes32, nodes8, nodesW, leafW;
     xtg::HostBuf morton, order, left, right;   // kept for xtgpu_bvh_export
     int64_t n_prims = 0;
     int32_t depth = 0;
     int32_t leaf_size = 2;
     int32_t layout = 0;
     int32_t last_format = XTGPU_NODES_FP32;
-    bool built32 = false, built8 = false;
+    bool built32 = false, built8 = false, builtW = false;
+    int32_t depthW = 0;        // levels of the 8-wide BVH
+    int32_t n_wide = 0;        // its nodes
     int device = 0;
     // host copies used by the service and the tests
     int32_t n_objects = 0;
@@ -116,8 +124,19 @@ xtgpu_status cuda_fail(cudaError_t e, const char *what, const char *file, int li
 xtgpu_status dalloc(HostBuf &b, size_t bytes, cudaStream_t s);
 void dfree(HostBuf &b);
 
-// BVH build (bvh.cu)
+// BVH build (bvh.cu); the 8-wide collapse of the built binary tree (wide.cu)
 xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, int layout, cudaStream_t s);
+xtgpu_status build_wide(xtgpu_scene *sc, cudaStream_t s);
+
+// node formats
+inline bool format_valid(int f) { return f == XTGPU_NODES_FP32 || f == XTGPU_NODES_Q8 || f == XTGPU_NODES_W8; }
+inline bool format_built(const xtgpu_scene *sc, int f)
+{
+    return (f == XTGPU_NODES_FP32 && sc->built32) || (f == XTGPU_NODES_Q8 && sc->built8) ||
+           (f == XTGPU_NODES_W8 && sc->builtW);
+}
+// traversal stack entries (32 or 64) for this scene's tree in format f
+int stack_for_scene(const xtgpu_scene *sc, int f, int requested);
 
 // the tuning a scene renders with: its own if autotuned, else the process-wide one
 const xtgpu_tuning &scene_tuning(const xtgpu_scene *sc);

@@ -71,7 +71,7 @@ def main():
     ap.add_argument("--scene", default="hairball2m")
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--rays", type=int, default=1 << 20)
-    ap.add_argument("--fmt", default="q8", choices=["fp32", "q8"])
+    ap.add_argument("--fmt", default="q8", choices=["fp32", "q8", "w8"])
     ap.add_argument("--iters", type=int, default=5)
     args = ap.parse_args()
     import torch
@@ -79,9 +79,9 @@ def main():
     torch.cuda.set_device(0)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    fmt = xtgpu.NODES_Q8 if args.fmt == "q8" else xtgpu.NODES_FP32
+    fmt = {"fp32": xtgpu.NODES_FP32, "q8": xtgpu.NODES_Q8, "w8": xtgpu.NODES_W8}[args.fmt]
     spec = scenes.jobstream_scene(args.scene, args.scale)
-    sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8))
+    sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8), leaf_size=1)
     side = int(math.ceil(math.sqrt(args.rays)))
     o, d = camera_rays(spec, side, side)
     o, d = o[:args.rays], d[:args.rays]
@@ -107,7 +107,7 @@ def main():
     counts = (C.c_uint64 * 2)()
     xtgpu.check(L.xtgpu_trace_counts(sc.handle, n, ptr(org), ptr(dr), ptr(hits_d), fmt, counts, sh))
     vn, vp = counts[0] / n, counts[1] / n
-    node_bytes = 32 if fmt == xtgpu.NODES_Q8 else 64
+    node_bytes = xtgpu.NODE_BYTES[fmt]
     bpr = 32 + 16 + vn * node_bytes + vp * 48
     times = []
     for _ in range(args.iters):

@@ -25,7 +25,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libxtgpu.so")
 
 STENCIL, DEPTH, AO, PATHTRACER = 0, 1, 2, 3
-NODES_FP32, NODES_Q8 = 0, 1
+NODES_FP32, NODES_Q8, NODES_W8 = 0, 1, 2
+# bytes one node visit reads, per format
+NODE_BYTES = {NODES_FP32: 64, NODES_Q8: 32, NODES_W8: 80}
 STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "NOMEM", 4: "LIMIT", 5: "TIMEOUT", 6: "NOT_FOUND", 7: "STATE"}
 
 
@@ -62,7 +64,8 @@ class BvhOpts(C.Structure):
 
 class BvhInfo(C.Structure):
     _fields_ = [("n_prims", C.c_int64), ("depth", C.c_int32), ("leaf_size", C.c_int32),
-                ("node_bytes_fp32", C.c_uint64), ("node_bytes_q8", C.c_uint64)]
+                ("node_bytes_fp32", C.c_uint64), ("node_bytes_q8", C.c_uint64), ("node_bytes_w8", C.c_uint64),
+                ("depth_w8", C.c_int32)]
 
 
 class Hit(C.Structure):
@@ -96,7 +99,7 @@ class Tuning(C.Structure):
     _fields_ = [("extend_variant", C.c_int32), ("extend_block", C.c_int32), ("extend_blocks_per_sm", C.c_int32),
                 ("tile", C.c_int32), ("wave_paths", C.c_int64), ("leaf_size", C.c_int32),
                 ("node_layout", C.c_int32), ("refill_threshold", C.c_int32), ("extend_min_blocks", C.c_int32),
-                ("stack_entries", C.c_int32)]
+                ("stack_entries", C.c_int32), ("steps_per_vote", C.c_int32)]
 
 
 def get_tuning() -> "Tuning":
