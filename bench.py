@@ -120,6 +120,11 @@ def measured_peaks():
 
 # ---------------------------------------------------------------------------
 SERVED_FORMAT = 2   # xtgpu.NODES_W8: 8-wide BVH, 8-bit quantised child bounds
+# DRAM bytes (read + write) per ray of the served extend kernel, from one ncu
+# capture of k_extend_pool<W8> on 1,048,576 hairball2m first-bounce rays
+# (profiles/k_extend_pool_w8_hairball2m_bounce_ncu.md); the roofline's
+# traffic is this figure times the rays of an average launch.
+NCU_TRAFFIC_BYTES_PER_RAY = 104.0
 
 
 def build_scenes(scale, autotune=False):
@@ -329,6 +334,8 @@ def main():
     ext_s = rst.extend_ms / 1000.0
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / ext_s / 1e9 if ext_s > 0 else None
+    rays_per_launch = float(per_scene.sum()) / max(1, rst.extend_launches)
+    traffic = NCU_TRAFFIC_BYTES_PER_RAY * rays_per_launch
 
     # end to end: same steps, every frame copied to host memory by the service
     e2e_svc = Service(gscenes, node_format=SERVED_FORMAT, use_graphs=True, merge_jobs=True, memory_budget=budget,
@@ -425,7 +432,11 @@ def main():
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 64 * len(timed[0]),
                     "d2h_bytes_per_step": d2h // max(1, len(timed))},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "traffic_source": "ncu DRAM read+write of k_extend_pool<W8> on 1M hairball2m bounce "
+                                           "rays, %.0f B/ray, times %.0f rays per launch" %
+                                           (NCU_TRAFFIC_BYTES_PER_RAY, rays_per_launch),
+                         "algorithmic_bytes_per_launch": alg_bytes / max(1, rst.extend_launches),
                          "kernel": "k_extend (closest-hit traversal)", "peak_kind": peak_kind,
                          "extend_ms": rst.extend_ms, "extend_launches": rst.extend_launches,
                          "timing": "CUDA events around every extend launch, same steps, one wave in flight",
