@@ -495,11 +495,12 @@ __global__ void __launch_bounds__(MINB > 0 ? 128 : 256, MINB > 0 ? MINB : 1)
     const unsigned lt = (1u << lane) - 1u;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(q.rays, (unsigned long long)n);
     const float4 *org = q.org[side], *dir = q.dir[side];
-    SceneView V = scene_view<FMT>(S1);
     RayPre r;
     float tmin = 0.f, tmax = 0.f, bu = 0.f, bv = 0.f;
     uint32_t prim = 0xffffffffu, nv = 0, np = 0, guard = 0, oct = 0;
-    int32_t cur = 0;
+    int32_t cur = 0, scn = 0;   // scene of the ray (several scenes): its view is
+                                // reloaded from the table each step (L1) rather
+                                // than held in registers
     int idx = 0, sp = 0;
     uint2 stack[STACK];
     bool active = false, exhausted = false;
@@ -521,10 +522,10 @@ __global__ void __launch_bounds__(MINB > 0 ? 128 : 256, MINB > 0 ? MINB : 1)
                     tmin = a.w;
                     tmax = b.w;
                     if (MULTI || q.job_rays) jb = q.meta[side][idx].y;
-                    if (MULTI) V = scene_view<FMT>(scenes[jobs[jb].scene]);
+                    if (MULTI) scn = jobs[jb].scene;
                     prim = 0xffffffffu;
                     bu = bv = 0.f;
-                    cur = V.root;
+                    cur = (MULTI ? scene_view<FMT>(scenes[scn]) : scene_view<FMT>(S1)).root;
                     oct = ray_octant(r);
                     sp = 0;
                     nv = np = guard = 0;
@@ -544,6 +545,7 @@ __global__ void __launch_bounds__(MINB > 0 ? 128 : 256, MINB > 0 ? MINB : 1)
         if (!active) continue;
         bool done = false;
         for (int k = 0; k < ksteps && !done; ++k) {
+            const SceneView V = MULTI ? scene_view<FMT>(scenes[scn]) : scene_view<FMT>(S1);
             if (++guard > (1u << 22)) {   // corrupted tree: report, never loop forever
                 q.ctl[3] = 1;
                 done = true;
@@ -555,6 +557,7 @@ __global__ void __launch_bounds__(MINB > 0 ? 128 : 256, MINB > 0 ? MINB : 1)
             }
         }
         if (done) {
+            const SceneView V = MULTI ? scene_view<FMT>(scenes[scn]) : scene_view<FMT>(S1);
             for (int p = 0; p < V.n_planes; ++p)
                 if (hit_plane(r, __ldg(V.planes + p), tmin, tmax)) {
                     prim = V.plane_base + (uint32_t)p;

@@ -21,10 +21,20 @@ constexpr int WIDE_MAX_LEAF = 3;
 
 __device__ __forceinline__ float q8(uint32_t w, int k) { return (float)((w >> (8 * k)) & 0xFFu); }
 
-// Ray sign bits: bit k set if direction component k is negative.
+// Ray sign bits: bit k set if component k of the (clamped) inverse direction
+// is negative; a zero component counts by the sign of its clamped inverse.
 __device__ __forceinline__ uint32_t ray_octant(const RayPre &r)
 {
-    return (r.d.x < 0.f ? 1u : 0u) | (r.d.y < 0.f ? 2u : 0u) | (r.d.z < 0.f ? 4u : 0u);
+    return (r.inv.x < 0.f ? 1u : 0u) | (r.inv.y < 0.f ? 2u : 0u) | (r.inv.z < 0.f ? 4u : 0u);
+}
+
+// Bit s of x moved to bit s ^ m (8 bits).
+__device__ __forceinline__ uint32_t permute_xor8(uint32_t x, uint32_t m)
+{
+    if (m & 1u) x = ((x & 0x55u) << 1) | ((x >> 1) & 0x55u);
+    if (m & 2u) x = ((x & 0x33u) << 2) | ((x >> 2) & 0x33u);
+    if (m & 4u) x = ((x & 0x0Fu) << 4) | ((x >> 4) & 0x0Fu);
+    return x;
 }
 
 // One step: visits `node`, tests its hit leaf primitives and sets `node` to
@@ -36,7 +46,7 @@ __device__ __forceinline__ bool wide_step(const SceneView &V, const RayPre &r, u
                                           uint2 *stack, int32_t *ctl_overflow, uint32_t &nv, uint32_t &np)
 {
     const uint4 *p = (const uint4 *)V.nodes + 5 * (size_t)node;
-    const uint4 w0 = __ldg(p), w1 = __ldg(p + 1), w2 = __ldg(p + 2), w3 = __ldg(p + 3), w4 = __ldg(p + 4);
+    const uint4 w0 = __ldg(p), w1 = __ldg(p + 1);
     ++nv;
     const float sx = __uint_as_float((w0.x & 0xFFu) << 23) * r.inv.x;
     const float sy = __uint_as_float((w0.y & 0xFFu) << 23) * r.inv.y;
@@ -45,24 +55,36 @@ __device__ __forceinline__ bool wide_step(const SceneView &V, const RayPre &r, u
     const float by = fmaf(__uint_as_float(w0.y & ~0xFFu), r.inv.y, -r.oinv.y);
     const float bz = fmaf(__uint_as_float(w0.z & ~0xFFu), r.inv.z, -r.oinv.z);
     const uint32_t imask = w0.w;
-    const uint32_t meta[2] = {w1.z, w1.w};
-    // qlo.x w2.x,w2.y  qlo.y w2.z,w2.w  qlo.z w3.x,w3.y  qhi.x w3.z,w3.w  qhi.y w4.x,w4.y  qhi.z w4.z,w4.w
-    const uint32_t lx[2] = {w2.x, w2.y}, ly[2] = {w2.z, w2.w}, lz[2] = {w3.x, w3.y};
-    const uint32_t hx[2] = {w3.z, w3.w}, hy[2] = {w4.x, w4.y}, hz[2] = {w4.z, w4.w};
-    uint32_t hits = 0, leaves = 0;
+    // bound words, 4 slots each: qlo.x at word 8+h, qlo.y 10+h, qlo.z 12+h,
+    // qhi.x 14+h, qhi.y 16+h, qhi.z 18+h (h = 0 for slots 0-3, 1 for 4-7);
+    // one half at a time keeps fewer words live.  The near plane of an axis is
+    // its lower bound when the ray goes up that axis, else the upper one, so
+    // each bound takes one FMA and no swap.  An unused slot (qlo 255 > qhi 0)
+    // is behind its own far plane and never hits.
+    const uint32_t *qw = (const uint32_t *)(p + 2);
+    uint32_t hitbits = 0;
+#pragma unroll 1
+    for (int h = 0; h < 2; ++h) {
+        const uint32_t lx = __ldg(qw + h), ly = __ldg(qw + 2 + h), lz = __ldg(qw + 4 + h);
+        const uint32_t hx = __ldg(qw + 6 + h), hy = __ldg(qw + 8 + h), hz = __ldg(qw + 10 + h);
+        const uint32_t nx = (m & 1u) ? hx : lx, fx = (m & 1u) ? lx : hx;
+        const uint32_t ny = (m & 2u) ? hy : ly, fy = (m & 2u) ? ly : hy;
+        const uint32_t nz = (m & 4u) ? hz : lz, fz = (m & 4u) ? lz : hz;
 #pragma unroll
-    for (int s = 0; s < 8; ++s) {
-        const int h = s >> 2, k = s & 3;
-        const uint32_t mb = (meta[h] >> (8 * k)) & 0xFFu;
-        const bool inner = (imask >> s) & 1u;
-        if (!inner && mb == 0u) continue;   // unused slot
-        const float tx0 = fmaf(q8(lx[h], k), sx, bx), tx1 = fmaf(q8(hx[h], k), sx, bx);
-        const float ty0 = fmaf(q8(ly[h], k), sy, by), ty1 = fmaf(q8(hy[h], k), sy, by);
-        const float tz0 = fmaf(q8(lz[h], k), sz, bz), tz1 = fmaf(q8(hz[h], k), sz, bz);
-        float tn;
-        if (!slab_t(tx0, tx1, ty0, ty1, tz0, tz1, tmin, tmax, XTG_TFAR_SCALE_W8, tn)) continue;
-        if (inner) hits |= 1u << (s ^ m);
-        else leaves |= ((1u << (mb >> 5)) - 1u) << (mb & 31u);
+        for (int k = 0; k < 4; ++k) {
+            const float tn = fmaxf(fmaxf(fmaf(q8(nx, k), sx, bx), fmaf(q8(ny, k), sy, by)),
+                                   fmaxf(fmaf(q8(nz, k), sz, bz), tmin));
+            const float tf = fminf(fminf(fmaf(q8(fx, k), sx, bx), fmaf(q8(fy, k), sy, by)),
+                                   fminf(fmaf(q8(fz, k), sz, bz), tmax));
+            hitbits |= (tn <= tf * XTG_TFAR_SCALE_W8 ? 1u : 0u) << (4 * h + k);
+        }
+    }
+    uint32_t hits = permute_xor8(hitbits & imask, m);
+    uint32_t leaves = 0;
+    for (uint32_t lh = hitbits & ~imask; lh; lh &= lh - 1u) {
+        const int slot = __ffs(lh) - 1;
+        const uint32_t mb = ((slot < 4 ? w1.z : w1.w) >> (8 * (slot & 3))) & 0xFFu;
+        leaves |= ((1u << (mb >> 5)) - 1u) << (mb & 31u);
     }
     // primitives of the hit leaf children
     const uint32_t pbase = w1.y;
