@@ -142,7 +142,8 @@ def build_scenes(scale, autotune=False):
             for f in (xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8):
                 sc.build_bvh(f, t.leaf_size)
             tunes[name] = {k: getattr(t, k) for k in ("leaf_size", "extend_variant", "steps_per_vote",
-                                                       "stack_entries", "tile", "extend_min_blocks", "wave_paths")}
+                                                       "primary_node_format", "primary_variant", "stack_entries",
+                                                       "tile", "extend_min_blocks", "wave_paths")}
         out.append(sc)
     return specs, out, tunes
 
@@ -315,9 +316,13 @@ def main():
     value = rays_all / t_max / 1e6
     lat_all = D.gather(lat)
 
-    # roofline of the extend kernel: the same steps again, one wave at a time
-    # so that each extend launch's CUDA-event duration is its own (with two
-    # waves in flight, launches share the SMs with the other wave's kernels)
+    # roofline of the W8 extend kernel: the same steps again, one wave at a time
+    # (with two waves in flight, an extend launch's CUDA-event span includes the
+    # other wave's kernels), every pass on W8 nodes so that the timed launches
+    # and the counted node visits are all of that kernel
+    saved = [{k: getattr(sc.tuning(), k) for k, _ in xtgpu.Tuning._fields_} for sc in gscenes]
+    for sc in gscenes:
+        sc.set_tuning(primary_node_format=-1)
     rsvc = Service(gscenes, node_format=SERVED_FORMAT, use_graphs=True, merge_jobs=True, memory_budget=budget,
                    time_kernels=True, waves_in_flight=1, stream=stream)
     run_slice(rsvc, slices[0])
@@ -328,6 +333,8 @@ def main():
     rst = rsvc.stats()
     rsvc.close()
     bpr = roofline_bytes_per_ray(specs, gscenes, SERVED_FORMAT)
+    for sc, t in zip(gscenes, saved):
+        sc.set_tuning(**t)
     scene_bpr = [b["bytes_per_ray"] for b in bpr]
     # rays of each scene in the timed steps times that scene's bytes per ray
     alg_bytes = float(np.dot(per_scene, scene_bpr))
@@ -376,6 +383,20 @@ def main():
         s1.record()
         torch.cuda.synchronize()
         ss = s0.elapsed_time(s1) / 1000.0
+        # the served form with W8 nodes for the camera rays too (no binary pass)
+        saved = [{k: getattr(sc.tuning(), k) for k, _ in xtgpu.Tuning._fields_} for sc in gscenes]
+        for sc in gscenes:
+            sc.set_tuning(primary_node_format=-1)
+        run_slice(served, slices[0])   # captures the graphs of this tuning
+        torch.cuda.synchronize()
+        w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0.record()
+        wr, _ = run_slice(served, timed[0])
+        w1.record()
+        torch.cuda.synchronize()
+        w8_only = wr / (w0.elapsed_time(w1) / 1000.0) / 1e6
+        for sc, t in zip(gscenes, saved):
+            sc.set_tuning(**t)
         # the served form with the other node formats on that step
         other = {}
         for fname, f in (("fp32", xtgpu.NODES_FP32), ("q8", xtgpu.NODES_Q8)):
@@ -393,6 +414,7 @@ def main():
         plain = {"value": pr / ps / 1e6, "unit": "Mrays/s", "step_jobs": len(timed[0]),
                  "p50_ms": 1000 * pct(pl, 50), "p99_ms": 1000 * pct(pl, 99),
                  "served_same_step_mrays": sr / ss / 1e6, "speedup": (sr / ss) / (pr / ps),
+                 "served_w8_only_same_step_mrays": w8_only,
                  "served_fp32_same_step_mrays": other["fp32"], "served_q8_same_step_mrays": other["q8"],
                  "form": "one job per launch, FP32 BVH, no CUDA graphs"}
 
@@ -425,7 +447,9 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single",
                        "cache": "inputs larger than L2 (resident scenes ~%.0f MB)" %
                                 (sum(s.device_bytes() for s in gscenes) / 1e6),
-                       "wave_paths": 1 << 22, "node_format": "w8 (8-wide, 8-bit quantised)", "cuda_graphs": True, "waves_in_flight": 2,
+                       "wave_paths": 1 << 22, "node_format": "w8 (8-wide, 8-bit quantised) for bounce rays; camera rays as tuned "
+                                      "per scene (primary_node_format: 0 = binary FP32, -1 = w8)",
+                       "cuda_graphs": True, "waves_in_flight": 2,
                        "autotuned": tunes},
             "p50_ms": 1000 * pct(lat_all, 50), "p99_ms": 1000 * pct(lat_all, 99),
             "latency_open_loop": latency, "plain": plain,
@@ -437,9 +461,11 @@ def main():
                                            "rays, %.0f B/ray, times %.0f rays per launch" %
                                            (NCU_TRAFFIC_BYTES_PER_RAY, rays_per_launch),
                          "algorithmic_bytes_per_launch": alg_bytes / max(1, rst.extend_launches),
-                         "kernel": "k_extend (closest-hit traversal)", "peak_kind": peak_kind,
+                         "kernel": "k_extend_pool<W8> / k_extend_batch<W8> (closest-hit traversal, 8-wide "
+                                   "quantised nodes)", "peak_kind": peak_kind,
                          "extend_ms": rst.extend_ms, "extend_launches": rst.extend_launches,
-                         "timing": "CUDA events around every extend launch, same steps, one wave in flight",
+                         "timing": "CUDA events around every extend launch, same steps, one wave in flight, "
+                                   "all passes on W8 nodes",
                          "bytes_per_ray": {b["scene"]: round(b["bytes_per_ray"], 1) for b in bpr},
                          "nodes_per_ray": {b["scene"]: round(b["nodes_per_ray"], 2) for b in bpr},
                          "prims_per_ray": {b["scene"]: round(b["prims_per_ray"], 2) for b in bpr}},

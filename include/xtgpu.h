@@ -290,6 +290,10 @@ typedef struct {
     int32_t stack_entries;         /* traversal stack: 32 or 64 entries (0 = smallest that
                                       holds the scene's BVH depth) */
     int32_t steps_per_vote;        /* variant 2: traversal steps between refill votes (1..64) */
+    int32_t primary_node_format;   /* node format of the first extend pass of a wave (the
+                                      coherent camera rays) when every scene of the wave
+                                      has it built; -1 = the wave's format */
+    int32_t primary_variant;       /* extend kernel of that pass; -1 = extend_variant */
 } xtgpu_tuning;
 XTGPU_API xtgpu_status xtgpu_get_tuning(xtgpu_tuning *t);
 XTGPU_API xtgpu_status xtgpu_set_tuning(const xtgpu_tuning *t);
@@ -304,6 +308,9 @@ XTGPU_API xtgpu_status xtgpu_autotune(xtgpu_scene *scene, int32_t node_format, d
                                       void *stream);
 /* Tuning stored with a scene (the process-wide one if it was never tuned). */
 XTGPU_API xtgpu_status xtgpu_scene_tuning(const xtgpu_scene *scene, xtgpu_tuning *t);
+/* Sets the tuning the scene renders with (as xtgpu_autotune does); its
+ * leaf_size must be the one the scene's BVH was built with. */
+XTGPU_API xtgpu_status xtgpu_scene_set_tuning(xtgpu_scene *scene, const xtgpu_tuning *tuning);
 
 /* Text of the last error on this thread ("" if none). */
 XTGPU_API const char *xtgpu_last_error(void);

@@ -224,6 +224,25 @@ def test_extend_variants_agree(variant, refill, steps, fmt):
     assert np.array_equal(ref["t"], got["t"])
 
 
+@pytest.mark.parametrize("pf,pv", [(xtgpu.NODES_FP32, 0), (xtgpu.NODES_W8, 0), (xtgpu.NODES_Q8, 2)])
+def test_primary_pass_format_keeps_frames(pf, pv):
+    """The camera rays may take another node format and extend kernel than the
+    bounce rays; every format and kernel returns the same hits, so the frames
+    are the same bit for bit."""
+    spec, w, h = small_scenes()["hairball20k"]
+    sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8), leaf_size=1)
+    ref, rr = sc.render(xtgpu.PATHTRACER, w, h, spp=8, rdepth=4, seed=9, node_format=xtgpu.NODES_W8)
+    keep = {k: getattr(xtgpu.get_tuning(), k) for k, _ in xtgpu.Tuning._fields_}
+    try:
+        xtgpu.set_tuning(primary_node_format=pf, primary_variant=pv)
+        got, rg = sc.render(xtgpu.PATHTRACER, w, h, spp=8, rdepth=4, seed=9, node_format=xtgpu.NODES_W8)
+    finally:
+        xtgpu.set_tuning(**keep)
+    sc.close()
+    assert rr == rg
+    assert np.array_equal(ref, got)
+
+
 @pytest.mark.parametrize("integ", [xtgpu.STENCIL, xtgpu.DEPTH, xtgpu.AO, xtgpu.PATHTRACER])
 def test_w8_frames_equal_fp32(integ):
     spec, w, h = small_scenes()["terrain20k"]

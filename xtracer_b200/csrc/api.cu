@@ -132,19 +132,41 @@ xtgpu_status xtgpu_scene_tuning(const xtgpu_scene *sc, xtgpu_tuning *t)
     return XTGPU_OK;
 }
 
+static bool tuning_valid(const xtgpu_tuning *t)
+{
+    return t && t->extend_variant >= 0 && t->extend_variant <= 2 && t->steps_per_vote >= 1 &&
+           t->steps_per_vote <= 64 && t->primary_node_format >= -1 && t->primary_node_format <= XTGPU_NODES_W8 &&
+           t->primary_variant >= -1 && t->primary_variant <= 2 && t->extend_block >= 32 && t->extend_block <= 256 &&
+           !(t->extend_block & 31) && t->extend_blocks_per_sm >= 1 && t->extend_blocks_per_sm <= 64 && t->tile >= 0 &&
+           t->tile <= 256 && t->wave_paths >= 1024 && t->wave_paths <= (1ll << 26) && t->leaf_size >= 1 &&
+           t->leaf_size <= MAX_LEAF && t->node_layout >= 0 && t->node_layout <= 1 && t->refill_threshold >= 1 &&
+           t->refill_threshold <= 32 &&
+           (t->extend_min_blocks == 0 || t->extend_min_blocks == 8 || t->extend_min_blocks == 10) &&
+           (t->stack_entries == 0 || t->stack_entries == 32 || t->stack_entries == 64);
+}
+
 xtgpu_status xtgpu_set_tuning(const xtgpu_tuning *t)
 {
-    if (!t || t->extend_variant < 0 || t->extend_variant > 2 || t->steps_per_vote < 1 || t->steps_per_vote > 64 || t->extend_block < 32 || t->extend_block > 256 ||
-        (t->extend_block & 31) || t->extend_blocks_per_sm < 1 || t->extend_blocks_per_sm > 64 || t->tile < 0 ||
-        t->tile > 256 || t->wave_paths < 1024 || t->wave_paths > (1ll << 26) || t->leaf_size < 1 ||
-        t->leaf_size > MAX_LEAF || t->node_layout < 0 || t->node_layout > 1 || t->refill_threshold < 1 ||
-        t->refill_threshold > 32 ||
-        !(t->extend_min_blocks == 0 || t->extend_min_blocks == 8 || t->extend_min_blocks == 10) ||
-        !(t->stack_entries == 0 || t->stack_entries == 32 || t->stack_entries == 64)) {
+    if (!tuning_valid(t)) {
         set_error("xtgpu_set_tuning: value out of range");
         return XTGPU_ERR_INVALID;
     }
     tuning() = *t;
+    return XTGPU_OK;
+}
+
+xtgpu_status xtgpu_scene_set_tuning(xtgpu_scene *sc, const xtgpu_tuning *t)
+{
+    if (!sc || !tuning_valid(t)) {
+        set_error("xtgpu_scene_set_tuning: NULL scene or value out of range");
+        return XTGPU_ERR_INVALID;
+    }
+    if (t->leaf_size != sc->leaf_size) {
+        set_error("xtgpu_scene_set_tuning: leaf_size differs from the built BVH (rebuild it instead)");
+        return XTGPU_ERR_STATE;
+    }
+    sc->tune = *t;
+    sc->tuned = true;
     return XTGPU_OK;
 }
 const char *xtgpu_version(void) { return "xtgpu 0.1 (sm_100a)"; }
@@ -499,6 +521,12 @@ xtgpu_status xtg::render_impl(xtgpu_scene *sc, const xtgpu_render_params *p, flo
     XTG_TRY(R->set_scenes(&sc->dev, 1, s));
     R->T = T;
     R->stack = stack_for_scene(sc, p->node_format, T.stack_entries);
+    R->fmt0 = -1;
+    if (T.primary_node_format >= 0 && T.primary_node_format != p->node_format &&
+        format_built(sc, T.primary_node_format)) {
+        R->fmt0 = T.primary_node_format;
+        R->stack0 = stack_for_scene(sc, R->fmt0, T.stack_entries);
+    }
     XTG_CUDA(cudaMemsetAsync(R->q.ctl, 0, 64, s));
     XTG_CUDA(cudaMemsetAsync(rgba, 0, sizeof(float4) * npix, s));
     DevJob J{};

@@ -122,6 +122,8 @@ extern "C" xtgpu_status xtgpu_autotune(xtgpu_scene *sc, int32_t fmt, double budg
         }
     };
     knob(&xtgpu_tuning::extend_variant, {0, 2});
+    if (fmt != XTGPU_NODES_FP32 && sc->built32) knob(&xtgpu_tuning::primary_node_format, {-1, XTGPU_NODES_FP32});
+    knob(&xtgpu_tuning::primary_variant, {-1, 0, 2});
     if (T.extend_variant == 2) knob(&xtgpu_tuning::steps_per_vote, {4, 8, 16});
     if ((fmt == XTGPU_NODES_W8 ? sc->depthW : sc->depth) <= 30) knob(&xtgpu_tuning::stack_entries, {32, 64});
     knob(&xtgpu_tuning::extend_min_blocks, {0, 8, 10});

@@ -939,11 +939,19 @@ void WaveRunner::enqueue(int njobs, int64_t total, int bounces, int fmt, bool mu
     int gb = sms * 8;
     k_camera<<<gb, 256, 0, s>>>(jobs, scenes, q);
     int side = 0;
+    // the first pass (camera rays) may use its own node format and kernel
+    xtgpu_tuning T0 = T;
+    if (T.primary_variant >= 0) T0.extend_variant = T.primary_variant;
+    const bool own0 = fmt0 >= 0 && fmt0 != fmt;
     for (int b = 0; b < bounces; ++b) {
         cudaMemsetAsync(q.ctl + 2, 0, sizeof(int32_t), s);
 
         if (time_extend && b < MAX_TIMED) rec(ev[2 * b]);
-        launch_extend_kernel(T, fmt, multi, single, scenes, jobs, q, side, sms, stack, s);
+        if (b == 0)
+            launch_extend_kernel(T0, own0 ? fmt0 : fmt, multi, single, scenes, jobs, q, side, sms, own0 ? stack0 : stack,
+                                 s);
+        else
+            launch_extend_kernel(T, fmt, multi, single, scenes, jobs, q, side, sms, stack, s);
         if (time_extend && b < MAX_TIMED) rec(ev[2 * b + 1]);
         cudaMemsetAsync(q.ctl + (side ^ 1), 0, sizeof(int32_t), s);
         k_shade<<<gb, 256, 0, s>>>(jobs, scenes, q, side);
@@ -1009,11 +1017,11 @@ xtgpu_status WaveRunner::run_wave(const std::vector<DevJob> &jobs, int bounces, 
     if (use_graph) {
         // One graph per (bounces, format, scene count) shape; kernel arguments
         // point at fixed buffers, so a graph replays any wave of that shape.
-        uint64_t key = ((uint64_t)bounces << 4) ^ (uint64_t)fmt ^ (multi ? 2ull : 0ull) ^ (time_extend ? 4ull : 0ull) ^
-                       (defer_acc ? (1ull << 48) : 0ull) ^
-                       (q.stats ? 8ull : 0ull) ^ ((uint64_t)stack << 12) ^ ((uint64_t)T.extend_min_blocks << 20) ^
-                       ((uint64_t)T.extend_variant << 28) ^ ((uint64_t)T.extend_blocks_per_sm << 32) ^
-                       ((uint64_t)T.extend_block << 40);
+        // every value the captured launches depend on
+        const GraphKey key = {bounces, fmt, multi ? 1 : 0, time_extend ? 1 : 0, defer_acc ? 1 : 0,
+                              q.stats ? 1 : 0, stack, T.extend_min_blocks, T.extend_variant,
+                              T.extend_blocks_per_sm, T.extend_block, T.refill_threshold, T.steps_per_vote,
+                              fmt0, T.primary_variant, stack0};
         auto it = graphs.find(key);
         if (it == graphs.end()) {
             cudaGraph_t g;
@@ -1061,9 +1069,10 @@ xtgpu_status WaveRunner::read_ctl(int32_t *overflow, unsigned long long *rays, c
 // Defaults from sweeps on a B200 (variant x leaf x node format x launch shape x
 // tile x register cap over terrain, hairball and sphere scenes, and the served
 // job stream): pooled lanes refilled when 8 are idle with a vote every 8 steps,
-// one primitive per leaf, depth-first node order, 8x8 pixel tiles, and 64
-// registers (8 resident 128-thread blocks per SM).
-static xtgpu_tuning g_tuning = {2, 128, 8, 8, 1ll << 22, 1, 1, 8, 8, 0, 8};
+// one primitive per leaf, depth-first node order, 8x8 pixel tiles, 64
+// registers (8 resident 128-thread blocks per SM); camera rays, which are
+// coherent, through binary FP32 nodes with warp-batched fetch.
+static xtgpu_tuning g_tuning = {2, 128, 8, 8, 1ll << 22, 1, 1, 8, 8, 0, 8, XTGPU_NODES_FP32, 0};
 xtgpu_tuning &tuning() { return g_tuning; }
 
 void launch_extend_kernel(const xtgpu_tuning &T, int fmt, bool multi, const DevScene &single,

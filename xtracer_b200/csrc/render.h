@@ -1,7 +1,8 @@
 // Host side of the wavefront: queue buffers, job table, CUDA-graph cache.
 #pragma once
 
-#include <unordered_map>
+#include <array>
+#include <map>
 #include <vector>
 
 #include "wavefront.cuh"
@@ -50,7 +51,10 @@ struct WaveRunner {
     DevScene single{};
     xtgpu_tuning T{};   // launch configuration of the next waves
     int stack = 64;     // traversal stack entries (32 or 64)
-    std::unordered_map<uint64_t, cudaGraphExec_t> graphs;
+    int fmt0 = -1;      // node format of the first extend pass (-1 = the wave's)
+    int stack0 = 64;    // its stack entries
+    using GraphKey = std::array<int32_t, 16>;
+    std::map<GraphKey, cudaGraphExec_t> graphs;
 
     xtgpu_status init(int64_t capacity, int max_jobs, int max_scenes, cudaStream_t s);
     void release();

@@ -182,6 +182,22 @@ static xtgpu_status launch_wave(xtgpu_service *v, WaveSlot &W, cudaEvent_t prev_
                 stack = std::max(stack, stack_for_scene(v->scenes[k], v->o.node_format,
                                                         scene_tuning(v->scenes[k]).stack_entries));
         W.R.stack = stack;
+        // first pass in its own format if every scene of the wave has it
+        const int pf = W.R.T.primary_node_format;
+        W.R.fmt0 = -1;
+        if (pf >= 0 && pf != v->o.node_format) {
+            bool ok = true;
+            int st0 = 32;
+            for (size_t k = 0; k < per.size(); ++k)
+                if (per[k] > 0) {
+                    ok = ok && format_built(v->scenes[k], pf);
+                    st0 = std::max(st0, stack_for_scene(v->scenes[k], pf, scene_tuning(v->scenes[k]).stack_entries));
+                }
+            if (ok) {
+                W.R.fmt0 = pf;
+                W.R.stack0 = st0;
+            }
+        }
     }
     // frames of newly admitted jobs are allocated and zeroed on the service stream
     XTG_CUDA(cudaEventRecord(v->admitted, v->s));

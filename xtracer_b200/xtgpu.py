@@ -99,7 +99,8 @@ class Tuning(C.Structure):
     _fields_ = [("extend_variant", C.c_int32), ("extend_block", C.c_int32), ("extend_blocks_per_sm", C.c_int32),
                 ("tile", C.c_int32), ("wave_paths", C.c_int64), ("leaf_size", C.c_int32),
                 ("node_layout", C.c_int32), ("refill_threshold", C.c_int32), ("extend_min_blocks", C.c_int32),
-                ("stack_entries", C.c_int32), ("steps_per_vote", C.c_int32)]
+                ("stack_entries", C.c_int32), ("steps_per_vote", C.c_int32),
+                ("primary_node_format", C.c_int32), ("primary_variant", C.c_int32)]
 
 
 def get_tuning() -> "Tuning":
@@ -155,6 +156,7 @@ SIGNATURES = {
     "xtgpu_set_tuning": [C.c_void_p],
     "xtgpu_autotune": [C.c_void_p, C.c_int32, C.c_double, C.c_void_p, C.c_void_p],
     "xtgpu_scene_tuning": [C.c_void_p, C.c_void_p],
+    "xtgpu_scene_set_tuning": [C.c_void_p, C.c_void_p],
 }
 
 _lib = None
@@ -262,6 +264,13 @@ class Scene:
         t = Tuning()
         check(lib().xtgpu_scene_tuning(self.handle, C.byref(t)))
         return t
+
+    def set_tuning(self, **kw) -> None:
+        """Changes fields of the tuning this scene renders with."""
+        t = self.tuning()
+        for k, v in kw.items():
+            setattr(t, k, v)
+        check(lib().xtgpu_scene_set_tuning(self.handle, C.byref(t)))
 
     def close(self) -> None:
         if getattr(self, "handle", None):
