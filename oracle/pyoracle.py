@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(HERE, "_build", "libxtoracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "xtref")
 
 XO_ACCEL_OCTREE, XO_ACCEL_BVH = 0, 1
-STENCIL, DEPTH, AO, PATHTRACER = 0, 1, 2, 3
+STENCIL, DEPTH, AO, PATHTRACER, NORMAL, UV, EMISSION, WIREFRAME = 0, 1, 2, 3, 4, 5, 6, 7
 INTEGRATOR_NAMES = {STENCIL: "stencil", DEPTH: "depth", AO: "ao", PATHTRACER: "pathtracer"}
 
 
@@ -36,7 +36,7 @@ class XoSceneDesc(C.Structure):
                 ("n_materials", C.c_int32), ("materials", C.c_void_p),
                 ("env_type", C.c_int32), ("env_a", C.c_float * 3), ("env_b", C.c_float * 3),
                 ("cam_pos", C.c_float * 3), ("cam_target", C.c_float * 3), ("cam_up", C.c_float * 3),
-                ("cam_fov", C.c_float)]
+                ("cam_fov", C.c_float), ("obj_uv_scale", C.c_void_p), ("tri_uvs", C.c_void_p)]
 
 
 class XoRenderParams(C.Structure):
@@ -129,6 +129,10 @@ class OracleScene:
         d.cam_target[:] = list(spec.camera.target)
         d.cam_up[:] = list(spec.camera.up)
         d.cam_fov = spec.camera.fov
+        uvs = getattr(spec, "obj_uv_scale", None)
+        d.obj_uv_scale = _ptr(arr(uvs.reshape(-1), np.float32)) if uvs is not None else None
+        tuv = getattr(spec, "tri_uvs", None)
+        d.tri_uvs = _ptr(arr(tuv.reshape(-1), np.float32)) if tuv is not None else None
         self._desc = d
         h = C.c_void_p()
         if lib().xo_scene_create(C.byref(d), accel, C.byref(h)) != 0:

@@ -32,6 +32,7 @@
 #include <xtcore/strpool.h>
 #include <xtcore/context.h>
 #include <xtcore/integrator.h>
+#include <xtcore/integrator/wireframe/integrator.h>
 #include <xtcore/parseutil.h>
 #include <xtcore/mesh.h>
 #include <xtcore/octree.h>
@@ -179,6 +180,10 @@ static int mode_render(int argc, char **argv)
     if (integ == "stencil") ig = new xtcore::integrator::stencil::Integrator();
     else if (integ == "depth") ig = new xtcore::integrator::depth::Integrator();
     else if (integ == "pathtracer") ig = new xtcore::integrator::pathtracer::Integrator();
+    else if (integ == "normal") ig = new xtcore::integrator::normal::Integrator();
+    else if (integ == "uv") ig = new xtcore::integrator::uv::Integrator();
+    else if (integ == "emission") ig = new xtcore::integrator::emission::Integrator();
+    else if (integ == "wireframe") ig = new xtcore::integrator::wireframe::Integrator();
     else if (integ == "ao") {
         if (ao_maxd == 100.0f) ig = new xtcore::integrator::ao::Integrator();
         else ig = new AoWithDistance(ao_maxd);

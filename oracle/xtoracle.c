@@ -18,6 +18,7 @@
 #include <string.h>
 
 #define XO_EPS 1e-8                    /* EPSILON, lib/nmath/precision.h:87-89 */
+#define XO_PI 3.14159265358979323846   /* nmath::PI, lib/nmath/precision.h:101 */
 #define XO_RADIAN 0.017453292519943    /* RADIAN, lib/nmath/precision.h:111 */
 #define XO_OCT_MAX_ITEMS 10            /* LIMITS_MAX_ITEMS_PER_NODE, mesh.h:11 */
 #define XO_OCT_MAX_DEPTH 10            /* LIMITS_MAX_DEPTH, mesh.h:12 */
@@ -183,10 +184,12 @@ typedef struct {
     int hit;
     double t;
     v3 point, normal;
+    double tu, tv;   /* hit_record_t::texcoord */
 } hrec;
 
-/* Sphere::intersection, math/sphere.cc:25-62 (the active #if 1 branch) */
-static int hit_sphere(v3 c, double radius, v3 o, v3 d, hrec *h)
+/* Sphere::intersection, math/sphere.cc:25-62 (the active #if 1 branch); usc is
+ * the surface's uv_scale (math/surface.h:26). */
+static int hit_sphere(v3 c, double radius, const double usc[2], v3 o, v3 d, hrec *h)
 {
     double b = 2 * dot(sub(o, c), d);
     double cc = dot(c, c) + dot(o, o) + 2 * dot(neg(c), o) - radius * radius;
@@ -200,6 +203,8 @@ static int hit_sphere(v3 c, double radius, v3 o, v3 d, hrec *h)
             h->t = t;
             h->point = add(o, muls(d, t));
             h->normal = muls(divs(sub(h->point, c), radius), (t1 * t2 > 0. ? 1. : -1));
+            h->tu = asin(h->normal.x / (usc[0] != 0.0f ? usc[0] : 1.0f)) / XO_PI + 0.5;
+            h->tv = asin(h->normal.y / (usc[1] != 0.0f ? usc[1] : 1.0f)) / XO_PI + 0.5;
             return 1;
         }
     }
@@ -207,7 +212,7 @@ static int hit_sphere(v3 c, double radius, v3 o, v3 d, hrec *h)
 }
 
 /* Plane::intersection, math/plane.cc:19-61 */
-static int hit_plane(v3 n, double offset, v3 o, v3 d, hrec *h)
+static int hit_plane(v3 n, double offset, const double usc[2], v3 o, v3 d, hrec *h)
 {
     double n_dot_dir = dot(n, d);
     if (fabs(n_dot_dir) < XO_EPS) return 0;
@@ -219,6 +224,20 @@ static int hit_plane(v3 n, double offset, v3 o, v3 d, hrec *h)
     h->t = t;
     h->point = add(o, muls(d, t));
     h->normal = n;
+    /* texture coordinates, plane.cc:47-58 */
+    v3 nn = normalized(n);
+    v3 uvec = V(nn.y, nn.z, -nn.x);
+    v3 vvec = cross(uvec, nn);
+    double tu = dot(uvec, add(v, h->point)) * usc[0];
+    double tv = dot(vvec, add(v, h->point)) * usc[1];
+    if (tu > 1.f) tu -= (float)(int)tu;
+    if (tv > 1.f) tv -= (float)(int)tv;
+    if (tu < -1.f) tu -= (float)(int)tu;
+    if (tv < -1.f) tv -= (float)(int)tv;
+    if (tu < 0.f) tu = 1.f + tu;
+    if (tv < 0.f) tv = 1.f + tv;
+    h->tu = tu;
+    h->tv = tv;
     return 1;
 }
 
@@ -238,8 +257,9 @@ static v3 tri_bary(const v3 *v, v3 p)
     return V(a0 / area, a1 / area, a2 / area);
 }
 
-/* Triangle::intersection, math/triangle.cc:82-123 (normal: calc_normal :142-147) */
-static int hit_triangle(const v3 *v, const v3 *vn, v3 o, v3 d, hrec *h)
+/* Triangle::intersection, math/triangle.cc:82-123 (normal: calc_normal :142-147);
+ * vt: the three texcoords (tc), z = 0 */
+static int hit_triangle(const v3 *v, const v3 *vn, const v3 *vt, v3 o, v3 d, hrec *h)
 {
     v3 normal = normalized(cross(sub(v[1], v[0]), sub(v[2], v[0])));
     double n_dot_dir = dot(normal, d);
@@ -253,6 +273,9 @@ static int hit_triangle(const v3 *v, const v3 *vn, v3 o, v3 d, hrec *h)
     if (s < 1.0 - XO_EPS || s > 1.0 + XO_EPS) return 0;
     h->t = t;
     h->point = pos;
+    v3 tc = add(add(muls(vt[0], bc.x), muls(vt[1], bc.y)), muls(vt[2], bc.z));
+    h->tu = tc.x;
+    h->tv = tc.y;
     v3 pn = add(add(muls(vn[0], bc.x), muls(vn[1], bc.y)), muls(vn[2], bc.z));
     h->normal = length(pn) ? pn : normal;
     return 1;
@@ -297,6 +320,7 @@ typedef struct {
     int32_t nnodes, cap;
     v3 *tv;           /* 3 vertices per triangle (double) */
     v3 *tn;           /* 3 normals per triangle */
+    v3 *tt;           /* 3 texcoords per triangle (z = 0) */
     v3 *amin, *amax;  /* item AABBs (Triangle::calc_aabb, triangle.cc:125-140) */
     int32_t ntris;
     /* FP64 BVH (XO_ACCEL_BVH) */
@@ -400,7 +424,7 @@ static int32_t otrace(const mesh_t *m, int32_t ni, v3 o, v3 d, hrec *out)
     for (int32_t k = 0; k < n->nitems; ++k) {
         hrec h;
         int32_t it = n->items[k];
-        if (hit_triangle(&m->tv[3 * it], &m->tn[3 * it], o, d, &h) && h.t < best.t) {
+        if (hit_triangle(&m->tv[3 * it], &m->tn[3 * it], &m->tt[3 * it], o, d, &h) && h.t < best.t) {
             best = h;
             closest = it;
         }
@@ -499,7 +523,7 @@ static int32_t btrace(const mesh_t *m, v3 o, v3 d, hrec *out)
             for (int32_t k = n->first; k < n->first + n->count; ++k) {
                 int32_t it = m->bidx[k];
                 hrec h;
-                if (hit_triangle(&m->tv[3 * it], &m->tn[3 * it], o, d, &h) &&
+                if (hit_triangle(&m->tv[3 * it], &m->tn[3 * it], &m->tt[3 * it], o, d, &h) &&
                     (h.t < best.t || (h.t == best.t && it < closest))) {
                     best = h;
                     closest = it;
@@ -535,6 +559,7 @@ int xo_scene_create(const xo_scene_desc *desc, int accel, xo_scene **out)
         m->ntris = count;
         m->tv = (v3 *)malloc(sizeof(v3) * 3 * (size_t)(count ? count : 1));
         m->tn = (v3 *)calloc(3 * (size_t)(count ? count : 1), sizeof(v3));
+        m->tt = (v3 *)calloc(3 * (size_t)(count ? count : 1), sizeof(v3));
         m->amin = (v3 *)malloc(sizeof(v3) * (size_t)(count ? count : 1));
         m->amax = (v3 *)malloc(sizeof(v3) * (size_t)(count ? count : 1));
         for (int32_t i = 0; i < count; ++i) {
@@ -542,6 +567,14 @@ int xo_scene_create(const xo_scene_desc *desc, int accel, xo_scene **out)
             for (int k = 0; k < 3; ++k) {
                 m->tv[3 * i + k] = vf(t + 3 * k);
                 if (desc->tri_normals) m->tn[3 * i + k] = vf(desc->tri_normals + 9 * (size_t)(first + i) + 3 * k);
+                if (desc->tri_uvs) {
+                    const float *uv = desc->tri_uvs + 6 * (size_t)(first + i) + 2 * k;
+                    m->tt[3 * i + k] = V(uv[0], uv[1], 0.0);
+                } else {
+                    /* the Triangle constructor's texcoords (math/triangle.cc:8-13):
+                     * tc[1] is set twice, tc[2] stays zero */
+                    m->tt[3 * i + k] = k == 1 ? V(1.0, 0.0, 0.0) : V(0.0, 0.0, 0.0);
+                }
             }
             /* Triangle::calc_aabb, triangle.cc:125-140 */
             v3 mn = V(INFINITY, INFINITY, INFINITY), mx = V(-INFINITY, -INFINITY, -INFINITY);
@@ -576,7 +609,7 @@ void xo_scene_destroy(xo_scene *s)
     for (int32_t oi = 0; oi < s->d.n_objects; ++oi) {
         mesh_t *m = &s->meshes[oi];
         for (int32_t i = 0; i < m->nnodes; ++i) free(m->nodes[i].items);
-        free(m->nodes); free(m->tv); free(m->tn); free(m->amin); free(m->amax); free(m->bvh); free(m->bidx);
+        free(m->nodes); free(m->tv); free(m->tn); free(m->tt); free(m->amin); free(m->amax); free(m->bvh); free(m->bidx);
     }
     free(s->meshes);
     free(s);
@@ -595,12 +628,14 @@ static int scene_hit(const xo_scene *s, v3 o, v3 d, hrec *res, int32_t *obj, int
         hrec h;
         int ok = 0;
         int32_t p = D->obj_first[oi];
+        const double usc[2] = {D->obj_uv_scale ? (double)D->obj_uv_scale[2 * oi] : 0.0,
+                               D->obj_uv_scale ? (double)D->obj_uv_scale[2 * oi + 1] : 0.0};
         if (D->obj_kind[oi] == XO_SPHERE) {
             const float *sp = D->spheres + 4 * (size_t)p;
-            ok = hit_sphere(V(sp[0], sp[1], sp[2]), (double)sp[3], o, d, &h);
+            ok = hit_sphere(V(sp[0], sp[1], sp[2]), (double)sp[3], usc, o, d, &h);
         } else if (D->obj_kind[oi] == XO_PLANE) {
             const float *pl = D->planes + 4 * (size_t)p;
-            ok = hit_plane(V(pl[0], pl[1], pl[2]), (double)pl[3], o, d, &h);
+            ok = hit_plane(V(pl[0], pl[1], pl[2]), (double)pl[3], usc, o, d, &h);
         } else {
             const mesh_t *m = &s->meshes[oi];
             int32_t it = (s->accel == XO_ACCEL_OCTREE) ? otrace(m, m->nnodes ? 0 : -1, o, d, &h)
@@ -800,6 +835,50 @@ int xo_render(const xo_scene *s, const xo_render_params *p, int64_t npix, const 
                 col[1] = clamp0((float)acc.y);
                 col[2] = clamp0((float)acc.z);
                 col[3] = 1.f;
+            } else if (p->integrator == XO_NORMAL) {    /* normal/integrator.cc:10-39 */
+                v3 acc = V(col[0], col[1], col[2]);
+                acc = V(acc.x * 2.0f - 1.0f, acc.y * 2.0f - 1.0f, acc.z * 2.0f - 1.0f);
+                ++nr;
+                if (scene_hit(s, O, Dd, &h, &oi, &pi)) {
+                    v3 nw = muls(add(h.normal, acc), 0.5f);
+                    v3 u = normalized(nw);
+                    acc = V((u.x + 1.0f) * 0.5f, (u.y + 1.0f) * 0.5f, (u.z + 1.0f) * 0.5f);
+                }
+                col[0] = clamp0((float)acc.x);
+                col[1] = clamp0((float)acc.y);
+                col[2] = clamp0((float)acc.z);
+                col[3] = 1.f;
+            } else if (p->integrator == XO_UV) {        /* uv/integrator.cc:10-42 */
+                v3 acc = V(col[0], col[1], col[2]);
+                double alpha = col[3], alpha_sample = 0.f;
+                ++nr;
+                if (scene_hit(s, O, Dd, &h, &oi, &pi)) {
+                    /* hit_record_t::texcoord is a Vector3f with z = 0 (hitrecord.h:33),
+                     * so the blue channel gains (0 * 0.5 + 0.5) * weight */
+                    acc = V(acc.x + (h.tu * 0.5f + 0.5f) * weight, acc.y + (h.tv * 0.5f + 0.5f) * weight,
+                            acc.z + (0.0 * 0.5f + 0.5f) * weight);
+                    alpha_sample += weight;
+                }
+                col[0] = clamp0((float)acc.x);
+                col[1] = clamp0((float)acc.y);
+                col[2] = clamp0((float)acc.z);
+                col[3] = clamp01((float)(alpha + weight * alpha_sample));
+            } else if (p->integrator == XO_EMISSION) {  /* emission/integrator.cc:10-38 */
+                ++nr;
+                if (scene_hit(s, O, Dd, &h, &oi, &pi)) {
+                    const xo_material *m = &D->materials[D->obj_material[oi]];
+                    c3 e = cmuls(C(m->emissive[0], m->emissive[1], m->emissive[2]), (float)weight);
+                    col[0] = clamp0(col[0] + e.r);
+                    col[1] = clamp0(col[1] + e.g);
+                    col[2] = clamp0(col[2] + e.b);
+                }
+                col[3] = 1.f;
+            } else if (p->integrator == XO_WIREFRAME) { /* wireframe/integrator.cc:10-35 */
+                ++nr;
+                if (scene_hit(s, O, Dd, &h, &oi, &pi)) {
+                    col[0] = col[1] = col[2] = 1.f;
+                    col[3] = clamp01((float)(col[3] + weight));
+                }
             } else {                                    /* pathtracer/integrator.cc:49-74 */
                 c3 v = pt_eval(s, (size_t)p->rdepth, C(1, 1, 1), O, Dd, &r, &nr);
                 c3 add_ = cmuls(v, (float)weight);
@@ -827,7 +906,8 @@ static void put_hit(int ok, const hrec *h, double out[7])
 int xo_kat_sphere(const double sph[4], const double o[3], const double d[3], double out[7])
 {
     hrec h;
-    int ok = hit_sphere(V(sph[0], sph[1], sph[2]), sph[3], V(o[0], o[1], o[2]), V(d[0], d[1], d[2]), &h);
+    const double usc[2] = {0.0, 0.0};
+    int ok = hit_sphere(V(sph[0], sph[1], sph[2]), sph[3], usc, V(o[0], o[1], o[2]), V(d[0], d[1], d[2]), &h);
     put_hit(ok, &h, out);
     return ok;
 }
@@ -835,7 +915,8 @@ int xo_kat_sphere(const double sph[4], const double o[3], const double d[3], dou
 int xo_kat_plane(const double pl[4], const double o[3], const double d[3], double out[7])
 {
     hrec h;
-    int ok = hit_plane(V(pl[0], pl[1], pl[2]), pl[3], V(o[0], o[1], o[2]), V(d[0], d[1], d[2]), &h);
+    const double usc[2] = {0.0, 0.0};
+    int ok = hit_plane(V(pl[0], pl[1], pl[2]), pl[3], usc, V(o[0], o[1], o[2]), V(d[0], d[1], d[2]), &h);
     put_hit(ok, &h, out);
     return ok;
 }
@@ -845,7 +926,8 @@ int xo_kat_triangle(const double v[9], const double n[9], const double o[3], con
     v3 tv[3] = {V(v[0], v[1], v[2]), V(v[3], v[4], v[5]), V(v[6], v[7], v[8])};
     v3 tn[3] = {V(n[0], n[1], n[2]), V(n[3], n[4], n[5]), V(n[6], n[7], n[8])};
     hrec h;
-    int ok = hit_triangle(tv, tn, V(o[0], o[1], o[2]), V(d[0], d[1], d[2]), &h);
+    const v3 tt[3] = {V(0, 0, 0), V(0, 0, 0), V(0, 0, 0)};
+    int ok = hit_triangle(tv, tn, tt, V(o[0], o[1], o[2]), V(d[0], d[1], d[2]), &h);
     put_hit(ok, &h, out);
     return ok;
 }

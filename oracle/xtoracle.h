@@ -23,7 +23,8 @@ extern "C" {
 enum { XO_SPHERE = 0, XO_PLANE = 1, XO_MESH = 2 };
 enum { XO_LAMBERT = 0, XO_PHONG = 1, XO_BLINNPHONG = 2, XO_EMISSIVE = 3, XO_DIELECTRIC = 4 };
 enum { XO_ENV_NONE = 0, XO_ENV_COLOR = 1, XO_ENV_GRADIENT = 2 };
-enum { XO_STENCIL = 0, XO_DEPTH = 1, XO_AO = 2, XO_PATHTRACER = 3 };
+enum { XO_STENCIL = 0, XO_DEPTH = 1, XO_AO = 2, XO_PATHTRACER = 3,
+       XO_NORMAL = 4, XO_UV = 5, XO_EMISSION = 6, XO_WIREFRAME = 7 };
 /* mesh intersector: 0 = octree restatement (exact reference order), 1 = FP64 BVH
  * with the reference's triangle test (same closest hit except exact t ties). */
 enum { XO_ACCEL_OCTREE = 0, XO_ACCEL_BVH = 1 };
@@ -56,6 +57,10 @@ typedef struct {
     float env_a[3], env_b[3];
     float cam_pos[3], cam_target[3], cam_up[3];
     float cam_fov;
+    const float *obj_uv_scale;   /* 2 floats per object (ISurface::uv_scale), or NULL = (0, 0),
+                                    what the loader sets without uscale/vscale */
+    const float *tri_uvs;        /* 6 floats per triangle (Triangle::tc[0..2].xy), or NULL = the
+                                    Triangle constructor's (0,0) (1,0) (0,0), triangle.cc:8-13 */
 } xo_scene_desc;
 
 typedef struct xo_scene xo_scene;
@@ -75,7 +80,7 @@ void xo_camera_ray(const float pos[3], const float target[3], const float up[3],
                    float x, float y, float w, float h, double org[3], double dir[3]);
 
 typedef struct {
-    int32_t integrator;    /* XO_STENCIL .. XO_PATHTRACER */
+    int32_t integrator;    /* XO_STENCIL .. XO_WIREFRAME */
     int32_t width, height, spp, rdepth;
     float ao_max_distance; /* 100 in the shipped AO integrator */
     uint64_t seed;         /* XO_RNG_STREAM key */

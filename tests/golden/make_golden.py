@@ -13,7 +13,11 @@ these fixtures are what pins the oracle restatement (oracle/xtoracle.c):
               Octree<Triangle> replica, t, point, normal) on small scenes;
 * render_*.npz stencil/depth frames (deterministic) and AO/pathtracer frames at
               several seeds (single thread, time() fixed by the driver) for the
-              statistical checks.
+              statistical checks;
+* render_primary_*.npz  frames of the normal, uv, emission and wireframe
+              integrators (deterministic, 3 samples per pixel) on scenes that
+              exercise every texture-coordinate path (`--primary` regenerates
+              only these).
 
 Run here (needs the reference sources and oracle/_ref/xtref):
     make -f oracle/ref.mk REF=<xtracer source tree> -j8
@@ -200,9 +204,31 @@ def small_scenes():
     return {"spheres64": (sp, 64, 64), "terrain20k": (te, 96, 54), "hairball20k": (hb, 64, 64)}
 
 
+def primary_scenes():
+    return {"spheres64": (scenes.spheres_scene(64, seed=1, name="spheres64"), 64, 64),
+            "terrain20k": (scenes.terrain_scene(20_000, seed=2, name="terrain20k"), 96, 54),
+            "uvscene": (scenes.uv_scene(6), 80, 60)}
+
+
+def make_primary(work):
+    for name, (spec, w, h) in primary_scenes().items():
+        scn = spec.write_scn(work)
+        rend = {}
+        for integ in ("normal", "uv", "emission", "wireframe"):
+            xy, rgba, st = po.ref_render(scn, integ, w, h, spp=3, threads=1, seed=1, workdir=work)
+            rend["%s_xy" % integ] = xy
+            rend["%s_rgba" % integ] = rgba
+            rend["%s_rays" % integ] = st["rays"]
+        np.savez_compressed(os.path.join(HERE, "render_primary_%s.npz" % name), width=w, height=h, spp=3, **rend)
+        print("render_primary", name, sorted(rend))
+
+
 def main():
     if not po.ref_available():
         raise SystemExit("oracle/_ref/xtref missing: make -f oracle/ref.mk REF=<xtracer sources>")
+    if "--primary" in sys.argv:
+        make_primary(tempfile.mkdtemp(prefix="xtgold"))
+        return
     rng = np.random.default_rng(20261203)
     kat = make_kat(rng)
     np.savez_compressed(os.path.join(HERE, "kat.npz"), **kat)

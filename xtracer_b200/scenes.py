@@ -70,6 +70,11 @@ class SceneSpec:
     tri_normals: Optional[np.ndarray] = None
     # mesh vertex/index form for writing OBJ (per mesh object): list of (verts, faces)
     mesh_obj: Optional[list] = None
+    # per object (u_scale, v_scale) of the geometry (ISurface::uv_scale; the
+    # loader's default is (0, 0)), and per triangle the texcoords of its three
+    # corners (Triangle::tc, OBJ "vt"); None = all zero
+    obj_uv_scale: Optional[np.ndarray] = None      # (O, 2) float32
+    tri_uvs: Optional[np.ndarray] = None           # (T, 3, 2) float32
 
     @property
     def n_tris(self) -> int:
@@ -103,19 +108,22 @@ class SceneSpec:
         for oi in range(len(self.obj_kind)):
             k, first = int(self.obj_kind[oi]), int(self.obj_first[oi])
             gname = "g%05d" % oi
+            uvs = []
+            if self.obj_uv_scale is not None and np.any(self.obj_uv_scale[oi] != 0):
+                uvs = ["    u_scale = %s" % f(self.obj_uv_scale[oi][0]), "    v_scale = %s" % f(self.obj_uv_scale[oi][1])]
             if k == SPHERE:
                 s = self.spheres[first]
                 out += ["  %s = {" % gname, "    type = sphere", "    position = %s" % v3(s[:3]),
-                        "    radius = %s" % f(s[3]), "  }"]
+                        "    radius = %s" % f(s[3])] + uvs + ["  }"]
             elif k == PLANE:
                 p = self.planes[first]
                 out += ["  %s = {" % gname, "    type = plane", "    normal = %s" % v3(p[:3]),
-                        "    distance = %s" % f(p[3]), "  }"]
+                        "    distance = %s" % f(p[3])] + uvs + ["  }"]
             else:
                 objname = "%s_m%02d.obj" % (self.name, mesh_i)
                 self._write_obj(os.path.join(directory, objname), mesh_i, first, int(self.obj_count[oi]))
                 mesh_i += 1
-                out += ["  %s = {" % gname, "    type = mesh", "    source = %s" % objname, "  }"]
+                out += ["  %s = {" % gname, "    type = mesh", "    source = %s" % objname] + uvs + ["  }"]
         out.append("}")
         out.append("material = {")
         for mi, m in enumerate(self.materials):
@@ -149,7 +157,14 @@ class SceneSpec:
             faces = np.arange(count * 3, dtype=np.int64).reshape(-1, 3)
         with open(path, "w") as fh:
             fh.write("".join("v %r %r %r\n" % (float(a), float(b), float(c)) for a, b, c in verts.tolist()))
-            fh.write("".join("f %d %d %d\n" % (a + 1, b + 1, c + 1) for a, b, c in faces.tolist()))
+            if self.tri_uvs is None:
+                fh.write("".join("f %d %d %d\n" % (a + 1, b + 1, c + 1) for a, b, c in faces.tolist()))
+            else:
+                # one texcoord per triangle corner, in face order
+                uv = self.tri_uvs[first:first + count].reshape(-1, 2)
+                fh.write("".join("vt %r %r\n" % (float(u), float(v)) for u, v in uv.tolist()))
+                fh.write("".join("f %d/%d %d/%d %d/%d\n" % (a + 1, 3 * i + 1, b + 1, 3 * i + 2, c + 1, 3 * i + 3)
+                                 for i, (a, b, c) in enumerate(faces.tolist())))
 
 
 # ----------------------------------------------------------------------
@@ -234,6 +249,38 @@ def terrain_mesh(grid: int = 708, seed: int = 2, half: float = 50.0, amplitude: 
     faces[0::2] = np.stack([a, c, b], axis=1)
     faces[1::2] = np.stack([b, c, d], axis=1)
     return verts, faces
+
+
+def uv_scene(seed: int = 6, name: str = "uvscene") -> SceneSpec:
+    """Texture-coordinate paths of every primitive kind: 24 spheres (half with
+    u/v scales), a ground plane with u/v scales, and a terrain patch whose
+    triangles carry OBJ texcoords; some materials emissive.  For the normal, uv
+    and emission integrators."""
+    rng = np.random.default_rng(seed)
+    base = spheres_scene(24, seed=seed, extent=5.0, name=name, with_light=False)
+    verts, faces = terrain_mesh(12, seed + 1, half=3.0, amplitude=0.5, octaves=2, offset=(0.0, 2.0))
+    verts = verts + np.array([0.0, 0.25, 2.0], np.float32)
+    tris = verts[faces].astype(np.float32)
+    uv = np.stack([(verts[:, 0] + 3.0) / 6.0, (verts[:, 2] - 2.0 + 3.0) / 6.0], axis=1)
+    tri_uvs = _q(uv[faces], 12).astype(np.float32)
+    n_obj = len(base.obj_kind)
+    scale = np.zeros((n_obj + 1, 2), np.float32)
+    scale[0] = (0.25, 0.5)                                # the plane
+    for oi in range(1, n_obj, 2):                         # every other sphere
+        scale[oi] = _q(rng.uniform(0.5, 2.0, 2), 8)
+    scale[n_obj] = (0.0, 0.0)                             # the mesh (triangles use tc only)
+    mats = list(base.materials)
+    for i in range(1, len(mats), 3):                      # every third sphere glows
+        e = _q(rng.uniform(0.2, 3.0, 3), 8)
+        mats[i] = Material(EMISSIVE, emissive=(float(e[0]), float(e[1]), float(e[2])))
+    mats.append(Material(LAMBERT, diffuse=(0.3, 0.6, 0.3), emissive=(0.5, 0.25, 0.125)))
+    kinds = np.concatenate([base.obj_kind, [MESH]]).astype(np.int32)
+    firsts = np.concatenate([base.obj_first, [0]]).astype(np.int32)
+    counts = np.concatenate([base.obj_count, [tris.shape[0]]]).astype(np.int32)
+    omat = np.concatenate([base.obj_material, [len(mats) - 1]]).astype(np.int32)
+    return SceneSpec(name, base.spheres, base.planes, tris, kinds, firsts, counts, omat, mats, base.camera,
+                     ENV_GRADIENT, base.env_a, base.env_b, mesh_obj=[(verts, faces)], obj_uv_scale=scale,
+                     tri_uvs=tri_uvs)
 
 
 def grid_for_tris(n_tris: int) -> int:
