@@ -62,7 +62,10 @@ enum { XTGPU_LAMBERT = 0, XTGPU_PHONG = 1, XTGPU_BLINNPHONG = 2, XTGPU_EMISSIVE 
 /* Environment samplers (sampler_col.cc, sampler_gradient.cc); none = black. */
 enum { XTGPU_ENV_NONE = 0, XTGPU_ENV_COLOR = 1, XTGPU_ENV_GRADIENT = 2 };
 /* Integrators. */
-enum { XTGPU_STENCIL = 0, XTGPU_DEPTH = 1, XTGPU_AO = 2, XTGPU_PATHTRACER = 3 };
+enum { XTGPU_STENCIL = 0, XTGPU_DEPTH = 1, XTGPU_AO = 2, XTGPU_PATHTRACER = 3,
+       /* primary-ray integrators (integrator/{normal,uv,emission,wireframe}) */
+       XTGPU_NORMAL = 4, XTGPU_UV = 5, XTGPU_EMISSION = 6, XTGPU_WIREFRAME = 7 };
+#define XTGPU_INTEGRATOR_LAST XTGPU_WIREFRAME
 /* BVH node formats: binary nodes with 64-byte FP32 child boxes or 32-byte
  * boxes quantised to 8 bits per bound with outward rounding; or 8-wide nodes
  * (80 bytes) with 8-bit quantised child boxes, collapsed from the binary tree
@@ -100,6 +103,10 @@ typedef struct {
     int32_t env_type;
     float env_a[3], env_b[3];
     xtgpu_camera camera;
+    const float *obj_uv_scale;     /* 2 floats per object: the surface's uv_scale (u_scale,
+                                      v_scale), or NULL = (0, 0), the loader's default */
+    const float *tri_uvs;          /* 6 floats per triangle: texcoords of its corners (OBJ vt),
+                                      or NULL = the Triangle constructor's (0,0) (1,0) (0,0) */
 } xtgpu_scene_desc;
 
 typedef struct xtgpu_scene xtgpu_scene;
@@ -163,7 +170,7 @@ XTGPU_API xtgpu_status xtgpu_trace_host(xtgpu_scene *scene, int64_t n, const flo
                               xtgpu_hit *hits, int32_t node_format, void *stream);
 
 typedef struct {
-    int32_t integrator;            /* XTGPU_STENCIL .. XTGPU_PATHTRACER */
+    int32_t integrator;            /* XTGPU_STENCIL .. XTGPU_WIREFRAME */
     int32_t width, height;         /* frame size (params_t, context.h:18-34) */
     int32_t spp;                   /* samples per pixel, weight 1/spp each (aa.cc:66-74) */
     int32_t rdepth;                /* pathtracer recursion depth */

@@ -364,3 +364,38 @@ def test_bad_arguments_return_invalid():
         sc.render(xtgpu.STENCIL, 8, 8, node_format=xtgpu.NODES_Q8)   # not built
     assert e.value.status == 7
     sc.close()
+
+
+def _primary_scene(name):
+    return {"spheres64": lambda: scenes.spheres_scene(64, seed=1, name="spheres64"),
+            "terrain20k": lambda: scenes.terrain_scene(20_000, seed=2, name="terrain20k"),
+            "uvscene": lambda: scenes.uv_scene(6)}[name]()
+
+
+@pytest.mark.parametrize("name", ["spheres64", "terrain20k", "uvscene"])
+@pytest.mark.parametrize("integ,code", [("normal", xtgpu.NORMAL), ("uv", xtgpu.UV), ("emission", xtgpu.EMISSION),
+                                        ("wireframe", xtgpu.WIREFRAME)])
+@pytest.mark.parametrize("fmt", [xtgpu.NODES_FP32, xtgpu.NODES_W8])
+def test_primary_integrators_vs_reference_golden(name, integ, code, fmt):
+    """normal, uv, emission and wireframe frames against the reference's own
+    renders (3 samples per pixel, so the per-sample folds are exercised).
+    Wireframe and emission fold the same floats as the reference; normal and
+    uv carry the FP32 hit point into their FP64 arithmetic (1e-4)."""
+    g = np.load(os.path.join(GOLD, "render_primary_%s.npz" % name))
+    spec = _primary_scene(name)
+    w, h, spp = int(g["width"]), int(g["height"]), int(g["spp"])
+    sc = xtgpu.Scene(spec, node_formats=(fmt,), leaf_size=1)
+    img, rays = sc.render(code, w, h, spp=spp, node_format=fmt)
+    sc.close()
+    assert rays == int(g["%s_rays" % integ]) == w * h * spp
+    xy = g["%s_xy" % integ]
+    got = img[xy[:, 1], xy[:, 0]]
+    ref = g["%s_rgba" % integ]
+    nan_g, nan_r = np.isnan(got).any(axis=1), np.isnan(ref).any(axis=1)
+    assert np.mean(nan_g == nan_r) >= 0.999
+    both = ~nan_g & ~nan_r
+    d = np.abs(got[both] - ref[both]).max(axis=1)
+    if integ in ("emission", "wireframe"):
+        assert np.mean(d == 0) >= 0.999, np.sort(d)[-5:]
+    else:
+        assert np.mean(d <= 1e-4) >= 0.995, np.sort(d)[-5:]

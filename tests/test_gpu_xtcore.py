@@ -15,7 +15,8 @@ from tests import xtcore_host as xh
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not xh.available(), reason="xtgpu-xtcore not built (needs the XTracer sources)")]
 
-NAMES = {xtgpu.STENCIL: "stencil", xtgpu.DEPTH: "depth", xtgpu.AO: "ao", xtgpu.PATHTRACER: "pathtracer"}
+NAMES = {xtgpu.STENCIL: "stencil", xtgpu.DEPTH: "depth", xtgpu.AO: "ao", xtgpu.PATHTRACER: "pathtracer",
+         xtgpu.NORMAL: "normal", xtgpu.UV: "uv", xtgpu.EMISSION: "emission", xtgpu.WIREFRAME: "wireframe"}
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -32,7 +33,7 @@ def cuda_device():
 def written(tmp_path_factory):
     d = tmp_path_factory.mktemp("scn")
     specs = [scenes.spheres_scene(64, seed=1, name="s64"), scenes.terrain_scene(5_000, seed=2, name="t5k"),
-             scenes.hairball_scene(3_000, seed=3, name="h3k")]
+             scenes.hairball_scene(3_000, seed=3, name="h3k"), scenes.uv_scene(6)]
     return [(s, s.write_scn(str(d))) for s in specs], d
 
 
@@ -45,10 +46,12 @@ def render_host(scn, kind, w, h, spp, rdepth, out, *extra):
 @pytest.mark.parametrize("kind, spp, rdepth, extra", [
     (xtgpu.STENCIL, 2, 1, ()), (xtgpu.DEPTH, 1, 1, ()), (xtgpu.AO, 4, 1, ()),
     (xtgpu.AO, 4, 1, ("--ao-distance", "0.25")), (xtgpu.PATHTRACER, 4, 4, ()),
-    (xtgpu.PATHTRACER, 3, 4, ("--q8", "--seed", "7", "--tile", "16"))])
+    (xtgpu.PATHTRACER, 3, 4, ("--q8", "--seed", "7", "--tile", "16")),
+    (xtgpu.PATHTRACER, 2, 4, ("--w8",)),
+    (xtgpu.NORMAL, 3, 1, ()), (xtgpu.UV, 3, 1, ()), (xtgpu.EMISSION, 3, 1, ()), (xtgpu.WIREFRAME, 2, 1, ())])
 def test_integrator_in_host_equals_c_abi(written, kind, spp, rdepth, extra):
     specs, d = written
-    fmt = xtgpu.NODES_Q8 if "--q8" in extra else xtgpu.NODES_FP32
+    fmt = xtgpu.NODES_Q8 if "--q8" in extra else (xtgpu.NODES_W8 if "--w8" in extra else xtgpu.NODES_FP32)
     seed = int(extra[extra.index("--seed") + 1]) if "--seed" in extra else 1
     aod = float(extra[extra.index("--ao-distance") + 1]) if "--ao-distance" in extra else 100.0
     for spec, scn in specs:
@@ -56,7 +59,8 @@ def test_integrator_in_host_equals_c_abi(written, kind, spp, rdepth, extra):
         sc = xtgpu.Scene(spec, node_formats=(fmt,))
         ref, _ = sc.render(kind, 80, 56, spp=spp, rdepth=rdepth, ao_max_distance=aod, seed=seed, node_format=fmt)
         sc.close()
-        assert np.array_equal(got, ref), "%s %s differs through the xtcore host" % (spec.name, NAMES[kind])
+        assert np.array_equal(got, ref, equal_nan=True), "%s %s differs through the xtcore host" % (spec.name,
+                                                                                                    NAMES[kind])
 
 
 @pytest.mark.parametrize("kind", [xtgpu.STENCIL, xtgpu.DEPTH])

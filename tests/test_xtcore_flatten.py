@@ -24,7 +24,8 @@ def flatten(spec, tmp_path):
 @pytest.mark.parametrize("make", [lambda: scenes.spheres_scene(64, seed=1, name="s64"),
                                   lambda: scenes.terrain_scene(5_000, seed=2, name="t5k"),
                                   lambda: scenes.hairball_scene(3_000, seed=3, name="h3k"),
-                                  lambda: scenes.precision_scene(scale=0.002, seed=5)])
+                                  lambda: scenes.precision_scene(scale=0.002, seed=5),
+                                  lambda: scenes.uv_scene(6)])
 def test_flattened_scene_equals_generator(make, tmp_path):
     spec = make()
     d = flatten(spec, tmp_path)
@@ -35,6 +36,12 @@ def test_flattened_scene_equals_generator(make, tmp_path):
     # mesh triangles come out of each Mesh's octree items, in OBJ face order
     assert np.array_equal(d["tris"], spec.tris)
     assert d["tri_normals"] is None
+    uvs = spec.obj_uv_scale if spec.obj_uv_scale is not None else np.zeros((len(spec.obj_kind), 2), np.float32)
+    assert np.array_equal(d["obj_uv_scale"], uvs)
+    if spec.tri_uvs is None:
+        assert d["tri_uvs"] is None          # the Triangle constructor's texcoords
+    else:
+        assert np.array_equal(d["tri_uvs"], spec.tri_uvs)
     assert d["env_type"] == spec.env_type
     assert np.array_equal(d["env_a"], np.float32(spec.env_a))
     if spec.env_type == scenes.ENV_GRADIENT:

@@ -29,7 +29,7 @@ def read_flat(path):
         off += a.nbytes
         return a
 
-    no, ns, npl, nt, nm, hn, env = (int(v) for v in take(np.int32, 7))
+    no, ns, npl, nt, nm, hn, env, hu = (int(v) for v in take(np.int32, 8))
     d = {"env_type": env}
     for key in ("obj_kind", "obj_first", "obj_count", "obj_material"):
         d[key] = take(np.int32, no)
@@ -37,6 +37,8 @@ def read_flat(path):
     d["planes"] = take(np.float32, 4 * npl).reshape(-1, 4)
     d["tris"] = take(np.float32, 9 * nt).reshape(-1, 3, 3)
     d["tri_normals"] = take(np.float32, 9 * nt).reshape(-1, 3, 3) if hn else None
+    d["obj_uv_scale"] = take(np.float32, 2 * no).reshape(-1, 2)
+    d["tri_uvs"] = take(np.float32, 6 * nt).reshape(-1, 3, 2) if hu else None
     d["materials"] = []
     for _ in range(nm):
         t = int(take(np.int32, 1)[0])

@@ -264,6 +264,16 @@ xtgpu_status xtgpu_scene_create(const xtgpu_scene_desc *d, void *stream, xtgpu_s
     }
     std::vector<int32_t> om((size_t)std::max(1, d->n_objects));
     for (int32_t i = 0; i < d->n_objects; ++i) om[i] = d->obj_material[i];
+    // texture-coordinate inputs of the uv integrator
+    std::vector<float2> ouv((size_t)std::max(1, d->n_objects), make_float2(0.f, 0.f));
+    if (d->obj_uv_scale)
+        for (int32_t i = 0; i < d->n_objects; ++i) ouv[i] = make_float2(d->obj_uv_scale[2 * i], d->obj_uv_scale[2 * i + 1]);
+    if ((st = dalloc(sc->obj_uvs, sizeof(float2) * ouv.size(), s)) != XTGPU_OK) return fail(st);
+    cudaMemcpy(sc->obj_uvs.p, ouv.data(), sizeof(float2) * ouv.size(), cudaMemcpyHostToDevice);
+    if (d->tri_uvs && d->n_tris) {
+        if ((st = dalloc(sc->tri_uv, sizeof(float2) * 3 * (size_t)d->n_tris, s)) != XTGPU_OK) return fail(st);
+        cudaMemcpy(sc->tri_uv.p, d->tri_uvs, sizeof(float2) * 3 * (size_t)d->n_tris, cudaMemcpyHostToDevice);
+    }
     if ((st = dalloc(sc->materials, sizeof(DevMaterial) * mats.size(), s)) != XTGPU_OK) return fail(st);
     if ((st = dalloc(sc->obj_material, sizeof(int32_t) * om.size(), s)) != XTGPU_OK) return fail(st);
     cudaMemcpy(sc->spheres.p, sp.data(), sizeof(float4) * sp.size(), cudaMemcpyHostToDevice);
@@ -281,6 +291,8 @@ xtgpu_status xtgpu_scene_create(const xtgpu_scene_desc *d, void *stream, xtgpu_s
     S.prim_obj = (const int32_t *)sc->prim_obj.p;
     S.obj_material = (const int32_t *)sc->obj_material.p;
     S.materials = (const DevMaterial *)sc->materials.p;
+    S.obj_uvs = (const float2 *)sc->obj_uvs.p;
+    S.tri_uv = (const float2 *)sc->tri_uv.p;
     S.n_tris = d->n_tris;
     S.n_spheres = d->n_spheres;
     S.n_planes = d->n_planes;
@@ -318,7 +330,7 @@ xtgpu_status xtgpu_scene_destroy(xtgpu_scene *sc)
 {
     if (!sc) return XTGPU_OK;
     for (HostBuf *b : {&sc->tri_v, &sc->tri_n, &sc->spheres, &sc->planes, &sc->prim_obj, &sc->obj_material,
-                       &sc->materials, &sc->leaf_prims, &sc->nodes32, &sc->nodes8, &sc->nodesW, &sc->leafW,
+                       &sc->obj_uvs, &sc->tri_uv, &sc->materials, &sc->leaf_prims, &sc->nodes32, &sc->nodes8, &sc->nodesW, &sc->leafW,
                        &sc->morton, &sc->order, &sc->left, &sc->right})
         dfree(*b);
     delete sc;
@@ -333,7 +345,7 @@ xtgpu_status xtgpu_scene_device_bytes(const xtgpu_scene *sc, uint64_t *bytes)
     }
     uint64_t b = 0;
     for (const HostBuf *h : {&sc->tri_v, &sc->tri_n, &sc->spheres, &sc->planes, &sc->prim_obj, &sc->obj_material,
-                             &sc->materials, &sc->leaf_prims, &sc->nodes32, &sc->nodes8, &sc->nodesW, &sc->leafW,
+                             &sc->obj_uvs, &sc->tri_uv, &sc->materials, &sc->leaf_prims, &sc->nodes32, &sc->nodes8, &sc->nodesW, &sc->leafW,
                              &sc->morton, &sc->order, &sc->left, &sc->right})
         b += h->bytes;
     *bytes = b;
@@ -495,7 +507,7 @@ xtgpu_status xtg::render_impl(xtgpu_scene *sc, const xtgpu_render_params *p, flo
         set_error("xtgpu_render: NULL argument");
         return XTGPU_ERR_INVALID;
     }
-    if (p->integrator < XTGPU_STENCIL || p->integrator > XTGPU_PATHTRACER || p->width <= 0 || p->height <= 0 ||
+    if (p->integrator < XTGPU_STENCIL || p->integrator > XTGPU_INTEGRATOR_LAST || p->width <= 0 || p->height <= 0 ||
         p->spp <= 0 || p->rdepth < 0 || (p->integrator == XTGPU_AO && !(p->ao_max_distance > 0.f))) {
         set_error("xtgpu_render: bad parameters");
         return XTGPU_ERR_INVALID;

@@ -89,7 +89,7 @@ extern "C" xtgpu_status xtgpu_render_tile_noalloc(xtgpu_scene *sc, const xtgpu_r
         set_error("xtgpu_render_tile_noalloc: NULL argument");
         return XTGPU_ERR_INVALID;
     }
-    if (p->integrator < XTGPU_STENCIL || p->integrator > XTGPU_PATHTRACER || p->width <= 0 || p->height <= 0 ||
+    if (p->integrator < XTGPU_STENCIL || p->integrator > XTGPU_INTEGRATOR_LAST || p->width <= 0 || p->height <= 0 ||
         p->spp <= 0 || p->rdepth < 0 || (p->integrator == XTGPU_AO && !(p->ao_max_distance > 0.f))) {
         set_error("xtgpu_render_tile_noalloc: bad parameters");
         return XTGPU_ERR_INVALID;

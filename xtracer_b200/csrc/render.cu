@@ -182,6 +182,52 @@ __device__ __forceinline__ float3 hit_normal(const DevScene &S, uint32_t prim, f
     return f3(S.planes[prim - S.n_tris - S.n_spheres]);
 }
 
+// hit_record_t::texcoord as the reference forms it: triangles interpolate
+// their corner texcoords (the Triangle constructor's (0,0) (1,0) (0,0) when the
+// scene gives none, math/triangle.cc:8-13), spheres asin of the normal over the
+// u/v scale (math/sphere.cc:52-53), planes a planar map wrapped into [0,1]
+// (math/plane.cc:47-58).  Spheres and planes in FP64 like the reference.
+__device__ float2 hit_texcoord(const DevScene &S, uint32_t prim, float3 o, float3 d, float t, float bu, float bv)
+{
+    if ((int)prim < S.n_tris) {
+        float2 a = make_float2(0.f, 0.f), b = make_float2(1.f, 0.f), c = make_float2(0.f, 0.f);
+        if (S.tri_uv) {
+            a = S.tri_uv[3 * prim];
+            b = S.tri_uv[3 * prim + 1];
+            c = S.tri_uv[3 * prim + 2];
+        }
+        const double bw = 1.0 - (double)bu - (double)bv;
+        return make_float2((float)(a.x * bw + b.x * (double)bu + c.x * (double)bv),
+                           (float)(a.y * bw + b.y * (double)bu + c.y * (double)bv));
+    }
+    const float2 sc = S.obj_uvs[S.prim_obj[prim]];
+    const double px = (double)o.x + (double)d.x * t, py = (double)o.y + (double)d.y * t,
+                 pz = (double)o.z + (double)d.z * t;
+    if ((int)prim < S.n_tris + S.n_spheres) {
+        const float4 s4 = S.spheres[prim - S.n_tris];
+        const double nx = (px - s4.x) / s4.w, ny = (py - s4.y) / s4.w;
+        const double PI = 3.14159265358979323846;
+        return make_float2((float)(asin(nx / (sc.x != 0.f ? (double)sc.x : 1.0)) / PI + 0.5),
+                           (float)(asin(ny / (sc.y != 0.f ? (double)sc.y : 1.0)) / PI + 0.5));
+    }
+    const float4 pl = S.planes[prim - S.n_tris - S.n_spheres];
+    const double l = sqrt((double)pl.x * pl.x + (double)pl.y * pl.y + (double)pl.z * pl.z);
+    const double nx = pl.x / l, ny = pl.y / l, nz = pl.z / l;
+    const double ux = ny, uy = nz, uz = -nx;                                    // uvec
+    const double vx = uy * nz - uz * ny, vy = uz * nx - ux * nz, vz = ux * ny - uy * nx;   // cross(uvec, n)
+    const double qx = fabs((double)pl.x) * pl.w + px, qy = fabs((double)pl.y) * pl.w + py,
+                 qz = fabs((double)pl.z) * pl.w + pz;
+    double tu = (ux * qx + uy * qy + uz * qz) * (double)sc.x;
+    double tv = (vx * qx + vy * qy + vz * qz) * (double)sc.y;
+    if (tu > 1.f) tu -= (float)(int)tu;
+    if (tv > 1.f) tv -= (float)(int)tv;
+    if (tu < -1.f) tu -= (float)(int)tu;
+    if (tv < -1.f) tv -= (float)(int)tv;
+    if (tu < 0.f) tu = 1.f + tu;
+    if (tv < 0.f) tv = 1.f + tv;
+    return make_float2((float)tu, (float)tv);
+}
+
 // Pixel of the k-th pixel slot of a job.  With tiles, slots run through
 // square tiles of `tile` pixels (row-major tiles, row-major inside a tile; the
 // last band and column may be partial), which keeps the rays of a warp close
@@ -677,8 +723,27 @@ __global__ void k_shade(const DevJob *__restrict__ jobs, const DevScene *__restr
                                                 (uint64_t)fy * (uint64_t)J.width + (uint64_t)fx);
             switch (J.integrator) {
             case XTGPU_STENCIL:
+            case XTGPU_WIREFRAME:   // the same hit test and fold (wireframe/integrator.cc:20-32)
                 q.contrib[lp] = make_float4(0.f, 0.f, 0.f, hit ? 1.f : 0.f);
                 break;
+            case XTGPU_NORMAL: {    // the hit record's normal (normal/integrator.cc:27-30)
+                float3 n = make_float3(0.f, 0.f, 0.f);
+                if (hit) n = hit_normal(S, h.prim, o + d * h.t, h.u, h.v);
+                q.contrib[lp] = make_float4(n.x, n.y, n.z, hit ? 1.f : 0.f);
+                break;
+            }
+            case XTGPU_UV: {        // the hit record's texcoord (uv/integrator.cc:28-31)
+                float2 tc = make_float2(0.f, 0.f);
+                if (hit) tc = hit_texcoord(S, h.prim, o, d, h.t, h.u, h.v);
+                q.contrib[lp] = make_float4(tc.x, tc.y, 0.f, hit ? 1.f : 0.f);
+                break;
+            }
+            case XTGPU_EMISSION: {  // the hit material's emissive colour (emission/integrator.cc:27-33)
+                float3 e = make_float3(0.f, 0.f, 0.f);
+                if (hit) e = S.materials[S.obj_material[S.prim_obj[h.prim]]].emissive;
+                q.contrib[lp] = make_float4(e.x, e.y, e.z, hit ? 1.f : 0.f);
+                break;
+            }
             case XTGPU_DEPTH: {
                 // 1 / log(|o - p|), computed in double as the reference does
                 float dv = hit ? (float)(1.0 / log((double)h.t)) : 0.f;
@@ -802,7 +867,35 @@ __global__ void k_accumulate(const DevJob *__restrict__ jobs, const int32_t *__r
         for (int64_t s = s_lo; s <= s_hi; ++s) {
             float4 v = contrib[J.offset + (s * npix + pix - a)];
             switch (J.integrator) {
+            case XTGPU_NORMAL: {    // normal/integrator.cc:22-36, in scalar_t (FP64)
+                double ax = (double)c.x * 2.0f - 1.0f, ay = (double)c.y * 2.0f - 1.0f, az = (double)c.z * 2.0f - 1.0f;
+                if (v.w != 0.f) {
+                    const double nx = ((double)v.x + ax) * 0.5f, ny = ((double)v.y + ay) * 0.5f,
+                                 nz = ((double)v.z + az) * 0.5f;
+                    const double l = sqrt(nx * nx + ny * ny + nz * nz);
+                    ax = (nx / l + 1.0f) * 0.5f;
+                    ay = (ny / l + 1.0f) * 0.5f;
+                    az = (nz / l + 1.0f) * 0.5f;
+                }
+                c = make_float4(c0((float)ax), c0((float)ay), c0((float)az), 1.f);
+                break;
+            }
+            case XTGPU_UV: {        // uv/integrator.cc:22-36; texcoord.z = 0 adds 0.5 to blue
+                double ax = c.x, ay = c.y, az = c.z;
+                const double alpha = c.w;
+                double as = 0.f;
+                if (v.w != 0.f) {
+                    ax += ((double)v.x * 0.5f + 0.5f) * w;
+                    ay += ((double)v.y * 0.5f + 0.5f) * w;
+                    az += (0.0 * 0.5f + 0.5f) * w;
+                    as += w;
+                }
+                const float al = (float)(alpha + w * as);
+                c = make_float4(c0((float)ax), c0((float)ay), c0((float)az), al < 0.f ? 0.f : (al > 1.f ? 1.f : al));
+                break;
+            }
             case XTGPU_STENCIL:
+            case XTGPU_WIREFRAME:
                 if (v.w != 0.f) {
                     float al = (float)((double)c.w + w);
                     c = make_float4(1.f, 1.f, 1.f, al < 0.f ? 0.f : (al > 1.f ? 1.f : al));
@@ -1175,6 +1268,7 @@ int stack_for_scene(const xtgpu_scene *sc, int f, int requested)
 
 int bounces_of(int integrator, int rdepth)
 {
+    // stencil, depth, normal, uv, emission, wireframe: the camera rays only
     if (integrator == XTGPU_AO) return 2;
     if (integrator == XTGPU_PATHTRACER) return std::max(0, rdepth);
     return 1;

@@ -396,7 +396,7 @@ xtgpu_status xtgpu_service_submit(xtgpu_service *v, const xtgpu_job_desc *d, dou
         return XTGPU_ERR_INVALID;
     }
     if (d->scene < 0 || d->scene >= (int32_t)v->scenes.size() || d->integrator < XTGPU_STENCIL ||
-        d->integrator > XTGPU_PATHTRACER || d->width <= 0 || d->height <= 0 || d->spp <= 0 || d->rdepth < 0 ||
+        d->integrator > XTGPU_INTEGRATOR_LAST || d->width <= 0 || d->height <= 0 || d->spp <= 0 || d->rdepth < 0 ||
         (d->integrator == XTGPU_AO && !(d->ao_max_distance > 0.f))) {
         set_error("xtgpu_service_submit: bad job");
         return XTGPU_ERR_INVALID;

@@ -59,6 +59,8 @@ struct DevScene {
     const int32_t *prim_obj;   // object of each primitive id (tris, spheres, planes)
     const int32_t *obj_material;
     const DevMaterial *materials;
+    const float2 *obj_uvs;     // per object: the surface's (u_scale, v_scale)
+    const float2 *tri_uv;      // 3 per triangle, or nullptr (constructor defaults)
     int32_t n_tris, n_spheres, n_planes;
     // BVH
     const float4 *leaf_prims;  // 3 per primitive, Morton order
@@ -84,7 +86,7 @@ struct HostBuf {
 
 struct xtgpu_scene {
     xtg::DevScene dev{};
-    xtg::HostBuf tri_v, tri_n, spheres, planes, prim_obj, obj_material, materials;
+    xtg::HostBuf tri_v, tri_n, spheres, planes, prim_obj, obj_material, materials, obj_uvs, tri_uv;
     xtg::HostBuf leaf_prims, nodes32, nodes8, nodesW, leafW;
     xtg::HostBuf morton, order, left, right;   // kept for xtgpu_bvh_export
     int64_t n_prims = 0;

@@ -49,6 +49,21 @@ const TriItems &mesh_triangles(const xtcore::surface::Mesh *m)
     return oct.*member_of(OctreeItemsTag());
 }
 
+// texcoords of a triangle's corners; true if they differ from the Triangle
+// constructor's (0,0) (1,0) (0,0) (math/triangle.cc:8-13)
+bool put_uvs(std::vector<float> &v, const xtcore::surface::Triangle &t)
+{
+    static const float dflt[6] = {0.f, 0.f, 1.f, 0.f, 0.f, 0.f};
+    bool differs = false;
+    for (int k = 0; k < 3; ++k) {
+        const float u = (float)t.tc[k].x, w = (float)t.tc[k].y;
+        v.push_back(u);
+        v.push_back(w);
+        differs |= u != dflt[2 * k] || w != dflt[2 * k + 1];
+    }
+    return differs;
+}
+
 void put3(std::vector<float> &v, const nmath::Vector3f &p)
 {
     v.push_back((float)p.x);
@@ -143,6 +158,7 @@ xtgpu_status flatten(xtcore::Scene &scene, HASH_UINT64 camera, FlatScene &F, std
                 put3(F.tri_normals, t->n[k]);
                 F.has_normals |= t->n[k].x != 0 || t->n[k].y != 0 || t->n[k].z != 0;
             }
+            F.has_uvs |= put_uvs(F.tri_uvs, *t);
         } else if (const xtcore::surface::Mesh *m = dynamic_cast<const xtcore::surface::Mesh *>(g)) {
             kind = XTGPU_MESH;
             first = (int32_t)(F.tris.size() / 9);
@@ -155,6 +171,7 @@ xtgpu_status flatten(xtcore::Scene &scene, HASH_UINT64 camera, FlatScene &F, std
                     put3(F.tri_normals, t.n[k]);
                     F.has_normals |= t.n[k].x != 0 || t.n[k].y != 0 || t.n[k].z != 0;
                 }
+                F.has_uvs |= put_uvs(F.tri_uvs, t);
             }
             if (count == 0) continue;   // an empty mesh is never hit
         } else {
@@ -175,6 +192,8 @@ xtgpu_status flatten(xtcore::Scene &scene, HASH_UINT64 camera, FlatScene &F, std
             F.materials.push_back(gm);
             mat_index[obj->material] = mi;
         }
+        F.obj_uv_scale.push_back((float)g->uv_scale.x);
+        F.obj_uv_scale.push_back((float)g->uv_scale.y);
         F.obj_kind.push_back(kind);
         F.obj_first.push_back(first);
         F.obj_count.push_back(count);
@@ -197,6 +216,8 @@ xtgpu_status flatten(xtcore::Scene &scene, HASH_UINT64 camera, FlatScene &F, std
     d.n_tris = (int32_t)(F.tris.size() / 9);
     d.tris = F.tris.data();
     d.tri_normals = F.has_normals ? F.tri_normals.data() : 0;
+    d.obj_uv_scale = F.obj_uv_scale.data();
+    d.tri_uvs = F.has_uvs ? F.tri_uvs.data() : 0;
     d.n_materials = (int32_t)F.materials.size();
     d.materials = F.materials.data();
 

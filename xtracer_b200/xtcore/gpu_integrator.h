@@ -41,8 +41,10 @@ struct FlatScene {
     std::vector<int32_t> obj_kind, obj_first, obj_count, obj_material;
     std::vector<HASH_UINT64> obj_id;          // Scene::m_objects key of each object
     std::vector<float> spheres, planes, tris, tri_normals;
+    std::vector<float> obj_uv_scale, tri_uvs;   // 2 per object, 6 per triangle
     std::vector<xtgpu_material> materials;
     bool has_normals = false;
+    bool has_uvs = false;     // a triangle's texcoords differ from the constructor's
     xtgpu_scene_desc desc;
 };
 
@@ -53,8 +55,9 @@ xtgpu_status flatten(xtcore::Scene &scene, HASH_UINT64 camera, FlatScene &out, s
 class Integrator : public xtcore::render::IIntegrator
 {
     public:
-    // kind: XTGPU_STENCIL, XTGPU_DEPTH, XTGPU_AO or XTGPU_PATHTRACER;
-    // node_format: XTGPU_NODES_FP32 or XTGPU_NODES_Q8
+    // kind: XTGPU_STENCIL .. XTGPU_WIREFRAME (stencil, depth, ao, pathtracer,
+    // normal, uv, emission, wireframe);
+    // node_format: XTGPU_NODES_FP32, XTGPU_NODES_Q8 or XTGPU_NODES_W8
     explicit Integrator(int kind, int node_format = XTGPU_NODES_FP32);
     ~Integrator();
 

@@ -4,9 +4,10 @@
 // comparison, as the GUI does it (src/frontend/gui/workspace.cc:55-81).
 //
 //   xtgpu-xtcore render <scn> <integrator> W H spp rdepth <out.bin> [options]
-//       integrator: stencil | depth | ao | pathtracer
+//       integrator: stencil | depth | ao | pathtracer | normal | uv | emission | wireframe
 //       --cpu          the reference's CPU integrator instead of the GPU one
-//       --q8           8-bit quantised BVH nodes (GPU)
+//       --q8           binary BVH with 8-bit quantised nodes (GPU)
+//       --w8           8-wide BVH with 8-bit quantised nodes (GPU)
 //       --seed N       sample stream key (GPU), default 1
 //       --ao-distance D  AO occlusion distance (GPU), default 100
 //       --threads N    OpenMP threads of the tile loop, default all
@@ -28,6 +29,7 @@
 #include <xtcore/log.h>
 #include <xtcore/context.h>
 #include <xtcore/integrator.h>
+#include <xtcore/integrator/wireframe/integrator.h>
 #include <xtcore/parseutil.h>
 
 #include "gpu_integrator.h"
@@ -57,8 +59,9 @@ void put(FILE *f, const T *p, size_t n)
 }
 
 // int32 n_objects, n_spheres, n_planes, n_tris, n_materials, has_normals,
-// env_type; int32 obj_kind/first/count/material [n_objects each]; float32
-// spheres [4n], planes [4n], tris [9n], tri_normals [9n] when has_normals;
+// env_type, has_uvs; int32 obj_kind/first/count/material [n_objects each];
+// float32 spheres [4n], planes [4n], tris [9n], tri_normals [9n] when
+// has_normals, obj_uv_scale [2 n_objects], tri_uvs [6n] when has_uvs;
 // per material int32 type + float32 diffuse[3] specular[3] emissive[3]
 // reflectance exponent ior; float32 env_a[3] env_b[3]; float32 camera
 // position[3] target[3] up[3] fov.
@@ -67,9 +70,9 @@ int write_flat(const xtcore::integrator::gpu::FlatScene &F, const char *out)
     const xtgpu_scene_desc &d = F.desc;
     FILE *f = fopen(out, "wb");
     if (!f) return 1;
-    int32_t head[7] = {d.n_objects, d.n_spheres, d.n_planes, d.n_tris, d.n_materials, d.tri_normals ? 1 : 0,
-                       d.env_type};
-    put(f, head, 7);
+    int32_t head[8] = {d.n_objects, d.n_spheres, d.n_planes, d.n_tris, d.n_materials, d.tri_normals ? 1 : 0,
+                       d.env_type, d.tri_uvs ? 1 : 0};
+    put(f, head, 8);
     put(f, d.obj_kind, (size_t)d.n_objects);
     put(f, d.obj_first, (size_t)d.n_objects);
     put(f, d.obj_count, (size_t)d.n_objects);
@@ -78,6 +81,8 @@ int write_flat(const xtcore::integrator::gpu::FlatScene &F, const char *out)
     put(f, d.planes, 4 * (size_t)d.n_planes);
     put(f, d.tris, 9 * (size_t)d.n_tris);
     if (d.tri_normals) put(f, d.tri_normals, 9 * (size_t)d.n_tris);
+    put(f, d.obj_uv_scale, 2 * (size_t)d.n_objects);
+    if (d.tri_uvs) put(f, d.tri_uvs, 6 * (size_t)d.n_tris);
     for (int32_t i = 0; i < d.n_materials; ++i) {
         const xtgpu_material &m = d.materials[i];
         put(f, &m.type, 1);
@@ -120,7 +125,7 @@ int mode_render(int argc, char **argv)
     size_t w = strtoul(argv[4], 0, 10), h = strtoul(argv[5], 0, 10);
     size_t spp = strtoul(argv[6], 0, 10), rdepth = strtoul(argv[7], 0, 10);
     const char *out = argv[8];
-    bool cpu = false, q8 = false;
+    bool cpu = false, q8 = false, w8 = false;
     unsigned long long seed = 1;
     float aod = 100.f;
     size_t threads = 0, tile = 32;
@@ -128,6 +133,7 @@ int mode_render(int argc, char **argv)
         std::string a = argv[i];
         if (a == "--cpu") cpu = true;
         else if (a == "--q8") q8 = true;
+        else if (a == "--w8") w8 = true;
         else if (a == "--seed" && i + 1 < argc) seed = strtoull(argv[++i], 0, 10);
         else if (a == "--ao-distance" && i + 1 < argc) aod = (float)atof(argv[++i]);
         else if (a == "--threads" && i + 1 < argc) threads = strtoul(argv[++i], 0, 10);
@@ -153,7 +159,8 @@ int mode_render(int argc, char **argv)
     xtcore::render::IIntegrator *ig = 0;
     xtcore::integrator::gpu::Integrator *gi = 0;
     int kind = integ == "stencil" ? XTGPU_STENCIL : integ == "depth" ? XTGPU_DEPTH : integ == "ao" ? XTGPU_AO
-             : integ == "pathtracer" ? XTGPU_PATHTRACER : -1;
+             : integ == "pathtracer" ? XTGPU_PATHTRACER : integ == "normal" ? XTGPU_NORMAL : integ == "uv" ? XTGPU_UV
+             : integ == "emission" ? XTGPU_EMISSION : integ == "wireframe" ? XTGPU_WIREFRAME : -1;
     if (kind < 0) {
         fprintf(stderr, "xtgpu-xtcore: unknown integrator %s\n", integ.c_str());
         return 2;
@@ -162,9 +169,13 @@ int mode_render(int argc, char **argv)
         if (kind == XTGPU_STENCIL) ig = new xtcore::integrator::stencil::Integrator();
         else if (kind == XTGPU_DEPTH) ig = new xtcore::integrator::depth::Integrator();
         else if (kind == XTGPU_AO) ig = new xtcore::integrator::ao::Integrator();
+        else if (kind == XTGPU_NORMAL) ig = new xtcore::integrator::normal::Integrator();
+        else if (kind == XTGPU_UV) ig = new xtcore::integrator::uv::Integrator();
+        else if (kind == XTGPU_EMISSION) ig = new xtcore::integrator::emission::Integrator();
+        else if (kind == XTGPU_WIREFRAME) ig = new xtcore::integrator::wireframe::Integrator();
         else ig = new xtcore::integrator::pathtracer::Integrator();
     } else {
-        gi = new xtcore::integrator::gpu::Integrator(kind, q8 ? XTGPU_NODES_Q8 : XTGPU_NODES_FP32);
+        gi = new xtcore::integrator::gpu::Integrator(kind, w8 ? XTGPU_NODES_W8 : q8 ? XTGPU_NODES_Q8 : XTGPU_NODES_FP32);
         gi->seed = seed;
         gi->ao_max_distance = aod;
         ig = gi;

@@ -24,7 +24,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libxtgpu.so")
 
-STENCIL, DEPTH, AO, PATHTRACER = 0, 1, 2, 3
+STENCIL, DEPTH, AO, PATHTRACER, NORMAL, UV, EMISSION, WIREFRAME = 0, 1, 2, 3, 4, 5, 6, 7
 NODES_FP32, NODES_Q8, NODES_W8 = 0, 1, 2
 # bytes one node visit reads, per format
 NODE_BYTES = {NODES_FP32: 64, NODES_Q8: 32, NODES_W8: 80}
@@ -55,7 +55,7 @@ class SceneDesc(C.Structure):
                 ("n_tris", C.c_int32), ("tris", C.c_void_p), ("tri_normals", C.c_void_p),
                 ("n_materials", C.c_int32), ("materials", C.c_void_p),
                 ("env_type", C.c_int32), ("env_a", C.c_float * 3), ("env_b", C.c_float * 3),
-                ("camera", CameraDesc)]
+                ("camera", CameraDesc), ("obj_uv_scale", C.c_void_p), ("tri_uvs", C.c_void_p)]
 
 
 class BvhOpts(C.Structure):
@@ -240,6 +240,10 @@ class Scene:
         d.camera.target[:] = list(cam.target)
         d.camera.up[:] = list(cam.up)
         d.camera.fov = cam.fov
+        if getattr(spec, "obj_uv_scale", None) is not None:
+            d.obj_uv_scale = arr(spec.obj_uv_scale.reshape(-1), np.float32)
+        if getattr(spec, "tri_uvs", None) is not None:
+            d.tri_uvs = arr(spec.tri_uvs.reshape(-1), np.float32)
         h = C.c_void_p()
         check(lib().xtgpu_scene_create(C.byref(d), stream_handle(stream), C.byref(h)))
         self.handle = h
@@ -373,3 +377,19 @@ class AOIntegrator(_Integrator):
 
 class PathtracerIntegrator(_Integrator):
     kind = PATHTRACER
+
+
+class NormalIntegrator(_Integrator):
+    kind = NORMAL
+
+
+class UVIntegrator(_Integrator):
+    kind = UV
+
+
+class EmissionIntegrator(_Integrator):
+    kind = EMISSION
+
+
+class WireframeIntegrator(_Integrator):
+    kind = WIREFRAME
