@@ -207,6 +207,21 @@ XTGPU_API xtgpu_status xtgpu_render_tile_noalloc(xtgpu_scene *scene, const xtgpu
                                                  float *rgba_dev, uint64_t *rays_traced, void *stream);
 
 /* ---------------------------------------------------------------------- */
+/* Output side (lib/nimg/img.cc:72-179, the save::png and save::exr writers
+ * fed by context.cc:38-52 assemble).  The frame is width*height RGBA floats,
+ * row-major, as xtgpu_render writes it. */
+/* 8-bit RGBA of a device frame, on the device: channel * 255, clamped at 255,
+ * truncated (the PNG writer's arithmetic; NaN gives 0). */
+XTGPU_API xtgpu_status xtgpu_frame_rgba8(const float *rgba_dev, int64_t n_pixels, uint8_t *rgba8_dev, void *stream);
+/* PNG file (8-bit RGBA) from host 8-bit pixels. */
+XTGPU_API xtgpu_status xtgpu_write_png(const char *path, int32_t width, int32_t height, const uint8_t *rgba8_host);
+/* OpenEXR file (uncompressed scanlines, float B, G, R) from a host frame. */
+XTGPU_API xtgpu_status xtgpu_write_exr(const char *path, int32_t width, int32_t height, const float *rgba_host);
+/* PNG of a host frame: uploaded, quantised by xtgpu_frame_rgba8, written. */
+XTGPU_API xtgpu_status xtgpu_save_png_host(const char *path, int32_t width, int32_t height, const float *rgba_host,
+                                           void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* Render service.  Scenes stay resident; jobs are admitted while their
  * accumulation buffers fit the memory budget and a job slot is free; the rays of
  * all admitted jobs are merged into shared wavefront launches (camera, extend,

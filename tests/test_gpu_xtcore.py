@@ -76,3 +76,30 @@ def test_integrator_in_host_matches_reference_cpu_integrator(written, kind):
             bad |= gpu[..., 3] != cpu[..., 3]
         # a mismatch is a hit/miss or primitive disagreement on a grazing ray
         assert bad.sum() <= 2, "%s %s: %d pixels differ" % (spec.name, NAMES[kind], bad.sum())
+
+
+@pytest.mark.parametrize("kind, spp, rdepth, scene", [(xtgpu.PATHTRACER, 4, 4, 0), (xtgpu.UV, 3, 1, 3),
+                                                       (xtgpu.DEPTH, 1, 1, 1), (xtgpu.STENCIL, 3, 1, 2)])
+def test_png_exr_output_match_reference_writers(written, kind, spp, rdepth, scene):
+    """The frame written through the GPU quantiser and this library's PNG and
+    EXR writers decodes to exactly what XTracer's own writers (nimg::io::save,
+    lib/nimg/img.cc:72-179) produce from the same assembled frame: PNG pixels
+    bit for bit (values above 1 clamped, NaN channels 0), EXR floats bit for bit."""
+    from PIL import Image
+    specs, d = written
+    spec, scn = specs[scene]
+    p = {k: str(d / ("%s_%d.%s" % (k.split(".")[0], kind, k.split(".")[1])))
+         for k in ("own.png", "ref.png", "own.exr", "ref.exr")}
+    r = xh.run("render", scn, NAMES[kind], 72, 40, spp, rdepth, d / "o.bin", "--png", p["own.png"],
+               "--ref-png", p["ref.png"], "--exr", p["own.exr"], "--ref-exr", p["ref.exr"])
+    assert r.returncode == 0, r.stdout + r.stderr
+    a = np.asarray(Image.open(p["own.png"]).convert("RGBA"))
+    b = np.asarray(Image.open(p["ref.png"]).convert("RGBA"))
+    assert a.shape == b.shape == (40, 72, 4)
+    assert np.array_equal(a, b)
+    ea, eb = xh.read_exr(p["own.exr"]), xh.read_exr(p["ref.exr"])
+    assert sorted(ea) == sorted(eb) == ["B", "G", "R"]
+    for c in "BGR":
+        assert np.array_equal(ea[c], eb[c], equal_nan=True)
+    frame = xh.read_frame(d / "o.bin")
+    assert np.array_equal(ea["R"], frame[..., 0], equal_nan=True)

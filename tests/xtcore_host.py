@@ -59,3 +59,32 @@ def read_frame(path):
 def material_row(m):
     return np.array(list(m.diffuse) + list(m.specular) + list(m.emissive) + [m.reflectance, m.exponent, m.ior],
                     np.float32)
+
+
+def read_exr(path):
+    """Channels of an uncompressed scanline OpenEXR file: {name: (H, W) float32}."""
+    b = open(path, "rb").read()
+    assert b[:4] == bytes([0x76, 0x2f, 0x31, 0x01])
+    off = 8
+    attrs = {}
+    while b[off] != 0:
+        e = b.index(b"\0", off); name = b[off:e].decode(); off = e + 1
+        e = b.index(b"\0", off); typ = b[off:e].decode(); off = e + 1
+        size = int(np.frombuffer(b, np.int32, 1, off)[0]); off += 4
+        attrs[name] = (typ, b[off:off + size]); off += size
+    off += 1
+    assert attrs["compression"][1][0] == 0, "compressed EXR"
+    x0, y0, x1, y1 = (int(v) for v in np.frombuffer(attrs["dataWindow"][1], np.int32))
+    w, h = x1 - x0 + 1, y1 - y0 + 1
+    chl, names, p = attrs["channels"][1], [], 0
+    while chl[p] != 0:
+        e = chl.index(b"\0", p); names.append(chl[p:e].decode()); p = e + 1 + 16
+    offsets = np.frombuffer(b, np.uint64, h, off)
+    out = {n: np.zeros((h, w), np.float32) for n in names}
+    for o in offsets:
+        o = int(o)
+        y = int(np.frombuffer(b, np.int32, 1, o)[0]) - y0
+        data = np.frombuffer(b, np.float32, w * len(names), o + 8)
+        for k, n in enumerate(names):
+            out[n][y] = data[k * w:(k + 1) * w]
+    return out

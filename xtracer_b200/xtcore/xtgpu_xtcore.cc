@@ -12,6 +12,10 @@
 //       --ao-distance D  AO occlusion distance (GPU), default 100
 //       --threads N    OpenMP threads of the tile loop, default all
 //       --tile N       tile size, default 32 (context.cc:5)
+//       --png P        the assembled frame as PNG through the GPU quantiser
+//       --exr P        the assembled frame as OpenEXR (this library's writer)
+//       --ref-png P, --ref-exr P   the same frame through XTracer's own writers
+//                      (nimg::io::save::png / exr), for comparison
 //   xtgpu-xtcore flatten <scn> <out.bin>
 //       writes the flattened scene description (see write_flat)
 //
@@ -31,6 +35,7 @@
 #include <xtcore/integrator.h>
 #include <xtcore/integrator/wireframe/integrator.h>
 #include <xtcore/parseutil.h>
+#include <nimg/img.h>
 
 #include "gpu_integrator.h"
 
@@ -129,6 +134,7 @@ int mode_render(int argc, char **argv)
     unsigned long long seed = 1;
     float aod = 100.f;
     size_t threads = 0, tile = 32;
+    std::string png, exr, ref_png, ref_exr;
     for (int i = 9; i < argc; ++i) {
         std::string a = argv[i];
         if (a == "--cpu") cpu = true;
@@ -138,6 +144,10 @@ int mode_render(int argc, char **argv)
         else if (a == "--ao-distance" && i + 1 < argc) aod = (float)atof(argv[++i]);
         else if (a == "--threads" && i + 1 < argc) threads = strtoul(argv[++i], 0, 10);
         else if (a == "--tile" && i + 1 < argc) tile = strtoul(argv[++i], 0, 10);
+        else if (a == "--png" && i + 1 < argc) png = argv[++i];
+        else if (a == "--exr" && i + 1 < argc) exr = argv[++i];
+        else if (a == "--ref-png" && i + 1 < argc) ref_png = argv[++i];
+        else if (a == "--ref-exr" && i + 1 < argc) ref_exr = argv[++i];
         else {
             fprintf(stderr, "xtgpu-xtcore: unknown option %s\n", a.c_str());
             return 2;
@@ -205,10 +215,32 @@ int mode_render(int argc, char **argv)
     }
     fclose(f);
     int rc = 0;
+    if (!png.empty() || !exr.empty()) {
+        std::vector<float> frame(4 * w * h);
+        for (size_t y = 0; y < h; ++y)
+            for (size_t x = 0; x < w; ++x) {
+                const nimg::ColorRGBAf &c = pm.pixel_ro(x, y);
+                float *o = &frame[4 * (y * w + x)];
+                o[0] = c.r();
+                o[1] = c.g();
+                o[2] = c.b();
+                o[3] = c.a();
+            }
+        if (!png.empty() && xtgpu_save_png_host(png.c_str(), (int32_t)w, (int32_t)h, frame.data(), 0) != XTGPU_OK) {
+            fprintf(stderr, "xtgpu-xtcore: %s\n", xtgpu_last_error());
+            rc = 1;
+        }
+        if (!exr.empty() && xtgpu_write_exr(exr.c_str(), (int32_t)w, (int32_t)h, frame.data()) != XTGPU_OK) {
+            fprintf(stderr, "xtgpu-xtcore: %s\n", xtgpu_last_error());
+            rc = 1;
+        }
+    }
+    if (!ref_png.empty() && nimg::io::save::png(ref_png.c_str(), pm)) rc = 1;
+    if (!ref_exr.empty() && nimg::io::save::exr(ref_exr.c_str(), pm)) rc = 1;
     if (gi) {
         printf("{\"integrator\": \"gpu:%s\", \"render_s\": %.9f, \"rays\": %llu, \"status\": %d, \"error\": \"%s\"}\n",
                integ.c_str(), secs, (unsigned long long)gi->rays(), (int)gi->status(), gi->error().c_str());
-        rc = gi->status() == XTGPU_OK ? 0 : 1;
+        if (gi->status() != XTGPU_OK) rc = 1;
     } else {
         printf("{\"integrator\": \"cpu:%s\", \"render_s\": %.9f, \"threads\": %d}\n", integ.c_str(), secs,
                threads ? (int)threads : omp_get_max_threads());

@@ -157,6 +157,10 @@ SIGNATURES = {
     "xtgpu_autotune": [C.c_void_p, C.c_int32, C.c_double, C.c_void_p, C.c_void_p],
     "xtgpu_scene_tuning": [C.c_void_p, C.c_void_p],
     "xtgpu_scene_set_tuning": [C.c_void_p, C.c_void_p],
+    "xtgpu_frame_rgba8": [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p],
+    "xtgpu_write_png": [C.c_char_p, C.c_int32, C.c_int32, C.c_void_p],
+    "xtgpu_write_exr": [C.c_char_p, C.c_int32, C.c_int32, C.c_void_p],
+    "xtgpu_save_png_host": [C.c_char_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p],
 }
 
 _lib = None
@@ -393,3 +397,31 @@ class EmissionIntegrator(_Integrator):
 
 class WireframeIntegrator(_Integrator):
     kind = WIREFRAME
+
+
+def save_png(path: str, frame, stream=None) -> None:
+    """Writes an RGBA float frame (H, W, 4) as an 8-bit PNG with XTracer's
+    quantisation (lib/nimg/img.cc:150-172), done on the GPU: a CUDA tensor is
+    quantised in place on its device, a host array is uploaded first."""
+    if hasattr(frame, "is_cuda") and frame.is_cuda:
+        import torch
+        f = frame.contiguous()
+        h, w = int(f.shape[0]), int(f.shape[1])
+        q = torch.empty((h, w, 4), dtype=torch.uint8, device=f.device)
+        check(lib().xtgpu_frame_rgba8(C.c_void_p(f.data_ptr()), h * w, C.c_void_p(q.data_ptr()),
+                                      stream_handle(stream)))
+        host = q.cpu().numpy()
+        check(lib().xtgpu_write_png(path.encode(), w, h, _ptr(np.ascontiguousarray(host))))
+        return
+    a = np.ascontiguousarray(frame, np.float32)
+    check(lib().xtgpu_save_png_host(path.encode(), a.shape[1], a.shape[0], _ptr(a), stream_handle(stream)))
+
+
+def save_exr(path: str, frame) -> None:
+    """Writes the R, G, B channels of an RGBA float frame (H, W, 4) as an
+    uncompressed OpenEXR file, the layout XTracer's EXR writer uses
+    (lib/nimg/img.cc:72-141)."""
+    if hasattr(frame, "is_cuda") and frame.is_cuda:
+        frame = frame.cpu().numpy()
+    a = np.ascontiguousarray(frame, np.float32)
+    check(lib().xtgpu_write_exr(path.encode(), a.shape[1], a.shape[0], _ptr(a)))
