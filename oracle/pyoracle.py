@@ -36,12 +36,14 @@ class XoSceneDesc(C.Structure):
                 ("n_materials", C.c_int32), ("materials", C.c_void_p),
                 ("env_type", C.c_int32), ("env_a", C.c_float * 3), ("env_b", C.c_float * 3),
                 ("cam_pos", C.c_float * 3), ("cam_target", C.c_float * 3), ("cam_up", C.c_float * 3),
-                ("cam_fov", C.c_float), ("obj_uv_scale", C.c_void_p), ("tri_uvs", C.c_void_p)]
+                ("cam_fov", C.c_float), ("obj_uv_scale", C.c_void_p), ("tri_uvs", C.c_void_p),
+                ("cam_type", C.c_int32), ("cam_orientation", C.c_float * 3), ("cam_ipd", C.c_float),
+                ("cam_flength", C.c_float), ("cam_aperture", C.c_float)]
 
 
 class XoRenderParams(C.Structure):
     _fields_ = [("integrator", C.c_int32), ("width", C.c_int32), ("height", C.c_int32),
-                ("spp", C.c_int32), ("rdepth", C.c_int32), ("ao_max_distance", C.c_float),
+                ("spp", C.c_int32), ("rdepth", C.c_int32), ("aa", C.c_int32), ("ao_max_distance", C.c_float),
                 ("seed", C.c_uint64)]
 
 
@@ -73,6 +75,10 @@ def lib():
         L.xo_kat_lobe.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]
         L.xo_kat_material.argtypes = [C.POINTER(XoMaterial), C.c_void_p, C.c_int32] + [C.c_void_p] * 4
         L.xo_kat_gradient.argtypes = [C.c_void_p] * 4
+        L.xo_kat_camera_dof.argtypes = [C.c_void_p, C.c_int32] + [C.c_void_p] * 3 + [C.c_float] * 7 + [C.c_void_p] * 2
+        L.xo_kat_camera_erp.argtypes = [C.c_void_p] * 2 + [C.c_float] * 4 + [C.c_void_p] * 2
+        L.xo_kat_camera_ods.argtypes = [C.c_void_p] * 2 + [C.c_float] * 5 + [C.c_void_p] * 2
+        L.xo_kat_camera_cubemap.argtypes = [C.c_void_p] + [C.c_float] * 4 + [C.c_void_p] * 2
         L.xo_stream_uniform.argtypes = [C.c_uint64, C.c_uint32]
         L.xo_stream_uniform.restype = C.c_double
         L.xo_path_key.argtypes = [C.c_uint64, C.c_uint64]
@@ -129,6 +135,11 @@ class OracleScene:
         d.cam_target[:] = list(spec.camera.target)
         d.cam_up[:] = list(spec.camera.up)
         d.cam_fov = spec.camera.fov
+        d.cam_type = getattr(spec.camera, "type", 0)
+        d.cam_orientation[:] = list(getattr(spec.camera, "orientation", (0.0, 0.0, 0.0)))
+        d.cam_ipd = getattr(spec.camera, "ipd", 0.0)
+        d.cam_flength = getattr(spec.camera, "flength", 0.0)
+        d.cam_aperture = getattr(spec.camera, "aperture", 0.0)
         uvs = getattr(spec, "obj_uv_scale", None)
         d.obj_uv_scale = _ptr(arr(uvs.reshape(-1), np.float32)) if uvs is not None else None
         tuv = getattr(spec, "tri_uvs", None)
@@ -158,12 +169,12 @@ class OracleScene:
         return dict(hit=hit, t=t, obj=obj, prim=prim, point=pt, normal=nr)
 
     def render(self, integrator: int, width: int, height: int, spp: int = 1, rdepth: int = 4,
-               ao_max_distance: float = 100.0, seed: int = 1, pixels: np.ndarray = None):
+               ao_max_distance: float = 100.0, seed: int = 1, pixels: np.ndarray = None, aa: int = 1):
         if pixels is None:
             ys, xs = np.mgrid[0:height, 0:width]
             pixels = np.stack([xs.ravel(), ys.ravel()], axis=1)
         pixels = np.ascontiguousarray(pixels, np.int32).reshape(-1, 2)
-        p = XoRenderParams(integrator, width, height, spp, rdepth, ao_max_distance, seed)
+        p = XoRenderParams(integrator, width, height, spp, rdepth, aa, ao_max_distance, seed)
         out = np.zeros((pixels.shape[0], 4), np.float32)
         rays = C.c_uint64(0)
         lib().xo_render(self.handle, C.byref(p), pixels.shape[0], _ptr(pixels), _ptr(out), C.byref(rays))

@@ -41,6 +41,9 @@
 #include <xtcore/math/triangle.h>
 #include <xtcore/math/aabb.h>
 #include <xtcore/camera/perspective.h>
+#include <xtcore/camera/erp.h>
+#include <xtcore/camera/ods.h>
+#include <xtcore/camera/cubemap.h>
 #include <xtcore/sampler_col.h>
 #include <xtcore/sampler_gradient.h>
 #include <xtcore/material/lambert.h>
@@ -359,6 +362,14 @@ static int mode_kat(int argc, char **argv)
     // its one-time srand(time(NULL)) before any srand(seed) below.
     {
         Vector3f n(0, 1, 0);
+        xtcore::camera::Perspective lens;   // the thin-lens ray draws in perspective.cc's unit
+        lens.position = Vector3f(0, 0, -5);
+        lens.target = Vector3f(0, 0, 0);
+        lens.up = Vector3f(0, 1, 0);
+        lens.fov = 45.f;
+        lens.flength = 5.f;
+        lens.aperture = 0.5f;
+        lens.get_primary_ray(1.f, 1.f, 4.f, 4.f);
         for (int i = 0; i < 4; ++i) {
             nmath::sample::hemisphere(n, n);
             nmath::sample::diffuse(n);
@@ -396,6 +407,45 @@ static int mode_kat(int argc, char **argv)
             c.up = Vector3f(a[6], a[7], a[8]);
             c.fov = (float)a[9];
             Ray r = c.get_primary_ray((float)a[12], (float)a[13], (float)a[10], (float)a[11]);
+            put3(out, r.origin);
+            put3(out, r.direction);
+        } else if (!strcmp(kind, "camera_dof")) {
+            // seed, position, target, up, fov, flength, aperture, w, h, x, y:
+            // the thin-lens ray draws two prng_c values (perspective.cc:73-82)
+            srand((unsigned)a[0]);
+            xtcore::camera::Perspective c;
+            c.position = Vector3f(a[1], a[2], a[3]);
+            c.target = Vector3f(a[4], a[5], a[6]);
+            c.up = Vector3f(a[7], a[8], a[9]);
+            c.fov = (float)a[10];
+            c.flength = (float)a[11];
+            c.aperture = (float)a[12];
+            Ray r = c.get_primary_ray((float)a[15], (float)a[16], (float)a[13], (float)a[14]);
+            put3(out, r.origin);
+            put3(out, r.direction);
+        } else if (!strcmp(kind, "camera_erp") || !strcmp(kind, "camera_ods")) {
+            // position, orientation, ipd, w, h, x, y
+            xtcore::asset::ICamera *c;
+            xtcore::camera::ERP erp;
+            xtcore::camera::ODS ods;
+            if (!strcmp(kind, "camera_erp")) {
+                erp.position = Vector3f(a[0], a[1], a[2]);
+                erp.orientation = Vector3f(a[3], a[4], a[5]);
+                c = &erp;
+            } else {
+                ods.position = Vector3f(a[0], a[1], a[2]);
+                ods.orientation = Vector3f(a[3], a[4], a[5]);
+                ods.ipd = (float)a[6];
+                c = &ods;
+            }
+            Ray r = c->get_primary_ray((float)a[9], (float)a[10], (float)a[7], (float)a[8]);
+            put3(out, r.origin);
+            put3(out, r.direction);
+        } else if (!strcmp(kind, "camera_cubemap")) {
+            // position, w, h, x, y
+            xtcore::camera::Cubemap c;
+            c.position = Vector3f(a[0], a[1], a[2]);
+            Ray r = c.get_primary_ray((float)a[5], (float)a[6], (float)a[3], (float)a[4]);
             put3(out, r.origin);
             put3(out, r.direction);
         } else if (!strcmp(kind, "sphere")) {

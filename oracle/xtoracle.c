@@ -695,6 +695,176 @@ void xo_camera_ray(const float pos[3], const float target[3], const float up[3],
     dir[0] = t.x; dir[1] = t.y; dir[2] = t.z;
 }
 
+/* Perspective with depth of field (camera/perspective.cc:38-98, flength > 0):
+ * the direction in camera space is the lens point (two prng_c draws, x then y,
+ * within half the aperture) to the focal-plane point; the origin is the lens
+ * point transformed and moved to the position. */
+static void camera_dof(rng_t *r, const float pos[3], const float target[3], const float up[3], float fov,
+                       float flength, float aperture, float x, float y, float w, float h, double org[3],
+                       double dir[3])
+{
+    double aspect = (double)w / (double)h;
+    v3 d = V((2.0 * (double)x / (double)w) - 1.0,
+             ((2.0 * (double)y / (double)h) - 1.0) / aspect,
+             1.0 / tan(fov * XO_RADIAN / 2.0));
+    v3 p = vf(pos);
+    v3 rz = normalized(sub(vf(target), p));
+    v3 rx = normalized(cross(vf(up), rz));
+    v3 ry = normalized(cross(rx, rz));
+    v3 lo = d;
+    double half = aperture / 2.f;
+    lo.x += prng(r, -half, half);
+    lo.y += prng(r, -half, half);
+    v3 fpip = add(d, muls(normalized(d), (double)flength));
+    v3 fd = sub(fpip, lo);
+    v3 t = V(rx.x * fd.x + ry.x * fd.y + rz.x * fd.z + 0.0,
+             rx.y * fd.x + ry.y * fd.y + rz.y * fd.z + 0.0,
+             rx.z * fd.x + ry.z * fd.y + rz.z * fd.z + 0.0);
+    t = normalize(t);
+    v3 o = V(rx.x * lo.x + ry.x * lo.y + rz.x * lo.z + 0.0,
+             rx.y * lo.x + ry.y * lo.y + rz.y * lo.z + 0.0,
+             rx.z * lo.x + ry.z * lo.y + rz.z * lo.z + 0.0);
+    o = add(o, p);
+    org[0] = o.x; org[1] = o.y; org[2] = o.z;
+    dir[0] = t.x; dir[1] = t.y; dir[2] = t.z;
+}
+
+/* Matrix4x4f::rotate(euler) applied to an identity matrix (lib/nmath/matrix.cc:
+ * 485-492, 414-427): I *= (xrot * yrot * zrot), products summed left to right. */
+static void euler_rotation(const float e3[3], double m[3][4])
+{
+    double ex = e3[0], ey = e3[1], ez = e3[2];
+    double xr[3][3] = {{1, 0, 0}, {0, cos(ex), -sin(ex)}, {0, sin(ex), cos(ex)}};
+    double yr[3][3] = {{cos(ey), 0, sin(ey)}, {0, 1, 0}, {-sin(ey), 0, cos(ey)}};
+    double zr[3][3] = {{cos(ez), -sin(ez), 0}, {sin(ez), cos(ez), 0}, {0, 0, 1}};
+    double t[3][3], r3[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) t[i][j] = xr[i][0] * yr[0][j] + xr[i][1] * yr[1][j] + xr[i][2] * yr[2][j];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) r3[i][j] = t[i][0] * zr[0][j] + t[i][1] * zr[1][j] + t[i][2] * zr[2][j];
+    double m4[4][4] = {{r3[0][0], r3[0][1], r3[0][2], 0}, {r3[1][0], r3[1][1], r3[1][2], 0},
+                       {r3[2][0], r3[2][1], r3[2][2], 0}, {0, 0, 0, 1}};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 4; ++j) {
+            double id0 = i == 0, id1 = i == 1, id2 = i == 2;
+            m[i][j] = id0 * m4[0][j] + id1 * m4[1][j] + id2 * m4[2][j] + 0.0 * m4[3][j];
+        }
+}
+
+static v3 transform4(const double m[3][4], v3 v)   /* Vector3f::transformed(Matrix4x4f), vector.inl:517-523 */
+{
+    return V(m[0][0] * v.x + m[0][1] * v.y + m[0][2] * v.z + m[0][3],
+             m[1][0] * v.x + m[1][1] * v.y + m[1][2] * v.z + m[1][3],
+             m[2][0] * v.x + m[2][1] * v.y + m[2][2] * v.z + m[2][3]);
+}
+
+/* ERP::get_primary_ray, camera/erp.cc:13-31 (angles in float, trig in double) */
+static void camera_erp(const float pos[3], const float orient[3], float x, float y, float w, float h,
+                       double org[3], double dir[3])
+{
+    float phi = (float)((x / w) * XO_PI * 2.f);
+    float theta = (float)((y / h) * XO_PI);
+    v3 d = V(sin(theta) * cos(phi), cos(theta), sin(theta) * sin(phi));
+    double m[3][4];
+    euler_rotation(orient, m);
+    d = transform4(m, d);
+    org[0] = pos[0]; org[1] = pos[1]; org[2] = pos[2];
+    dir[0] = d.x; dir[1] = d.y; dir[2] = d.z;
+}
+
+/* ODS::get_primary_ray, camera/ods.cc:17-40: the upper half of the frame is
+ * one eye, the lower the other, each origin on a circle of radius ipd/2 */
+static void camera_ods(const float pos[3], const float orient[3], float ipd, float x, float y, float w, float h,
+                       double org[3], double dir[3])
+{
+    float hh = h * .5f;
+    float scale = ipd * .5f * ((y < hh) ? -1 : 1);
+    if (y > hh) y = y - hh;
+    float theta = (float)((x / w) * 2.f * XO_PI);
+    float phi = (float)(XO_PI * .5f - (y / hh) * XO_PI);
+    v3 o = add(muls(V(cos(theta), 0, sin(theta)), (double)scale), vf(pos));
+    v3 d = V(sin(theta) * cos(phi), sin(phi), -cos(theta) * cos(phi));
+    double m[3][4];
+    euler_rotation(orient, m);
+    d = transform4(m, d);
+    org[0] = o.x; org[1] = o.y; org[2] = o.z;
+    dir[0] = d.x; dir[1] = d.y; dir[2] = d.z;
+}
+
+/* Cubemap::get_primary_ray, camera/cubemap.cc:21-69 (vertical strip of six
+ * square faces +x -x +y -y +z -z) */
+static void camera_cubemap(const float pos[3], float x, float y, float w, float h, double org[3], double dir[3])
+{
+    size_t face_size = (size_t)(h) / 6;
+    size_t face = (size_t)(y) / face_size;
+    v3 camdir = V(0, 0, 0), up = V(0, 0, 0);
+    switch (face) {
+    case 0: camdir = V(1, 0, 0); up = V(0, 1, 0); break;
+    case 1: camdir = V(-1, 0, 0); up = V(0, 1, 0); break;
+    case 2: camdir = V(0, 1, 0); up = V(0, 0, -1); break;
+    case 3: camdir = V(0, -1, 0); up = V(0, 0, 1); break;
+    case 4: camdir = V(0, 0, 1); up = V(0, 1, 0); break;
+    case 5: camdir = V(0, 0, -1); up = V(0, 1, 0); break;
+    }
+    y -= (float)(face * face_size);
+    v3 d = V((2.f * (double)x / (double)w) - 1.f, (2.f * (double)y / (double)face_size) - 1.f, 1.f);
+    d = normalize(d);
+    v3 rz = camdir;
+    v3 rx = normalize(cross(up, rz));
+    v3 ry = normalize(cross(rx, rz));
+    d = V(rx.x * d.x + ry.x * d.y + rz.x * d.z + 0.0, rx.y * d.x + ry.y * d.y + rz.y * d.z + 0.0,
+          rx.z * d.x + ry.z * d.y + rz.z * d.z + 0.0);
+    d = normalize(d);
+    org[0] = pos[0]; org[1] = pos[1]; org[2] = pos[2];
+    dir[0] = d.x; dir[1] = d.y; dir[2] = d.z;
+}
+
+/* The scene's camera at (x, y); r supplies the depth-of-field draws. */
+static void camera_any(const xo_scene_desc *D, rng_t *r, float x, float y, float w, float h, double o[3],
+                       double d[3])
+{
+    switch (D->cam_type) {
+    case XO_CAM_ERP: camera_erp(D->cam_pos, D->cam_orientation, x, y, w, h, o, d); return;
+    case XO_CAM_ODS: camera_ods(D->cam_pos, D->cam_orientation, D->cam_ipd, x, y, w, h, o, d); return;
+    case XO_CAM_CUBEMAP: camera_cubemap(D->cam_pos, x, y, w, h, o, d); return;
+    default:
+        if (D->cam_flength > 0)
+            camera_dof(r, D->cam_pos, D->cam_target, D->cam_up, D->cam_fov, D->cam_flength, D->cam_aperture, x, y,
+                       w, h, o, d);
+        else
+            xo_camera_ray(D->cam_pos, D->cam_target, D->cam_up, D->cam_fov, x, y, w, h, o, d);
+    }
+}
+
+void xo_kat_camera_dof(const int32_t *table, int32_t rand_max, const float pos[3], const float target[3],
+                       const float up[3], float fov, float flength, float aperture, float x, float y, float w,
+                       float h, double org[3], double dir[3])
+{
+    rng_t r;
+    memset(&r, 0, sizeof(r));
+    r.kind = XO_RNG_TABLE;
+    r.table = table;
+    r.rand_max = rand_max;
+    camera_dof(&r, pos, target, up, fov, flength, aperture, x, y, w, h, org, dir);
+}
+
+void xo_kat_camera_erp(const float pos[3], const float orient[3], float x, float y, float w, float h,
+                       double org[3], double dir[3])
+{
+    camera_erp(pos, orient, x, y, w, h, org, dir);
+}
+
+void xo_kat_camera_ods(const float pos[3], const float orient[3], float ipd, float x, float y, float w, float h,
+                       double org[3], double dir[3])
+{
+    camera_ods(pos, orient, ipd, x, y, w, h, org, dir);
+}
+
+void xo_kat_camera_cubemap(const float pos[3], float x, float y, float w, float h, double org[3], double dir[3])
+{
+    camera_cubemap(pos, x, y, w, h, org, dir);
+}
+
 /* ------------------------------------------------------------------------ */
 /* Materials: IMaterial::sample_path (src/xtcore/material/).                  */
 typedef struct {
@@ -780,21 +950,30 @@ int xo_render(const xo_scene *s, const xo_render_params *p, int64_t npix, const 
 {
     const xo_scene_desc *D = &s->d;
     uint64_t nr = 0;
-    double weight = 1.f;
-    weight *= 1. / (double)p->spp;   /* aa.cc:66-74 */
+    /* aa.cc:7-32, 51-77: per pixel aa^2 grid positions (rows of the grid in
+     * order), each taken spp times; weight 1/(aa^2) as a float, times 1/spp */
+    const int32_t L = p->aa > 1 ? p->aa : 1;
+    double weight = L == 1 ? 1.f : (double)(1.f / (float)(L * L));
+    weight *= 1. / (double)p->spp;
+    const float sub_pixel = 1.f / (float)L, offset = sub_pixel * 0.5f;
     for (int64_t i = 0; i < npix; ++i) {
         int32_t x = px[2 * i], y = px[2 * i + 1];
         float col[4] = {0, 0, 0, 0};
-        double o[3], d[3];
-        xo_camera_ray(D->cam_pos, D->cam_target, D->cam_up, D->cam_fov, (float)x + 0.5f, (float)y + 0.5f,
-                      (float)p->width, (float)p->height, o, d);
-        v3 O = V(o[0], o[1], o[2]), Dd = V(d[0], d[1], d[2]);
-        for (int32_t si = 0; si < p->spp; ++si) {
+        for (int32_t si = 0; si < L * L * p->spp; ++si) {
             rng_t r;
             memset(&r, 0, sizeof(r));
             r.kind = XO_RNG_STREAM;
             r.key = xo_path_key(p->seed, (uint64_t)si * (uint64_t)p->width * (uint64_t)p->height +
                                              (uint64_t)y * (uint64_t)p->width + (uint64_t)x);
+            const int32_t gi = si / p->spp;   /* grid position of the sample */
+            double cx = (double)x + 0.5f, cy = (double)y + 0.5f;
+            if (L > 1) {
+                cx = ((double)x + (double)(gi % L) * (double)sub_pixel) + (double)offset;
+                cy = ((double)y + (double)(gi / L) * (double)sub_pixel) + (double)offset;
+            }
+            double o[3], d[3];
+            camera_any(D, &r, (float)cx, (float)cy, (float)p->width, (float)p->height, o, d);
+            v3 O = V(o[0], o[1], o[2]), Dd = V(d[0], d[1], d[2]);
             hrec h;
             int32_t oi, pi;
             if (p->integrator == XO_STENCIL) {          /* stencil/integrator.cc:13-33 */

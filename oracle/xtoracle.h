@@ -31,6 +31,9 @@ enum { XO_ACCEL_OCTREE = 0, XO_ACCEL_BVH = 1 };
 /* random source: 0 = table of libc rand() values (known-answer tests),
  * 1 = the counter stream shared with the GPU path (SplitMix64 of key+counter). */
 enum { XO_RNG_TABLE = 0, XO_RNG_STREAM = 1 };
+/* cameras (src/xtcore/camera/): thin-lens perspective, equirectangular,
+ * omni-directional stereo, cubemap vertical strip */
+enum { XO_CAM_PERSPECTIVE = 0, XO_CAM_ERP = 1, XO_CAM_ODS = 2, XO_CAM_CUBEMAP = 3 };
 
 typedef struct {
     int32_t type;
@@ -61,6 +64,10 @@ typedef struct {
                                     what the loader sets without uscale/vscale */
     const float *tri_uvs;        /* 6 floats per triangle (Triangle::tc[0..2].xy), or NULL = the
                                     Triangle constructor's (0,0) (1,0) (0,0), triangle.cc:8-13 */
+    int32_t cam_type;            /* XO_CAM_* */
+    float cam_orientation[3];    /* ERP, ODS: euler angles (Matrix4x4f::rotate) */
+    float cam_ipd;               /* ODS */
+    float cam_flength, cam_aperture;   /* perspective: depth of field when flength > 0 */
 } xo_scene_desc;
 
 typedef struct xo_scene xo_scene;
@@ -82,13 +89,14 @@ void xo_camera_ray(const float pos[3], const float target[3], const float up[3],
 typedef struct {
     int32_t integrator;    /* XO_STENCIL .. XO_WIREFRAME */
     int32_t width, height, spp, rdepth;
+    int32_t aa;            /* grid anti-aliasing level (aa.cc:7-32); 0 or 1 = pixel centre */
     float ao_max_distance; /* 100 in the shipped AO integrator */
     uint64_t seed;         /* XO_RNG_STREAM key */
 } xo_render_params;
 
-/* Renders the listed pixels (x,y pairs) with aa = 1 (one pixel-centre ray per
- * sample, aa.cc:11-18) and `spp` samples of weight 1/spp (aa.cc:66-74).  Output
- * RGBA per listed pixel; *rays = number of Scene::intersection calls. */
+/* Renders the listed pixels (x,y pairs): aa^2 grid positions per pixel, each
+ * taken `spp` times with weight 1/(aa^2 spp) (aa.cc:7-32, 51-77).  Output RGBA
+ * per listed pixel; *rays = number of Scene::intersection calls. */
 int xo_render(const xo_scene *s, const xo_render_params *p, int64_t npix, const int32_t *px,
               float *rgba, uint64_t *rays);
 
@@ -104,6 +112,17 @@ void xo_kat_lobe(const int32_t *table, int32_t rand_max, const double n[3], cons
 int  xo_kat_material(const xo_material *m, const int32_t *table, int32_t rand_max, const double p[3],
                      const double n[3], const double inc[3], double out[9]);
 void xo_kat_gradient(const float a[3], const float b[3], const double d[3], float out[3]);
+
+/* Camera rays of every camera type, known-answer hooks: perspective with depth
+ * of field (the two prng_c draws from `table`), equirectangular, ODS, cubemap. */
+void xo_kat_camera_dof(const int32_t *table, int32_t rand_max, const float pos[3], const float target[3],
+                       const float up[3], float fov, float flength, float aperture, float x, float y, float w,
+                       float h, double org[3], double dir[3]);
+void xo_kat_camera_erp(const float pos[3], const float orient[3], float x, float y, float w, float h,
+                       double org[3], double dir[3]);
+void xo_kat_camera_ods(const float pos[3], const float orient[3], float ipd, float x, float y, float w, float h,
+                       double org[3], double dir[3]);
+void xo_kat_camera_cubemap(const float pos[3], float x, float y, float w, float h, double org[3], double dir[3]);
 
 /* The counter stream shared with the GPU path, exposed for tests. */
 double xo_stream_uniform(uint64_t key, uint32_t counter);

@@ -17,7 +17,11 @@ these fixtures are what pins the oracle restatement (oracle/xtoracle.c):
 * render_primary_*.npz  frames of the normal, uv, emission and wireframe
               integrators (deterministic, 3 samples per pixel) on scenes that
               exercise every texture-coordinate path (`--primary` regenerates
-              only these).
+              only these);
+* kat_cameras.npz, render_cameras.npz  rays of the ERP, ODS, cubemap and
+              depth-of-field cameras (with the rand() values the latter drew),
+              and stencil/depth/normal frames through each camera with grid
+              anti-aliasing (`--cameras` regenerates only these).
 
 Run here (needs the reference sources and oracle/_ref/xtref):
     make -f oracle/ref.mk REF=<xtracer source tree> -j8
@@ -223,11 +227,95 @@ def make_primary(work):
         print("render_primary", name, sorted(rend))
 
 
+def make_cameras(work, rng):
+    kat = {}
+    # equirectangular and omni-directional stereo (camera/erp.cc, ods.cc)
+    for kind in ("erp", "ods"):
+        rows = []
+        for i in range(96):
+            pos = rng.uniform(-5, 5, 3)
+            ori = rng.uniform(-np.pi, np.pi, 3) if i % 4 else np.zeros(3)
+            ipd = rng.uniform(0.05, 0.2)
+            w, h = [(128, 64), (256, 256), (64, 48), (1000, 500)][i % 4]
+            x, y = rng.uniform(0, w), rng.uniform(0, h)
+            rows.append(np.concatenate([pos, ori, [ipd, w, h, x, y]]).astype(np.float32).astype(np.float64))
+        rows = np.array(rows)
+        res = po.ref_kat([_line("camera_" + kind, *r) for r in rows])
+        kat[kind + "_in"] = rows
+        kat[kind + "_out"] = np.array([[float.fromhex(t) for t in r[1:]] for r in res])
+    # cubemap vertical strip (camera/cubemap.cc)
+    rows = []
+    for i in range(96):
+        pos = rng.uniform(-5, 5, 3)
+        w = [16, 64, 100, 31][i % 4]
+        h = 6 * [16, 64, 100, 7][i % 4]
+        x, y = rng.uniform(0, w), rng.uniform(0, h)
+        rows.append(np.concatenate([pos, [w, h, x, y]]).astype(np.float32).astype(np.float64))
+    rows = np.array(rows)
+    res = po.ref_kat([_line("camera_cubemap", *r) for r in rows])
+    kat["cubemap_in"] = rows
+    kat["cubemap_out"] = np.array([[float.fromhex(t) for t in r[1:]] for r in res])
+    # perspective with depth of field (perspective.cc:73-95): two prng_c draws
+    rows, seeds = [], rng.integers(1, 2 ** 31 - 1, 96)
+    for i in range(96):
+        pos = rng.uniform(-10, 10, 3); tgt = pos + rng.uniform(-5, 5, 3)
+        up = np.array([0, 1, 0.0]) if i % 3 else rng.uniform(-1, 1, 3)
+        fov = rng.choice([30.0, 45.0, 60.0]); fl = rng.uniform(0.5, 20.0); ap = rng.uniform(0.0, 2.0)
+        w, h = [(64, 64), (1920, 1080), (100, 50)][i % 3]
+        x, y = rng.uniform(0, w), rng.uniform(0, h)
+        rows.append(np.concatenate([[seeds[i]], pos, tgt, up, [fov, fl, ap, w, h, x, y]]).astype(np.float32)
+                    .astype(np.float64))
+    rows = np.array(rows)
+    rows[:, 0] = seeds
+    res = po.ref_kat([_line("camera_dof", *r) for r in rows])
+    kat["dof_in"] = rows
+    kat["dof_out"] = np.array([[float.fromhex(t) for t in r[1:]] for r in res])
+    tab = po.ref_kat(["rand %d 8" % s for s in seeds])
+    kat["dof_table"] = np.array([[int(t) for t in r[1:9]] for r in tab], np.int64)
+    kat["rand_max"] = int(tab[0][9])
+    np.savez_compressed(os.path.join(HERE, "kat_cameras.npz"), **kat)
+    print("kat_cameras.npz", {k: np.shape(v) for k, v in kat.items()})
+    # frames through each camera, grid anti-aliasing
+    rend = {}
+    for tag, cam, w, h, aa in camera_cases():
+        spec = scenes.spheres_scene(64, seed=1, name="cam_" + tag, camera=cam)
+        scn = spec.write_scn(work)
+        for integ in ("stencil", "depth", "normal"):
+            xy, rgba, st = po.ref_render(scn, integ, w, h, spp=2, aa=aa, threads=1, seed=1, workdir=work)
+            rend["%s_%s_xy" % (tag, integ)] = xy
+            rend["%s_%s_rgba" % (tag, integ)] = rgba
+            rend["%s_%s_rays" % (tag, integ)] = st["rays"]
+    dof = scenes.Camera((0.0, 3.0, -12.0), (0.0, 1.5, 0.0), (0.0, 1.0, 0.0), 50.0, flength=11.0, aperture=0.75)
+    spec = scenes.spheres_scene(64, seed=1, name="cam_dof", camera=dof)
+    scn = spec.write_scn(work)
+    imgs = []
+    for seed in (31, 32, 33, 34):
+        xy, rgba, st = po.ref_render(scn, "depth", 48, 48, spp=16, threads=1, seed=seed, workdir=work)
+        imgs.append(rgba)
+    rend["dof_depth_xy"] = xy
+    rend["dof_depth_rgba"] = np.stack(imgs)
+    np.savez_compressed(os.path.join(HERE, "render_cameras.npz"), **rend)
+    print("render_cameras.npz", sorted(rend))
+
+
+def camera_cases():
+    """(tag, camera, width, height, aa) of the camera frame fixtures."""
+    C = scenes.Camera
+    return [("persp_aa3", C((0.0, 6.0, -14.0), (0.0, 1.0, 0.0), (0.0, 1.0, 0.0), 60.0), 48, 40, 3),
+            ("erp_aa2", C((0.5, 2.0, 0.25), type=scenes.CAM_ERP, orientation=(0.25, -0.5, 0.125)), 96, 48, 2),
+            ("ods_aa2", C((0.5, 2.0, 0.25), type=scenes.CAM_ODS, orientation=(0.0, 0.75, 0.0), ipd=0.125),
+             64, 64, 2),
+            ("cubemap_aa2", C((0.5, 2.0, 0.25), type=scenes.CAM_CUBEMAP), 24, 144, 2)]
+
+
 def main():
     if not po.ref_available():
         raise SystemExit("oracle/_ref/xtref missing: make -f oracle/ref.mk REF=<xtracer sources>")
     if "--primary" in sys.argv:
         make_primary(tempfile.mkdtemp(prefix="xtgold"))
+        return
+    if "--cameras" in sys.argv:
+        make_cameras(tempfile.mkdtemp(prefix="xtgold"), np.random.default_rng(20261204))
         return
     rng = np.random.default_rng(20261203)
     kat = make_kat(rng)

@@ -219,3 +219,57 @@ def test_primary_integrators_golden(name, integ, code):
     # a u/v scale below 1 drives asin out of its domain on spheres: the
     # reference writes NaN there, and so must the restatement
     assert np.array_equal(out, ref, equal_nan=True), np.nanmax(np.abs(out - ref))
+
+
+def _f3(v):
+    return np.ascontiguousarray(v, np.float32).ctypes.data_as(C.c_void_p)
+
+
+def test_camera_kat_erp_ods_cubemap_dof():
+    """ERP, ODS, cubemap and thin-lens depth-of-field rays (camera/*.cc),
+    including the Matrix4x4f euler rotation and the two prng_c lens draws,
+    bit for bit against the reference."""
+    k = np.load(os.path.join(GOLD, "kat_cameras.npz"))
+    L = po.lib()
+    o, d = np.zeros(3), np.zeros(3)
+    P = lambda a: a.ctypes.data_as(C.c_void_p)
+    for kind in ("erp", "ods"):
+        for r, want in zip(k[kind + "_in"], k[kind + "_out"]):
+            if kind == "erp":
+                L.xo_kat_camera_erp(_f3(r[0:3]), _f3(r[3:6]), r[9], r[10], r[7], r[8], P(o), P(d))
+            else:
+                L.xo_kat_camera_ods(_f3(r[0:3]), _f3(r[3:6]), r[6], r[9], r[10], r[7], r[8], P(o), P(d))
+            assert np.array_equal(np.concatenate([o, d]), want), (kind, r)
+    for r, want in zip(k["cubemap_in"], k["cubemap_out"]):
+        L.xo_kat_camera_cubemap(_f3(r[0:3]), r[5], r[6], r[3], r[4], P(o), P(d))
+        assert np.array_equal(np.concatenate([o, d]), want), ("cubemap", r)
+    for r, tab, want in zip(k["dof_in"], k["dof_table"], k["dof_out"]):
+        t = np.ascontiguousarray(tab, np.int32)
+        L.xo_kat_camera_dof(P(t), int(k["rand_max"]), _f3(r[1:4]), _f3(r[4:7]), _f3(r[7:10]), r[10], r[11], r[12],
+                            r[15], r[16], r[13], r[14], P(o), P(d))
+        assert np.array_equal(np.concatenate([o, d]), want), ("dof", r)
+
+
+def _camera_cases():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLD, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    return mg.camera_cases()
+
+
+@pytest.mark.parametrize("case", range(4))
+def test_camera_frames_with_grid_antialiasing_golden(case):
+    """Stencil, depth and normal frames through the perspective (aa 3), ERP,
+    ODS and cubemap (aa 2) cameras: grid positions, weights 1/(aa^2 spp) and
+    per-sample folds equal the reference's frames bit for bit."""
+    g = np.load(os.path.join(GOLD, "render_cameras.npz"))
+    tag, cam, w, h, aa = _camera_cases()[case]
+    spec = scenes.spheres_scene(64, seed=1, name="cam_" + tag, camera=cam)
+    orc = po.OracleScene(spec, po.XO_ACCEL_OCTREE)
+    for integ, code in (("stencil", po.STENCIL), ("depth", po.DEPTH), ("normal", po.NORMAL)):
+        xy = g["%s_%s_xy" % (tag, integ)]
+        out, rays = orc.render(code, w, h, spp=2, pixels=xy, aa=aa)
+        assert rays == int(g["%s_%s_rays" % (tag, integ)])
+        ref = g["%s_%s_rgba" % (tag, integ)]
+        assert np.array_equal(out, ref, equal_nan=True), (tag, integ, np.nanmax(np.abs(out - ref)))

@@ -42,12 +42,21 @@ class Material:
     ior: float = 1.0
 
 
+CAM_PERSPECTIVE, CAM_ERP, CAM_ODS, CAM_CUBEMAP = 0, 1, 2, 3
+CAMERA_NAMES = {CAM_PERSPECTIVE: "thin-lens", CAM_ERP: "erp", CAM_ODS: "ods", CAM_CUBEMAP: "cubemap"}
+
+
 @dataclasses.dataclass
 class Camera:
     position: tuple = (0.0, 0.0, -10.0)
     target: tuple = (0.0, 0.0, 0.0)
     up: tuple = (0.0, 1.0, 0.0)
     fov: float = 60.0
+    type: int = CAM_PERSPECTIVE
+    orientation: tuple = (0.0, 0.0, 0.0)   # ERP, ODS: euler angles (radians)
+    ipd: float = 0.0                       # ODS: eye separation
+    flength: float = 0.0                   # perspective: focal length (depth of field when > 0)
+    aperture: float = 0.0
 
 
 @dataclasses.dataclass
@@ -100,9 +109,17 @@ class SceneSpec:
             out += ["environment = {", "  type = color", "  config = {",
                     "    value = %s" % c3(self.env_a), "  }", "}"]
         cam = self.camera
-        out += ["camera = {", "  default = {", "    type = thin-lens",
-                "    position = %s" % v3(cam.position), "    target = %s" % v3(cam.target),
-                "    up = %s" % v3(cam.up), "    fov = %s" % f(cam.fov), "  }", "}"]
+        out += ["camera = {", "  default = {", "    type = %s" % CAMERA_NAMES[cam.type],
+                "    position = %s" % v3(cam.position)]
+        if cam.type == CAM_PERSPECTIVE:
+            out += ["    target = %s" % v3(cam.target), "    up = %s" % v3(cam.up), "    fov = %s" % f(cam.fov)]
+            if cam.flength > 0:
+                out += ["    flength = %s" % f(cam.flength), "    aperture = %s" % f(cam.aperture)]
+        elif cam.type in (CAM_ERP, CAM_ODS):
+            out += ["    orientation = %s" % v3(cam.orientation)]
+            if cam.type == CAM_ODS:
+                out += ["    ipd = %s" % f(cam.ipd)]
+        out += ["  }", "}"]
         out.append("geometry = {")
         mesh_i = 0
         for oi in range(len(self.obj_kind)):
