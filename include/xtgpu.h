@@ -61,6 +61,10 @@ enum { XTGPU_SPHERE = 0, XTGPU_PLANE = 1, XTGPU_MESH = 2 };
 enum { XTGPU_LAMBERT = 0, XTGPU_PHONG = 1, XTGPU_BLINNPHONG = 2, XTGPU_EMISSIVE = 3, XTGPU_DIELECTRIC = 4 };
 /* Environment samplers (sampler_col.cc, sampler_gradient.cc); none = black. */
 enum { XTGPU_ENV_NONE = 0, XTGPU_ENV_COLOR = 1, XTGPU_ENV_GRADIENT = 2 };
+/* Cameras (src/xtcore/camera/): thin-lens perspective, equirectangular,
+ * omni-directional stereo (upper half one eye, lower the other), cubemap
+ * vertical strip (faces +x -x +y -y +z -z, height a multiple of 6). */
+enum { XTGPU_CAM_PERSPECTIVE = 0, XTGPU_CAM_ERP = 1, XTGPU_CAM_ODS = 2, XTGPU_CAM_CUBEMAP = 3 };
 /* Integrators. */
 enum { XTGPU_STENCIL = 0, XTGPU_DEPTH = 1, XTGPU_AO = 2, XTGPU_PATHTRACER = 3,
        /* primary-ray integrators (integrator/{normal,uv,emission,wireframe}) */
@@ -81,6 +85,12 @@ typedef struct {
 typedef struct {
     float position[3], target[3], up[3];
     float fov;                     /* degrees, horizontal (perspective.cc:48-50) */
+    int32_t type;                  /* XTGPU_CAM_PERSPECTIVE (default) .. XTGPU_CAM_CUBEMAP */
+    float orientation[3];          /* ERP, ODS: euler angles in radians (Matrix4x4f::rotate) */
+    float ipd;                     /* ODS: inter-pupillary distance (ods.cc:20-23) */
+    float flength, aperture;       /* perspective: depth of field when flength > 0
+                                      (perspective.cc:73-95); lens draws come first on
+                                      each sample's random stream */
 } xtgpu_camera;
 
 /* A flattened Scene.  Objects are listed in the order Scene::intersection
@@ -178,12 +188,14 @@ typedef struct {
     uint64_t seed;                 /* random stream key: results depend only on (seed, pixel, sample) */
     int32_t node_format;           /* BVH to traverse */
     int32_t x0, y0, x1, y1;        /* pixel rectangle to render; x1 = y1 = 0 means the whole frame */
+    int32_t aa;                    /* grid anti-aliasing level, 0 or 1 = the pixel centre
+                                      (params_t::aa, grid distribution, aa.cc:7-32) */
 } xtgpu_render_params;
 
-/* Renders the rectangle with aa = 1 (one pixel-centre ray per sample,
- * aa.cc:11-18) and writes RGBA float per pixel of the rectangle (row-major)
- * into rgba_dev (device memory).  rays_traced (optional, host) receives the
- * number of rays traced. */
+/* Renders the rectangle and writes RGBA float per pixel of the rectangle
+ * (row-major) into rgba_dev (device memory).  Each pixel takes aa^2 grid
+ * positions, each spp times, of weight 1/(aa^2 spp) (aa.cc:51-77).
+ * rays_traced (optional, host) receives the number of rays traced. */
 XTGPU_API xtgpu_status xtgpu_render(xtgpu_scene *scene, const xtgpu_render_params *params, float *rgba_dev,
                           uint64_t *rays_traced, void *stream);
 /* The same into host memory (copy included). */
@@ -198,7 +210,7 @@ XTGPU_API xtgpu_status xtgpu_render_host(xtgpu_scene *scene, const xtgpu_render_
  * leaves it to another allocator); a render loop that must not meet an
  * allocation failure mid-frame.  Scratch is one static device array of about
  * 11.5 MB held by every GPU that loads the library; a call renders at most
- * XTGPU_NOALLOC_MAX_PATHS paths (rectangle pixels x spp) and larger requests
+ * XTGPU_NOALLOC_MAX_PATHS paths (rectangle pixels x aa^2 x spp) and larger requests
  * return XTGPU_ERR_LIMIT.  Calls that overlap on the GPU race on the shared
  * array.  The first call on a device looks up the array's address; make it
  * before any stream capture.  Output: rgba_dev as in xtgpu_render. */
@@ -254,6 +266,7 @@ typedef struct {
     int32_t width, height, spp, rdepth;
     float ao_max_distance;
     uint64_t seed;
+    int32_t aa;                    /* grid anti-aliasing level, 0 or 1 = pixel centre */
 } xtgpu_job_desc;
 
 typedef struct {

@@ -103,3 +103,31 @@ def test_png_exr_output_match_reference_writers(written, kind, spp, rdepth, scen
         assert np.array_equal(ea[c], eb[c], equal_nan=True)
     frame = xh.read_frame(d / "o.bin")
     assert np.array_equal(ea["R"], frame[..., 0], equal_nan=True)
+
+
+@pytest.mark.parametrize("cam, w, h", [
+    (scenes.Camera((0.0, 3.0, -12.0), (0.0, 1.5, 0.0), (0.0, 1.0, 0.0), 50.0, flength=11.0, aperture=0.75), 48, 40),
+    (scenes.Camera((0.5, 2.0, 0.25), type=scenes.CAM_ERP, orientation=(0.25, -0.5, 0.125)), 96, 48),
+    (scenes.Camera((0.5, 2.0, 0.25), type=scenes.CAM_ODS, orientation=(0.0, 0.75, 0.0), ipd=0.125), 64, 64),
+    (scenes.Camera((0.5, 2.0, 0.25), type=scenes.CAM_CUBEMAP), 24, 144)], ids=["dof", "erp", "ods", "cubemap"])
+def test_cameras_and_aa_in_host_equal_c_abi(tmp_path, cam, w, h):
+    """Every camera type of a .scn and the context's aa level (grid
+    distribution) reach the GPU through the xtcore host unchanged."""
+    spec = scenes.spheres_scene(64, seed=1, name="hostcam", camera=cam)
+    scn = spec.write_scn(str(tmp_path))
+    for kind, spp, aa in ((xtgpu.DEPTH, 2, 2), (xtgpu.AO, 2, 3)):
+        got = render_host(scn, kind, w, h, spp, 1, tmp_path / "f.bin", "--aa", str(aa), "--ao-distance", "0.5")
+        sc = xtgpu.Scene(spec)
+        ref, _ = sc.render(kind, w, h, spp=spp, rdepth=1, ao_max_distance=0.5, seed=1, aa=aa)
+        sc.close()
+        assert np.array_equal(got, ref, equal_nan=True), NAMES[kind]
+
+
+def test_aa_zero_writes_no_pixel(written):
+    """aa = 0: antialiasing::produce gives the tiles no samples (aa.cc:9), so
+    the frame keeps what tile->init wrote, as with the CPU integrators."""
+    specs, d = written
+    spec, scn = specs[0]
+    gpu = render_host(scn, xtgpu.STENCIL, 32, 24, 1, 1, d / "g0.bin", "--aa", "0")
+    cpu = render_host(scn, xtgpu.STENCIL, 32, 24, 1, 1, d / "c0.bin", "--aa", "0", "--cpu")
+    assert np.array_equal(gpu, cpu)

@@ -48,6 +48,7 @@ def test_flattened_scene_equals_generator(make, tmp_path):
         assert np.array_equal(d["env_b"], np.float32(spec.env_b))
     cam = spec.camera
     assert np.array_equal(d["camera"], np.float32(list(cam.position) + list(cam.target) + list(cam.up) + [cam.fov]))
+    assert d["camera_type"] == scenes.CAM_PERSPECTIVE and d["camera_flength"] == 0.0
     for oi in range(len(spec.obj_kind)):
         t, row = d["materials"][d["obj_material"][oi]]
         m = spec.materials[spec.obj_material[oi]]
@@ -97,7 +98,6 @@ TEXTURE = "          type = texture\n          source = missing.png"
 
 
 @pytest.mark.parametrize("extra, geom, sampler, why", [
-    ("    flength = 2\n    aperture = 0.1\n", "sphere", COLOUR, "depth of field"),
     ("", "sphere", TEXTURE, "not a solid colour"),
 ])
 def test_unsupported_features_are_refused(tmp_path, extra, geom, sampler, why):
@@ -118,3 +118,28 @@ def test_point_geometry_is_a_zero_radius_sphere(tmp_path):
     d = xh.read_flat(tmp_path / "f.bin")
     assert d["obj_kind"].tolist() == [scenes.SPHERE]
     assert d["spheres"].tolist() == [[0.0, 0.0, 0.0, 0.0]]
+
+
+@pytest.mark.parametrize("cam", [
+    scenes.Camera((0.5, 3.0, -12.0), (0.0, 1.5, 0.0), (0.0, 1.0, 0.0), 50.0, flength=11.0, aperture=0.75),
+    scenes.Camera((0.25, 1.0, -0.5), type=scenes.CAM_ERP, orientation=(0.1, -0.4, 0.2)),
+    scenes.Camera((0.0, 1.0, 0.25), type=scenes.CAM_ODS, orientation=(0.0, 0.3, 0.0), ipd=0.125),
+    scenes.Camera((1.0, 0.5, -2.0), type=scenes.CAM_CUBEMAP),
+], ids=["thin-lens-dof", "erp", "ods", "cubemap"])
+def test_every_camera_type_is_flattened(cam, tmp_path):
+    """Thin-lens (with depth of field), ERP, ODS and cubemap cameras of a .scn
+    reach the C ABI's camera with the loader's values (parseutil.cc camera
+    fields: position, orientation, ipd, flength, aperture)."""
+    spec = scenes.spheres_scene(16, seed=4, name="cams")
+    spec.camera = cam
+    d = flatten(spec, tmp_path)
+    assert d["camera_type"] == cam.type
+    assert np.array_equal(d["camera"][:3], np.float32(cam.position))
+    if cam.type == scenes.CAM_PERSPECTIVE:
+        assert np.array_equal(d["camera"][3:], np.float32(list(cam.target) + list(cam.up) + [cam.fov]))
+        assert d["camera_flength"] == np.float32(cam.flength)
+        assert d["camera_aperture"] == np.float32(cam.aperture)
+    if cam.type in (scenes.CAM_ERP, scenes.CAM_ODS):
+        assert np.array_equal(d["camera_orientation"], np.float32(cam.orientation))
+    if cam.type == scenes.CAM_ODS:
+        assert d["camera_ipd"] == np.float32(cam.ipd)

@@ -45,6 +45,9 @@ def read_flat(path):
         d["materials"].append((t, take(np.float32, 12)))
     d["env_a"], d["env_b"] = take(np.float32, 3), take(np.float32, 3)
     d["camera"] = take(np.float32, 10)
+    d["camera_type"] = int(take(np.int32, 1)[0])
+    d["camera_orientation"] = take(np.float32, 3)
+    d["camera_ipd"], d["camera_flength"], d["camera_aperture"] = (float(v) for v in take(np.float32, 3))
     assert off == len(b), "trailing bytes in the flattened scene"
     return d
 

@@ -70,7 +70,46 @@ DevCamera make_camera(const xtgpu_camera &c)
     k.rz[0] = rz.x; k.rz[1] = rz.y; k.rz[2] = rz.z;
     const double RADIAN = 0.017453292519943;   // lib/nmath/precision.h:111
     k.dz = 1.0 / std::tan(c.fov * RADIAN / 2.0);
+    k.type = c.type;
+    k.ipd = c.ipd;
+    k.flength = c.flength;
+    k.aperture = c.aperture;
+    // ERP and ODS turn their direction by Matrix4x4f::rotate(orientation)
+    // applied to the identity (lib/nmath/matrix.cc:414-427, 485-492):
+    // I *= (xrot * yrot * zrot), every product summed left to right.
+    const double ex = c.orientation[0], ey = c.orientation[1], ez = c.orientation[2];
+    const double xr[3][3] = {{1, 0, 0}, {0, std::cos(ex), -std::sin(ex)}, {0, std::sin(ex), std::cos(ex)}};
+    const double yr[3][3] = {{std::cos(ey), 0, std::sin(ey)}, {0, 1, 0}, {-std::sin(ey), 0, std::cos(ey)}};
+    const double zr[3][3] = {{std::cos(ez), -std::sin(ez), 0}, {std::sin(ez), std::cos(ez), 0}, {0, 0, 1}};
+    double xy[3][3], r3[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) xy[i][j] = xr[i][0] * yr[0][j] + xr[i][1] * yr[1][j] + xr[i][2] * yr[2][j];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) r3[i][j] = xy[i][0] * zr[0][j] + xy[i][1] * zr[1][j] + xy[i][2] * zr[2][j];
+    const double m4[4][4] = {{r3[0][0], r3[0][1], r3[0][2], 0}, {r3[1][0], r3[1][1], r3[1][2], 0},
+                             {r3[2][0], r3[2][1], r3[2][2], 0}, {0, 0, 0, 1}};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 4; ++j) {
+            const double e0 = i == 0, e1 = i == 1, e2 = i == 2;
+            k.rot[i][j] = e0 * m4[0][j] + e1 * m4[1][j] + e2 * m4[2][j] + 0.0 * m4[3][j];
+        }
     return k;
+}
+
+bool camera_valid(const xtgpu_camera &c)
+{
+    return c.type >= XTGPU_CAM_PERSPECTIVE && c.type <= XTGPU_CAM_CUBEMAP && std::isfinite(c.ipd) &&
+           std::isfinite(c.flength) && std::isfinite(c.aperture) && std::isfinite(c.orientation[0]) &&
+           std::isfinite(c.orientation[1]) && std::isfinite(c.orientation[2]);
+}
+
+// The frame a camera can render and the grid level: a cubemap is a vertical
+// strip of six square faces, so its height must split into them.
+bool view_valid(const DevCamera &c, int width, int height, int aa)
+{
+    (void)width;
+    if (aa < 0 || aa > MAX_AA) return false;
+    return c.type != XTGPU_CAM_CUBEMAP || (height >= 6 && height % 6 == 0);
 }
 
 const xtgpu_tuning &scene_tuning(const xtgpu_scene *sc) { return sc->tuned ? sc->tune : tuning(); }
@@ -183,6 +222,10 @@ xtgpu_status xtgpu_scene_create(const xtgpu_scene_desc *d, void *stream, xtgpu_s
         (d->n_objects && (!d->obj_kind || !d->obj_first || !d->obj_count || !d->obj_material)) ||
         (d->n_materials && !d->materials)) {
         set_error("xtgpu_scene_create: inconsistent sizes or NULL arrays");
+        return XTGPU_ERR_INVALID;
+    }
+    if (!camera_valid(d->camera)) {
+        set_error("xtgpu_scene_create: bad camera type or non-finite camera parameters");
         return XTGPU_ERR_INVALID;
     }
     const int64_t nprim = (int64_t)d->n_tris + d->n_spheres + d->n_planes;
@@ -512,6 +555,10 @@ xtgpu_status xtg::render_impl(xtgpu_scene *sc, const xtgpu_render_params *p, flo
         set_error("xtgpu_render: bad parameters");
         return XTGPU_ERR_INVALID;
     }
+    if (!view_valid(sc->dev.cam, p->width, p->height, p->aa)) {
+        set_error("xtgpu_render: aa outside 0..16, or a cubemap height that is not six square faces");
+        return XTGPU_ERR_INVALID;
+    }
     int x0 = p->x0, y0 = p->y0, x1 = p->x1, y1 = p->y1;
     if (x1 == 0 && y1 == 0) {
         x0 = y0 = 0;
@@ -525,7 +572,8 @@ xtgpu_status xtg::render_impl(xtgpu_scene *sc, const xtgpu_render_params *p, flo
     XTG_TRY(check_format(sc, p->node_format));
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t npix = (int64_t)(x1 - x0) * (y1 - y0);
-    const int64_t paths = npix * p->spp;
+    const int64_t aa = p->aa > 1 ? p->aa : 1;
+    const int64_t paths = npix * aa * aa * p->spp;
     const int64_t cap = std::min<int64_t>(paths, T.wave_paths);
     std::lock_guard<std::mutex> lock(g_runner_mu);
     WaveRunner *R = nullptr;
@@ -545,7 +593,7 @@ xtgpu_status xtg::render_impl(xtgpu_scene *sc, const xtgpu_render_params *p, flo
     J.integrator = p->integrator;
     J.width = p->width;
     J.height = p->height;
-    J.spp = p->spp;
+    set_samples(J, p->spp, p->aa);
     J.rdepth = p->rdepth;
     J.ao_maxd = p->ao_max_distance;
     J.seed = p->seed;

@@ -14,7 +14,7 @@
 //
 // Limits and sharing:
 //   * at most XTGPU_NOALLOC_MAX_PATHS (65536) paths per call, i.e. rectangle
-//     pixels x spp (one 32x32 tile at 64 spp); larger requests are rejected
+//     pixels x aa^2 x spp (one 32x32 tile at 64 spp); larger requests are rejected
 //     with XTGPU_ERR_LIMIT;
 //   * the array (NOALLOC_BYTES, about 11.5 MB) is held by every GPU that loads
 //     the library, until the process exits;
@@ -94,6 +94,10 @@ extern "C" xtgpu_status xtgpu_render_tile_noalloc(xtgpu_scene *sc, const xtgpu_r
         set_error("xtgpu_render_tile_noalloc: bad parameters");
         return XTGPU_ERR_INVALID;
     }
+    if (!view_valid(sc->dev.cam, p->width, p->height, p->aa)) {
+        set_error("xtgpu_render_tile_noalloc: aa outside 0..16, or a cubemap height that is not six square faces");
+        return XTGPU_ERR_INVALID;
+    }
     int x0 = p->x0, y0 = p->y0, x1 = p->x1, y1 = p->y1;
     if (x1 == 0 && y1 == 0) {
         x0 = y0 = 0;
@@ -105,9 +109,10 @@ extern "C" xtgpu_status xtgpu_render_tile_noalloc(xtgpu_scene *sc, const xtgpu_r
         return XTGPU_ERR_INVALID;
     }
     const int64_t npix = (int64_t)(x1 - x0) * (y1 - y0);
-    const int64_t paths = npix * p->spp;
+    const int64_t aa = p->aa > 1 ? p->aa : 1;
+    const int64_t paths = npix * aa * aa * p->spp;
     if (paths > NA_PATHS) {
-        set_error("xtgpu_render_tile_noalloc: rectangle pixels x spp exceeds the 65536-path scratch array; "
+        set_error("xtgpu_render_tile_noalloc: rectangle pixels x aa^2 x spp exceeds the 65536-path scratch array; "
                   "split the frame into smaller tiles");
         return XTGPU_ERR_LIMIT;
     }
@@ -145,7 +150,7 @@ extern "C" xtgpu_status xtgpu_render_tile_noalloc(xtgpu_scene *sc, const xtgpu_r
     J.integrator = p->integrator;
     J.width = p->width;
     J.height = p->height;
-    J.spp = p->spp;
+    set_samples(J, p->spp, p->aa);
     J.rdepth = p->rdepth;
     J.ao_maxd = p->ao_max_distance;
     J.seed = p->seed;

@@ -59,25 +59,119 @@ __device__ __forceinline__ float3 cmul(float3 a, float3 b) { return make_float3(
 __device__ __forceinline__ float3 cmuls(float3 a, float s) { return make_float3(c0(a.x * s), c0(a.y * s), c0(a.z * s)); }
 
 // Perspective::get_primary_ray (camera/perspective.cc:38-98), FP64, no contraction.
-__device__ __forceinline__ void camera_ray(const DevCamera &c, float x, float y, float w, float h, float3 &o,
-                                           float3 &d)
+// Camera rays in FP64, each operation rounded on its own (no contraction), as
+// the reference computes them: Perspective::get_primary_ray (perspective.cc:
+// 38-98, with the thin-lens draws of :73-95 when flength > 0), ERP (erp.cc:
+// 13-31), ODS (ods.cc:17-40) and Cubemap (cubemap.cc:21-69).  `key` and `ctr`
+// are the sample's random stream; the lens draws are its first two values.
+__device__ __forceinline__ double dlen3(const double t[3])
 {
-    double aspect = __ddiv_rn((double)w, (double)h);
-    double dx = __dsub_rn(__ddiv_rn(__dmul_rn(2.0, (double)x), (double)w), 1.0);
-    double dy = __ddiv_rn(__dsub_rn(__ddiv_rn(__dmul_rn(2.0, (double)y), (double)h), 1.0), aspect);
-    double dz = c.dz;
-    double t[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-        t[k] = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(c.rx[k], dx), __dmul_rn(c.ry[k], dy)), __dmul_rn(c.rz[k], dz)),
-                         0.0);
-    double len = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(t[0], t[0]), __dmul_rn(t[1], t[1])), __dmul_rn(t[2], t[2])));
+    return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(t[0], t[0]), __dmul_rn(t[1], t[1])), __dmul_rn(t[2], t[2])));
+}
+__device__ __forceinline__ void dnormalize3(double t[3])
+{
+    const double len = dlen3(t);
     if (len != 0.0) {
         t[0] = __ddiv_rn(t[0], len);
         t[1] = __ddiv_rn(t[1], len);
         t[2] = __ddiv_rn(t[2], len);
     }
-    o = make_float3((float)c.pos[0], (float)c.pos[1], (float)c.pos[2]);
+}
+// (a*x + b*y + c*z) + w, left to right
+__device__ __forceinline__ double dsum4(double a, double x, double b, double y, double c, double z, double w)
+{
+    return __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(a, x), __dmul_rn(b, y)), __dmul_rn(c, z)), w);
+}
+
+__device__ void camera_ray(const DevCamera &c, float x, float y, float w, float h, uint64_t key, uint32_t &ctr,
+                           float3 &o, float3 &d)
+{
+    double to[3] = {c.pos[0], c.pos[1], c.pos[2]}, t[3];
+    if (c.type == XTGPU_CAM_ERP || c.type == XTGPU_CAM_ODS) {
+        double dir[3];
+        if (c.type == XTGPU_CAM_ERP) {
+            const float phi = (float)__dmul_rn(__dmul_rn((double)__fdiv_rn(x, w), 3.14159265358979323846), 2.0);
+            const float theta = (float)__dmul_rn((double)__fdiv_rn(y, h), 3.14159265358979323846);
+            const double st = sin((double)theta);
+            dir[0] = __dmul_rn(st, cos((double)phi));
+            dir[1] = cos((double)theta);
+            dir[2] = __dmul_rn(st, sin((double)phi));
+        } else {
+            const float hh = __fmul_rn(h, .5f);
+            const float scale = __fmul_rn(__fmul_rn(c.ipd, .5f), (y < hh) ? -1.f : 1.f);
+            if (y > hh) y = __fsub_rn(y, hh);
+            const float theta = (float)__dmul_rn((double)__fmul_rn(__fdiv_rn(x, w), 2.f), 3.14159265358979323846);
+            const float phi = (float)__dsub_rn(__dmul_rn(3.14159265358979323846, 0.5),
+                                               __dmul_rn((double)__fdiv_rn(y, hh), 3.14159265358979323846));
+            const double ct = cos((double)theta), st = sin((double)theta), cp = cos((double)phi);
+            to[0] = __dadd_rn(__dmul_rn(ct, (double)scale), c.pos[0]);
+            to[1] = __dadd_rn(__dmul_rn(0.0, (double)scale), c.pos[1]);
+            to[2] = __dadd_rn(__dmul_rn(st, (double)scale), c.pos[2]);
+            dir[0] = __dmul_rn(st, cp);
+            dir[1] = sin((double)phi);
+            dir[2] = __dmul_rn(-ct, cp);
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) t[k] = dsum4(c.rot[k][0], dir[0], c.rot[k][1], dir[1], c.rot[k][2], dir[2], c.rot[k][3]);
+    } else if (c.type == XTGPU_CAM_CUBEMAP) {
+        const unsigned long long face_size = (unsigned long long)h / 6ull;
+        const unsigned long long face = face_size ? (unsigned long long)y / face_size : 0ull;
+        double cd[3] = {0, 0, 0}, up[3] = {0, 0, 0};
+        switch (face) {
+        case 0: cd[0] = 1; up[1] = 1; break;
+        case 1: cd[0] = -1; up[1] = 1; break;
+        case 2: cd[1] = 1; up[2] = -1; break;
+        case 3: cd[1] = -1; up[2] = 1; break;
+        case 4: cd[2] = 1; up[1] = 1; break;
+        case 5: cd[2] = -1; up[1] = 1; break;
+        }
+        y = __fsub_rn(y, (float)(face * face_size));
+        double v[3] = {__dsub_rn(__ddiv_rn(__dmul_rn(2.0, (double)x), (double)w), 1.0),
+                       __dsub_rn(__ddiv_rn(__dmul_rn(2.0, (double)y), (double)face_size), 1.0), 1.0};
+        dnormalize3(v);
+        double rx[3] = {__dsub_rn(__dmul_rn(up[1], cd[2]), __dmul_rn(up[2], cd[1])),
+                        __dsub_rn(__dmul_rn(up[2], cd[0]), __dmul_rn(up[0], cd[2])),
+                        __dsub_rn(__dmul_rn(up[0], cd[1]), __dmul_rn(up[1], cd[0]))};
+        dnormalize3(rx);
+        double ry[3] = {__dsub_rn(__dmul_rn(rx[1], cd[2]), __dmul_rn(rx[2], cd[1])),
+                        __dsub_rn(__dmul_rn(rx[2], cd[0]), __dmul_rn(rx[0], cd[2])),
+                        __dsub_rn(__dmul_rn(rx[0], cd[1]), __dmul_rn(rx[1], cd[0]))};
+        dnormalize3(ry);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) t[k] = dsum4(rx[k], v[0], ry[k], v[1], cd[k], v[2], 0.0);
+    } else {
+        const double aspect = __ddiv_rn((double)w, (double)h);
+        double dc[3] = {__dsub_rn(__ddiv_rn(__dmul_rn(2.0, (double)x), (double)w), 1.0),
+                        __ddiv_rn(__dsub_rn(__ddiv_rn(__dmul_rn(2.0, (double)y), (double)h), 1.0), aspect), c.dz};
+        if (c.flength > 0.f) {
+            // the lens point: the camera-space direction moved within half the
+            // aperture (two prng_c draws, x then y); the ray aims at the point
+            // of the focal plane the undisturbed direction meets
+            const double half = (double)__fdiv_rn(c.aperture, 2.f);
+            double lo[3] = {dc[0], dc[1], dc[2]};
+            const double u0 = (double)uniform(key, ctr), u1 = (double)uniform(key, ctr);
+            lo[0] = __dadd_rn(lo[0], __dadd_rn(__dmul_rn(u0, __dsub_rn(half, -half)), -half));
+            lo[1] = __dadd_rn(lo[1], __dadd_rn(__dmul_rn(u1, __dsub_rn(half, -half)), -half));
+            const double len = dlen3(dc);
+            double fd[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const double nk = len != 0.0 ? __ddiv_rn(dc[k], len) : dc[k];
+                fd[k] = __dsub_rn(__dadd_rn(dc[k], __dmul_rn(nk, (double)c.flength)), lo[k]);
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                t[k] = dsum4(c.rx[k], fd[0], c.ry[k], fd[1], c.rz[k], fd[2], 0.0);
+                to[k] = __dadd_rn(dsum4(c.rx[k], lo[0], c.ry[k], lo[1], c.rz[k], lo[2], 0.0), c.pos[k]);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) t[k] = dsum4(c.rx[k], dc[0], c.ry[k], dc[1], c.rz[k], dc[2], 0.0);
+        }
+        dnormalize3(t);
+    }
+    if (c.type == XTGPU_CAM_CUBEMAP) dnormalize3(t);
+    o = make_float3((float)to[0], (float)to[1], (float)to[2]);
     d = make_float3((float)t[0], (float)t[1], (float)t[2]);
 }
 
@@ -289,12 +383,25 @@ __global__ void k_camera(const DevJob *__restrict__ jobs, const DevScene *__rest
         int64_t s = p / npix, pix = p - s * npix;
         int x, y;
         pixel_of(J, pix, x, y);
+        // grid position of the sample (aa.cc:51-77): aa^2 positions per
+        // pixel, rows in order, each taken spp1 times
+        float cx = (float)x + 0.5f, cy = (float)y + 0.5f;
+        if (J.aa > 1) {
+            const int gi = (int)(s / J.spp1);
+            const float sub = __fdiv_rn(1.f, (float)J.aa), off = __fmul_rn(sub, 0.5f);
+            cx = (float)__dadd_rn(__dadd_rn((double)x, __dmul_rn((double)(gi % J.aa), (double)sub)), (double)off);
+            cy = (float)__dadd_rn(__dadd_rn((double)y, __dmul_rn((double)(gi / J.aa), (double)sub)), (double)off);
+        }
+        const uint64_t key = path_key(J.seed, (uint64_t)s * (uint64_t)J.width * (uint64_t)J.height +
+                                                  (uint64_t)y * (uint64_t)J.width + (uint64_t)x);
+        uint32_t ctr = 0;
         float3 o, d;
-        camera_ray(scenes[J.scene].cam, (float)x + 0.5f, (float)y + 0.5f, (float)J.width, (float)J.height, o, d);
+        camera_ray(scenes[J.scene].cam, cx, cy, (float)J.width, (float)J.height, key, ctr, o, d);
         q.org[0][i] = make_float4(o.x, o.y, o.z, 0.f);
         q.dir[0][i] = make_float4(d.x, d.y, d.z, INFINITY);
         q.meta[0][i] = make_uint2((uint32_t)i, (uint32_t)jn);
-        q.P[0][i] = make_float4(1.f, 1.f, 1.f, __uint_as_float(0u));
+        // the integrators draw from the stream after the lens draws
+        q.P[0][i] = make_float4(1.f, 1.f, 1.f, __uint_as_float(ctr));
         q.I[0][i] = make_float4(1.f, 1.f, 1.f, __int_as_float(J.bounces));
         q.contrib[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
@@ -862,8 +969,7 @@ __global__ void k_accumulate(const DevJob *__restrict__ jobs, const int32_t *__r
         pixel_of(J, pix, fx, fy);
         const int64_t fpix = (int64_t)(fy - J.y0) * J.rw + (fx - J.x0);
         float4 c = J.frame[fpix];
-        double w = 1.f;
-        w *= 1.0 / (double)J.spp;
+        const double w = J.wt;
         for (int64_t s = s_lo; s <= s_hi; ++s) {
             float4 v = contrib[J.offset + (s * npix + pix - a)];
             switch (J.integrator) {

@@ -150,7 +150,7 @@ static xtgpu_status launch_wave(xtgpu_service *v, WaveSlot &W, cudaEvent_t prev_
         dj.integrator = J.d.integrator;
         dj.width = J.d.width;
         dj.height = J.d.height;
-        dj.spp = J.d.spp;
+        set_samples(dj, J.d.spp, J.d.aa);
         dj.rdepth = J.d.rdepth;
         dj.ao_maxd = J.d.ao_max_distance;
         dj.seed = J.d.seed;
@@ -401,7 +401,12 @@ xtgpu_status xtgpu_service_submit(xtgpu_service *v, const xtgpu_job_desc *d, dou
         set_error("xtgpu_service_submit: bad job");
         return XTGPU_ERR_INVALID;
     }
-    int64_t paths = (int64_t)d->width * d->height * d->spp;
+    if (!view_valid(v->scenes[d->scene]->dev.cam, d->width, d->height, d->aa)) {
+        set_error("xtgpu_service_submit: aa outside 0..16, or a cubemap height that is not six square faces");
+        return XTGPU_ERR_INVALID;
+    }
+    const int64_t aa = d->aa > 1 ? d->aa : 1;
+    int64_t paths = (int64_t)d->width * d->height * aa * aa * d->spp;
     if (paths <= 0 || paths > (1ll << 40)) {
         set_error("xtgpu_service_submit: job too large");
         return XTGPU_ERR_INVALID;

@@ -21,7 +21,9 @@ namespace xtg {
 
 // One job's share of a wave.
 struct DevJob {
-    int32_t integrator, width, height, spp, rdepth;
+    int32_t integrator, width, height;
+    int32_t spp;                     // samples per pixel: aa^2 grid positions x spp1
+    int32_t rdepth;
     float ao_maxd;
     uint64_t seed;
     int32_t x0, y0, rw, rh;          // rectangle rendered
@@ -32,7 +34,21 @@ struct DevJob {
     int64_t first;                   // first path id of the job in this wave
     int64_t count;                   // paths of the job in this wave
     int64_t offset;                  // wave-local index of the job's first path
+    int32_t aa;                      // grid anti-aliasing level (1 = pixel centre)
+    int32_t spp1;                    // samples per grid position
+    double wt;                       // weight of one sample: 1/(aa^2) as a float, times 1/spp1
 };
+
+// Fills the sample fields of a job from params_t's samples and aa (aa.cc:7-32,
+// 51-77): aa^2 positions of weight 1.f/(aa*aa) each taken spp times at 1/spp.
+inline void set_samples(DevJob &j, int spp, int aa)
+{
+    const int L = aa > 1 ? aa : 1;
+    j.aa = L;
+    j.spp1 = spp;
+    j.spp = L * L * spp;
+    j.wt = (L == 1 ? 1.0 : (double)(1.f / (float)(L * L))) * (1.0 / (double)spp);
+}
 
 struct WaveQueues {
     float4 *org[2], *dir[2];         // (org, tmin), (dir, tmax)

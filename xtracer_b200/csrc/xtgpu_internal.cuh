@@ -44,10 +44,16 @@ struct DevMaterial {
 // Camera basis precomputed on the host in FP64 exactly as
 // Perspective::calculate_transform (camera/perspective.cc:26-36).
 struct DevCamera {
+    int type;             // XTGPU_CAM_*
     double pos[3];
     double rx[3], ry[3], rz[3];
     double dz;            // 1 / tan(fov * RADIAN / 2)
+    double rot[3][4];     // ERP, ODS: Matrix4x4f::rotate(orientation) of an identity
+    float ipd;            // ODS
+    float flength, aperture;   // perspective depth of field (flength > 0)
 };
+// grid anti-aliasing levels accepted (aa^2 rays per sample)
+constexpr int MAX_AA = 16;
 
 // Everything a kernel needs to intersect and shade one scene.
 struct DevScene {
@@ -139,6 +145,12 @@ inline bool format_built(const xtgpu_scene *sc, int f)
 }
 // traversal stack entries (32 or 64) for this scene's tree in format f
 int stack_for_scene(const xtgpu_scene *sc, int f, int requested);
+
+// cameras: the device form of a camera, whether a camera description is
+// acceptable, and whether a frame size and grid level suit a camera
+DevCamera make_camera(const xtgpu_camera &c);
+bool camera_valid(const xtgpu_camera &c);
+bool view_valid(const DevCamera &c, int width, int height, int aa);
 
 // the tuning a scene renders with: its own if autotuned, else the process-wide one
 const xtgpu_tuning &scene_tuning(const xtgpu_scene *sc);

@@ -12,6 +12,9 @@
 #include <xtcore/sampler_col.h>
 #include <xtcore/sampler_gradient.h>
 #include <xtcore/camera/perspective.h>
+#include <xtcore/camera/erp.h>
+#include <xtcore/camera/ods.h>
+#include <xtcore/camera/cubemap.h>
 #include <xtcore/math/sphere.h>
 #include <xtcore/math/plane.h>
 #include <xtcore/math/triangle.h>
@@ -237,28 +240,44 @@ xtgpu_status flatten(xtcore::Scene &scene, HASH_UINT64 camera, FlatScene &F, std
         }
     }
 
-    // camera (Perspective::get_primary_ray, camera/perspective.cc:38-98)
+    // camera: Perspective (with depth of field when flength > 0,
+    // camera/perspective.cc:38-98), ERP (erp.cc:13-31), ODS (ods.cc:17-40) or
+    // Cubemap (cubemap.cc:21-69)
     xtcore::asset::ICamera *cam = scene.get_camera(camera);
     if (!cam) return fail("no camera");
-    xtcore::camera::Perspective *pc = dynamic_cast<xtcore::camera::Perspective *>(cam);
-    if (!pc) return fail(std::string("unsupported camera type ") + cam->get_type());
-    if (pc->flength > 0) return fail("depth of field (flength > 0) is not supported");
     auto set3 = [](float *o, const nmath::Vector3f &v) {
         o[0] = (float)v.x;
         o[1] = (float)v.y;
         o[2] = (float)v.z;
     };
-    set3(d.camera.position, pc->position);
-    set3(d.camera.target, pc->target);
-    set3(d.camera.up, pc->up);
-    d.camera.fov = pc->fov;
+    set3(d.camera.position, cam->position);
+    if (xtcore::camera::Perspective *pc = dynamic_cast<xtcore::camera::Perspective *>(cam)) {
+        d.camera.type = XTGPU_CAM_PERSPECTIVE;
+        set3(d.camera.target, pc->target);
+        set3(d.camera.up, pc->up);
+        d.camera.fov = pc->fov;
+        d.camera.flength = pc->flength;
+        d.camera.aperture = pc->aperture;
+    } else if (xtcore::camera::ERP *ec = dynamic_cast<xtcore::camera::ERP *>(cam)) {
+        d.camera.type = XTGPU_CAM_ERP;
+        set3(d.camera.orientation, ec->orientation);
+    } else if (xtcore::camera::ODS *oc = dynamic_cast<xtcore::camera::ODS *>(cam)) {
+        d.camera.type = XTGPU_CAM_ODS;
+        set3(d.camera.orientation, oc->orientation);
+        d.camera.ipd = oc->ipd;
+    } else if (dynamic_cast<xtcore::camera::Cubemap *>(cam)) {
+        d.camera.type = XTGPU_CAM_CUBEMAP;
+    } else {
+        return fail(std::string("unsupported camera type ") + cam->get_type());
+    }
     return XTGPU_OK;
 }
 
 // ---------------------------------------------------------------------------
 Integrator::Integrator(int kind, int node_format)
     : ao_max_distance(100.f), seed(1), m_kind(kind), m_format(node_format), m_scene(0), m_uploaded(0),
-      m_x0(0), m_y0(0), m_w(0), m_h(0), m_served(0), m_ready(false), m_status(XTGPU_OK), m_rays(0)
+      m_x0(0), m_y0(0), m_w(0), m_h(0), m_served(0), m_ready(false), m_empty(false), m_status(XTGPU_OK),
+      m_rays(0)
 {}
 
 Integrator::~Integrator()
@@ -275,10 +294,14 @@ void Integrator::invalidate_scene()
 xtgpu_status Integrator::render_frame()
 {
     xtcore::render::params_t &p = ctx->params;
-    if (p.aa != 1 || p.sample_distribution != xtcore::antialiasing::SAMPLE_DISTRIBUTION_GRID) {
-        m_error = "only aa = 1 with the grid sample distribution is supported";
+    if (p.aa > 1 && p.sample_distribution != xtcore::antialiasing::SAMPLE_DISTRIBUTION_GRID) {
+        m_error = "aa > 1 is supported with the grid sample distribution only";
         return XTGPU_ERR_INVALID;
     }
+    // aa = 0 or samples = 0: antialiasing::produce gives the tiles no samples
+    // (aa.cc:9, 67), so the CPU integrators write no pixel
+    m_empty = p.aa == 0 || p.samples == 0;
+    if (m_empty) return XTGPU_OK;
     if (!m_scene || m_uploaded != &ctx->scene) {
         FlatScene F;
         xtgpu_status st = flatten(ctx->scene, p.camera, F, m_error);
@@ -322,6 +345,7 @@ xtgpu_status Integrator::render_frame()
     rp.y0 = (int32_t)y0;
     rp.x1 = (int32_t)x1;
     rp.y1 = (int32_t)y1;
+    rp.aa = (int32_t)p.aa;
     m_x0 = x0;
     m_y0 = y0;
     m_w = x1 - x0;
@@ -351,7 +375,7 @@ void Integrator::render_tile(xtcore::render::tile_t *tile)
         xtcore::antialiasing::sample_rgba_t s;
         tile->samples.pop(s);
     }
-    if (m_status == XTGPU_OK) {
+    if (m_status == XTGPU_OK && !m_empty) {
         for (size_t y = tile->y0(); y < tile->y1(); ++y)
             for (size_t x = tile->x0(); x < tile->x1(); ++x) {
                 const float *c = &m_frame[4 * ((y - m_y0) * m_w + (x - m_x0))];

@@ -14,12 +14,14 @@
 // Scene::intersection visits them, scene.cc:191-216) and uploaded once; call
 // invalidate_scene() after changing it.
 //
-// Supported: perspective cameras without depth of field, spheres (and points,
-// which the loader makes spheres of radius 0), planes, triangles, meshes,
-// solid-colour material samplers, no / solid-colour / gradient environment,
-// aa = 1 with grid sample distribution (the context defaults).  Anything else
-// makes the frame fail: status() and error() say why, the tiles stay as
-// tile->init() left them, and a warning goes to xtcore's log.
+// Supported: perspective (with depth of field), ERP, ODS and cubemap cameras
+// (a cubemap's height a multiple of 6), spheres (and points, which the loader
+// makes spheres of radius 0), planes, triangles, meshes, solid-colour material
+// samplers, no / solid-colour / gradient environment, any aa with the grid
+// sample distribution (aa <= 1 with the random one).  Anything else makes the
+// frame fail: status() and error() say why, the tiles stay as tile->init()
+// left them, and a warning goes to xtcore's log.  The depth-of-field lens
+// draws come from the GPU's sample streams, not from the C library's rand().
 #ifndef XTGPU_XTCORE_GPU_INTEGRATOR_H
 #define XTGPU_XTCORE_GPU_INTEGRATOR_H
 
@@ -82,6 +84,7 @@ class Integrator : public xtcore::render::IIntegrator
     size_t m_x0, m_y0, m_w, m_h;
     size_t m_served;                   // tiles served from the current frame
     bool m_ready;
+    bool m_empty;                      // the context gives the tiles no samples
     xtgpu_status m_status;
     std::string m_error;
     uint64_t m_rays;

@@ -12,6 +12,7 @@
 //       --ao-distance D  AO occlusion distance (GPU), default 100
 //       --threads N    OpenMP threads of the tile loop, default all
 //       --tile N       tile size, default 32 (context.cc:5)
+//       --aa N         anti-aliasing level (grid distribution), default 1
 //       --png P        the assembled frame as PNG through the GPU quantiser
 //       --exr P        the assembled frame as OpenEXR (this library's writer)
 //       --ref-png P, --ref-exr P   the same frame through XTracer's own writers
@@ -69,7 +70,8 @@ void put(FILE *f, const T *p, size_t n)
 // has_normals, obj_uv_scale [2 n_objects], tri_uvs [6n] when has_uvs;
 // per material int32 type + float32 diffuse[3] specular[3] emissive[3]
 // reflectance exponent ior; float32 env_a[3] env_b[3]; float32 camera
-// position[3] target[3] up[3] fov.
+// position[3] target[3] up[3] fov; int32 camera type; float32 orientation[3]
+// ipd flength aperture.
 int write_flat(const xtcore::integrator::gpu::FlatScene &F, const char *out)
 {
     const xtgpu_scene_desc &d = F.desc;
@@ -103,6 +105,10 @@ int write_flat(const xtcore::integrator::gpu::FlatScene &F, const char *out)
     put(f, d.camera.target, 3);
     put(f, d.camera.up, 3);
     put(f, &d.camera.fov, 1);
+    put(f, &d.camera.type, 1);
+    put(f, d.camera.orientation, 3);
+    float lens[3] = {d.camera.ipd, d.camera.flength, d.camera.aperture};
+    put(f, lens, 3);
     fclose(f);
     return 0;
 }
@@ -133,7 +139,7 @@ int mode_render(int argc, char **argv)
     bool cpu = false, q8 = false, w8 = false;
     unsigned long long seed = 1;
     float aod = 100.f;
-    size_t threads = 0, tile = 32;
+    size_t threads = 0, tile = 32, aa = 1;
     std::string png, exr, ref_png, ref_exr;
     for (int i = 9; i < argc; ++i) {
         std::string a = argv[i];
@@ -144,6 +150,7 @@ int mode_render(int argc, char **argv)
         else if (a == "--ao-distance" && i + 1 < argc) aod = (float)atof(argv[++i]);
         else if (a == "--threads" && i + 1 < argc) threads = strtoul(argv[++i], 0, 10);
         else if (a == "--tile" && i + 1 < argc) tile = strtoul(argv[++i], 0, 10);
+        else if (a == "--aa" && i + 1 < argc) aa = strtoul(argv[++i], 0, 10);
         else if (a == "--png" && i + 1 < argc) png = argv[++i];
         else if (a == "--exr" && i + 1 < argc) exr = argv[++i];
         else if (a == "--ref-png" && i + 1 < argc) ref_png = argv[++i];
@@ -164,6 +171,7 @@ int mode_render(int argc, char **argv)
     ctx.params.rdepth = rdepth;
     ctx.params.threads = threads;
     ctx.params.tile_size = tile;
+    ctx.params.aa = aa;
     ctx.init();   // segments the frame into tiles (context.cc)
 
     xtcore::render::IIntegrator *ig = 0;

@@ -44,7 +44,9 @@ class Material(C.Structure):
 
 
 class CameraDesc(C.Structure):
-    _fields_ = [("position", C.c_float * 3), ("target", C.c_float * 3), ("up", C.c_float * 3), ("fov", C.c_float)]
+    _fields_ = [("position", C.c_float * 3), ("target", C.c_float * 3), ("up", C.c_float * 3), ("fov", C.c_float),
+                ("type", C.c_int32), ("orientation", C.c_float * 3), ("ipd", C.c_float), ("flength", C.c_float),
+                ("aperture", C.c_float)]
 
 
 class SceneDesc(C.Structure):
@@ -79,7 +81,7 @@ class RenderParams(C.Structure):
     _fields_ = [("integrator", C.c_int32), ("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32),
                 ("rdepth", C.c_int32), ("ao_max_distance", C.c_float), ("seed", C.c_uint64),
                 ("node_format", C.c_int32), ("x0", C.c_int32), ("y0", C.c_int32), ("x1", C.c_int32),
-                ("y1", C.c_int32)]
+                ("y1", C.c_int32), ("aa", C.c_int32)]
 
 
 class ServiceOpts(C.Structure):
@@ -118,7 +120,8 @@ def set_tuning(**kw) -> None:
 
 class JobDesc(C.Structure):
     _fields_ = [("scene", C.c_int32), ("integrator", C.c_int32), ("width", C.c_int32), ("height", C.c_int32),
-                ("spp", C.c_int32), ("rdepth", C.c_int32), ("ao_max_distance", C.c_float), ("seed", C.c_uint64)]
+                ("spp", C.c_int32), ("rdepth", C.c_int32), ("ao_max_distance", C.c_float), ("seed", C.c_uint64),
+                ("aa", C.c_int32)]
 
 
 class JobStatus(C.Structure):
@@ -244,6 +247,11 @@ class Scene:
         d.camera.target[:] = list(cam.target)
         d.camera.up[:] = list(cam.up)
         d.camera.fov = cam.fov
+        d.camera.type = getattr(cam, "type", 0)
+        d.camera.orientation[:] = list(getattr(cam, "orientation", (0.0, 0.0, 0.0)))
+        d.camera.ipd = getattr(cam, "ipd", 0.0)
+        d.camera.flength = getattr(cam, "flength", 0.0)
+        d.camera.aperture = getattr(cam, "aperture", 0.0)
         if getattr(spec, "obj_uv_scale", None) is not None:
             d.obj_uv_scale = arr(spec.obj_uv_scale.reshape(-1), np.float32)
         if getattr(spec, "tri_uvs", None) is not None:
@@ -320,9 +328,11 @@ class Scene:
         return hits
 
     def render(self, integrator: int, width: int, height: int, spp: int = 1, rdepth: int = 4,
-               ao_max_distance: float = 100.0, seed: int = 1, node_format: int = NODES_FP32, rect=None):
+               ao_max_distance: float = 100.0, seed: int = 1, node_format: int = NODES_FP32, rect=None,
+               aa: int = 1):
         x0, y0, x1, y1 = rect if rect is not None else (0, 0, 0, 0)
-        p = RenderParams(integrator, width, height, spp, rdepth, ao_max_distance, seed, node_format, x0, y0, x1, y1)
+        p = RenderParams(integrator, width, height, spp, rdepth, ao_max_distance, seed, node_format, x0, y0, x1, y1,
+                         aa)
         rw, rh = (x1 - x0, y1 - y0) if rect is not None else (width, height)
         out = np.zeros((rh, rw, 4), np.float32)
         rays = C.c_uint64()
@@ -331,12 +341,14 @@ class Scene:
 
 
 class Params:
-    """params_t (context.h:18-34) for the GPU integrators; aa is fixed at 1."""
+    """params_t (context.h:18-34) for the GPU integrators (grid sample
+    distribution)."""
 
     def __init__(self, width=500, height=500, samples=1, rdepth=100, seed=1, node_format=NODES_FP32,
-                 ao_max_distance=100.0):
+                 ao_max_distance=100.0, aa=1):
         self.width, self.height, self.samples, self.rdepth = width, height, samples, rdepth
         self.seed, self.node_format, self.ao_max_distance = seed, node_format, ao_max_distance
+        self.aa = aa
 
 
 class Context:
@@ -363,7 +375,7 @@ class _Integrator:
             return None
         p = self.ctx.params
         img, self.rays = self.ctx.scene.render(self.kind, p.width, p.height, p.samples, p.rdepth,
-                                               p.ao_max_distance, p.seed, p.node_format)
+                                               p.ao_max_distance, p.seed, p.node_format, aa=p.aa)
         return img
 
 
