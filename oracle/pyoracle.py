@@ -27,6 +27,37 @@ class XoMaterial(C.Structure):
                 ("ior", C.c_float)]
 
 
+class XoTexture(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("filtering", C.c_int32), ("pad", C.c_int32),
+                ("offset", C.c_int64)]
+
+
+class XoSampler(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("texture", C.c_int32), ("a", C.c_float * 3), ("b", C.c_float * 3)]
+
+
+def texture_structs(textures, struct=None):
+    """(K, 4) rows (width, height, filtering, first texel) as a ctypes array."""
+    struct = struct or XoTexture
+    out = (struct * max(1, len(textures)))()
+    for i, (w, h, f, off) in enumerate(np.asarray(textures).tolist()):
+        out[i].width, out[i].height, out[i].filtering, out[i].offset = int(w), int(h), int(f), int(off)
+    return out
+
+
+def sampler_structs(samp, struct=None):
+    """Per material three (kind, texture, a, b) tuples as a ctypes array."""
+    struct = struct or XoSampler
+    out = (struct * max(1, 3 * len(samp)))()
+    for i, row in enumerate(samp):
+        for ch, (kind, tex, a, b) in enumerate(row):
+            k = out[3 * i + ch]
+            k.kind, k.texture = int(kind), int(tex)
+            k.a[:] = [float(v) for v in a]
+            k.b[:] = [float(v) for v in b]
+    return out
+
+
 class XoSceneDesc(C.Structure):
     _fields_ = [("n_objects", C.c_int32), ("obj_kind", C.c_void_p), ("obj_first", C.c_void_p),
                 ("obj_count", C.c_void_p), ("obj_material", C.c_void_p),
@@ -38,7 +69,9 @@ class XoSceneDesc(C.Structure):
                 ("cam_pos", C.c_float * 3), ("cam_target", C.c_float * 3), ("cam_up", C.c_float * 3),
                 ("cam_fov", C.c_float), ("obj_uv_scale", C.c_void_p), ("tri_uvs", C.c_void_p),
                 ("cam_type", C.c_int32), ("cam_orientation", C.c_float * 3), ("cam_ipd", C.c_float),
-                ("cam_flength", C.c_float), ("cam_aperture", C.c_float)]
+                ("cam_flength", C.c_float), ("cam_aperture", C.c_float),
+                ("n_textures", C.c_int32), ("textures", C.c_void_p), ("texels", C.c_void_p),
+                ("mat_samplers", C.c_void_p), ("env_texture", C.c_int32)]
 
 
 class XoRenderParams(C.Structure):
@@ -75,6 +108,9 @@ def lib():
         L.xo_kat_lobe.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]
         L.xo_kat_material.argtypes = [C.POINTER(XoMaterial), C.c_void_p, C.c_int32] + [C.c_void_p] * 4
         L.xo_kat_gradient.argtypes = [C.c_void_p] * 4
+        L.xo_kat_texture.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_void_p]
+        L.xo_kat_erp.argtypes = [C.c_void_p] * 4
+        L.xo_kat_cubemap.argtypes = [C.c_void_p] * 4
         L.xo_kat_camera_dof.argtypes = [C.c_void_p, C.c_int32] + [C.c_void_p] * 3 + [C.c_float] * 7 + [C.c_void_p] * 2
         L.xo_kat_camera_erp.argtypes = [C.c_void_p] * 2 + [C.c_float] * 4 + [C.c_void_p] * 2
         L.xo_kat_camera_ods.argtypes = [C.c_void_p] * 2 + [C.c_float] * 5 + [C.c_void_p] * 2
@@ -144,6 +180,16 @@ class OracleScene:
         d.obj_uv_scale = _ptr(arr(uvs.reshape(-1), np.float32)) if uvs is not None else None
         tuv = getattr(spec, "tri_uvs", None)
         d.tri_uvs = _ptr(arr(tuv.reshape(-1), np.float32)) if tuv is not None else None
+        d.env_texture = -1
+        if hasattr(spec, "texture_tables"):
+            textures, texels, samp, env_tex = spec.texture_tables()
+            tstructs, sstructs = texture_structs(textures), sampler_structs(samp)
+            self._keep += [tstructs, sstructs]
+            d.n_textures = len(textures)
+            d.textures = C.cast(tstructs, C.c_void_p)
+            d.texels = _ptr(arr(texels.reshape(-1), np.float32))
+            d.mat_samplers = C.cast(sstructs, C.c_void_p) if samp else None
+            d.env_texture = env_tex
         self._desc = d
         h = C.c_void_p()
         if lib().xo_scene_create(C.byref(d), accel, C.byref(h)) != 0:

@@ -46,6 +46,9 @@
 #include <xtcore/camera/cubemap.h>
 #include <xtcore/sampler_col.h>
 #include <xtcore/sampler_gradient.h>
+#include <xtcore/sampler_tex.h>
+#include <xtcore/sampler_erp.h>
+#include <xtcore/sampler_cubemap.h>
 #include <xtcore/material/lambert.h>
 #include <xtcore/material/phong.h>
 #include <xtcore/material/blinnphong.h>
@@ -350,6 +353,11 @@ static std::vector<double> parse_nums(char *s)
 static void put(FILE *f, double x) { fprintf(f, " %a", x); }
 static void put3(FILE *f, const Vector3f &v) { put(f, v.x); put(f, v.y); put(f, v.z); }
 
+// samplers loaded by the tex_load / erp_load / cube_load lines
+static xtcore::sampler::Texture2D g_tex[16];
+static xtcore::sampler::ERP g_erp[4];
+static xtcore::sampler::Cubemap g_cube[4];
+
 static int mode_kat(int argc, char **argv)
 {
     if (argc < 4) return 2;
@@ -393,6 +401,8 @@ static int mode_kat(int argc, char **argv)
     while (fgets(line, sizeof(line), in)) {
         char kind[64];
         if (sscanf(line, "%63s", kind) != 1) continue;
+        char raw[8192];
+        memcpy(raw, line, sizeof(raw));
         std::vector<double> a = parse_nums(line + strlen(kind));
         fprintf(out, "%s", kind);
         if (!strcmp(kind, "rand")) {
@@ -531,6 +541,51 @@ static int mode_kat(int argc, char **argv)
             put3(out, res.ray.direction);
             put(out, res.intensity.r()); put(out, res.intensity.g()); put(out, res.intensity.b());
             delete m;
+        } else if (!strcmp(kind, "tex_load")) {
+            // tex_load slot filtering flip_x flip_y path: Texture2D as
+            // deserialize_texture sets it up (parseutil.cc:478-508)
+            int slot, filt, fx, fy;
+            char path[4096];
+            if (sscanf(raw + strlen(kind), "%d %d %d %d %4095s", &slot, &filt, &fx, &fy, path) != 5 || slot < 0 ||
+                slot >= 16) {
+                fprintf(out, " bad");
+            } else {
+                g_tex[slot] = xtcore::sampler::Texture2D();
+                int r = g_tex[slot].load(path);
+                g_tex[slot].set_filtering(filt ? xtcore::sampler::FILTERING_BILINEAR
+                                               : xtcore::sampler::FILTERING_NEAREST);
+                if (fx) g_tex[slot].flip_horizontal();
+                if (fy) g_tex[slot].flip_vertical();
+                fprintf(out, " %d", r);
+            }
+        } else if (!strcmp(kind, "tex_sample")) {
+            nimg::ColorRGBf c = g_tex[(int)a[0] & 15].sample(Vector3f(a[1], a[2], 0));
+            put(out, c.r()); put(out, c.g()); put(out, c.b());
+        } else if (!strcmp(kind, "erp_load")) {
+            int slot;
+            char path[4096];
+            if (sscanf(raw + strlen(kind), "%d %4095s", &slot, path) != 2 || slot < 0 || slot >= 4) {
+                fprintf(out, " bad");
+            } else {
+                fprintf(out, " %d", g_erp[slot].load(path));
+            }
+        } else if (!strcmp(kind, "erp_sample")) {
+            nimg::ColorRGBf c = g_erp[(int)a[0] & 3].sample(Vector3f(a[1], a[2], a[3]));
+            put(out, c.r()); put(out, c.g()); put(out, c.b());
+        } else if (!strcmp(kind, "cube_load")) {
+            // cube_load slot left right top bottom front back
+            int slot;
+            char p[6][1024];
+            if (sscanf(raw + strlen(kind), "%d %1023s %1023s %1023s %1023s %1023s %1023s", &slot, p[0], p[1], p[2],
+                       p[3], p[4], p[5]) != 7 || slot < 0 || slot >= 4) {
+                fprintf(out, " bad");
+            } else {
+                for (int f = 0; f < 6; ++f)
+                    fprintf(out, " %d", g_cube[slot].load(p[f], (xtcore::sampler::CUBEMAP_FACE)f));
+            }
+        } else if (!strcmp(kind, "cube_sample")) {
+            nimg::ColorRGBf c = g_cube[(int)a[0] & 3].sample(Vector3f(a[1], a[2], a[3]));
+            put(out, c.r()); put(out, c.g()); put(out, c.b());
         } else if (!strcmp(kind, "gradient")) {
             xtcore::sampler::Gradient g;
             g.a = nimg::ColorRGBf((float)a[0], (float)a[1], (float)a[2]);

@@ -19,6 +19,7 @@
 
 #define XO_EPS 1e-8                    /* EPSILON, lib/nmath/precision.h:87-89 */
 #define XO_PI 3.14159265358979323846   /* nmath::PI, lib/nmath/precision.h:101 */
+#define XO_PI_DOUBLE 6.283185307179586232   /* nmath::PI_DOUBLE, lib/nmath/precision.h:100 */
 #define XO_RADIAN 0.017453292519943    /* RADIAN, lib/nmath/precision.h:111 */
 #define XO_OCT_MAX_ITEMS 10            /* LIMITS_MAX_ITEMS_PER_NODE, mesh.h:11 */
 #define XO_OCT_MAX_DEPTH 10            /* LIMITS_MAX_DEPTH, mesh.h:12 */
@@ -872,11 +873,158 @@ typedef struct {
     c3 intensity;
 } hres;
 
-static int sample_path(const xo_material *m, rng_t *r, v3 point, v3 normal, v3 incident, hres *out)
+/* ------------------------------------------------------------------------ */
+/* Samplers                                                                   */
+
+/* The x86-64 conversion the reference's (int) cast of a float compiles to
+ * (cvttss2si): a value outside int's range, NaN included, gives INT_MIN. */
+static int32_t f2i_x86(float f)
 {
-    c3 dif = C(m->diffuse[0], m->diffuse[1], m->diffuse[2]);
-    c3 spe = C(m->specular[0], m->specular[1], m->specular[2]);
-    c3 emi = C(m->emissive[0], m->emissive[1], m->emissive[2]);
+    return (f != f || f >= 2147483648.f || f < -2147483648.f) ? INT32_MIN : (int32_t)f;
+}
+
+/* Pixmap::pixel_ro clamps both coordinates to the last column / row
+ * (lib/nimg/pixmap.cc:44-50). */
+static const float *texel(const xo_texture *t, const float *tx, uint64_t x, uint64_t y)
+{
+    uint64_t nx = x >= (uint64_t)t->width ? (uint64_t)t->width - 1 : x;
+    uint64_t ny = y >= (uint64_t)t->height ? (uint64_t)t->height - 1 : y;
+    return tx + 4 * (t->offset + (int64_t)(ny * (uint64_t)t->width + nx));
+}
+
+/* nimg::sample::nearest, lib/nimg/sample.cc:8-17: wrap into [0, 1], then
+ * (size_t)(u * (float)width); a NaN coordinate converts to 2^63 on x86-64
+ * and is clamped to the last texel. */
+static c3 tex_nearest(const xo_texture *t, const float *tx, double u, double v)
+{
+    u = u < 0 ? 0 : (u > 1 ? u - floor(u) : u);
+    v = v < 0 ? 0 : (v > 1 ? v - floor(v) : v);
+    double fx = u * (float)t->width, fy = v * (float)t->height;
+    uint64_t x = fx == fx ? (uint64_t)fx : (1ull << 63);
+    uint64_t y = fy == fy ? (uint64_t)fy : (1ull << 63);
+    const float *c = texel(t, tx, x, y);
+    return C(c[0], c[1], c[2]);
+}
+
+/* nimg::sample::bilinear, lib/nimg/sample.cc:19-52: the int texel index is
+ * taken modulo the size_t width (so a negative index wraps through 2^64), the
+ * four colours scaled and summed as ColorRGBAf, each step clamped at 0. */
+static c3 tex_bilinear(const xo_texture *t, const float *tx, double u, double v)
+{
+    const uint64_t w = (uint64_t)t->width, h = (uint64_t)t->height;
+    float fu = (float)(u * (double)w);
+    float fv = (float)(v * (double)h);
+    int32_t u1 = (int32_t)((uint64_t)(int64_t)f2i_x86(fu) % w);
+    int32_t v1 = (int32_t)((uint64_t)(int64_t)f2i_x86(fv) % h);
+    int32_t u2 = (int32_t)((uint64_t)(int64_t)(u1 + 1) % w);
+    int32_t v2 = (int32_t)((uint64_t)(int64_t)(v1 + 1) % h);
+    float fracu = fu - floorf(fu);
+    float fracv = fv - floorf(fv);
+    float w1 = (1 - fracu) * (1 - fracv);
+    float w2 = fracu * (1 - fracv);
+    float w3 = (1 - fracu) * fracv;
+    float w4 = fracu * fracv;
+    const float *a = texel(t, tx, (uint64_t)u1, (uint64_t)v1), *b = texel(t, tx, (uint64_t)u2, (uint64_t)v1);
+    const float *c = texel(t, tx, (uint64_t)u1, (uint64_t)v2), *d = texel(t, tx, (uint64_t)u2, (uint64_t)v2);
+    c3 s = cadd(cadd(cadd(cmuls(C(a[0], a[1], a[2]), w1), cmuls(C(b[0], b[1], b[2]), w2)),
+                     cmuls(C(c[0], c[1], c[2]), w3)), cmuls(C(d[0], d[1], d[2]), w4));
+    return s;
+}
+
+/* Texture2D::sample, sampler_tex.cc:37-45 */
+static c3 tex_sample(const xo_texture *t, const float *tx, double u, double v)
+{
+    return t->filtering == XO_FILTER_BILINEAR ? tex_bilinear(t, tx, u, v) : tex_nearest(t, tx, u, v);
+}
+
+/* ERP::sample, sampler_erp.cc:13-26 (angles rounded to float) */
+static c3 erp_sample(const xo_texture *t, const float *tx, v3 tc)
+{
+    v3 dir = normalized(tc);
+    float theta = (float)acos(dir.y);
+    float phi = (float)atan2(dir.x, -dir.z);
+    float u = (float)(0.5f + phi / XO_PI_DOUBLE);
+    float v = (float)(theta / XO_PI);
+    return tex_sample(t, tx, u, v);
+}
+
+/* Cubemap::sample, sampler_cubemap.cc:13-36: the face of the largest
+ * component, u and v from the other two (faces in CUBEMAP_FACE order:
+ * 0 left, 1 right, 2 top, 3 bottom, 4 front, 5 back). */
+static c3 cube_sample(const xo_texture *faces, const float *tx, v3 tc)
+{
+    v3 dir = normalized(tc);
+    int face = 2;
+    float u = 0.f, v = 0.f;
+    double ax = fabs(dir.x), ay = fabs(dir.y), az = fabs(dir.z);
+    if ((ax >= ay) && (ax >= az)) {
+        if (dir.x > 0.0f) { face = 1; u = (float)((dir.z / dir.x + 1.0f) * 0.5f); v = (float)(1.f - (dir.y / dir.x + 1.0f) * 0.5f); }
+        else if (dir.x < 0.0f) { face = 0; u = (float)((dir.z / dir.x + 1.0f) * 0.5f); v = (float)((dir.y / dir.x + 1.0f) * 0.5f); }
+    } else if ((ay >= ax) && (ay >= az)) {
+        if (dir.y > 0.0f) { face = 2; u = (float)((dir.x / dir.y + 1.0f) * 0.5f); v = (float)(1.f - (dir.z / dir.y + 1.0f) * 0.5f); }
+        else if (dir.y < 0.0f) { face = 3; u = (float)(1. - (dir.x / dir.y + 1.0f) * 0.5f); v = (float)(1.f - (dir.z / dir.y + 1.0f) * 0.5f); }
+    } else if ((az >= ax) && (az >= ay)) {
+        if (dir.z > 0.0f) { face = 5; u = (float)(1. - (dir.x / dir.z + 1.0f) * 0.5f); v = (float)(1.f - (dir.y / dir.z + 1.0f) * 0.5f); }
+        else if (dir.z < 0.0f) { face = 4; u = (float)(1. - (dir.x / dir.z + 1.0f) * 0.5f); v = (float)((dir.y / dir.z + 1.0f) * 0.5f); }
+    }
+    return tex_sample(&faces[face], tx, u, v);
+}
+
+/* Gradient::sample, sampler_gradient.cc:11-17, on a direction or texcoord */
+static c3 gradient_sample(const float a3[3], const float b3[3], v3 tc)
+{
+    v3 d = normalized(tc);
+    float t = (float)(0.5f * d.y + 1.0);
+    c3 a = C(a3[0], a3[1], a3[2]), b = C(b3[0], b3[1], b3[2]);
+    return cadd(cmuls(a, (float)(1.0 - t)), cmuls(b, t));
+}
+
+static c3 sampler_eval(const xo_scene_desc *D, const xo_sampler *sm, v3 tc)
+{
+    switch (sm->kind) {
+    case XO_SAMPLER_GRADIENT: return gradient_sample(sm->a, sm->b, tc);
+    case XO_SAMPLER_TEXTURE: return tex_sample(&D->textures[sm->texture], D->texels, tc.x, tc.y);
+    case XO_SAMPLER_ERP: return erp_sample(&D->textures[sm->texture], D->texels, tc);
+    case XO_SAMPLER_CUBEMAP: return cube_sample(&D->textures[sm->texture], D->texels, tc);
+    default: return C(sm->a[0], sm->a[1], sm->a[2]);
+    }
+}
+
+/* IMaterial::get_sample, material.cc:65-70, at hit_record_t::texcoord (tu, tv,
+ * 0); ch 0 diffuse, 1 specular, 2 emissive.  An absent sampler is black. */
+static c3 mat_sample(const xo_scene_desc *D, int32_t mi, int ch, double tu, double tv)
+{
+    if (!D->mat_samplers) {
+        const xo_material *m = &D->materials[mi];
+        const float *c = ch == 0 ? m->diffuse : (ch == 1 ? m->specular : m->emissive);
+        return C(c[0], c[1], c[2]);
+    }
+    return sampler_eval(D, &D->mat_samplers[3 * mi + ch], V(tu, tv, 0.0));
+}
+
+void xo_kat_texture(const xo_texture *t, const float *texels, double u, double v, float out[3])
+{
+    c3 c = tex_sample(t, texels, u, v);
+    out[0] = c.r; out[1] = c.g; out[2] = c.b;
+}
+
+void xo_kat_erp(const xo_texture *t, const float *texels, const double d[3], float out[3])
+{
+    c3 c = erp_sample(t, texels, V(d[0], d[1], d[2]));
+    out[0] = c.r; out[1] = c.g; out[2] = c.b;
+}
+
+void xo_kat_cubemap(const xo_texture *faces, const float *texels, const double d[3], float out[3])
+{
+    c3 c = cube_sample(faces, texels, V(d[0], d[1], d[2]));
+    out[0] = c.r; out[1] = c.g; out[2] = c.b;
+}
+
+/* The material's three samples are resolved by the caller (samplers draw no
+ * random numbers, so resolving all three changes nothing). */
+static int sample_path_c(const xo_material *m, c3 dif, c3 spe, c3 emi, rng_t *r, v3 point, v3 normal,
+                         v3 incident, hres *out)
+{
     switch (m->type) {
     case XO_LAMBERT:   /* lambert.cc:30-40 */
         out->org = add(point, muls(normal, XO_EPS));
@@ -911,15 +1059,19 @@ static int sample_path(const xo_material *m, rng_t *r, v3 point, v3 normal, v3 i
     }
 }
 
+static int sample_path(const xo_material *m, rng_t *r, v3 point, v3 normal, v3 incident, hres *out)
+{
+    return sample_path_c(m, C(m->diffuse[0], m->diffuse[1], m->diffuse[2]),
+                         C(m->specular[0], m->specular[1], m->specular[2]),
+                         C(m->emissive[0], m->emissive[1], m->emissive[2]), r, point, normal, incident, out);
+}
+
 static c3 environment(const xo_scene_desc *D, v3 dir)
 {
     if (D->env_type == XO_ENV_COLOR) return C(D->env_a[0], D->env_a[1], D->env_a[2]);
-    if (D->env_type == XO_ENV_GRADIENT) {   /* sampler_gradient.cc:11-17 */
-        v3 d = normalized(dir);
-        float t = (float)(0.5f * d.y + 1.0);
-        c3 a = C(D->env_a[0], D->env_a[1], D->env_a[2]), b = C(D->env_b[0], D->env_b[1], D->env_b[2]);
-        return cadd(cmuls(a, (float)(1.0 - t)), cmuls(b, t));
-    }
+    if (D->env_type == XO_ENV_GRADIENT) return gradient_sample(D->env_a, D->env_b, dir);
+    if (D->env_type == XO_ENV_ERP) return erp_sample(&D->textures[D->env_texture], D->texels, dir);
+    if (D->env_type == XO_ENV_CUBEMAP) return cube_sample(&D->textures[D->env_texture], D->texels, dir);
     return C(0, 0, 0);   /* scene.cc:142-145 */
 }
 
@@ -932,12 +1084,14 @@ static c3 pt_eval(const xo_scene *s, size_t depth, c3 in_int, v3 o, v3 d, rng_t 
     ++*rays;
     int hit = scene_hit(s, o, d, &h, &oi, &pi);
     if (hit) {
-        const xo_material *m = &s->d.materials[s->d.obj_material[oi]];
+        const int32_t mi = s->d.obj_material[oi];
+        const xo_material *m = &s->d.materials[mi];
         hres res;
         res.org = V(0, 0, 0);
         res.dir = V(0, 0, 1);
         res.intensity = C(0, 0, 0);
-        int cont = sample_path(m, r, h.point, h.normal, d, &res);
+        int cont = sample_path_c(m, mat_sample(&s->d, mi, 0, h.tu, h.tv), mat_sample(&s->d, mi, 1, h.tu, h.tv),
+                                 mat_sample(&s->d, mi, 2, h.tu, h.tv), r, h.point, h.normal, d, &res);
         c3 value = cmul(in_int, res.intensity);
         if (cont) value = cmul(value, pt_eval(s, depth - 1, res.intensity, res.org, res.dir, r, rays));
         return value;
@@ -1045,8 +1199,7 @@ int xo_render(const xo_scene *s, const xo_render_params *p, int64_t npix, const 
             } else if (p->integrator == XO_EMISSION) {  /* emission/integrator.cc:10-38 */
                 ++nr;
                 if (scene_hit(s, O, Dd, &h, &oi, &pi)) {
-                    const xo_material *m = &D->materials[D->obj_material[oi]];
-                    c3 e = cmuls(C(m->emissive[0], m->emissive[1], m->emissive[2]), (float)weight);
+                    c3 e = cmuls(mat_sample(D, D->obj_material[oi], 2, h.tu, h.tv), (float)weight);
                     col[0] = clamp0(col[0] + e.r);
                     col[1] = clamp0(col[1] + e.g);
                     col[2] = clamp0(col[2] + e.b);

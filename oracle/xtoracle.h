@@ -22,7 +22,12 @@ extern "C" {
 
 enum { XO_SPHERE = 0, XO_PLANE = 1, XO_MESH = 2 };
 enum { XO_LAMBERT = 0, XO_PHONG = 1, XO_BLINNPHONG = 2, XO_EMISSIVE = 3, XO_DIELECTRIC = 4 };
-enum { XO_ENV_NONE = 0, XO_ENV_COLOR = 1, XO_ENV_GRADIENT = 2 };
+enum { XO_ENV_NONE = 0, XO_ENV_COLOR = 1, XO_ENV_GRADIENT = 2, XO_ENV_ERP = 3, XO_ENV_CUBEMAP = 4 };
+/* material samplers (sampler_col.cc, sampler_gradient.cc, sampler_tex.cc,
+ * sampler_erp.cc, sampler_cubemap.cc); texture filtering (sampler.h:11-15) */
+enum { XO_SAMPLER_COLOR = 0, XO_SAMPLER_GRADIENT = 1, XO_SAMPLER_TEXTURE = 2, XO_SAMPLER_ERP = 3,
+       XO_SAMPLER_CUBEMAP = 4 };
+enum { XO_FILTER_NEAREST = 0, XO_FILTER_BILINEAR = 1 };
 enum { XO_STENCIL = 0, XO_DEPTH = 1, XO_AO = 2, XO_PATHTRACER = 3,
        XO_NORMAL = 4, XO_UV = 5, XO_EMISSION = 6, XO_WIREFRAME = 7 };
 /* mesh intersector: 0 = octree restatement (exact reference order), 1 = FP64 BVH
@@ -40,6 +45,21 @@ typedef struct {
     float diffuse[3], specular[3], emissive[3];
     float reflectance, exponent, ior;
 } xo_material;
+
+/* A loaded Texture2D: its Pixmap (RGBA float per texel, rows top first, as
+ * nimg::io::load::image fills it after the flips) and its filtering. */
+typedef struct {
+    int32_t width, height, filtering, pad;
+    int64_t offset;              /* first texel in xo_scene_desc::texels */
+} xo_texture;
+
+/* A material sampler: COLOR a; GRADIENT a, b; TEXTURE and ERP one texture;
+ * CUBEMAP six consecutive textures in CUBEMAP_FACE order (left, right, top,
+ * bottom, front, back; sampler_cubemap.h:11-19). */
+typedef struct {
+    int32_t kind, texture;
+    float a[3], b[3];
+} xo_sampler;
 
 typedef struct {
     int32_t n_objects;
@@ -68,6 +88,12 @@ typedef struct {
     float cam_orientation[3];    /* ERP, ODS: euler angles (Matrix4x4f::rotate) */
     float cam_ipd;               /* ODS */
     float cam_flength, cam_aperture;   /* perspective: depth of field when flength > 0 */
+    int32_t n_textures;
+    const xo_texture *textures;
+    const float *texels;         /* 4 floats (r g b a) per texel */
+    const xo_sampler *mat_samplers;    /* 3 per material (diffuse, specular, emissive), or
+                                          NULL = the materials' colours */
+    int32_t env_texture;         /* XO_ENV_ERP: its texture; XO_ENV_CUBEMAP: the first of six */
 } xo_scene_desc;
 
 typedef struct xo_scene xo_scene;
@@ -112,6 +138,12 @@ void xo_kat_lobe(const int32_t *table, int32_t rand_max, const double n[3], cons
 int  xo_kat_material(const xo_material *m, const int32_t *table, int32_t rand_max, const double p[3],
                      const double n[3], const double inc[3], double out[9]);
 void xo_kat_gradient(const float a[3], const float b[3], const double d[3], float out[3]);
+/* Texture2D::sample (sampler_tex.cc:37-45: nimg::sample::nearest / bilinear),
+ * ERP::sample (sampler_erp.cc:13-26) and Cubemap::sample (sampler_cubemap.cc:
+ * 13-36) on textures of the given layout; faces: six textures. */
+void xo_kat_texture(const xo_texture *t, const float *texels, double u, double v, float out[3]);
+void xo_kat_erp(const xo_texture *t, const float *texels, const double d[3], float out[3]);
+void xo_kat_cubemap(const xo_texture *faces, const float *texels, const double d[3], float out[3]);
 
 /* Camera rays of every camera type, known-answer hooks: perspective with depth
  * of field (the two prng_c draws from `table`), equirectangular, ODS, cubemap. */

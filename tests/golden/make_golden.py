@@ -21,7 +21,12 @@ these fixtures are what pins the oracle restatement (oracle/xtoracle.c):
 * kat_cameras.npz, render_cameras.npz  rays of the ERP, ODS, cubemap and
               depth-of-field cameras (with the rand() values the latter drew),
               and stencil/depth/normal frames through each camera with grid
-              anti-aliasing (`--cameras` regenerates only these).
+              anti-aliasing (`--cameras` regenerates only these);
+* kat_textures.npz, render_textures.npz  Texture2D (nearest and bilinear,
+              flipped), ERP and Cubemap samples on PNG files the reference
+              loads, and frames of textured scenes with ERP and cubemap
+              environments: emission and depth-1 pathtracer (deterministic)
+              and depth-4 pathtracer at four seeds (`--textures`).
 
 Run here (needs the reference sources and oracle/_ref/xtref):
     make -f oracle/ref.mk REF=<xtracer source tree> -j8
@@ -298,6 +303,93 @@ def make_cameras(work, rng):
     print("render_cameras.npz", sorted(rend))
 
 
+def sampler_kat_textures(rng):
+    """The textures of the sampler known-answer vectors: (pixels, filtering,
+    flip_x, flip_y) with odd sizes, RGB and RGBA, both filters and flips."""
+    out = []
+    for i, (h, w, c) in enumerate([(5, 7, 3), (6, 9, 4), (8, 8, 3), (1, 3, 3), (4, 16, 4), (3, 1, 3)]):
+        out.append((rng.integers(0, 256, (h, w, c), dtype=np.uint8), i % 2, int(i in (1, 4)), int(i in (2, 4))))
+    return out
+
+
+def make_textures(work, rng):
+    """Sampler known-answer vectors (Texture2D nearest / bilinear, ERP,
+    Cubemap on PNG files loaded by the reference) and frames of the textured
+    scenes rendered by the reference."""
+    kat = {}
+    texs = sampler_kat_textures(rng)
+    lines = []
+    for i, (px, filt, fx, fy) in enumerate(texs):
+        path = os.path.join(work, "kat_t%d.png" % i)
+        scenes.write_png(path, px)
+        lines.append("tex_load %d %d %d %d %s" % (i, filt, fx, fy, path))
+        kat["tex%d_pixels" % i] = px
+        kat["tex%d_mode" % i] = np.array([filt, fx, fy], np.int32)
+    uv = np.concatenate([rng.uniform(-2.5, 2.5, (160, 2)), rng.uniform(0, 1, (160, 2)),
+                         np.array([[0, 0], [1, 1], [0.5, 1], [1, 0.5], [-0.0, 0.25], [2, -1], [3.75, -2.25],
+                                   [np.nan, 0.5], [0.5, np.nan], [np.inf, 0.5], [-np.inf, 0.5], [1e10, -1e10]])])
+    rows = []
+    for i in range(len(texs)):
+        for u, v in uv:
+            lines.append("tex_sample %d %s %s" % (i, H(float(u)), H(float(v))))
+            rows.append((i, u, v))
+    erp = rng.integers(0, 256, (9, 17, 3), dtype=np.uint8)
+    faces = [rng.integers(0, 256, (4 + k % 3, 5 + k % 2, 3), dtype=np.uint8) for k in range(6)]
+    scenes.write_png(os.path.join(work, "kat_erp.png"), erp)
+    fpaths = []
+    for k, f in enumerate(faces):
+        fpaths.append(os.path.join(work, "kat_face%d.png" % k))
+        scenes.write_png(fpaths[-1], f)
+    lines += ["erp_load 0 %s" % os.path.join(work, "kat_erp.png"), "cube_load 0 %s" % " ".join(fpaths)]
+    dirs = np.concatenate([rng.normal(size=(300, 3)),
+                           np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1],
+                                     [0, 0, 0], [1, 1, 0], [1, -1, 1], [0.5, 0.5, -0.5], [np.nan, 0, 1]])])
+    for v in dirs:
+        lines.append(_line("erp_sample", 0, *v))
+        lines.append(_line("cube_sample", 0, *v))
+    res = po.ref_kat(lines)
+    assert all(r[1:] == ["0"] for r in res if r[0] in ("tex_load", "erp_load")), "texture load failed"
+    tex_out = [[float.fromhex(t) for t in r[1:4]] for r in res if r[0] == "tex_sample"]
+    kat["tex_in"] = np.array(rows, np.float64)
+    kat["tex_out"] = np.array(tex_out, np.float32)
+    kat["erp_pixels"] = erp
+    for k, f in enumerate(faces):
+        kat["face%d_pixels" % k] = f
+    kat["dirs"] = dirs
+    kat["erp_out"] = np.array([[float.fromhex(t) for t in r[1:4]] for r in res if r[0] == "erp_sample"], np.float32)
+    kat["cube_out"] = np.array([[float.fromhex(t) for t in r[1:4]] for r in res if r[0] == "cube_sample"], np.float32)
+    np.savez_compressed(os.path.join(HERE, "kat_textures.npz"), **kat)
+    print("kat_textures.npz", sorted(kat))
+
+    rend = {}
+    for env in ("erp", "cubemap"):
+        spec = scenes.textured_scene(env)
+        scn = spec.write_scn(work)
+        w, h = texture_frame_size()
+        # emission folds each sample's emissive texel; a pathtracer of depth 1
+        # returns the environment's texel on a miss and the emissive sampler's
+        # on an emissive hit (eval(0) is black), so both are deterministic
+        for integ, spp, rdepth, aa in (("emission", 2, 1, 2), ("pathtracer", 2, 1, 1)):
+            xy, rgba, st = po.ref_render(scn, integ, w, h, spp=spp, rdepth=rdepth, aa=aa, threads=1, seed=1,
+                                         workdir=work)
+            rend["%s_%s_xy" % (env, integ)] = xy
+            rend["%s_%s_rgba" % (env, integ)] = rgba
+            rend["%s_%s_rays" % (env, integ)] = st["rays"]
+        imgs = []
+        for seed in (51, 52, 53, 54):
+            xy, rgba, st = po.ref_render(scn, "pathtracer", w, h, spp=16, rdepth=4, threads=1, seed=seed,
+                                         workdir=work)
+            imgs.append(rgba)
+        rend["%s_pt_xy" % env] = xy
+        rend["%s_pt_rgba" % env] = np.stack(imgs)
+    np.savez_compressed(os.path.join(HERE, "render_textures.npz"), **rend)
+    print("render_textures.npz", sorted(rend))
+
+
+def texture_frame_size():
+    return 64, 48
+
+
 def camera_cases():
     """(tag, camera, width, height, aa) of the camera frame fixtures."""
     C = scenes.Camera
@@ -316,6 +408,9 @@ def main():
         return
     if "--cameras" in sys.argv:
         make_cameras(tempfile.mkdtemp(prefix="xtgold"), np.random.default_rng(20261204))
+        return
+    if "--textures" in sys.argv:
+        make_textures(tempfile.mkdtemp(prefix="xtgold"), np.random.default_rng(20261205))
         return
     rng = np.random.default_rng(20261203)
     kat = make_kat(rng)

@@ -273,3 +273,93 @@ def test_camera_frames_with_grid_antialiasing_golden(case):
         assert rays == int(g["%s_%s_rays" % (tag, integ)])
         ref = g["%s_%s_rgba" % (tag, integ)]
         assert np.array_equal(out, ref, equal_nan=True), (tag, integ, np.nanmax(np.abs(out - ref)))
+
+
+def _kat_textures(k):
+    """The sampler fixtures' textures as the reference holds them after
+    loading: texels and ctypes layout rows (one texel array per texture)."""
+    out = []
+    i = 0
+    while "tex%d_pixels" % i in k:
+        filt, fx, fy = (int(v) for v in k["tex%d_mode" % i])
+        t = scenes.Texture(k["tex%d_pixels" % i], filt, bool(fx), bool(fy))
+        tx = t.texels()
+        out.append((po.texture_structs(np.array([[tx.shape[1], tx.shape[0], filt, 0]])), tx))
+        i += 1
+    return out
+
+
+def test_texture_sampler_kat():
+    """Texture2D::sample with nearest and bilinear filtering, flips, RGB and
+    RGBA textures of odd sizes, texcoords outside [0, 1], NaN and infinities
+    (sampler_tex.cc:37-45, nimg/sample.cc:8-52): bit for bit."""
+    k = np.load(os.path.join(GOLD, "kat_textures.npz"))
+    texs = _kat_textures(k)
+    L = po.lib()
+    out = (C.c_float * 3)()
+    for (i, u, v), want in zip(k["tex_in"], k["tex_out"]):
+        st, tx = texs[int(i)]
+        L.xo_kat_texture(C.cast(st, C.c_void_p), P(tx), float(u), float(v), out)
+        assert np.array_equal(np.float32(out), want, equal_nan=True), (int(i), u, v, list(out), want)
+
+
+def test_erp_and_cubemap_sampler_kat():
+    """ERP::sample and Cubemap::sample (sampler_erp.cc:13-26,
+    sampler_cubemap.cc:13-36) on random, axis-aligned, zero and NaN
+    directions: bit for bit."""
+    k = np.load(os.path.join(GOLD, "kat_textures.npz"))
+    L = po.lib()
+    etx = scenes.Texture(k["erp_pixels"]).texels()
+    est = po.texture_structs(np.array([[etx.shape[1], etx.shape[0], 0, 0]]))
+    ftx = [scenes.Texture(k["face%d_pixels" % f]).texels() for f in range(6)]
+    offs = np.cumsum([0] + [t.shape[0] * t.shape[1] for t in ftx])[:-1]
+    fst = po.texture_structs(np.array([[t.shape[1], t.shape[0], 0, o] for t, o in zip(ftx, offs)]))
+    fall = np.ascontiguousarray(np.concatenate([t.reshape(-1, 4) for t in ftx]))
+    out = (C.c_float * 3)()
+    for d, we, wc in zip(k["dirs"], k["erp_out"], k["cube_out"]):
+        dv = np.ascontiguousarray(d, np.float64)
+        L.xo_kat_erp(C.cast(est, C.c_void_p), P(etx), P(dv), out)
+        assert np.array_equal(np.float32(out), we, equal_nan=True), ("erp", d)
+        L.xo_kat_cubemap(C.cast(fst, C.c_void_p), P(fall), P(dv), out)
+        assert np.array_equal(np.float32(out), wc, equal_nan=True), ("cubemap", d)
+
+
+@pytest.mark.parametrize("env", ["erp", "cubemap"])
+def test_textured_frames_golden(env):
+    """Textured scenes through the reference's own loader (PNG files,
+    filtering and flip keys): the emission frame (aa 2) folds each sample's
+    emissive texel, and the depth-1 pathtracer frame is the environment's texel
+    on a miss and the emissive sampler's on an emissive hit.  Bit for bit."""
+    import importlib.util
+    spec_ = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLD, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec_)
+    spec_.loader.exec_module(mg)
+    w, h = mg.texture_frame_size()
+    g = np.load(os.path.join(GOLD, "render_textures.npz"))
+    spec = scenes.textured_scene(env)
+    orc = po.OracleScene(spec, po.XO_ACCEL_OCTREE)
+    for integ, code, spp, rdepth, aa in (("emission", po.EMISSION, 2, 1, 2), ("pathtracer", po.PATHTRACER, 2, 1, 1)):
+        xy = g["%s_%s_xy" % (env, integ)]
+        out, rays = orc.render(code, w, h, spp=spp, rdepth=rdepth, pixels=xy, aa=aa)
+        assert rays == int(g["%s_%s_rays" % (env, integ)])
+        ref = g["%s_%s_rgba" % (env, integ)]
+        assert np.array_equal(out, ref, equal_nan=True), (env, integ, np.nanmax(np.abs(out - ref)))
+
+
+@pytest.mark.parametrize("env", ["erp", "cubemap"])
+def test_textured_pathtracer_within_reference_noise(env):
+    """Depth-4 paths over textured diffuse, specular and emissive samplers:
+    within the reference's noise (four reference seeds)."""
+    g = np.load(os.path.join(GOLD, "render_textures.npz"))
+    spec = scenes.textured_scene(env)
+    orc = po.OracleScene(spec, po.XO_ACCEL_BVH)
+    w, h = 64, 48
+    O, _ = orc.render(po.PATHTRACER, w, h, spp=16, rdepth=4, seed=777, pixels=g["%s_pt_xy" % env])
+    R = g["%s_pt_rgba" % env]
+    got, ref = stochastic_agreement(O, R)
+    assert got <= 1.25 * ref + 1e-6, (got, ref)
+    n = R.shape[0]
+    for ch in range(3):
+        diff = O[:, ch] - R[:, :, ch].mean(0)
+        se = np.sqrt(R[:, :, ch].var(0, ddof=1).mean() / diff.size * (1 + 1.0 / n))
+        assert abs(diff.mean()) < 4.5 * se + 1e-5, (ch, diff.mean(), se)

@@ -26,9 +26,49 @@ import numpy as np
 
 SPHERE, PLANE, MESH = 0, 1, 2
 LAMBERT, PHONG, BLINNPHONG, EMISSIVE, DIELECTRIC = 0, 1, 2, 3, 4
-ENV_NONE, ENV_COLOR, ENV_GRADIENT = 0, 1, 2
+ENV_NONE, ENV_COLOR, ENV_GRADIENT, ENV_ERP, ENV_CUBEMAP = 0, 1, 2, 3, 4
 MATERIAL_NAMES = {LAMBERT: "lambert", PHONG: "phong", BLINNPHONG: "blinn_phong",
                   EMISSIVE: "emissive", DIELECTRIC: "dielectric"}
+# material samplers (sampler_col.cc, sampler_gradient.cc, sampler_tex.cc,
+# sampler_erp.cc, sampler_cubemap.cc) and texture filtering (sampler.h:11-15)
+SAMPLER_COLOR, SAMPLER_GRADIENT, SAMPLER_TEXTURE, SAMPLER_ERP, SAMPLER_CUBEMAP = 0, 1, 2, 3, 4
+FILTER_NEAREST, FILTER_BILINEAR = 0, 1
+# the .scn keys of the six cubemap faces in CUBEMAP_FACE order (left, right,
+# top, bottom, front, back: sampler_cubemap.h:11-19, parseutil.cc:177-182)
+CUBE_FACE_KEYS = ("negx", "posx", "posy", "negy", "posz", "negz")
+
+
+@dataclasses.dataclass(eq=False)
+class Texture:
+    """An 8-bit RGB or RGBA image, written as PNG for the reference, which
+    loads it with stbi_load and divides each channel by 255.f (alpha 1 for
+    RGB, nimg/img.cc:17-66), then applies flip_x / flip_y (sampler_tex.cc)."""
+    pixels: np.ndarray                 # (H, W, 3 or 4) uint8, top row first
+    filtering: int = FILTER_NEAREST
+    flip_x: bool = False
+    flip_y: bool = False
+
+    def texels(self) -> np.ndarray:
+        """(H, W, 4) float32 as Texture2D holds them after loading."""
+        p = np.asarray(self.pixels, np.uint8)
+        rgba = np.ones(p.shape[:2] + (4,), np.float32)
+        rgba[..., :p.shape[2]] = p.astype(np.float32) / np.float32(255.0)
+        if self.flip_x:
+            rgba = rgba[:, ::-1]
+        if self.flip_y:
+            rgba = rgba[::-1]
+        return np.ascontiguousarray(rgba)
+
+
+@dataclasses.dataclass
+class Sampler:
+    """A material or environment sampler: a colour, a gradient over the
+    normalised texcoord (or direction), a 2D texture, an equirectangular map
+    or a cubemap (six textures in CUBEMAP_FACE order)."""
+    kind: int = SAMPLER_COLOR
+    a: tuple = (0.0, 0.0, 0.0)
+    b: tuple = (0.0, 0.0, 0.0)
+    textures: tuple = ()
 
 
 @dataclasses.dataclass
@@ -40,6 +80,31 @@ class Material:
     reflectance: float = 0.0
     exponent: float = 0.0
     ior: float = 1.0
+    # "diffuse" / "specular" / "emissive" -> Sampler, replacing that colour
+    samplers: Optional[dict] = None
+
+    def sampler(self, key: str) -> "Sampler":
+        if self.samplers and key in self.samplers:
+            return self.samplers[key]
+        return Sampler(SAMPLER_COLOR, tuple(getattr(self, key)))
+
+
+def write_png(path: str, pixels: np.ndarray) -> None:
+    """8-bit RGB or RGBA PNG (one IDAT, filter 0 on every row)."""
+    import struct
+    import zlib
+    p = np.ascontiguousarray(np.asarray(pixels, np.uint8))
+    h, w, c = p.shape
+    raw = b"".join(b"\x00" + p[y].tobytes() for y in range(h))
+
+    def chunk(tag, data):
+        return struct.pack(">I", len(data)) + tag + data + struct.pack(">I", zlib.crc32(tag + data) & 0xFFFFFFFF)
+
+    with open(path, "wb") as fh:
+        fh.write(b"\x89PNG\r\n\x1a\n")
+        fh.write(chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, 2 if c == 3 else 6, 0, 0, 0)))
+        fh.write(chunk(b"IDAT", zlib.compress(raw, 6)))
+        fh.write(chunk(b"IEND", b""))
 
 
 CAM_PERSPECTIVE, CAM_ERP, CAM_ODS, CAM_CUBEMAP = 0, 1, 2, 3
@@ -84,6 +149,49 @@ class SceneSpec:
     # corners (Triangle::tc, OBJ "vt"); None = all zero
     obj_uv_scale: Optional[np.ndarray] = None      # (O, 2) float32
     tri_uvs: Optional[np.ndarray] = None           # (T, 3, 2) float32
+    # ENV_ERP: one texture; ENV_CUBEMAP: six in CUBEMAP_FACE order
+    env_textures: tuple = ()
+
+    def texture_tables(self):
+        """The scene's textures and samplers as the C ABI takes them:
+        textures (K, 4) int64 rows (width, height, filtering, first texel),
+        texels (N, 4) float32, mat_samplers (M, 3) of (kind, first texture,
+        a, b) per diffuse/specular/emissive, env_texture.  A texture object
+        used several times is stored once; cubemap faces are consecutive."""
+        rows, blocks, index = [], [], {}
+        total = 0
+
+        def add(texs):
+            nonlocal total
+            key = tuple(id(t) for t in texs)
+            if key in index:
+                return index[key]
+            first = len(rows)
+            for t in texs:
+                tx = t.texels()
+                rows.append((tx.shape[1], tx.shape[0], t.filtering, total))
+                blocks.append(tx.reshape(-1, 4))
+                total += tx.shape[0] * tx.shape[1]
+            index[key] = first
+            return first
+
+        samp = []
+        for m in self.materials:
+            row = []
+            for key in ("diffuse", "specular", "emissive"):
+                sm = m.sampler(key)
+                tex = add(sm.textures) if sm.kind in (SAMPLER_TEXTURE, SAMPLER_ERP, SAMPLER_CUBEMAP) else -1
+                row.append((sm.kind, tex, tuple(sm.a), tuple(sm.b)))
+            samp.append(row)
+        env_tex = add(self.env_textures) if self.env_type in (ENV_ERP, ENV_CUBEMAP) else -1
+        textures = np.array(rows, np.int64).reshape(-1, 4)
+        texels = np.concatenate(blocks).astype(np.float32) if blocks else np.zeros((0, 4), np.float32)
+        return textures, texels, samp, env_tex
+
+    @property
+    def has_textures(self) -> bool:
+        return self.env_type in (ENV_ERP, ENV_CUBEMAP) or any(
+            m.samplers and any(v.kind != SAMPLER_COLOR for v in m.samplers.values()) for m in self.materials)
 
     @property
     def n_tris(self) -> int:
@@ -102,7 +210,40 @@ class SceneSpec:
         v3 = lambda v: "vec3(%s,%s,%s)" % (f(v[0]), f(v[1]), f(v[2]))
         c3 = lambda v: "col3(%s,%s,%s)" % (f(v[0]), f(v[1]), f(v[2]))
         out = ["title = %s" % self.name, "version = 1.0", ""]
-        if self.env_type == ENV_GRADIENT:
+        pngs = {}
+
+        def png(t):
+            if id(t) not in pngs:
+                pngs[id(t)] = "%s_t%02d.png" % (self.name, len(pngs))
+                write_png(os.path.join(directory, pngs[id(t)]), t.pixels)
+            return pngs[id(t)]
+
+        def sampler_lines(sm, ind):
+            if sm.kind == SAMPLER_COLOR:
+                return [ind + "type = color", ind + "value = %s" % c3(sm.a)]
+            if sm.kind == SAMPLER_GRADIENT:
+                return [ind + "type = gradient", ind + "a = %s" % c3(sm.a), ind + "b = %s" % c3(sm.b)]
+            if sm.kind == SAMPLER_TEXTURE:
+                t = sm.textures[0]
+                return [ind + "type = texture", ind + "source = %s" % png(t),
+                        ind + "filtering = %s" % ("bilinear" if t.filtering == FILTER_BILINEAR else "nearest"),
+                        ind + "flip_x = %s" % ("true" if t.flip_x else "false"),
+                        ind + "flip_y = %s" % ("true" if t.flip_y else "false")]
+            # the ERP and cubemap textures load with nearest filtering, unflipped
+            assert all(t.filtering == FILTER_NEAREST and not t.flip_x and not t.flip_y for t in sm.textures)
+            if sm.kind == SAMPLER_ERP:
+                return [ind + "type = erp", ind + "source = %s" % png(sm.textures[0])]
+            return [ind + "type = cubemap"] + [ind + "%s = %s" % (k, png(t))
+                                               for k, t in zip(CUBE_FACE_KEYS, sm.textures)]
+
+        if self.env_type == ENV_ERP:
+            out += ["environment = {", "  type = erp", "  config = {",
+                    "    source = %s" % png(self.env_textures[0]), "  }", "}"]
+        elif self.env_type == ENV_CUBEMAP:
+            out += ["environment = {", "  type = cubemap", "  config = {"]
+            out += ["    %s = %s" % (k, png(t)) for k, t in zip(CUBE_FACE_KEYS, self.env_textures)]
+            out += ["  }", "}"]
+        elif self.env_type == ENV_GRADIENT:
             out += ["environment = {", "  type = gradient", "  config = {",
                     "    a = %s" % c3(self.env_a), "    b = %s" % c3(self.env_b), "  }", "}"]
         elif self.env_type == ENV_COLOR:
@@ -147,8 +288,7 @@ class SceneSpec:
             out += ["  m%05d = {" % mi, "    type = %s" % MATERIAL_NAMES[m.type], "    properties = {",
                     "      samplers = {"]
             for key in ("diffuse", "specular", "emissive"):
-                out += ["        %s = {" % key, "          type = color",
-                        "          value = %s" % c3(getattr(m, key)), "        }"]
+                out += ["        %s = {" % key] + sampler_lines(m.sampler(key), "          ") + ["        }"]
             out += ["      }", "      scalars = {", "        reflectance = %s" % f(m.reflectance),
                     "        exponent = %s" % f(m.exponent), "        ior = %s" % f(m.ior),
                     "      }", "    }", "  }"]
@@ -298,6 +438,47 @@ def uv_scene(seed: int = 6, name: str = "uvscene") -> SceneSpec:
     return SceneSpec(name, base.spheres, base.planes, tris, kinds, firsts, counts, omat, mats, base.camera,
                      ENV_GRADIENT, base.env_a, base.env_b, mesh_obj=[(verts, faces)], obj_uv_scale=scale,
                      tri_uvs=tri_uvs)
+
+
+def textured_scene(env: str = "erp", seed: int = 9, name: str = None) -> SceneSpec:
+    """Every sampler kind on every primitive kind: the uv scene's spheres,
+    ground plane and texcoord-carrying terrain patch with 2D textures (nearest
+    and bilinear, flipped and not, RGB and RGBA, odd sizes), ERP, cubemap and
+    gradient material samplers on diffuse, specular and emissive, and an ERP
+    or cubemap environment."""
+    rng = np.random.default_rng(seed)
+    base = uv_scene(seed=6, name=name or ("tex_" + env))
+    img = lambda h, w, c=3: rng.integers(0, 256, (h, w, c), dtype=np.uint8)
+    t_near = Texture(img(5, 7), FILTER_NEAREST)
+    t_bil = Texture(img(6, 9, 4), FILTER_BILINEAR, flip_x=True)
+    t_flip = Texture(img(8, 8), FILTER_BILINEAR, flip_y=True)
+    t_wide = Texture(img(4, 16), FILTER_NEAREST, flip_x=True, flip_y=True)
+    m_erp = Texture(img(9, 17))
+    m_cube = tuple(Texture(img(4 + i % 3, 5)) for i in range(6))
+    samplers = [
+        {"diffuse": Sampler(SAMPLER_TEXTURE, textures=(t_near,))},
+        {"emissive": Sampler(SAMPLER_TEXTURE, textures=(t_bil,))},
+        {"diffuse": Sampler(SAMPLER_ERP, textures=(m_erp,)), "emissive": Sampler(SAMPLER_ERP, textures=(m_erp,))},
+        {"emissive": Sampler(SAMPLER_CUBEMAP, textures=m_cube)},
+        {"diffuse": Sampler(SAMPLER_GRADIENT, (0.25, 0.5, 1.0), (1.0, 0.5, 0.125)),
+         "specular": Sampler(SAMPLER_TEXTURE, textures=(t_wide,)),
+         "emissive": Sampler(SAMPLER_GRADIENT, (0.5, 0.25, 0.0), (0.0, 0.75, 1.0))},
+        {"emissive": Sampler(SAMPLER_TEXTURE, textures=(t_flip,))},
+    ]
+    mats = []
+    for i, m in enumerate(base.materials):
+        mats.append(dataclasses.replace(m, samplers=samplers[i % len(samplers)]))
+    # u/v scales of at least 1 keep every sphere texcoord finite (a scale below
+    # 1 drives asin out of its domain: NaN texcoords, covered by the uv scenes)
+    uvs = base.obj_uv_scale.copy()
+    small = (uvs > 0) & (uvs < 1)
+    uvs[small] = _q(1.0 / uvs[small], 8)
+    spec = dataclasses.replace(base, materials=mats, obj_uv_scale=uvs)
+    if env == "erp":
+        spec.env_type, spec.env_textures = ENV_ERP, (Texture(img(16, 32)),)
+    else:
+        spec.env_type, spec.env_textures = ENV_CUBEMAP, tuple(Texture(img(6 + i, 6 + i)) for i in range(6))
+    return spec
 
 
 def grid_for_tris(n_tris: int) -> int:
