@@ -59,8 +59,14 @@ typedef enum {
 enum { XTGPU_SPHERE = 0, XTGPU_PLANE = 1, XTGPU_MESH = 2 };
 /* Materials (src/xtcore/material/, names in matdefs.h:4-12). */
 enum { XTGPU_LAMBERT = 0, XTGPU_PHONG = 1, XTGPU_BLINNPHONG = 2, XTGPU_EMISSIVE = 3, XTGPU_DIELECTRIC = 4 };
-/* Environment samplers (sampler_col.cc, sampler_gradient.cc); none = black. */
-enum { XTGPU_ENV_NONE = 0, XTGPU_ENV_COLOR = 1, XTGPU_ENV_GRADIENT = 2 };
+/* Environment samplers (sampler_col.cc, sampler_gradient.cc, sampler_erp.cc,
+ * sampler_cubemap.cc); none = black (scene.cc:142-145). */
+enum { XTGPU_ENV_NONE = 0, XTGPU_ENV_COLOR = 1, XTGPU_ENV_GRADIENT = 2, XTGPU_ENV_ERP = 3, XTGPU_ENV_CUBEMAP = 4 };
+/* Material samplers (IMaterial::get_sample, material.cc:65-70, at the hit's
+ * texcoord) and texture filtering (sampler.h:11-15). */
+enum { XTGPU_SAMPLER_COLOR = 0, XTGPU_SAMPLER_GRADIENT = 1, XTGPU_SAMPLER_TEXTURE = 2, XTGPU_SAMPLER_ERP = 3,
+       XTGPU_SAMPLER_CUBEMAP = 4 };
+enum { XTGPU_FILTER_NEAREST = 0, XTGPU_FILTER_BILINEAR = 1 };
 /* Cameras (src/xtcore/camera/): thin-lens perspective, equirectangular,
  * omni-directional stereo (upper half one eye, lower the other), cubemap
  * vertical strip (faces +x -x +y -y +z -z, height a multiple of 6). */
@@ -93,6 +99,24 @@ typedef struct {
                                       each sample's random stream */
 } xtgpu_camera;
 
+/* A loaded Texture2D (sampler_tex.h:14-37): its Pixmap as RGBA floats, rows
+ * top first, after the loader's flips, and its filtering. */
+typedef struct {
+    int32_t width, height;
+    int32_t filtering;             /* XTGPU_FILTER_NEAREST / XTGPU_FILTER_BILINEAR */
+    int32_t reserved;
+    int64_t offset;                /* first texel in xtgpu_scene_desc::texels */
+} xtgpu_texture;
+
+/* A sampler: COLOR a; GRADIENT a, b (over the normalised texcoord); TEXTURE
+ * and ERP one texture; CUBEMAP six consecutive textures in CUBEMAP_FACE order
+ * (left, right, top, bottom, front, back; sampler_cubemap.h:11-19). */
+typedef struct {
+    int32_t kind;                  /* XTGPU_SAMPLER_* */
+    int32_t texture;
+    float a[3], b[3];
+} xtgpu_sampler;
+
 /* A flattened Scene.  Objects are listed in the order Scene::intersection
  * visits them (the std::map order of their ids).  Host pointers; copied. */
 typedef struct {
@@ -117,6 +141,14 @@ typedef struct {
                                       v_scale), or NULL = (0, 0), the loader's default */
     const float *tri_uvs;          /* 6 floats per triangle: texcoords of its corners (OBJ vt),
                                       or NULL = the Triangle constructor's (0,0) (1,0) (0,0) */
+    int32_t n_textures;
+    const xtgpu_texture *textures;
+    int64_t n_texels;
+    const float *texels;           /* 4 floats (r g b a) per texel */
+    const xtgpu_sampler *mat_samplers;  /* 3 per material (diffuse, specular, emissive), or
+                                           NULL = the materials' colours */
+    int32_t env_texture;           /* XTGPU_ENV_ERP: its texture; XTGPU_ENV_CUBEMAP: the first
+                                      of its six faces */
 } xtgpu_scene_desc;
 
 typedef struct xtgpu_scene xtgpu_scene;

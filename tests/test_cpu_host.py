@@ -118,3 +118,41 @@ def test_cpu_lbvh_replica_is_a_valid_karras_tree(n_sph):
         leaves = np.concatenate([~left[left < 0], ~right[right < 0]])
         assert np.array_equal(np.sort(inner), np.arange(1, n - 1))
         assert np.array_equal(np.sort(leaves), np.arange(n))
+
+
+def test_bad_textures_and_cameras_are_rejected_without_device_work():
+    """Texture tables, sampler texture indices, environment textures and camera
+    types are checked on the host before any device allocation."""
+    L = xtgpu.lib()
+    out = C.c_void_p()
+
+    def desc():
+        d = xtgpu.SceneDesc()
+        d.env_texture = -1
+        return d
+
+    texels = np.zeros((6, 4), np.float32)
+    tex = (xtgpu.Texture * 1)()
+    tex[0].width, tex[0].height, tex[0].filtering, tex[0].offset = 3, 3, 0, 0   # 9 texels > 6
+    d = desc()
+    d.n_textures, d.textures, d.n_texels = 1, C.cast(tex, C.c_void_p), 6
+    d.texels = texels.ctypes.data_as(C.c_void_p)
+    assert L.xtgpu_scene_create(C.byref(d), None, C.byref(out)) == 1
+    assert b"texture 0" in L.xtgpu_last_error()
+    tex[0].width, tex[0].height, tex[0].filtering = 2, 3, 7                      # bad filtering
+    assert L.xtgpu_scene_create(C.byref(d), None, C.byref(out)) == 1
+    tex[0].filtering = 1
+    d.env_type, d.env_texture = 4, 0                                               # cubemap needs 6
+    assert L.xtgpu_scene_create(C.byref(d), None, C.byref(out)) == 1
+    assert b"environment texture" in L.xtgpu_last_error()
+    d.env_type = 3
+    mats = (xtgpu.Material * 1)()
+    sam = (xtgpu.SamplerDesc * 3)()
+    sam[0].kind, sam[0].texture = 2, 1                                             # texture 1 of 1
+    d.n_materials, d.materials, d.mat_samplers = 1, C.cast(mats, C.c_void_p), C.cast(sam, C.c_void_p)
+    assert L.xtgpu_scene_create(C.byref(d), None, C.byref(out)) == 1
+    assert b"material sampler 0" in L.xtgpu_last_error()
+    d = desc()
+    d.camera.type = 9
+    assert L.xtgpu_scene_create(C.byref(d), None, C.byref(out)) == 1
+    assert b"camera" in L.xtgpu_last_error()

@@ -131,3 +131,18 @@ def test_aa_zero_writes_no_pixel(written):
     gpu = render_host(scn, xtgpu.STENCIL, 32, 24, 1, 1, d / "g0.bin", "--aa", "0")
     cpu = render_host(scn, xtgpu.STENCIL, 32, 24, 1, 1, d / "c0.bin", "--aa", "0", "--cpu")
     assert np.array_equal(gpu, cpu)
+
+
+@pytest.mark.parametrize("env", ["erp", "cubemap"])
+def test_textured_scene_in_host_equals_c_abi(tmp_path, env):
+    """PNG textures, filtering and flip keys, ERP / cubemap samplers and
+    environments loaded by XTracer's own loader render, through the xtcore
+    host, to the C ABI's bits for the generator's scene."""
+    spec = scenes.textured_scene(env)
+    scn = spec.write_scn(str(tmp_path))
+    for kind, spp, rdepth, aa in ((xtgpu.EMISSION, 2, 1, 2), (xtgpu.PATHTRACER, 4, 4, 1)):
+        got = render_host(scn, kind, 64, 48, spp, rdepth, tmp_path / "f.bin", "--aa", str(aa))
+        sc = xtgpu.Scene(spec)
+        ref, _ = sc.render(kind, 64, 48, spp=spp, rdepth=rdepth, seed=1, aa=aa)
+        sc.close()
+        assert np.array_equal(got, ref), NAMES[kind]

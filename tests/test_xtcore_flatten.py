@@ -98,7 +98,7 @@ TEXTURE = "          type = texture\n          source = missing.png"
 
 
 @pytest.mark.parametrize("extra, geom, sampler, why", [
-    ("", "sphere", TEXTURE, "not a solid colour"),
+    ("", "sphere", TEXTURE, "failed to load"),
 ])
 def test_unsupported_features_are_refused(tmp_path, extra, geom, sampler, why):
     scn = tmp_path / "u.scn"
@@ -143,3 +143,37 @@ def test_every_camera_type_is_flattened(cam, tmp_path):
         assert np.array_equal(d["camera_orientation"], np.float32(cam.orientation))
     if cam.type == scenes.CAM_ODS:
         assert d["camera_ipd"] == np.float32(cam.ipd)
+
+
+def _texture_of(d, idx):
+    w, h, filt, off = d["textures"][idx]
+    return d["texels"][off:off + w * h].reshape(h, w, 4), filt
+
+
+@pytest.mark.parametrize("env", ["erp", "cubemap"])
+def test_textured_scene_samplers_are_flattened(env, tmp_path):
+    """Every material's diffuse, specular and emissive sampler and the
+    environment reach the C ABI as the loader built them: kinds, colours,
+    and the texels of each texture (PNG loaded by stbi, /255, flips applied)
+    with its filtering; a cubemap's six faces in CUBEMAP_FACE order."""
+    spec = scenes.textured_scene(env)
+    d = flatten(spec, tmp_path)
+    assert d["samplers"] is not None
+    for oi in range(len(spec.obj_kind)):
+        m = spec.materials[spec.obj_material[oi]]
+        for ch, key in enumerate(("diffuse", "specular", "emissive")):
+            kind, tex, a, b = d["samplers"][3 * d["obj_material"][oi] + ch]
+            want = m.sampler(key)
+            assert kind == want.kind, (oi, key)
+            if kind in (scenes.SAMPLER_COLOR, scenes.SAMPLER_GRADIENT):
+                assert np.array_equal(a, np.float32(want.a)), (oi, key)
+            if kind == scenes.SAMPLER_GRADIENT:
+                assert np.array_equal(b, np.float32(want.b)), (oi, key)
+            for k, t in enumerate(want.textures):
+                texels, filt = _texture_of(d, tex + k)
+                assert np.array_equal(texels, t.texels()), (oi, key, k)
+                assert filt == t.filtering
+    assert d["env_type"] == (scenes.ENV_ERP if env == "erp" else scenes.ENV_CUBEMAP)
+    for k, t in enumerate(spec.env_textures):
+        texels, filt = _texture_of(d, d["env_texture"] + k)
+        assert np.array_equal(texels, t.texels()), ("env", k)

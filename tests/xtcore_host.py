@@ -48,6 +48,19 @@ def read_flat(path):
     d["camera_type"] = int(take(np.int32, 1)[0])
     d["camera_orientation"] = take(np.float32, 3)
     d["camera_ipd"], d["camera_flength"], d["camera_aperture"] = (float(v) for v in take(np.float32, 3))
+    n_tex, has_samp, d["env_texture"] = (int(v) for v in take(np.int32, 3))
+    d["textures"] = []
+    for _ in range(n_tex):
+        w, h, filt = (int(v) for v in take(np.int32, 3))
+        d["textures"].append((w, h, filt, int(take(np.int64, 1)[0])))
+    n_texels = int(take(np.int64, 1)[0])
+    d["texels"] = take(np.float32, 4 * n_texels).reshape(-1, 4)
+    d["samplers"] = None
+    if has_samp:
+        d["samplers"] = []
+        for _ in range(3 * len(d["materials"])):
+            kind, tex = (int(v) for v in take(np.int32, 2))
+            d["samplers"].append((kind, tex, take(np.float32, 3), take(np.float32, 3)))
     assert off == len(b), "trailing bytes in the flattened scene"
     return d
 

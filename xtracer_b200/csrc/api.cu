@@ -256,8 +256,40 @@ xtgpu_status xtgpu_scene_create(const xtgpu_scene_desc *d, void *stream, xtgpu_s
             set_error("xtgpu_scene_create: a primitive belongs to no object");
             return XTGPU_ERR_INVALID;
         }
-    if (d->env_type < XTGPU_ENV_NONE || d->env_type > XTGPU_ENV_GRADIENT) {
+    if (d->env_type < XTGPU_ENV_NONE || d->env_type > XTGPU_ENV_CUBEMAP) {
         set_error("xtgpu_scene_create: bad environment type");
+        return XTGPU_ERR_INVALID;
+    }
+    // textures: every texel of every texture inside texels; samplers name
+    // textures that exist (a cubemap six of them)
+    if (d->n_textures < 0 || d->n_texels < 0 || (d->n_textures && (!d->textures || !d->texels))) {
+        set_error("xtgpu_scene_create: inconsistent texture arrays");
+        return XTGPU_ERR_INVALID;
+    }
+    for (int32_t i = 0; i < d->n_textures; ++i) {
+        const xtgpu_texture &t = d->textures[i];
+        if (t.width <= 0 || t.height <= 0 || t.offset < 0 || (t.filtering != XTGPU_FILTER_NEAREST &&
+                                                              t.filtering != XTGPU_FILTER_BILINEAR) ||
+            (int64_t)t.width * t.height > d->n_texels - t.offset) {
+            set_error("xtgpu_scene_create: texture " + std::to_string(i) + " out of bounds or bad filtering");
+            return XTGPU_ERR_INVALID;
+        }
+    }
+    auto tex_ok = [&](int kind, int tex) {
+        if (kind == XTGPU_SAMPLER_TEXTURE || kind == XTGPU_SAMPLER_ERP) return tex >= 0 && tex < d->n_textures;
+        if (kind == XTGPU_SAMPLER_CUBEMAP) return tex >= 0 && (int64_t)tex + 6 <= d->n_textures;
+        return kind == XTGPU_SAMPLER_COLOR || kind == XTGPU_SAMPLER_GRADIENT;
+    };
+    if (d->mat_samplers)
+        for (int64_t i = 0; i < 3 * (int64_t)d->n_materials; ++i)
+            if (!tex_ok(d->mat_samplers[i].kind, d->mat_samplers[i].texture)) {
+                set_error("xtgpu_scene_create: material sampler " + std::to_string(i) +
+                          ": bad kind or texture index");
+                return XTGPU_ERR_INVALID;
+            }
+    if ((d->env_type == XTGPU_ENV_ERP && !tex_ok(XTGPU_SAMPLER_ERP, d->env_texture)) ||
+        (d->env_type == XTGPU_ENV_CUBEMAP && !tex_ok(XTGPU_SAMPLER_CUBEMAP, d->env_texture))) {
+        set_error("xtgpu_scene_create: environment texture out of range");
         return XTGPU_ERR_INVALID;
     }
 
@@ -304,7 +336,39 @@ xtgpu_status xtgpu_scene_create(const xtgpu_scene_desc *d, void *stream, xtgpu_s
         mats[i].reflectance = m.reflectance;
         mats[i].exponent = m.exponent;
         mats[i].ior = m.ior;
+        mats[i].textured = 0;
+        const float3 col[3] = {mats[i].diffuse, mats[i].specular, mats[i].emissive};
+        for (int ch = 0; ch < 3; ++ch) {
+            DevSampler &k = mats[i].s[ch];
+            k = DevSampler{XTGPU_SAMPLER_COLOR, -1, col[ch], make_float3(0.f, 0.f, 0.f)};
+            if (!d->mat_samplers) continue;
+            const xtgpu_sampler &x = d->mat_samplers[3 * (size_t)i + ch];
+            k.kind = x.kind;
+            k.tex = x.texture;
+            k.a = make_float3(x.a[0], x.a[1], x.a[2]);
+            k.b = make_float3(x.b[0], x.b[1], x.b[2]);
+            if (x.kind == XTGPU_SAMPLER_COLOR) {
+                // the colour replaces the material's (get_sample of the sampler)
+                (ch == 0 ? mats[i].diffuse : ch == 1 ? mats[i].specular : mats[i].emissive) = k.a;
+            } else {
+                mats[i].textured = 1;
+            }
+        }
     }
+    std::vector<DevTexture> texs((size_t)std::max(1, d->n_textures));
+    for (int32_t i = 0; i < d->n_textures; ++i)
+    {
+        const uint64_t W = (uint64_t)d->textures[i].width, Hh = (uint64_t)d->textures[i].height;
+        texs[i] = DevTexture{d->textures[i].width, d->textures[i].height, d->textures[i].filtering, 0,
+                             d->textures[i].offset, (uint32_t)((UINT64_MAX % W + 1) % W),
+                             (uint32_t)((UINT64_MAX % Hh + 1) % Hh)};
+    }
+    if ((st = dalloc(sc->textures, sizeof(DevTexture) * texs.size(), s)) != XTGPU_OK) return fail(st);
+    cudaMemcpy(sc->textures.p, texs.data(), sizeof(DevTexture) * texs.size(), cudaMemcpyHostToDevice);
+    if ((st = dalloc(sc->texels, sizeof(float4) * (size_t)std::max<int64_t>(1, d->n_texels), s)) != XTGPU_OK)
+        return fail(st);
+    if (d->n_texels)
+        cudaMemcpy(sc->texels.p, d->texels, sizeof(float4) * (size_t)d->n_texels, cudaMemcpyHostToDevice);
     std::vector<int32_t> om((size_t)std::max(1, d->n_objects));
     for (int32_t i = 0; i < d->n_objects; ++i) om[i] = d->obj_material[i];
     // texture-coordinate inputs of the uv integrator
@@ -341,6 +405,9 @@ xtgpu_status xtgpu_scene_create(const xtgpu_scene_desc *d, void *stream, xtgpu_s
     S.n_planes = d->n_planes;
     S.root = EMPTY_REF;
     S.env_type = d->env_type;
+    S.env_tex = d->env_texture;
+    S.textures = (const DevTexture *)sc->textures.p;
+    S.texels = (const float4 *)sc->texels.p;
     S.env_a = make_float3(d->env_a[0], d->env_a[1], d->env_a[2]);
     S.env_b = make_float3(d->env_b[0], d->env_b[1], d->env_b[2]);
     S.cam = make_camera(d->camera);
@@ -373,7 +440,7 @@ xtgpu_status xtgpu_scene_destroy(xtgpu_scene *sc)
 {
     if (!sc) return XTGPU_OK;
     for (HostBuf *b : {&sc->tri_v, &sc->tri_n, &sc->spheres, &sc->planes, &sc->prim_obj, &sc->obj_material,
-                       &sc->obj_uvs, &sc->tri_uv, &sc->materials, &sc->leaf_prims, &sc->nodes32, &sc->nodes8, &sc->nodesW, &sc->leafW,
+                       &sc->obj_uvs, &sc->tri_uv, &sc->materials, &sc->textures, &sc->texels, &sc->leaf_prims, &sc->nodes32, &sc->nodes8, &sc->nodesW, &sc->leafW,
                        &sc->morton, &sc->order, &sc->left, &sc->right})
         dfree(*b);
     delete sc;
@@ -388,7 +455,7 @@ xtgpu_status xtgpu_scene_device_bytes(const xtgpu_scene *sc, uint64_t *bytes)
     }
     uint64_t b = 0;
     for (const HostBuf *h : {&sc->tri_v, &sc->tri_n, &sc->spheres, &sc->planes, &sc->prim_obj, &sc->obj_material,
-                             &sc->obj_uvs, &sc->tri_uv, &sc->materials, &sc->leaf_prims, &sc->nodes32, &sc->nodes8, &sc->nodesW, &sc->leafW,
+                             &sc->obj_uvs, &sc->tri_uv, &sc->materials, &sc->textures, &sc->texels, &sc->leaf_prims, &sc->nodes32, &sc->nodes8, &sc->nodesW, &sc->leafW,
                              &sc->morton, &sc->order, &sc->left, &sc->right})
         b += h->bytes;
     *bytes = b;

@@ -13,6 +13,7 @@
 //               blinnphong.cc:34-61, emissive.cc:20-27, dielectric.cc:22-31)
 //   sampling    lib/nmath/sample.inl:28-107, in FP32
 #include <algorithm>
+#include <climits>
 #include <vector>
 
 #include "render.h"
@@ -62,8 +63,9 @@ __device__ __forceinline__ float3 cmuls(float3 a, float s) { return make_float3(
 // Camera rays in FP64, each operation rounded on its own (no contraction), as
 // the reference computes them: Perspective::get_primary_ray (perspective.cc:
 // 38-98, with the thin-lens draws of :73-95 when flength > 0), ERP (erp.cc:
-// 13-31), ODS (ods.cc:17-40) and Cubemap (cubemap.cc:21-69).  `key` and `ctr`
-// are the sample's random stream; the lens draws are its first two values.
+// 13-31), ODS (ods.cc:17-40) and Cubemap (cubemap.cc:21-69).  `seed`, `path`
+// and `ctr` are the sample's random stream; the lens draws are its first two
+// values.
 __device__ __forceinline__ double dlen3(const double t[3])
 {
     return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(t[0], t[0]), __dmul_rn(t[1], t[1])), __dmul_rn(t[2], t[2])));
@@ -83,8 +85,8 @@ __device__ __forceinline__ double dsum4(double a, double x, double b, double y, 
     return __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(a, x), __dmul_rn(b, y)), __dmul_rn(c, z)), w);
 }
 
-__device__ void camera_ray(const DevCamera &c, float x, float y, float w, float h, uint64_t key, uint32_t &ctr,
-                           float3 &o, float3 &d)
+__device__ void camera_ray(const DevCamera &c, float x, float y, float w, float h, uint64_t seed, uint64_t path,
+                           uint32_t &ctr, float3 &o, float3 &d)
 {
     double to[3] = {c.pos[0], c.pos[1], c.pos[2]}, t[3];
     if (c.type == XTGPU_CAM_ERP || c.type == XTGPU_CAM_ODS) {
@@ -147,6 +149,7 @@ __device__ void camera_ray(const DevCamera &c, float x, float y, float w, float 
             // the lens point: the camera-space direction moved within half the
             // aperture (two prng_c draws, x then y); the ray aims at the point
             // of the focal plane the undisturbed direction meets
+            const uint64_t key = path_key(seed, path);
             const double half = (double)__fdiv_rn(c.aperture, 2.f);
             double lo[3] = {dc[0], dc[1], dc[2]};
             const double u0 = (double)uniform(key, ctr), u1 = (double)uniform(key, ctr);
@@ -241,17 +244,6 @@ __device__ float3 s_lobe(float3 n, float3 dir, float e, uint64_t key, uint32_t &
     return vdotr > 0.f ? normalized(vc) : make_float3(0.f, 0.f, 0.f);
 }
 
-__device__ __forceinline__ float3 environment(const DevScene &S, float3 dir)
-{
-    if (S.env_type == XTGPU_ENV_COLOR) return S.env_a;
-    if (S.env_type == XTGPU_ENV_GRADIENT) {   // sampler_gradient.cc:11-17
-        float3 d = normalized(dir);
-        float t = 0.5f * d.y + 1.0f;
-        float3 a = cmuls(S.env_a, 1.0f - t), b = cmuls(S.env_b, t);
-        return make_float3(c0(a.x + b.x), c0(a.y + b.y), c0(a.z + b.z));
-    }
-    return make_float3(0.f, 0.f, 0.f);
-}
 
 // Hit record normal as the reference forms it: triangles the face normal (or the
 // barycentric blend of vertex normals when given, not renormalised), spheres
@@ -281,7 +273,7 @@ __device__ __forceinline__ float3 hit_normal(const DevScene &S, uint32_t prim, f
 // scene gives none, math/triangle.cc:8-13), spheres asin of the normal over the
 // u/v scale (math/sphere.cc:52-53), planes a planar map wrapped into [0,1]
 // (math/plane.cc:47-58).  Spheres and planes in FP64 like the reference.
-__device__ float2 hit_texcoord(const DevScene &S, uint32_t prim, float3 o, float3 d, float t, float bu, float bv)
+__device__ double2 hit_texcoord_d(const DevScene &S, uint32_t prim, float3 o, float3 d, float t, float bu, float bv)
 {
     if ((int)prim < S.n_tris) {
         float2 a = make_float2(0.f, 0.f), b = make_float2(1.f, 0.f), c = make_float2(0.f, 0.f);
@@ -291,8 +283,7 @@ __device__ float2 hit_texcoord(const DevScene &S, uint32_t prim, float3 o, float
             c = S.tri_uv[3 * prim + 2];
         }
         const double bw = 1.0 - (double)bu - (double)bv;
-        return make_float2((float)(a.x * bw + b.x * (double)bu + c.x * (double)bv),
-                           (float)(a.y * bw + b.y * (double)bu + c.y * (double)bv));
+        return make_double2(a.x * bw + b.x * (double)bu + c.x * (double)bv, a.y * bw + b.y * (double)bu + c.y * (double)bv);
     }
     const float2 sc = S.obj_uvs[S.prim_obj[prim]];
     const double px = (double)o.x + (double)d.x * t, py = (double)o.y + (double)d.y * t,
@@ -301,8 +292,8 @@ __device__ float2 hit_texcoord(const DevScene &S, uint32_t prim, float3 o, float
         const float4 s4 = S.spheres[prim - S.n_tris];
         const double nx = (px - s4.x) / s4.w, ny = (py - s4.y) / s4.w;
         const double PI = 3.14159265358979323846;
-        return make_float2((float)(asin(nx / (sc.x != 0.f ? (double)sc.x : 1.0)) / PI + 0.5),
-                           (float)(asin(ny / (sc.y != 0.f ? (double)sc.y : 1.0)) / PI + 0.5));
+        return make_double2(asin(nx / (sc.x != 0.f ? (double)sc.x : 1.0)) / PI + 0.5,
+                            asin(ny / (sc.y != 0.f ? (double)sc.y : 1.0)) / PI + 0.5);
     }
     const float4 pl = S.planes[prim - S.n_tris - S.n_spheres];
     const double l = sqrt((double)pl.x * pl.x + (double)pl.y * pl.y + (double)pl.z * pl.z);
@@ -319,7 +310,178 @@ __device__ float2 hit_texcoord(const DevScene &S, uint32_t prim, float3 o, float
     if (tv < -1.f) tv -= (float)(int)tv;
     if (tu < 0.f) tu = 1.f + tu;
     if (tv < 0.f) tv = 1.f + tv;
-    return make_float2((float)tu, (float)tv);
+    return make_double2(tu, tv);
+}
+
+__device__ __forceinline__ float2 hit_texcoord(const DevScene &S, uint32_t prim, float3 o, float3 d, float t,
+                                               float bu, float bv)
+{
+    const double2 tc = hit_texcoord_d(S, prim, o, d, t, bu, bv);
+    return make_float2((float)tc.x, (float)tc.y);
+}
+
+// ---------------------------------------------------------------------------
+// Samplers (sampler_*.cc) with the reference's arithmetic: every operation
+// rounded on its own, colours clamped at 0 after each step (color.inl).
+
+// the x86-64 int conversion of a float (cvttss2si): INT_MIN outside int's
+// range and for NaN
+__device__ __forceinline__ int f2i_x86(float f)
+{
+    return (f != f || f >= 2147483648.f || f < -2147483648.f) ? INT_MIN : __float2int_rz(f);
+}
+
+// Pixmap::pixel_ro (lib/nimg/pixmap.cc:44-50): coordinates clamped to the
+// last column and row
+__device__ __forceinline__ float3 texel_at(const DevScene &S, const DevTexture &t, uint64_t x, uint64_t y)
+{
+    const uint64_t nx = x >= (uint64_t)t.width ? (uint64_t)t.width - 1 : x;
+    const uint64_t ny = y >= (uint64_t)t.height ? (uint64_t)t.height - 1 : y;
+    const float4 c = __ldg(&S.texels[t.offset + (int64_t)(ny * (uint64_t)t.width + nx)]);
+    return make_float3(c.x, c.y, c.z);
+}
+
+__device__ __forceinline__ float3 cscale_rn(float3 c, float s)
+{
+    return make_float3(c0(__fmul_rn(c.x, s)), c0(__fmul_rn(c.y, s)), c0(__fmul_rn(c.z, s)));
+}
+__device__ __forceinline__ float3 cadd_rn(float3 a, float3 b)
+{
+    return make_float3(c0(__fadd_rn(a.x, b.x)), c0(__fadd_rn(a.y, b.y)), c0(__fadd_rn(a.z, b.z)));
+}
+
+// nimg::sample::nearest (lib/nimg/sample.cc:8-17): wrapped into [0, 1], then
+// (size_t)(u * (float)width); NaN converts to 2^63 on x86-64 (the last texel)
+__device__ float3 tex_nearest(const DevScene &S, const DevTexture &t, double u, double v)
+{
+    u = u < 0 ? 0.0 : (u > 1 ? __dsub_rn(u, floor(u)) : u);
+    v = v < 0 ? 0.0 : (v > 1 ? __dsub_rn(v, floor(v)) : v);
+    const double fx = __dmul_rn(u, (double)(float)t.width), fy = __dmul_rn(v, (double)(float)t.height);
+    const uint64_t x = fx == fx ? (uint64_t)fx : (1ull << 63);
+    const uint64_t y = fy == fy ? (uint64_t)fy : (1ull << 63);
+    return texel_at(S, t, x, y);
+}
+
+// ((size_t)i) % n for an int i, as the reference's `int % size_t` computes
+// it: a negative i converts to 2^64 + i.  With m = 2^64 mod n (precomputed
+// per texture) that is (m + n - (-i mod n)) mod n, all in 32 bits.
+__device__ __forceinline__ uint32_t wrap_index(int i, uint32_t n, uint32_t m)
+{
+    if (i >= 0) return (uint32_t)i % n;
+    const uint32_t a = (uint32_t)(-(int64_t)i % (int64_t)n);
+    return (uint32_t)(((uint64_t)m + n - a) % n);
+}
+
+// nimg::sample::bilinear (lib/nimg/sample.cc:19-52): int texel index modulo
+// the size_t size (a negative index wraps through 2^64), weights in float,
+// four colours scaled and summed as ColorRGBAf
+__device__ float3 tex_bilinear(const DevScene &S, const DevTexture &t, double u, double v)
+{
+    const uint32_t w = (uint32_t)t.width, h = (uint32_t)t.height;
+    const float fu = (float)__dmul_rn(u, (double)w), fv = (float)__dmul_rn(v, (double)h);
+    const int u1 = (int)wrap_index(f2i_x86(fu), w, t.wrap_w), v1 = (int)wrap_index(f2i_x86(fv), h, t.wrap_h);
+    const int u2 = (int)((uint32_t)(u1 + 1) % w), v2 = (int)((uint32_t)(v1 + 1) % h);
+    const float fru = __fsub_rn(fu, floorf(fu)), frv = __fsub_rn(fv, floorf(fv));
+    const float iu = __fsub_rn(1.f, fru), iv = __fsub_rn(1.f, frv);
+    const float w1 = __fmul_rn(iu, iv), w2 = __fmul_rn(fru, iv), w3 = __fmul_rn(iu, frv), w4 = __fmul_rn(fru, frv);
+    float3 c = cadd_rn(cscale_rn(texel_at(S, t, u1, v1), w1), cscale_rn(texel_at(S, t, u2, v1), w2));
+    c = cadd_rn(c, cscale_rn(texel_at(S, t, u1, v2), w3));
+    return cadd_rn(c, cscale_rn(texel_at(S, t, u2, v2), w4));
+}
+
+// Texture2D::sample, sampler_tex.cc:37-45
+__device__ __forceinline__ float3 tex_sample(const DevScene &S, int ti, double u, double v)
+{
+    const DevTexture t = S.textures[ti];
+    return t.filtering == XTGPU_FILTER_BILINEAR ? tex_bilinear(S, t, u, v) : tex_nearest(S, t, u, v);
+}
+
+// Vector3f::normalized (vector.inl:444-448)
+__device__ __forceinline__ void dnormalized(double &x, double &y, double &z)
+{
+    const double l = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+    if (l != 0.0) {
+        x = __ddiv_rn(x, l);
+        y = __ddiv_rn(y, l);
+        z = __ddiv_rn(z, l);
+    }
+}
+
+// ERP::sample, sampler_erp.cc:13-26 (angles rounded to float)
+__device__ float3 erp_sample(const DevScene &S, int ti, double x, double y, double z)
+{
+    dnormalized(x, y, z);
+    const float theta = (float)acos(y);
+    const float phi = (float)atan2(x, -z);
+    const float u = (float)__dadd_rn(0.5, __ddiv_rn((double)phi, 6.283185307179586232));
+    const float v = (float)__ddiv_rn((double)theta, 3.14159265358979323846);
+    return tex_sample(S, ti, u, v);
+}
+
+// Cubemap::sample, sampler_cubemap.cc:13-36: the face of the largest
+// component (CUBEMAP_FACE order: left, right, top, bottom, front, back)
+__device__ float3 cube_sample(const DevScene &S, int ti, double x, double y, double z)
+{
+    dnormalized(x, y, z);
+    int face = 2;
+    double u = 0.0, v = 0.0;
+    const double ax = fabs(x), ay = fabs(y), az = fabs(z);
+    auto half = [](double p, double q) { return __dmul_rn(__dadd_rn(__ddiv_rn(p, q), 1.0), 0.5); };
+    if (ax >= ay && ax >= az) {
+        if (x > 0.0) { face = 1; u = half(z, x); v = __dsub_rn(1.0, half(y, x)); }
+        else if (x < 0.0) { face = 0; u = half(z, x); v = half(y, x); }
+    } else if (ay >= ax && ay >= az) {
+        if (y > 0.0) { face = 2; u = half(x, y); v = __dsub_rn(1.0, half(z, y)); }
+        else if (y < 0.0) { face = 3; u = __dsub_rn(1.0, half(x, y)); v = __dsub_rn(1.0, half(z, y)); }
+    } else if (az >= ax && az >= ay) {
+        if (z > 0.0) { face = 5; u = __dsub_rn(1.0, half(x, z)); v = __dsub_rn(1.0, half(y, z)); }
+        else if (z < 0.0) { face = 4; u = __dsub_rn(1.0, half(x, z)); v = half(y, z); }
+    }
+    // u and v are floats in the reference
+    return tex_sample(S, ti + face, (double)(float)u, (double)(float)v);
+}
+
+// Gradient::sample, sampler_gradient.cc:11-17, on a direction or texcoord
+__device__ float3 gradient_sample(float3 a, float3 b, double x, double y, double z)
+{
+    dnormalized(x, y, z);
+    const float t = (float)__dadd_rn(__dmul_rn(0.5, y), 1.0);
+    return cadd_rn(cscale_rn(make_float3(c0(a.x), c0(a.y), c0(a.z)), (float)__dsub_rn(1.0, (double)t)),
+                   cscale_rn(make_float3(c0(b.x), c0(b.y), c0(b.z)), t));
+}
+
+__device__ float3 sampler_eval(const DevScene &S, const DevSampler &k, double x, double y, double z)
+{
+    switch (k.kind) {
+    case XTGPU_SAMPLER_GRADIENT: return gradient_sample(k.a, k.b, x, y, z);
+    case XTGPU_SAMPLER_TEXTURE: return tex_sample(S, k.tex, x, y);
+    case XTGPU_SAMPLER_ERP: return erp_sample(S, k.tex, x, y, z);
+    case XTGPU_SAMPLER_CUBEMAP: return cube_sample(S, k.tex, x, y, z);
+    default: return make_float3(c0(k.a.x), c0(k.a.y), c0(k.a.z));
+    }
+}
+
+// IMaterial::get_sample (material.cc:65-70) of channel ch (0 diffuse, 1
+// specular, 2 emissive) at the hit's texcoord (u, v, 0), which is formed only
+// for a textured material
+__device__ __forceinline__ float3 mat_color(const DevScene &S, const DevMaterial &M, int ch, const xtgpu_hit &h,
+                                            float3 o, float3 d)
+{
+    if (!M.textured) return ch == 0 ? M.diffuse : (ch == 1 ? M.specular : M.emissive);
+    const double2 tc = hit_texcoord_d(S, h.prim, o, d, h.t, h.u, h.v);
+    return sampler_eval(S, M.s[ch], tc.x, tc.y, 0.0);
+}
+
+// Scene::sample_environment (scene.cc:142-145): black without an environment
+__device__ float3 environment(const DevScene &S, float3 dir)
+{
+    switch (S.env_type) {
+    case XTGPU_ENV_COLOR: return S.env_a;
+    case XTGPU_ENV_GRADIENT: return gradient_sample(S.env_a, S.env_b, dir.x, dir.y, dir.z);
+    case XTGPU_ENV_ERP: return erp_sample(S, S.env_tex, dir.x, dir.y, dir.z);
+    case XTGPU_ENV_CUBEMAP: return cube_sample(S, S.env_tex, dir.x, dir.y, dir.z);
+    default: return make_float3(0.f, 0.f, 0.f);
+    }
 }
 
 // Pixel of the k-th pixel slot of a job.  With tiles, slots run through
@@ -392,11 +554,12 @@ __global__ void k_camera(const DevJob *__restrict__ jobs, const DevScene *__rest
             cx = (float)__dadd_rn(__dadd_rn((double)x, __dmul_rn((double)(gi % J.aa), (double)sub)), (double)off);
             cy = (float)__dadd_rn(__dadd_rn((double)y, __dmul_rn((double)(gi / J.aa), (double)sub)), (double)off);
         }
-        const uint64_t key = path_key(J.seed, (uint64_t)s * (uint64_t)J.width * (uint64_t)J.height +
-                                                  (uint64_t)y * (uint64_t)J.width + (uint64_t)x);
+        // the sample's random stream, keyed as in k_shade
+        const uint64_t path = (uint64_t)s * (uint64_t)J.width * (uint64_t)J.height + (uint64_t)y * (uint64_t)J.width +
+                              (uint64_t)x;
         uint32_t ctr = 0;
         float3 o, d;
-        camera_ray(scenes[J.scene].cam, cx, cy, (float)J.width, (float)J.height, key, ctr, o, d);
+        camera_ray(scenes[J.scene].cam, cx, cy, (float)J.width, (float)J.height, J.seed, path, ctr, o, d);
         q.org[0][i] = make_float4(o.x, o.y, o.z, 0.f);
         q.dir[0][i] = make_float4(d.x, d.y, d.z, INFINITY);
         q.meta[0][i] = make_uint2((uint32_t)i, (uint32_t)jn);
@@ -798,7 +961,8 @@ __global__ void __launch_bounds__(MINB > 0 ? 128 : 256, MINB > 0 ? MINB : 1)
     }
 }
 
-__global__ void k_shade(const DevJob *__restrict__ jobs, const DevScene *__restrict__ scenes, WaveQueues q, int side)
+// 64 registers: four blocks per SM, as before the samplers were added
+__global__ void __launch_bounds__(256, 4) k_shade(const DevJob *__restrict__ jobs, const DevScene *__restrict__ scenes, WaveQueues q, int side)
 {
     const int n = q.ctl[side];
     const int out = side ^ 1;
@@ -847,7 +1011,10 @@ __global__ void k_shade(const DevJob *__restrict__ jobs, const DevScene *__restr
             }
             case XTGPU_EMISSION: {  // the hit material's emissive colour (emission/integrator.cc:27-33)
                 float3 e = make_float3(0.f, 0.f, 0.f);
-                if (hit) e = S.materials[S.obj_material[S.prim_obj[h.prim]]].emissive;
+                if (hit) {
+                    const DevMaterial &M = S.materials[S.obj_material[S.prim_obj[h.prim]]];
+                    e = mat_color(S, M, 2, h, o, d);
+                }
                 q.contrib[lp] = make_float4(e.x, e.y, e.z, hit ? 1.f : 0.f);
                 break;
             }
@@ -893,18 +1060,18 @@ __global__ void k_shade(const DevJob *__restrict__ jobs, const DevScene *__restr
                 bool go = true;
                 if (M.type == XTGPU_LAMBERT) {
                     nd3 = normalized(s_diffuse(nrm, key, ctr));
-                    f = cmuls(M.diffuse, dot3(nrm, nd3));
+                    f = cmuls(mat_color(S, M, 0, h, o, d), dot3(nrm, nd3));
                 } else if (M.type == XTGPU_PHONG || M.type == XTGPU_BLINNPHONG) {
                     float k = uniform(key, ctr);
                     if (k > M.reflectance) {
-                        f = M.diffuse;
+                        f = mat_color(S, M, 0, h, o, d);
                         nd3 = s_diffuse(nrm, key, ctr);
                     } else {
-                        f = M.specular;
+                        f = mat_color(S, M, 1, h, o, d);
                         nd3 = s_lobe(nrm, make_float3(-d.x, -d.y, -d.z), M.exponent, key, ctr);
                     }
                 } else if (M.type == XTGPU_EMISSIVE) {
-                    float3 L = cmul(Pp, cmul(Ii, M.emissive));
+                    float3 L = cmul(Pp, cmul(Ii, mat_color(S, M, 2, h, o, d)));
                     q.contrib[lp] = make_float4(L.x, L.y, L.z, 1.f);
                     go = false;
                 } else {

@@ -35,10 +35,26 @@ __host__ __device__ inline int32_t leaf_ref(uint32_t first, uint32_t count)
 __host__ __device__ inline uint32_t leaf_first(int32_t ref) { return ((uint32_t)~ref) >> LEAF_BITS; }
 __host__ __device__ inline uint32_t leaf_count(int32_t ref) { return ((uint32_t)~ref) & MAX_LEAF; }
 
+// A sampler (xtgpu_sampler): kind, texture index, colours a and b.
+struct DevSampler {
+    int kind, tex;
+    float3 a, b;
+};
+
+struct DevTexture {
+    int32_t width, height, filtering, reserved;
+    int64_t offset;
+    uint32_t wrap_w, wrap_h;   // 2^64 mod width, 2^64 mod height (bilinear index wrap)
+};
+
+// diffuse, specular and emissive are the colours of COLOR samplers; a
+// textured material (any other sampler kind) samples s[] at the hit texcoord.
 struct DevMaterial {
     int type;
     float3 diffuse, specular, emissive;
     float reflectance, exponent, ior;
+    int textured;
+    DevSampler s[3];      // diffuse, specular, emissive
 };
 
 // Camera basis precomputed on the host in FP64 exactly as
@@ -79,6 +95,9 @@ struct DevScene {
     int32_t rootW;             // 0, or -1 for an empty scene
     int32_t env_type;
     float3 env_a, env_b;
+    int32_t env_tex;           // XTGPU_ENV_ERP / XTGPU_ENV_CUBEMAP: its (first) texture
+    const DevTexture *textures;
+    const float4 *texels;
     DevCamera cam;
 };
 
@@ -93,6 +112,7 @@ struct HostBuf {
 struct xtgpu_scene {
     xtg::DevScene dev{};
     xtg::HostBuf tri_v, tri_n, spheres, planes, prim_obj, obj_material, materials, obj_uvs, tri_uv;
+    xtg::HostBuf textures, texels;
     xtg::HostBuf leaf_prims, nodes32, nodes8, nodesW, leafW;
     xtg::HostBuf morton, order, left, right;   // kept for xtgpu_bvh_export
     int64_t n_prims = 0;

@@ -11,6 +11,9 @@
 #include <xtcore/material.h>
 #include <xtcore/sampler_col.h>
 #include <xtcore/sampler_gradient.h>
+#include <xtcore/sampler_tex.h>
+#include <xtcore/sampler_erp.h>
+#include <xtcore/sampler_cubemap.h>
 #include <xtcore/camera/perspective.h>
 #include <xtcore/camera/erp.h>
 #include <xtcore/camera/ods.h>
@@ -46,6 +49,29 @@ struct OctreeItemsTag {
 template struct Expose<MeshOctreeTag, &xtcore::surface::Mesh::m_octree>;
 template struct Expose<OctreeItemsTag, &TriOctree::m_items>;
 
+// The texture samplers keep their images private (sampler_tex.h:34-35,
+// sampler_erp.h:20, sampler_cubemap.h:30); reached the same way.
+struct TexMapTag {
+    typedef nimg::Pixmap xtcore::sampler::Texture2D::*type;
+    friend type member_of(TexMapTag);
+};
+struct TexFilterTag {
+    typedef xtcore::sampler::FILTERING xtcore::sampler::Texture2D::*type;
+    friend type member_of(TexFilterTag);
+};
+struct ErpTexTag {
+    typedef xtcore::sampler::Texture2D xtcore::sampler::ERP::*type;
+    friend type member_of(ErpTexTag);
+};
+struct CubeTexTag {
+    typedef xtcore::sampler::Texture2D (xtcore::sampler::Cubemap::*type)[6];
+    friend type member_of(CubeTexTag);
+};
+template struct Expose<TexMapTag, &xtcore::sampler::Texture2D::m_map>;
+template struct Expose<TexFilterTag, &xtcore::sampler::Texture2D::m_filtering>;
+template struct Expose<ErpTexTag, &xtcore::sampler::ERP::m_texture>;
+template struct Expose<CubeTexTag, &xtcore::sampler::Cubemap::m_textures>;
+
 const TriItems &mesh_triangles(const xtcore::surface::Mesh *m)
 {
     const TriOctree &oct = m->*member_of(MeshOctreeTag());
@@ -74,25 +100,110 @@ void put3(std::vector<float> &v, const nmath::Vector3f &p)
     v.push_back((float)p.z);
 }
 
-// A material sampler as a constant colour: absent samplers are black, as in
-// IMaterial::get_sample (material.cc:65-70); only SolidColor samplers are
-// constant, any other kind (textures, cubemaps) fails the flattening.
-bool solid_colour(const xtcore::asset::IMaterial *m, const char *name, float out[3], std::string &err)
+// Appends the images of n textures (a cubemap's six faces in CUBEMAP_FACE
+// order) as consecutive xtgpu_textures; the same sampler object is stored once.
+bool add_textures(xtcore::integrator::gpu::FlatScene &F, const void *owner,
+                  const xtcore::sampler::Texture2D *const *tex, int n, int32_t &first, std::string &err)
 {
-    out[0] = out[1] = out[2] = 0.f;
-    for (size_t i = 0; i < m->get_sampler_count(); ++i) {
-        std::string n;
-        xtcore::sampler::ISampler *s = const_cast<xtcore::asset::IMaterial *>(m)->get_sampler_by_index(i, &n);
-        if (n != name) continue;
-        if (!dynamic_cast<xtcore::sampler::SolidColor *>(s)) {
-            err = std::string("material sampler '") + name + "' is not a solid colour";
+    auto it = F.tex_index.find(owner);
+    if (it != F.tex_index.end()) {
+        first = it->second;
+        return true;
+    }
+    first = (int32_t)F.textures.size();
+    for (int k = 0; k < n; ++k) {
+        const nimg::Pixmap &pm = tex[k]->*member_of(TexMapTag());
+        if (pm.width() == 0 || pm.height() == 0) {
+            err = "a texture failed to load (empty image)";
             return false;
         }
-        nimg::ColorRGBf c = s->sample(nmath::Vector3f(0, 0, 0));
-        out[0] = c.r();
-        out[1] = c.g();
-        out[2] = c.b();
-        return true;
+        xtgpu_texture t = xtgpu_texture();
+        t.width = (int32_t)pm.width();
+        t.height = (int32_t)pm.height();
+        t.filtering = tex[k]->*member_of(TexFilterTag()) == xtcore::sampler::FILTERING_BILINEAR
+                          ? XTGPU_FILTER_BILINEAR : XTGPU_FILTER_NEAREST;
+        t.offset = (int64_t)(F.texels.size() / 4);
+        for (size_t y = 0; y < pm.height(); ++y)
+            for (size_t x = 0; x < pm.width(); ++x) {
+                const nimg::ColorRGBAf &c = pm.pixel_ro(x, y);
+                F.texels.push_back(c.r());
+                F.texels.push_back(c.g());
+                F.texels.push_back(c.b());
+                F.texels.push_back(c.a());
+            }
+        F.textures.push_back(t);
+    }
+    F.tex_index[owner] = first;
+    return true;
+}
+
+// A sampler (sampler_*.h) as the C ABI's xtgpu_sampler.
+bool sampler_of(xtcore::integrator::gpu::FlatScene &F, xtcore::sampler::ISampler *s, xtgpu_sampler &out,
+                std::string &err)
+{
+    using namespace xtcore::sampler;
+    out = xtgpu_sampler();
+    out.kind = XTGPU_SAMPLER_COLOR;
+    out.texture = -1;
+    if (!s) {
+        // a texture that failed to load leaves a null sampler (parseutil.cc:
+        // 492-496), which the CPU integrators would dereference
+        err = "a material sampler failed to load";
+        return false;
+    }
+    if (SolidColor *c = dynamic_cast<SolidColor *>(s)) {
+        nimg::ColorRGBf v = c->sample(nmath::Vector3f(0, 0, 0));
+        out.a[0] = v.r(); out.a[1] = v.g(); out.a[2] = v.b();
+    } else if (Gradient *g = dynamic_cast<Gradient *>(s)) {
+        out.kind = XTGPU_SAMPLER_GRADIENT;
+        out.a[0] = g->a.r(); out.a[1] = g->a.g(); out.a[2] = g->a.b();
+        out.b[0] = g->b.r(); out.b[1] = g->b.g(); out.b[2] = g->b.b();
+    } else if (Texture2D *t = dynamic_cast<Texture2D *>(s)) {
+        out.kind = XTGPU_SAMPLER_TEXTURE;
+        const Texture2D *p = t;
+        return add_textures(F, s, &p, 1, out.texture, err);
+    } else if (ERP *e = dynamic_cast<ERP *>(s)) {
+        out.kind = XTGPU_SAMPLER_ERP;
+        const Texture2D *p = &(e->*member_of(ErpTexTag()));
+        return add_textures(F, s, &p, 1, out.texture, err);
+    } else if (Cubemap *cb = dynamic_cast<Cubemap *>(s)) {
+        out.kind = XTGPU_SAMPLER_CUBEMAP;
+        Texture2D (&faces)[6] = cb->*member_of(CubeTexTag());
+        const Texture2D *p[6] = {&faces[0], &faces[1], &faces[2], &faces[3], &faces[4], &faces[5]};
+        return add_textures(F, s, p, 6, out.texture, err);
+    } else {
+        err = "unknown sampler class";
+        return false;
+    }
+    return true;
+}
+
+// The material's diffuse, specular and emissive samplers (absent = black, as
+// IMaterial::get_sample returns, material.cc:65-70), appended to F.samplers;
+// colour samplers also fill the material's colours.
+bool samplers_of(xtcore::integrator::gpu::FlatScene &F, const xtcore::asset::IMaterial *m, xtgpu_material &gm,
+                 std::string &err)
+{
+    static const char *names[3] = {MAT_SAMPLER_DIFFUSE, MAT_SAMPLER_SPECULAR, MAT_SAMPLER_EMISSIVE};
+    float *colours[3] = {gm.diffuse, gm.specular, gm.emissive};
+    for (int ch = 0; ch < 3; ++ch) {
+        xtgpu_sampler k = xtgpu_sampler();
+        k.texture = -1;
+        for (size_t i = 0; m && i < m->get_sampler_count(); ++i) {
+            std::string n;
+            xtcore::sampler::ISampler *s = const_cast<xtcore::asset::IMaterial *>(m)->get_sampler_by_index(i, &n);
+            if (n != names[ch]) continue;
+            if (!sampler_of(F, s, k, err)) {
+                err = std::string("material sampler '") + names[ch] + "': " + err;
+                return false;
+            }
+            break;
+        }
+        if (k.kind == XTGPU_SAMPLER_COLOR)
+            for (int c = 0; c < 3; ++c) colours[ch][c] = k.a[c];
+        else
+            F.has_textures = true;
+        F.samplers.push_back(k);
     }
     return true;
 }
@@ -110,9 +221,6 @@ bool material_of(const xtcore::asset::IMaterial *m, xtgpu_material &out, std::st
         err = "unknown material class";
         return false;
     }
-    if (!solid_colour(m, MAT_SAMPLER_DIFFUSE, out.diffuse, err)) return false;
-    if (!solid_colour(m, MAT_SAMPLER_SPECULAR, out.specular, err)) return false;
-    if (!solid_colour(m, MAT_SAMPLER_EMISSIVE, out.emissive, err)) return false;
     out.reflectance = m->get_scalar(MAT_SCALART_REFLECTANCE);
     out.exponent = m->get_scalar(MAT_SCALART_EXPONENT);
     out.ior = m->get_scalar(MAT_SCALART_IOR);
@@ -190,7 +298,9 @@ xtgpu_status flatten(xtcore::Scene &scene, HASH_UINT64 camera, FlatScene &F, std
             xtgpu_material gm = xtgpu_material();
             gm.type = XTGPU_LAMBERT;
             auto ms = scene.m_materials.find(obj->material);
-            if (ms != scene.m_materials.end() && ms->second && !material_of(ms->second, gm, err)) return XTGPU_ERR_INVALID;
+            const xtcore::asset::IMaterial *mat = ms != scene.m_materials.end() ? ms->second : 0;
+            if (mat && !material_of(mat, gm, err)) return XTGPU_ERR_INVALID;
+            if (!samplers_of(F, mat, gm, err)) return XTGPU_ERR_INVALID;
             mi = (int32_t)F.materials.size();
             F.materials.push_back(gm);
             mat_index[obj->material] = mi;
@@ -226,6 +336,7 @@ xtgpu_status flatten(xtcore::Scene &scene, HASH_UINT64 camera, FlatScene &F, std
 
     // environment (Scene::sample_environment, scene.cc:142-145)
     d.env_type = XTGPU_ENV_NONE;
+    d.env_texture = -1;
     if (scene.m_environment) {
         if (xtcore::sampler::Gradient *gr = dynamic_cast<xtcore::sampler::Gradient *>(scene.m_environment)) {
             d.env_type = XTGPU_ENV_GRADIENT;
@@ -235,10 +346,22 @@ xtgpu_status flatten(xtcore::Scene &scene, HASH_UINT64 camera, FlatScene &F, std
             d.env_type = XTGPU_ENV_COLOR;
             nimg::ColorRGBf c = scene.m_environment->sample(nmath::Vector3f(0, 0, 0));
             d.env_a[0] = c.r(); d.env_a[1] = c.g(); d.env_a[2] = c.b();
+        } else if (dynamic_cast<xtcore::sampler::ERP *>(scene.m_environment) ||
+                   dynamic_cast<xtcore::sampler::Cubemap *>(scene.m_environment)) {
+            xtgpu_sampler k;
+            if (!sampler_of(F, scene.m_environment, k, err)) return fail(std::string("environment: ") + err);
+            d.env_type = k.kind == XTGPU_SAMPLER_ERP ? XTGPU_ENV_ERP : XTGPU_ENV_CUBEMAP;
+            d.env_texture = k.texture;
+            F.has_textures = true;
         } else {
             return fail("unsupported environment sampler");
         }
     }
+    d.n_textures = (int32_t)F.textures.size();
+    d.textures = F.textures.data();
+    d.n_texels = (int64_t)(F.texels.size() / 4);
+    d.texels = F.texels.data();
+    d.mat_samplers = F.has_textures ? F.samplers.data() : 0;
 
     // camera: Perspective (with depth of field when flength > 0,
     // camera/perspective.cc:38-98), ERP (erp.cc:13-31), ODS (ods.cc:17-40) or

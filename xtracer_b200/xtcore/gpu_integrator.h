@@ -16,8 +16,9 @@
 //
 // Supported: perspective (with depth of field), ERP, ODS and cubemap cameras
 // (a cubemap's height a multiple of 6), spheres (and points, which the loader
-// makes spheres of radius 0), planes, triangles, meshes, solid-colour material
-// samplers, no / solid-colour / gradient environment, any aa with the grid
+// makes spheres of radius 0), planes, triangles, meshes, colour, gradient,
+// texture, ERP and cubemap material samplers, no / colour / gradient / ERP /
+// cubemap environment, any aa with the grid
 // sample distribution (aa <= 1 with the random one).  Anything else makes the
 // frame fail: status() and error() say why, the tiles stay as tile->init()
 // left them, and a warning goes to xtcore's log.  The depth-of-field lens
@@ -25,6 +26,7 @@
 #ifndef XTGPU_XTCORE_GPU_INTEGRATOR_H
 #define XTGPU_XTCORE_GPU_INTEGRATOR_H
 
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -45,6 +47,11 @@ struct FlatScene {
     std::vector<float> spheres, planes, tris, tri_normals;
     std::vector<float> obj_uv_scale, tri_uvs;   // 2 per object, 6 per triangle
     std::vector<xtgpu_material> materials;
+    std::vector<xtgpu_texture> textures;
+    std::vector<float> texels;                 // 4 per texel
+    std::vector<xtgpu_sampler> samplers;       // 3 per material
+    std::map<const void *, int32_t> tex_index; // sampler object -> its first texture
+    bool has_textures = false;                 // a non-colour sampler is used
     bool has_normals = false;
     bool has_uvs = false;     // a triangle's texcoords differ from the constructor's
     xtgpu_scene_desc desc;

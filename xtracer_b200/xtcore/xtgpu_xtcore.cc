@@ -71,7 +71,10 @@ void put(FILE *f, const T *p, size_t n)
 // per material int32 type + float32 diffuse[3] specular[3] emissive[3]
 // reflectance exponent ior; float32 env_a[3] env_b[3]; float32 camera
 // position[3] target[3] up[3] fov; int32 camera type; float32 orientation[3]
-// ipd flength aperture.
+// ipd flength aperture; int32 n_textures, has_samplers, env_texture; per
+// texture int32 width height filtering, int64 offset; int64 n_texels; float32
+// texels [4n]; when has_samplers, per material 3 x (int32 kind texture,
+// float32 a[3] b[3]).
 int write_flat(const xtcore::integrator::gpu::FlatScene &F, const char *out)
 {
     const xtgpu_scene_desc &d = F.desc;
@@ -109,6 +112,23 @@ int write_flat(const xtcore::integrator::gpu::FlatScene &F, const char *out)
     put(f, d.camera.orientation, 3);
     float lens[3] = {d.camera.ipd, d.camera.flength, d.camera.aperture};
     put(f, lens, 3);
+    int32_t th[3] = {d.n_textures, d.mat_samplers ? 1 : 0, d.env_texture};
+    put(f, th, 3);
+    for (int32_t i = 0; i < d.n_textures; ++i) {
+        int32_t t3[3] = {d.textures[i].width, d.textures[i].height, d.textures[i].filtering};
+        put(f, t3, 3);
+        put(f, &d.textures[i].offset, 1);
+    }
+    put(f, &d.n_texels, 1);
+    put(f, d.texels, 4 * (size_t)d.n_texels);
+    if (d.mat_samplers)
+        for (int32_t i = 0; i < 3 * d.n_materials; ++i) {
+            const xtgpu_sampler &k = d.mat_samplers[i];
+            int32_t kt[2] = {k.kind, k.texture};
+            put(f, kt, 2);
+            put(f, k.a, 3);
+            put(f, k.b, 3);
+        }
     fclose(f);
     return 0;
 }

@@ -49,6 +49,15 @@ class CameraDesc(C.Structure):
                 ("aperture", C.c_float)]
 
 
+class Texture(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("filtering", C.c_int32), ("reserved", C.c_int32),
+                ("offset", C.c_int64)]
+
+
+class SamplerDesc(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("texture", C.c_int32), ("a", C.c_float * 3), ("b", C.c_float * 3)]
+
+
 class SceneDesc(C.Structure):
     _fields_ = [("n_objects", C.c_int32), ("obj_kind", C.c_void_p), ("obj_first", C.c_void_p),
                 ("obj_count", C.c_void_p), ("obj_material", C.c_void_p),
@@ -57,7 +66,9 @@ class SceneDesc(C.Structure):
                 ("n_tris", C.c_int32), ("tris", C.c_void_p), ("tri_normals", C.c_void_p),
                 ("n_materials", C.c_int32), ("materials", C.c_void_p),
                 ("env_type", C.c_int32), ("env_a", C.c_float * 3), ("env_b", C.c_float * 3),
-                ("camera", CameraDesc), ("obj_uv_scale", C.c_void_p), ("tri_uvs", C.c_void_p)]
+                ("camera", CameraDesc), ("obj_uv_scale", C.c_void_p), ("tri_uvs", C.c_void_p),
+                ("n_textures", C.c_int32), ("textures", C.c_void_p), ("n_texels", C.c_int64),
+                ("texels", C.c_void_p), ("mat_samplers", C.c_void_p), ("env_texture", C.c_int32)]
 
 
 class BvhOpts(C.Structure):
@@ -256,6 +267,27 @@ class Scene:
             d.obj_uv_scale = arr(spec.obj_uv_scale.reshape(-1), np.float32)
         if getattr(spec, "tri_uvs", None) is not None:
             d.tri_uvs = arr(spec.tri_uvs.reshape(-1), np.float32)
+        d.env_texture = -1
+        if hasattr(spec, "texture_tables"):
+            # textures, texels and the materials' samplers (sampler_*.cc)
+            textures, texels, samp, env_tex = spec.texture_tables()
+            tex = (Texture * max(1, len(textures)))()
+            for i, (w, h, f, off) in enumerate(np.asarray(textures).tolist()):
+                tex[i].width, tex[i].height, tex[i].filtering, tex[i].offset = int(w), int(h), int(f), int(off)
+            sam = (SamplerDesc * max(1, 3 * len(samp)))()
+            for i, row in enumerate(samp):
+                for ch, (kind, t, a, b) in enumerate(row):
+                    k = sam[3 * i + ch]
+                    k.kind, k.texture = int(kind), int(t)
+                    k.a[:] = [float(v) for v in a]
+                    k.b[:] = [float(v) for v in b]
+            keep += [tex, sam]
+            d.n_textures = len(textures)
+            d.textures = C.cast(tex, C.c_void_p)
+            d.n_texels = int(texels.shape[0])
+            d.texels = arr(texels.reshape(-1), np.float32)
+            d.mat_samplers = C.cast(sam, C.c_void_p) if samp else None
+            d.env_texture = env_tex
         h = C.c_void_p()
         check(lib().xtgpu_scene_create(C.byref(d), stream_handle(stream), C.byref(h)))
         self.handle = h
