@@ -233,6 +233,19 @@ XTGPU_API xtgpu_status xtgpu_render(xtgpu_scene *scene, const xtgpu_render_param
 /* The same into host memory (copy included). */
 XTGPU_API xtgpu_status xtgpu_render_host(xtgpu_scene *scene, const xtgpu_render_params *params, float *rgba_host,
                                uint64_t *rays_traced, void *stream);
+/* The depth integrator recording its raygraph (depth/integrator.cc:43-51),
+ * which the GUI exports as PLY: params->integrator must be XTGPU_DEPTH.
+ * raygraph_dev receives 10 floats per sample: the ray origin, the hit point
+ * ((0,0,0) on a miss) and the pixel's RGBA after the sample; rectangle pixels
+ * row-major, each pixel's aa^2 x spp samples in order. */
+XTGPU_API xtgpu_status xtgpu_render_raygraph(xtgpu_scene *scene, const xtgpu_render_params *params, float *rgba_dev,
+                                             float *raygraph_dev, uint64_t *rays_traced, void *stream);
+XTGPU_API xtgpu_status xtgpu_render_raygraph_host(xtgpu_scene *scene, const xtgpu_render_params *params,
+                                                  float *rgba_host, float *raygraph_host, uint64_t *rays_traced,
+                                                  void *stream);
+/* raygraph::write (util/raygraph.cc:8-75): n_paths two-vertex paths as ASCII
+ * PLY, records (10 floats each, as above) in the order they are listed. */
+XTGPU_API xtgpu_status xtgpu_write_raygraph_ply(const char *path, int64_t n_paths, const float *records);
 
 /* xtgpu_render for one rectangle without allocating any memory.  No
  * counterpart in the reference.  For callers that cannot allocate device

@@ -97,6 +97,8 @@ def lib():
         L.xo_scene_destroy.argtypes = [C.c_void_p]
         L.xo_trace.argtypes = [C.c_void_p, C.c_int64] + [C.c_void_p] * 8
         L.xo_camera_ray.argtypes = [C.c_void_p] * 3 + [C.c_float] * 5 + [C.c_void_p] * 2
+        L.xo_render_raygraph.argtypes = [C.c_void_p, C.POINTER(XoRenderParams), C.c_int64, C.c_void_p,
+                                         C.c_void_p, C.c_void_p, C.c_void_p]
         L.xo_render.argtypes = [C.c_void_p, C.POINTER(XoRenderParams), C.c_int64, C.c_void_p,
                                 C.c_void_p, C.POINTER(C.c_uint64)]
         for n in ("xo_kat_sphere", "xo_kat_plane"):
@@ -227,6 +229,52 @@ class OracleScene:
         return out, int(rays.value)
 
 
+    def render_raygraph(self, width: int, height: int, spp: int = 1, aa: int = 1, pixels: np.ndarray = None):
+        """The depth integrator's frame and raygraph records (origin, hit point,
+        colour after the sample: 10 per sample, pixels in the given order)."""
+        pixels = np.ascontiguousarray(pixels, np.int32).reshape(-1, 2)
+        p = XoRenderParams(DEPTH, width, height, spp, 1, aa, 100.0, 1)
+        out = np.zeros((pixels.shape[0], 4), np.float32)
+        n = pixels.shape[0] * max(aa, 1) ** 2 * spp
+        rec = np.zeros((n, 10), np.float64)
+        rays = C.c_uint64(0)
+        lib().xo_render_raygraph(self.handle, C.byref(p), pixels.shape[0], _ptr(pixels), _ptr(out), _ptr(rec),
+                                 C.byref(rays))
+        return out, rec
+
+
+def raygraph_pixel_order(width: int, height: int, tile_size: int = 32) -> np.ndarray:
+    """Pixels in the order the reference's raygraph lists their samples: tiles
+    of segment_framebuffer (tile.cc:67-94, row by row), and inside a tile the
+    order antialiasing::produce queues them (aa.cc:55-58: column by column)."""
+    out = []
+    for y0 in range(0, height, tile_size):
+        for x0 in range(0, width, tile_size):
+            for x in range(x0, min(x0 + tile_size, width)):
+                for y in range(y0, min(y0 + tile_size, height)):
+                    out.append((x, y))
+    return np.array(out, np.int32)
+
+
+def raygraph_ply(records) -> str:
+    """raygraph::write (util/raygraph.cc:8-75) of two-sample paths: the origin
+    with the default colour (0, 0, 0) and the hit point with the pixel's colour;
+    numbers as an ostream prints them (6 significant digits, %g)."""
+    rec = np.asarray(records, np.float64).reshape(-1, 10)
+    n = rec.shape[0]
+    g = lambda v: "%g" % v
+    head = ["ply", "format ascii 1.0", "comment object: A single line", "element vertex %d" % (2 * n),
+            "property float x", "property float y", "property float z", "property float red",
+            "property float green", "property float blue", "element edge %d" % n, "property int vertex1",
+            "property int vertex2", "end_header"]
+    lines = []
+    for r in rec.tolist():
+        lines.append("%s %s %s 0 0 0" % (g(r[0]), g(r[1]), g(r[2])))
+        lines.append("%s %s %s %s %s %s" % (g(r[3]), g(r[4]), g(r[5]), g(r[6]), g(r[7]), g(r[8])))
+    edges = ["%d %d" % (2 * k, 2 * k + 1) for k in range(n)]
+    return "\n".join(head + lines + edges) + "\n"
+
+
 def camera_rays(spec, width: int, height: int, pixels: np.ndarray):
     """Pixel-centre primary rays (x+0.5, y+0.5) in FP64."""
     pixels = np.asarray(pixels).reshape(-1, 2)
@@ -259,10 +307,12 @@ def ref_available() -> bool:
 
 
 def ref_render(scn: str, integrator: str, width: int, height: int, spp: int = 1, aa: int = 1, rdepth: int = 4,
-               threads: int = 1, seed: int = 1, tiles=None, ao_max_distance: float = None, workdir: str = "/tmp"):
+               threads: int = 1, seed: int = 1, tiles=None, ao_max_distance: float = None, workdir: str = "/tmp",
+               raygraph: str = None):
     """Runs the reference integrator through IIntegrator::render on the given tiles
-    ((x0,y0,x1,y1) list, or None for the full frame).  Returns (pixels xy, rgba,
-    stats dict with render_s / rays / threads)."""
+    ((x0,y0,x1,y1) list, or None for 32-pixel tiles over the frame).  Returns
+    (pixels xy, rgba, stats dict with render_s / rays / threads).  raygraph: a
+    path to write the tiles' raygraph to as PLY (the GUI's export)."""
     import json
     import tempfile
     fd, out = tempfile.mkstemp(suffix=".bin", dir=workdir)
@@ -274,8 +324,10 @@ def ref_render(scn: str, integrator: str, width: int, height: int, spp: int = 1,
             fh.write("".join("%d %d %d %d\n" % tuple(t) for t in tiles))
     cmd = [REF_BIN, "render", scn, integrator, str(width), str(height), str(spp), str(aa), str(rdepth),
            str(threads), str(seed), tfile, out]
-    if ao_max_distance is not None:
-        cmd.append(repr(float(ao_max_distance)))
+    if ao_max_distance is not None or raygraph:
+        cmd.append(repr(float(ao_max_distance if ao_max_distance is not None else 100.0)))
+    if raygraph:
+        cmd.append(raygraph)
     env = dict(os.environ)
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)

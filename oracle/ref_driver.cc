@@ -49,6 +49,7 @@
 #include <xtcore/sampler_tex.h>
 #include <xtcore/sampler_erp.h>
 #include <xtcore/sampler_cubemap.h>
+#include <xtcore/util/raygraph.h>
 #include <xtcore/material/lambert.h>
 #include <xtcore/material/phong.h>
 #include <xtcore/material/blinnphong.h>
@@ -165,6 +166,7 @@ static int mode_render(int argc, char **argv)
     g_fixed_time = (time_t)atoll(argv[10]);
     const char *tiles_path = argv[11], *out = argv[12];
     float ao_maxd = argc > 13 ? (float)atof(argv[13]) : 100.0f;
+    const char *raygraph_out = argc > 14 ? argv[14] : 0;
 
     xtcore::init();
     xtcore::render::context_t ctx;
@@ -221,6 +223,13 @@ static int mode_render(int argc, char **argv)
             }
     }
     fclose(f);
+    if (raygraph_out && strcmp(raygraph_out, "-")) {
+        // the GUI's raygraph export (gui/action.cc:65-85): the tiles' bundles
+        // in tile order, written by raygraph::write (util/raygraph.cc:8-75)
+        xtcore::raygraph::raygraph_t rg;
+        xtcore::render::assemble(rg, ctx);
+        if (xtcore::raygraph::write(raygraph_out, rg)) return 1;
+    }
     int nthr = threads ? (int)threads : omp_get_max_threads();
     printf("{\"render_s\": %.9f, \"rays\": %llu, \"pixels\": %lld, \"threads\": %d}\n",
            secs, (unsigned long long)g_rays.load(), npx, nthr);

@@ -1099,8 +1099,29 @@ static c3 pt_eval(const xo_scene *s, size_t depth, c3 in_int, v3 o, v3 d, rng_t 
     return environment(&s->d, d);
 }
 
+static int render_impl(const xo_scene *s, const xo_render_params *p, int64_t npix, const int32_t *px,
+                       float *rgba, uint64_t *rays, double *raygraph);
+
 int xo_render(const xo_scene *s, const xo_render_params *p, int64_t npix, const int32_t *px,
               float *rgba, uint64_t *rays)
+{
+    return render_impl(s, p, npix, px, rgba, rays, NULL);
+}
+
+/* The depth integrator with the raygraph it records (depth/integrator.cc:
+ * 43-51): per sample, in pixel then sample order, the ray origin, the hit
+ * point ((0,0,0) on a miss: Scene::intersection copies a default record,
+ * scene.cc:212) and the pixel's colour after the sample: 10 doubles. */
+int xo_render_raygraph(const xo_scene *s, const xo_render_params *p, int64_t npix, const int32_t *px,
+                       float *rgba, double *raygraph, uint64_t *rays)
+{
+    xo_render_params q = *p;
+    q.integrator = XO_DEPTH;
+    return render_impl(s, &q, npix, px, rgba, rays, raygraph);
+}
+
+static int render_impl(const xo_scene *s, const xo_render_params *p, int64_t npix, const int32_t *px,
+                       float *rgba, uint64_t *rays, double *raygraph)
 {
     const xo_scene_desc *D = &s->d;
     uint64_t nr = 0;
@@ -1139,13 +1160,20 @@ int xo_render(const xo_scene *s, const xo_render_params *p, int64_t npix, const 
             } else if (p->integrator == XO_DEPTH) {     /* depth/integrator.cc:15-54 */
                 ++nr;
                 float depth = 0.f;
-                if (scene_hit(s, O, Dd, &h, &oi, &pi)) {
+                const int dhit = scene_hit(s, O, Dd, &h, &oi, &pi);
+                if (dhit) {
                     depth = (float)(1. / log(length(sub(O, h.point))));
                     depth = (float)(col[0] + depth * weight);
                     col[0] = col[1] = col[2] = clamp0(depth);
                     col[3] = 1;
                 }
                 col[3] = 1;
+                if (raygraph) {
+                    double *rg = raygraph + 10 * (i * (int64_t)L * L * p->spp + si);
+                    rg[0] = O.x; rg[1] = O.y; rg[2] = O.z;
+                    rg[3] = dhit ? h.point.x : 0.0; rg[4] = dhit ? h.point.y : 0.0; rg[5] = dhit ? h.point.z : 0.0;
+                    for (int k = 0; k < 4; ++k) rg[6 + k] = col[k];
+                }
             } else if (p->integrator == XO_AO) {        /* ao/integrator.cc:14-52 */
                 v3 acc = V(col[0], col[1], col[2]);
                 float w = 1.0f;

@@ -125,6 +125,11 @@ typedef struct {
  * per listed pixel; *rays = number of Scene::intersection calls. */
 int xo_render(const xo_scene *s, const xo_render_params *p, int64_t npix, const int32_t *px,
               float *rgba, uint64_t *rays);
+/* The depth integrator (whatever p->integrator says) recording its raygraph:
+ * 10 doubles per sample (origin, hit point, colour after the sample), pixels
+ * in px order, each pixel's samples in order. */
+int xo_render_raygraph(const xo_scene *s, const xo_render_params *p, int64_t npix, const int32_t *px,
+                       float *rgba, double *raygraph, uint64_t *rays);
 
 /* Known-answer hooks for single reference functions.  `table` holds libc rand()
  * values (consumed in order) and rand_max their RAND_MAX. */

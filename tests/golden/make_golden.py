@@ -26,7 +26,10 @@ these fixtures are what pins the oracle restatement (oracle/xtoracle.c):
               flipped), ERP and Cubemap samples on PNG files the reference
               loads, and frames of textured scenes with ERP and cubemap
               environments: emission and depth-1 pathtracer (deterministic)
-              and depth-4 pathtracer at four seeds (`--textures`).
+              and depth-4 pathtracer at four seeds (`--textures`);
+* raygraph.npz  the depth integrator's raygraph exported as PLY the way the GUI
+              does it (render::assemble + raygraph::write), with the frame
+              (`--raygraph`).
 
 Run here (needs the reference sources and oracle/_ref/xtref):
     make -f oracle/ref.mk REF=<xtracer source tree> -j8
@@ -386,6 +389,24 @@ def make_textures(work, rng):
     print("render_textures.npz", sorted(rend))
 
 
+def raygraph_case():
+    """(scene, width, height, spp, aa) of the raygraph fixture: partial tiles,
+    grid anti-aliasing, hits and misses."""
+    return scenes.spheres_scene(16, seed=1, name="raygraph"), 40, 24, 1, 2
+
+
+def make_raygraph(work):
+    """The depth integrator's raygraph as the GUI exports it (assemble +
+    raygraph::write) from the reference's own render."""
+    spec, w, h, spp, aa = raygraph_case()
+    scn = spec.write_scn(work)
+    ply = os.path.join(work, "raygraph.ply")
+    xy, rgba, st = po.ref_render(scn, "depth", w, h, spp=spp, aa=aa, threads=1, workdir=work, raygraph=ply)
+    text = open(ply, "rb").read()
+    np.savez_compressed(os.path.join(HERE, "raygraph.npz"), ply=np.frombuffer(text, np.uint8), xy=xy, rgba=rgba)
+    print("raygraph.npz", len(text), "bytes of PLY")
+
+
 def texture_frame_size():
     return 64, 48
 
@@ -408,6 +429,9 @@ def main():
         return
     if "--cameras" in sys.argv:
         make_cameras(tempfile.mkdtemp(prefix="xtgold"), np.random.default_rng(20261204))
+        return
+    if "--raygraph" in sys.argv:
+        make_raygraph(tempfile.mkdtemp(prefix="xtgold"))
         return
     if "--textures" in sys.argv:
         make_textures(tempfile.mkdtemp(prefix="xtgold"), np.random.default_rng(20261205))

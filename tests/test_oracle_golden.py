@@ -363,3 +363,19 @@ def test_textured_pathtracer_within_reference_noise(env):
         diff = O[:, ch] - R[:, :, ch].mean(0)
         se = np.sqrt(R[:, :, ch].var(0, ddof=1).mean() / diff.size * (1 + 1.0 / n))
         assert abs(diff.mean()) < 4.5 * se + 1e-5, (ch, diff.mean(), se)
+
+
+def test_raygraph_golden():
+    """The depth integrator's raygraph (depth/integrator.cc:43-51) exported as
+    the GUI does (render::assemble, raygraph::write): the oracle's records,
+    listed in the reference's tile and produce order and printed as an ostream
+    prints them, give the reference's PLY byte for byte."""
+    import importlib.util
+    spec_ = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLD, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec_)
+    spec_.loader.exec_module(mg)
+    spec, w, h, spp, aa = mg.raygraph_case()
+    g = np.load(os.path.join(GOLD, "raygraph.npz"))
+    orc = po.OracleScene(spec, po.XO_ACCEL_OCTREE)
+    out, rec = orc.render_raygraph(w, h, spp=spp, aa=aa, pixels=po.raygraph_pixel_order(w, h))
+    assert po.raygraph_ply(rec) == g["ply"].tobytes().decode()

@@ -611,7 +611,7 @@ xtgpu_status xtgpu_render(xtgpu_scene *sc, const xtgpu_render_params *p, float *
 }  // extern "C"
 
 xtgpu_status xtg::render_impl(xtgpu_scene *sc, const xtgpu_render_params *p, float *rgba, uint64_t *rays,
-                              cudaStream_t stream, const xtgpu_tuning &T)
+                              cudaStream_t stream, const xtgpu_tuning &T, float *raygraph)
 {
     if (!sc || !p || !rgba) {
         set_error("xtgpu_render: NULL argument");
@@ -672,6 +672,7 @@ xtgpu_status xtg::render_impl(xtgpu_scene *sc, const xtgpu_render_params *p, flo
     J.bounces = bounces_of(p->integrator, p->rdepth);
     J.tile = T.tile;
     J.frame = (float4 *)rgba;
+    J.raygraph = p->integrator == XTGPU_DEPTH ? raygraph : nullptr;
     std::vector<DevJob> jobs(1, J);
     // waves of the tuned size (the shared runner may be larger from an earlier call)
     const int64_t wave = std::max<int64_t>(1, std::min<int64_t>(R->cap, cap));
@@ -692,6 +693,55 @@ xtgpu_status xtg::render_impl(xtgpu_scene *sc, const xtgpu_render_params *p, flo
 }
 
 extern "C" {
+
+xtgpu_status xtgpu_render_raygraph(xtgpu_scene *sc, const xtgpu_render_params *p, float *rgba, float *raygraph,
+                                   uint64_t *rays, void *stream)
+{
+    if (!sc || !p || !raygraph) {
+        set_error("xtgpu_render_raygraph: NULL argument");
+        return XTGPU_ERR_INVALID;
+    }
+    if (p->integrator != XTGPU_DEPTH) {
+        set_error("xtgpu_render_raygraph: the raygraph is recorded by the depth integrator only");
+        return XTGPU_ERR_INVALID;
+    }
+    return render_impl(sc, p, rgba, rays, (cudaStream_t)stream, scene_tuning(sc), raygraph);
+}
+
+xtgpu_status xtgpu_render_raygraph_host(xtgpu_scene *sc, const xtgpu_render_params *p, float *rgba_host,
+                                        float *raygraph_host, uint64_t *rays, void *stream)
+{
+    if (!sc || !p || !rgba_host || !raygraph_host) {
+        set_error("xtgpu_render_raygraph_host: NULL argument");
+        return XTGPU_ERR_INVALID;
+    }
+    const int64_t w = (p->x1 == 0 && p->y1 == 0) ? p->width : p->x1 - p->x0;
+    const int64_t h = (p->x1 == 0 && p->y1 == 0) ? p->height : p->y1 - p->y0;
+    const int64_t aa = p->aa > 1 ? p->aa : 1;
+    if (w <= 0 || h <= 0 || p->spp <= 0 || p->aa < 0 || p->aa > MAX_AA) {
+        set_error("xtgpu_render_raygraph_host: bad rectangle or samples");
+        return XTGPU_ERR_INVALID;
+    }
+    const int64_t paths = w * h * aa * aa * p->spp;
+    cudaStream_t s = (cudaStream_t)stream;
+    float *d = nullptr, *r = nullptr;
+    XTG_CUDA(cudaMallocAsync((void **)&d, sizeof(float4) * w * h, s));
+    cudaError_t e = cudaMallocAsync((void **)&r, sizeof(float) * 10 * paths, s);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(d, s);
+        return cuda_fail(e, "cudaMallocAsync", __FILE__, __LINE__);
+    }
+    xtgpu_status st = xtgpu_render_raygraph(sc, p, d, r, rays, stream);
+    if (st == XTGPU_OK) {
+        e = cudaMemcpyAsync(rgba_host, d, sizeof(float4) * w * h, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(raygraph_host, r, sizeof(float) * 10 * paths, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = cuda_fail(e, "cudaMemcpyAsync", __FILE__, __LINE__);
+    }
+    cudaFreeAsync(d, s);
+    cudaFreeAsync(r, s);
+    return st;
+}
 
 xtgpu_status xtgpu_render_host(xtgpu_scene *sc, const xtgpu_render_params *p, float *rgba_host, uint64_t *rays,
                                void *stream)

@@ -13,6 +13,8 @@
 
 #include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <string>
 #include <vector>
 
 #include "xtgpu_internal.cuh"
@@ -212,6 +214,53 @@ xtgpu_status xtgpu_save_png_host(const char *path, int32_t width, int32_t height
     if (e != cudaSuccess) return cuda_fail(e, "xtgpu_save_png_host", __FILE__, __LINE__);
     if (st != XTGPU_OK) return st;
     return xtgpu_write_png(path, width, height, host.data());
+}
+
+// raygraph::write (util/raygraph.cc:8-75) of two-sample paths: the ply header,
+// per path the origin with the default ColorRGBAf (0, 0, 0) and the hit point
+// with its colour, then one edge per path.  Positions print as the doubles the
+// reference holds (Vector3f), colours as floats, through an ostream with its
+// default format, as the reference writes them.
+xtgpu_status xtgpu_write_raygraph_ply(const char *path, int64_t n_paths, const float *records)
+{
+    if (!path || n_paths < 0 || (n_paths && !records)) {
+        set_error("xtgpu_write_raygraph_ply: bad argument");
+        return XTGPU_ERR_INVALID;
+    }
+    std::ofstream file(path);
+    if (!file) {
+        set_error(std::string("xtgpu_write_raygraph_ply: cannot open ") + path);
+        return XTGPU_ERR_INVALID;
+    }
+    file << "ply" << std::endl;
+    file << "format ascii 1.0" << std::endl;
+    file << "comment object: A single line" << std::endl;
+    file << "element vertex " << (size_t)(2 * n_paths) << std::endl;
+    file << "property float x" << std::endl;
+    file << "property float y" << std::endl;
+    file << "property float z" << std::endl;
+    file << "property float red" << std::endl;
+    file << "property float green" << std::endl;
+    file << "property float blue" << std::endl;
+    file << "element edge " << (size_t)n_paths << std::endl;
+    file << "property int vertex1" << std::endl;
+    file << "property int vertex2" << std::endl;
+    file << "end_header" << std::endl;
+    const float zero = 0.f;
+    for (int64_t i = 0; i < n_paths; ++i) {
+        const float *r = records + 10 * i;
+        file << (double)r[0] << " " << (double)r[1] << " " << (double)r[2] << " " << zero << " " << zero << " "
+             << zero << std::endl;
+        file << (double)r[3] << " " << (double)r[4] << " " << (double)r[5] << " " << r[6] << " " << r[7] << " "
+             << r[8] << std::endl;
+    }
+    for (int64_t i = 0; i < n_paths; ++i) file << (size_t)(2 * i) << " " << (size_t)(2 * i + 1) << std::endl;
+    file.close();
+    if (!file) {
+        set_error(std::string("xtgpu_write_raygraph_ply: write failed: ") + path);
+        return XTGPU_ERR_CUDA;
+    }
+    return XTGPU_OK;
 }
 
 }  // extern "C"

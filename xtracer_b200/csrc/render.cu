@@ -1022,6 +1022,15 @@ __global__ void __launch_bounds__(256, 4) k_shade(const DevJob *__restrict__ job
                 // 1 / log(|o - p|), computed in double as the reference does
                 float dv = hit ? (float)(1.0 / log((double)h.t)) : 0.f;
                 q.contrib[lp] = make_float4(dv, 0.f, 0.f, hit ? 1.f : 0.f);
+                if (J.raygraph) {
+                    // the sample's raygraph path (depth/integrator.cc:43-51): ray
+                    // origin and hit point, (0,0,0) on a miss (scene.cc:212)
+                    float *r = J.raygraph + 10 * (((fy - J.y0) * (int64_t)J.rw + (fx - J.x0)) * J.spp + smp);
+                    r[0] = o.x; r[1] = o.y; r[2] = o.z;
+                    r[3] = hit ? (float)((double)o.x + (double)d.x * (double)h.t) : 0.f;
+                    r[4] = hit ? (float)((double)o.y + (double)d.y * (double)h.t) : 0.f;
+                    r[5] = hit ? (float)((double)o.z + (double)d.z * (double)h.t) : 0.f;
+                }
                 break;
             }
             case XTGPU_AO: {
@@ -1180,6 +1189,10 @@ __global__ void k_accumulate(const DevJob *__restrict__ jobs, const int32_t *__r
                     c = make_float4(dv, dv, dv, 1.f);
                 }
                 c.w = 1.f;
+                if (J.raygraph) {   // the pixel's colour after this sample
+                    float *r = J.raygraph + 10 * (fpix * J.spp + s);
+                    r[6] = c.x; r[7] = c.y; r[8] = c.z; r[9] = c.w;
+                }
                 break;
             case XTGPU_AO: {
                 float r = c0((float)((double)c.x + (double)v.x * w));

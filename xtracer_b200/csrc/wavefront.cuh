@@ -37,6 +37,9 @@ struct DevJob {
     int32_t aa;                      // grid anti-aliasing level (1 = pixel centre)
     int32_t spp1;                    // samples per grid position
     double wt;                       // weight of one sample: 1/(aa^2) as a float, times 1/spp1
+    float *raygraph;                 // depth integrator: 10 floats per sample (origin, hit
+                                     // point, colour after the sample), rectangle pixels
+                                     // row-major, each pixel's samples in order; or null
 };
 
 // Fills the sample fields of a job from params_t's samples and aa (aa.cc:7-32,

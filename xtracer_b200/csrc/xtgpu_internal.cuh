@@ -175,7 +175,8 @@ bool view_valid(const DevCamera &c, int width, int height, int aa);
 // the tuning a scene renders with: its own if autotuned, else the process-wide one
 const xtgpu_tuning &scene_tuning(const xtgpu_scene *sc);
 // xtgpu_render with an explicit launch configuration (the autotuner's probe)
+// raygraph: the depth integrator's per-sample records (DevJob::raygraph), or null
 xtgpu_status render_impl(xtgpu_scene *sc, const xtgpu_render_params *p, float *rgba, uint64_t *rays,
-                         cudaStream_t s, const xtgpu_tuning &T);
+                         cudaStream_t s, const xtgpu_tuning &T, float *raygraph = nullptr);
 
 }  // namespace xtg

@@ -6,6 +6,8 @@
 #include <map>
 
 #include <xtcore/log.h>
+#include <xtcore/tile.h>
+#include <xtcore/util/raygraph.h>
 #include <xtcore/mesh.h>
 #include <xtcore/octree.h>
 #include <xtcore/material.h>
@@ -398,9 +400,9 @@ xtgpu_status flatten(xtcore::Scene &scene, HASH_UINT64 camera, FlatScene &F, std
 
 // ---------------------------------------------------------------------------
 Integrator::Integrator(int kind, int node_format)
-    : ao_max_distance(100.f), seed(1), m_kind(kind), m_format(node_format), m_scene(0), m_uploaded(0),
-      m_x0(0), m_y0(0), m_w(0), m_h(0), m_served(0), m_ready(false), m_empty(false), m_status(XTGPU_OK),
-      m_rays(0)
+    : ao_max_distance(100.f), seed(1), record_raygraph(true), m_kind(kind), m_format(node_format), m_scene(0),
+      m_uploaded(0), m_x0(0), m_y0(0), m_w(0), m_h(0), m_spx(1), m_served(0), m_ready(false), m_empty(false),
+      m_status(XTGPU_OK), m_rays(0)
 {}
 
 Integrator::~Integrator()
@@ -474,7 +476,16 @@ xtgpu_status Integrator::render_frame()
     m_w = x1 - x0;
     m_h = y1 - y0;
     m_frame.assign(4 * m_w * m_h, 0.f);
-    xtgpu_status st = xtgpu_render_host(m_scene, &rp, m_frame.data(), &m_rays, 0);
+    xtgpu_status st;
+    m_spx = (size_t)(p.aa > 1 ? p.aa * p.aa : 1) * p.samples;
+    if (m_kind == XTGPU_DEPTH && record_raygraph) {
+        // the depth integrator's raygraph (depth/integrator.cc:43-51)
+        m_raygraph.assign(10 * m_w * m_h * m_spx, 0.f);
+        st = xtgpu_render_raygraph_host(m_scene, &rp, m_frame.data(), m_raygraph.data(), &m_rays, 0);
+    } else {
+        m_raygraph.clear();
+        st = xtgpu_render_host(m_scene, &rp, m_frame.data(), &m_rays, 0);
+    }
     if (st != XTGPU_OK) m_error = xtgpu_last_error();
     return st;
 }
@@ -504,6 +515,25 @@ void Integrator::render_tile(xtcore::render::tile_t *tile)
                 const float *c = &m_frame[4 * ((y - m_y0) * m_w + (x - m_x0))];
                 tile->write(x, y, nimg::ColorRGBAf(c[0], c[1], c[2], c[3]));
             }
+        if (!m_raygraph.empty()) {
+            // one two-sample path per sample, in the order the tile's queue
+            // held them (antialiasing::produce, aa.cc:55-75: column by column,
+            // each pixel's grid positions and repeats in order), appended as
+            // the CPU depth integrator appends them
+            for (size_t x = tile->x0(); x < tile->x1(); ++x)
+                for (size_t y = tile->y0(); y < tile->y1(); ++y)
+                    for (size_t k = 0; k < m_spx; ++k) {
+                        const float *r = &m_raygraph[10 * (((y - m_y0) * m_w + (x - m_x0)) * m_spx + k)];
+                        xtcore::raygraph::path_t path;
+                        xtcore::raygraph::sample_t s0, s1;
+                        s0.position = nmath::Vector3f(r[0], r[1], r[2]);
+                        s1.position = nmath::Vector3f(r[3], r[4], r[5]);
+                        s1.color = nimg::ColorRGBAf(r[6], r[7], r[8], r[9]);
+                        path.samples.push_back(s0);
+                        path.samples.push_back(s1);
+                        tile->raygraph_bundle.paths.push_back(path);
+                    }
+        }
     }
     std::lock_guard<std::mutex> lock(m_mutex);
     if (++m_served >= ctx->tiles.size()) m_ready = false;

@@ -74,6 +74,9 @@ class Integrator : public xtcore::render::IIntegrator
 
     float ao_max_distance;   // AO occlusion distance; the CPU integrator's is 100
     uint64_t seed;           // sample streams are keyed by (seed, pixel, sample)
+    // depth: append each sample's raygraph path to its tile's bundle, as the
+    // CPU depth integrator does (depth/integrator.cc:43-51); on by default
+    bool record_raygraph;
 
     void invalidate_scene();
     xtgpu_status status() const { return m_status; }   // of the last frame
@@ -88,7 +91,9 @@ class Integrator : public xtcore::render::IIntegrator
     xtgpu_scene *m_scene;
     const xtcore::Scene *m_uploaded;
     std::vector<float> m_frame;        // RGBA of the rectangle, row-major
+    std::vector<float> m_raygraph;     // depth: 10 floats per sample, pixels row-major
     size_t m_x0, m_y0, m_w, m_h;
+    size_t m_spx;                      // samples per pixel (aa^2 x samples)
     size_t m_served;                   // tiles served from the current frame
     bool m_ready;
     bool m_empty;                      // the context gives the tiles no samples

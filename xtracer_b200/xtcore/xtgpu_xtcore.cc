@@ -13,6 +13,8 @@
 //       --threads N    OpenMP threads of the tile loop, default all
 //       --tile N       tile size, default 32 (context.cc:5)
 //       --aa N         anti-aliasing level (grid distribution), default 1
+//       --raygraph P   the depth integrator's raygraph as PLY, exported the
+//                      GUI's way (render::assemble + raygraph::write)
 //       --png P        the assembled frame as PNG through the GPU quantiser
 //       --exr P        the assembled frame as OpenEXR (this library's writer)
 //       --ref-png P, --ref-exr P   the same frame through XTracer's own writers
@@ -36,6 +38,7 @@
 #include <xtcore/integrator.h>
 #include <xtcore/integrator/wireframe/integrator.h>
 #include <xtcore/parseutil.h>
+#include <xtcore/util/raygraph.h>
 #include <nimg/img.h>
 
 #include "gpu_integrator.h"
@@ -160,7 +163,7 @@ int mode_render(int argc, char **argv)
     unsigned long long seed = 1;
     float aod = 100.f;
     size_t threads = 0, tile = 32, aa = 1;
-    std::string png, exr, ref_png, ref_exr;
+    std::string png, exr, ref_png, ref_exr, raygraph;
     for (int i = 9; i < argc; ++i) {
         std::string a = argv[i];
         if (a == "--cpu") cpu = true;
@@ -171,6 +174,7 @@ int mode_render(int argc, char **argv)
         else if (a == "--threads" && i + 1 < argc) threads = strtoul(argv[++i], 0, 10);
         else if (a == "--tile" && i + 1 < argc) tile = strtoul(argv[++i], 0, 10);
         else if (a == "--aa" && i + 1 < argc) aa = strtoul(argv[++i], 0, 10);
+        else if (a == "--raygraph" && i + 1 < argc) raygraph = argv[++i];
         else if (a == "--png" && i + 1 < argc) png = argv[++i];
         else if (a == "--exr" && i + 1 < argc) exr = argv[++i];
         else if (a == "--ref-png" && i + 1 < argc) ref_png = argv[++i];
@@ -262,6 +266,11 @@ int mode_render(int argc, char **argv)
             fprintf(stderr, "xtgpu-xtcore: %s\n", xtgpu_last_error());
             rc = 1;
         }
+    }
+    if (!raygraph.empty()) {
+        xtcore::raygraph::raygraph_t rg;
+        xtcore::render::assemble(rg, ctx);
+        if (xtcore::raygraph::write(raygraph.c_str(), rg)) rc = 1;
     }
     if (!ref_png.empty() && nimg::io::save::png(ref_png.c_str(), pm)) rc = 1;
     if (!ref_exr.empty() && nimg::io::save::exr(ref_exr.c_str(), pm)) rc = 1;

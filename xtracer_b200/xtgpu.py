@@ -175,6 +175,11 @@ SIGNATURES = {
     "xtgpu_write_png": [C.c_char_p, C.c_int32, C.c_int32, C.c_void_p],
     "xtgpu_write_exr": [C.c_char_p, C.c_int32, C.c_int32, C.c_void_p],
     "xtgpu_save_png_host": [C.c_char_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p],
+    "xtgpu_render_raygraph": [C.c_void_p, C.POINTER(RenderParams), C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64),
+                              C.c_void_p],
+    "xtgpu_render_raygraph_host": [C.c_void_p, C.POINTER(RenderParams), C.c_void_p, C.c_void_p,
+                                   C.POINTER(C.c_uint64), C.c_void_p],
+    "xtgpu_write_raygraph_ply": [C.c_char_p, C.c_int64, C.c_void_p],
 }
 
 _lib = None
@@ -370,6 +375,45 @@ class Scene:
         rays = C.c_uint64()
         check(lib().xtgpu_render_host(self.handle, C.byref(p), _ptr(out), C.byref(rays), None))
         return out, int(rays.value)
+
+    def render_raygraph(self, width: int, height: int, spp: int = 1, aa: int = 1, node_format: int = NODES_FP32,
+                        rect=None, tile_size: int = 32):
+        """The depth integrator with its raygraph: (frame, records) where the
+        records (n, 10: origin, hit point, RGBA after the sample) are listed in
+        XTracer's raygraph order (tiles, then columns, then samples)."""
+        x0, y0, x1, y1 = rect if rect is not None else (0, 0, 0, 0)
+        p = RenderParams(DEPTH, width, height, spp, 1, 100.0, 1, node_format, x0, y0, x1, y1, aa)
+        rw, rh = (x1 - x0, y1 - y0) if rect is not None else (width, height)
+        S = max(aa, 1) ** 2 * spp
+        out = np.zeros((rh, rw, 4), np.float32)
+        rec = np.zeros((rh * rw * S, 10), np.float32)
+        rays = C.c_uint64()
+        check(lib().xtgpu_render_raygraph_host(self.handle, C.byref(p), _ptr(out), _ptr(rec), C.byref(rays), None))
+        px = raygraph_pixel_order(width, height, tile_size, rect if rect is not None else None)
+        ox, oy = (x0, y0) if rect is not None else (0, 0)
+        pix = (px[:, 1] - oy) * rw + (px[:, 0] - ox)
+        order = (pix[:, None] * S + np.arange(S)[None, :]).reshape(-1)
+        return out, rec[order]
+
+
+def raygraph_pixel_order(width: int, height: int, tile_size: int = 32, rect=None) -> np.ndarray:
+    """Pixels in the order XTracer's raygraph lists them: the tiles of
+    segment_framebuffer (tile.cc:67-94) row by row, and inside a tile column
+    by column, as antialiasing::produce queues them (aa.cc:55-58)."""
+    x0, y0, x1, y1 = rect if rect is not None else (0, 0, width, height)
+    out = []
+    for ty in range(0, height, tile_size):
+        for tx in range(0, width, tile_size):
+            for x in range(max(tx, x0), min(tx + tile_size, width, x1)):
+                for y in range(max(ty, y0), min(ty + tile_size, height, y1)):
+                    out.append((x, y))
+    return np.array(out, np.int32).reshape(-1, 2)
+
+
+def save_raygraph_ply(path: str, records) -> None:
+    """raygraph::write of the records (n, 10), in the order given."""
+    r = np.ascontiguousarray(records, np.float32).reshape(-1, 10)
+    check(lib().xtgpu_write_raygraph_ply(path.encode(), r.shape[0], _ptr(r)))
 
 
 class Params:
