@@ -29,7 +29,11 @@ these fixtures are what pins the oracle restatement (oracle/xtoracle.c):
               and depth-4 pathtracer at four seeds (`--textures`);
 * raygraph.npz  the depth integrator's raygraph exported as PLY the way the GUI
               does it (render::assemble + raygraph::write), with the frame
-              (`--raygraph`).
+              (`--raygraph`);
+* render_mtl.npz  frames of meshes loaded from an OBJ with an MTL library
+              (BlinnPhong / Emissive materials, map_Kd / map_Ks / map_Ke
+              textures): depth, uv, emission, depth-1 pathtracer, and a
+              depth-4 pathtracer at four seeds (`--mtl`).
 
 Run here (needs the reference sources and oracle/_ref/xtref):
     make -f oracle/ref.mk REF=<xtracer source tree> -j8
@@ -407,6 +411,26 @@ def make_raygraph(work):
     print("raygraph.npz", len(text), "bytes of PLY")
 
 
+def make_mtl(work):
+    """Frames of the OBJ-with-MTL scene (meshes through the loader's external
+    object path): deterministic depth, uv, emission and depth-1 pathtracer,
+    and a depth-4 pathtracer at four seeds."""
+    spec = scenes.mtl_scene()
+    scn = spec.write_scn(work)
+    rend = {}
+    for integ, rdepth in (("depth", 1), ("uv", 1), ("emission", 1), ("pathtracer", 1)):
+        xy, rgba, st = po.ref_render(scn, integ, 64, 48, spp=2, rdepth=rdepth, threads=1, workdir=work)
+        rend["%s_xy" % integ], rend["%s_rgba" % integ], rend["%s_rays" % integ] = xy, rgba, st["rays"]
+    imgs = []
+    for seed in (71, 72, 73, 74):
+        xy, rgba, st = po.ref_render(scn, "pathtracer", 64, 48, spp=16, rdepth=4, threads=1, seed=seed,
+                                     workdir=work)
+        imgs.append(rgba)
+    rend["pt_xy"], rend["pt_rgba"] = xy, np.stack(imgs)
+    np.savez_compressed(os.path.join(HERE, "render_mtl.npz"), **rend)
+    print("render_mtl.npz", sorted(rend))
+
+
 def texture_frame_size():
     return 64, 48
 
@@ -429,6 +453,9 @@ def main():
         return
     if "--cameras" in sys.argv:
         make_cameras(tempfile.mkdtemp(prefix="xtgold"), np.random.default_rng(20261204))
+        return
+    if "--mtl" in sys.argv:
+        make_mtl(tempfile.mkdtemp(prefix="xtgold"))
         return
     if "--raygraph" in sys.argv:
         make_raygraph(tempfile.mkdtemp(prefix="xtgold"))

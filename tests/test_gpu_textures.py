@@ -119,3 +119,33 @@ def test_textured_jobs_alone_equal_jobs_in_the_mix():
     svc.close()
     for r in res:
         r.close()
+
+
+def test_obj_mtl_frames_vs_reference_golden():
+    """Meshes loaded from an OBJ with an MTL library (BlinnPhong with Kd / Ks or
+    map_Kd / map_Ks, Emissive with Ke or map_Ke, textures flipped
+    horizontally): against the reference's frames of the same files."""
+    g = np.load(os.path.join(GOLD, "render_mtl.npz"))
+    sc = xtgpu.Scene(scenes.mtl_scene())
+    for integ, code in (("depth", xtgpu.DEPTH), ("uv", xtgpu.UV), ("emission", xtgpu.EMISSION),
+                        ("pathtracer", xtgpu.PATHTRACER)):
+        img, rays = sc.render(code, 64, 48, spp=2, rdepth=1)
+        assert rays == int(g["%s_rays" % integ])
+        xy = g["%s_xy" % integ]
+        got, ref = img[xy[:, 1], xy[:, 0]], g["%s_rgba" % integ]
+        d = np.abs(got - ref).max(axis=1)
+        if integ == "depth":   # 1/log(t): 1e-5 relative in t
+            D = np.abs(ref[:, 0].astype(np.float64))
+            assert np.mean(d <= 1e-5 * D * np.maximum(1.0, D) + 1e-7) >= 0.998, np.sort(d)[-5:]
+        elif integ == "uv":    # texcoords from the FP32 hit
+            assert np.mean(d <= 1e-4) >= 0.998, np.sort(d)[-5:]
+        else:
+            assert np.mean(d <= 1e-5) >= 0.998, (integ, np.sort(d)[-5:])
+    img, _ = sc.render(xtgpu.PATHTRACER, 64, 48, spp=16, rdepth=4, seed=777)
+    sc.close()
+    xy = g["pt_xy"]
+    O, R = img[xy[:, 1], xy[:, 0]], g["pt_rgba"]
+    n = R.shape[0]
+    ref = np.mean([_rmse(R[i], R[[j for j in range(n) if j != i]].mean(0)) for i in range(n)])
+    got = np.mean([_rmse(O, R[[j for j in range(n) if j != i]].mean(0)) for i in range(n)])
+    assert got <= 1.25 * ref + 1e-6, (got, ref)

@@ -146,3 +146,17 @@ def test_textured_scene_in_host_equals_c_abi(tmp_path, env):
         ref, _ = sc.render(kind, 64, 48, spp=spp, rdepth=rdepth, seed=1, aa=aa)
         sc.close()
         assert np.array_equal(got, ref), NAMES[kind]
+
+
+def test_obj_mtl_scene_in_host_equals_c_abi(tmp_path):
+    """Meshes, materials and textures from an OBJ + MTL, loaded by XTracer's
+    external object path, render through the xtcore host to the C ABI's bits
+    for the generator's scene."""
+    spec = scenes.mtl_scene()
+    scn = spec.write_scn(str(tmp_path))
+    for kind, spp, rdepth in ((xtgpu.EMISSION, 2, 1), (xtgpu.PATHTRACER, 4, 4)):
+        got = render_host(scn, kind, 64, 48, spp, rdepth, tmp_path / "f.bin")
+        sc = xtgpu.Scene(spec)
+        ref, _ = sc.render(kind, 64, 48, spp=spp, rdepth=rdepth, seed=1)
+        sc.close()
+        assert np.array_equal(got, ref), NAMES[kind]

@@ -379,3 +379,23 @@ def test_raygraph_golden():
     orc = po.OracleScene(spec, po.XO_ACCEL_OCTREE)
     out, rec = orc.render_raygraph(w, h, spp=spp, aa=aa, pixels=po.raygraph_pixel_order(w, h))
     assert po.raygraph_ply(rec) == g["ply"].tobytes().decode()
+
+
+def test_obj_mtl_frames_golden():
+    """Meshes loaded from an OBJ with an MTL library (parseutil.cc:588-682):
+    the shapes come last in the scene's object map, BlinnPhong materials carry
+    Kd / Ks or map_Kd / map_Ks, Emissive ones Ke or map_Ke, textures flipped
+    horizontally (create_sampler); the generator's description of that scene
+    renders the reference's depth, uv, emission and depth-1 pathtracer frames
+    bit for bit, and depth-4 paths within its noise."""
+    g = np.load(os.path.join(GOLD, "render_mtl.npz"))
+    spec = scenes.mtl_scene()
+    orc = po.OracleScene(spec, po.XO_ACCEL_OCTREE)
+    for integ, code in (("depth", po.DEPTH), ("uv", po.UV), ("emission", po.EMISSION), ("pathtracer", po.PATHTRACER)):
+        out, rays = orc.render(code, 64, 48, spp=2, rdepth=1, pixels=g["%s_xy" % integ])
+        assert rays == int(g["%s_rays" % integ])
+        assert np.array_equal(out, g["%s_rgba" % integ], equal_nan=True), integ
+    O, _ = po.OracleScene(spec, po.XO_ACCEL_BVH).render(po.PATHTRACER, 64, 48, spp=16, rdepth=4, seed=777,
+                                                        pixels=g["pt_xy"])
+    got, ref = stochastic_agreement(O, g["pt_rgba"])
+    assert got <= 1.25 * ref + 1e-6, (got, ref)

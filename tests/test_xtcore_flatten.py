@@ -177,3 +177,30 @@ def test_textured_scene_samplers_are_flattened(env, tmp_path):
     for k, t in enumerate(spec.env_textures):
         texels, filt = _texture_of(d, d["env_texture"] + k)
         assert np.array_equal(texels, t.texels()), ("env", k)
+
+
+def test_obj_mtl_scene_is_flattened(tmp_path):
+    """Meshes from an OBJ with an MTL library (the loader's external object
+    path): the flattened objects, triangles, texcoords, materials and samplers
+    equal the generator's; the OBJ's shapes follow the .scn objects."""
+    spec = scenes.mtl_scene()
+    d = flatten(spec, tmp_path)
+    for key in ("obj_kind", "obj_first", "obj_count"):
+        assert np.array_equal(d[key], getattr(spec, key)), key
+    assert np.array_equal(d["tris"], spec.tris)
+    assert np.array_equal(d["tri_uvs"], spec.tri_uvs)
+    assert np.array_equal(d["obj_uv_scale"], spec.obj_uv_scale)
+    for oi in range(len(spec.obj_kind)):
+        m = spec.materials[spec.obj_material[oi]]
+        t, row = d["materials"][d["obj_material"][oi]]
+        assert t == m.type, oi
+        assert row[9] == m.reflectance and row[10] == m.exponent and row[11] == m.ior, oi
+        for ch, key in enumerate(("diffuse", "specular", "emissive")):
+            kind, tex, a, b = d["samplers"][3 * d["obj_material"][oi] + ch]
+            want = m.sampler(key)
+            assert kind == want.kind, (oi, key)
+            if kind == scenes.SAMPLER_COLOR:
+                assert np.array_equal(a, np.float32(want.a)), (oi, key)
+            else:
+                texels, filt = _texture_of(d, tex)
+                assert np.array_equal(texels, want.textures[0].texels()) and filt == scenes.FILTER_NEAREST

@@ -151,6 +151,10 @@ class SceneSpec:
     tri_uvs: Optional[np.ndarray] = None           # (T, 3, 2) float32
     # ENV_ERP: one texture; ENV_CUBEMAP: six in CUBEMAP_FACE order
     env_textures: tuple = ()
+    # write every mesh object into one OBJ with an MTL material library, read
+    # by the loader's external-object path (parseutil.cc:588-682); the meshes
+    # must be the last objects and their materials expressible in MTL
+    mtl_meshes: bool = False
 
     def texture_tables(self):
         """The scene's textures and samplers as the C ABI takes them:
@@ -263,7 +267,10 @@ class SceneSpec:
         out += ["  }", "}"]
         out.append("geometry = {")
         mesh_i = 0
+        mtl_objs = [oi for oi in range(len(self.obj_kind)) if self.mtl_meshes and self.obj_kind[oi] == MESH]
         for oi in range(len(self.obj_kind)):
+            if oi in mtl_objs:
+                continue
             k, first = int(self.obj_kind[oi]), int(self.obj_first[oi])
             gname = "g%05d" % oi
             uvs = []
@@ -283,8 +290,12 @@ class SceneSpec:
                 mesh_i += 1
                 out += ["  %s = {" % gname, "    type = mesh", "    source = %s" % objname] + uvs + ["  }"]
         out.append("}")
+        mtl_mats = sorted({int(self.obj_material[oi]) for oi in mtl_objs})
         out.append("material = {")
         for mi, m in enumerate(self.materials):
+            if mi in mtl_mats and not any(int(self.obj_material[o]) == mi for o in range(len(self.obj_kind))
+                                          if o not in mtl_objs):
+                continue
             out += ["  m%05d = {" % mi, "    type = %s" % MATERIAL_NAMES[m.type], "    properties = {",
                     "      samplers = {"]
             for key in ("diffuse", "specular", "emissive"):
@@ -295,13 +306,74 @@ class SceneSpec:
         out.append("}")
         out.append("object = {")
         for oi in range(len(self.obj_kind)):
+            if oi in mtl_objs:
+                continue
             out += ["  o%05d = {" % oi, "    geometry = g%05d" % oi,
                     "    material = m%05d" % int(self.obj_material[oi]), "  }"]
+        if mtl_objs:
+            # processed after every other object, so its shapes come last in
+            # the scene's object map (string-pool ids follow insertion order)
+            assert mtl_objs == list(range(len(self.obj_kind) - len(mtl_objs), len(self.obj_kind)))
+            objname = self._write_obj_mtl(directory, mtl_objs, png)
+            out += ["  o%05d = {" % len(self.obj_kind), "    source = %s" % objname, "    prefix = x", "  }"]
         out.append("}")
         path = os.path.join(directory, self.name + ".scn")
         with open(path, "w") as fh:
             fh.write("\n".join(out) + "\n")
         return path
+
+    def _write_obj_mtl(self, directory: str, objs, png) -> str:
+        """One OBJ (a shape per mesh object, each with its usemtl) and its MTL
+        library.  A material becomes Emissive when it has an emissive colour or
+        texture, else BlinnPhong with Kd / Ks (or map_Kd / map_Ks), Ns and Ni
+        (parseutil.cc:604-648); textures load unfiltered and flipped
+        horizontally (create_sampler, parseutil.cc:567-585)."""
+        f = lambda v: repr(float(v))
+        objname, mtlname = self.name + "_ext.obj", self.name + "_ext.mtl"
+        mats = sorted({int(self.obj_material[oi]) for oi in objs})
+        lines = []
+        for mi in mats:
+            m = self.materials[mi]
+            lines.append("newmtl mat%03d" % mi)
+            for key, tag in (("diffuse", "Kd"), ("specular", "Ks"), ("emissive", "Ke")):
+                sm = m.sampler(key)
+                if sm.kind == SAMPLER_TEXTURE:
+                    t = sm.textures[0]
+                    assert t.flip_x and not t.flip_y and t.filtering == FILTER_NEAREST
+                    lines.append("map_%s %s" % (tag, png(t)))
+                else:
+                    assert sm.kind == SAMPLER_COLOR
+                    lines.append("%s %s %s %s" % ((tag,) + tuple(f(c) for c in sm.a)))
+            lines += ["Ns %s" % f(m.exponent), "Ni %s" % f(m.ior), ""]
+            emissive = m.sampler("emissive").kind != SAMPLER_COLOR or any(c > 0 for c in m.emissive)
+            if emissive:
+                assert m.type == EMISSIVE
+            else:
+                assert m.type == BLINNPHONG and m.reflectance == 0.0
+        with open(os.path.join(directory, mtlname), "w") as fh:
+            fh.write("\n".join(lines) + "\n")
+        out = ["mtllib %s" % mtlname]
+        base_v = base_t = 0
+        for oi in objs:
+            first, count = int(self.obj_first[oi]), int(self.obj_count[oi])
+            verts = self.tris[first:first + count].reshape(-1, 3)
+            out.append("o shape%05d" % oi)
+            out += ["v %r %r %r" % (float(a), float(b), float(c)) for a, b, c in verts.tolist()]
+            if self.tri_uvs is not None:
+                out += ["vt %r %r" % (float(u), float(v)) for u, v in self.tri_uvs[first:first + count].reshape(-1, 2).tolist()]
+            out.append("usemtl mat%03d" % int(self.obj_material[oi]))
+            for i in range(count):
+                a, b, c = base_v + 3 * i + 1, base_v + 3 * i + 2, base_v + 3 * i + 3
+                if self.tri_uvs is not None:
+                    t = base_t + 3 * i
+                    out.append("f %d/%d %d/%d %d/%d" % (a, t + 1, b, t + 2, c, t + 3))
+                else:
+                    out.append("f %d %d %d" % (a, b, c))
+            base_v += 3 * count
+            base_t += 3 * count if self.tri_uvs is not None else 0
+        with open(os.path.join(directory, objname), "w") as fh:
+            fh.write("\n".join(out) + "\n")
+        return objname
 
     def mesh_obj_path(self, directory: str, mesh_index: int = 0) -> str:
         return os.path.join(directory, "%s_m%02d.obj" % (self.name, mesh_index))
@@ -479,6 +551,49 @@ def textured_scene(env: str = "erp", seed: int = 9, name: str = None) -> SceneSp
     else:
         spec.env_type, spec.env_textures = ENV_CUBEMAP, tuple(Texture(img(6 + i, 6 + i)) for i in range(6))
     return spec
+
+
+def mtl_scene(seed: int = 12, name: str = "mtlscene") -> SceneSpec:
+    """Meshes from one OBJ with an MTL library behind the loader's external
+    object path: BlinnPhong shapes with Kd / Ks colours or map_Kd / map_Ks
+    textures and Emissive shapes with Ke or map_Ke, with OBJ texcoords; spheres
+    and a ground plane from the .scn before them; gradient sky."""
+    rng = np.random.default_rng(seed)
+    base = spheres_scene(12, seed=seed, extent=5.0, name=name, with_light=False)
+    img = lambda h, w: rng.integers(0, 256, (h, w, 3), dtype=np.uint8)
+    tex = [Texture(img(6, 5), FILTER_NEAREST, flip_x=True), Texture(img(4, 9), FILTER_NEAREST, flip_x=True),
+           Texture(img(8, 8), FILTER_NEAREST, flip_x=True)]
+    tris, uvs, kinds, firsts, counts, omat = [], [], [], [], [], []
+    mats = list(base.materials)
+    col = lambda: tuple(float(v) for v in _q(rng.uniform(0.1, 0.9, 3), 8))
+    specs = [Material(BLINNPHONG, diffuse=col(), specular=col(), exponent=16.0, ior=1.5),
+             Material(BLINNPHONG, diffuse=col(), specular=col(), exponent=64.0, ior=1.25,
+                      samplers={"diffuse": Sampler(SAMPLER_TEXTURE, textures=(tex[0],))}),
+             Material(BLINNPHONG, diffuse=col(), exponent=8.0, ior=1.0,
+                      samplers={"specular": Sampler(SAMPLER_TEXTURE, textures=(tex[1],))}),
+             # Emissive materials from MTL get no scalars (ior and exponent read 0)
+             Material(EMISSIVE, emissive=(2.0, 1.5, 0.5), ior=0.0),
+             Material(EMISSIVE, samplers={"emissive": Sampler(SAMPLER_TEXTURE, textures=(tex[2],))}, ior=0.0)]
+    n = 0
+    for k, m in enumerate(specs):
+        verts, faces = terrain_mesh(6, seed + k, half=1.0, amplitude=0.25, octaves=2, offset=(0.0, 0.0))
+        verts = verts + np.array([-4.0 + 2.0 * k, 1.5, 2.0 + (k % 2)], np.float32)
+        t = verts[faces].astype(np.float32)
+        uv = np.stack([(verts[:, 0] - verts[:, 0].min()) / 2.0, (verts[:, 2] - verts[:, 2].min()) / 2.0], axis=1)
+        tris.append(t)
+        uvs.append(_q(uv[faces], 12).astype(np.float32))
+        mats.append(m)
+        kinds.append(MESH); firsts.append(n); counts.append(t.shape[0]); omat.append(len(mats) - 1)
+        n += t.shape[0]
+    n_base = len(base.obj_kind)
+    scale = np.zeros((n_base + len(specs), 2), np.float32)
+    scale[n_base:] = 1.0            # ISurface's default (surface.cc:8): the OBJ meshes keep it
+    return SceneSpec(name, base.spheres, base.planes, np.concatenate(tris), np.concatenate([base.obj_kind, kinds]),
+                     np.concatenate([base.obj_first, firsts]).astype(np.int32),
+                     np.concatenate([base.obj_count, counts]).astype(np.int32),
+                     np.concatenate([base.obj_material, omat]).astype(np.int32), mats, base.camera,
+                     ENV_GRADIENT, base.env_a, base.env_b, obj_uv_scale=scale, tri_uvs=np.concatenate(uvs),
+                     mtl_meshes=True)
 
 
 def grid_for_tris(n_tris: int) -> int:
