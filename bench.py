@@ -346,8 +346,11 @@ def main():
 
     # end to end: same steps, every frame copied to host memory by the service
     e2e_svc = Service(gscenes, node_format=SERVED_FORMAT, use_graphs=True, merge_jobs=True, memory_budget=budget,
-                      host_results=True, stream=stream)
-    run_slice(e2e_svc, slices[0])
+                      host_results=True, waves_in_flight=2, stream=stream)
+    # the same untimed warm-up steps as the served arm (graphs, device and
+    # pinned host pools)
+    for w in range(args.warmup):
+        run_slice(e2e_svc, slices[w % nslices], record=[], view=True)
     D.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()

@@ -37,8 +37,17 @@ struct SvcJob {
     uint64_t frame_bytes = 0;
     float4 *frame = nullptr;
     float4 *host = nullptr;          // pinned host copy (host_results)
+    uint64_t host_bytes = 0;         // its allocated size (a size class)
     cudaEvent_t copied = nullptr;    // set while the host copy is in flight
 };
+
+// Size class of a pinned host frame: the next power of two, at least 64 KB.
+static uint64_t pinned_class(uint64_t bytes)
+{
+    uint64_t c = 1ull << 16;
+    while (c < bytes) c <<= 1;
+    return c;
+}
 
 // One wave in flight: its runner (queues, job table, graphs), the stream it
 // runs on, and what the host needs when it retires.
@@ -229,12 +238,19 @@ static xtgpu_status retire_wave(xtgpu_service *v, WaveSlot &W)
         if (v->o.host_results) {
             // frame -> pinned host memory on the service stream; the device
             // frame is freed behind the copy, so its budget is free at once
-            auto it = v->pinned_free.find(J.frame_bytes);
-            if (it != v->pinned_free.end()) {
+            // pinned frames come in power-of-two size classes (from 64 KB) and
+            // are reused by any job whose frame fits in at most twice its
+            // size: pinning memory is slow and may wait for the device, so a
+            // stream of varied frame sizes should reach a steady pool
+            const uint64_t cls = pinned_class(J.frame_bytes);
+            auto it = v->pinned_free.lower_bound(J.frame_bytes);
+            if (it != v->pinned_free.end() && it->first <= 2 * cls) {
                 J.host = it->second;
+                J.host_bytes = it->first;
                 v->pinned_free.erase(it);
             } else {
-                XTG_CUDA(cudaMallocHost((void **)&J.host, J.frame_bytes));
+                XTG_CUDA(cudaMallocHost((void **)&J.host, cls));
+                J.host_bytes = cls;
             }
             if (!v->events_free.empty()) {
                 J.copied = v->events_free.back();
@@ -599,7 +615,7 @@ xtgpu_status xtgpu_service_release(xtgpu_service *v, int64_t id)
         v->mem_used -= J.frame_bytes;
     }
     if (J.host) {
-        v->pinned_free.emplace(J.frame_bytes, J.host);
+        v->pinned_free.emplace(J.host_bytes, J.host);
         J.host = nullptr;
     }
     return XTGPU_OK;
