@@ -160,6 +160,17 @@ typedef struct {
 
 /* Uploads the scene (geometry, materials, camera) to the current device. */
 XTGPU_API xtgpu_status xtgpu_scene_create(const xtgpu_scene_desc *desc, void *stream, xtgpu_scene **out);
+/* Re-uploads the parts of a scene that need no BVH rebuild, from a
+ * description of the same geometry (an edited Scene, or one loaded with other
+ * -mod values): XTGPU_UPDATE_SHADING replaces the materials, their samplers,
+ * the textures, the objects' materials, the u/v scales and triangle texcoords
+ * (texturing only) and the environment; XTGPU_UPDATE_CAMERA
+ * the camera.  Geometry fields are ignored.  Work on `stream` is waited for;
+ * renders of the scene on other streams must have finished.  A service that
+ * holds the scene sees the change after xtgpu_service_update_scene. */
+enum { XTGPU_UPDATE_SHADING = 1, XTGPU_UPDATE_CAMERA = 2 };
+XTGPU_API xtgpu_status xtgpu_scene_update(xtgpu_scene *scene, const xtgpu_scene_desc *desc, int32_t what,
+                                          void *stream);
 /* Builds the scene's LBVH on the device: 30-bit Morton codes, in-house radix
  * sort, Karras hierarchy, bottom-up refit, optional 8-bit quantisation.  Both
  * node formats can be built and kept; the last one built is used by default. */
@@ -324,6 +335,9 @@ typedef struct {
 
 XTGPU_API xtgpu_status xtgpu_service_create(const xtgpu_service_opts *opts, void *stream, xtgpu_service **out);
 XTGPU_API xtgpu_status xtgpu_service_add_scene(xtgpu_service *svc, xtgpu_scene *scene, int32_t *scene_id);
+/* Refreshes the service's copy of a resident scene's tables after
+ * xtgpu_scene_update (waits for the waves in flight). */
+XTGPU_API xtgpu_status xtgpu_service_update_scene(xtgpu_service *service, int32_t scene);
 /* Queues a job; submit_s is the arrival time on the service clock (seconds
  * since xtgpu_service_create), or a negative value for "now". */
 XTGPU_API xtgpu_status xtgpu_service_submit(xtgpu_service *svc, const xtgpu_job_desc *job, double submit_s, int64_t *job_id);

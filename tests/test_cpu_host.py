@@ -156,3 +156,10 @@ def test_bad_textures_and_cameras_are_rejected_without_device_work():
     d.camera.type = 9
     assert L.xtgpu_scene_create(C.byref(d), None, C.byref(out)) == 1
     assert b"camera" in L.xtgpu_last_error()
+
+
+def test_scene_update_arguments_are_checked_without_device_work():
+    L = xtgpu.lib()
+    d = xtgpu.SceneDesc()
+    assert L.xtgpu_scene_update(None, C.byref(d), 1, None) == 1
+    assert L.xtgpu_service_update_scene(None, 0) == 1

@@ -160,3 +160,23 @@ def test_obj_mtl_scene_in_host_equals_c_abi(tmp_path):
         ref, _ = sc.render(kind, 64, 48, spp=spp, rdepth=rdepth, seed=1)
         sc.close()
         assert np.array_equal(got, ref), NAMES[kind]
+
+
+def test_camera_switch_in_host(tmp_path):
+    """The context renders through another camera of the same scene: the GPU
+    integrator follows it (camera re-upload, geometry kept), matching the C
+    ABI's render through that camera and the CPU integrator."""
+    import dataclasses
+    spec = scenes.spheres_scene(64, seed=1, name="twocams")
+    alt = scenes.Camera((0.5, 2.0, 0.25), type=scenes.CAM_ERP, orientation=(0.0, 0.5, 0.0))
+    spec = dataclasses.replace(spec, extra_cameras={"alt": alt})
+    scn = spec.write_scn(str(tmp_path))
+    got = render_host(scn, xtgpu.DEPTH, 64, 32, 2, 1, tmp_path / "g.bin", "--then-camera", "alt")
+    cpu = render_host(scn, xtgpu.DEPTH, 64, 32, 2, 1, tmp_path / "c.bin", "--then-camera", "alt", "--cpu",
+                      "--threads", "2")
+    sc = xtgpu.Scene(dataclasses.replace(spec, camera=alt))
+    ref, _ = sc.render(xtgpu.DEPTH, 64, 32, spp=2)
+    sc.close()
+    assert np.array_equal(got, ref)
+    D = np.abs(cpu[..., 0].astype(np.float64))
+    assert np.mean(np.abs(got[..., 0] - cpu[..., 0]) <= 1e-5 * D * np.maximum(1.0, D) + 1e-7) >= 0.99

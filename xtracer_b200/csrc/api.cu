@@ -210,6 +210,144 @@ xtgpu_status xtgpu_scene_set_tuning(xtgpu_scene *sc, const xtgpu_tuning *t)
 }
 const char *xtgpu_version(void) { return "xtgpu 0.1 (sm_100a)"; }
 
+// Materials, samplers, textures and the environment of a description.
+static xtgpu_status check_shading(const xtgpu_scene_desc *d, const std::string &who)
+{
+    if (d->env_type < XTGPU_ENV_NONE || d->env_type > XTGPU_ENV_CUBEMAP) {
+        set_error(who + ": bad environment type");
+        return XTGPU_ERR_INVALID;
+    }
+    // textures: every texel of every texture inside texels; samplers name
+    // textures that exist (a cubemap six of them)
+    if (d->n_textures < 0 || d->n_texels < 0 || (d->n_textures && (!d->textures || !d->texels))) {
+        set_error(who + ": inconsistent texture arrays");
+        return XTGPU_ERR_INVALID;
+    }
+    for (int32_t i = 0; i < d->n_textures; ++i) {
+        const xtgpu_texture &t = d->textures[i];
+        if (t.width <= 0 || t.height <= 0 || t.offset < 0 || (t.filtering != XTGPU_FILTER_NEAREST &&
+                                                              t.filtering != XTGPU_FILTER_BILINEAR) ||
+            (int64_t)t.width * t.height > d->n_texels - t.offset) {
+            set_error(who + ": texture " + std::to_string(i) + " out of bounds or bad filtering");
+            return XTGPU_ERR_INVALID;
+        }
+    }
+    auto tex_ok = [&](int kind, int tex) {
+        if (kind == XTGPU_SAMPLER_TEXTURE || kind == XTGPU_SAMPLER_ERP) return tex >= 0 && tex < d->n_textures;
+        if (kind == XTGPU_SAMPLER_CUBEMAP) return tex >= 0 && (int64_t)tex + 6 <= d->n_textures;
+        return kind == XTGPU_SAMPLER_COLOR || kind == XTGPU_SAMPLER_GRADIENT;
+    };
+    if (d->mat_samplers)
+        for (int64_t i = 0; i < 3 * (int64_t)d->n_materials; ++i)
+            if (!tex_ok(d->mat_samplers[i].kind, d->mat_samplers[i].texture)) {
+                set_error(who + ": material sampler " + std::to_string(i) +
+                          ": bad kind or texture index");
+                return XTGPU_ERR_INVALID;
+            }
+    if ((d->env_type == XTGPU_ENV_ERP && !tex_ok(XTGPU_SAMPLER_ERP, d->env_texture)) ||
+        (d->env_type == XTGPU_ENV_CUBEMAP && !tex_ok(XTGPU_SAMPLER_CUBEMAP, d->env_texture))) {
+        set_error(who + ": environment texture out of range");
+        return XTGPU_ERR_INVALID;
+    }
+
+    return XTGPU_OK;
+}
+
+// Uploads a description's materials (with their samplers), textures, object
+// materials, texture-coordinate inputs and environment into new device
+// buffers, then swaps them in: the scene's geometry and BVH are untouched.
+static xtgpu_status upload_shading(xtgpu_scene *sc, const xtgpu_scene_desc *d, cudaStream_t s)
+{
+    std::vector<DevMaterial> mats((size_t)std::max(1, d->n_materials));
+    for (int32_t i = 0; i < d->n_materials; ++i) {
+        const xtgpu_material &m = d->materials[i];
+        mats[i].type = m.type;
+        mats[i].diffuse = make_float3(m.diffuse[0], m.diffuse[1], m.diffuse[2]);
+        mats[i].specular = make_float3(m.specular[0], m.specular[1], m.specular[2]);
+        mats[i].emissive = make_float3(m.emissive[0], m.emissive[1], m.emissive[2]);
+        mats[i].reflectance = m.reflectance;
+        mats[i].exponent = m.exponent;
+        mats[i].ior = m.ior;
+        mats[i].textured = 0;
+        const float3 col[3] = {mats[i].diffuse, mats[i].specular, mats[i].emissive};
+        for (int ch = 0; ch < 3; ++ch) {
+            DevSampler &k = mats[i].s[ch];
+            k = DevSampler{XTGPU_SAMPLER_COLOR, -1, col[ch], make_float3(0.f, 0.f, 0.f)};
+            if (!d->mat_samplers) continue;
+            const xtgpu_sampler &x = d->mat_samplers[3 * (size_t)i + ch];
+            k.kind = x.kind;
+            k.tex = x.texture;
+            k.a = make_float3(x.a[0], x.a[1], x.a[2]);
+            k.b = make_float3(x.b[0], x.b[1], x.b[2]);
+            if (x.kind == XTGPU_SAMPLER_COLOR) {
+                // the colour replaces the material's (get_sample of the sampler)
+                (ch == 0 ? mats[i].diffuse : ch == 1 ? mats[i].specular : mats[i].emissive) = k.a;
+            } else {
+                mats[i].textured = 1;
+            }
+        }
+    }
+    std::vector<DevTexture> texs((size_t)std::max(1, d->n_textures));
+    for (int32_t i = 0; i < d->n_textures; ++i)
+    {
+        const uint64_t W = (uint64_t)d->textures[i].width, Hh = (uint64_t)d->textures[i].height;
+        texs[i] = DevTexture{d->textures[i].width, d->textures[i].height, d->textures[i].filtering, 0,
+                             d->textures[i].offset, (uint32_t)((UINT64_MAX % W + 1) % W),
+                             (uint32_t)((UINT64_MAX % Hh + 1) % Hh)};
+    }
+    std::vector<int32_t> om((size_t)std::max(1, d->n_objects));
+    for (int32_t i = 0; i < d->n_objects; ++i) om[i] = d->obj_material[i];
+    // texture-coordinate inputs: the surfaces' u/v scales, the triangles' texcoords
+    std::vector<float2> ouv((size_t)std::max(1, d->n_objects), make_float2(0.f, 0.f));
+    if (d->obj_uv_scale)
+        for (int32_t i = 0; i < d->n_objects; ++i) ouv[i] = make_float2(d->obj_uv_scale[2 * i], d->obj_uv_scale[2 * i + 1]);
+    const bool tuv = d->tri_uvs && d->n_tris;
+    HostBuf nm, no, nt, nx, nu, nv;
+    auto drop = [&](xtgpu_status st) {
+        dfree(nm); dfree(no); dfree(nt); dfree(nx); dfree(nu); dfree(nv);
+        return st;
+    };
+    {
+        xtgpu_status st;
+        if ((st = dalloc(nu, sizeof(float2) * ouv.size(), s)) != XTGPU_OK) return drop(st);
+        if (tuv && (st = dalloc(nv, sizeof(float2) * 3 * (size_t)d->n_tris, s)) != XTGPU_OK) return drop(st);
+        cudaError_t e = cudaMemcpy(nu.p, ouv.data(), sizeof(float2) * ouv.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && tuv)
+            e = cudaMemcpy(nv.p, d->tri_uvs, sizeof(float2) * 3 * (size_t)d->n_tris, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return drop(cuda_fail(e, "cudaMemcpy", __FILE__, __LINE__));
+    }
+    xtgpu_status st;
+    if ((st = dalloc(nm, sizeof(DevMaterial) * mats.size(), s)) != XTGPU_OK) return drop(st);
+    if ((st = dalloc(no, sizeof(int32_t) * om.size(), s)) != XTGPU_OK) return drop(st);
+    if ((st = dalloc(nt, sizeof(DevTexture) * texs.size(), s)) != XTGPU_OK) return drop(st);
+    if ((st = dalloc(nx, sizeof(float4) * (size_t)std::max<int64_t>(1, d->n_texels), s)) != XTGPU_OK) return drop(st);
+    cudaError_t e = cudaMemcpy(nm.p, mats.data(), sizeof(DevMaterial) * mats.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(no.p, om.data(), sizeof(int32_t) * om.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(nt.p, texs.data(), sizeof(DevTexture) * texs.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && d->n_texels)
+        e = cudaMemcpy(nx.p, d->texels, sizeof(float4) * (size_t)d->n_texels, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return drop(cuda_fail(e, "cudaMemcpy", __FILE__, __LINE__));
+    std::swap(sc->materials, nm);
+    std::swap(sc->obj_material, no);
+    std::swap(sc->textures, nt);
+    std::swap(sc->texels, nx);
+    std::swap(sc->obj_uvs, nu);
+    std::swap(sc->tri_uv, nv);
+    dfree(nm); dfree(no); dfree(nt); dfree(nx); dfree(nu); dfree(nv);   // the previous buffers
+    DevScene &S = sc->dev;
+    S.obj_uvs = (const float2 *)sc->obj_uvs.p;
+    S.tri_uv = (const float2 *)sc->tri_uv.p;
+    S.materials = (const DevMaterial *)sc->materials.p;
+    S.obj_material = (const int32_t *)sc->obj_material.p;
+    S.textures = (const DevTexture *)sc->textures.p;
+    S.texels = (const float4 *)sc->texels.p;
+    S.env_type = d->env_type;
+    S.env_tex = d->env_texture;
+    S.env_a = make_float3(d->env_a[0], d->env_a[1], d->env_a[2]);
+    S.env_b = make_float3(d->env_b[0], d->env_b[1], d->env_b[2]);
+    return XTGPU_OK;
+}
+
 xtgpu_status xtgpu_scene_create(const xtgpu_scene_desc *d, void *stream, xtgpu_scene **out)
 {
     if (!d || !out) {
@@ -256,42 +394,7 @@ xtgpu_status xtgpu_scene_create(const xtgpu_scene_desc *d, void *stream, xtgpu_s
             set_error("xtgpu_scene_create: a primitive belongs to no object");
             return XTGPU_ERR_INVALID;
         }
-    if (d->env_type < XTGPU_ENV_NONE || d->env_type > XTGPU_ENV_CUBEMAP) {
-        set_error("xtgpu_scene_create: bad environment type");
-        return XTGPU_ERR_INVALID;
-    }
-    // textures: every texel of every texture inside texels; samplers name
-    // textures that exist (a cubemap six of them)
-    if (d->n_textures < 0 || d->n_texels < 0 || (d->n_textures && (!d->textures || !d->texels))) {
-        set_error("xtgpu_scene_create: inconsistent texture arrays");
-        return XTGPU_ERR_INVALID;
-    }
-    for (int32_t i = 0; i < d->n_textures; ++i) {
-        const xtgpu_texture &t = d->textures[i];
-        if (t.width <= 0 || t.height <= 0 || t.offset < 0 || (t.filtering != XTGPU_FILTER_NEAREST &&
-                                                              t.filtering != XTGPU_FILTER_BILINEAR) ||
-            (int64_t)t.width * t.height > d->n_texels - t.offset) {
-            set_error("xtgpu_scene_create: texture " + std::to_string(i) + " out of bounds or bad filtering");
-            return XTGPU_ERR_INVALID;
-        }
-    }
-    auto tex_ok = [&](int kind, int tex) {
-        if (kind == XTGPU_SAMPLER_TEXTURE || kind == XTGPU_SAMPLER_ERP) return tex >= 0 && tex < d->n_textures;
-        if (kind == XTGPU_SAMPLER_CUBEMAP) return tex >= 0 && (int64_t)tex + 6 <= d->n_textures;
-        return kind == XTGPU_SAMPLER_COLOR || kind == XTGPU_SAMPLER_GRADIENT;
-    };
-    if (d->mat_samplers)
-        for (int64_t i = 0; i < 3 * (int64_t)d->n_materials; ++i)
-            if (!tex_ok(d->mat_samplers[i].kind, d->mat_samplers[i].texture)) {
-                set_error("xtgpu_scene_create: material sampler " + std::to_string(i) +
-                          ": bad kind or texture index");
-                return XTGPU_ERR_INVALID;
-            }
-    if ((d->env_type == XTGPU_ENV_ERP && !tex_ok(XTGPU_SAMPLER_ERP, d->env_texture)) ||
-        (d->env_type == XTGPU_ENV_CUBEMAP && !tex_ok(XTGPU_SAMPLER_CUBEMAP, d->env_texture))) {
-        set_error("xtgpu_scene_create: environment texture out of range");
-        return XTGPU_ERR_INVALID;
-    }
+    XTG_TRY(check_shading(d, "xtgpu_scene_create"));
 
     cudaStream_t s = (cudaStream_t)stream;
     xtgpu_scene *sc = new xtgpu_scene();
@@ -326,69 +429,12 @@ xtgpu_status xtgpu_scene_create(const xtgpu_scene_desc *d, void *stream, xtgpu_s
     if ((st = dalloc(sc->spheres, sizeof(float4) * sp.size(), s)) != XTGPU_OK) return fail(st);
     if ((st = dalloc(sc->planes, sizeof(float4) * pl.size(), s)) != XTGPU_OK) return fail(st);
     if ((st = dalloc(sc->prim_obj, sizeof(int32_t) * prim_obj.size(), s)) != XTGPU_OK) return fail(st);
-    std::vector<DevMaterial> mats((size_t)std::max(1, d->n_materials));
-    for (int32_t i = 0; i < d->n_materials; ++i) {
-        const xtgpu_material &m = d->materials[i];
-        mats[i].type = m.type;
-        mats[i].diffuse = make_float3(m.diffuse[0], m.diffuse[1], m.diffuse[2]);
-        mats[i].specular = make_float3(m.specular[0], m.specular[1], m.specular[2]);
-        mats[i].emissive = make_float3(m.emissive[0], m.emissive[1], m.emissive[2]);
-        mats[i].reflectance = m.reflectance;
-        mats[i].exponent = m.exponent;
-        mats[i].ior = m.ior;
-        mats[i].textured = 0;
-        const float3 col[3] = {mats[i].diffuse, mats[i].specular, mats[i].emissive};
-        for (int ch = 0; ch < 3; ++ch) {
-            DevSampler &k = mats[i].s[ch];
-            k = DevSampler{XTGPU_SAMPLER_COLOR, -1, col[ch], make_float3(0.f, 0.f, 0.f)};
-            if (!d->mat_samplers) continue;
-            const xtgpu_sampler &x = d->mat_samplers[3 * (size_t)i + ch];
-            k.kind = x.kind;
-            k.tex = x.texture;
-            k.a = make_float3(x.a[0], x.a[1], x.a[2]);
-            k.b = make_float3(x.b[0], x.b[1], x.b[2]);
-            if (x.kind == XTGPU_SAMPLER_COLOR) {
-                // the colour replaces the material's (get_sample of the sampler)
-                (ch == 0 ? mats[i].diffuse : ch == 1 ? mats[i].specular : mats[i].emissive) = k.a;
-            } else {
-                mats[i].textured = 1;
-            }
-        }
-    }
-    std::vector<DevTexture> texs((size_t)std::max(1, d->n_textures));
-    for (int32_t i = 0; i < d->n_textures; ++i)
-    {
-        const uint64_t W = (uint64_t)d->textures[i].width, Hh = (uint64_t)d->textures[i].height;
-        texs[i] = DevTexture{d->textures[i].width, d->textures[i].height, d->textures[i].filtering, 0,
-                             d->textures[i].offset, (uint32_t)((UINT64_MAX % W + 1) % W),
-                             (uint32_t)((UINT64_MAX % Hh + 1) % Hh)};
-    }
-    if ((st = dalloc(sc->textures, sizeof(DevTexture) * texs.size(), s)) != XTGPU_OK) return fail(st);
-    cudaMemcpy(sc->textures.p, texs.data(), sizeof(DevTexture) * texs.size(), cudaMemcpyHostToDevice);
-    if ((st = dalloc(sc->texels, sizeof(float4) * (size_t)std::max<int64_t>(1, d->n_texels), s)) != XTGPU_OK)
-        return fail(st);
-    if (d->n_texels)
-        cudaMemcpy(sc->texels.p, d->texels, sizeof(float4) * (size_t)d->n_texels, cudaMemcpyHostToDevice);
-    std::vector<int32_t> om((size_t)std::max(1, d->n_objects));
-    for (int32_t i = 0; i < d->n_objects; ++i) om[i] = d->obj_material[i];
-    // texture-coordinate inputs of the uv integrator
-    std::vector<float2> ouv((size_t)std::max(1, d->n_objects), make_float2(0.f, 0.f));
-    if (d->obj_uv_scale)
-        for (int32_t i = 0; i < d->n_objects; ++i) ouv[i] = make_float2(d->obj_uv_scale[2 * i], d->obj_uv_scale[2 * i + 1]);
-    if ((st = dalloc(sc->obj_uvs, sizeof(float2) * ouv.size(), s)) != XTGPU_OK) return fail(st);
-    cudaMemcpy(sc->obj_uvs.p, ouv.data(), sizeof(float2) * ouv.size(), cudaMemcpyHostToDevice);
-    if (d->tri_uvs && d->n_tris) {
-        if ((st = dalloc(sc->tri_uv, sizeof(float2) * 3 * (size_t)d->n_tris, s)) != XTGPU_OK) return fail(st);
-        cudaMemcpy(sc->tri_uv.p, d->tri_uvs, sizeof(float2) * 3 * (size_t)d->n_tris, cudaMemcpyHostToDevice);
-    }
-    if ((st = dalloc(sc->materials, sizeof(DevMaterial) * mats.size(), s)) != XTGPU_OK) return fail(st);
-    if ((st = dalloc(sc->obj_material, sizeof(int32_t) * om.size(), s)) != XTGPU_OK) return fail(st);
     cudaMemcpy(sc->spheres.p, sp.data(), sizeof(float4) * sp.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(sc->planes.p, pl.data(), sizeof(float4) * pl.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(sc->prim_obj.p, prim_obj.data(), sizeof(int32_t) * prim_obj.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(sc->materials.p, mats.data(), sizeof(DevMaterial) * mats.size(), cudaMemcpyHostToDevice);
-    if (cudaMemcpy(sc->obj_material.p, om.data(), sizeof(int32_t) * om.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    if (cudaMemcpy(sc->prim_obj.p, prim_obj.data(), sizeof(int32_t) * prim_obj.size(), cudaMemcpyHostToDevice) !=
+        cudaSuccess)
         return fail(cuda_fail(cudaGetLastError(), "cudaMemcpy", __FILE__, __LINE__));
+    if ((st = upload_shading(sc, d, s)) != XTGPU_OK) return fail(st);
 
     DevScene &S = sc->dev;
     S.tri_v = (const float4 *)sc->tri_v.p;
@@ -396,23 +442,44 @@ xtgpu_status xtgpu_scene_create(const xtgpu_scene_desc *d, void *stream, xtgpu_s
     S.spheres = (const float4 *)sc->spheres.p;
     S.planes = (const float4 *)sc->planes.p;
     S.prim_obj = (const int32_t *)sc->prim_obj.p;
-    S.obj_material = (const int32_t *)sc->obj_material.p;
-    S.materials = (const DevMaterial *)sc->materials.p;
-    S.obj_uvs = (const float2 *)sc->obj_uvs.p;
-    S.tri_uv = (const float2 *)sc->tri_uv.p;
     S.n_tris = d->n_tris;
     S.n_spheres = d->n_spheres;
     S.n_planes = d->n_planes;
     S.root = EMPTY_REF;
-    S.env_type = d->env_type;
-    S.env_tex = d->env_texture;
-    S.textures = (const DevTexture *)sc->textures.p;
-    S.texels = (const float4 *)sc->texels.p;
-    S.env_a = make_float3(d->env_a[0], d->env_a[1], d->env_a[2]);
-    S.env_b = make_float3(d->env_b[0], d->env_b[1], d->env_b[2]);
     S.cam = make_camera(d->camera);
     sc->n_objects = d->n_objects;
     *out = sc;
+    return XTGPU_OK;
+}
+
+xtgpu_status xtgpu_scene_update(xtgpu_scene *sc, const xtgpu_scene_desc *d, int32_t what, void *stream)
+{
+    if (!sc || !d || !what || (what & ~(XTGPU_UPDATE_SHADING | XTGPU_UPDATE_CAMERA))) {
+        set_error("xtgpu_scene_update: NULL argument or bad flags");
+        return XTGPU_ERR_INVALID;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    if (what & XTGPU_UPDATE_SHADING) {
+        if (d->n_objects != sc->n_objects || d->n_materials < 0 || (d->n_materials && !d->materials) ||
+            (d->n_objects && !d->obj_material) || (d->tri_uvs && d->n_tris != sc->dev.n_tris)) {
+            set_error("xtgpu_scene_update: the object or triangle count differs from the scene's, or NULL arrays");
+            return XTGPU_ERR_INVALID;
+        }
+        for (int32_t o = 0; o < d->n_objects; ++o)
+            if (d->obj_material[o] < 0 || d->obj_material[o] >= d->n_materials) {
+                set_error("xtgpu_scene_update: object material out of range");
+                return XTGPU_ERR_INVALID;
+            }
+        XTG_TRY(check_shading(d, "xtgpu_scene_update"));
+    }
+    if ((what & XTGPU_UPDATE_CAMERA) && !camera_valid(d->camera)) {
+        set_error("xtgpu_scene_update: bad camera type or non-finite camera parameters");
+        return XTGPU_ERR_INVALID;
+    }
+    // renders read the buffers being replaced: let those on this stream finish
+    XTG_CUDA(cudaStreamSynchronize(s));
+    if (what & XTGPU_UPDATE_SHADING) XTG_TRY(upload_shading(sc, d, s));
+    if (what & XTGPU_UPDATE_CAMERA) sc->dev.cam = make_camera(d->camera);
     return XTGPU_OK;
 }
 

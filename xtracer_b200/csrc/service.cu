@@ -405,6 +405,22 @@ xtgpu_status xtgpu_service_add_scene(xtgpu_service *v, xtgpu_scene *sc, int32_t 
     return XTGPU_OK;
 }
 
+xtgpu_status xtgpu_service_update_scene(xtgpu_service *v, int32_t scene)
+{
+    if (!v || scene < 0 || scene >= (int32_t)v->scenes.size()) {
+        set_error("xtgpu_service_update_scene: NULL service or unknown scene");
+        return XTGPU_ERR_INVALID;
+    }
+    // waves in flight read the scene table: it changes between waves only
+    for (int k = 0; k < v->nslots; ++k)
+        if (v->slot[k].s) XTG_CUDA(cudaStreamSynchronize(v->slot[k].s));
+    XTG_CUDA(cudaStreamSynchronize(v->s));
+    v->dev[(size_t)scene] = v->scenes[(size_t)scene]->dev;
+    for (int k = 0; k < v->nslots; ++k) XTG_TRY(v->slot[k].R.set_scenes(v->dev.data(), (int)v->dev.size(), v->s));
+    XTG_CUDA(cudaStreamSynchronize(v->s));
+    return XTGPU_OK;
+}
+
 xtgpu_status xtgpu_service_submit(xtgpu_service *v, const xtgpu_job_desc *d, double submit_s, int64_t *id)
 {
     if (!v || !d || !id) {

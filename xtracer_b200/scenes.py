@@ -151,6 +151,8 @@ class SceneSpec:
     tri_uvs: Optional[np.ndarray] = None           # (T, 3, 2) float32
     # ENV_ERP: one texture; ENV_CUBEMAP: six in CUBEMAP_FACE order
     env_textures: tuple = ()
+    # further cameras of the .scn, by name (the scene's own is "default")
+    extra_cameras: Optional[dict] = None
     # write every mesh object into one OBJ with an MTL material library, read
     # by the loader's external-object path (parseutil.cc:588-682); the meshes
     # must be the last objects and their materials expressible in MTL
@@ -253,18 +255,20 @@ class SceneSpec:
         elif self.env_type == ENV_COLOR:
             out += ["environment = {", "  type = color", "  config = {",
                     "    value = %s" % c3(self.env_a), "  }", "}"]
-        cam = self.camera
-        out += ["camera = {", "  default = {", "    type = %s" % CAMERA_NAMES[cam.type],
-                "    position = %s" % v3(cam.position)]
-        if cam.type == CAM_PERSPECTIVE:
-            out += ["    target = %s" % v3(cam.target), "    up = %s" % v3(cam.up), "    fov = %s" % f(cam.fov)]
-            if cam.flength > 0:
-                out += ["    flength = %s" % f(cam.flength), "    aperture = %s" % f(cam.aperture)]
-        elif cam.type in (CAM_ERP, CAM_ODS):
-            out += ["    orientation = %s" % v3(cam.orientation)]
-            if cam.type == CAM_ODS:
-                out += ["    ipd = %s" % f(cam.ipd)]
-        out += ["  }", "}"]
+        out.append("camera = {")
+        for cname, cam in [("default", self.camera)] + sorted((self.extra_cameras or {}).items()):
+            out += ["  %s = {" % cname, "    type = %s" % CAMERA_NAMES[cam.type],
+                    "    position = %s" % v3(cam.position)]
+            if cam.type == CAM_PERSPECTIVE:
+                out += ["    target = %s" % v3(cam.target), "    up = %s" % v3(cam.up), "    fov = %s" % f(cam.fov)]
+                if cam.flength > 0:
+                    out += ["    flength = %s" % f(cam.flength), "    aperture = %s" % f(cam.aperture)]
+            elif cam.type in (CAM_ERP, CAM_ODS):
+                out += ["    orientation = %s" % v3(cam.orientation)]
+                if cam.type == CAM_ODS:
+                    out += ["    ipd = %s" % f(cam.ipd)]
+            out.append("  }")
+        out.append("}")
         out.append("geometry = {")
         mesh_i = 0
         mtl_objs = [oi for oi in range(len(self.obj_kind)) if self.mtl_meshes and self.obj_kind[oi] == MESH]

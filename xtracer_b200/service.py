@@ -28,6 +28,10 @@ class Service:
             check(lib().xtgpu_service_add_scene(self.handle, sc.handle, C.byref(sid)))
             self.scene_ids.append(sid.value)
 
+    def update_scene(self, scene: int) -> None:
+        """Takes a resident scene's tables again after Scene.update."""
+        check(lib().xtgpu_service_update_scene(self.handle, self.scene_ids[scene]))
+
     def submit(self, scene: int, integrator: int, width: int, height: int, spp: int, rdepth: int = 4,
                ao_max_distance: float = 100.0, seed: int = 1, submit_s: float = -1.0, aa: int = 1) -> int:
         d = xtgpu.JobDesc(self.scene_ids[scene], integrator, width, height, spp, rdepth, ao_max_distance, seed,

@@ -235,6 +235,46 @@ namespace xtcore {
     namespace integrator {
         namespace gpu {
 
+bool camera_of(xtcore::Scene &scene, HASH_UINT64 camera, xtgpu_camera &out, std::string &err)
+{
+    out = xtgpu_camera();
+    // camera: Perspective (with depth of field when flength > 0,
+    // camera/perspective.cc:38-98), ERP (erp.cc:13-31), ODS (ods.cc:17-40) or
+    // Cubemap (cubemap.cc:21-69)
+    xtcore::asset::ICamera *cam = scene.get_camera(camera);
+    if (!cam) {
+        err = "no camera";
+        return false;
+    }
+    auto set3 = [](float *o, const nmath::Vector3f &v) {
+        o[0] = (float)v.x;
+        o[1] = (float)v.y;
+        o[2] = (float)v.z;
+    };
+    set3(out.position, cam->position);
+    if (xtcore::camera::Perspective *pc = dynamic_cast<xtcore::camera::Perspective *>(cam)) {
+        out.type = XTGPU_CAM_PERSPECTIVE;
+        set3(out.target, pc->target);
+        set3(out.up, pc->up);
+        out.fov = pc->fov;
+        out.flength = pc->flength;
+        out.aperture = pc->aperture;
+    } else if (xtcore::camera::ERP *ec = dynamic_cast<xtcore::camera::ERP *>(cam)) {
+        out.type = XTGPU_CAM_ERP;
+        set3(out.orientation, ec->orientation);
+    } else if (xtcore::camera::ODS *oc = dynamic_cast<xtcore::camera::ODS *>(cam)) {
+        out.type = XTGPU_CAM_ODS;
+        set3(out.orientation, oc->orientation);
+        out.ipd = oc->ipd;
+    } else if (dynamic_cast<xtcore::camera::Cubemap *>(cam)) {
+        out.type = XTGPU_CAM_CUBEMAP;
+    } else {
+        err = std::string("unsupported camera type ") + cam->get_type();
+        return false;
+    }
+    return true;
+}
+
 xtgpu_status flatten(xtcore::Scene &scene, HASH_UINT64 camera, FlatScene &F, std::string &err)
 {
     F = FlatScene();
@@ -365,44 +405,14 @@ xtgpu_status flatten(xtcore::Scene &scene, HASH_UINT64 camera, FlatScene &F, std
     d.texels = F.texels.data();
     d.mat_samplers = F.has_textures ? F.samplers.data() : 0;
 
-    // camera: Perspective (with depth of field when flength > 0,
-    // camera/perspective.cc:38-98), ERP (erp.cc:13-31), ODS (ods.cc:17-40) or
-    // Cubemap (cubemap.cc:21-69)
-    xtcore::asset::ICamera *cam = scene.get_camera(camera);
-    if (!cam) return fail("no camera");
-    auto set3 = [](float *o, const nmath::Vector3f &v) {
-        o[0] = (float)v.x;
-        o[1] = (float)v.y;
-        o[2] = (float)v.z;
-    };
-    set3(d.camera.position, cam->position);
-    if (xtcore::camera::Perspective *pc = dynamic_cast<xtcore::camera::Perspective *>(cam)) {
-        d.camera.type = XTGPU_CAM_PERSPECTIVE;
-        set3(d.camera.target, pc->target);
-        set3(d.camera.up, pc->up);
-        d.camera.fov = pc->fov;
-        d.camera.flength = pc->flength;
-        d.camera.aperture = pc->aperture;
-    } else if (xtcore::camera::ERP *ec = dynamic_cast<xtcore::camera::ERP *>(cam)) {
-        d.camera.type = XTGPU_CAM_ERP;
-        set3(d.camera.orientation, ec->orientation);
-    } else if (xtcore::camera::ODS *oc = dynamic_cast<xtcore::camera::ODS *>(cam)) {
-        d.camera.type = XTGPU_CAM_ODS;
-        set3(d.camera.orientation, oc->orientation);
-        d.camera.ipd = oc->ipd;
-    } else if (dynamic_cast<xtcore::camera::Cubemap *>(cam)) {
-        d.camera.type = XTGPU_CAM_CUBEMAP;
-    } else {
-        return fail(std::string("unsupported camera type ") + cam->get_type());
-    }
-    return XTGPU_OK;
+    return camera_of(scene, camera, d.camera, err) ? XTGPU_OK : XTGPU_ERR_INVALID;
 }
 
 // ---------------------------------------------------------------------------
 Integrator::Integrator(int kind, int node_format)
     : ao_max_distance(100.f), seed(1), record_raygraph(true), m_kind(kind), m_format(node_format), m_scene(0),
-      m_uploaded(0), m_x0(0), m_y0(0), m_w(0), m_h(0), m_spx(1), m_served(0), m_ready(false), m_empty(false),
-      m_status(XTGPU_OK), m_rays(0)
+      m_uploaded(0), m_camera(0), m_shading_dirty(false), m_x0(0), m_y0(0), m_w(0), m_h(0), m_spx(1), m_served(0),
+      m_ready(false), m_empty(false), m_status(XTGPU_OK), m_rays(0)
 {}
 
 Integrator::~Integrator()
@@ -414,6 +424,12 @@ void Integrator::invalidate_scene()
 {
     std::lock_guard<std::mutex> lock(m_mutex);
     m_uploaded = 0;
+}
+
+void Integrator::invalidate_shading()
+{
+    std::lock_guard<std::mutex> lock(m_mutex);
+    m_shading_dirty = true;
 }
 
 xtgpu_status Integrator::render_frame()
@@ -443,6 +459,31 @@ xtgpu_status Integrator::render_frame()
             return st;
         }
         m_uploaded = &ctx->scene;
+        m_camera = p.camera;
+        m_shading_dirty = false;
+    } else if (m_shading_dirty) {
+        // materials, samplers, textures, environment and camera again, the
+        // geometry and BVH kept
+        FlatScene F;
+        xtgpu_status st = flatten(ctx->scene, p.camera, F, m_error);
+        if (st != XTGPU_OK) return st;
+        if ((st = xtgpu_scene_update(m_scene, &F.desc, XTGPU_UPDATE_SHADING | XTGPU_UPDATE_CAMERA, 0)) !=
+            XTGPU_OK) {
+            m_error = xtgpu_last_error();
+            return st;
+        }
+        m_camera = p.camera;
+        m_shading_dirty = false;
+    } else if (p.camera != m_camera) {
+        // the context renders through another camera of the scene
+        xtgpu_scene_desc d = xtgpu_scene_desc();
+        if (!camera_of(ctx->scene, p.camera, d.camera, m_error)) return XTGPU_ERR_INVALID;
+        xtgpu_status st = xtgpu_scene_update(m_scene, &d, XTGPU_UPDATE_CAMERA, 0);
+        if (st != XTGPU_OK) {
+            m_error = xtgpu_last_error();
+            return st;
+        }
+        m_camera = p.camera;
     }
     // bounding rectangle of the context's tiles
     size_t x0 = (size_t)-1, y0 = (size_t)-1, x1 = 0, y1 = 0;

@@ -12,7 +12,9 @@
 //
 // The loaded Scene is flattened (objects in Scene::m_objects order, the order
 // Scene::intersection visits them, scene.cc:191-216) and uploaded once; call
-// invalidate_scene() after changing it.
+// invalidate_scene() after changing its geometry, invalidate_shading() after
+// changing only materials, samplers, the environment or cameras.  A context
+// that switches to another camera of the scene is followed on its own.
 //
 // Supported: perspective (with depth of field), ERP, ODS and cubemap cameras
 // (a cubemap's height a multiple of 6), spheres (and points, which the loader
@@ -57,6 +59,10 @@ struct FlatScene {
     xtgpu_scene_desc desc;
 };
 
+// The scene camera `camera` as the C ABI's camera; false (reason in err) for a
+// missing or unsupported camera.
+bool camera_of(xtcore::Scene &scene, HASH_UINT64 camera, xtgpu_camera &out, std::string &err);
+
 // Flattens ctx.scene with the given camera.  Returns XTGPU_OK, or
 // XTGPU_ERR_INVALID with the reason in err for what the GPU path cannot render.
 xtgpu_status flatten(xtcore::Scene &scene, HASH_UINT64 camera, FlatScene &out, std::string &err);
@@ -78,7 +84,11 @@ class Integrator : public xtcore::render::IIntegrator
     // CPU depth integrator does (depth/integrator.cc:43-51); on by default
     bool record_raygraph;
 
+    // after the scene's geometry changed: flatten, upload and rebuild the BVH
     void invalidate_scene();
+    // after materials, samplers, the environment or cameras changed (an edit
+    // or a -mod of those): re-upload them, keep the geometry and BVH
+    void invalidate_shading();
     xtgpu_status status() const { return m_status; }   // of the last frame
     const std::string &error() const { return m_error; }
     uint64_t rays() const { return m_rays; }           // rays traced by the last frame
@@ -90,6 +100,8 @@ class Integrator : public xtcore::render::IIntegrator
     std::mutex m_mutex;
     xtgpu_scene *m_scene;
     const xtcore::Scene *m_uploaded;
+    HASH_UINT64 m_camera;              // the camera uploaded
+    bool m_shading_dirty;
     std::vector<float> m_frame;        // RGBA of the rectangle, row-major
     std::vector<float> m_raygraph;     // depth: 10 floats per sample, pixels row-major
     size_t m_x0, m_y0, m_w, m_h;

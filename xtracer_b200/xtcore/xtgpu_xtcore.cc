@@ -15,6 +15,8 @@
 //       --aa N         anti-aliasing level (grid distribution), default 1
 //       --raygraph P   the depth integrator's raygraph as PLY, exported the
 //                      GUI's way (render::assemble + raygraph::write)
+//       --then-camera N  render once more through the scene's camera N (the
+//                      output is that second frame)
 //       --png P        the assembled frame as PNG through the GPU quantiser
 //       --exr P        the assembled frame as OpenEXR (this library's writer)
 //       --ref-png P, --ref-exr P   the same frame through XTracer's own writers
@@ -38,6 +40,7 @@
 #include <xtcore/integrator.h>
 #include <xtcore/integrator/wireframe/integrator.h>
 #include <xtcore/parseutil.h>
+#include <xtcore/strpool.h>
 #include <xtcore/util/raygraph.h>
 #include <nimg/img.h>
 
@@ -163,7 +166,7 @@ int mode_render(int argc, char **argv)
     unsigned long long seed = 1;
     float aod = 100.f;
     size_t threads = 0, tile = 32, aa = 1;
-    std::string png, exr, ref_png, ref_exr, raygraph;
+    std::string png, exr, ref_png, ref_exr, raygraph, then_camera;
     for (int i = 9; i < argc; ++i) {
         std::string a = argv[i];
         if (a == "--cpu") cpu = true;
@@ -175,6 +178,7 @@ int mode_render(int argc, char **argv)
         else if (a == "--tile" && i + 1 < argc) tile = strtoul(argv[++i], 0, 10);
         else if (a == "--aa" && i + 1 < argc) aa = strtoul(argv[++i], 0, 10);
         else if (a == "--raygraph" && i + 1 < argc) raygraph = argv[++i];
+        else if (a == "--then-camera" && i + 1 < argc) then_camera = argv[++i];
         else if (a == "--png" && i + 1 < argc) png = argv[++i];
         else if (a == "--exr" && i + 1 < argc) exr = argv[++i];
         else if (a == "--ref-png" && i + 1 < argc) ref_png = argv[++i];
@@ -226,6 +230,18 @@ int mode_render(int argc, char **argv)
     auto t0 = std::chrono::steady_clock::now();
     ig->render();
     auto t1 = std::chrono::steady_clock::now();
+    if (!then_camera.empty()) {
+        // the GUI's camera selection (workspace.cc): another camera of the
+        // loaded scene, the same integrator
+        ctx.params.camera = xtcore::pool::str::add(then_camera.c_str());
+        if (ctx.scene.m_cameras.find(ctx.params.camera) == ctx.scene.m_cameras.end()) {
+            fprintf(stderr, "xtgpu-xtcore: no camera %s\n", then_camera.c_str());
+            return 1;
+        }
+        t0 = std::chrono::steady_clock::now();
+        ig->render();
+        t1 = std::chrono::steady_clock::now();
+    }
     double secs = std::chrono::duration<double>(t1 - t0).count();
 
     nimg::Pixmap pm;

@@ -180,6 +180,8 @@ SIGNATURES = {
     "xtgpu_render_raygraph_host": [C.c_void_p, C.POINTER(RenderParams), C.c_void_p, C.c_void_p,
                                    C.POINTER(C.c_uint64), C.c_void_p],
     "xtgpu_write_raygraph_ply": [C.c_char_p, C.c_int64, C.c_void_p],
+    "xtgpu_scene_update": [C.c_void_p, C.POINTER(SceneDesc), C.c_int32, C.c_void_p],
+    "xtgpu_service_update_scene": [C.c_void_p, C.c_int32],
 }
 
 _lib = None
@@ -220,85 +222,100 @@ def stream_handle(stream=None) -> Optional[int]:
     return int(getattr(stream, "cuda_stream", stream))
 
 
+def scene_desc(spec):
+    """The C ABI's xtgpu_scene_desc of a scene spec (scenes.SceneSpec), and the
+    arrays it points into (keep them alive while the description is used)."""
+    keep = []
+
+    def arr(a, dt):
+        a = np.ascontiguousarray(a, dtype=dt)
+        keep.append(a)
+        return _ptr(a)
+
+    d = SceneDesc()
+    d.n_objects = len(spec.obj_kind)
+    d.obj_kind = arr(spec.obj_kind, np.int32)
+    d.obj_first = arr(spec.obj_first, np.int32)
+    d.obj_count = arr(spec.obj_count, np.int32)
+    d.obj_material = arr(spec.obj_material, np.int32)
+    d.n_spheres = spec.spheres.shape[0]
+    d.spheres = arr(spec.spheres.reshape(-1), np.float32)
+    d.n_planes = spec.planes.shape[0]
+    d.planes = arr(spec.planes.reshape(-1), np.float32)
+    d.n_tris = spec.tris.shape[0]
+    d.tris = arr(spec.tris.reshape(-1), np.float32)
+    d.tri_normals = arr(spec.tri_normals.reshape(-1), np.float32) if spec.tri_normals is not None else None
+    mats = (Material * max(1, len(spec.materials)))()
+    for i, m in enumerate(spec.materials):
+        mats[i].type = m.type
+        mats[i].diffuse[:] = list(m.diffuse)
+        mats[i].specular[:] = list(m.specular)
+        mats[i].emissive[:] = list(m.emissive)
+        mats[i].reflectance, mats[i].exponent, mats[i].ior = m.reflectance, m.exponent, m.ior
+    keep.append(mats)
+    d.n_materials = len(spec.materials)
+    d.materials = C.cast(mats, C.c_void_p)
+    d.env_type = spec.env_type
+    d.env_a[:] = list(spec.env_a)
+    d.env_b[:] = list(spec.env_b)
+    cam = spec.camera
+    d.camera.position[:] = list(cam.position)
+    d.camera.target[:] = list(cam.target)
+    d.camera.up[:] = list(cam.up)
+    d.camera.fov = cam.fov
+    d.camera.type = getattr(cam, "type", 0)
+    d.camera.orientation[:] = list(getattr(cam, "orientation", (0.0, 0.0, 0.0)))
+    d.camera.ipd = getattr(cam, "ipd", 0.0)
+    d.camera.flength = getattr(cam, "flength", 0.0)
+    d.camera.aperture = getattr(cam, "aperture", 0.0)
+    if getattr(spec, "obj_uv_scale", None) is not None:
+        d.obj_uv_scale = arr(spec.obj_uv_scale.reshape(-1), np.float32)
+    if getattr(spec, "tri_uvs", None) is not None:
+        d.tri_uvs = arr(spec.tri_uvs.reshape(-1), np.float32)
+    d.env_texture = -1
+    if hasattr(spec, "texture_tables"):
+        # textures, texels and the materials' samplers (sampler_*.cc)
+        textures, texels, samp, env_tex = spec.texture_tables()
+        tex = (Texture * max(1, len(textures)))()
+        for i, (w, h, f, off) in enumerate(np.asarray(textures).tolist()):
+            tex[i].width, tex[i].height, tex[i].filtering, tex[i].offset = int(w), int(h), int(f), int(off)
+        sam = (SamplerDesc * max(1, 3 * len(samp)))()
+        for i, row in enumerate(samp):
+            for ch, (kind, t, a, b) in enumerate(row):
+                k = sam[3 * i + ch]
+                k.kind, k.texture = int(kind), int(t)
+                k.a[:] = [float(v) for v in a]
+                k.b[:] = [float(v) for v in b]
+        keep += [tex, sam]
+        d.n_textures = len(textures)
+        d.textures = C.cast(tex, C.c_void_p)
+        d.n_texels = int(texels.shape[0])
+        d.texels = arr(texels.reshape(-1), np.float32)
+        d.mat_samplers = C.cast(sam, C.c_void_p) if samp else None
+        d.env_texture = env_tex
+    return d, keep
+
+
 class Scene:
     """A flattened xtcore Scene resident on the current CUDA device."""
 
     def __init__(self, spec, node_formats=(NODES_FP32,), leaf_size: int = 2, stream=None):
         self.spec = spec
-        keep = []
-
-        def arr(a, dt):
-            a = np.ascontiguousarray(a, dtype=dt)
-            keep.append(a)
-            return _ptr(a)
-
-        d = SceneDesc()
-        d.n_objects = len(spec.obj_kind)
-        d.obj_kind = arr(spec.obj_kind, np.int32)
-        d.obj_first = arr(spec.obj_first, np.int32)
-        d.obj_count = arr(spec.obj_count, np.int32)
-        d.obj_material = arr(spec.obj_material, np.int32)
-        d.n_spheres = spec.spheres.shape[0]
-        d.spheres = arr(spec.spheres.reshape(-1), np.float32)
-        d.n_planes = spec.planes.shape[0]
-        d.planes = arr(spec.planes.reshape(-1), np.float32)
-        d.n_tris = spec.tris.shape[0]
-        d.tris = arr(spec.tris.reshape(-1), np.float32)
-        d.tri_normals = arr(spec.tri_normals.reshape(-1), np.float32) if spec.tri_normals is not None else None
-        mats = (Material * max(1, len(spec.materials)))()
-        for i, m in enumerate(spec.materials):
-            mats[i].type = m.type
-            mats[i].diffuse[:] = list(m.diffuse)
-            mats[i].specular[:] = list(m.specular)
-            mats[i].emissive[:] = list(m.emissive)
-            mats[i].reflectance, mats[i].exponent, mats[i].ior = m.reflectance, m.exponent, m.ior
-        keep.append(mats)
-        d.n_materials = len(spec.materials)
-        d.materials = C.cast(mats, C.c_void_p)
-        d.env_type = spec.env_type
-        d.env_a[:] = list(spec.env_a)
-        d.env_b[:] = list(spec.env_b)
-        cam = spec.camera
-        d.camera.position[:] = list(cam.position)
-        d.camera.target[:] = list(cam.target)
-        d.camera.up[:] = list(cam.up)
-        d.camera.fov = cam.fov
-        d.camera.type = getattr(cam, "type", 0)
-        d.camera.orientation[:] = list(getattr(cam, "orientation", (0.0, 0.0, 0.0)))
-        d.camera.ipd = getattr(cam, "ipd", 0.0)
-        d.camera.flength = getattr(cam, "flength", 0.0)
-        d.camera.aperture = getattr(cam, "aperture", 0.0)
-        if getattr(spec, "obj_uv_scale", None) is not None:
-            d.obj_uv_scale = arr(spec.obj_uv_scale.reshape(-1), np.float32)
-        if getattr(spec, "tri_uvs", None) is not None:
-            d.tri_uvs = arr(spec.tri_uvs.reshape(-1), np.float32)
-        d.env_texture = -1
-        if hasattr(spec, "texture_tables"):
-            # textures, texels and the materials' samplers (sampler_*.cc)
-            textures, texels, samp, env_tex = spec.texture_tables()
-            tex = (Texture * max(1, len(textures)))()
-            for i, (w, h, f, off) in enumerate(np.asarray(textures).tolist()):
-                tex[i].width, tex[i].height, tex[i].filtering, tex[i].offset = int(w), int(h), int(f), int(off)
-            sam = (SamplerDesc * max(1, 3 * len(samp)))()
-            for i, row in enumerate(samp):
-                for ch, (kind, t, a, b) in enumerate(row):
-                    k = sam[3 * i + ch]
-                    k.kind, k.texture = int(kind), int(t)
-                    k.a[:] = [float(v) for v in a]
-                    k.b[:] = [float(v) for v in b]
-            keep += [tex, sam]
-            d.n_textures = len(textures)
-            d.textures = C.cast(tex, C.c_void_p)
-            d.n_texels = int(texels.shape[0])
-            d.texels = arr(texels.reshape(-1), np.float32)
-            d.mat_samplers = C.cast(sam, C.c_void_p) if samp else None
-            d.env_texture = env_tex
+        d, self._keep = scene_desc(spec)
         h = C.c_void_p()
         check(lib().xtgpu_scene_create(C.byref(d), stream_handle(stream), C.byref(h)))
         self.handle = h
         self.formats = set()
         for f in node_formats:
             self.build_bvh(f, leaf_size, stream)
+
+    def update(self, spec, what: int = 3, stream=None) -> None:
+        """xtgpu_scene_update from a spec of the same geometry: what = 1
+        (UPDATE_SHADING) the materials, samplers, textures, object materials
+        and environment, 2 (UPDATE_CAMERA) the camera, 3 both."""
+        d, keep = scene_desc(spec)
+        check(lib().xtgpu_scene_update(self.handle, C.byref(d), what, stream_handle(stream)))
+        self.spec = spec
 
     def build_bvh(self, node_format: int = NODES_FP32, leaf_size: int = 2, stream=None) -> None:
         o = BvhOpts(node_format, leaf_size)
