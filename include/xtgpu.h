@@ -388,6 +388,9 @@ typedef struct {
                                       coherent camera rays) when every scene of the wave
                                       has it built; -1 = the wave's format */
     int32_t primary_variant;       /* extend kernel of that pass; -1 = extend_variant */
+    int32_t bvh_builder;           /* hierarchy over the Morton order: 0 = LBVH (Karras radix
+                                      splits), 1 = PLOC agglomerative clustering (Meister and
+                                      Bittner 2018; a lower-cost tree, same closest hits) */
 } xtgpu_tuning;
 XTGPU_API xtgpu_status xtgpu_get_tuning(xtgpu_tuning *t);
 XTGPU_API xtgpu_status xtgpu_set_tuning(const xtgpu_tuning *t);

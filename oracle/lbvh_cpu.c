@@ -1,8 +1,8 @@
 /*
- * lbvh_cpu.c — CPU re-implementation of the GPU LBVH build's integer steps
+ * lbvh_cpu.c — CPU re-implementation of the GPU BVH build's deterministic steps
  * (xtracer_b200/csrc/bvh.cu): primitive boxes, 30-bit Morton codes, stable sort,
- * Karras hierarchy.  TEST INFRASTRUCTURE: the GPU build must reproduce these
- * arrays bit for bit.  The reference renderer has no BVH (its BVH file,
+ * Karras hierarchy, and the PLOC hierarchy with its depth-first leaf order.
+ * TEST INFRASTRUCTURE: the GPU build must reproduce these arrays bit for bit.  The reference renderer has no BVH (its BVH file,
  * src/xtcore/bvh.cc, is commented out); this checks the new builder only.
  *
  * Float steps use the same operations as the device code, in round-to-nearest
@@ -121,4 +121,120 @@ int xo_lbvh_build(int n_tris, const float *tris, int n_sph, const float *sph,
         right[i] = (mx == g + 1) ? ~(g + 1) : g + 1;
     }
     return 0;
+}
+
+/* PLOC (Meister and Bittner, TVCG 2018) as the GPU runs it (bvh.cu k_ploc_*):
+ * clusters in Morton order; per iteration each cluster's nearest neighbour
+ * within PLOC_R positions by the half surface area of the merged box (operation
+ * by operation in float; ties to nearer positions, then pairs starting at an
+ * even position, then the lower position); mutual pairs merge at
+ * the lower position into inner node base-1-rank (rank = position order of the
+ * merges of the iteration); survivors compacted in order.  Then the leaves are
+ * renumbered in depth-first order (left before right) and keys, order and the
+ * leaf references follow. */
+#define PLOC_R 16
+static float half_area(const float alo[3], const float ahi[3], const float blo[3], const float bhi[3])
+{
+    float dx = fmaxf(ahi[0], bhi[0]) - fminf(alo[0], blo[0]);
+    float dy = fmaxf(ahi[1], bhi[1]) - fminf(alo[1], blo[1]);
+    float dz = fmaxf(ahi[2], bhi[2]) - fminf(alo[2], blo[2]);
+    float a = dx * dy;
+    float b = dy * dz;
+    float c = dz * dx;
+    return (a + b) + c;
+}
+
+int xo_ploc_build(int n_tris, const float *tris, int n_sph, const float *sph,
+                  uint32_t *keys, uint32_t *order, int32_t *left, int32_t *right)
+{
+    int n = n_tris + n_sph;
+    if (n <= 0) return 0;
+    int32_t *tl = malloc(sizeof(int32_t) * (size_t)(n > 1 ? n - 1 : 1));
+    int32_t *tr = malloc(sizeof(int32_t) * (size_t)(n > 1 ? n - 1 : 1));
+    /* the Morton order of the LBVH build */
+    xo_lbvh_build(n_tris, tris, n_sph, sph, keys, order, tl, tr);
+    if (n == 1) { free(tl); free(tr); return 0; }
+    float (*clo)[3] = malloc(sizeof(float[3]) * (size_t)n), (*chi)[3] = malloc(sizeof(float[3]) * (size_t)n);
+    float (*olo)[3] = malloc(sizeof(float[3]) * (size_t)n), (*ohi)[3] = malloc(sizeof(float[3]) * (size_t)n);
+    int32_t *cid = malloc(sizeof(int32_t) * (size_t)n), *oid = malloc(sizeof(int32_t) * (size_t)n);
+    int32_t *nn = malloc(sizeof(int32_t) * (size_t)n), *cnt = malloc(sizeof(int32_t) * (size_t)n);
+    int32_t *pint = malloc(sizeof(int32_t) * (size_t)n), *pleaf = malloc(sizeof(int32_t) * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        prim_box((int)order[i], n_tris, tris, sph, clo[i], chi[i]);
+        cid[i] = ~i;
+    }
+    for (int i = 0; i < n - 1; ++i) pint[i] = -1;
+    int m = n, base = n - 1, rc = 0;
+    while (m > 1) {
+        for (int i = 0; i < m; ++i) {
+            float best = INFINITY;
+            uint64_t bkey = ~0ull;
+            int bj = -1;
+            for (int o = -PLOC_R; o <= PLOC_R; ++o) {
+                int j = i + o;
+                if (o == 0 || j < 0 || j >= m) continue;
+                float a = half_area(clo[i], chi[i], clo[j], chi[j]);
+                /* ties: nearer positions, then pairs at an even position, then lower */
+                uint32_t lo = (uint32_t)(i < j ? i : j), d = (uint32_t)(o < 0 ? -o : o);
+                uint64_t key = ((uint64_t)d << 33) | ((uint64_t)(lo & 1u) << 32) | lo;
+                if (a < best || (a == best && key < bkey)) { best = a; bkey = key; bj = j; }
+            }
+            nn[i] = bj;
+        }
+        int merges = 0, pos = 0;
+        for (int i = 0; i < m; ++i) {
+            int j = nn[i];
+            int mutual = j >= 0 && nn[j] == i;
+            if (mutual && i > j) continue;
+            if (!mutual) {
+                for (int a = 0; a < 3; ++a) { olo[pos][a] = clo[i][a]; ohi[pos][a] = chi[i][a]; }
+                oid[pos++] = cid[i];
+                continue;
+            }
+            int k = base - 1 - merges++;
+            int32_t a_ = cid[i], b_ = cid[j];
+            tl[k] = a_;
+            tr[k] = b_;
+            cnt[k] = (a_ < 0 ? 1 : cnt[a_]) + (b_ < 0 ? 1 : cnt[b_]);
+            if (a_ < 0) pleaf[~a_] = k; else pint[a_] = k;
+            if (b_ < 0) pleaf[~b_] = k; else pint[b_] = k;
+            for (int a = 0; a < 3; ++a) {
+                olo[pos][a] = fminf(clo[i][a], clo[j][a]);
+                ohi[pos][a] = fmaxf(chi[i][a], chi[j][a]);
+            }
+            oid[pos++] = k;
+        }
+        if (merges == 0) { rc = 1; break; }
+        base -= merges;
+        m = pos;
+        float (*t3)[3] = clo; clo = olo; olo = t3;
+        t3 = chi; chi = ohi; ohi = t3;
+        int32_t *ti = cid; cid = oid; oid = ti;
+    }
+    if (!rc) {
+        /* leaf offsets in depth-first order */
+        int32_t *newpos = malloc(sizeof(int32_t) * (size_t)n);
+        for (int i = 0; i < n; ++i) {
+            int32_t child = ~i, node = pleaf[i];
+            int off = 0;
+            for (;;) {
+                if (tr[node] == child) off += tl[node] < 0 ? 1 : cnt[tl[node]];
+                if (node == 0) break;
+                child = node;
+                node = pint[node];
+            }
+            newpos[i] = off;
+        }
+        uint32_t *k2 = malloc(sizeof(uint32_t) * (size_t)n), *o2 = malloc(sizeof(uint32_t) * (size_t)n);
+        for (int i = 0; i < n; ++i) { k2[newpos[i]] = keys[i]; o2[newpos[i]] = order[i]; }
+        for (int i = 0; i < n; ++i) { keys[i] = k2[i]; order[i] = o2[i]; }
+        for (int i = 0; i < n - 1; ++i) {
+            left[i] = tl[i] < 0 ? ~newpos[~tl[i]] : tl[i];
+            right[i] = tr[i] < 0 ? ~newpos[~tr[i]] : tr[i];
+        }
+        free(k2); free(o2); free(newpos);
+    }
+    free(clo); free(chi); free(olo); free(ohi); free(cid); free(oid); free(nn); free(cnt); free(pint);
+    free(pleaf); free(tl); free(tr);
+    return rc;
 }

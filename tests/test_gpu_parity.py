@@ -56,6 +56,35 @@ def lbvh_cpu(spec):
     return keys[:n], order[:n], left[:max(n - 1, 0)], right[:max(n - 1, 0)]
 
 
+def ploc_cpu(spec):
+    L = po.lib()
+    L.xo_ploc_build.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p] + [C.c_void_p] * 4
+    n = spec.n_tris + spec.spheres.shape[0]
+    keys = np.zeros(max(n, 1), np.uint32); order = np.zeros(max(n, 1), np.uint32)
+    left = np.zeros(max(n - 1, 1), np.int32); right = np.zeros(max(n - 1, 1), np.int32)
+    tris = np.ascontiguousarray(spec.tris.reshape(-1), np.float32)
+    sph = np.ascontiguousarray(spec.spheres.reshape(-1), np.float32)
+    assert L.xo_ploc_build(spec.n_tris, tris.ctypes.data_as(C.c_void_p), spec.spheres.shape[0],
+                           sph.ctypes.data_as(C.c_void_p),
+                           *[a.ctypes.data_as(C.c_void_p) for a in (keys, order, left, right)]) == 0
+    return keys[:n], order[:n], left[:max(n - 1, 0)], right[:max(n - 1, 0)]
+
+
+def with_builder(builder):
+    """Sets the process-wide BVH builder for scenes created inside; restores it."""
+    import contextlib
+
+    @contextlib.contextmanager
+    def ctx():
+        keep = xtgpu.get_tuning().bvh_builder
+        xtgpu.set_tuning(bvh_builder=builder)
+        try:
+            yield
+        finally:
+            xtgpu.set_tuning(bvh_builder=keep)
+    return ctx()
+
+
 def duplicate_scene():
     """Many triangles with identical centroids: equal Morton codes everywhere."""
     t = np.array([[[0, 0, 0], [1, 0, 0], [0, 1, 0]]], np.float32)
@@ -83,7 +112,8 @@ def test_lbvh_bit_exact_vs_cpu(name):
         spec = scenes.hairball_scene(300_000, seed=5)
     else:
         spec = tiny_scene(int(name[-1]))
-    sc = xtgpu.Scene(spec)
+    with with_builder(0):
+        sc = xtgpu.Scene(spec)
     ex = sc.bvh_export()
     keys, order, left, right = lbvh_cpu(spec)
     assert np.array_equal(ex["morton"], keys)
@@ -156,6 +186,47 @@ def test_primary_hits_terrain_200k_vs_oracle():
     m = (g_hit == 1) & (r["hit"] == 1) & (g_gid == r_gid)
     rel = np.abs(hits["t"][m].astype(np.float64) - r["t"][m]) / r["t"][m]
     assert rel.max() <= 1e-5, rel.max()
+
+
+@pytest.mark.parametrize("name", ["spheres64", "terrain20k", "hairball20k", "dup", "tiny2", "tiny3",
+                                  "hairball300k"])
+def test_ploc_bit_exact_vs_cpu(name):
+    """The PLOC hierarchy (bvh_builder 1): clustering, node numbering and the
+    depth-first leaf order equal the CPU re-implementation bit for bit."""
+    if name in small_scenes():
+        spec = small_scenes()[name][0]
+    elif name == "dup":
+        spec = duplicate_scene()
+    elif name == "hairball300k":
+        spec = scenes.hairball_scene(300_000, seed=5)
+    else:
+        spec = tiny_scene(int(name[-1]))
+    with with_builder(1):
+        sc = xtgpu.Scene(spec)
+        ex = sc.bvh_export()
+        sc.close()
+    keys, order, left, right = ploc_cpu(spec)
+    assert np.array_equal(ex["order"], order)
+    assert np.array_equal(ex["morton"], keys)
+    assert np.array_equal(ex["left"], left)
+    assert np.array_equal(ex["right"], right)
+
+
+@pytest.mark.parametrize("name", ["spheres64", "terrain20k", "hairball20k"])
+@pytest.mark.parametrize("fmt", [xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8])
+def test_ploc_tree_gives_the_same_hits(name, fmt):
+    """Any hierarchy gives the same closest hits (ties go to the lower
+    primitive id): PLOC and LBVH frames are equal bit for bit."""
+    spec, w, h = small_scenes()[name]
+    a = xtgpu.Scene(spec, node_formats=(fmt,), leaf_size=1)
+    with with_builder(1):
+        b = xtgpu.Scene(spec, node_formats=(fmt,), leaf_size=1)
+    for integ in (xtgpu.DEPTH, xtgpu.PATHTRACER):
+        ia, ra = a.render(integ, w, h, spp=4, rdepth=4, seed=8, node_format=fmt)
+        ib, rb = b.render(integ, w, h, spp=4, rdepth=4, seed=8, node_format=fmt)
+        assert ra == rb and np.array_equal(ia, ib)
+    a.close()
+    b.close()
 
 
 @pytest.mark.parametrize("name", ["spheres64", "terrain20k", "hairball20k"])

@@ -181,7 +181,8 @@ static bool tuning_valid(const xtgpu_tuning *t)
            t->leaf_size <= MAX_LEAF && t->node_layout >= 0 && t->node_layout <= 1 && t->refill_threshold >= 1 &&
            t->refill_threshold <= 32 &&
            (t->extend_min_blocks == 0 || t->extend_min_blocks == 8 || t->extend_min_blocks == 10) &&
-           (t->stack_entries == 0 || t->stack_entries == 32 || t->stack_entries == 64);
+           (t->stack_entries == 0 || t->stack_entries == 32 || t->stack_entries == 64) && t->bvh_builder >= 0 &&
+           t->bvh_builder <= 1;
 }
 
 xtgpu_status xtgpu_set_tuning(const xtgpu_tuning *t)
@@ -200,8 +201,8 @@ xtgpu_status xtgpu_scene_set_tuning(xtgpu_scene *sc, const xtgpu_tuning *t)
         set_error("xtgpu_scene_set_tuning: NULL scene or value out of range");
         return XTGPU_ERR_INVALID;
     }
-    if (t->leaf_size != sc->leaf_size) {
-        set_error("xtgpu_scene_set_tuning: leaf_size differs from the built BVH (rebuild it instead)");
+    if (t->leaf_size != sc->leaf_size || t->bvh_builder != sc->builder) {
+        set_error("xtgpu_scene_set_tuning: leaf_size or bvh_builder differs from the built BVH (rebuild it instead)");
         return XTGPU_ERR_STATE;
     }
     sc->tune = *t;
@@ -500,7 +501,7 @@ xtgpu_status xtgpu_bvh_build(xtgpu_scene *sc, const xtgpu_bvh_opts *opts, void *
         set_error("xtgpu_bvh_build: leaf_size out of range");
         return XTGPU_ERR_INVALID;
     }
-    return build_bvh(sc, fmt, leaf, scene_tuning(sc).node_layout, (cudaStream_t)stream);
+    return build_bvh(sc, fmt, leaf, scene_tuning(sc).node_layout, (cudaStream_t)stream, scene_tuning(sc).bvh_builder);
 }
 
 xtgpu_status xtgpu_scene_destroy(xtgpu_scene *sc)

@@ -48,11 +48,11 @@ xtgpu_status probe_ms(Probe &P, const xtgpu_tuning &T, float *ms)
     return XTGPU_OK;
 }
 
-xtgpu_status rebuild(xtgpu_scene *sc, int fmt, int leaf, int layout, cudaStream_t s)
+xtgpu_status rebuild(xtgpu_scene *sc, int fmt, int leaf, int layout, int builder, cudaStream_t s)
 {
     sc->built32 = sc->built8 = sc->builtW = false;   // force a new topology
-    XTG_TRY(build_bvh(sc, XTGPU_NODES_FP32, leaf, layout, s));
-    if (fmt != XTGPU_NODES_FP32) XTG_TRY(build_bvh(sc, fmt, leaf, layout, s));
+    XTG_TRY(build_bvh(sc, XTGPU_NODES_FP32, leaf, layout, s, builder));
+    if (fmt != XTGPU_NODES_FP32) XTG_TRY(build_bvh(sc, fmt, leaf, layout, s, builder));
     return XTGPU_OK;
 }
 
@@ -82,17 +82,39 @@ extern "C" xtgpu_status xtgpu_autotune(xtgpu_scene *sc, int32_t fmt, double budg
     xtgpu_tuning T = scene_tuning(sc);
     xtgpu_status st = XTGPU_OK;
     float cur = 0.f;
-    if (fmt != XTGPU_NODES_FP32 && !format_built(sc, fmt)) st = build_bvh(sc, fmt, sc->leaf_size, sc->layout, s);
+    if (fmt != XTGPU_NODES_FP32 && !format_built(sc, fmt))
+        st = build_bvh(sc, fmt, sc->leaf_size, sc->layout, s, sc->builder);
     if (st == XTGPU_OK) {
         T.leaf_size = sc->leaf_size;
+        T.bvh_builder = sc->builder;
         st = probe_ms(P, T, &cur);
+    }
+    // 0. the hierarchy builder (rebuilds the BVH)
+    if (st == XTGPU_OK && elapsed_ms() <= budget_ms) {
+        const int other = 1 - T.bvh_builder;
+        // a tree the other builder cannot make (too deep for the stack) keeps the first
+        if (rebuild(sc, fmt, T.leaf_size, T.node_layout, other, s) != XTGPU_OK) {
+            st = rebuild(sc, fmt, T.leaf_size, T.node_layout, T.bvh_builder, s);
+        } else {
+            xtgpu_tuning C = T;
+            C.bvh_builder = other;
+            float t = 0.f;
+            if ((st = probe_ms(P, C, &t)) == XTGPU_OK) {
+                if (t < cur) {
+                    cur = t;
+                    T = C;
+                } else {
+                    st = rebuild(sc, fmt, T.leaf_size, T.node_layout, T.bvh_builder, s);
+                }
+            }
+        }
     }
     // 1. primitives per leaf (rebuilds the BVH)
     if (st == XTGPU_OK) {
         int best_leaf = T.leaf_size;
         for (int leaf : {1, 2, fmt == XTGPU_NODES_W8 ? 3 : 4}) {
             if (leaf == T.leaf_size || elapsed_ms() > budget_ms) continue;
-            if ((st = rebuild(sc, fmt, leaf, T.node_layout, s)) != XTGPU_OK) break;
+            if ((st = rebuild(sc, fmt, leaf, T.node_layout, T.bvh_builder, s)) != XTGPU_OK) break;
             xtgpu_tuning C = T;
             C.leaf_size = leaf;
             float t = 0.f;
@@ -102,7 +124,8 @@ extern "C" xtgpu_status xtgpu_autotune(xtgpu_scene *sc, int32_t fmt, double budg
                 best_leaf = leaf;
             }
         }
-        if (st == XTGPU_OK && sc->leaf_size != best_leaf) st = rebuild(sc, fmt, best_leaf, T.node_layout, s);
+        if (st == XTGPU_OK && sc->leaf_size != best_leaf)
+            st = rebuild(sc, fmt, best_leaf, T.node_layout, T.bvh_builder, s);
         T.leaf_size = best_leaf;
     }
     // 2. launch knobs, one at a time

@@ -10,6 +10,8 @@
 //      and k-d Trees", HPG 2012: split search on the common-prefix length of
 //      the sorted codes, ties broken by index.
 //   5. bottom-up refit with arrival counters     (k_refit)
+//   4'-5'. or, with builder 1, PLOC clustering over the same Morton order and
+//      a depth-first renumbering of the leaves (k_ploc_*, build_ploc)
 //   6. leaf collapse (subtrees of <= leaf_size primitives become one leaf) and
 //      FP32 node emission                        (k_emit)
 //   7. optional 8-bit quantisation, rounded outward (k_quantise)
@@ -466,9 +468,256 @@ __global__ void k_gather(int n, int n_tris, const uint32_t *order, const float4 
     }
 }
 
+// --- PLOC hierarchy ---------------------------------------------------------
+// D. Meister and J. Bittner, "Parallel Locally-Ordered Clustering for Bounding
+// Volume Hierarchy Construction", IEEE TVCG 24(3), 2018.  The clusters start as
+// the leaves in Morton order.  Each iteration every cluster finds, among the
+// clusters within PLOC_R positions, the one whose merged box has the smallest
+// surface area (ties by ploc_tie); mutual nearest neighbours merge into a new
+// internal node at the lower position; the survivors are compacted in order.
+// The least pair under (area, ploc_tie) is mutual, so every iteration merges.  Internal nodes are numbered
+// from n-2 down, in iteration order and by position within one, so the last
+// merge (the root) is node 0 and children have larger indices than parents.
+constexpr int PLOC_R = 16;
+constexpr int PLOC_T = 256;   // clusters per block of the neighbour search
+
+__device__ __forceinline__ float half_area(float4 alo, float4 ahi, float4 blo, float4 bhi)
+{
+    // rounded operation by operation, so a CPU replica reproduces every choice
+    const float dx = __fsub_rn(fmaxf(ahi.x, bhi.x), fminf(alo.x, blo.x));
+    const float dy = __fsub_rn(fmaxf(ahi.y, bhi.y), fminf(alo.y, blo.y));
+    const float dz = __fsub_rn(fmaxf(ahi.z, bhi.z), fminf(alo.z, blo.z));
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dy), __fmul_rn(dy, dz)), __fmul_rn(dz, dx));
+}
+
+// Tie order of the pair {i, j}, the same from both ends: nearer positions
+// first, then pairs starting at an even position, then the lower position.
+// Equal boxes (duplicated primitives) thus merge (0,1) (2,3) ... at once, and
+// as the order over pairs is total, the least pair is always mutual.
+__device__ __forceinline__ uint64_t ploc_tie(int i, int j)
+{
+    const uint32_t lo = (uint32_t)min(i, j), d = (uint32_t)abs(i - j);
+    return ((uint64_t)d << 33) | ((uint64_t)(lo & 1u) << 32) | lo;
+}
+
+__global__ void k_ploc_init(int n, const float4 *plo, const float4 *phi, const uint32_t *order, float4 *clo,
+                            float4 *chi, int32_t *cid)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t p = order[i];
+    clo[i] = plo[p];
+    chi[i] = phi[p];
+    cid[i] = ~i;
+}
+
+__global__ void __launch_bounds__(PLOC_T) k_ploc_nn(int m, const float4 *clo, const float4 *chi, int32_t *nn)
+{
+    __shared__ float4 slo[PLOC_T + 2 * PLOC_R], shi[PLOC_T + 2 * PLOC_R];
+    const int base = blockIdx.x * PLOC_T;
+    for (int t = threadIdx.x; t < PLOC_T + 2 * PLOC_R; t += blockDim.x) {
+        const int g = base - PLOC_R + t;
+        if (g >= 0 && g < m) {
+            slo[t] = clo[g];
+            shi[t] = chi[g];
+        }
+    }
+    __syncthreads();
+    const int i = base + threadIdx.x;
+    if (i >= m) return;
+    const float4 alo = slo[threadIdx.x + PLOC_R], ahi = shi[threadIdx.x + PLOC_R];
+    float best = INFINITY;
+    uint64_t bkey = ~0ull;
+    int bj = -1;
+    for (int o = -PLOC_R; o <= PLOC_R; ++o) {
+        const int j = i + o;
+        if (o == 0 || j < 0 || j >= m) continue;
+        const float a = half_area(alo, ahi, slo[threadIdx.x + PLOC_R + o], shi[threadIdx.x + PLOC_R + o]);
+        const uint64_t key = ploc_tie(i, j);
+        if (a < best || (a == best && key < bkey)) {
+            best = a;
+            bkey = key;
+            bj = j;
+        }
+    }
+    nn[i] = bj;
+}
+
+// per cluster: merges (the lower of a mutual pair) in the low word, survives
+// (not absorbed by a lower partner) in the high word
+__global__ void k_ploc_flags(int m, const int32_t *nn, unsigned long long *f)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const int j = nn[i];
+    const bool mutual = j >= 0 && nn[j] == i;
+    f[i] = (unsigned long long)(mutual && i < j) | ((unsigned long long)!(mutual && i > j) << 32);
+}
+
+__global__ void k_ploc_write(int m, int base, const int32_t *nn, const unsigned long long *ex, const float4 *clo,
+                             const float4 *chi, const int32_t *cid, float4 *olo, float4 *ohi, int32_t *oid,
+                             int32_t *left, int32_t *right, float4 *nlo, float4 *nhi, int32_t *cnt, int32_t *height,
+                             int32_t *pint, int32_t *pleaf)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const int j = nn[i];
+    const bool mutual = j >= 0 && nn[j] == i;
+    if (mutual && i > j) return;   // absorbed by its lower partner
+    const unsigned long long e = ex[i];
+    const int pos = (int)(e >> 32);
+    if (!mutual) {
+        olo[pos] = clo[i];
+        ohi[pos] = chi[i];
+        oid[pos] = cid[i];
+        return;
+    }
+    const int k = base - 1 - (int)(e & 0xffffffffull);
+    const int32_t a = cid[i], b = cid[j];
+    const float4 alo = clo[i], ahi = chi[i], blo = clo[j], bhi = chi[j];
+    const float4 lo = make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), 0.f);
+    const float4 hi = make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.f);
+    left[k] = a;
+    right[k] = b;
+    nlo[k] = lo;
+    nhi[k] = hi;
+    cnt[k] = (a < 0 ? 1 : cnt[a]) + (b < 0 ? 1 : cnt[b]);
+    height[k] = 1 + max(a < 0 ? 0 : height[a], b < 0 ? 0 : height[b]);
+    if (a < 0) pleaf[~a] = k;
+    else pint[a] = k;
+    if (b < 0) pleaf[~b] = k;
+    else pint[b] = k;
+    olo[pos] = lo;
+    ohi[pos] = hi;
+    oid[pos] = k;
+}
+
+// Exclusive scan of 64-bit counters: tiles of 1024 per block, then the tile
+// sums (one block), then the offsets added.
+constexpr int SCAN_T = 1024;
+__device__ __forceinline__ unsigned long long block_scan_ex(unsigned long long v, unsigned long long *sw,
+                                                            unsigned long long &total)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sw[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        unsigned long long t = lane < (int)(blockDim.x >> 5) ? sw[lane] : 0ull;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        sw[lane] = t;   // inclusive warp sums
+    }
+    __syncthreads();
+    total = sw[(blockDim.x >> 5) - 1];
+    const unsigned long long before = w ? sw[w - 1] : 0ull;
+    return before + x - v;
+}
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_tiles(int m, const unsigned long long *in, unsigned long long *out,
+                                                       unsigned long long *sums)
+{
+    __shared__ unsigned long long sw[32];
+    const int i = blockIdx.x * SCAN_T + threadIdx.x;
+    const unsigned long long v = i < m ? in[i] : 0ull;
+    unsigned long long total;
+    const unsigned long long e = block_scan_ex(v, sw, total);
+    if (i < m) out[i] = e;
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+// one block: exclusive scan of the tile sums in place, the grand total after them
+__global__ void __launch_bounds__(SCAN_T) k_scan_sums(int ntiles, unsigned long long *sums)
+{
+    __shared__ unsigned long long sw[32];
+    unsigned long long carry = 0;
+    for (int base = 0; base < ntiles; base += SCAN_T) {
+        const int i = base + threadIdx.x;
+        const unsigned long long v = i < ntiles ? sums[i] : 0ull;
+        unsigned long long total;
+        const unsigned long long e = block_scan_ex(v, sw, total);
+        __syncthreads();
+        if (i < ntiles) sums[i] = carry + e;
+        carry += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) sums[ntiles] = carry;
+}
+
+__global__ void k_scan_add(int m, unsigned long long *out, const unsigned long long *sums)
+{
+    const int i = blockIdx.x * SCAN_T + threadIdx.x;
+    if (i < m) out[i] += sums[blockIdx.x];
+}
+
+// Leaf offset of a node in the depth-first order of the finished tree: the
+// leaves of every left sibling on its way to the root.
+__device__ __forceinline__ int ploc_offset(int32_t child, int32_t node, const int32_t *left, const int32_t *right,
+                                           const int32_t *cnt, const int32_t *pint, uint32_t *err)
+{
+    int off = 0;
+    for (int guard = 0;; ++guard) {
+        if (guard > 4096 || node < 0) {
+            atomicOr(err, 8u);
+            return 0;
+        }
+        if (right[node] == child) {
+            const int32_t l = left[node];
+            off += l < 0 ? 1 : cnt[l];
+        }
+        if (node == 0) return off;
+        child = node;
+        node = pint[node];
+    }
+}
+
+// Inner node ranges of the depth-first leaf order (lo, hi, split as the
+// Karras arrays give them) and every leaf's new position.
+__global__ void k_ploc_ranges(int n, const int32_t *left, const int32_t *right, const int32_t *cnt,
+                              const int32_t *pint, const int32_t *pleaf, int32_t *rlo, int32_t *rhi, int32_t *gam,
+                              int32_t *newpos, uint32_t *err)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n - 1) {
+        const int off = i == 0 ? 0 : ploc_offset(i, pint[i], left, right, cnt, pint, err);
+        const int32_t l = left[i];
+        rlo[i] = off;
+        rhi[i] = off + cnt[i] - 1;
+        gam[i] = off + (l < 0 ? 1 : cnt[l]) - 1;
+    }
+    if (i < n) newpos[i] = ploc_offset(~i, pleaf[i], left, right, cnt, pint, err);
+}
+
+// Leaf references, Morton keys, primitive order and leaf parents in the new
+// leaf order.
+__global__ void k_ploc_relabel(int n, int32_t *left, int32_t *right, const int32_t *newpos, const uint32_t *keys,
+                               const uint32_t *order, const int32_t *pleaf, uint32_t *keys2, uint32_t *order2,
+                               int32_t *pleaf2)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n - 1) {
+        if (left[i] < 0) left[i] = ~newpos[~left[i]];
+        if (right[i] < 0) right[i] = ~newpos[~right[i]];
+    }
+    if (i < n) {
+        const int q = newpos[i];
+        keys2[q] = keys[i];
+        order2[q] = order[i];
+        pleaf2[q] = pleaf[i];
+    }
+}
+
 struct Tmp {
     cudaStream_t s;
-    void *ptrs[32];
+    void *ptrs[64];
     int n = 0;
     ~Tmp()
     {
@@ -487,7 +736,82 @@ inline int blocks(int64_t n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
 
-xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, int layout, cudaStream_t s)
+// PLOC over the Morton order (see k_ploc_nn): fills left/right, the inner
+// boxes, heights and parents, then renumbers the leaves in depth-first order
+// (keys, order and leaf parents permuted) and gives every inner node its leaf
+// range and split as k_karras does, so the rest of the build is shared.
+static xtgpu_status build_ploc(int n, cudaStream_t s, Tmp &tmp, const float4 *plo, const float4 *phi,
+                               uint32_t *keys, uint32_t *vals, uint32_t *k2, uint32_t *v2, int32_t *left,
+                               int32_t *right, int32_t *rlo, int32_t *rhi, int32_t *gam, int32_t *pint, int32_t *pleaf,
+                               int32_t *height, float4 *nlo, float4 *nhi, uint32_t *err)
+{
+    const int ni = n - 1;
+    float4 *clo[2], *chi[2];
+    int32_t *cid[2], *nn, *cnt, *newpos, *pleaf2;
+    unsigned long long *flg, *ex, *sums;
+    for (int k = 0; k < 2; ++k) {
+        XTG_CUDA(tmp.get(&clo[k], n));
+        XTG_CUDA(tmp.get(&chi[k], n));
+        XTG_CUDA(tmp.get(&cid[k], n));
+    }
+    XTG_CUDA(tmp.get(&nn, n));
+    XTG_CUDA(tmp.get(&cnt, ni));
+    XTG_CUDA(tmp.get(&newpos, n));
+    XTG_CUDA(tmp.get(&pleaf2, n));
+    XTG_CUDA(tmp.get(&flg, n));
+    XTG_CUDA(tmp.get(&ex, n));
+    XTG_CUDA(tmp.get(&sums, blocks(n, SCAN_T) + 1));
+    unsigned long long *total_h = nullptr;
+    XTG_CUDA(cudaMallocHost((void **)&total_h, sizeof(unsigned long long)));
+    k_ploc_init<<<blocks(n, 256), 256, 0, s>>>(n, plo, phi, vals, clo[0], chi[0], cid[0]);
+    int m = n, base = ni, cur = 0;
+    xtgpu_status st = XTGPU_OK;
+    for (int it = 0; m > 1; ++it) {
+        if (it > 100000) {   // every iteration merges; a bound all the same
+            set_error("xtgpu_bvh_build: PLOC did not finish");
+            st = XTGPU_ERR_CUDA;
+            break;
+        }
+        const int nt = blocks(m, SCAN_T);
+        k_ploc_nn<<<blocks(m, PLOC_T), PLOC_T, 0, s>>>(m, clo[cur], chi[cur], nn);
+        k_ploc_flags<<<blocks(m, 256), 256, 0, s>>>(m, nn, flg);
+        k_scan_tiles<<<nt, SCAN_T, 0, s>>>(m, flg, ex, sums);
+        k_scan_sums<<<1, SCAN_T, 0, s>>>(nt, sums);
+        k_scan_add<<<nt, SCAN_T, 0, s>>>(m, ex, sums);
+        cudaError_t e = cudaMemcpyAsync(total_h, sums + nt, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            st = cuda_fail(e, "PLOC", __FILE__, __LINE__);
+            break;
+        }
+        const int merges = (int)(*total_h & 0xffffffffull), next = (int)(*total_h >> 32);
+        if (merges <= 0 || merges > base || next != m - merges) {
+            set_error("xtgpu_bvh_build: PLOC made no progress (non-finite primitive bounds?)");
+            st = XTGPU_ERR_CUDA;
+            break;
+        }
+        k_ploc_write<<<blocks(m, 256), 256, 0, s>>>(m, base, nn, ex, clo[cur], chi[cur], cid[cur], clo[1 - cur],
+                                                    chi[1 - cur], cid[1 - cur], left, right, nlo, nhi, cnt, height,
+                                                    pint, pleaf);
+        cur = 1 - cur;
+        base -= merges;
+        m = next;
+    }
+    cudaFreeHost(total_h);
+    if (st != XTGPU_OK) return st;
+    if (base != 0) {
+        set_error("xtgpu_bvh_build: PLOC left inner nodes unnumbered");
+        return XTGPU_ERR_CUDA;
+    }
+    k_ploc_ranges<<<blocks(n, 256), 256, 0, s>>>(n, left, right, cnt, pint, pleaf, rlo, rhi, gam, newpos, err);
+    k_ploc_relabel<<<blocks(n, 256), 256, 0, s>>>(n, left, right, newpos, keys, vals, pleaf, k2, v2, pleaf2);
+    XTG_CUDA(cudaMemcpyAsync(keys, k2, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));
+    XTG_CUDA(cudaMemcpyAsync(vals, v2, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));
+    XTG_CUDA(cudaMemcpyAsync(pleaf, pleaf2, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
+    return XTGPU_OK;
+}
+
+xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, int layout, cudaStream_t s, int builder)
 {
     DevScene &S = sc->dev;
     const int n = S.n_tris + S.n_spheres;
@@ -500,7 +824,8 @@ xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, int layo
 
     // Morton order, keys and topology are the same for both node formats: build
     // them once and keep them.
-    bool need_topology = !(sc->built32 || sc->built8) || sc->leaf_size != leaf_size || sc->layout != layout;
+    bool need_topology = !(sc->built32 || sc->built8) || sc->leaf_size != leaf_size || sc->layout != layout ||
+                         sc->builder != builder;
     if (need_topology) {
         sc->built32 = sc->built8 = sc->builtW = false;
         dfree(sc->nodes32);
@@ -514,6 +839,7 @@ xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, int layo
         dfree(sc->right);
         sc->leaf_size = leaf_size;
         sc->layout = layout;
+        sc->builder = builder;
         if (n == 0) {
             S.root = EMPTY_REF;
             sc->depth = 0;
@@ -548,7 +874,9 @@ xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, int layo
             XTG_TRY(dalloc(sc->left, sizeof(int32_t) * (size_t)std::max(1, n - 1), s));
             XTG_TRY(dalloc(sc->right, sizeof(int32_t) * (size_t)std::max(1, n - 1), s));
             int32_t *left = (int32_t *)sc->left.p, *right = (int32_t *)sc->right.p;
-            k_gather<<<blocks(n, 256), 256, 0, s>>>(n, S.n_tris, vals, S.tri_v, S.spheres, (float4 *)sc->leaf_prims.p);
+            if (builder != 1 || n < 2)
+                k_gather<<<blocks(n, 256), 256, 0, s>>>(n, S.n_tris, vals, S.tri_v, S.spheres,
+                                                        (float4 *)sc->leaf_prims.p);
             S.leaf_prims = (const float4 *)sc->leaf_prims.p;
             if (n == 1) {
                 S.root = leaf_ref(0, 1u);
@@ -572,9 +900,17 @@ xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, int layo
                 XTG_CUDA(tmp.get(&nhi, ni));
                 XTG_CUDA(cudaMemsetAsync(flags, 0, sizeof(uint32_t) * (ni + 2), s));
                 XTG_CUDA(cudaMemsetAsync(pint, 0xff, sizeof(int32_t) * ni, s));
-                k_karras<<<blocks(ni, 256), 256, 0, s>>>(keys, n, left, right, rlo, rhi, gam, pint, pleaf);
-                k_refit<<<blocks(n, 256), 256, 0, s>>>(n, left, right, pint, pleaf, plo, phi, vals, nlo, nhi, height,
-                                                       flags);
+                if (builder == 1) {
+                    XTG_TRY(build_ploc(n, s, tmp, plo, phi, keys, vals, k2, v2, left, right, rlo, rhi, gam, pint,
+                                       pleaf, height, nlo, nhi, flags + ni + 1));
+                    // primitives in the new leaf order
+                    k_gather<<<blocks(n, 256), 256, 0, s>>>(n, S.n_tris, vals, S.tri_v, S.spheres,
+                                                            (float4 *)sc->leaf_prims.p);
+                } else {
+                    k_karras<<<blocks(ni, 256), 256, 0, s>>>(keys, n, left, right, rlo, rhi, gam, pint, pleaf);
+                    k_refit<<<blocks(n, 256), 256, 0, s>>>(n, left, right, pint, pleaf, plo, phi, vals, nlo, nhi,
+                                                           height, flags);
+                }
                 XTG_TRY(dalloc(sc->nodes32, sizeof(float4) * 4 * (size_t)ni, s));
                 int32_t *pos = nullptr;
                 if (layout == 1) {

@@ -119,6 +119,7 @@ struct xtgpu_scene {
     int32_t depth = 0;
     int32_t leaf_size = 2;
     int32_t layout = 0;
+    int32_t builder = 0;
     int32_t last_format = XTGPU_NODES_FP32;
     bool built32 = false, built8 = false, builtW = false;
     int32_t depthW = 0;        // levels of the 8-wide BVH
@@ -153,7 +154,8 @@ xtgpu_status dalloc(HostBuf &b, size_t bytes, cudaStream_t s);
 void dfree(HostBuf &b);
 
 // BVH build (bvh.cu); the 8-wide collapse of the built binary tree (wide.cu)
-xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, int layout, cudaStream_t s);
+// builder: 0 = LBVH (Karras), 1 = PLOC over the same Morton order
+xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, int layout, cudaStream_t s, int builder);
 xtgpu_status build_wide(xtgpu_scene *sc, cudaStream_t s);
 
 // node formats
