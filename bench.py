@@ -129,8 +129,9 @@ NCU_TRAFFIC_BYTES_PER_RAY = 104.0
 
 def build_scenes(scale, autotune=False):
     """The resident scenes with FP32, Q8 and W8 nodes; with autotune, each
-    scene's leaf size, extend kernel, stack, tile, register cap and wave size
-    are picked by xtgpu_autotune for the served format (W8)."""
+    scene's BVH builder (LBVH or PLOC), leaf size, extend kernel, stack, tile,
+    register cap and wave size are picked by xtgpu_autotune for the served
+    format (W8)."""
     from xtracer_b200 import scenes, xtgpu
     out, specs, tunes = [], [], {}
     for name, _ in scenes.JOBSTREAM_SCENES:
@@ -143,7 +144,7 @@ def build_scenes(scale, autotune=False):
                 sc.build_bvh(f, t.leaf_size)
             tunes[name] = {k: getattr(t, k) for k in ("leaf_size", "extend_variant", "steps_per_vote",
                                                        "primary_node_format", "primary_variant", "stack_entries",
-                                                       "tile", "extend_min_blocks", "wave_paths")}
+                                                       "tile", "extend_min_blocks", "wave_paths", "bvh_builder")}
         out.append(sc)
     return specs, out, tunes
 
