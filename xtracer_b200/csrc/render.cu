@@ -1298,6 +1298,7 @@ xtgpu_status WaveRunner::set_scenes(const DevScene *scenes, int n, cudaStream_t 
     }
     XTG_CUDA(cudaMemcpyAsync(scenebuf.p, scenes, sizeof(DevScene) * (size_t)n, cudaMemcpyHostToDevice, s));
     nscenes = n;
+    host_scenes.assign(scenes, scenes + n);
     single = scenes[0];
     return XTGPU_OK;
 }
@@ -1377,7 +1378,13 @@ xtgpu_status WaveRunner::run_wave(const std::vector<DevJob> &jobs, int bounces, 
         set_error("wave larger than the queue capacity");
         return XTGPU_ERR_LIMIT;
     }
-    bool multi = nscenes > 1;
+    // a wave whose jobs all render one scene runs the single-scene extend
+    // kernels (the scene by value, no per-ray scene lookup)
+    int sc0 = nj > 0 ? jobs[0].scene : 0;
+    for (int j = 1; j < nj; ++j)
+        if (jobs[j].scene != sc0) sc0 = -1;
+    const bool multi = nscenes > 1 && sc0 < 0;
+    if (!multi) single = host_scenes[(size_t)std::max(0, sc0)];
     XTG_CUDA(cudaMemcpyAsync(jobbuf.p, S.jobs, sizeof(DevJob) * nj, cudaMemcpyHostToDevice, s));
     XTG_CUDA(cudaMemcpyAsync(prefixbuf.p, S.prefix, sizeof(int64_t) * (nj + 1), cudaMemcpyHostToDevice, s));
     // queue A holds the wave's primary rays; its count is the wave size.  The
@@ -1394,13 +1401,14 @@ xtgpu_status WaveRunner::run_wave(const std::vector<DevJob> &jobs, int bounces, 
     S.pending = true;
     if (job_rays_enabled) XTG_CUDA(cudaMemsetAsync(q.job_rays, 0, sizeof(unsigned long long) * nj, s));
     if (use_graph) {
-        // One graph per (bounces, format, scene count) shape; kernel arguments
-        // point at fixed buffers, so a graph replays any wave of that shape.
-        // every value the captured launches depend on
+        // One graph per shape: kernel arguments point at fixed buffers, so a
+        // graph replays any wave of the same key, which holds every value the
+        // captured launches depend on (a single-scene wave's scene is passed
+        // by value, so it is part of the key)
         const GraphKey key = {bounces, fmt, multi ? 1 : 0, time_extend ? 1 : 0, defer_acc ? 1 : 0,
                               q.stats ? 1 : 0, stack, T.extend_min_blocks, T.extend_variant,
                               T.extend_blocks_per_sm, T.extend_block, T.refill_threshold, T.steps_per_vote,
-                              fmt0, T.primary_variant, stack0};
+                              fmt0, T.primary_variant, stack0, multi ? -1 : std::max(0, sc0)};
         auto it = graphs.find(key);
         if (it == graphs.end()) {
             cudaGraph_t g;

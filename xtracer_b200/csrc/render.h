@@ -48,12 +48,13 @@ struct WaveRunner {
     int64_t cap = 0;
     int max_jobs = 0, max_scenes = 0, nscenes = 0;
     int sms = 148;
-    DevScene single{};
+    DevScene single{};                 // the scene of a wave whose jobs share one
+    std::vector<DevScene> host_scenes; // host copy of the scene table
     xtgpu_tuning T{};   // launch configuration of the next waves
     int stack = 64;     // traversal stack entries (32 or 64)
     int fmt0 = -1;      // node format of the first extend pass (-1 = the wave's)
     int stack0 = 64;    // its stack entries
-    using GraphKey = std::array<int32_t, 16>;
+    using GraphKey = std::array<int32_t, 17>;
     std::map<GraphKey, cudaGraphExec_t> graphs;
 
     xtgpu_status init(int64_t capacity, int max_jobs, int max_scenes, cudaStream_t s);
