@@ -403,10 +403,11 @@ XTGPU_API xtgpu_status xtgpu_set_tuning(const xtgpu_tuning *t);
  * uses its tile for the scene's jobs.  *best receives it. */
 XTGPU_API xtgpu_status xtgpu_autotune(xtgpu_scene *scene, int32_t node_format, double budget_ms, xtgpu_tuning *best,
                                       void *stream);
-/* Tuning stored with a scene (the process-wide one if it was never tuned). */
+/* Tuning stored with a scene (the process-wide one if it was never tuned),
+ * with the leaf size and builder of the BVH the scene was built with. */
 XTGPU_API xtgpu_status xtgpu_scene_tuning(const xtgpu_scene *scene, xtgpu_tuning *t);
 /* Sets the tuning the scene renders with (as xtgpu_autotune does); its
- * leaf_size must be the one the scene's BVH was built with. */
+ * leaf_size and bvh_builder must be those the scene's BVH was built with. */
 XTGPU_API xtgpu_status xtgpu_scene_set_tuning(xtgpu_scene *scene, const xtgpu_tuning *tuning);
 
 /* Text of the last error on this thread ("" if none). */

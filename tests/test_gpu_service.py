@@ -137,3 +137,20 @@ def test_autotune_keeps_results(resident):
     assert np.array_equal(before[0], after[0])
     assert np.array_equal(before[1], after[1])
     s.close()
+
+
+def test_scene_tuning_reports_the_built_tree(resident):
+    """A scene that was never tuned reports the process-wide tuning with its
+    own leaf size and builder, so a read-modify-write of its tuning is
+    accepted and changes nothing it renders."""
+    sc = resident[0]
+    t = sc.tuning()
+    assert t.leaf_size == 2 and t.bvh_builder == 0   # Scene() builds leaves of 2 with LBVH
+    ref, _ = sc.render(xtgpu.PATHTRACER, 32, 24, spp=2, rdepth=4, seed=3, node_format=xtgpu.NODES_W8)
+    keep = {k: getattr(t, k) for k, _ in xtgpu.Tuning._fields_}
+    try:
+        sc.set_tuning(primary_variant=0)
+        got, _ = sc.render(xtgpu.PATHTRACER, 32, 24, spp=2, rdepth=4, seed=3, node_format=xtgpu.NODES_W8)
+    finally:
+        sc.set_tuning(**keep)
+    assert np.array_equal(ref, got)

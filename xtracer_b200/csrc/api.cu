@@ -168,6 +168,11 @@ xtgpu_status xtgpu_scene_tuning(const xtgpu_scene *sc, xtgpu_tuning *t)
         return XTGPU_ERR_INVALID;
     }
     *t = scene_tuning(sc);
+    // the hierarchy the scene was built with, whatever the process-wide values
+    if (sc->built32 || sc->built8 || sc->builtW) {
+        t->leaf_size = sc->leaf_size;
+        t->bvh_builder = sc->builder;
+    }
     return XTGPU_OK;
 }
 
