@@ -71,6 +71,12 @@ enum { XTGPU_FILTER_NEAREST = 0, XTGPU_FILTER_BILINEAR = 1 };
  * omni-directional stereo (upper half one eye, lower the other), cubemap
  * vertical strip (faces +x -x +y -y +z -z, height a multiple of 6). */
 enum { XTGPU_CAM_PERSPECTIVE = 0, XTGPU_CAM_ERP = 1, XTGPU_CAM_ODS = 2, XTGPU_CAM_CUBEMAP = 3 };
+/* Sample distributions (aa.h:14-18, aa.cc:7-48): GRID takes aa^2 positions per
+ * pixel on a regular grid of weight 1/aa^2; RANDOM takes aa positions of weight
+ * 1/aa, each at offsets in [0,1)^2 from the pixel corner drawn from a random
+ * stream keyed by (seed, position, pixel) where the reference draws libc
+ * rand().  Either way each position is taken spp times at 1/spp. */
+enum { XTGPU_SAMPLES_GRID = 0, XTGPU_SAMPLES_RANDOM = 1 };
 /* Integrators. */
 enum { XTGPU_STENCIL = 0, XTGPU_DEPTH = 1, XTGPU_AO = 2, XTGPU_PATHTRACER = 3,
        /* primary-ray integrators (integrator/{normal,uv,emission,wireframe}) */
@@ -231,13 +237,16 @@ typedef struct {
     uint64_t seed;                 /* random stream key: results depend only on (seed, pixel, sample) */
     int32_t node_format;           /* BVH to traverse */
     int32_t x0, y0, x1, y1;        /* pixel rectangle to render; x1 = y1 = 0 means the whole frame */
-    int32_t aa;                    /* grid anti-aliasing level, 0 or 1 = the pixel centre
-                                      (params_t::aa, grid distribution, aa.cc:7-32) */
+    int32_t aa;                    /* anti-aliasing level (params_t::aa): grid, 0..16, 0 or 1 =
+                                      the pixel centre (aa.cc:7-32); random, 0..256 */
+    int32_t sample_distribution;   /* XTGPU_SAMPLES_GRID (0) or XTGPU_SAMPLES_RANDOM
+                                      (params_t::sample_distribution, aa.h:14-18) */
 } xtgpu_render_params;
 
 /* Renders the rectangle and writes RGBA float per pixel of the rectangle
- * (row-major) into rgba_dev (device memory).  Each pixel takes aa^2 grid
- * positions, each spp times, of weight 1/(aa^2 spp) (aa.cc:51-77).
+ * (row-major) into rgba_dev (device memory).  Each pixel takes P positions
+ * of the sample distribution (aa^2 on the grid, aa random), each spp times,
+ * of weight 1/(P spp) (aa.cc:51-77).
  * rays_traced (optional, host) receives the number of rays traced. */
 XTGPU_API xtgpu_status xtgpu_render(xtgpu_scene *scene, const xtgpu_render_params *params, float *rgba_dev,
                           uint64_t *rays_traced, void *stream);
@@ -248,7 +257,7 @@ XTGPU_API xtgpu_status xtgpu_render_host(xtgpu_scene *scene, const xtgpu_render_
  * which the GUI exports as PLY: params->integrator must be XTGPU_DEPTH.
  * raygraph_dev receives 10 floats per sample: the ray origin, the hit point
  * ((0,0,0) on a miss) and the pixel's RGBA after the sample; rectangle pixels
- * row-major, each pixel's aa^2 x spp samples in order. */
+ * row-major, each pixel's positions x spp samples in order. */
 XTGPU_API xtgpu_status xtgpu_render_raygraph(xtgpu_scene *scene, const xtgpu_render_params *params, float *rgba_dev,
                                              float *raygraph_dev, uint64_t *rays_traced, void *stream);
 XTGPU_API xtgpu_status xtgpu_render_raygraph_host(xtgpu_scene *scene, const xtgpu_render_params *params,
@@ -266,7 +275,7 @@ XTGPU_API xtgpu_status xtgpu_write_raygraph_ply(const char *path, int64_t n_path
  * leaves it to another allocator); a render loop that must not meet an
  * allocation failure mid-frame.  Scratch is one static device array of about
  * 11.5 MB held by every GPU that loads the library; a call renders at most
- * XTGPU_NOALLOC_MAX_PATHS paths (rectangle pixels x aa^2 x spp) and larger requests
+ * XTGPU_NOALLOC_MAX_PATHS paths (rectangle pixels x positions x spp) and larger requests
  * return XTGPU_ERR_LIMIT.  Calls that overlap on the GPU race on the shared
  * array.  The first call on a device looks up the array's address; make it
  * before any stream capture.  Output: rgba_dev as in xtgpu_render. */
@@ -322,7 +331,8 @@ typedef struct {
     int32_t width, height, spp, rdepth;
     float ao_max_distance;
     uint64_t seed;
-    int32_t aa;                    /* grid anti-aliasing level, 0 or 1 = pixel centre */
+    int32_t aa;                    /* anti-aliasing level, as xtgpu_render_params::aa */
+    int32_t sample_distribution;   /* XTGPU_SAMPLES_GRID or XTGPU_SAMPLES_RANDOM */
 } xtgpu_job_desc;
 
 typedef struct {

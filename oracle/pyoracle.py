@@ -74,10 +74,20 @@ class XoSceneDesc(C.Structure):
                 ("mat_samplers", C.c_void_p), ("env_texture", C.c_int32)]
 
 
+SAMPLES_GRID, SAMPLES_RANDOM = 0, 1   # aa.h SAMPLE_DISTRIBUTION
+
+
+def sample_positions(aa: int, distribution: int = SAMPLES_GRID) -> int:
+    """Positions per pixel: aa^2 on the grid (aa.cc:7-32), aa jittered ones
+    (aa.cc:34-48); level 0 renders as level 1."""
+    L = max(int(aa), 1)
+    return L if distribution == SAMPLES_RANDOM else L * L
+
+
 class XoRenderParams(C.Structure):
     _fields_ = [("integrator", C.c_int32), ("width", C.c_int32), ("height", C.c_int32),
                 ("spp", C.c_int32), ("rdepth", C.c_int32), ("aa", C.c_int32), ("ao_max_distance", C.c_float),
-                ("seed", C.c_uint64)]
+                ("seed", C.c_uint64), ("distribution", C.c_int32)]
 
 
 _lib = None
@@ -217,25 +227,27 @@ class OracleScene:
         return dict(hit=hit, t=t, obj=obj, prim=prim, point=pt, normal=nr)
 
     def render(self, integrator: int, width: int, height: int, spp: int = 1, rdepth: int = 4,
-               ao_max_distance: float = 100.0, seed: int = 1, pixels: np.ndarray = None, aa: int = 1):
+               ao_max_distance: float = 100.0, seed: int = 1, pixels: np.ndarray = None, aa: int = 1,
+               distribution: int = SAMPLES_GRID):
         if pixels is None:
             ys, xs = np.mgrid[0:height, 0:width]
             pixels = np.stack([xs.ravel(), ys.ravel()], axis=1)
         pixels = np.ascontiguousarray(pixels, np.int32).reshape(-1, 2)
-        p = XoRenderParams(integrator, width, height, spp, rdepth, aa, ao_max_distance, seed)
+        p = XoRenderParams(integrator, width, height, spp, rdepth, aa, ao_max_distance, seed, distribution)
         out = np.zeros((pixels.shape[0], 4), np.float32)
         rays = C.c_uint64(0)
         lib().xo_render(self.handle, C.byref(p), pixels.shape[0], _ptr(pixels), _ptr(out), C.byref(rays))
         return out, int(rays.value)
 
 
-    def render_raygraph(self, width: int, height: int, spp: int = 1, aa: int = 1, pixels: np.ndarray = None):
+    def render_raygraph(self, width: int, height: int, spp: int = 1, aa: int = 1, pixels: np.ndarray = None,
+                        distribution: int = SAMPLES_GRID):
         """The depth integrator's frame and raygraph records (origin, hit point,
         colour after the sample: 10 per sample, pixels in the given order)."""
         pixels = np.ascontiguousarray(pixels, np.int32).reshape(-1, 2)
-        p = XoRenderParams(DEPTH, width, height, spp, 1, aa, 100.0, 1)
+        p = XoRenderParams(DEPTH, width, height, spp, 1, aa, 100.0, 1, distribution)
         out = np.zeros((pixels.shape[0], 4), np.float32)
-        n = pixels.shape[0] * max(aa, 1) ** 2 * spp
+        n = pixels.shape[0] * sample_positions(aa, distribution) * spp
         rec = np.zeros((n, 10), np.float64)
         rays = C.c_uint64(0)
         lib().xo_render_raygraph(self.handle, C.byref(p), pixels.shape[0], _ptr(pixels), _ptr(out), _ptr(rec),
@@ -308,11 +320,12 @@ def ref_available() -> bool:
 
 def ref_render(scn: str, integrator: str, width: int, height: int, spp: int = 1, aa: int = 1, rdepth: int = 4,
                threads: int = 1, seed: int = 1, tiles=None, ao_max_distance: float = None, workdir: str = "/tmp",
-               raygraph: str = None):
+               raygraph: str = None, distribution: int = SAMPLES_GRID):
     """Runs the reference integrator through IIntegrator::render on the given tiles
     ((x0,y0,x1,y1) list, or None for 32-pixel tiles over the frame).  Returns
     (pixels xy, rgba, stats dict with render_s / rays / threads).  raygraph: a
-    path to write the tiles' raygraph to as PLY (the GUI's export)."""
+    path to write the tiles' raygraph to as PLY (the GUI's export).  The random
+    distribution's offsets come from libc rand(), seeded once from time()."""
     import json
     import tempfile
     fd, out = tempfile.mkstemp(suffix=".bin", dir=workdir)
@@ -324,10 +337,12 @@ def ref_render(scn: str, integrator: str, width: int, height: int, spp: int = 1,
             fh.write("".join("%d %d %d %d\n" % tuple(t) for t in tiles))
     cmd = [REF_BIN, "render", scn, integrator, str(width), str(height), str(spp), str(aa), str(rdepth),
            str(threads), str(seed), tfile, out]
-    if ao_max_distance is not None or raygraph:
+    if ao_max_distance is not None or raygraph or distribution:
         cmd.append(repr(float(ao_max_distance if ao_max_distance is not None else 100.0)))
-    if raygraph:
-        cmd.append(raygraph)
+    if raygraph or distribution:
+        cmd.append(raygraph or "-")
+    if distribution:
+        cmd.append(str(int(distribution)))
     env = dict(os.environ)
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)

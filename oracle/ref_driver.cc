@@ -9,6 +9,7 @@
 //
 // Modes
 //   xtref render <scn> <integrator> W H spp aa rdepth threads seed <tiles.txt|-> <out.bin> [ao_maxdist]
+//                [raygraph.ply|-] [distribution: 0 grid, 1 random]
 //   xtref hits   <scn> W H <tiles.txt|-> <out.bin> [mesh.obj]
 //   xtref kat    <in.txt> <out.txt>
 //
@@ -167,6 +168,7 @@ static int mode_render(int argc, char **argv)
     const char *tiles_path = argv[11], *out = argv[12];
     float ao_maxd = argc > 13 ? (float)atof(argv[13]) : 100.0f;
     const char *raygraph_out = argc > 14 ? argv[14] : 0;
+    const int random = argc > 15 && atoi(argv[15]) == 1;
 
     xtcore::init();
     xtcore::render::context_t ctx;
@@ -176,6 +178,8 @@ static int mode_render(int argc, char **argv)
     ctx.params.height = h;
     ctx.params.samples = spp;
     ctx.params.aa = aa;
+    ctx.params.sample_distribution = random ? xtcore::antialiasing::SAMPLE_DISTRIBUTION_RANDOM
+                                            : xtcore::antialiasing::SAMPLE_DISTRIBUTION_GRID;
     ctx.params.rdepth = rdepth;
     ctx.params.threads = threads;
     ctx.params.camera = cam;

@@ -100,6 +100,12 @@ double xo_stream_uniform(uint64_t key, uint32_t counter)
     return (double)(uint32_t)(x >> 40) * (1.0 / 16777216.0);
 }
 
+uint64_t xo_jitter_key(uint64_t seed, int32_t position, int32_t width, int32_t height, int32_t x, int32_t y)
+{
+    return xo_path_key(seed ^ XO_JITTER_SALT, (uint64_t)position * (uint64_t)width * (uint64_t)height +
+                                                 (uint64_t)y * (uint64_t)width + (uint64_t)x);
+}
+
 /* prng_c(a, b) (lib/nmath/prng.inl:54-83): rand() * ((b - a) / RAND_MAX) + a. */
 static double prng(rng_t *r, double a, double b)
 {
@@ -1125,24 +1131,32 @@ static int render_impl(const xo_scene *s, const xo_render_params *p, int64_t npi
 {
     const xo_scene_desc *D = &s->d;
     uint64_t nr = 0;
-    /* aa.cc:7-32, 51-77: per pixel aa^2 grid positions (rows of the grid in
-     * order), each taken spp times; weight 1/(aa^2) as a float, times 1/spp */
+    /* aa.cc:7-48, 51-77: per pixel P positions, each taken spp times: the
+     * grid's aa^2 (rows of the grid in order) or the random distribution's aa
+     * jittered ones; weight 1/P as a float, times 1/spp */
+    const int random = p->distribution == XO_SAMPLES_RANDOM;
     const int32_t L = p->aa > 1 ? p->aa : 1;
-    double weight = L == 1 ? 1.f : (double)(1.f / (float)(L * L));
+    const int32_t P = random ? L : L * L;
+    double weight = P == 1 ? 1.f : (double)(1.f / (float)P);
     weight *= 1. / (double)p->spp;
     const float sub_pixel = 1.f / (float)L, offset = sub_pixel * 0.5f;
     for (int64_t i = 0; i < npix; ++i) {
         int32_t x = px[2 * i], y = px[2 * i + 1];
         float col[4] = {0, 0, 0, 0};
-        for (int32_t si = 0; si < L * L * p->spp; ++si) {
+        for (int32_t si = 0; si < P * p->spp; ++si) {
             rng_t r;
             memset(&r, 0, sizeof(r));
             r.kind = XO_RNG_STREAM;
             r.key = xo_path_key(p->seed, (uint64_t)si * (uint64_t)p->width * (uint64_t)p->height +
                                              (uint64_t)y * (uint64_t)p->width + (uint64_t)x);
-            const int32_t gi = si / p->spp;   /* grid position of the sample */
+            const int32_t gi = si / p->spp;   /* position of the sample */
             double cx = (double)x + 0.5f, cy = (double)y + 0.5f;
-            if (L > 1) {
+            if (random) {
+                /* gen_samples_random (aa.cc:34-48): pixel + (float)prng_c(0, 1) per axis */
+                const uint64_t jk = xo_jitter_key(p->seed, gi, p->width, p->height, x, y);
+                cx = (double)x + (double)(float)xo_stream_uniform(jk, 0);
+                cy = (double)y + (double)(float)xo_stream_uniform(jk, 1);
+            } else if (L > 1) {
                 cx = ((double)x + (double)(gi % L) * (double)sub_pixel) + (double)offset;
                 cy = ((double)y + (double)(gi / L) * (double)sub_pixel) + (double)offset;
             }
@@ -1169,7 +1183,7 @@ static int render_impl(const xo_scene *s, const xo_render_params *p, int64_t npi
                 }
                 col[3] = 1;
                 if (raygraph) {
-                    double *rg = raygraph + 10 * (i * (int64_t)L * L * p->spp + si);
+                    double *rg = raygraph + 10 * (i * (int64_t)P * p->spp + si);
                     rg[0] = O.x; rg[1] = O.y; rg[2] = O.z;
                     rg[3] = dhit ? h.point.x : 0.0; rg[4] = dhit ? h.point.y : 0.0; rg[5] = dhit ? h.point.z : 0.0;
                     for (int k = 0; k < 4; ++k) rg[6 + k] = col[k];

@@ -115,10 +115,17 @@ void xo_camera_ray(const float pos[3], const float target[3], const float up[3],
 typedef struct {
     int32_t integrator;    /* XO_STENCIL .. XO_WIREFRAME */
     int32_t width, height, spp, rdepth;
-    int32_t aa;            /* grid anti-aliasing level (aa.cc:7-32); 0 or 1 = pixel centre */
+    int32_t aa;            /* anti-aliasing level; grid (aa.cc:7-32): 0 or 1 = pixel centre */
     float ao_max_distance; /* 100 in the shipped AO integrator */
     uint64_t seed;         /* XO_RNG_STREAM key */
+    int32_t distribution;  /* XO_SAMPLES_GRID or XO_SAMPLES_RANDOM (aa.h SAMPLE_DISTRIBUTION) */
 } xo_render_params;
+
+/* Sample distributions (aa.cc:7-48).  RANDOM takes aa positions per pixel at
+ * offsets drawn from a stream keyed by (seed ^ XO_JITTER_SALT, position,
+ * pixel) where the reference draws libc rand(). */
+enum { XO_SAMPLES_GRID = 0, XO_SAMPLES_RANDOM = 1 };
+#define XO_JITTER_SALT 0xA0761D6478BD642FULL
 
 /* Renders the listed pixels (x,y pairs): aa^2 grid positions per pixel, each
  * taken `spp` times with weight 1/(aa^2 spp) (aa.cc:7-32, 51-77).  Output RGBA
@@ -164,6 +171,8 @@ void xo_kat_camera_cubemap(const float pos[3], float x, float y, float w, float 
 /* The counter stream shared with the GPU path, exposed for tests. */
 double xo_stream_uniform(uint64_t key, uint32_t counter);
 uint64_t xo_path_key(uint64_t seed, uint64_t path);
+/* Key of the random distribution's offsets of one position of one pixel. */
+uint64_t xo_jitter_key(uint64_t seed, int32_t position, int32_t width, int32_t height, int32_t x, int32_t y);
 
 #ifdef __cplusplus
 }

@@ -33,7 +33,10 @@ these fixtures are what pins the oracle restatement (oracle/xtoracle.c):
 * render_mtl.npz  frames of meshes loaded from an OBJ with an MTL library
               (BlinnPhong / Emissive materials, map_Kd / map_Ks / map_Ke
               textures): depth, uv, emission, depth-1 pathtracer, and a
-              depth-4 pathtracer at four seeds (`--mtl`).
+              depth-4 pathtracer at four seeds (`--mtl`);
+* render_random.npz  stencil and depth frames with the random sample
+              distribution (aa.cc:34-48) at four seeds, one reproducible set of
+              rand() jitter offsets each (`--random`).
 
 Run here (needs the reference sources and oracle/_ref/xtref):
     make -f oracle/ref.mk REF=<xtracer source tree> -j8
@@ -431,6 +434,35 @@ def make_mtl(work):
     print("render_mtl.npz", sorted(rend))
 
 
+def random_case():
+    """(camera, width, height, spp, (integrator, aa) pairs, seeds) of the random
+    sample distribution fixture."""
+    cam = scenes.Camera((0.0, 6.0, -14.0), (0.0, 1.0, 0.0), (0.0, 1.0, 0.0), 60.0)
+    return cam, 48, 40, 2, [("stencil", 1), ("stencil", 4), ("depth", 4)], (41, 42, 43, 44)
+
+
+def make_random(work):
+    """Frames of the random sample distribution (aa.cc:34-48): the reference
+    seeds rand() from time(), which the driver fixes to the given seed, so
+    each seed is one reproducible draw of the jitter offsets."""
+    cam, w, h, spp, cases, seeds = random_case()
+    spec = scenes.spheres_scene(64, seed=1, name="cam_random", camera=cam)
+    scn = spec.write_scn(work)
+    rend = {}
+    for integ, aa in cases:
+        imgs, rays = [], []
+        for seed in seeds:
+            xy, rgba, st = po.ref_render(scn, integ, w, h, spp=spp, aa=aa, threads=1, seed=seed, workdir=work,
+                                         distribution=po.SAMPLES_RANDOM)
+            imgs.append(rgba)
+            rays.append(st["rays"])
+        rend["%s_aa%d_xy" % (integ, aa)] = xy
+        rend["%s_aa%d_rgba" % (integ, aa)] = np.stack(imgs)
+        rend["%s_aa%d_rays" % (integ, aa)] = np.array(rays, np.int64)
+    np.savez_compressed(os.path.join(HERE, "render_random.npz"), **rend)
+    print("render_random.npz", sorted(rend))
+
+
 def texture_frame_size():
     return 64, 48
 
@@ -459,6 +491,9 @@ def main():
         return
     if "--raygraph" in sys.argv:
         make_raygraph(tempfile.mkdtemp(prefix="xtgold"))
+        return
+    if "--random" in sys.argv:
+        make_random(tempfile.mkdtemp(prefix="xtgold"))
         return
     if "--textures" in sys.argv:
         make_textures(tempfile.mkdtemp(prefix="xtgold"), np.random.default_rng(20261205))

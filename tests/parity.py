@@ -104,3 +104,37 @@ def classify(spec, org, dirs, g_hit, g_gid, g_t, r_hit, r_gid, r_t, tie_rel=1e-5
             else:
                 bad.append(i)
     return int(agree.sum()), tie, graze_n, bad
+
+
+def random_distribution_agreement(R, O, channel, aa=None):
+    """Checks frames of the random sample distribution (aa.cc:34-48) from two
+    sources of jitter offsets against each other: R, the reference's frames at
+    several seeds (libc rand()), and O, frames from this library's stream at as
+    many seeds, both (seeds, pixels, 4) in the same pixel order.
+
+    * the frame mean of `channel` agrees within 4.5 standard errors (the
+      per-pixel variance across seeds of both sides);
+    * the per-pixel mean over seeds differs between the sources by at most 1.5
+      times what it differs between two halves of the seeds of one source;
+    * for stencil (channel 3, given aa): every coverage value is a multiple of
+      1/aa (each position's spp samples see the same ray), the sources use the
+      same values, and the fraction of partly covered pixels agrees within
+      4.5 binomial standard errors."""
+    r = np.asarray(R, np.float64)[..., channel]
+    o = np.asarray(O, np.float64)[..., channel]
+    n, npix = r.shape
+    assert o.shape == r.shape
+    se = np.sqrt((r.var(0, ddof=1).sum() + o.var(0, ddof=1).sum()) / n) / npix
+    assert abs(r.mean() - o.mean()) <= 4.5 * se + 1e-6, (r.mean(), o.mean(), se)
+    h = n // 2
+    split = 0.5 * (np.abs(r[:h].mean(0) - r[h:].mean(0)).mean() + np.abs(o[:h].mean(0) - o[h:].mean(0)).mean())
+    cross = np.abs(r.mean(0) - o.mean(0)).mean()
+    assert cross <= 1.5 * split + 1e-6, (cross, split)
+    if aa is not None:
+        for x in (r, o):
+            k = x * aa
+            assert np.allclose(k, np.round(k), atol=1e-5), np.unique(x)
+        assert set(np.round(r * aa).astype(int).ravel()) == set(np.round(o * aa).astype(int).ravel())
+        pr, po_ = ((r > 0) & (r < 1)).mean(), ((o > 0) & (o < 1)).mean()
+        p = 0.5 * (pr + po_)
+        assert abs(pr - po_) <= 4.5 * np.sqrt(p * (1 - p) * 2.0 / r.size) + 1e-9, (pr, po_)

@@ -163,3 +163,37 @@ def test_scene_update_arguments_are_checked_without_device_work():
     d = xtgpu.SceneDesc()
     assert L.xtgpu_scene_update(None, C.byref(d), 1, None) == 1
     assert L.xtgpu_service_update_scene(None, 0) == 1
+
+
+def test_ctypes_structs_match_the_c_header(tmp_path):
+    """Every structure of include/xtgpu.h that the Python binding mirrors has
+    the header's size and field offsets (compiled with gcc here)."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    from xtracer_b200 import xtgpu
+    pairs = {"xtgpu_material": xtgpu.Material, "xtgpu_camera": xtgpu.CameraDesc, "xtgpu_texture": xtgpu.Texture,
+             "xtgpu_sampler": xtgpu.SamplerDesc, "xtgpu_scene_desc": xtgpu.SceneDesc,
+             "xtgpu_bvh_opts": xtgpu.BvhOpts, "xtgpu_bvh_info": xtgpu.BvhInfo, "xtgpu_hit": xtgpu.Hit,
+             "xtgpu_render_params": xtgpu.RenderParams, "xtgpu_service_opts": xtgpu.ServiceOpts,
+             "xtgpu_service_stats": xtgpu.ServiceStats, "xtgpu_tuning": xtgpu.Tuning,
+             "xtgpu_job_desc": xtgpu.JobDesc, "xtgpu_job_status": xtgpu.JobStatus}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "xtgpu.h"', "int main(void) {"]
+    for cname, py in pairs.items():
+        lines.append('printf("%s %%zu\\n", sizeof(%s));' % (cname, cname))
+        for f in py._fields_:
+            lines.append('printf("%s.%s %%zu\\n", offsetof(%s, %s));' % (cname, f[0], cname, f[0]))
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    exe = tmp_path / "layout"
+    subprocess.run([gcc, "-I", inc, str(src), "-o", str(exe)], check=True)
+    out = dict(l.split() for l in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                 text=True).stdout.splitlines())
+    for cname, py in pairs.items():
+        assert int(out[cname]) == C.sizeof(py), cname
+        for f in py._fields_:
+            assert int(out["%s.%s" % (cname, f[0])]) == getattr(py, f[0]).offset, (cname, f[0])

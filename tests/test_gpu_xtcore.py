@@ -123,6 +123,25 @@ def test_cameras_and_aa_in_host_equal_c_abi(tmp_path, cam, w, h):
         assert np.array_equal(got, ref, equal_nan=True), NAMES[kind]
 
 
+def test_random_distribution_in_host_equals_c_abi(tmp_path):
+    """params_t::sample_distribution = RANDOM reaches the GPU: aa jittered
+    positions per pixel, the frame equal to the C ABI's with the same seed;
+    aa = 0 with it writes no pixel, as the CPU integrators do."""
+    spec = scenes.spheres_scene(64, seed=1, name="hostrnd")
+    scn = spec.write_scn(str(tmp_path))
+    sc = xtgpu.Scene(spec)
+    for kind, spp, aa in ((xtgpu.DEPTH, 2, 3), (xtgpu.AO, 2, 5), (xtgpu.STENCIL, 1, 1)):
+        got = render_host(scn, kind, 48, 40, spp, 1, tmp_path / "f.bin", "--aa", str(aa), "--random",
+                          "--ao-distance", "0.5", "--seed", "9")
+        ref, _ = sc.render(kind, 48, 40, spp=spp, rdepth=1, ao_max_distance=0.5, seed=9, aa=aa,
+                           distribution=xtgpu.SAMPLES_RANDOM)
+        assert np.array_equal(got, ref, equal_nan=True), NAMES[kind]
+    sc.close()
+    gpu = render_host(scn, xtgpu.STENCIL, 32, 24, 1, 1, tmp_path / "g0.bin", "--aa", "0", "--random")
+    cpu = render_host(scn, xtgpu.STENCIL, 32, 24, 1, 1, tmp_path / "c0.bin", "--aa", "0", "--random", "--cpu")
+    assert np.array_equal(gpu, cpu)
+
+
 def test_aa_zero_writes_no_pixel(written):
     """aa = 0: antialiasing::produce gives the tiles no samples (aa.cc:9), so
     the frame keeps what tile->init wrote, as with the CPU integrators."""

@@ -399,3 +399,31 @@ def test_obj_mtl_frames_golden():
                                                         pixels=g["pt_xy"])
     got, ref = stochastic_agreement(O, g["pt_rgba"])
     assert got <= 1.25 * ref + 1e-6, (got, ref)
+
+
+def test_random_distribution_within_reference_noise():
+    """The random sample distribution (aa.cc:34-48): aa positions per pixel,
+    each taken spp times at weight 1/(aa spp).  The reference draws the jitter
+    offsets from rand(); the oracle from a stream keyed by (seed, position,
+    pixel).  Rays traced are equal, stencil coverage takes the same multiples
+    of 1/aa, and stencil and depth frames agree within the noise of four
+    seeds on each side."""
+    import importlib.util
+    from tests.parity import random_distribution_agreement
+    spec_ = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLD, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec_)
+    spec_.loader.exec_module(mg)
+    cam, w, h, spp, cases, seeds = mg.random_case()
+    g = np.load(os.path.join(GOLD, "render_random.npz"))
+    orc = po.OracleScene(scenes.spheres_scene(64, seed=1, name="cam_random", camera=cam), po.XO_ACCEL_BVH)
+    for integ, aa in cases:
+        key = "%s_aa%d" % (integ, aa)
+        code = po.STENCIL if integ == "stencil" else po.DEPTH
+        O = []
+        for s, ref_rays in zip(seeds, g[key + "_rays"]):
+            o, rays = orc.render(code, w, h, spp=spp, seed=s, pixels=g[key + "_xy"], aa=aa,
+                                 distribution=po.SAMPLES_RANDOM)
+            assert rays == int(ref_rays) == w * h * aa * spp
+            O.append(o)
+        random_distribution_agreement(g[key + "_rgba"], np.stack(O), 3 if integ == "stencil" else 0,
+                                      aa if integ == "stencil" else None)

@@ -105,10 +105,12 @@ bool camera_valid(const xtgpu_camera &c)
 
 // The frame a camera can render and the grid level: a cubemap is a vertical
 // strip of six square faces, so its height must split into them.
-bool view_valid(const DevCamera &c, int width, int height, int aa)
+bool view_valid(const DevCamera &c, int width, int height, int aa, int dist, int spp)
 {
     (void)width;
-    if (aa < 0 || aa > MAX_AA) return false;
+    if (dist != XTGPU_SAMPLES_GRID && dist != XTGPU_SAMPLES_RANDOM) return false;
+    if (aa < 0 || aa > (dist == XTGPU_SAMPLES_RANDOM ? MAX_AA * MAX_AA : MAX_AA)) return false;
+    if (spp <= 0 || (int64_t)sample_positions(aa, dist) * spp > INT32_MAX) return false;
     return c.type != XTGPU_CAM_CUBEMAP || (height >= 6 && height % 6 == 0);
 }
 
@@ -695,8 +697,9 @@ xtgpu_status xtg::render_impl(xtgpu_scene *sc, const xtgpu_render_params *p, flo
         set_error("xtgpu_render: bad parameters");
         return XTGPU_ERR_INVALID;
     }
-    if (!view_valid(sc->dev.cam, p->width, p->height, p->aa)) {
-        set_error("xtgpu_render: aa outside 0..16, or a cubemap height that is not six square faces");
+    if (!view_valid(sc->dev.cam, p->width, p->height, p->aa, p->sample_distribution, p->spp)) {
+        set_error("xtgpu_render: sample_distribution not grid or random, aa outside 0..16 (grid) or 0..256 "
+                  "(random), samples per pixel above 2^31, or a cubemap height that is not six square faces");
         return XTGPU_ERR_INVALID;
     }
     int x0 = p->x0, y0 = p->y0, x1 = p->x1, y1 = p->y1;
@@ -712,8 +715,7 @@ xtgpu_status xtg::render_impl(xtgpu_scene *sc, const xtgpu_render_params *p, flo
     XTG_TRY(check_format(sc, p->node_format));
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t npix = (int64_t)(x1 - x0) * (y1 - y0);
-    const int64_t aa = p->aa > 1 ? p->aa : 1;
-    const int64_t paths = npix * aa * aa * p->spp;
+    const int64_t paths = npix * sample_positions(p->aa, p->sample_distribution) * p->spp;
     const int64_t cap = std::min<int64_t>(paths, T.wave_paths);
     std::lock_guard<std::mutex> lock(g_runner_mu);
     WaveRunner *R = nullptr;
@@ -733,7 +735,7 @@ xtgpu_status xtg::render_impl(xtgpu_scene *sc, const xtgpu_render_params *p, flo
     J.integrator = p->integrator;
     J.width = p->width;
     J.height = p->height;
-    set_samples(J, p->spp, p->aa);
+    set_samples(J, p->spp, p->aa, p->sample_distribution);
     J.rdepth = p->rdepth;
     J.ao_maxd = p->ao_max_distance;
     J.seed = p->seed;
@@ -790,12 +792,12 @@ xtgpu_status xtgpu_render_raygraph_host(xtgpu_scene *sc, const xtgpu_render_para
     }
     const int64_t w = (p->x1 == 0 && p->y1 == 0) ? p->width : p->x1 - p->x0;
     const int64_t h = (p->x1 == 0 && p->y1 == 0) ? p->height : p->y1 - p->y0;
-    const int64_t aa = p->aa > 1 ? p->aa : 1;
-    if (w <= 0 || h <= 0 || p->spp <= 0 || p->aa < 0 || p->aa > MAX_AA) {
+    if (w <= 0 || h <= 0 || p->spp <= 0 || p->aa < 0 || p->aa > MAX_AA * MAX_AA ||
+        (p->sample_distribution != XTGPU_SAMPLES_GRID && p->sample_distribution != XTGPU_SAMPLES_RANDOM)) {
         set_error("xtgpu_render_raygraph_host: bad rectangle or samples");
         return XTGPU_ERR_INVALID;
     }
-    const int64_t paths = w * h * aa * aa * p->spp;
+    const int64_t paths = w * h * sample_positions(p->aa, p->sample_distribution) * p->spp;
     cudaStream_t s = (cudaStream_t)stream;
     float *d = nullptr, *r = nullptr;
     XTG_CUDA(cudaMallocAsync((void **)&d, sizeof(float4) * w * h, s));

@@ -94,8 +94,9 @@ extern "C" xtgpu_status xtgpu_render_tile_noalloc(xtgpu_scene *sc, const xtgpu_r
         set_error("xtgpu_render_tile_noalloc: bad parameters");
         return XTGPU_ERR_INVALID;
     }
-    if (!view_valid(sc->dev.cam, p->width, p->height, p->aa)) {
-        set_error("xtgpu_render_tile_noalloc: aa outside 0..16, or a cubemap height that is not six square faces");
+    if (!view_valid(sc->dev.cam, p->width, p->height, p->aa, p->sample_distribution, p->spp)) {
+        set_error("xtgpu_render_tile_noalloc: sample_distribution not grid or random, aa outside 0..16 (grid) or "
+                  "0..256 (random), samples per pixel above 2^31, or a cubemap height that is not six square faces");
         return XTGPU_ERR_INVALID;
     }
     int x0 = p->x0, y0 = p->y0, x1 = p->x1, y1 = p->y1;
@@ -109,10 +110,9 @@ extern "C" xtgpu_status xtgpu_render_tile_noalloc(xtgpu_scene *sc, const xtgpu_r
         return XTGPU_ERR_INVALID;
     }
     const int64_t npix = (int64_t)(x1 - x0) * (y1 - y0);
-    const int64_t aa = p->aa > 1 ? p->aa : 1;
-    const int64_t paths = npix * aa * aa * p->spp;
+    const int64_t paths = npix * sample_positions(p->aa, p->sample_distribution) * p->spp;
     if (paths > NA_PATHS) {
-        set_error("xtgpu_render_tile_noalloc: rectangle pixels x aa^2 x spp exceeds the 65536-path scratch array; "
+        set_error("xtgpu_render_tile_noalloc: rectangle pixels x positions x spp exceeds the 65536-path scratch array; "
                   "split the frame into smaller tiles");
         return XTGPU_ERR_LIMIT;
     }
@@ -150,7 +150,7 @@ extern "C" xtgpu_status xtgpu_render_tile_noalloc(xtgpu_scene *sc, const xtgpu_r
     J.integrator = p->integrator;
     J.width = p->width;
     J.height = p->height;
-    set_samples(J, p->spp, p->aa);
+    set_samples(J, p->spp, p->aa, p->sample_distribution);
     J.rdepth = p->rdepth;
     J.ao_maxd = p->ao_max_distance;
     J.seed = p->seed;

@@ -545,10 +545,19 @@ __global__ void k_camera(const DevJob *__restrict__ jobs, const DevScene *__rest
         int64_t s = p / npix, pix = p - s * npix;
         int x, y;
         pixel_of(J, pix, x, y);
-        // grid position of the sample (aa.cc:51-77): aa^2 positions per
-        // pixel, rows in order, each taken spp1 times
+        // position of the sample (aa.cc:7-77), each taken spp1 times: the
+        // grid's aa^2 (rows in order) or aa jittered ones
         float cx = (float)x + 0.5f, cy = (float)y + 0.5f;
-        if (J.aa > 1) {
+        if (J.dist == XTGPU_SAMPLES_RANDOM) {
+            // gen_samples_random (aa.cc:34-48): pixel + (float)prng_c(0, 1) per axis
+            const uint64_t jk = path_key(J.seed ^ JITTER_SALT, (uint64_t)(s / J.spp1) * (uint64_t)J.width *
+                                                                   (uint64_t)J.height +
+                                                               (uint64_t)y * (uint64_t)J.width + (uint64_t)x);
+            uint32_t jc = 0;
+            const float u = uniform(jk, jc), v = uniform(jk, jc);
+            cx = (float)__dadd_rn((double)x, (double)u);
+            cy = (float)__dadd_rn((double)y, (double)v);
+        } else if (J.aa > 1) {
             const int gi = (int)(s / J.spp1);
             const float sub = __fdiv_rn(1.f, (float)J.aa), off = __fmul_rn(sub, 0.5f);
             cx = (float)__dadd_rn(__dadd_rn((double)x, __dmul_rn((double)(gi % J.aa), (double)sub)), (double)off);

@@ -159,7 +159,7 @@ static xtgpu_status launch_wave(xtgpu_service *v, WaveSlot &W, cudaEvent_t prev_
         dj.integrator = J.d.integrator;
         dj.width = J.d.width;
         dj.height = J.d.height;
-        set_samples(dj, J.d.spp, J.d.aa);
+        set_samples(dj, J.d.spp, J.d.aa, J.d.sample_distribution);
         dj.rdepth = J.d.rdepth;
         dj.ao_maxd = J.d.ao_max_distance;
         dj.seed = J.d.seed;
@@ -433,12 +433,12 @@ xtgpu_status xtgpu_service_submit(xtgpu_service *v, const xtgpu_job_desc *d, dou
         set_error("xtgpu_service_submit: bad job");
         return XTGPU_ERR_INVALID;
     }
-    if (!view_valid(v->scenes[d->scene]->dev.cam, d->width, d->height, d->aa)) {
-        set_error("xtgpu_service_submit: aa outside 0..16, or a cubemap height that is not six square faces");
+    if (!view_valid(v->scenes[d->scene]->dev.cam, d->width, d->height, d->aa, d->sample_distribution, d->spp)) {
+        set_error("xtgpu_service_submit: sample_distribution not grid or random, aa outside 0..16 (grid) or 0..256 "
+                  "(random), samples per pixel above 2^31, or a cubemap height that is not six square faces");
         return XTGPU_ERR_INVALID;
     }
-    const int64_t aa = d->aa > 1 ? d->aa : 1;
-    int64_t paths = (int64_t)d->width * d->height * aa * aa * d->spp;
+    int64_t paths = (int64_t)d->width * d->height * sample_positions(d->aa, d->sample_distribution) * d->spp;
     if (paths <= 0 || paths > (1ll << 40)) {
         set_error("xtgpu_service_submit: job too large");
         return XTGPU_ERR_INVALID;

@@ -22,7 +22,7 @@ namespace xtg {
 // One job's share of a wave.
 struct DevJob {
     int32_t integrator, width, height;
-    int32_t spp;                     // samples per pixel: aa^2 grid positions x spp1
+    int32_t spp;                     // samples per pixel: positions x spp1
     int32_t rdepth;
     float ao_maxd;
     uint64_t seed;
@@ -34,23 +34,38 @@ struct DevJob {
     int64_t first;                   // first path id of the job in this wave
     int64_t count;                   // paths of the job in this wave
     int64_t offset;                  // wave-local index of the job's first path
-    int32_t aa;                      // grid anti-aliasing level (1 = pixel centre)
-    int32_t spp1;                    // samples per grid position
-    double wt;                       // weight of one sample: 1/(aa^2) as a float, times 1/spp1
+    int32_t aa;                      // anti-aliasing level (grid: 1 = pixel centre)
+    int32_t spp1;                    // samples per position
+    double wt;                       // weight of one sample: 1/positions as a float, times 1/spp1
     float *raygraph;                 // depth integrator: 10 floats per sample (origin, hit
                                      // point, colour after the sample), rectangle pixels
                                      // row-major, each pixel's samples in order; or null
+    int32_t dist;                    // XTGPU_SAMPLES_GRID or XTGPU_SAMPLES_RANDOM
 };
 
-// Fills the sample fields of a job from params_t's samples and aa (aa.cc:7-32,
-// 51-77): aa^2 positions of weight 1.f/(aa*aa) each taken spp times at 1/spp.
-inline void set_samples(DevJob &j, int spp, int aa)
+// Key of the random distribution's offsets of one position of one pixel: a
+// stream apart from the paths' (seed ^ this salt).
+constexpr uint64_t JITTER_SALT = 0xA0761D6478BD642Full;
+
+// Positions per pixel (aa.cc:7-48): the grid's aa^2, the random
+// distribution's aa; level 0 renders as level 1.
+inline int sample_positions(int aa, int dist)
 {
     const int L = aa > 1 ? aa : 1;
+    return dist == XTGPU_SAMPLES_RANDOM ? L : L * L;
+}
+
+// Fills the sample fields of a job from params_t's samples, aa and
+// sample_distribution (aa.cc:7-77): P positions of weight 1.f/P each taken
+// spp times at 1/spp.
+inline void set_samples(DevJob &j, int spp, int aa, int dist)
+{
+    const int L = aa > 1 ? aa : 1, P = sample_positions(aa, dist);
     j.aa = L;
+    j.dist = dist;
     j.spp1 = spp;
-    j.spp = L * L * spp;
-    j.wt = (L == 1 ? 1.0 : (double)(1.f / (float)(L * L))) * (1.0 / (double)spp);
+    j.spp = P * spp;
+    j.wt = (P == 1 ? 1.0 : (double)(1.f / (float)P)) * (1.0 / (double)spp);
 }
 
 struct WaveQueues {

@@ -68,7 +68,8 @@ struct DevCamera {
     float ipd;            // ODS
     float flength, aperture;   // perspective depth of field (flength > 0)
 };
-// grid anti-aliasing levels accepted (aa^2 rays per sample)
+// anti-aliasing levels accepted: grid up to 16 (aa^2 positions per pixel),
+// random up to 256 (aa positions)
 constexpr int MAX_AA = 16;
 
 // Everything a kernel needs to intersect and shade one scene.
@@ -169,10 +170,11 @@ inline bool format_built(const xtgpu_scene *sc, int f)
 int stack_for_scene(const xtgpu_scene *sc, int f, int requested);
 
 // cameras: the device form of a camera, whether a camera description is
-// acceptable, and whether a frame size and grid level suit a camera
+// acceptable, and whether a frame size suits a camera and the samples
+// (distribution, level, samples per position) are within range
 DevCamera make_camera(const xtgpu_camera &c);
 bool camera_valid(const xtgpu_camera &c);
-bool view_valid(const DevCamera &c, int width, int height, int aa);
+bool view_valid(const DevCamera &c, int width, int height, int aa, int dist, int spp);
 
 // the tuning a scene renders with: its own if autotuned, else the process-wide one
 const xtgpu_tuning &scene_tuning(const xtgpu_scene *sc);

@@ -33,9 +33,10 @@ class Service:
         check(lib().xtgpu_service_update_scene(self.handle, self.scene_ids[scene]))
 
     def submit(self, scene: int, integrator: int, width: int, height: int, spp: int, rdepth: int = 4,
-               ao_max_distance: float = 100.0, seed: int = 1, submit_s: float = -1.0, aa: int = 1) -> int:
+               ao_max_distance: float = 100.0, seed: int = 1, submit_s: float = -1.0, aa: int = 1,
+               distribution: int = xtgpu.SAMPLES_GRID) -> int:
         d = xtgpu.JobDesc(self.scene_ids[scene], integrator, width, height, spp, rdepth, ao_max_distance, seed,
-                          aa)
+                          aa, distribution)
         jid = C.c_int64()
         check(lib().xtgpu_service_submit(self.handle, C.byref(d), submit_s, C.byref(jid)))
         self.shapes[jid.value] = (height, width)

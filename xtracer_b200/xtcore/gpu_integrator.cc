@@ -435,10 +435,7 @@ void Integrator::invalidate_shading()
 xtgpu_status Integrator::render_frame()
 {
     xtcore::render::params_t &p = ctx->params;
-    if (p.aa > 1 && p.sample_distribution != xtcore::antialiasing::SAMPLE_DISTRIBUTION_GRID) {
-        m_error = "aa > 1 is supported with the grid sample distribution only";
-        return XTGPU_ERR_INVALID;
-    }
+    const bool random = p.sample_distribution == xtcore::antialiasing::SAMPLE_DISTRIBUTION_RANDOM;
     // aa = 0 or samples = 0: antialiasing::produce gives the tiles no samples
     // (aa.cc:9, 67), so the CPU integrators write no pixel
     m_empty = p.aa == 0 || p.samples == 0;
@@ -512,13 +509,14 @@ xtgpu_status Integrator::render_frame()
     rp.x1 = (int32_t)x1;
     rp.y1 = (int32_t)y1;
     rp.aa = (int32_t)p.aa;
+    rp.sample_distribution = random ? XTGPU_SAMPLES_RANDOM : XTGPU_SAMPLES_GRID;
     m_x0 = x0;
     m_y0 = y0;
     m_w = x1 - x0;
     m_h = y1 - y0;
     m_frame.assign(4 * m_w * m_h, 0.f);
     xtgpu_status st;
-    m_spx = (size_t)(p.aa > 1 ? p.aa * p.aa : 1) * p.samples;
+    m_spx = (size_t)(random ? p.aa : p.aa * p.aa) * p.samples;
     if (m_kind == XTGPU_DEPTH && record_raygraph) {
         // the depth integrator's raygraph (depth/integrator.cc:43-51)
         m_raygraph.assign(10 * m_w * m_h * m_spx, 0.f);

@@ -12,7 +12,9 @@
 //       --ao-distance D  AO occlusion distance (GPU), default 100
 //       --threads N    OpenMP threads of the tile loop, default all
 //       --tile N       tile size, default 32 (context.cc:5)
-//       --aa N         anti-aliasing level (grid distribution), default 1
+//       --aa N         anti-aliasing level, default 1
+//       --random       the random sample distribution (aa jittered positions
+//                      per pixel) instead of the grid
 //       --raygraph P   the depth integrator's raygraph as PLY, exported the
 //                      GUI's way (render::assemble + raygraph::write)
 //       --then-camera N  render once more through the scene's camera N (the
@@ -162,7 +164,7 @@ int mode_render(int argc, char **argv)
     size_t w = strtoul(argv[4], 0, 10), h = strtoul(argv[5], 0, 10);
     size_t spp = strtoul(argv[6], 0, 10), rdepth = strtoul(argv[7], 0, 10);
     const char *out = argv[8];
-    bool cpu = false, q8 = false, w8 = false;
+    bool cpu = false, q8 = false, w8 = false, random = false;
     unsigned long long seed = 1;
     float aod = 100.f;
     size_t threads = 0, tile = 32, aa = 1;
@@ -177,6 +179,7 @@ int mode_render(int argc, char **argv)
         else if (a == "--threads" && i + 1 < argc) threads = strtoul(argv[++i], 0, 10);
         else if (a == "--tile" && i + 1 < argc) tile = strtoul(argv[++i], 0, 10);
         else if (a == "--aa" && i + 1 < argc) aa = strtoul(argv[++i], 0, 10);
+        else if (a == "--random") random = true;
         else if (a == "--raygraph" && i + 1 < argc) raygraph = argv[++i];
         else if (a == "--then-camera" && i + 1 < argc) then_camera = argv[++i];
         else if (a == "--png" && i + 1 < argc) png = argv[++i];
@@ -200,6 +203,8 @@ int mode_render(int argc, char **argv)
     ctx.params.threads = threads;
     ctx.params.tile_size = tile;
     ctx.params.aa = aa;
+    ctx.params.sample_distribution = random ? xtcore::antialiasing::SAMPLE_DISTRIBUTION_RANDOM
+                                            : xtcore::antialiasing::SAMPLE_DISTRIBUTION_GRID;
     ctx.init();   // segments the frame into tiles (context.cc)
 
     xtcore::render::IIntegrator *ig = 0;

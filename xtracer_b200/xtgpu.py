@@ -88,11 +88,22 @@ class Hit(C.Structure):
 HIT_DTYPE = np.dtype([("t", np.float32), ("prim", np.uint32), ("u", np.float32), ("v", np.float32)])
 
 
+# sample distributions (aa.h:14-18)
+SAMPLES_GRID, SAMPLES_RANDOM = 0, 1
+
+
+def sample_positions(aa: int, distribution: int = SAMPLES_GRID) -> int:
+    """Positions per pixel: aa^2 on the grid (aa.cc:7-32), aa jittered ones
+    (aa.cc:34-48); level 0 renders as level 1."""
+    L = max(int(aa), 1)
+    return L if distribution == SAMPLES_RANDOM else L * L
+
+
 class RenderParams(C.Structure):
     _fields_ = [("integrator", C.c_int32), ("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32),
                 ("rdepth", C.c_int32), ("ao_max_distance", C.c_float), ("seed", C.c_uint64),
                 ("node_format", C.c_int32), ("x0", C.c_int32), ("y0", C.c_int32), ("x1", C.c_int32),
-                ("y1", C.c_int32), ("aa", C.c_int32)]
+                ("y1", C.c_int32), ("aa", C.c_int32), ("sample_distribution", C.c_int32)]
 
 
 class ServiceOpts(C.Structure):
@@ -132,7 +143,7 @@ def set_tuning(**kw) -> None:
 class JobDesc(C.Structure):
     _fields_ = [("scene", C.c_int32), ("integrator", C.c_int32), ("width", C.c_int32), ("height", C.c_int32),
                 ("spp", C.c_int32), ("rdepth", C.c_int32), ("ao_max_distance", C.c_float), ("seed", C.c_uint64),
-                ("aa", C.c_int32)]
+                ("aa", C.c_int32), ("sample_distribution", C.c_int32)]
 
 
 class JobStatus(C.Structure):
@@ -383,10 +394,10 @@ class Scene:
 
     def render(self, integrator: int, width: int, height: int, spp: int = 1, rdepth: int = 4,
                ao_max_distance: float = 100.0, seed: int = 1, node_format: int = NODES_FP32, rect=None,
-               aa: int = 1):
+               aa: int = 1, distribution: int = SAMPLES_GRID):
         x0, y0, x1, y1 = rect if rect is not None else (0, 0, 0, 0)
         p = RenderParams(integrator, width, height, spp, rdepth, ao_max_distance, seed, node_format, x0, y0, x1, y1,
-                         aa)
+                         aa, distribution)
         rw, rh = (x1 - x0, y1 - y0) if rect is not None else (width, height)
         out = np.zeros((rh, rw, 4), np.float32)
         rays = C.c_uint64()
@@ -394,14 +405,14 @@ class Scene:
         return out, int(rays.value)
 
     def render_raygraph(self, width: int, height: int, spp: int = 1, aa: int = 1, node_format: int = NODES_FP32,
-                        rect=None, tile_size: int = 32):
+                        rect=None, tile_size: int = 32, distribution: int = SAMPLES_GRID):
         """The depth integrator with its raygraph: (frame, records) where the
         records (n, 10: origin, hit point, RGBA after the sample) are listed in
         XTracer's raygraph order (tiles, then columns, then samples)."""
         x0, y0, x1, y1 = rect if rect is not None else (0, 0, 0, 0)
-        p = RenderParams(DEPTH, width, height, spp, 1, 100.0, 1, node_format, x0, y0, x1, y1, aa)
+        p = RenderParams(DEPTH, width, height, spp, 1, 100.0, 1, node_format, x0, y0, x1, y1, aa, distribution)
         rw, rh = (x1 - x0, y1 - y0) if rect is not None else (width, height)
-        S = max(aa, 1) ** 2 * spp
+        S = sample_positions(aa, distribution) * spp
         out = np.zeros((rh, rw, 4), np.float32)
         rec = np.zeros((rh * rw * S, 10), np.float32)
         rays = C.c_uint64()
@@ -434,14 +445,13 @@ def save_raygraph_ply(path: str, records) -> None:
 
 
 class Params:
-    """params_t (context.h:18-34) for the GPU integrators (grid sample
-    distribution)."""
+    """params_t (context.h:18-34) for the GPU integrators."""
 
     def __init__(self, width=500, height=500, samples=1, rdepth=100, seed=1, node_format=NODES_FP32,
-                 ao_max_distance=100.0, aa=1):
+                 ao_max_distance=100.0, aa=1, sample_distribution=SAMPLES_GRID):
         self.width, self.height, self.samples, self.rdepth = width, height, samples, rdepth
         self.seed, self.node_format, self.ao_max_distance = seed, node_format, ao_max_distance
-        self.aa = aa
+        self.aa, self.sample_distribution = aa, sample_distribution
 
 
 class Context:
@@ -468,7 +478,8 @@ class _Integrator:
             return None
         p = self.ctx.params
         img, self.rays = self.ctx.scene.render(self.kind, p.width, p.height, p.samples, p.rdepth,
-                                               p.ao_max_distance, p.seed, p.node_format, aa=p.aa)
+                                               p.ao_max_distance, p.seed, p.node_format, aa=p.aa,
+                                               distribution=p.sample_distribution)
         return img
 
 
