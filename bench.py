@@ -120,6 +120,7 @@ def measured_peaks():
 
 # ---------------------------------------------------------------------------
 SERVED_FORMAT = 2   # xtgpu.NODES_W8: 8-wide BVH, 8-bit quantised child bounds
+WAVES_IN_FLIGHT = 3   # served form: waves on streams of their own, each filling the earlier ones' tails
 # DRAM bytes (read + write) per ray of the served extend kernel, from one ncu
 # capture of k_extend_pool<W8> on 1,048,576 hairball2m first-bounce rays
 # (profiles/k_extend_pool_w8_hairball2m_bounce_ncu.md); the roofline's
@@ -288,7 +289,7 @@ def main():
     budget = 48 << 30
 
     served = Service(gscenes, node_format=SERVED_FORMAT, use_graphs=True, merge_jobs=True, memory_budget=budget,
-                     waves_in_flight=2, stream=stream)
+                     waves_in_flight=WAVES_IN_FLIGHT, stream=stream)
     # warm-up steps (untimed): graphs captured, allocator pools primed
     for w in range(args.warmup):
         run_slice(served, slices[w % nslices])
@@ -347,7 +348,7 @@ def main():
 
     # end to end: same steps, every frame copied to host memory by the service
     e2e_svc = Service(gscenes, node_format=SERVED_FORMAT, use_graphs=True, merge_jobs=True, memory_budget=budget,
-                      host_results=True, waves_in_flight=2, stream=stream)
+                      host_results=True, waves_in_flight=WAVES_IN_FLIGHT, stream=stream)
     # the same untimed warm-up steps as the served arm (graphs, device and
     # pinned host pools)
     for w in range(args.warmup):
@@ -405,7 +406,7 @@ def main():
         other = {}
         for fname, f in (("fp32", xtgpu.NODES_FP32), ("q8", xtgpu.NODES_Q8)):
             fsvc = Service(gscenes, node_format=f, use_graphs=True, merge_jobs=True,
-                           memory_budget=budget, waves_in_flight=2, stream=stream)
+                           memory_budget=budget, waves_in_flight=WAVES_IN_FLIGHT, stream=stream)
             run_slice(fsvc, slices[0])
             torch.cuda.synchronize()
             f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -453,7 +454,7 @@ def main():
                                 (sum(s.device_bytes() for s in gscenes) / 1e6),
                        "wave_paths": 1 << 22, "node_format": "w8 (8-wide, 8-bit quantised) for bounce rays; camera rays as tuned "
                                       "per scene (primary_node_format: 0 = binary FP32, -1 = w8)",
-                       "cuda_graphs": True, "waves_in_flight": 2,
+                       "cuda_graphs": True, "waves_in_flight": WAVES_IN_FLIGHT,
                        "autotuned": tunes},
             "p50_ms": 1000 * pct(lat_all, 50), "p99_ms": 1000 * pct(lat_all, 99),
             "latency_open_loop": latency, "plain": plain,

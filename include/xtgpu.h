@@ -320,10 +320,12 @@ typedef struct {
     int32_t count_visits;          /* 1 = count BVH nodes visited / primitives tested */
     int32_t policy;                /* wave planning: 0 = fewest remaining paths first,
                                       1 = equal share per running job */
-    int32_t waves_in_flight;       /* 1 = one wave at a time; 2 (or 0) = the next wave is
-                                      launched on a second stream while the previous one
-                                      drains, so its kernels fill the previous tail */
+    int32_t waves_in_flight;       /* 1 = one wave at a time; 2 (or 0) up to
+                                      XTGPU_MAX_WAVES_IN_FLIGHT = the next waves are launched
+                                      on streams of their own while the earlier ones drain,
+                                      so their kernels fill the earlier waves' tails */
 } xtgpu_service_opts;
+#define XTGPU_MAX_WAVES_IN_FLIGHT 4
 
 typedef struct {
     int32_t scene;                 /* id from xtgpu_service_add_scene */

@@ -59,6 +59,9 @@ def test_invalid_arguments_are_rejected_without_device_work():
     assert L.xtgpu_service_create(None, None, C.byref(out)) == 1
     o = xtgpu.ServiceOpts(1 << 20, 0, 0, 0, 1, 1, 0, 0, 0, 0)   # max_jobs 0
     assert L.xtgpu_service_create(C.byref(o), None, C.byref(out)) == 1
+    for wif in (-1, 5):   # waves in flight outside 0..XTGPU_MAX_WAVES_IN_FLIGHT
+        o = xtgpu.ServiceOpts(1 << 20, 8, 0, 0, 1, 1, 0, 0, 0, 0, wif)
+        assert L.xtgpu_service_create(C.byref(o), None, C.byref(out)) == 1
     assert L.xtgpu_scene_destroy(None) == 0
 
 

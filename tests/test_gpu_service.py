@@ -43,7 +43,8 @@ def test_job_alone_equals_job_in_mix(resident, fmt):
         alone.append(img)
     # small waves split every job over many waves; with two in flight their
     # accumulates overlap other waves' kernels and must still fold in order
-    for wave, graphs, inflight in ((1 << 22, True, 2), (777, True, 2), (777, True, 1), (5000, False, 2)):
+    for wave, graphs, inflight in ((1 << 22, True, 2), (777, True, 2), (777, True, 1), (5000, False, 2),
+                                   (777, True, 3), (901, True, 4)):
         svc = Service(resident, node_format=fmt, wave_paths=wave, use_graphs=graphs, merge_jobs=True,
                       memory_budget=1 << 30, waves_in_flight=inflight)
         ids = [svc.submit(s, integ, w, h, spp, d, md, seed) for (s, integ, w, h, spp, d, md, seed) in JOBS]
@@ -88,7 +89,7 @@ def test_memory_budget_limits_concurrency(resident):
     svc.close()
 
 
-@pytest.mark.parametrize("inflight", [1, 2])
+@pytest.mark.parametrize("inflight", [1, 2, 4])
 def test_host_results_match(resident, inflight):
     """host_results: frames copied to pinned host memory asynchronously (device
     frames freed behind the copies) equal the frames of a plain render; the

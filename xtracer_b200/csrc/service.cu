@@ -67,7 +67,7 @@ struct xtgpu_service {
     cudaStream_t s = nullptr;  // admission, frees, results
     bool own_stream = false;   // created here: the legacy default stream cannot be captured
     int nslots = 2;
-    xtg::WaveSlot slot[2];
+    xtg::WaveSlot slot[XTGPU_MAX_WAVES_IN_FLIGHT];
     cudaEvent_t admitted = nullptr;   // frames of admitted jobs allocated and zeroed
     std::vector<xtgpu_scene *> scenes;
     std::vector<xtg::DevScene> dev;
@@ -328,7 +328,8 @@ extern "C" {
 xtgpu_status xtgpu_service_create(const xtgpu_service_opts *opts, void *stream, xtgpu_service **out)
 {
     if (!opts || !out || opts->max_jobs <= 0 || opts->max_jobs > 1024 || opts->wave_paths < 0 ||
-        !format_valid(opts->node_format)) {
+        !format_valid(opts->node_format) || opts->waves_in_flight < 0 ||
+        opts->waves_in_flight > XTGPU_MAX_WAVES_IN_FLIGHT) {
         set_error("xtgpu_service_create: bad options");
         return XTGPU_ERR_INVALID;
     }
@@ -346,7 +347,7 @@ xtgpu_status xtgpu_service_create(const xtgpu_service_opts *opts, void *stream, 
     xtgpu_service *v = new xtgpu_service();
     v->o = *opts;
     v->s = (cudaStream_t)stream;
-    v->nslots = opts->waves_in_flight == 1 ? 1 : 2;
+    v->nslots = opts->waves_in_flight > 0 ? opts->waves_in_flight : 2;
     int64_t cap = opts->wave_paths > 0 ? opts->wave_paths : (1ll << 22);
     auto fail = [&](xtgpu_status st) {
         destroy_service(v);
