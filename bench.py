@@ -380,7 +380,17 @@ def main():
         p1.record()
         torch.cuda.synchronize()
         ps = p0.elapsed_time(p1) / 1000.0
+        # equal RMSE (untimed): frames of the step's first jobs from the plain
+        # path and from the served form; every node format and kernel returns
+        # the same hits, so the frames are equal bit for bit
+        check_jobs = timed[0][:16]
+        pf, sf = [], []
+        run_slice(psvc, check_jobs, record=pf)
         psvc.close()
+        run_slice(served, check_jobs, record=sf)
+        diff = max(float(np.nanmax(np.abs(a - b))) if a.size else 0.0 for a, b in zip(pf, sf))
+        same = all(np.array_equal(a, b, equal_nan=True) for a, b in zip(pf, sf))
+        del pf, sf
         # the served path on exactly that step, for a like-for-like ratio
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s0.record()
@@ -421,7 +431,9 @@ def main():
                  "served_same_step_mrays": sr / ss / 1e6, "speedup": (sr / ss) / (pr / ps),
                  "served_w8_only_same_step_mrays": w8_only,
                  "served_fp32_same_step_mrays": other["fp32"], "served_q8_same_step_mrays": other["q8"],
-                 "form": "one job per launch, FP32 BVH, no CUDA graphs"}
+                 "form": "one job per launch, FP32 BVH, no CUDA graphs",
+                 "equal_rmse": {"jobs": len(check_jobs), "frames_bit_identical": bool(same),
+                                "max_abs_diff": diff}}
 
     # open-loop latency: Poisson arrivals at 1.5x the plain path's job rate
     latency = None
