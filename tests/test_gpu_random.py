@@ -198,6 +198,9 @@ def test_bad_distributions_and_levels_are_refused():
     assert rays == 4 * 4
     with pytest.raises(xtgpu.XtgpuError):
         sc.render(xtgpu.STENCIL, 4, 4, spp=1 << 24, aa=256, distribution=RANDOM)     # 2^32 samples per pixel
+    for aa, dist in ((17, xtgpu.SAMPLES_GRID), (257, RANDOM), (1, 2)):   # refused before any buffer is sized
+        with pytest.raises(xtgpu.XtgpuError):
+            sc.render_raygraph(8, 8, spp=1, aa=aa, distribution=dist)
     svc = Service([sc], wave_paths=1 << 16)
     with pytest.raises(xtgpu.XtgpuError):
         svc.submit(0, xtgpu.STENCIL, 8, 8, 1, aa=2, distribution=3)

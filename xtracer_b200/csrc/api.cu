@@ -792,8 +792,7 @@ xtgpu_status xtgpu_render_raygraph_host(xtgpu_scene *sc, const xtgpu_render_para
     }
     const int64_t w = (p->x1 == 0 && p->y1 == 0) ? p->width : p->x1 - p->x0;
     const int64_t h = (p->x1 == 0 && p->y1 == 0) ? p->height : p->y1 - p->y0;
-    if (w <= 0 || h <= 0 || p->spp <= 0 || p->aa < 0 || p->aa > MAX_AA * MAX_AA ||
-        (p->sample_distribution != XTGPU_SAMPLES_GRID && p->sample_distribution != XTGPU_SAMPLES_RANDOM)) {
+    if (w <= 0 || h <= 0 || !view_valid(sc->dev.cam, p->width, p->height, p->aa, p->sample_distribution, p->spp)) {
         set_error("xtgpu_render_raygraph_host: bad rectangle or samples");
         return XTGPU_ERR_INVALID;
     }
