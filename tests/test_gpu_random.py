@@ -75,6 +75,31 @@ def test_random_same_stream_as_oracle(aa, fmt):
     sc.close()
 
 
+@pytest.mark.parametrize("cam, w, h", [
+    (scenes.Camera((0.5, 2.0, 0.25), type=scenes.CAM_ERP, orientation=(0.25, -0.5, 0.125)), 64, 32),
+    (scenes.Camera((0.5, 2.0, 0.25), type=scenes.CAM_ODS, orientation=(0.0, 0.75, 0.0), ipd=0.125), 48, 48),
+    (scenes.Camera((0.5, 2.0, 0.25), type=scenes.CAM_CUBEMAP), 16, 96)], ids=["erp", "ods", "cubemap"])
+def test_random_through_every_camera_same_stream_as_oracle(cam, w, h):
+    """The jittered positions feed the equirectangular, omni-directional stereo
+    and cubemap cameras as they feed the pinhole one: stencil equal to the
+    oracle's, depth within 1e-5 relative in the hit distance (|d depth| <=
+    1e-5 |depth| max(1, |depth|), depth being 1/log t)."""
+    spec = scenes.spheres_scene(64, seed=1, name="rnd_cam", camera=cam)
+    sc = xtgpu.Scene(spec)
+    for code in (xtgpu.STENCIL, xtgpu.DEPTH):
+        img, rays = sc.render(code, w, h, spp=2, seed=23, aa=3, distribution=RANDOM)
+        o, orays = _oracle_full(spec, code, w, h, 2, 23, 3)
+        assert rays == orays == w * h * 6
+        got = img.reshape(-1, 4)
+        if code == xtgpu.STENCIL:
+            assert (got == o).all(axis=1).mean() >= 0.998, (got != o).any(axis=1).sum()
+        else:
+            D = np.abs(o[:, 0].astype(np.float64))
+            rel = np.abs(got[:, 0] - o[:, 0]) / np.maximum(D, 1e-6)
+            assert np.mean(rel <= 1e-5 * np.maximum(1.0, D)) >= 0.99, np.sort(rel)[-5:]
+    sc.close()
+
+
 def test_random_with_lens_and_ao_same_stream_as_oracle():
     """The jitter comes from a stream of its own, so the thin-lens draws and
     AO's hemisphere draws keep their places on the sample's stream."""
