@@ -123,7 +123,7 @@ SERVED_FORMAT = 2   # xtgpu.NODES_W8: 8-wide BVH, 8-bit quantised child bounds
 WAVES_IN_FLIGHT = 3   # served form: waves on streams of their own, each filling the earlier ones' tails
 # DRAM bytes (read + write) per ray of the served extend kernel, from one ncu
 # capture of k_extend_pool<W8> on 1,048,576 hairball2m first-bounce rays
-# (profiles/k_extend_pool_w8_hairball2m_bounce_ncu.md); the roofline's
+# (python -m xtracer_b200.profile_extend --scene hairball2m); the roofline's
 # traffic is this figure times the rays of an average launch.
 NCU_TRAFFIC_BYTES_PER_RAY = 104.0
 

@@ -3,8 +3,9 @@
  * XTracer (4rknova/xtracer).
  *
  * XTracer's C++ host (the .scn loader, Scene, IIntegrator, tiles, image output)
- * stays as it is.  A GPU integrator flattens the loaded
- * Scene into an xtgpu_scene_desc and calls the entry points below.  Plain
+ * stays as it is.  A GPU integrator (an IIntegrator subclass built into
+ * XTracer's tree) flattens the loaded Scene into an xtgpu_scene_desc and calls
+ * the entry points below.  Plain
  * pointers and sizes only; every call returns an xtgpu_status and never throws;
  * xtgpu_last_error() gives the text of the last failure on the calling thread.
  *
@@ -278,7 +279,9 @@ XTGPU_API xtgpu_status xtgpu_write_raygraph_ply(const char *path, int64_t n_path
  * XTGPU_NOALLOC_MAX_PATHS paths (rectangle pixels x positions x spp) and larger requests
  * return XTGPU_ERR_LIMIT.  Calls that overlap on the GPU race on the shared
  * array.  The first call on a device looks up the array's address; make it
- * before any stream capture.  Output: rgba_dev as in xtgpu_render. */
+ * before any stream capture.  Every call copies its job from host memory and
+ * waits for `stream` before it returns; a stream that is capturing is refused
+ * (XTGPU_ERR_STATE).  Output: rgba_dev as in xtgpu_render. */
 #define XTGPU_NOALLOC_MAX_PATHS 65536
 XTGPU_API xtgpu_status xtgpu_render_tile_noalloc(xtgpu_scene *scene, const xtgpu_render_params *params,
                                                  float *rgba_dev, uint64_t *rays_traced, void *stream);
@@ -303,7 +306,16 @@ XTGPU_API xtgpu_status xtgpu_save_png_host(const char *path, int32_t width, int3
  * accumulation buffers fit the memory budget and a job slot is free; the rays of
  * all admitted jobs are merged into shared wavefront launches (camera, extend,
  * shade, accumulate) replayed as CUDA graphs.  Results depend only on the job
- * (seed, pixel, sample), never on what else is in flight.                   */
+ * (seed, pixel, sample), never on what else is in flight.  No counterpart in
+ * the reference, whose IIntegrator::render (integrator.cc:29-53) renders one
+ * frame per blocking call.
+ *
+ * Threads: one thread at a time runs xtgpu_service_run.  While it runs, any
+ * other thread may call xtgpu_service_submit, _poll, _result, _result_host,
+ * _release, _open and _get_stats; a job submitted then is admitted as slots
+ * and memory free up and joins the next wave launched.  One job's result and
+ * release come from one thread.  xtgpu_service_add_scene, _update_scene,
+ * _reset_stats and _destroy must not overlap a run.                         */
 typedef struct xtgpu_service xtgpu_service;
 
 typedef struct {
@@ -348,14 +360,24 @@ typedef struct {
 XTGPU_API xtgpu_status xtgpu_service_create(const xtgpu_service_opts *opts, void *stream, xtgpu_service **out);
 XTGPU_API xtgpu_status xtgpu_service_add_scene(xtgpu_service *svc, xtgpu_scene *scene, int32_t *scene_id);
 /* Refreshes the service's copy of a resident scene's tables after
- * xtgpu_scene_update (waits for the waves in flight). */
+ * xtgpu_scene_update, and after a BVH rebuild of the scene (xtgpu_bvh_build,
+ * xtgpu_autotune or a tuning change that rebuilds): the service's waves read
+ * node and leaf buffers through that copy, and its captured graphs that hold
+ * the old buffers are dropped.  Waits for the waves in flight. */
 XTGPU_API xtgpu_status xtgpu_service_update_scene(xtgpu_service *service, int32_t scene);
 /* Queues a job; submit_s is the arrival time on the service clock (seconds
  * since xtgpu_service_create), or a negative value for "now". */
 XTGPU_API xtgpu_status xtgpu_service_submit(xtgpu_service *svc, const xtgpu_job_desc *job, double submit_s, int64_t *job_id);
 /* Runs admission + waves until every queued job whose arrival time has passed
- * is done, or max_seconds of service clock elapsed (0 = no limit). */
+ * is done, or max_seconds of service clock elapsed (0 = no limit).  While the
+ * service is open (xtgpu_service_open), running out of work does not end the
+ * run: it waits for submissions until the service is closed. */
 XTGPU_API xtgpu_status xtgpu_service_run(xtgpu_service *svc, double max_seconds);
+/* Opens (1) or closes (0) the service to live submissions: while open, a
+ * running xtgpu_service_run waits for new jobs when it has none; once closed
+ * it returns after the jobs already submitted are done.  Callable from any
+ * thread. */
+XTGPU_API xtgpu_status xtgpu_service_open(xtgpu_service *svc, int32_t open);
 XTGPU_API xtgpu_status xtgpu_service_poll(xtgpu_service *svc, int64_t job_id, xtgpu_job_status *status);
 /* Copies a finished job's RGBA frame (width*height*4 floats) to host memory. */
 XTGPU_API xtgpu_status xtgpu_service_result(xtgpu_service *svc, int64_t job_id, float *rgba_host);

@@ -5,12 +5,14 @@
 # fixtures, pinning of the C restatement) and the timed CPU baseline.  It never
 # feeds the GPU product path.
 #
-#   make -f oracle/ref.mk REF=/root/reference -j8
+#   make -f oracle/ref.mk REF=<XTracer source tree> -j8
 #
 # Flags: -O2 -fopenmp.  The reference's own CMake "Release" flags are -O0
 # (CMakeLists.txt:157); -O2 is used so the CPU baseline is not handicapped.
 
-REF      ?= /root/reference
+ifndef REF
+$(error REF must name the XTracer source tree: make -f oracle/ref.mk REF=<dir>)
+endif
 HERE     := $(dir $(lastword $(MAKEFILE_LIST)))
 OUT      := $(HERE)_ref
 OBJDIR   := $(OUT)/obj

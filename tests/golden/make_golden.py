@@ -36,7 +36,12 @@ these fixtures are what pins the oracle restatement (oracle/xtoracle.c):
               depth-4 pathtracer at four seeds (`--mtl`);
 * render_random.npz  stencil and depth frames with the random sample
               distribution (aa.cc:34-48) at four seeds, one reproducible set of
-              rand() jitter offsets each (`--random`).
+              rand() jitter offsets each (`--random`);
+* render_phong.npz  depth-4 pathtracer frames of Phong and Blinn-Phong
+              spheres and plane (reflectance 0.5 and 1, exponents 8 and 256)
+              at four seeds, and known answers of sample::lobe where its frame
+              is the identity (direction along the normal) or its result
+              underflows (`--phong`).
 
 Run here (needs the reference sources and oracle/_ref/xtref):
     make -f oracle/ref.mk REF=<xtracer source tree> -j8
@@ -463,6 +468,67 @@ def make_random(work):
     print("render_random.npz", sorted(rend))
 
 
+def phong_case():
+    """(scene, width, height, spp, depth, seeds) of the Phong fixture; odd
+    width and height put the centre pixel's ray on the camera axis."""
+    return scenes.phong_scene(), 65, 49, 16, 4, (51, 52, 53, 54)
+
+
+def lobe_edge_cases(rng):
+    """(seed, normal, direction, exponent) rows for sample::lobe at the edges
+    of sample.inl:61-90: the direction equal to the normal (identity frame),
+    1 - d.n just below and just above 1e-8, and exponents up to 2000, where
+    pow(vdotr, e) underflows."""
+    rows = []
+    seeds = np.arange(1, 65, dtype=np.int64) * 104729
+    for i, sd in enumerate(seeds):
+        n = _unit(rng, 1)[0]
+        if i % 8 == 0:
+            n = np.array([0.0, 0.0, -1.0])
+        e = [8.0, 64.0, 256.0, 2000.0][i % 4]
+        kind = (i // 4) % 4
+        if kind == 0:
+            d = n.copy()
+        else:
+            # rotate n by an angle whose 1 - cos is 5e-9, 2e-8 or 1e-3
+            ang = {1: np.arccos(1 - 5e-9), 2: np.arccos(1 - 2e-8), 3: np.arccos(1 - 1e-3)}[kind]
+            a = np.cross(n, _unit(rng, 1)[0])
+            a /= np.linalg.norm(a)
+            d = n * np.cos(ang) + np.cross(a, n) * np.sin(ang)
+        rows.append((int(sd), n, d, e))
+    return rows
+
+
+def make_phong(work):
+    """Depth-4 pathtracer frames of the Phong scene at four seeds, and
+    sample::lobe known answers at its edges with the rand() values each call
+    consumed."""
+    spec, w, h, spp, depth, seeds = phong_case()
+    scn = spec.write_scn(work)
+    rend = {}
+    imgs, rays = [], []
+    for seed in seeds:
+        xy, rgba, st = po.ref_render(scn, "pathtracer", w, h, spp=spp, rdepth=depth, threads=1, seed=seed,
+                                     workdir=work)
+        imgs.append(rgba)
+        rays.append(st["rays"])
+    rend["pt_xy"], rend["pt_rgba"], rend["pt_rays"] = xy, np.stack(imgs), np.array(rays, np.int64)
+    rows = lobe_edge_cases(np.random.default_rng(20261206))
+    res = po.ref_kat(["rand %d 8" % r[0] for r in rows])
+    rend["lobe_rand"] = np.array([[int(t) for t in r[1:9]] for r in res], np.int64)
+    rend["rand_max"] = np.int64(int(res[0][9]))
+    res = po.ref_kat(["lobe %d %s %s %s %s %s %s %s" % ((r[0],) + tuple(H(float(x)) for x in r[1]) +
+                                                        tuple(H(float(x)) for x in r[2]) + (H(r[3]),))
+                      for r in rows])
+    rend["lobe_n"] = np.array([r[1] for r in rows])
+    rend["lobe_d"] = np.array([r[2] for r in rows])
+    rend["lobe_e"] = np.array([r[3] for r in rows])
+    rend["lobe_out"] = np.array([[float.fromhex(t) for t in r[1:]] for r in res])
+    np.savez_compressed(os.path.join(HERE, "render_phong.npz"), width=w, height=h, spp=spp, depth=depth,
+                        seeds=np.array(seeds), **rend)
+    print("render_phong.npz", sorted(rend))
+
+
 def texture_frame_size():
     return 64, 48
 
@@ -491,6 +557,9 @@ def main():
         return
     if "--raygraph" in sys.argv:
         make_raygraph(tempfile.mkdtemp(prefix="xtgold"))
+        return
+    if "--phong" in sys.argv:
+        make_phong(tempfile.mkdtemp(prefix="xtgold"))
         return
     if "--random" in sys.argv:
         make_random(tempfile.mkdtemp(prefix="xtgold"))

@@ -138,3 +138,59 @@ def random_distribution_agreement(R, O, channel, aa=None):
         pr, po_ = ((r > 0) & (r < 1)).mean(), ((o > 0) & (o < 1)).mean()
         p = 0.5 * (pr + po_)
         assert abs(pr - po_) <= 4.5 * np.sqrt(p * (1 - p) * 2.0 / r.size) + 1e-9, (pr, po_)
+
+
+def rmse(a, b):
+    """Per-pixel RMSE over the colour channels of two (npix, 4) frames."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.sqrt(np.mean((a[:, :3] - b[:, :3]) ** 2)))
+
+
+def converged_rmse_bar(frames, truth, ref_rmse, label="", tol=1.05):
+    """The stochastic bar as the hot-path contract words it: per-pixel RMSE
+    against a 4096-spp render must sit within the sampling noise of the
+    reference CPU renderer at equal spp.
+
+    frames: (k >= 2, npix, 4) frames under test at that spp (different seeds);
+    truth: (npix, 4) the converged render; ref_rmse: the reference's own RMSE
+    against the same truth, one per reference seed.  Asserts
+    * the mean RMSE of the frames <= tol x the largest reference RMSE (the
+      reference's RMSE varies by 2-3 % between seeds at these sizes);
+    * per channel, the frames' mean minus the truth's mean within 4.5 standard
+      errors (from the per-pixel variance between the frames).
+    Prints and returns (mean RMSE, reference RMSEs)."""
+    F = np.asarray(frames, np.float64)
+    T = np.asarray(truth, np.float64)
+    k, npix = F.shape[0], F.shape[1]
+    assert k >= 2
+    got = [rmse(F[i], T) for i in range(k)]
+    ref = [float(x) for x in np.asarray(ref_rmse).ravel()]
+    print("[%s] RMSE vs 4096-spp: frames %s, reference %s, ratio %.3f (bar %.2f x max)" %
+          (label, np.round(got, 5), np.round(ref, 5), np.mean(got) / max(ref), tol))
+    assert np.mean(got) <= tol * max(ref), (got, ref)
+    for ch in range(3):
+        se = np.sqrt(F[:, :, ch].var(0, ddof=1).mean() / npix / k)
+        bias = F[:, :, ch].mean() - T[:, ch].mean()
+        assert abs(bias) <= 4.5 * se + 1e-6, (label, ch, bias, se)
+    return float(np.mean(got)), ref
+
+
+def same_stream_bar(gpu, oracle, oracle_other, label="", frac=0.25):
+    """GPU (FP32) and oracle (FP64) frames drawn from the same random stream
+    differ only where rounding sends a path another way: an edge or grazing
+    hit, a tie between primitives, a secondary ray's origin offset.  Bar: the
+    RMSE between them is at most `frac` of one frame's sampling noise at that
+    spp, measured as the RMSE between the oracle's frames at two seeds over
+    sqrt(2); the divergence then adds at most frac^2 to the frame's variance.
+    Prints the ratio and the share of pixels equal within 1e-3."""
+    g = np.asarray(gpu, np.float64).reshape(-1, 4)
+    o = np.asarray(oracle, np.float64).reshape(-1, 4)
+    o2 = np.asarray(oracle_other, np.float64).reshape(-1, 4)
+    noise = rmse(o, o2) / np.sqrt(2.0)
+    div = rmse(g, o)
+    same = float(np.mean(np.abs(g[:, :3] - o[:, :3]).max(axis=1) < 1e-3))
+    print("[%s] same stream: RMSE(gpu, oracle) %.3g = %.3f of the noise %.3g (bar %.2f); %.4f of pixels within 1e-3"
+          % (label, div, div / max(noise, 1e-30), noise, frac, same))
+    assert div <= frac * noise, (label, div, noise)
+    return div / max(noise, 1e-30), same

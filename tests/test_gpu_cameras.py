@@ -17,6 +17,7 @@ import numpy as np
 import pytest
 
 from oracle import pyoracle as po
+from tests import parity
 from xtracer_b200 import scenes, xtgpu
 from xtracer_b200.service import Service
 
@@ -100,6 +101,7 @@ def test_depth_of_field_same_stream_as_oracle():
     assert rays == orays == w * h * 16
     got = img.reshape(-1, 4)
     rel = np.abs(got[:, 0] - o[:, 0]) / np.maximum(np.abs(o[:, 0]), 1e-6)
+    print("[dof depth] %.4f of pixels within 1e-5 of the oracle (16 rays each)" % np.mean(rel <= 1e-5))
     assert np.mean(rel <= 1e-5) >= 0.99, np.sort(rel)[-5:]
 
 
@@ -111,34 +113,29 @@ def test_ao_after_lens_draws_same_stream_as_oracle():
     img, rays = sc.render(xtgpu.AO, w, h, spp=8, seed=43, ao_max_distance=0.5)
     sc.close()
     o, orays = _oracle_full(spec, po.AO, w, h, 8, 43, md=0.5)
-    d = np.abs(img.reshape(-1, 4)[:, :3] - o[:, :3]).max(axis=1)
-    assert np.mean(d < 1e-3) >= 0.97, np.mean(d < 1e-3)
+    o2, _ = _oracle_full(spec, po.AO, w, h, 8, 44, md=0.5)
+    parity.same_stream_bar(img, o, o2, "dof ao")
     assert abs(rays - orays) <= 0.01 * orays
 
 
-def _rmse(a, b):
-    return float(np.sqrt(np.mean((a[:, :3] - b[:, :3]) ** 2)))
-
-
 def test_depth_of_field_within_reference_noise():
-    """The reference draws its lens offsets from the C library's rand(); four
-    reference renders (seeds 31-34) give its noise, and the GPU's frame from
-    its own stream must sit within it."""
+    """The reference draws its lens offsets from the C library's rand(); its
+    depth frames at four seeds (31-34) give its noise at 16 spp.  The GPU's
+    frames, from their own stream, have per-pixel RMSE against the 4096-spp
+    render within that noise."""
     g = np.load(os.path.join(GOLD, "render_cameras.npz"))
+    t = np.load(os.path.join(GOLD, "truth.npz"))
+    xy, truth = t["dof_depth_xy"], t["dof_depth_rgba"]
+    assert np.array_equal(xy, g["dof_depth_xy"])
     spec = scenes.spheres_scene(64, seed=1, name="cam_dof", camera=DOF)
     sc = xtgpu.Scene(spec)
-    img, _ = sc.render(xtgpu.DEPTH, 48, 48, spp=16, seed=777)
+    frames = []
+    for seed in (777, 778):
+        img, _ = sc.render(xtgpu.DEPTH, 48, 48, spp=16, seed=seed)
+        frames.append(img[xy[:, 1], xy[:, 0]])
     sc.close()
-    xy = g["dof_depth_xy"]
-    O = img[xy[:, 1], xy[:, 0]]
-    R = g["dof_depth_rgba"]
-    n = R.shape[0]
-    ref = np.mean([_rmse(R[i], R[[j for j in range(n) if j != i]].mean(0)) for i in range(n)])
-    got = np.mean([_rmse(O, R[[j for j in range(n) if j != i]].mean(0)) for i in range(n)])
-    assert got <= 1.25 * ref + 1e-6, (got, ref)
-    diff = O[:, 0] - R[:, :, 0].mean(0)
-    se = np.sqrt(R[:, :, 0].var(0, ddof=1).mean() / diff.size * (1 + 1.0 / n))
-    assert abs(diff.mean()) < 4.5 * se + 1e-5, (diff.mean(), se)
+    parity.converged_rmse_bar(np.stack(frames), truth, [parity.rmse(r, truth) for r in g["dof_depth_rgba"]],
+                              "dof depth")
 
 
 def test_aa_jobs_alone_equal_jobs_in_the_mix():

@@ -1,19 +1,24 @@
 """Parity at the full sizes of the benchmark configurations.
 
 * Pathtracer, 64 spheres + plane, 256x256, 16 spp, depth 4: per-pixel RMSE
-  against a converged 4096-spp frame equals the oracle's at equal spp (the
-  oracle restates the reference and is pinned to it by the golden fixtures).
+  against a 4096-spp render made on the CPU by the oracle (truth.npz) within
+  the reference renderer's own RMSE at 16 spp (four reference seeds, rendered
+  by XTracer's code when the fixture was made).
 * Depth + stencil, 999,698-triangle terrain, 1920x1080, 1 spp: primary hits on
-  every 8th pixel in x and y against the FP64 oracle (every disagreement a tie
-  or a grazing hit), depth values within 1e-5, and the Q8 frames equal to the
-  FP32 frames.
-* AO, 2M-triangle hairball, 1024x1024, 64 spp, distance 0.2: against the
-  oracle on the same random stream, per ray (1 spp, every 4th pixel) and per
-  pixel (64 spp, a 32x32 lattice); Q8 frame equal to FP32.
+  every 8th pixel in x and y against the FP64 oracle (>= 99.99 % agreement,
+  every disagreement a tie or a grazing hit), and on every pixel where the
+  primitive agrees the stencil equal and the hit distance within 1e-5
+  relative; the Q8 and W8 frames equal to the FP32 frames.
+* AO, 2M-triangle hairball, 1024x1024, 64 spp, distance 0.2: per-pixel RMSE
+  on a 32x32 lattice against a 4096-spp oracle render within the equal-spp
+  noise, and against the oracle on the same random stream (the divergence
+  below a quarter of the noise); Q8 and W8 frames equal to FP32.
 * Precision scene, 8M triangles, Phong/Blinn-Phong, sphere and mesh lights:
-  primary hits of FP32 and Q8 nodes against the FP64 oracle on every 8th pixel,
-  and the 1920x1080, 256-spp, depth-8 pathtracer frame with Q8 nodes equal to
-  the one with FP32 nodes (hence equal RMSE).
+  primary hits of FP32, Q8 and W8 nodes against the FP64 oracle on every 8th
+  pixel; a 64x64 crop at 16 spp, depth 8, against a 4096-spp oracle render
+  within the equal-spp noise and against the oracle on the same stream; the
+  1920x1080, 256-spp, depth-8 frame with Q8 and W8 nodes equal to the one
+  with FP32 nodes (hence equal RMSE).
 """
 import numpy as np
 import pytest
@@ -58,26 +63,31 @@ def hits_vs_oracle(spec, sc, orc, w, h, px, fmt):
     return n_agree / g_hit.size, float(rel.max()) if rel.size else 0.0
 
 
-def test_config_pathtracer_spheres_rmse_matches_oracle():
+def _truth(name):
+    import os
+    t = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "truth.npz"))
+    return {k[len(name) + 1:]: t[k] for k in t.files if k.startswith(name + "_")}
+
+
+def test_config_pathtracer_spheres_rmse_within_reference_noise():
+    """The north star's bar at config 1's size: RMSE against the 4096-spp
+    render within the reference's own at equal spp."""
     spec = scenes.spheres_scene(64, seed=1)
     w = h = 256
+    T = _truth("config1")
+    xy = T["xy"]
     sc = xtgpu.Scene(spec)
-    ref, _ = sc.render(xtgpu.PATHTRACER, w, h, spp=4096, rdepth=4, seed=1000)
-    gpu, rays = sc.render(xtgpu.PATHTRACER, w, h, spp=16, rdepth=4, seed=1)
+    frames, rays = [], []
+    for seed in (1, 2):
+        img, r = sc.render(xtgpu.PATHTRACER, w, h, spp=16, rdepth=4, seed=seed)
+        frames.append(img[xy[:, 1], xy[:, 0]])
+        rays.append(r)
     sc.close()
-    orc = po.OracleScene(spec, po.XO_ACCEL_BVH)
-    o, orays = orc.render(po.PATHTRACER, w, h, spp=16, rdepth=4, seed=2)
-    R = ref.reshape(-1, 4)[:, :3].astype(np.float64)
-    G = gpu.reshape(-1, 4)[:, :3].astype(np.float64)
-    O = o[:, :3].astype(np.float64)
-    rmse_g = np.sqrt(np.mean((G - R) ** 2))
-    rmse_o = np.sqrt(np.mean((O - R) ** 2))
-    # 65,536 pixels: the RMSE of either estimate is known to well under 1 %
-    assert abs(rmse_g / rmse_o - 1.0) < 0.03, (rmse_g, rmse_o)
-    for ch in range(3):
-        d = G[:, ch] - O[:, ch]
-        assert abs(d.mean()) < 4.5 * d.std() / np.sqrt(d.size) + 1e-6, ch
-    assert abs(rays - orays) < 0.01 * orays
+    parity.converged_rmse_bar(np.stack(frames), T["rgba"], T["ref_rmse"], "config1 pt 256x256 16spp")
+    # the reference's frame means at 16 spp bracket the GPU's within their spread
+    gm = np.mean([f[:, :3].astype(np.float64).mean(0) for f in frames], axis=0)
+    rm = T["ref_mean"]
+    assert np.all(np.abs(gm - rm.mean(0)) <= 5 * rm.std(0, ddof=1) + 1e-4), (gm, rm)
 
 
 def test_config_terrain_1m_depth_stencil_full_hd():
@@ -99,16 +109,26 @@ def test_config_terrain_1m_depth_stencil_full_hd():
         for fmt in (xtgpu.NODES_Q8, xtgpu.NODES_W8):
             same = np.all(frames[xtgpu.NODES_FP32, integ] == frames[fmt, integ], axis=2)
             assert same.mean() >= 0.9999, (integ, fmt, same.mean())
-    # depth values on the lattice against the oracle's depth integrator
+    # stencil and depth on the lattice against the oracle's integrators,
+    # pixel by pixel where the primitive agrees
+    org, dirs = po.camera_rays(spec, w, h, px)
+    r = orc.trace(org, dirs)
+    gtr = sc.intersection(org.astype(np.float32), dirs.astype(np.float32))
+    r_gid = parity.oracle_global_prim(spec, r["obj"], r["prim"])
+    g_gid = np.where(gtr["prim"] != 0xffffffff, gtr["prim"].astype(np.int64), -1)
+    same = g_gid == r_gid
+    print("[terrain1m lattice] primitive agrees on %.6f of %d pixels" % (same.mean(), same.size))
+    assert same.mean() >= 0.9999
     od, _ = orc.render(po.DEPTH, w, h, spp=1, pixels=px)
-    gd = frames[xtgpu.NODES_FP32, xtgpu.DEPTH][px[:, 1], px[:, 0]]
-    both = (od[:, 3] > 0) & (gd[:, 3] > 0)
-    assert np.mean((od[:, 3] > 0) == (gd[:, 3] > 0)) >= 0.9999
-    rel = np.abs(gd[both, 0].astype(np.float64) - od[both, 0]) / np.maximum(np.abs(od[both, 0]), 1e-30)
-    assert np.mean(rel <= 1e-5) >= 0.9999, np.sort(rel)[-5:]
+    gd = frames[xtgpu.NODES_FP32, xtgpu.DEPTH][px[:, 1], px[:, 0]].astype(np.float64)
+    hit = same & (od[:, 0] != 0)
+    assert np.array_equal(gd[same & ~hit], od[same & ~hit])
+    dl = np.abs(1.0 / gd[hit, 0] - 1.0 / od[hit, 0].astype(np.float64))
+    print("[terrain1m depth] max |ln t_gpu - ln t_oracle| %.3g over %d pixels" % (dl.max(), hit.sum()))
+    assert dl.max() <= 1e-5, np.sort(dl)[-5:]
     os_, _ = orc.render(po.STENCIL, w, h, spp=1, pixels=px)
     gs = frames[xtgpu.NODES_FP32, xtgpu.STENCIL][px[:, 1], px[:, 0]]
-    assert np.all(gs == os_, axis=1).mean() >= 0.9999
+    assert np.array_equal(gs[same], os_[same])
     sc.close()
 
 
@@ -121,6 +141,7 @@ def test_config_hairball_2m_ao_same_stream_as_oracle():
     w = h = 1024
     sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8))
     img, rays = sc.render(xtgpu.AO, w, h, spp=64, ao_max_distance=0.2, seed=31)
+    img2, _ = sc.render(xtgpu.AO, w, h, spp=64, ao_max_distance=0.2, seed=35)
     img8, rays8 = sc.render(xtgpu.AO, w, h, spp=64, ao_max_distance=0.2, seed=31, node_format=xtgpu.NODES_Q8)
     imgw, raysw = sc.render(xtgpu.AO, w, h, spp=64, ao_max_distance=0.2, seed=31, node_format=xtgpu.NODES_W8)
     assert np.array_equal(img, imgw) and rays == raysw
@@ -129,18 +150,21 @@ def test_config_hairball_2m_ao_same_stream_as_oracle():
     assert np.all(img == img8, axis=2).mean() >= 0.9999
     assert rays == rays8
     orc = po.OracleScene(spec, po.XO_ACCEL_BVH)
-    # per ray: one AO ray per pixel on a dense lattice
+    # per ray: one AO ray per pixel on a dense lattice, same stream
     px1 = lattice(w, h, 4)
     o1, _ = orc.render(po.AO, w, h, spp=1, ao_max_distance=0.2, seed=31, pixels=px1)
-    d1 = np.abs(one[px1[:, 1], px1[:, 0], 0].astype(np.float64) - o1[:, 0])
-    assert np.mean(d1 > 1e-3) <= 0.01, np.mean(d1 > 1e-3)
-    # per pixel at 64 spp on a 32x32 lattice
-    px = lattice(w, h, 32)
+    o1b, _ = orc.render(po.AO, w, h, spp=1, ao_max_distance=0.2, seed=32, pixels=px1)
+    parity.same_stream_bar(one[px1[:, 1], px1[:, 0]], o1, o1b, "hairball2m ao 1spp")
+    # per pixel at 64 spp on a 32x32 lattice: same stream, and the north
+    # star's bar against the 4096-spp render
+    T = _truth("hairball2m_ao")
+    px = T["xy"]
     o, _ = orc.render(po.AO, w, h, spp=64, ao_max_distance=0.2, seed=31, pixels=px)
-    g = img[px[:, 1], px[:, 0], 0].astype(np.float64)
-    d = np.abs(g - o[:, 0])
-    assert np.mean(d < 1e-3) >= 0.75, np.mean(d < 1e-3)
-    assert abs(g.mean() - float(o[:, 0].mean())) < 1e-3
+    o2, _ = orc.render(po.AO, w, h, spp=64, ao_max_distance=0.2, seed=33, pixels=px)
+    parity.same_stream_bar(img[px[:, 1], px[:, 0]], o, o2, "hairball2m ao 64spp")
+    frames = [img[px[:, 1], px[:, 0]], img2[px[:, 1], px[:, 0]]]
+    noise = T["ref_rmse"] if "ref_rmse" in T else T["oracle_rmse"]
+    parity.converged_rmse_bar(np.stack(frames), T["rgba"], noise, "hairball2m ao 64spp lattice")
 
 
 def test_config_precision_8m_q8_vs_fp32_vs_fp64():
@@ -153,6 +177,19 @@ def test_config_precision_8m_q8_vs_fp32_vs_fp64():
     for fmt in (xtgpu.NODES_FP32, xtgpu.NODES_Q8, xtgpu.NODES_W8):
         agree, rel = hits_vs_oracle(spec, sc, orc, w, h, px, fmt)
         assert agree >= 0.9999 and rel <= 1e-5, (fmt, agree, rel)
+    # a 64x64 crop at 16 spp, depth 8: same stream as the oracle, and RMSE
+    # against the 4096-spp render within the equal-spp noise
+    T = _truth("precision_crop")
+    cx = T["xy"]
+    rect = (int(cx[:, 0].min()), int(cx[:, 1].min()), int(cx[:, 0].max()) + 1, int(cx[:, 1].max()) + 1)
+    crops = []
+    for seed in (51, 52):
+        c, _ = sc.render(xtgpu.PATHTRACER, w, h, spp=16, rdepth=8, seed=seed, rect=rect, node_format=xtgpu.NODES_W8)
+        crops.append(c[cx[:, 1] - rect[1], cx[:, 0] - rect[0]])
+    o, _ = orc.render(po.PATHTRACER, w, h, spp=16, rdepth=8, seed=51, pixels=cx)
+    o2, _ = orc.render(po.PATHTRACER, w, h, spp=16, rdepth=8, seed=53, pixels=cx)
+    parity.same_stream_bar(crops[0], o, o2, "precision8m crop pt")
+    parity.converged_rmse_bar(np.stack(crops), T["rgba"], T["oracle_rmse"], "precision8m crop 16spp depth 8")
     del orc
     a, ra = sc.render(xtgpu.PATHTRACER, w, h, spp=256, rdepth=8, seed=5, node_format=xtgpu.NODES_FP32)
     b, rb = sc.render(xtgpu.PATHTRACER, w, h, spp=256, rdepth=8, seed=5, node_format=xtgpu.NODES_Q8)

@@ -162,8 +162,10 @@ def test_primary_hits_vs_reference_golden(name, fmt):
     r_gid = np.array([parity.global_prim(spec, o, p) if o >= 0 else -1 for o, p in zip(g["obj"], g["prim"])])
     n_agree, tie, graze, bad = parity.classify(spec, org, dirs, g_hit, g_gid, hits["t"].astype(np.float64),
                                                r_hit, r_gid, g["t"])
+    print("[%s fmt %d] primitive agreement %.6f of %d rays (%d ties, %d grazing)" %
+          (name, fmt, n_agree / g_hit.size, g_hit.size, tie, graze))
     assert not bad, "unexplained disagreements at %s" % bad[:10]
-    assert n_agree >= 0.999 * g_hit.size
+    assert n_agree >= 0.9999 * g_hit.size
     m = (g_hit == 1) & (r_hit == 1) & (g_gid == r_gid)
     rel = np.abs(hits["t"][m].astype(np.float64) - g["t"][m]) / g["t"][m]
     assert rel.max() <= 1e-5, rel.max()
@@ -327,27 +329,48 @@ def test_w8_frames_equal_fp32(integ):
 
 @pytest.mark.parametrize("name", ["spheres64", "terrain20k", "hairball20k"])
 def test_stencil_depth_frames_vs_reference_golden(name):
+    """Stencil and depth frames (2 samples per pixel, each the pixel-centre
+    ray) against the reference's, pixel by pixel: on every pixel whose primary
+    ray hits the same primitive as the reference's (hits_*.npz), the stencil
+    pixel is equal and the depth pixel gives the hit distance within 1e-5
+    relative (depth = 1/ln t, so |1/depth_gpu - 1/depth_ref| = |ln t_gpu -
+    ln t_ref| bounds the relative error of t); the primitive agrees on
+    >= 99.99 % of pixels."""
     spec, w, h = small_scenes()[name]
     g = np.load(os.path.join(GOLD, "render_%s.npz" % name))
+    hits_ref = np.load(os.path.join(GOLD, "hits_%s.npz" % name))
     sc = xtgpu.Scene(spec)
+    # the primitive each pixel's ray meets, GPU and reference
+    xy = hits_ref["xy"]
+    _, _, gh = gpu_primary(spec, w, h, xtgpu.NODES_FP32, sc, px=xy)
+    g_gid = np.where(gh["prim"] != 0xffffffff, gh["prim"].astype(np.int64), -1)
+    r_gid = np.array([parity.global_prim(spec, o, p) if o >= 0 else -1
+                      for o, p in zip(hits_ref["obj"], hits_ref["prim"])])
+    agree_at = {tuple(p): bool(a) for p, a in zip(xy.tolist(), (g_gid == r_gid).tolist())}
     for key, integ in (("stencil", xtgpu.STENCIL), ("depth", xtgpu.DEPTH)):
         spp = int(g[key + "_spp"])
         img, rays = sc.render(integ, w, h, spp=spp)
-        xy = g[key + "_xy"]
-        got = img[xy[:, 1], xy[:, 0]]
-        ref = g[key + "_rgba"]
+        pxy = g[key + "_xy"]
+        got = img[pxy[:, 1], pxy[:, 0]].astype(np.float64)
+        ref = g[key + "_rgba"].astype(np.float64)
+        same = np.array([agree_at[tuple(p)] for p in pxy.tolist()])
+        print("[%s %s] primitive agrees on %.6f of %d pixels" % (name, key, same.mean(), same.size))
+        assert same.mean() >= 0.9999
         if integ == xtgpu.STENCIL:
-            assert (got == ref).all(axis=1).mean() >= 0.999
+            assert np.array_equal(got[same], ref[same])
         else:
-            both = (ref[:, 3] > 0)
-            rel = np.abs(got[:, 0] - ref[:, 0]) / np.maximum(np.abs(ref[:, 0]), 1e-6)
-            assert np.mean(rel[both] <= 1e-5) >= 0.999, np.sort(rel)[-5:]
+            hit = same & (ref[:, 3] > 0) & (ref[:, 0] != 0)
+            assert np.array_equal(got[same & ~hit], ref[same & ~hit])
+            dl = np.abs(1.0 / got[hit, 0] - 1.0 / ref[hit, 0])
+            print("[%s depth] max |ln t_gpu - ln t_ref| %.3g over %d hit pixels" % (name, dl.max(), hit.sum()))
+            assert dl.max() <= 1e-5, np.sort(dl)[-5:]
         assert rays == w * h * spp
     sc.close()
 
 
-def _rmse(a, b):
-    return float(np.sqrt(np.mean((a[:, :3] - b[:, :3]) ** 2)))
+def _truth(name):
+    t = np.load(os.path.join(GOLD, "truth.npz"))
+    return t[name + "_xy"], t[name + "_rgba"]
 
 
 @pytest.mark.parametrize("name,key,integ,md", [
@@ -356,39 +379,94 @@ def _rmse(a, b):
     ("hairball20k", "ao100", xtgpu.AO, 100.0), ("hairball20k", "ao0.2", xtgpu.AO, 0.2),
     ("spheres64", "pt", xtgpu.PATHTRACER, 100.0)])
 def test_stochastic_frames_within_reference_noise(name, key, integ, md):
+    """Per-pixel RMSE against the 4096-spp render (truth.npz) within the
+    reference's own at equal spp (its frames at four seeds, render_*.npz)."""
     spec, w, h = small_scenes()[name]
     g = np.load(os.path.join(GOLD, "render_%s.npz" % name))
-    sc = xtgpu.Scene(spec)
-    img, rays = sc.render(integ, w, h, spp=int(g[key + "_spp"]), rdepth=4, ao_max_distance=md, seed=777)
+    txy, truth = _truth("%s_%s" % (name, key))
     xy = g[key + "_xy"]
-    O = img[xy[:, 1], xy[:, 0]]
+    assert np.array_equal(xy, txy)
     R = g[key + "_rgba"]
-    n = R.shape[0]
-    ref = np.mean([_rmse(R[i], R[[j for j in range(n) if j != i]].mean(0)) for i in range(n)])
-    got = np.mean([_rmse(O, R[[j for j in range(n) if j != i]].mean(0)) for i in range(n)])
-    assert got <= 1.25 * ref + 1e-6, (got, ref)
-    for ch in range(3):
-        diff = O[:, ch] - R[:, :, ch].mean(0)
-        se = np.sqrt(R[:, :, ch].var(0, ddof=1).mean() / diff.size * (1 + 1.0 / n))
-        assert abs(diff.mean()) < 4.5 * se + 1e-5, (ch, diff.mean(), se)
+    sc = xtgpu.Scene(spec)
+    frames = []
+    for seed in (777, 778):
+        img, rays = sc.render(integ, w, h, spp=int(g[key + "_spp"]), rdepth=4, ao_max_distance=md, seed=seed)
+        frames.append(img[xy[:, 1], xy[:, 0]])
     sc.close()
+    parity.converged_rmse_bar(np.stack(frames), truth, [parity.rmse(r, truth) for r in R], "%s %s" % (name, key))
 
 
 @pytest.mark.parametrize("integ,md", [(xtgpu.AO, 0.5), (xtgpu.PATHTRACER, 100.0)])
 def test_stochastic_same_stream_as_oracle(integ, md):
     """With the same random stream, GPU (FP32) and oracle (FP64) frames differ
-    only where a rounding difference sends a path another way."""
+    only where a rounding difference sends a path another way: at most a
+    quarter of the sampling noise, and the rays traced within 1 %."""
     spec, w, h = small_scenes()["spheres64"]
     sc = xtgpu.Scene(spec)
     img, rays = sc.render(integ, w, h, spp=16, rdepth=4, ao_max_distance=md, seed=99)
+    sc.close()
     orc = po.OracleScene(spec, po.XO_ACCEL_BVH)
     ys, xs = np.mgrid[0:h, 0:w]
-    o, orays = orc.render(po.AO if integ == xtgpu.AO else po.PATHTRACER, w, h, spp=16, rdepth=4,
-                          ao_max_distance=md, seed=99, pixels=np.stack([xs.ravel(), ys.ravel()], 1))
-    d = np.abs(img.reshape(-1, 4)[:, :3] - o[:, :3]).max(axis=1)
-    assert np.mean(d < 1e-3) >= 0.97, np.mean(d < 1e-3)
+    px = np.stack([xs.ravel(), ys.ravel()], 1)
+    code = po.AO if integ == xtgpu.AO else po.PATHTRACER
+    o, orays = orc.render(code, w, h, spp=16, rdepth=4, ao_max_distance=md, seed=99, pixels=px)
+    o2, _ = orc.render(code, w, h, spp=16, rdepth=4, ao_max_distance=md, seed=100, pixels=px)
+    parity.same_stream_bar(img, o, o2, "spheres64 %s" % ("ao" if integ == xtgpu.AO else "pt"))
     assert abs(rays - orays) <= 0.01 * orays
+
+
+def _phong():
+    return scenes.phong_scene(), 65, 49
+
+
+@pytest.mark.parametrize("fmt", [xtgpu.NODES_FP32, xtgpu.NODES_W8])
+def test_phong_pathtracer_within_reference_noise(fmt):
+    """Phong and Blinn-Phong (reflectance 0.5 and 1, exponents 8 and 256) at
+    depth 4: per-pixel RMSE against the 4096-spp render within the reference's
+    own at equal spp (four reference seeds, render_phong.npz), rays traced
+    within the reference's spread."""
+    spec, w, h = _phong()
+    g = np.load(os.path.join(GOLD, "render_phong.npz"))
+    txy, truth = _truth("phong_pt")
+    xy = g["pt_xy"]
+    assert np.array_equal(xy, txy)
+    R = g["pt_rgba"]
+    sc = xtgpu.Scene(spec, node_formats=(fmt,))
+    frames, rays = [], []
+    for seed in (5, 6):
+        img, r = sc.render(xtgpu.PATHTRACER, w, h, spp=int(g["spp"]), rdepth=int(g["depth"]), seed=seed,
+                           node_format=fmt)
+        frames.append(img[xy[:, 1], xy[:, 0]])
+        rays.append(r)
     sc.close()
+    parity.converged_rmse_bar(np.stack(frames), truth, [parity.rmse(r, truth) for r in R], "phong fmt %d" % fmt)
+    ref_rays = g["pt_rays"].astype(np.float64)
+    # the GPU scores a lobe without a direction as a miss instead of tracing it
+    assert abs(np.mean(rays) - ref_rays.mean()) <= 5 * ref_rays.std() + 0.005 * ref_rays.mean(), (rays, ref_rays)
+
+
+def test_phong_same_stream_as_oracle():
+    """The specular lobe in FP64 on the GPU (sample.inl:61-90, step by step)
+    follows the oracle path by path.  The centre pixel's ray meets a Phong
+    sphere head-on (identity frame), where most lobe vectors underflow and the
+    next ray has no direction: the GPU scores those as the environment in
+    that direction, as the reference's ray meets nothing; the centre pixel
+    equals the oracle's within 1e-5."""
+    spec, w, h = _phong()
+    sc = xtgpu.Scene(spec)
+    img, rays = sc.render(xtgpu.PATHTRACER, w, h, spp=16, rdepth=4, seed=123)
+    sc.close()
+    orc = po.OracleScene(spec, po.XO_ACCEL_BVH)
+    ys, xs = np.mgrid[0:h, 0:w]
+    px = np.stack([xs.ravel(), ys.ravel()], 1)
+    o, orays = orc.render(po.PATHTRACER, w, h, spp=16, rdepth=4, seed=123, pixels=px)
+    o2, _ = orc.render(po.PATHTRACER, w, h, spp=16, rdepth=4, seed=124, pixels=px)
+    parity.same_stream_bar(img, o, o2, "phong pt")
+    centre = img[h // 2, w // 2].astype(np.float64)
+    oc = o.reshape(h, w, 4)[h // 2, w // 2].astype(np.float64)
+    print("[phong centre] gpu %s oracle %s" % (centre, oc))
+    assert np.allclose(centre, oc, rtol=1e-5, atol=1e-6)
+    assert abs(rays - orays) <= 0.01 * orays
 
 
 def test_render_is_deterministic_and_rect_consistent():

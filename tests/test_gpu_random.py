@@ -18,6 +18,7 @@ import numpy as np
 import pytest
 
 from oracle import pyoracle as po
+from tests import parity
 from tests.parity import random_distribution_agreement
 from xtracer_b200 import scenes, xtgpu
 from xtracer_b200.service import Service
@@ -113,8 +114,8 @@ def test_random_with_lens_and_ao_same_stream_as_oracle():
     assert np.mean(rel <= 1e-5) >= 0.99, np.sort(rel)[-5:]
     img, rays = sc.render(xtgpu.AO, w, h, spp=4, seed=43, ao_max_distance=0.5, aa=2, distribution=RANDOM)
     o, orays = _oracle_full(spec, po.AO, w, h, 4, 43, 2, md=0.5)
-    d = np.abs(img.reshape(-1, 4)[:, :3] - o[:, :3]).max(axis=1)
-    assert np.mean(d < 1e-3) >= 0.97, np.mean(d < 1e-3)
+    o2, _ = _oracle_full(spec, po.AO, w, h, 4, 44, 2, md=0.5)
+    parity.same_stream_bar(img, o, o2, "random aa2 dof ao")
     assert abs(rays - orays) <= 0.01 * orays
     sc.close()
 

@@ -88,3 +88,30 @@ def test_update_refuses_other_geometry():
     with pytest.raises(xtgpu.XtgpuError):
         sc.update(other, what=1)
     sc.close()
+
+
+def test_service_after_bvh_rebuild():
+    """A service's captured single-scene graphs hold the scene's node and leaf
+    buffers; after a rebuild with another leaf size (new buffers) and
+    xtgpu_service_update_scene, graphed waves render the rebuilt tree and
+    equal xtgpu_render's frame."""
+    spec = scenes.terrain_scene(20_000, seed=2, name="upd_rebuild")
+    sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_W8,), leaf_size=1)
+    svc = Service([sc], node_format=xtgpu.NODES_W8, use_graphs=True, wave_paths=1 << 14)
+    j = svc.submit(0, xtgpu.PATHTRACER, 64, 48, 8, 4, 100.0, 7)
+    svc.run()
+    first = svc.result(j).copy()
+    svc.release(j)
+    sc.build_bvh(xtgpu.NODES_W8, leaf_size=3)
+    svc.update_scene(0)
+    for _ in range(2):
+        j = svc.submit(0, xtgpu.PATHTRACER, 64, 48, 8, 4, 100.0, 7)
+        svc.run()
+        got = svc.result(j).copy()
+        svc.release(j)
+        ref, _ = sc.render(xtgpu.PATHTRACER, 64, 48, spp=8, rdepth=4, seed=7, node_format=xtgpu.NODES_W8)
+        assert np.array_equal(got, ref)
+        # every tree gives the same closest hits, so the frame is the first one
+        assert np.array_equal(got, first)
+    svc.close()
+    sc.close()

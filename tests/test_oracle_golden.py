@@ -427,3 +427,50 @@ def test_random_distribution_within_reference_noise():
             O.append(o)
         random_distribution_agreement(g[key + "_rgba"], np.stack(O), 3 if integ == "stencil" else 0,
                                       aa if integ == "stencil" else None)
+
+
+def test_lobe_edge_kat():
+    """sample::lobe (sample.inl:61-90) at its edges: the direction along the
+    normal (the frame stays the identity), 1 - d.n just below and above 1e-8,
+    exponents up to 2000 where pow(vdotr, e) underflows and the result is the
+    zero or unnormalised vector: the oracle returns the reference's bits."""
+    g = np.load(os.path.join(GOLD, "render_phong.npz"))
+    L = po.lib()
+    rm = int(g["rand_max"])
+    zero = 0
+    for i in range(g["lobe_out"].shape[0]):
+        tab = np.ascontiguousarray(g["lobe_rand"][i], np.int32)
+        out = np.zeros(3)
+        L.xo_kat_lobe(P(tab), rm, P(g["lobe_n"][i]), P(g["lobe_d"][i]), float(g["lobe_e"][i]), P(out))
+        assert np.array_equal(out, g["lobe_out"][i]), (i, out, g["lobe_out"][i])
+        zero += int(np.dot(out, out) == 0.0)
+    assert zero >= 4   # the identity-frame rows that give no direction are covered
+
+
+def test_phong_pathtracer_within_reference_noise():
+    """Phong and Blinn-Phong paths (render_phong.npz, four reference seeds):
+    the oracle's frames have per-pixel RMSE against the 4096-spp render within
+    the reference's at 16 spp, and the centre pixel (a head-on hit, identity
+    lobe frame) agrees with the reference's to within its noise."""
+    from tests import parity
+    g = np.load(os.path.join(GOLD, "render_phong.npz"))
+    t = np.load(os.path.join(GOLD, "truth.npz"))
+    xy, truth = t["phong_pt_xy"], t["phong_pt_rgba"]
+    assert np.array_equal(xy, g["pt_xy"])
+    spec = scenes.phong_scene()
+    orc = po.OracleScene(spec, po.XO_ACCEL_BVH)
+    frames, rays = [], []
+    for seed in (777, 778):
+        o, r = orc.render(po.PATHTRACER, int(g["width"]), int(g["height"]), spp=int(g["spp"]),
+                          rdepth=int(g["depth"]), seed=seed, pixels=xy)
+        frames.append(o)
+        rays.append(r)
+    R = g["pt_rgba"]
+    parity.converged_rmse_bar(np.stack(frames), truth, [parity.rmse(r, truth) for r in R], "oracle phong")
+    ref_rays = g["pt_rays"].astype(np.float64)
+    assert abs(np.mean(rays) - ref_rays.mean()) <= 5 * ref_rays.std() + 0.005 * ref_rays.mean()
+    c = np.nonzero((xy[:, 0] == int(g["width"]) // 2) & (xy[:, 1] == int(g["height"]) // 2))[0][0]
+    rc = R[:, c, :3].astype(np.float64)
+    oc = np.stack(frames)[:, c, :3].astype(np.float64)
+    assert np.all(np.abs(oc.mean(0) - rc.mean(0)) <= 4.5 * np.sqrt(rc.var(0, ddof=1) / 4 + oc.var(0, ddof=1) / 2)
+                  + 1e-3), (oc, rc)

@@ -7,7 +7,7 @@ import socket
 import pytest
 import torch.multiprocessing as mp
 
-from xtracer_b200 import replicas
+from xtracer_b200 import replicas, scenes
 
 
 def _free_port():
@@ -25,8 +25,8 @@ def _worker(rank, world, port, q):
     jobs = replicas.rank_stream(rank, n_jobs=16)
     t = 1.0 + rank            # rank 1 is slower
     rays = 1000 * (rank + 1)
-    out = dict(rank=rank, first=(jobs[0].scene, jobs[0].width, jobs[0].spp), tmax=g.max(t), rays=g.sum(rays),
-               lat=g.gather([float(rank)] * (rank + 2)))
+    out = dict(rank=rank, seeds=[j.seed for j in jobs], shapes=[(j.scene, j.width, j.spp) for j in jobs],
+               tmax=g.max(t), rays=g.sum(rays), lat=g.gather([float(rank)] * (rank + 2)))
     g.barrier()
     g.close()
     q.put(out)
@@ -46,8 +46,15 @@ def test_two_gloo_ranks():
     assert res[0]["tmax"] == res[1]["tmax"] == 2.0
     assert res[0]["rays"] == res[1]["rays"] == 3000
     assert res[0]["lat"] == res[1]["lat"] == [0.0, 0.0, 1.0, 1.0, 1.0]
-    assert res[0]["first"] != res[1]["first"] or replicas.rank_stream(0, 16)[1:] != replicas.rank_stream(1, 16)[1:]
-    assert replicas.rank_stream(1, 16)[0].seed == replicas.rank_stream(1, 16)[0].seed
+    # each rank serves the seeded stream of its own rank (seed 4 + rank), made
+    # inside the rank's process: its jobs' seeds and shapes are that stream's,
+    # and no sample seed is shared between the ranks
+    for r in (0, 1):
+        want = scenes.job_stream(16, seed=4 + r)
+        assert res[r]["seeds"] == [j.seed for j in want]
+        assert res[r]["shapes"] == [(j.scene, j.width, j.spp) for j in want]
+    assert not set(res[0]["seeds"]) & set(res[1]["seeds"])
+    assert res[0]["shapes"] != res[1]["shapes"]
 
 
 def test_single_rank_is_identity():

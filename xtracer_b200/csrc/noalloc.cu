@@ -23,7 +23,10 @@
 //     on it and corrupt each other's results;
 //   * the first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (once per device); make that first call before any
-//     stream capture.
+//     stream capture;
+//   * every call copies its job from host memory and waits for its stream
+//     before it returns, so the stream it is given must not be capturing
+//     (XTGPU_ERR_STATE).
 #include <mutex>
 
 #include "render.h"
@@ -120,6 +123,13 @@ extern "C" xtgpu_status xtgpu_render_tile_noalloc(xtgpu_scene *sc, const xtgpu_r
         set_error("xtgpu_render_tile_noalloc: node format not built for this scene");
         return XTGPU_ERR_STATE;
     }
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    XTG_CUDA(cudaStreamIsCapturing((cudaStream_t)stream, &cap));
+    if (cap != cudaStreamCaptureStatusNone) {
+        set_error("xtgpu_render_tile_noalloc: the stream is capturing; each call copies its job from host memory "
+                  "and waits for the stream");
+        return XTGPU_ERR_STATE;
+    }
     unsigned char *base = nullptr;
     int dev = 0;
     XTG_TRY(noalloc_scratch(&base, &dev));
@@ -180,8 +190,15 @@ extern "C" xtgpu_status xtgpu_render_tile_noalloc(xtgpu_scene *sc, const xtgpu_r
     XTG_CUDA(cudaMemsetAsync(rgba, 0, sizeof(float4) * npix, s));
     int sms = 148;
     XTG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    // the camera rays take the tuned node format when it is built, as in xtgpu_render
+    int fmt0 = -1, stack0 = 0;
+    if (T.primary_node_format >= 0 && T.primary_node_format != p->node_format &&
+        format_built(sc, T.primary_node_format)) {
+        fmt0 = T.primary_node_format;
+        stack0 = stack_for_scene(sc, fmt0, T.stack_entries);
+    }
     enqueue_wave_raw(T, q, jobs_dev, scene_dev, sc->dev, prefix_dev, J.bounces, p->node_format, sms,
-                     stack_for_scene(sc, p->node_format, T.stack_entries), s);
+                     stack_for_scene(sc, p->node_format, T.stack_entries), fmt0, stack0, s);
     XTG_CUDA(cudaGetLastError());
     int32_t back[16];
     XTG_CUDA(cudaMemcpyAsync(back, q.ctl, sizeof(back), cudaMemcpyDeviceToHost, s));

@@ -14,6 +14,7 @@
 //   sampling    lib/nmath/sample.inl:28-107, in FP32
 #include <algorithm>
 #include <climits>
+#include <cstring>
 #include <vector>
 
 #include "render.h"
@@ -222,26 +223,72 @@ __device__ float3 s_diffuse(float3 n, uint64_t key, uint32_t &ctr)
     return normalized(p + n);
 }
 
-// sample::lobe (sample.inl:61-90).  vc * pow(vdotr, e) normalised is vc (or 0).
-__device__ float3 s_lobe(float3 n, float3 dir, float e, uint64_t key, uint32_t &ctr)
+// sample::lobe (sample.inl:61-90) in FP64, step by step: the frame (ivec,
+// refl, kvec) as columns, or the identity when 1 - d.n <= 1e-8 (the raw,
+// unnormalised vectors, as the reference tests them); then vc * pow(vdotr, e)
+// normalised.  Returns false when that product is too small for its length to
+// be nonzero in FP64 (vdotr clamped to 0, or pow underflowing, which happens
+// with the identity frame, where vc need not lie around the reflection): the
+// reference then keeps the unnormalised, zero or subnormal vector as the next
+// ray's direction, and that ray meets nothing (every primitive test rejects a
+// direction whose dot products are below 1e-8).  `out` is the direction
+// rounded to FP32; `twice` normalises it once more first, as
+// BlinnPhong::sample_path does (blinnphong.cc:55).  `raw` is the FP64
+// vector, which the environment takes in the degenerate case.
+__device__ __forceinline__ double ddot3(const double a[3], const double b[3])
 {
-    float3 i = normalized(dir), nn = normalized(n);
-    float3 refl = nn * (2.f * dot3(i, nn)) - i;
-    float3 cx = make_float3(1.f, 0.f, 0.f), cy = make_float3(0.f, 1.f, 0.f), cz = make_float3(0.f, 0.f, 1.f);
-    if (1.0f - dot3(dir, n) > 1e-8f) {
-        cx = normalized(cross3(dir, refl));
-        cy = refl;
-        cz = cross3(refl, cx);
+    return __dadd_rn(__dadd_rn(__dmul_rn(a[0], b[0]), __dmul_rn(a[1], b[1])), __dmul_rn(a[2], b[2]));
+}
+__device__ __forceinline__ void dcross3(const double a[3], const double b[3], double r[3])
+{
+    r[0] = __dsub_rn(__dmul_rn(a[1], b[2]), __dmul_rn(a[2], b[1]));
+    r[1] = __dsub_rn(__dmul_rn(a[2], b[0]), __dmul_rn(a[0], b[2]));
+    r[2] = __dsub_rn(__dmul_rn(a[0], b[1]), __dmul_rn(a[1], b[0]));
+}
+__device__ __noinline__ bool s_lobe(float3 nf, float3 df, float e, bool twice, uint64_t key, uint32_t &ctr, float3 &out,
+                       double3 &raw)
+{
+    const double n[3] = {nf.x, nf.y, nf.z}, d[3] = {df.x, df.y, df.z};
+    double i[3] = {d[0], d[1], d[2]}, nn[3] = {n[0], n[1], n[2]};
+    dnormalize3(i);
+    dnormalize3(nn);
+    // Vector3f::reflected (vector.inl:455-460): (2 * dot(i, n) * n) - i
+    const double k2 = __dmul_rn(2.0, ddot3(i, nn));
+    double refl[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) refl[c] = __dsub_rn(__dmul_rn(k2, nn[c]), i[c]);
+    double cx[3] = {1.0, 0.0, 0.0}, cy[3] = {0.0, 1.0, 0.0}, cz[3] = {0.0, 0.0, 1.0};   // Matrix3x3f() = identity
+    if (__dsub_rn(1.0, ddot3(d, n)) > 1e-8) {
+        dcross3(d, refl, cx);
+        dnormalize3(cx);
+        cy[0] = refl[0]; cy[1] = refl[1]; cy[2] = refl[2];
+        dcross3(refl, cx, cz);
     }
-    float u = uniform(key, ctr), v = uniform(key, ctr);
-    float theta = 6.283185307179586f * u;
-    float phi = acosf(powf(v, 1.0f / (e + 1.0f)));
-    float sp, cp, st, ct;
-    sincosf(phi, &sp, &cp);
-    sincosf(theta, &st, &ct);
-    float3 vc = cx * (ct * sp) + cy * cp + cz * (st * sp);
-    float vdotr = dot3(refl, vc);
-    return vdotr > 0.f ? normalized(vc) : make_float3(0.f, 0.f, 0.f);
+    const double u = (double)uniform(key, ctr), v = (double)uniform(key, ctr);
+    const double theta = __dmul_rn(__dmul_rn(2.0, 3.14159265358979323846), u);
+    const double phi = acos(pow(v, __ddiv_rn(1.0, __dadd_rn((double)e, 1.0))));
+    const double sp = sin(phi), cp = cos(phi), st = sin(theta), ct = cos(theta);
+    const double l[3] = {__dmul_rn(ct, sp), cp, __dmul_rn(st, sp)};
+    double vc[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)   // Vector3f::transformed: the matrix times the column vector
+        vc[c] = __dadd_rn(__dadd_rn(__dmul_rn(cx[c], l[0]), __dmul_rn(cy[c], l[1])), __dmul_rn(cz[c], l[2]));
+    double vdotr = ddot3(refl, vc);
+    if (vdotr < 0.0) vdotr = 0.0;
+    const double p = pow(vdotr, (double)e);
+    double w[3] = {__dmul_rn(vc[0], p), __dmul_rn(vc[1], p), __dmul_rn(vc[2], p)};
+    const double len = dlen3(w);
+    raw = make_double3(w[0], w[1], w[2]);
+    if (len == 0.0) {
+        out = make_float3(0.f, 0.f, 0.f);
+        return false;
+    }
+    w[0] = __ddiv_rn(w[0], len);
+    w[1] = __ddiv_rn(w[1], len);
+    w[2] = __ddiv_rn(w[2], len);
+    if (twice) dnormalize3(w);
+    out = make_float3((float)w[0], (float)w[1], (float)w[2]);
+    return true;
 }
 
 
@@ -473,15 +520,19 @@ __device__ __forceinline__ float3 mat_color(const DevScene &S, const DevMaterial
 }
 
 // Scene::sample_environment (scene.cc:142-145): black without an environment
-__device__ float3 environment(const DevScene &S, float3 dir)
+__device__ float3 environment_d(const DevScene &S, double x, double y, double z)
 {
     switch (S.env_type) {
     case XTGPU_ENV_COLOR: return S.env_a;
-    case XTGPU_ENV_GRADIENT: return gradient_sample(S.env_a, S.env_b, dir.x, dir.y, dir.z);
-    case XTGPU_ENV_ERP: return erp_sample(S, S.env_tex, dir.x, dir.y, dir.z);
-    case XTGPU_ENV_CUBEMAP: return cube_sample(S, S.env_tex, dir.x, dir.y, dir.z);
+    case XTGPU_ENV_GRADIENT: return gradient_sample(S.env_a, S.env_b, x, y, z);
+    case XTGPU_ENV_ERP: return erp_sample(S, S.env_tex, x, y, z);
+    case XTGPU_ENV_CUBEMAP: return cube_sample(S, S.env_tex, x, y, z);
     default: return make_float3(0.f, 0.f, 0.f);
     }
+}
+__device__ __forceinline__ float3 environment(const DevScene &S, float3 dir)
+{
+    return environment_d(S, dir.x, dir.y, dir.z);
 }
 
 // Pixel of the k-th pixel slot of a job.  With tiles, slots run through
@@ -1075,7 +1126,8 @@ __global__ void __launch_bounds__(256, 4) k_shade(const DevJob *__restrict__ job
                 float3 nrm = hit_normal(S, h.prim, p, h.u, h.v);
                 const DevMaterial &M = S.materials[S.obj_material[S.prim_obj[h.prim]]];
                 float3 f, nd3;
-                bool go = true;
+                double3 lobe_raw = make_double3(0.0, 0.0, 0.0);
+                bool go = true, aimed = true;
                 if (M.type == XTGPU_LAMBERT) {
                     nd3 = normalized(s_diffuse(nrm, key, ctr));
                     f = cmuls(mat_color(S, M, 0, h, o, d), dot3(nrm, nd3));
@@ -1086,7 +1138,8 @@ __global__ void __launch_bounds__(256, 4) k_shade(const DevJob *__restrict__ job
                         nd3 = s_diffuse(nrm, key, ctr);
                     } else {
                         f = mat_color(S, M, 1, h, o, d);
-                        nd3 = s_lobe(nrm, make_float3(-d.x, -d.y, -d.z), M.exponent, key, ctr);
+                        aimed = s_lobe(nrm, make_float3(-d.x, -d.y, -d.z), M.exponent, M.type == XTGPU_BLINNPHONG,
+                                       key, ctr, nd3, lobe_raw);
                     }
                 } else if (M.type == XTGPU_EMISSIVE) {
                     float3 L = cmul(Pp, cmul(Ii, mat_color(S, M, 2, h, o, d)));
@@ -1104,6 +1157,13 @@ __global__ void __launch_bounds__(256, 4) k_shade(const DevJob *__restrict__ job
                     // zero prefix stays zero: both end the path at value 0
                     if (depth_left - 1 <= 0 || (np.x == 0.f && np.y == 0.f && np.z == 0.f)) {
                         q.contrib[lp] = make_float4(0.f, 0.f, 0.f, 1.f);
+                    } else if (!aimed) {
+                        // a specular lobe without a direction: the reference's
+                        // next ray meets nothing, so eval() returns the
+                        // environment in that (zero) direction; it is scored
+                        // here instead of being traced
+                        float3 L = cmul(np, environment_d(S, lobe_raw.x, lobe_raw.y, lobe_raw.z));
+                        q.contrib[lp] = make_float4(L.x, L.y, L.z, 1.f);
                     } else {
                         float3 org = offset_ray(p, normalized(nrm));
                         no = make_float4(org.x, org.y, org.z, 0.f);
@@ -1304,6 +1364,18 @@ xtgpu_status WaveRunner::set_scenes(const DevScene *scenes, int n, cudaStream_t 
     if (n > max_scenes) {
         set_error("too many scenes for the wave runner");
         return XTGPU_ERR_LIMIT;
+    }
+    // A captured single-scene graph holds its scene by value (node and leaf
+    // pointers included), keyed only by the scene's index.  When a scene's
+    // description changes (a rebuilt BVH moves its buffers), every captured
+    // graph goes; the caller has let the runner's waves finish.
+    bool changed = (size_t)n < host_scenes.size();
+    for (int i = 0; i < n && (size_t)i < host_scenes.size() && !changed; ++i)
+        changed = memcmp(&host_scenes[(size_t)i], &scenes[i], sizeof(DevScene)) != 0;
+    if (changed) {
+        for (auto &g : graphs)
+            if (g.second) cudaGraphExecDestroy(g.second);
+        graphs.clear();
     }
     XTG_CUDA(cudaMemcpyAsync(scenebuf.p, scenes, sizeof(DevScene) * (size_t)n, cudaMemcpyHostToDevice, s));
     nscenes = n;
@@ -1536,14 +1608,23 @@ void launch_extend_kernel(const xtgpu_tuning &T, int fmt, bool multi, const DevS
 
 void enqueue_wave_raw(const xtgpu_tuning &T, const WaveQueues &q, const DevJob *jobs, const DevScene *scenes,
                       const DevScene &single, const int64_t *prefix, int bounces, int fmt, int sms, int stack,
-                      cudaStream_t s)
+                      int fmt0, int stack0, cudaStream_t s)
 {
     const int gb = sms * 8;
     k_camera<<<gb, 256, 0, s>>>(jobs, scenes, q);
     int side = 0;
+    // the camera rays may take their own node format and extend kernel, as in
+    // WaveRunner::enqueue
+    xtgpu_tuning T0 = T;
+    if (T.primary_variant >= 0) T0.extend_variant = T.primary_variant;
+    const bool own0 = fmt0 >= 0 && fmt0 != fmt;
     for (int b = 0; b < bounces; ++b) {
         cudaMemsetAsync(q.ctl + 2, 0, sizeof(int32_t), s);
-        launch_extend_kernel(T, fmt, false, single, scenes, jobs, q, side, sms, stack, s);
+        if (b == 0)
+            launch_extend_kernel(T0, own0 ? fmt0 : fmt, false, single, scenes, jobs, q, side, sms, own0 ? stack0 : stack,
+                                 s);
+        else
+            launch_extend_kernel(T, fmt, false, single, scenes, jobs, q, side, sms, stack, s);
         cudaMemsetAsync(q.ctl + (side ^ 1), 0, sizeof(int32_t), s);
         k_shade<<<gb, 256, 0, s>>>(jobs, scenes, q, side);
         side ^= 1;

@@ -80,7 +80,7 @@ int stack_for_depth(int depth, int requested);
 // wave (ctl[0] = ctl[5] = paths, ctl[4] = jobs, other counters zero).
 void enqueue_wave_raw(const xtgpu_tuning &T, const WaveQueues &q, const DevJob *jobs, const DevScene *scenes,
                       const DevScene &single, const int64_t *prefix, int bounces, int fmt, int sms, int stack,
-                      cudaStream_t s);
+                      int fmt0, int stack0, cudaStream_t s);
 // Closest hit of the q.ctl[side] rays of queue `side` (no job table needed).
 void launch_extend(const xtgpu_tuning &T, int fmt, const DevScene &S, const WaveQueues &q, int side, int sms,
                    int stack, cudaStream_t s);

@@ -4,8 +4,8 @@ One scene of the served job stream; primary rays of its camera, then a batch of
 first-bounce rays, cosine-distributed around the face normal at each primary
 hit (primary rays that missed stay in the batch).  Times xtgpu_trace on the
 bounce batch with CUDA events and reports Mrays/s, nodes and primitives per ray,
-algorithmic bytes per ray and achieved GB/s.  The ncu summaries under profiles/
-are captures of this script.
+algorithmic bytes per ray and achieved GB/s; the extend kernel's ncu captures
+run this script.
 
     python -m xtracer_b200.profile_extend --scene hairball2m --rays 1048576 --fmt q8 --iters 5
 """

@@ -1,8 +1,8 @@
 """One frame of one served-stream scene through xtgpu_render, for kernel
 captures of the whole wavefront (camera, extend, shade, accumulate) on full
 waves.  Renders the job `--iters` times after one warm-up render and reports
-the device time per frame and Mrays/s.  The ncu summaries of k_shade under
-profiles/ are captures of this script.
+the device time per frame and Mrays/s; the shade kernel's ncu captures run
+this script.
 
     python -m xtracer_b200.profile_render --scene terrain200k --size 1024 --spp 4
 """

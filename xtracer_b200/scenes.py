@@ -448,6 +448,50 @@ def spheres_scene(n_spheres: int = 64, seed: int = 1, extent: float = 5.0, name:
                      k, f, cnt, om, mats, cam, ENV_GRADIENT, (1.0, 1.0, 1.0), (0.5, 0.7, 1.0))
 
 
+def phong_scene(seed: int = 51, name: str = "phongscene") -> SceneSpec:
+    """Spheres and a plane with Phong and Blinn-Phong materials (phong.cc,
+    blinnphong.cc), for the specular lobe (sample.inl:61-90):
+
+    * 16 spheres cycling over {Phong, Blinn-Phong} x reflectance {0.5, 1.0} x
+      exponent {8, 256}, colours uniform in [0.1, 0.9]^3;
+    * a Blinn-Phong ground plane (reflectance 0.5, exponent 8) and a small
+      emissive sphere, under a gradient sky;
+    * a Phong sphere (reflectance 1, exponent 256) centred on the camera axis.
+      With an odd frame width and height the centre pixel's ray meets it
+      head-on, so d.n = 1 and the lobe takes the identity frame; its lobe
+      vectors then mostly have vdotr <= 0 or pow(vdotr, 256) below FP64's
+      range, and the next ray has no direction."""
+    rng = np.random.default_rng(seed)
+    mats = [Material(BLINNPHONG, diffuse=(0.5, 0.5, 0.5), specular=(0.8, 0.8, 0.8), reflectance=0.5,
+                     exponent=8.0)]
+    kinds, firsts, counts, omat = [PLANE], [0], [1], [0]
+    sph = []
+    for i in range(16):
+        gx, gz = i % 4, i // 4
+        c = (gx * 2.5 - 3.75 + rng.uniform(-0.3, 0.3), rng.uniform(0.6, 1.2), gz * 2.5 - 1.0 + rng.uniform(-0.3, 0.3))
+        r = rng.uniform(0.5, 0.9)
+        mtype = PHONG if i % 2 == 0 else BLINNPHONG
+        refl = 0.5 if (i // 2) % 2 == 0 else 1.0
+        ex = 8.0 if (i // 4) % 2 == 0 else 256.0
+        dif, spe = _q(rng.uniform(0.1, 0.9, 3), 16), _q(rng.uniform(0.1, 0.9, 3), 16)
+        mats.append(Material(mtype, diffuse=tuple(float(x) for x in dif), specular=tuple(float(x) for x in spe),
+                             reflectance=refl, exponent=ex))
+        sph.append(list(_q(np.array(c), 16)) + [_qs(r, 16)])
+        kinds.append(SPHERE); firsts.append(i); counts.append(1); omat.append(len(mats) - 1)
+    # on the camera axis: camera (0, 4, -12) looking at (0, 1, 0)
+    mats.append(Material(PHONG, diffuse=(0.5, 0.5, 0.5), specular=(0.9, 0.8, 0.7), reflectance=1.0, exponent=256.0))
+    sph.append([0.0, 2.5, -6.0, 0.75])
+    kinds.append(SPHERE); firsts.append(16); counts.append(1); omat.append(len(mats) - 1)
+    mats.append(Material(EMISSIVE, emissive=(6.0, 5.5, 5.0)))
+    sph.append([2.0, 4.5, 3.0, 0.5])
+    kinds.append(SPHERE); firsts.append(17); counts.append(1); omat.append(len(mats) - 1)
+    planes = np.array([[0.0, 1.0, 0.0, 0.0]], np.float32)
+    k, f, cnt, om = _objects(kinds, firsts, counts, omat)
+    cam = Camera((0.0, 4.0, -12.0), (0.0, 1.0, 0.0), (0.0, 1.0, 0.0), 60.0)
+    return SceneSpec(name, np.array(sph, np.float32), planes, np.zeros((0, 3, 3), np.float32), k, f, cnt, om,
+                     mats, cam, ENV_GRADIENT, (1.0, 1.0, 1.0), (0.5, 0.7, 1.0))
+
+
 def _value_noise(x: np.ndarray, z: np.ndarray, lattice: np.ndarray) -> np.ndarray:
     """Value noise with smoothstep interpolation on a periodic random lattice."""
     L = lattice.shape[0]

@@ -8,7 +8,9 @@
 # Outputs go to xtracer_b200/_build/: xtcore_obj/ (the host objects) and
 # xtgpu-xtcore (rpath $ORIGIN, next to libxtgpu.so, which must be built first).
 
-REF      ?= /root/reference
+ifndef REF
+$(error REF must name the XTracer source tree: make -f xtracer_b200/xtcore/xtcore.mk REF=<dir>)
+endif
 HERE     := $(dir $(lastword $(MAKEFILE_LIST)))
 BUILD    := $(HERE)../_build
 OBJDIR   := $(BUILD)/xtcore_obj
