@@ -173,6 +173,47 @@ def run_slice(svc, jobs, record=None, per_scene=None, view=False):
     return rays, lat
 
 
+def serve_open_loop(svc, jobs, arrivals):
+    """Open-loop serving with live arrivals: one thread runs the (open)
+    service while this one submits each job when its arrival time (seconds
+    from the start) comes, whatever is on the GPU then.  Returns the jobs'
+    latencies (result available minus submission, service clock), their rays
+    and the wall time from the first arrival to the last result."""
+    from xtracer_b200 import xtgpu
+    errors = []
+
+    def serve():
+        try:
+            svc.run()
+        except Exception as e:   # re-raised below
+            errors.append(e)
+
+    svc.open(True)
+    th = threading.Thread(target=serve)
+    th.start()
+    ids = []
+    t0 = time.perf_counter()
+    for j, a in zip(jobs, arrivals):
+        dt = float(a) - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        ids.append(svc.submit(j.scene, xtgpu.PATHTRACER, j.width, j.height, j.spp, j.depth, 100.0, j.seed))
+    svc.open(False)
+    th.join()
+    wall = time.perf_counter() - t0
+    if errors:
+        raise errors[0]
+    lats, rays = [], 0
+    for i in ids:
+        st = svc.poll(i)
+        if st.state != 2:
+            raise RuntimeError("job %d did not finish (state %d)" % (i, st.state))
+        lats.append(st.finish_s - st.submit_s)
+        rays += st.rays
+        svc.release(i)
+    return lats, rays, wall
+
+
 def pct(v, q):
     return float(np.percentile(np.asarray(v), q)) if len(v) else None
 
@@ -201,37 +242,91 @@ def roofline_bytes_per_ray(specs, gpu_scenes, node_format):
 
 
 # ---------------------------------------------------------------------------
-def cpu_reference_sample(scale, threads, budget_s=20.0):
-    """The reference renderer (oracle/_ref/xtref, XTracer's xtcore built from its
-    sources) on the host cores: pathtracer depth 4 over crops of stream jobs on
-    the scenes it loads quickly (spheres64, spheres4096, terrain10k,
-    terrain50k).  The octree build of the larger meshes alone takes minutes, so
-    they are left out of the sample."""
+# The fixed sample the reference renderer (oracle/_ref/xtref: XTracer's xtcore
+# built from its sources) is timed on, the same in the --impl reference arm and
+# in the cpu_baseline leg: for each of the 8 resident scenes, one pathtracer
+# job of the stream's kind (256x256 frame, depth 4, seed 7) rendered on a
+# centred crop.  Crop edge and spp per scene keep each render to a few seconds
+# on the host cores; the reference's cost per ray grows with the mesh
+# (Octree::r_intersection tests every triangle of every node a ray's box
+# meets, octree.tml:206-249).  Scene load and octree build are timed apart.
+CPU_SAMPLE = [("terrain10k", 32, 4), ("terrain50k", 20, 4), ("terrain200k", 12, 4), ("terrain500k", 8, 4),
+              ("terrain1m", 6, 4), ("hairball2m", 6, 1), ("spheres64", 64, 16), ("spheres4096", 24, 4)]
+CPU_FRAME = 256
+
+
+def cpu_sample_text():
+    return ("pathtracer depth 4, seed 7, on centred crops of %dx%d frames: " % (CPU_FRAME, CPU_FRAME) +
+            ", ".join("%s %dx%d x %d spp" % (n, c, c, spp) for n, c, spp in CPU_SAMPLE) +
+            " (IIntegrator::render timed, rays counted at Scene::intersection; scene load and octree build "
+            "timed apart)")
+
+
+def cpu_crop(c):
+    x0 = (CPU_FRAME - c) // 2
+    return (x0, x0, x0 + c, x0 + c)
+
+
+def cpu_reference_runs(scale, threads, repeats):
+    """Per scene of CPU_SAMPLE: the reference loads the scene once and renders
+    its crop `repeats` times.  Returns [{"scene", "load_s", "renders": [...]}]
+    or None when the harness is not built."""
     from oracle import pyoracle as po
     from xtracer_b200 import scenes
     if not po.ref_available():
         return None
     work = tempfile.mkdtemp(prefix="xtref")
-    total_rays, total_s, parts = 0, 0.0, []
-    plan = [("spheres64", 256, 16, 48), ("terrain10k", 256, 16, 48), ("terrain50k", 256, 16, 32),
-            ("spheres4096", 256, 4, 12)]
-    for name, res, spp, crop in plan:
+    out = []
+    for name, crop, spp in CPU_SAMPLE:
         spec = scenes.jobstream_scene(name, scale)
         scn = spec.write_scn(work)
-        x0 = (res - crop) // 2
-        tiles = [(x0, x0, x0 + crop, x0 + crop)]
-        t0 = time.time()
-        xy, rgba, st = po.ref_render(scn, "pathtracer", res, res, spp=spp, rdepth=4, threads=threads, seed=7,
-                                     tiles=tiles, workdir=work)
-        total_rays += st["rays"]
-        total_s += st["render_s"]
-        parts.append("%s %dx%d crop of %d^2 x %d spp" % (name, crop, crop, res, spp))
-        budget_s -= time.time() - t0
-        if budget_s <= 0:
-            break
-    return {"value": total_rays / total_s / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "reference",
-            "sample": "; ".join(parts) + " (pathtracer depth 4, IIntegrator::render timed, rays counted at "
-                                        "Scene::intersection)", "rays": total_rays, "seconds": total_s}
+        r = po.ref_bench(scn, "pathtracer", CPU_FRAME, CPU_FRAME, spp, 4, threads, 7, [cpu_crop(crop)], repeats,
+                         workdir=work)
+        r["scene"] = name
+        out.append(r)
+    return out
+
+
+def cpu_reference_sample(scale, threads):
+    """The cpu_baseline leg: one untimed and one timed render of every crop of
+    the sample; Mrays/s over the timed renders, per scene and in total."""
+    runs = cpu_reference_runs(scale, threads, 2)
+    if runs is None:
+        return None
+    rays = sum(r["renders"][1]["rays"] for r in runs)
+    secs = sum(r["renders"][1]["render_s"] for r in runs)
+    return {"value": rays / secs / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "reference",
+            "sample": cpu_sample_text(), "rays": rays, "seconds": secs,
+            "per_scene": {r["scene"]: {"mrays": r["renders"][1]["rays"] / r["renders"][1]["render_s"] / 1e6,
+                                       "rays": r["renders"][1]["rays"], "render_s": r["renders"][1]["render_s"],
+                                       "load_s": r["load_s"]} for r in runs}}
+
+
+def gpu_on_cpu_sample(gscenes, specs):
+    """The GPU (xtgpu_render, FP32 nodes, one job per call) on the jobs of the
+    CPU sample: each crop as the CPU rendered it, and the job's whole frame;
+    Mrays/s per scene from CUDA events (best of 3 after a warm-up)."""
+    import torch
+    from xtracer_b200 import xtgpu
+    names = [s.name for s in specs]
+    out = {}
+    for name, crop, spp in CPU_SAMPLE:
+        sc = gscenes[names.index(name)]
+        row = {}
+        for tag, rect in (("crop", cpu_crop(crop)), ("frame", None)):
+            best = None
+            for it in range(4):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                _, rays = sc.render(xtgpu.PATHTRACER, CPU_FRAME, CPU_FRAME, spp=spp, rdepth=4, seed=7, rect=rect)
+                e1.record()
+                torch.cuda.synchronize()
+                if it:
+                    t = e0.elapsed_time(e1) / 1000.0
+                    best = t if best is None else min(best, t)
+            row[tag + "_mrays"] = rays / best / 1e6
+        out[name] = row
+    return out
 
 
 def reference_arm(args):
@@ -239,26 +334,26 @@ def reference_arm(args):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    vals = []
-    for _ in range(args.warmup):
-        cpu_reference_sample(args.scale, threads, budget_s=5.0)
-    t_all, r_all = 0.0, 0
-    for _ in range(args.steps):
-        r = cpu_reference_sample(args.scale, threads, budget_s=5.0)
-        if r is None:
-            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/xtref was not built"}))
-            return 0
-        t_all += r["seconds"]
-        r_all += r["rays"]
-        vals.append(r)
+    runs = cpu_reference_runs(args.scale, threads, args.warmup + args.steps)
+    if runs is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/xtref was not built"}))
+        return 0
+    # step k: every crop of the sample rendered once (the k-th render of each
+    # scene's process); the scenes were loaded before the first step
+    steps = range(args.warmup, args.warmup + args.steps)
+    t_all = sum(r["renders"][k]["render_s"] for r in runs for k in steps)
+    r_all = sum(r["renders"][k]["rays"] for r in runs for k in steps)
     value = r_all / t_all / 1e6
+    per_scene = {r["scene"]: {"mrays": sum(r["renders"][k]["rays"] for k in steps) /
+                              sum(r["renders"][k]["render_s"] for k in steps) / 1e6,
+                              "load_s": r["load_s"]} for r in runs}
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_all / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded scenes and job stream)",
-            "config": {"workload": WORKLOAD, "sample": vals[-1]["sample"]},
+            "config": {"workload": WORKLOAD, "sample": cpu_sample_text()},
             "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": "reference",
-                             "sample": vals[-1]["sample"]},
+                             "sample": cpu_sample_text(), "per_scene": per_scene},
             "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -435,24 +530,48 @@ def main():
                  "equal_rmse": {"jobs": len(check_jobs), "frames_bit_identical": bool(same),
                                 "max_abs_diff": diff}}
 
-    # open-loop latency: Poisson arrivals at 1.5x the plain path's job rate
+    # open-loop latency over the rank's whole stream: its jobs arrive as a
+    # Poisson process at 1.5x the plain path's job rate (offered load above the
+    # plain path's capacity) and are submitted live while earlier jobs are on
+    # the GPU; the served form and the plain path on the same arrivals
     latency = None
     if not args.no_latency:
         rate = 1.5 * len(timed[0]) / ps if plain is not None else 50.0
+        arr = np.cumsum(np.random.default_rng(4 + rank).exponential(1.0 / rate, len(jobs)))
+        arr -= arr[0]
         lsvc = Service(gscenes, node_format=SERVED_FORMAT, use_graphs=True, merge_jobs=True, memory_budget=budget,
-                       stream=stream)
-        arr = np.cumsum(np.random.default_rng(4).exponential(1.0 / rate, len(timed[0])))
-        ids = [lsvc.submit(j.scene, xtgpu.PATHTRACER, j.width, j.height, j.spp, j.depth, 100.0, j.seed,
-                           submit_s=0.05 + float(a)) for j, a in zip(timed[0], arr)]
-        lsvc.run()
-        lats = [lsvc.poll(i).finish_s - lsvc.poll(i).submit_s for i in ids]
+                       waves_in_flight=WAVES_IN_FLIGHT, stream=stream)
+        run_slice(lsvc, slices[0])   # graphs of this service captured before the arrivals start
+        lats, lrays, lwall = serve_open_loop(lsvc, jobs, arr)
         lsvc.close()
-        latency = {"arrivals": "Poisson, %.2f jobs/s (1.5x the plain path's job rate)" % rate,
-                   "jobs": len(ids), "p50_ms": 1000 * pct(lats, 50), "p99_ms": 1000 * pct(lats, 99)}
+        lat_all_open = D.gather(lats)
+        latency = {"arrivals": "Poisson, %.2f jobs/s (1.5x the plain path's job rate), submitted live" % rate,
+                   "jobs": len(lat_all_open), "p50_ms": 1000 * pct(lat_all_open, 50),
+                   "p99_ms": 1000 * pct(lat_all_open, 99), "max_ms": 1000 * max(lat_all_open),
+                   "mrays_s_wall": D.sum(lrays) / D.max(lwall) / 1e6, "wall_s": D.max(lwall),
+                   "memory_budget_gb": budget / 2 ** 30}
+        if plain is not None:
+            psvc = Service(gscenes, node_format=xtgpu.NODES_FP32, use_graphs=False, merge_jobs=False,
+                           memory_budget=budget, waves_in_flight=1, stream=stream)
+            plats, prays, pwall = serve_open_loop(psvc, jobs, arr)
+            psvc.close()
+            plat_all = D.gather(plats)
+            latency["plain"] = {"p50_ms": 1000 * pct(plat_all, 50), "p99_ms": 1000 * pct(plat_all, 99),
+                                "max_ms": 1000 * max(plat_all), "wall_s": D.max(pwall),
+                                "mrays_s_wall": D.sum(prays) / D.max(pwall) / 1e6}
 
     cpu = None
     if not args.no_cpu and rank == 0:
         cpu = cpu_reference_sample(args.scale, os.cpu_count() or 1)
+        if cpu is not None:
+            gpu_same = gpu_on_cpu_sample(gscenes, specs)
+            for name, row in gpu_same.items():
+                cpu["per_scene"][name].update({"gpu_" + k: v for k, v in row.items()})
+            # the reference's rate on the served stream's own ray mix: the CPU
+            # time of each scene's rays in the timed steps at that scene's rate
+            cpu_s = sum(per_scene[k] / (cpu["per_scene"][sp.name]["mrays"] * 1e6)
+                        for k, sp in enumerate(specs) if per_scene[k] > 0)
+            cpu["stream_mix_mrays"] = float(per_scene.sum()) / cpu_s / 1e6 if cpu_s > 0 else None
     served.close()
 
     if rank == 0:

@@ -359,6 +359,28 @@ def ref_render(scn: str, integrator: str, width: int, height: int, spp: int = 1,
     return rec["xy"].copy(), rec["rgba"].copy(), stats
 
 
+def ref_bench(scn: str, integrator: str, width: int, height: int, spp: int, rdepth: int, threads: int, seed: int,
+              tiles, repeats: int, workdir: str = "/tmp"):
+    """The reference renderer as the timed CPU baseline: loads the scene once
+    (load and octree build timed on their own), then runs
+    IIntegrator::render `repeats` times over the same tiles.  Returns
+    {"load_s", "threads", "renders": [{"render_s", "rays"}, ...]}."""
+    import json
+    import tempfile
+    fd, tfile = tempfile.mkstemp(suffix=".txt", dir=workdir)
+    with os.fdopen(fd, "w") as fh:
+        fh.write("".join("%d %d %d %d\n" % tuple(t) for t in tiles))
+    env = dict(os.environ)
+    env["OMP_NUM_THREADS"] = str(threads)
+    cmd = [REF_BIN, "bench", scn, integrator, str(width), str(height), str(spp), str(rdepth), str(threads),
+           str(seed), tfile, str(repeats)]
+    r = subprocess.run(cmd, capture_output=True, text=True, env=env)
+    os.unlink(tfile)
+    if r.returncode != 0:
+        raise RuntimeError("xtref bench failed: %s %s" % (r.stdout, r.stderr))
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
 def ref_hits(scn: str, width: int, height: int, tiles=None, obj_path: str = None, workdir: str = "/tmp"):
     """Primary-ray closest hits through the reference's Scene::intersection, plus
     the triangle index from an Octree<Triangle> replica of the mesh."""

@@ -12,6 +12,10 @@
 //                [raygraph.ply|-] [distribution: 0 grid, 1 random]
 //   xtref hits   <scn> W H <tiles.txt|-> <out.bin> [mesh.obj]
 //   xtref kat    <in.txt> <out.txt>
+//   xtref bench  <scn> <integrator> W H spp rdepth threads seed <tiles.txt|-> repeats
+//                (the CPU baseline: the scene is loaded once, its load and
+//                octree build timed on their own, then IIntegrator::render runs
+//                `repeats` times over the same tiles, each timed)
 //
 // Two link-time hooks (-Wl,--wrap, no reference source is modified):
 //   * Scene::intersection is counted, so the ray count of a render is exact;
@@ -157,6 +161,22 @@ static int load_scene(xtcore::render::context_t &ctx, const char *scn)
     return 0;
 }
 
+static xtcore::render::IIntegrator *make_integrator(const std::string &integ, float ao_maxd)
+{
+    if (integ == "stencil") return new xtcore::integrator::stencil::Integrator();
+    if (integ == "depth") return new xtcore::integrator::depth::Integrator();
+    if (integ == "pathtracer") return new xtcore::integrator::pathtracer::Integrator();
+    if (integ == "normal") return new xtcore::integrator::normal::Integrator();
+    if (integ == "uv") return new xtcore::integrator::uv::Integrator();
+    if (integ == "emission") return new xtcore::integrator::emission::Integrator();
+    if (integ == "wireframe") return new xtcore::integrator::wireframe::Integrator();
+    if (integ == "ao") {
+        if (ao_maxd == 100.0f) return new xtcore::integrator::ao::Integrator();
+        return new AoWithDistance(ao_maxd);
+    }
+    return 0;
+}
+
 static int mode_render(int argc, char **argv)
 {
     if (argc < 13) return 2;
@@ -188,18 +208,7 @@ static int mode_render(int argc, char **argv)
         return 1;
     }
 
-    xtcore::render::IIntegrator *ig = 0;
-    if (integ == "stencil") ig = new xtcore::integrator::stencil::Integrator();
-    else if (integ == "depth") ig = new xtcore::integrator::depth::Integrator();
-    else if (integ == "pathtracer") ig = new xtcore::integrator::pathtracer::Integrator();
-    else if (integ == "normal") ig = new xtcore::integrator::normal::Integrator();
-    else if (integ == "uv") ig = new xtcore::integrator::uv::Integrator();
-    else if (integ == "emission") ig = new xtcore::integrator::emission::Integrator();
-    else if (integ == "wireframe") ig = new xtcore::integrator::wireframe::Integrator();
-    else if (integ == "ao") {
-        if (ao_maxd == 100.0f) ig = new xtcore::integrator::ao::Integrator();
-        else ig = new AoWithDistance(ao_maxd);
-    }
+    xtcore::render::IIntegrator *ig = make_integrator(integ, ao_maxd);
     if (!ig) { fprintf(stderr, "xtref: unknown integrator %s\n", integ.c_str()); return 1; }
 
     ig->setup(ctx);
@@ -615,10 +624,56 @@ static int mode_kat(int argc, char **argv)
     return 0;
 }
 
+static int mode_bench(int argc, char **argv)
+{
+    if (argc < 12) return 2;
+    const char *scn = argv[2];
+    std::string integ = argv[3];
+    size_t w = atol(argv[4]), h = atol(argv[5]), spp = atol(argv[6]);
+    size_t rdepth = atol(argv[7]), threads = atol(argv[8]);
+    g_fixed_time = (time_t)atoll(argv[9]);
+    const char *tiles_path = argv[10];
+    int repeats = atoi(argv[11]);
+    if (repeats < 1) return 2;
+
+    xtcore::init();
+    xtcore::render::context_t ctx;
+    auto l0 = std::chrono::steady_clock::now();
+    if (load_scene(ctx, scn)) return 1;
+    double load_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - l0).count();
+    HASH_UINT64 cam = ctx.params.camera;
+    ctx.params.width = w;
+    ctx.params.height = h;
+    ctx.params.samples = spp;
+    ctx.params.aa = 1;
+    ctx.params.rdepth = rdepth;
+    ctx.params.threads = threads;
+    ctx.params.camera = cam;
+    if (!read_tiles(tiles_path, w, h, ctx.tiles)) {
+        fprintf(stderr, "xtref: bad tiles %s\n", tiles_path);
+        return 1;
+    }
+    xtcore::render::IIntegrator *ig = make_integrator(integ, 100.0f);
+    if (!ig) { fprintf(stderr, "xtref: unknown integrator %s\n", integ.c_str()); return 1; }
+    ig->setup(ctx);
+    printf("{\"load_s\": %.9f, \"threads\": %d, \"renders\": [", load_s,
+           threads ? (int)threads : omp_get_max_threads());
+    for (int r = 0; r < repeats; ++r) {
+        g_rays = 0;
+        auto t0 = std::chrono::steady_clock::now();
+        ig->render();
+        double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        printf("%s{\"render_s\": %.9f, \"rays\": %llu}", r ? ", " : "", secs, (unsigned long long)g_rays.load());
+    }
+    printf("]}\n");
+    delete ig;
+    return 0;
+}
+
 int main(int argc, char **argv)
 {
     if (argc < 2) {
-        fprintf(stderr, "usage: xtref render|hits|kat ...\n");
+        fprintf(stderr, "usage: xtref render|hits|kat|bench ...\n");
         return 2;
     }
     std::string m = argv[1];
@@ -626,6 +681,7 @@ int main(int argc, char **argv)
     if (m == "render") rc = mode_render(argc, argv);
     else if (m == "hits") rc = mode_hits(argc, argv);
     else if (m == "kat") rc = mode_kat(argc, argv);
+    else if (m == "bench") rc = mode_bench(argc, argv);
     if (rc == 2) fprintf(stderr, "xtref: bad arguments\n");
     return rc;
 }

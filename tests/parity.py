@@ -155,8 +155,10 @@ def converged_rmse_bar(frames, truth, ref_rmse, label="", tol=1.05):
     frames: (k >= 2, npix, 4) frames under test at that spp (different seeds);
     truth: (npix, 4) the converged render; ref_rmse: the reference's own RMSE
     against the same truth, one per reference seed.  Asserts
-    * the mean RMSE of the frames <= tol x the largest reference RMSE (the
-      reference's RMSE varies by 2-3 % between seeds at these sizes);
+    * the mean RMSE of the frames <= (tol + 3 cv) x the largest reference
+      RMSE, where cv is the relative spread of the reference's RMSEs between
+      its seeds (at least 1 %): the noise estimate is itself a sample, whose
+      spread runs from 1-3 % on busy frames to 25 % where few pixels vary;
     * per channel, the frames' mean minus the truth's mean within 4.5 standard
       errors (from the per-pixel variance between the frames).
     Prints and returns (mean RMSE, reference RMSEs)."""
@@ -166,9 +168,11 @@ def converged_rmse_bar(frames, truth, ref_rmse, label="", tol=1.05):
     assert k >= 2
     got = [rmse(F[i], T) for i in range(k)]
     ref = [float(x) for x in np.asarray(ref_rmse).ravel()]
-    print("[%s] RMSE vs 4096-spp: frames %s, reference %s, ratio %.3f (bar %.2f x max)" %
-          (label, np.round(got, 5), np.round(ref, 5), np.mean(got) / max(ref), tol))
-    assert np.mean(got) <= tol * max(ref), (got, ref)
+    cv = max(0.01, float(np.std(ref, ddof=1) / np.mean(ref))) if len(ref) > 1 else 0.01
+    bar = tol + 3.0 * cv
+    print("[%s] RMSE vs 4096-spp: frames %s, reference %s, ratio %.3f (bar %.3f x max)" %
+          (label, np.round(got, 5), np.round(ref, 5), np.mean(got) / max(ref), bar))
+    assert np.mean(got) <= bar * max(ref), (got, ref, bar)
     for ch in range(3):
         se = np.sqrt(F[:, :, ch].var(0, ddof=1).mean() / npix / k)
         bias = F[:, :, ch].mean() - T[:, ch].mean()

@@ -155,3 +155,73 @@ def test_scene_tuning_reports_the_built_tree(resident):
     finally:
         sc.set_tuning(**keep)
     assert np.array_equal(ref, got)
+
+
+def test_live_submissions_join_waves_in_flight(resident):
+    """Continuous batching with live arrivals: while one thread serves
+    (xtgpu_service_run on an open service, GIL released), another submits jobs
+    as waves of a long job are on the GPU.  They are admitted before that job
+    finishes, so their paths share its waves, and each renders the same bits
+    as alone; the run returns once the service is closed and drained."""
+    import threading
+    import time
+    fmt = xtgpu.NODES_W8
+    long_job = (1, xtgpu.PATHTRACER, 512, 512, 32, 4, 100.0, 21)   # 8 Mi paths: 256 waves of 2^15
+    later = [(0, xtgpu.PATHTRACER, 64, 48, 8, 4, 100.0, 22), (2, xtgpu.AO, 48, 48, 8, 2, 0.2, 23),
+             (1, xtgpu.DEPTH, 40, 30, 2, 1, 100.0, 24), (0, xtgpu.PATHTRACER, 96, 64, 4, 4, 100.0, 25),
+             (2, xtgpu.PATHTRACER, 32, 32, 16, 4, 100.0, 26), (1, xtgpu.STENCIL, 33, 17, 3, 1, 100.0, 27)]
+    alone = [resident[s].render(integ, w, h, spp=spp, rdepth=d, ao_max_distance=md, seed=seed, node_format=fmt)[0]
+             for (s, integ, w, h, spp, d, md, seed) in [long_job] + later]
+    svc = Service(resident, node_format=fmt, wave_paths=1 << 15, use_graphs=True, merge_jobs=True,
+                  memory_budget=1 << 30, waves_in_flight=3)
+    svc.open(True)
+    errors = []
+
+    def serve():
+        try:
+            svc.run(max_seconds=120.0)
+        except Exception as e:   # reported on the main thread
+            errors.append(e)
+
+    th = threading.Thread(target=serve)
+    th.start()
+    j0 = svc.submit(*long_job)
+    t = time.time()
+    while svc.poll(j0).state != 1 and time.time() - t < 30:
+        time.sleep(0.0005)
+    ids = []
+    for j in later:
+        ids.append(svc.submit(*j))
+        time.sleep(0.002)
+    svc.open(False)
+    th.join(timeout=120)
+    assert not th.is_alive() and not errors, errors
+    s0 = svc.poll(j0)
+    assert s0.state == 2
+    starts = [svc.poll(i).start_s for i in ids]
+    print("[live] long job done at %.3fs; later jobs admitted at %s" % (s0.render_done_s, np.round(starts, 3)))
+    assert sum(s < s0.render_done_s for s in starts) >= 3, (starts, s0.render_done_s)
+    for jid, ref in zip([j0] + ids, alone):
+        st = svc.poll(jid)
+        assert st.state == 2 and st.start_s >= st.submit_s - 1e-6
+        assert np.array_equal(svc.result(jid), ref), "job %d" % jid
+        svc.release(jid)
+    svc.close()
+
+
+def test_run_while_running_is_refused(resident):
+    """One thread at a time runs the service."""
+    import threading
+    import time
+    svc = Service(resident, node_format=xtgpu.NODES_W8, merge_jobs=True)
+    svc.open(True)
+    th = threading.Thread(target=lambda: svc.run(max_seconds=30.0))
+    th.start()
+    time.sleep(0.2)
+    with pytest.raises(xtgpu.XtgpuError) as e:
+        svc.run()
+    assert e.value.status == 7   # XTGPU_ERR_STATE
+    svc.open(False)
+    th.join(timeout=60)
+    assert not th.is_alive()
+    svc.close()

@@ -264,7 +264,17 @@ static xtgpu_status check_shading(const xtgpu_scene_desc *d, const std::string &
 // Uploads a description's materials (with their samplers), textures, object
 // materials, texture-coordinate inputs and environment into new device
 // buffers, then swaps them in: the scene's geometry and BVH are untouched.
-static xtgpu_status upload_shading(xtgpu_scene *sc, const xtgpu_scene_desc *d, cudaStream_t s)
+// material of every primitive id, so that shading reads one table entry per
+// hit instead of going through the primitive's object (Scene::get_material,
+// scene.cc:55-61, keyed by the hit record's object)
+__global__ void k_prim_material(int64_t n, const int32_t *__restrict__ prim_obj,
+                                const int32_t *__restrict__ obj_material, int32_t *__restrict__ prim_mat)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        prim_mat[i] = obj_material[prim_obj[i]];
+}
+
+static xtgpu_status upload_shading(xtgpu_scene *sc, const xtgpu_scene_desc *d, int64_t nprim, cudaStream_t s)
 {
     std::vector<DevMaterial> mats((size_t)std::max(1, d->n_materials));
     for (int32_t i = 0; i < d->n_materials; ++i) {
@@ -335,14 +345,28 @@ static xtgpu_status upload_shading(xtgpu_scene *sc, const xtgpu_scene_desc *d, c
     if (e == cudaSuccess && d->n_texels)
         e = cudaMemcpy(nx.p, d->texels, sizeof(float4) * (size_t)d->n_texels, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return drop(cuda_fail(e, "cudaMemcpy", __FILE__, __LINE__));
+    HostBuf npm;
+    if ((st = dalloc(npm, sizeof(int32_t) * (size_t)std::max<int64_t>(1, nprim), s)) != XTGPU_OK) return drop(st);
+    if (nprim > 0) {
+        k_prim_material<<<(int)std::min<int64_t>((nprim + 255) / 256, 4096), 256, 0, s>>>(
+            nprim, (const int32_t *)sc->prim_obj.p, (const int32_t *)no.p, (int32_t *)npm.p);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            dfree(npm);
+            return drop(cuda_fail(e, "k_prim_material", __FILE__, __LINE__));
+        }
+    }
     std::swap(sc->materials, nm);
     std::swap(sc->obj_material, no);
+    std::swap(sc->prim_mat, npm);
     std::swap(sc->textures, nt);
     std::swap(sc->texels, nx);
     std::swap(sc->obj_uvs, nu);
     std::swap(sc->tri_uv, nv);
-    dfree(nm); dfree(no); dfree(nt); dfree(nx); dfree(nu); dfree(nv);   // the previous buffers
+    dfree(nm); dfree(no); dfree(npm); dfree(nt); dfree(nx); dfree(nu); dfree(nv);   // the previous buffers
     DevScene &S = sc->dev;
+    S.prim_mat = (const int32_t *)sc->prim_mat.p;
     S.obj_uvs = (const float2 *)sc->obj_uvs.p;
     S.tri_uv = (const float2 *)sc->tri_uv.p;
     S.materials = (const DevMaterial *)sc->materials.p;
@@ -442,7 +466,7 @@ xtgpu_status xtgpu_scene_create(const xtgpu_scene_desc *d, void *stream, xtgpu_s
     if (cudaMemcpy(sc->prim_obj.p, prim_obj.data(), sizeof(int32_t) * prim_obj.size(), cudaMemcpyHostToDevice) !=
         cudaSuccess)
         return fail(cuda_fail(cudaGetLastError(), "cudaMemcpy", __FILE__, __LINE__));
-    if ((st = upload_shading(sc, d, s)) != XTGPU_OK) return fail(st);
+    if ((st = upload_shading(sc, d, nprim, s)) != XTGPU_OK) return fail(st);
 
     DevScene &S = sc->dev;
     S.tri_v = (const float4 *)sc->tri_v.p;
@@ -486,7 +510,8 @@ xtgpu_status xtgpu_scene_update(xtgpu_scene *sc, const xtgpu_scene_desc *d, int3
     }
     // renders read the buffers being replaced: let those on this stream finish
     XTG_CUDA(cudaStreamSynchronize(s));
-    if (what & XTGPU_UPDATE_SHADING) XTG_TRY(upload_shading(sc, d, s));
+    if (what & XTGPU_UPDATE_SHADING)
+        XTG_TRY(upload_shading(sc, d, (int64_t)sc->dev.n_tris + sc->dev.n_spheres + sc->dev.n_planes, s));
     if (what & XTGPU_UPDATE_CAMERA) sc->dev.cam = make_camera(d->camera);
     return XTGPU_OK;
 }
@@ -515,7 +540,7 @@ xtgpu_status xtgpu_scene_destroy(xtgpu_scene *sc)
 {
     if (!sc) return XTGPU_OK;
     for (HostBuf *b : {&sc->tri_v, &sc->tri_n, &sc->spheres, &sc->planes, &sc->prim_obj, &sc->obj_material,
-                       &sc->obj_uvs, &sc->tri_uv, &sc->materials, &sc->textures, &sc->texels, &sc->leaf_prims, &sc->nodes32, &sc->nodes8, &sc->nodesW, &sc->leafW,
+                       &sc->prim_mat, &sc->obj_uvs, &sc->tri_uv, &sc->materials, &sc->textures, &sc->texels, &sc->leaf_prims, &sc->nodes32, &sc->nodes8, &sc->nodesW, &sc->leafW,
                        &sc->morton, &sc->order, &sc->left, &sc->right})
         dfree(*b);
     delete sc;
@@ -530,7 +555,7 @@ xtgpu_status xtgpu_scene_device_bytes(const xtgpu_scene *sc, uint64_t *bytes)
     }
     uint64_t b = 0;
     for (const HostBuf *h : {&sc->tri_v, &sc->tri_n, &sc->spheres, &sc->planes, &sc->prim_obj, &sc->obj_material,
-                             &sc->obj_uvs, &sc->tri_uv, &sc->materials, &sc->textures, &sc->texels, &sc->leaf_prims, &sc->nodes32, &sc->nodes8, &sc->nodesW, &sc->leafW,
+                             &sc->prim_mat, &sc->obj_uvs, &sc->tri_uv, &sc->materials, &sc->textures, &sc->texels, &sc->leaf_prims, &sc->nodes32, &sc->nodes8, &sc->nodesW, &sc->leafW,
                              &sc->morton, &sc->order, &sc->left, &sc->right})
         b += h->bytes;
     *bytes = b;

@@ -245,10 +245,9 @@ __device__ __forceinline__ void dcross3(const double a[3], const double b[3], do
     r[1] = __dsub_rn(__dmul_rn(a[2], b[0]), __dmul_rn(a[0], b[2]));
     r[2] = __dsub_rn(__dmul_rn(a[0], b[1]), __dmul_rn(a[1], b[0]));
 }
-__device__ __noinline__ bool s_lobe(float3 nf, float3 df, float e, bool twice, uint64_t key, uint32_t &ctr, float3 &out,
-                       double3 &raw)
+__device__ __forceinline__ bool s_lobe(const double n[3], const double d[3], float e, bool twice, uint64_t key,
+                                       uint32_t &ctr, float3 &out, double3 &raw)
 {
-    const double n[3] = {nf.x, nf.y, nf.z}, d[3] = {df.x, df.y, df.z};
     double i[3] = {d[0], d[1], d[2]}, nn[3] = {n[0], n[1], n[2]};
     dnormalize3(i);
     dnormalize3(nn);
@@ -313,6 +312,59 @@ __device__ __forceinline__ float3 hit_normal(const DevScene &S, uint32_t prim, f
         return make_float3((p.x - s.x) / s.w, (p.y - s.y) / s.w, (p.z - s.z) / s.w);
     }
     return f3(S.planes[prim - S.n_tris - S.n_spheres]);
+}
+
+// The hit record's normal in FP64, as the reference forms it from its FP64 hit
+// point: triangles the face normal normalised in FP64 from the float vertices
+// (Triangle::calc_normal, triangle.cc:142-147), or the barycentric blend of the
+// vertex normals when it is not zero; spheres (o + d t - c) / r
+// (sphere.cc:52); planes the stored normal.  The FP32 normal's own rounding
+// (a few 1e-8 in its length) would decide sample::lobe's 1 - d.n <= 1e-8 test
+// for head-on hits differently from the reference.
+__device__ void hit_normal_d(const DevScene &S, uint32_t prim, float3 o, float3 d, float t, float bu, float bv,
+                             double n[3])
+{
+    if ((int)prim < S.n_tris) {
+        const float4 a = S.tri_v[3 * prim], b = S.tri_v[3 * prim + 1], c = S.tri_v[3 * prim + 2];
+        const double e1[3] = {__dsub_rn(b.x, a.x), __dsub_rn(b.y, a.y), __dsub_rn(b.z, a.z)};
+        const double e2[3] = {__dsub_rn(c.x, a.x), __dsub_rn(c.y, a.y), __dsub_rn(c.z, a.z)};
+        dcross3(e1, e2, n);
+        dnormalize3(n);
+        if (S.tri_n) {
+            const double w0 = 1.0 - (double)bu - (double)bv;
+            const float4 na = S.tri_n[3 * prim], nb = S.tri_n[3 * prim + 1], nc = S.tri_n[3 * prim + 2];
+            const double pn[3] = {__dadd_rn(__dadd_rn(__dmul_rn(na.x, w0), __dmul_rn(nb.x, bu)), __dmul_rn(nc.x, bv)),
+                                  __dadd_rn(__dadd_rn(__dmul_rn(na.y, w0), __dmul_rn(nb.y, bu)), __dmul_rn(nc.y, bv)),
+                                  __dadd_rn(__dadd_rn(__dmul_rn(na.z, w0), __dmul_rn(nb.z, bu)), __dmul_rn(nc.z, bv))};
+            if (dlen3(pn) != 0.0) {
+                n[0] = pn[0]; n[1] = pn[1]; n[2] = pn[2];
+            }
+        }
+        return;
+    }
+    if ((int)prim < S.n_tris + S.n_spheres) {
+        const float4 c = S.spheres[prim - S.n_tris];
+        n[0] = __ddiv_rn(__dsub_rn(__dadd_rn(o.x, __dmul_rn(d.x, t)), c.x), c.w);
+        n[1] = __ddiv_rn(__dsub_rn(__dadd_rn(o.y, __dmul_rn(d.y, t)), c.y), c.w);
+        n[2] = __ddiv_rn(__dsub_rn(__dadd_rn(o.z, __dmul_rn(d.z, t)), c.z), c.w);
+        return;
+    }
+    const float4 pl = S.planes[prim - S.n_tris - S.n_spheres];
+    n[0] = pl.x; n[1] = pl.y; n[2] = pl.z;
+}
+
+// The specular branch of Phong / BlinnPhong::sample_path (phong.cc:48-52,
+// blinnphong.cc:52-56): sample::lobe around the reflection of the incident
+// direction, with the hit normal in FP64 and the ray's direction normalised in
+// FP64 (the reference's is a normalised double).  Kept out of line: it is the
+// only FP64 vector work of the shade kernel.
+__device__ __noinline__ bool phong_lobe(const DevScene &S, const xtgpu_hit &h, float3 o, float3 d, float e, bool twice,
+                                        uint64_t key, uint32_t &ctr, float3 &out, double3 &raw)
+{
+    double n[3], dir[3] = {-(double)d.x, -(double)d.y, -(double)d.z};
+    hit_normal_d(S, h.prim, o, d, h.t, h.u, h.v, n);
+    dnormalize3(dir);
+    return s_lobe(n, dir, e, twice, key, ctr, out, raw);
 }
 
 // hit_record_t::texcoord as the reference forms it: triangles interpolate
@@ -1072,7 +1124,7 @@ __global__ void __launch_bounds__(256, 4) k_shade(const DevJob *__restrict__ job
             case XTGPU_EMISSION: {  // the hit material's emissive colour (emission/integrator.cc:27-33)
                 float3 e = make_float3(0.f, 0.f, 0.f);
                 if (hit) {
-                    const DevMaterial &M = S.materials[S.obj_material[S.prim_obj[h.prim]]];
+                    const DevMaterial &M = S.materials[S.prim_mat[h.prim]];
                     e = mat_color(S, M, 2, h, o, d);
                 }
                 q.contrib[lp] = make_float4(e.x, e.y, e.z, hit ? 1.f : 0.f);
@@ -1124,7 +1176,7 @@ __global__ void __launch_bounds__(256, 4) k_shade(const DevJob *__restrict__ job
                 }
                 float3 p = o + d * h.t;
                 float3 nrm = hit_normal(S, h.prim, p, h.u, h.v);
-                const DevMaterial &M = S.materials[S.obj_material[S.prim_obj[h.prim]]];
+                const DevMaterial &M = S.materials[S.prim_mat[h.prim]];
                 float3 f, nd3;
                 double3 lobe_raw = make_double3(0.0, 0.0, 0.0);
                 bool go = true, aimed = true;
@@ -1138,8 +1190,8 @@ __global__ void __launch_bounds__(256, 4) k_shade(const DevJob *__restrict__ job
                         nd3 = s_diffuse(nrm, key, ctr);
                     } else {
                         f = mat_color(S, M, 1, h, o, d);
-                        aimed = s_lobe(nrm, make_float3(-d.x, -d.y, -d.z), M.exponent, M.type == XTGPU_BLINNPHONG,
-                                       key, ctr, nd3, lobe_raw);
+                        aimed = phong_lobe(S, h, o, d, M.exponent, M.type == XTGPU_BLINNPHONG, key, ctr, nd3,
+                                           lobe_raw);
                     }
                 } else if (M.type == XTGPU_EMISSIVE) {
                     float3 L = cmul(Pp, cmul(Ii, mat_color(S, M, 2, h, o, d)));

@@ -14,11 +14,20 @@
 //
 // Because paths are keyed by (seed, pixel, sample) and folded per pixel in
 // sample order, a job's frame is bit-identical whatever it is merged with.
+//
+// Threads: xtgpu_service_run runs the loop on the calling thread.  Other
+// threads may submit, poll, read results, release jobs and open or close the
+// service meanwhile: those calls and the loop's bookkeeping share one mutex,
+// which the loop drops while it waits for a wave or for arrivals, and a
+// submission wakes the loop.  A job submitted while waves are in flight is
+// admitted as slots and memory free up and joins the next wave launched.
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
 #include <cstring>
 #include <deque>
 #include <map>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -82,6 +91,12 @@ struct xtgpu_service {
     std::multimap<uint64_t, float4 *> pinned_free;
     std::vector<cudaEvent_t> events_free;
     std::vector<int64_t> copying;    // finished on the GPU, host copy in flight
+    // the job table and everything above it that submit, poll, result and
+    // release touch; run() holds it except while it waits
+    std::mutex mu;
+    std::condition_variable arrived;  // a submission or xtgpu_service_open
+    bool open = false;                // run() waits for submissions while set
+    bool running = false;             // one run() at a time
 
     double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
 };
@@ -446,16 +461,20 @@ xtgpu_status xtgpu_service_submit(xtgpu_service *v, const xtgpu_job_desc *d, dou
     }
     SvcJob J;
     J.d = *d;
-    J.submit_s = submit_s >= 0 ? submit_s : v->now();
     J.paths = paths;
     J.frame_bytes = sizeof(float4) * (uint64_t)d->width * d->height;
-    int64_t jid = v->next_id++;
-    // keep the pending queue ordered by arrival time (stable for equal times)
-    auto it = v->pending.end();
-    while (it != v->pending.begin() && v->jobs[*(it - 1)].submit_s > J.submit_s) --it;
-    v->jobs[jid] = J;
-    v->pending.insert(it, jid);
-    *id = jid;
+    {
+        std::lock_guard<std::mutex> lock(v->mu);
+        J.submit_s = submit_s >= 0 ? submit_s : v->now();
+        int64_t jid = v->next_id++;
+        // keep the pending queue ordered by arrival time (stable for equal times)
+        auto it = v->pending.end();
+        while (it != v->pending.begin() && v->jobs[*(it - 1)].submit_s > J.submit_s) --it;
+        v->jobs[jid] = J;
+        v->pending.insert(it, jid);
+        *id = jid;
+    }
+    v->arrived.notify_all();
     return XTGPU_OK;
 }
 
@@ -465,6 +484,7 @@ namespace {
 
 static xtgpu_status run_loop(xtgpu_service *v, double max_seconds)
 {
+    std::unique_lock<std::mutex> lk(v->mu);
     const double t_end = max_seconds > 0 ? v->now() + max_seconds : 1e300;
     // slots in flight, oldest first; `last` is the most recently launched one,
     // whose accumulate the next wave's accumulate waits for
@@ -493,10 +513,16 @@ static xtgpu_status run_loop(xtgpu_service *v, double max_seconds)
             last = k;
             continue;
         }
-        // 2. retire the oldest wave in flight
+        // 2. retire the oldest wave in flight; other threads may submit, poll
+        //    and release while the loop waits for it
         if (!flight.empty()) {
             WaveSlot &W = v->slot[flight.front()];
             flight.pop_front();
+            cudaEvent_t fin = W.fin;
+            lk.unlock();
+            cudaError_t e = cudaEventSynchronize(fin);
+            lk.lock();
+            if (e != cudaSuccess) return cuda_fail(e, "xtgpu_service_run: wave", __FILE__, __LINE__);
             XTG_TRY(retire_wave(v, W));
             XTG_TRY(finish_copies(v, false));
             if (v->now() >= t_end) out_of_time = true;
@@ -509,12 +535,19 @@ static xtgpu_status run_loop(xtgpu_service *v, double max_seconds)
             set_error("xtgpu_service_run: inconsistent job state");
             return XTGPU_ERR_STATE;
         }
-        if (v->pending.empty()) return XTGPU_OK;
+        if (v->pending.empty()) {
+            if (!v->open) return XTGPU_OK;
+            // open: wait for a submission or for the service to close
+            if (now >= t_end) return XTGPU_ERR_TIMEOUT;
+            XTG_TRY(finish_copies(v, false));
+            v->arrived.wait_for(lk, std::chrono::duration<double>(std::min(t_end - now, 0.01)));
+            continue;
+        }
         double next = v->jobs[v->pending.front()].submit_s;
         if (next > now) {
             if (now >= t_end) return XTGPU_ERR_TIMEOUT;
             double dt = std::min(next, t_end) - now;
-            std::this_thread::sleep_for(std::chrono::duration<double>(std::min(dt, 0.01)));
+            v->arrived.wait_for(lk, std::chrono::duration<double>(std::min(dt, 0.01)));
             continue;
         }
         // the head job does not fit yet and nothing runs: cannot happen
@@ -538,10 +571,34 @@ xtgpu_status xtgpu_service_run(xtgpu_service *v, double max_seconds)
         set_error("xtgpu_service_run: no scene");
         return XTGPU_ERR_STATE;
     }
+    {
+        std::lock_guard<std::mutex> lock(v->mu);
+        if (v->running) {
+            set_error("xtgpu_service_run: already running on another thread");
+            return XTGPU_ERR_STATE;
+        }
+        v->running = true;
+    }
     xtgpu_status st = run_loop(v, max_seconds);
+    std::lock_guard<std::mutex> lock(v->mu);
     // host copies of finished frames still in flight land before returning
     xtgpu_status cst = finish_copies(v, true);
+    v->running = false;
     return st != XTGPU_OK ? st : cst;
+}
+
+xtgpu_status xtgpu_service_open(xtgpu_service *v, int32_t open)
+{
+    if (!v) {
+        set_error("xtgpu_service_open: NULL service");
+        return XTGPU_ERR_INVALID;
+    }
+    {
+        std::lock_guard<std::mutex> lock(v->mu);
+        v->open = open != 0;
+    }
+    v->arrived.notify_all();
+    return XTGPU_OK;
 }
 
 xtgpu_status xtgpu_service_poll(xtgpu_service *v, int64_t id, xtgpu_job_status *st)
@@ -550,6 +607,7 @@ xtgpu_status xtgpu_service_poll(xtgpu_service *v, int64_t id, xtgpu_job_status *
         set_error("xtgpu_service_poll: NULL argument");
         return XTGPU_ERR_INVALID;
     }
+    std::lock_guard<std::mutex> lock(v->mu);
     auto it = v->jobs.find(id);
     if (it == v->jobs.end()) {
         set_error("xtgpu_service_poll: unknown job");
@@ -571,21 +629,29 @@ xtgpu_status xtgpu_service_result(xtgpu_service *v, int64_t id, float *rgba)
         set_error("xtgpu_service_result: NULL argument");
         return XTGPU_ERR_INVALID;
     }
-    auto it = v->jobs.find(id);
-    if (it == v->jobs.end()) {
-        set_error("xtgpu_service_result: unknown job");
-        return XTGPU_ERR_NOT_FOUND;
+    const float4 *frame = nullptr;
+    uint64_t bytes = 0;
+    {
+        std::lock_guard<std::mutex> lock(v->mu);
+        auto it = v->jobs.find(id);
+        if (it == v->jobs.end()) {
+            set_error("xtgpu_service_result: unknown job");
+            return XTGPU_ERR_NOT_FOUND;
+        }
+        SvcJob &J = it->second;
+        if (J.state == 2 && J.host) {
+            memcpy(rgba, J.host, J.frame_bytes);
+            return XTGPU_OK;
+        }
+        if (J.state != 2 || !J.frame) {
+            set_error("xtgpu_service_result: job not finished or released");
+            return XTGPU_ERR_STATE;
+        }
+        frame = J.frame;
+        bytes = J.frame_bytes;
     }
-    SvcJob &J = it->second;
-    if (J.state == 2 && J.host) {
-        memcpy(rgba, J.host, J.frame_bytes);
-        return XTGPU_OK;
-    }
-    if (J.state != 2 || !J.frame) {
-        set_error("xtgpu_service_result: job not finished or released");
-        return XTGPU_ERR_STATE;
-    }
-    XTG_CUDA(cudaMemcpyAsync(rgba, J.frame, J.frame_bytes, cudaMemcpyDeviceToHost, v->s));
+    // the frame stays until this job is released (by the caller)
+    XTG_CUDA(cudaMemcpyAsync(rgba, frame, bytes, cudaMemcpyDeviceToHost, v->s));
     XTG_CUDA(cudaStreamSynchronize(v->s));
     return XTGPU_OK;
 }
@@ -596,6 +662,7 @@ xtgpu_status xtgpu_service_result_host(xtgpu_service *v, int64_t id, const float
         set_error("xtgpu_service_result_host: NULL argument");
         return XTGPU_ERR_INVALID;
     }
+    std::lock_guard<std::mutex> lock(v->mu);
     auto it = v->jobs.find(id);
     if (it == v->jobs.end()) {
         set_error("xtgpu_service_result_host: unknown job");
@@ -616,6 +683,7 @@ xtgpu_status xtgpu_service_release(xtgpu_service *v, int64_t id)
         set_error("xtgpu_service_release: NULL service");
         return XTGPU_ERR_INVALID;
     }
+    std::lock_guard<std::mutex> lock(v->mu);
     auto it = v->jobs.find(id);
     if (it == v->jobs.end()) {
         set_error("xtgpu_service_release: unknown job");
@@ -644,6 +712,7 @@ xtgpu_status xtgpu_service_get_stats(xtgpu_service *v, xtgpu_service_stats *st)
         set_error("xtgpu_service_get_stats: NULL argument");
         return XTGPU_ERR_INVALID;
     }
+    std::lock_guard<std::mutex> lock(v->mu);
     *st = xtgpu_service_stats{};
     for (int k = 0; k < v->nslots; ++k) {
         WaveRunner &R = v->slot[k].R;

@@ -81,6 +81,7 @@ struct DevScene {
     const float4 *planes;      // (n, offset)
     const int32_t *prim_obj;   // object of each primitive id (tris, spheres, planes)
     const int32_t *obj_material;
+    const int32_t *prim_mat;   // material of each primitive id (obj_material[prim_obj[i]])
     const DevMaterial *materials;
     const float2 *obj_uvs;     // per object: the surface's (u_scale, v_scale)
     const float2 *tri_uv;      // 3 per triangle, or nullptr (constructor defaults)
@@ -112,7 +113,7 @@ struct HostBuf {
 
 struct xtgpu_scene {
     xtg::DevScene dev{};
-    xtg::HostBuf tri_v, tri_n, spheres, planes, prim_obj, obj_material, materials, obj_uvs, tri_uv;
+    xtg::HostBuf tri_v, tri_n, spheres, planes, prim_obj, obj_material, prim_mat, materials, obj_uvs, tri_uv;
     xtg::HostBuf textures, texels;
     xtg::HostBuf leaf_prims, nodes32, nodes8, nodesW, leafW;
     xtg::HostBuf morton, order, left, right;   // kept for xtgpu_bvh_export

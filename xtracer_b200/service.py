@@ -43,7 +43,15 @@ class Service:
         return jid.value
 
     def run(self, max_seconds: float = 0.0) -> None:
+        """Serves until the submitted jobs are done (xtgpu_service_run).  The
+        call releases the GIL, so other Python threads may submit, poll and
+        release meanwhile; while the service is open it waits for them."""
         check(lib().xtgpu_service_run(self.handle, max_seconds))
+
+    def open(self, on: bool = True) -> None:
+        """Opens (or closes) the service to live submissions: an open service's
+        run() waits for new jobs instead of returning when idle."""
+        check(lib().xtgpu_service_open(self.handle, int(on)))
 
     def poll(self, jid: int) -> xtgpu.JobStatus:
         st = xtgpu.JobStatus()

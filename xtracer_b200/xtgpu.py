@@ -170,6 +170,7 @@ SIGNATURES = {
     "xtgpu_service_add_scene": [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)],
     "xtgpu_service_submit": [C.c_void_p, C.POINTER(JobDesc), C.c_double, C.POINTER(C.c_int64)],
     "xtgpu_service_run": [C.c_void_p, C.c_double],
+    "xtgpu_service_open": [C.c_void_p, C.c_int32],
     "xtgpu_service_poll": [C.c_void_p, C.c_int64, C.POINTER(JobStatus)],
     "xtgpu_service_result": [C.c_void_p, C.c_int64, C.c_void_p],
     "xtgpu_service_result_host": [C.c_void_p, C.c_int64, C.POINTER(C.POINTER(C.c_float))],
