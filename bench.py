@@ -545,11 +545,22 @@ def main():
         lats, lrays, lwall = serve_open_loop(lsvc, jobs, arr)
         lsvc.close()
         lat_all_open = D.gather(lats)
+        # the same arrivals with waves shared equally between the running jobs
+        # (policy 1) instead of fewest remaining paths first
+        esvc = Service(gscenes, node_format=SERVED_FORMAT, use_graphs=True, merge_jobs=True, memory_budget=budget,
+                       waves_in_flight=WAVES_IN_FLIGHT, stream=stream, policy=1)
+        run_slice(esvc, slices[0])
+        elats, erays, ewall = serve_open_loop(esvc, jobs, arr)
+        esvc.close()
+        elat_all = D.gather(elats)
         latency = {"arrivals": "Poisson, %.2f jobs/s (1.5x the plain path's job rate), submitted live" % rate,
                    "jobs": len(lat_all_open), "p50_ms": 1000 * pct(lat_all_open, 50),
                    "p99_ms": 1000 * pct(lat_all_open, 99), "max_ms": 1000 * max(lat_all_open),
                    "mrays_s_wall": D.sum(lrays) / D.max(lwall) / 1e6, "wall_s": D.max(lwall),
-                   "memory_budget_gb": budget / 2 ** 30}
+                   "memory_budget_gb": budget / 2 ** 30, "policy": "fewest remaining paths first",
+                   "equal_share": {"p50_ms": 1000 * pct(elat_all, 50), "p99_ms": 1000 * pct(elat_all, 99),
+                                   "max_ms": 1000 * max(elat_all), "wall_s": D.max(ewall),
+                                   "mrays_s_wall": D.sum(erays) / D.max(ewall) / 1e6}}
         if plain is not None:
             psvc = Service(gscenes, node_format=xtgpu.NODES_FP32, use_graphs=False, merge_jobs=False,
                            memory_budget=budget, waves_in_flight=1, stream=stream)

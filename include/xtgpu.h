@@ -425,6 +425,11 @@ typedef struct {
     int32_t bvh_builder;           /* hierarchy over the Morton order: 0 = LBVH (Karras radix
                                       splits), 1 = PLOC agglomerative clustering (Meister and
                                       Bittner 2018; a lower-cost tree, same closest hits) */
+    int32_t wide_collapse;         /* 8-wide nodes from the binary tree: 1 = cost-optimal
+                                      (surface-area costs by dynamic programming, subtrees of
+                                      up to 3 primitives as leaves; Ylitie, Karras and Laine
+                                      2017), 0 = greedy largest-area opening */
+    float wide_prim_cost;          /* that cost of a primitive test, in node visits (0 = 0.3) */
 } xtgpu_tuning;
 XTGPU_API xtgpu_status xtgpu_get_tuning(xtgpu_tuning *t);
 XTGPU_API xtgpu_status xtgpu_set_tuning(const xtgpu_tuning *t);

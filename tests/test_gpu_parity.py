@@ -244,16 +244,25 @@ def test_q8_hits_equal_fp32(name):
 
 @pytest.mark.parametrize("name", ["spheres64", "terrain20k", "hairball20k", "dup", "tiny1", "tiny2", "tiny3"])
 @pytest.mark.parametrize("leaf", [1, 2, 3])
-def test_w8_hits_equal_fp32(name, leaf):
-    """The 8-wide quantised BVH finds the same closest hits as the binary FP32
-    BVH, bit for bit: conservative boxes, the same primitive tests, and ties
-    broken by primitive id whatever the visiting order."""
+@pytest.mark.parametrize("collapse", [0, 1])
+def test_w8_hits_equal_fp32(name, leaf, collapse):
+    """The 8-wide quantised BVH, collapsed greedily (0) or by surface-area
+    cost with subtrees of up to 3 primitives as leaves (1), finds the same
+    closest hits as the binary FP32 BVH, bit for bit: conservative boxes, the
+    same primitive tests, and ties broken by primitive id whatever the visiting
+    order."""
     if name in small_scenes():
         spec, w, h = small_scenes()[name]
     else:
         spec = duplicate_scene() if name == "dup" else tiny_scene(int(name[-1]))
         w, h = 48, 32
-    sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_W8), leaf_size=leaf)
+    keep = xtgpu.get_tuning().wide_collapse
+    try:
+        xtgpu.set_tuning(wide_collapse=collapse)
+        sc = xtgpu.Scene(spec, node_formats=(xtgpu.NODES_FP32, xtgpu.NODES_W8), leaf_size=leaf)
+    finally:
+        xtgpu.set_tuning(wide_collapse=keep)
+    assert sc.tuning().wide_collapse == collapse
     info = sc.bvh_export()["info"]
     assert info.node_bytes_w8 > 0 and info.depth_w8 >= 1
     org, dirs, a = gpu_primary(spec, w, h, xtgpu.NODES_FP32, sc)

@@ -175,6 +175,10 @@ xtgpu_status xtgpu_scene_tuning(const xtgpu_scene *sc, xtgpu_tuning *t)
         t->leaf_size = sc->leaf_size;
         t->bvh_builder = sc->builder;
     }
+    if (sc->builtW) {
+        t->wide_collapse = sc->wide_collapse;
+        t->wide_prim_cost = sc->wide_prim_cost;
+    }
     return XTGPU_OK;
 }
 
@@ -189,7 +193,8 @@ static bool tuning_valid(const xtgpu_tuning *t)
            t->refill_threshold <= 32 &&
            (t->extend_min_blocks == 0 || t->extend_min_blocks == 8 || t->extend_min_blocks == 10) &&
            (t->stack_entries == 0 || t->stack_entries == 32 || t->stack_entries == 64) && t->bvh_builder >= 0 &&
-           t->bvh_builder <= 1;
+           t->bvh_builder <= 1 && t->wide_collapse >= 0 && t->wide_collapse <= 1 && t->wide_prim_cost >= 0.f &&
+           t->wide_prim_cost <= 100.f;
 }
 
 xtgpu_status xtgpu_set_tuning(const xtgpu_tuning *t)
@@ -208,8 +213,10 @@ xtgpu_status xtgpu_scene_set_tuning(xtgpu_scene *sc, const xtgpu_tuning *t)
         set_error("xtgpu_scene_set_tuning: NULL scene or value out of range");
         return XTGPU_ERR_INVALID;
     }
-    if (t->leaf_size != sc->leaf_size || t->bvh_builder != sc->builder) {
-        set_error("xtgpu_scene_set_tuning: leaf_size or bvh_builder differs from the built BVH (rebuild it instead)");
+    if (t->leaf_size != sc->leaf_size || t->bvh_builder != sc->builder ||
+        (sc->builtW && (t->wide_collapse != sc->wide_collapse || t->wide_prim_cost != sc->wide_prim_cost))) {
+        set_error("xtgpu_scene_set_tuning: leaf_size, bvh_builder or the 8-wide collapse differs from the built BVH "
+                  "(rebuild it instead)");
         return XTGPU_ERR_STATE;
     }
     sc->tune = *t;

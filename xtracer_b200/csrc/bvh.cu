@@ -953,7 +953,11 @@ xtgpu_status build_bvh(xtgpu_scene *sc, int node_format, int leaf_size, int layo
         set_error("xtgpu_bvh_build: BVH depth exceeds the traversal stack");
         return XTGPU_ERR_LIMIT;
     }
-    if (node_format == XTGPU_NODES_W8 && !sc->builtW) XTG_TRY(build_wide(sc, s));
+    // the 8-wide nodes again when the collapse asked for differs from the built one
+    const xtgpu_tuning &TW = scene_tuning(sc);
+    if (node_format == XTGPU_NODES_W8 &&
+        (!sc->builtW || sc->wide_collapse != TW.wide_collapse || sc->wide_prim_cost != TW.wide_prim_cost))
+        XTG_TRY(build_wide(sc, s));
     sc->last_format = node_format;
     XTG_CUDA(cudaStreamSynchronize(s));
     return XTGPU_OK;

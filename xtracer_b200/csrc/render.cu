@@ -1073,8 +1073,13 @@ __global__ void __launch_bounds__(MINB > 0 ? 128 : 256, MINB > 0 ? MINB : 1)
     }
 }
 
-// 64 registers: four blocks per SM, as before the samplers were added
-__global__ void __launch_bounds__(256, 4) k_shade(const DevJob *__restrict__ jobs, const DevScene *__restrict__ scenes, WaveQueues q, int side)
+// 64 registers: four blocks per SM, as before the samplers were added.  A wave
+// of one scene passes it by value (MULTI false): the hit's primitive and
+// material loads then wait only for the hit, not for the job and scene tables.
+template <bool MULTI>
+__global__ void __launch_bounds__(256, 4)
+    k_shade(const __grid_constant__ DevScene S1, const DevJob *__restrict__ jobs,
+            const DevScene *__restrict__ scenes, WaveQueues q, int side)
 {
     const int n = q.ctl[side];
     const int out = side ^ 1;
@@ -1087,7 +1092,7 @@ __global__ void __launch_bounds__(256, 4) k_shade(const DevJob *__restrict__ job
         if (valid) {
             meta = q.meta[side][i];
             const DevJob &J = jobs[meta.y];
-            const DevScene &S = scenes[J.scene];
+            const DevScene &S = MULTI ? scenes[J.scene] : S1;
             xtgpu_hit h = q.hit[i];
             float4 a = q.org[side][i], b = q.dir[side][i];
             float3 o = f3(a), d = f3(b);
@@ -1467,7 +1472,10 @@ void WaveRunner::enqueue(int njobs, int64_t total, int bounces, int fmt, bool mu
             launch_extend_kernel(T, fmt, multi, single, scenes, jobs, q, side, sms, stack, s);
         if (time_extend && b < MAX_TIMED) rec(ev[2 * b + 1]);
         cudaMemsetAsync(q.ctl + (side ^ 1), 0, sizeof(int32_t), s);
-        k_shade<<<gb, 256, 0, s>>>(jobs, scenes, q, side);
+        if (multi)
+            k_shade<true><<<gb, 256, 0, s>>>(single, jobs, scenes, q, side);
+        else
+            k_shade<false><<<gb, 256, 0, s>>>(single, jobs, scenes, q, side);
         side ^= 1;
     }
     if (!defer_acc) k_accumulate<<<gb, 256, 0, s>>>(jobs, q.ctl, (const int64_t *)prefixbuf.p, q.contrib);
@@ -1592,7 +1600,7 @@ xtgpu_status WaveRunner::read_ctl(int32_t *overflow, unsigned long long *rays, c
 // one primitive per leaf, depth-first node order, 8x8 pixel tiles, 64
 // registers (8 resident 128-thread blocks per SM); camera rays, which are
 // coherent, through binary FP32 nodes with warp-batched fetch.
-static xtgpu_tuning g_tuning = {2, 128, 8, 8, 1ll << 22, 1, 1, 8, 8, 0, 8, XTGPU_NODES_FP32, 0};
+static xtgpu_tuning g_tuning = {2, 128, 8, 8, 1ll << 22, 1, 1, 8, 8, 0, 8, XTGPU_NODES_FP32, 0, 0, 1, 0.3f};
 xtgpu_tuning &tuning() { return g_tuning; }
 
 void launch_extend_kernel(const xtgpu_tuning &T, int fmt, bool multi, const DevScene &single,
@@ -1678,7 +1686,7 @@ void enqueue_wave_raw(const xtgpu_tuning &T, const WaveQueues &q, const DevJob *
         else
             launch_extend_kernel(T, fmt, false, single, scenes, jobs, q, side, sms, stack, s);
         cudaMemsetAsync(q.ctl + (side ^ 1), 0, sizeof(int32_t), s);
-        k_shade<<<gb, 256, 0, s>>>(jobs, scenes, q, side);
+        k_shade<false><<<gb, 256, 0, s>>>(single, jobs, scenes, q, side);
         side ^= 1;
     }
     k_accumulate<<<gb, 256, 0, s>>>(jobs, q.ctl, prefix, q.contrib);

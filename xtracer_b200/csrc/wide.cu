@@ -1,12 +1,25 @@
 // 8-wide BVH with 8-bit quantised child bounds, collapsed from the binary LBVH
-// on the device.  The node layout and the traversal order follow Ylitie,
-// Karras and Laine, "Efficient Incoherent Ray Traversal on GPUs Through
-// Compressed Wide BVHs" (HPG 2017); the collapse is a greedy one.
+// on the device.  The node layout, the traversal order and the cost-optimal
+// collapse follow Ylitie, Karras and Laine, "Efficient Incoherent Ray Traversal
+// on GPUs Through Compressed Wide BVHs" (HPG 2017).
+//
+// Which binary nodes become wide nodes, and which subtrees become leaves, is
+// chosen one of two ways (xtgpu_tuning::wide_collapse):
+//   * 1, cost-optimal (default): a bottom-up dynamic programme over the binary
+//     tree (k_wide_dp) gives every node n and budget i = 1..7 the lowest
+//     surface-area cost C(n, i) of representing n's subtree by at most i
+//     children of a wide node.  C(n, 1) is the cheaper of one leaf (at most 3
+//     primitives: A(n) * c_prim * P(n)) and one internal wide node (A(n) *
+//     c_node + the best split of 8 children between n's two binary
+//     children); C(n, i > 1) is the better of C(n, i - 1) and the best split of
+//     i between the two children.  The emission follows the recorded choices;
+//   * 0, greedy: a wide node repeatedly opens the internal child with the
+//     largest surface area until it has 8 children or only leaves are left,
+//     and every binary leaf is one wide leaf.
 //
 // Build, one kernel launch per level of the wide tree (top down):
-//   * a wide node starts from one binary internal node and repeatedly opens the
-//     internal child with the largest surface area until it has 8 children or
-//     only leaves are left;
+//   * a wide node starts from one binary internal node and takes its children
+//     as above;
 //   * the children take slots by direction: the child whose centroid lies
 //     furthest towards octant s (relative to the node's centre) gets slot s, so
 //     a ray visits slots in the order slot ^ m (m = the ray's sign bits) and
@@ -118,12 +131,181 @@ __device__ __forceinline__ void bin_child(const float4 *nodes, int32_t i, int c,
     ref = __float_as_int(c == 0 ? d.x : d.y);
 }
 
+// --- cost-optimal collapse --------------------------------------------------
+// Per binary internal node: C(n, i) for i = 1..7, the left child's share k of
+// the best split of j = 2..8 children, which C(n, i) come from a split (bit
+// i - 1, i >= 2) and whether C(n, 1) is a leaf (bit 7), and P(n).
+struct WideDP {
+    float c[7];
+    uint8_t split[7];
+    uint8_t use;
+    int32_t prims;
+};
+
+constexpr float WIDE_NODE_COST = 1.0f;
+
+__device__ __forceinline__ float3 fmin3(float3 a, float3 b)
+{
+    return make_float3(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z));
+}
+__device__ __forceinline__ float3 fmax3(float3 a, float3 b)
+{
+    return make_float3(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z));
+}
+
+__global__ void k_wide_parents(int ni, const float4 *__restrict__ bnodes, int32_t *__restrict__ parent)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ni) return;
+    const float4 d = bnodes[4 * (size_t)n + 3];
+    const int32_t c0 = __float_as_int(d.x), c1 = __float_as_int(d.y);
+    if (c0 >= 0 && c0 < ni) parent[c0] = n;
+    if (c1 >= 0 && c1 < ni) parent[c1] = n;
+}
+
+// the DP entry of binary node n from its children's (computed before)
+__device__ void wide_dp_node(const float4 *__restrict__ bnodes, WideDP *dp, int32_t n, float cprim)
+{
+    float ck[2][7];
+    int32_t pk[2];
+    float3 lo = make_float3(INFINITY, INFINITY, INFINITY), hi = make_float3(-INFINITY, -INFINITY, -INFINITY);
+    for (int c = 0; c < 2; ++c) {
+        int32_t ref;
+        float3 cl, ch;
+        bin_child(bnodes, n, c, ref, cl, ch);
+        lo = fmin3(lo, cl);
+        hi = fmax3(hi, ch);
+        if (ref >= 0) {
+            // written by another thread before its fence: read past L1
+            const float *src = (const float *)(dp + ref);
+            for (int i = 0; i < 7; ++i) ck[c][i] = __ldcg(src + i);
+            pk[c] = __ldcg(&dp[ref].prims);
+        } else {
+            const int cnt = (int)leaf_count(ref);
+            const float v = ref == EMPTY_REF ? 0.f : area_of(cl, ch) * cprim * (float)cnt;
+            for (int i = 0; i < 7; ++i) ck[c][i] = v;
+            pk[c] = cnt;
+        }
+    }
+    WideDP out;
+    out.prims = pk[0] + pk[1];
+    float dist[9];
+    for (int j = 2; j <= 8; ++j) {
+        float best = INFINITY;
+        int bk = 1;
+        for (int k = 1; k < j; ++k) {
+            const float v = ck[0][k - 1] + ck[1][j - k - 1];
+            if (v < best) {
+                best = v;
+                bk = k;
+            }
+        }
+        dist[j] = best;
+        out.split[j - 2] = (uint8_t)bk;
+    }
+    const float A = area_of(lo, hi);
+    const float cleaf = out.prims <= WIDE_MAX_LEAF ? A * cprim * (float)out.prims : INFINITY;
+    const float cint = A * WIDE_NODE_COST + dist[8];
+    out.use = 0;
+    out.c[0] = fminf(cleaf, cint);
+    if (cleaf <= cint) out.use |= 0x80u;
+    for (int i = 2; i <= 7; ++i) {
+        if (dist[i] < out.c[i - 2]) {
+            out.c[i - 1] = dist[i];
+            out.use |= (uint8_t)(1u << (i - 1));
+        } else {
+            out.c[i - 1] = out.c[i - 2];
+        }
+    }
+    dp[n] = out;
+}
+
+// Bottom up: a thread starts at every node without internal children and
+// climbs while it is the last of a node's internal children to finish.
+__global__ void k_wide_dp(int ni, const float4 *__restrict__ bnodes, const int32_t *__restrict__ parent,
+                          unsigned *__restrict__ arrived, WideDP *dp, float cprim, int *err)
+{
+    int32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ni) return;
+    {
+        const float4 d = bnodes[4 * (size_t)n + 3];
+        if (__float_as_int(d.x) >= 0 || __float_as_int(d.y) >= 0) return;
+    }
+    for (int guard = 0;; ++guard) {
+        if (guard > 256) {   // deeper than any tree this build makes: report, never loop forever
+            atomicExch(err, 1);
+            return;
+        }
+        wide_dp_node(bnodes, dp, n, cprim);
+        __threadfence();
+        const int32_t p = parent[n];
+        if (p < 0) return;
+        const float4 d = bnodes[4 * (size_t)p + 3];
+        const unsigned need = (__float_as_int(d.x) >= 0 ? 1u : 0u) + (__float_as_int(d.y) >= 0 ? 1u : 0u);
+        if (atomicAdd(&arrived[p], 1u) + 1u < need) return;
+        __threadfence();
+        n = p;
+    }
+}
+
+// The children of the wide node made from binary node `root` under the DP's
+// choices: up to 8 (ref, box) pairs; a subtree chosen as a leaf becomes the
+// leaf ref of its primitives (contiguous in the leaf order).
+__device__ int wide_children_dp(const float4 *__restrict__ bnodes, const WideDP *__restrict__ dp, int32_t root,
+                                int32_t cref[8], float3 clo[8], float3 chi[8])
+{
+    int32_t sref[16];
+    int sb[16];
+    float3 slo[16], shi[16];
+    int sp = 0, n = 0;
+    const int k8 = dp[root].split[8 - 2];
+    bin_child(bnodes, root, 1, sref[sp], slo[sp], shi[sp]);
+    sb[sp++] = 8 - k8;
+    bin_child(bnodes, root, 0, sref[sp], slo[sp], shi[sp]);
+    sb[sp++] = k8;
+    while (sp > 0 && n < 8) {
+        --sp;
+        const int32_t ref = sref[sp];
+        int i = sb[sp];
+        const float3 lo = slo[sp], hi = shi[sp];
+        if (ref < 0) {
+            cref[n] = ref;
+            clo[n] = lo;
+            chi[n] = hi;
+            ++n;
+            continue;
+        }
+        const WideDP &D = dp[ref];
+        while (i > 1 && !(D.use & (1u << (i - 1)))) --i;
+        if (i == 1) {
+            if (D.use & 0x80u) {
+                int32_t r = ref;
+                for (int g = 0; r >= 0 && g < 64; ++g) r = __float_as_int(bnodes[4 * (size_t)r + 3].x);
+                cref[n] = leaf_ref(leaf_first(r), (uint32_t)D.prims);
+            } else {
+                cref[n] = ref;
+            }
+            clo[n] = lo;
+            chi[n] = hi;
+            ++n;
+            continue;
+        }
+        if (sp + 2 > 16) break;   // budgets sum to at most 8: cannot happen
+        const int k = D.split[i - 2];
+        bin_child(bnodes, ref, 1, sref[sp], slo[sp], shi[sp]);
+        sb[sp++] = i - k;
+        bin_child(bnodes, ref, 0, sref[sp], slo[sp], shi[sp]);
+        sb[sp++] = k;
+    }
+    return n;
+}
+
 // One wide node per thread.  ctr[0]: wide nodes allocated, ctr[1]: leaf
 // primitives placed, ctr[2]: items of the next level, ctr[3]: error flag.
 __global__ void k_wide_level(const float4 *__restrict__ bnodes, const float4 *__restrict__ bprims,
-                             const WideItem *__restrict__ items, int nitems, WideItem *__restrict__ next,
-                             int max_nodes, uint4 *__restrict__ wnodes, float4 *__restrict__ wprims, int n_prims,
-                             int *ctr)
+                             const WideDP *__restrict__ dp, const WideItem *__restrict__ items, int nitems,
+                             WideItem *__restrict__ next, int max_nodes, uint4 *__restrict__ wnodes,
+                             float4 *__restrict__ wprims, int n_prims, int *ctr)
 {
     const int it = blockIdx.x * blockDim.x + threadIdx.x;
     if (it >= nitems) return;
@@ -131,7 +313,9 @@ __global__ void k_wide_level(const float4 *__restrict__ bnodes, const float4 *__
     int32_t cref[8];
     float3 clo[8], chi[8];
     int n = 0;
-    if (W.bref >= 0) {
+    if (W.bref >= 0 && dp) {
+        n = wide_children_dp(bnodes, dp, W.bref, cref, clo, chi);
+    } else if (W.bref >= 0) {
         bin_child(bnodes, W.bref, 0, cref[0], clo[0], chi[0]);
         bin_child(bnodes, W.bref, 1, cref[1], clo[1], chi[1]);
         n = 2;
@@ -304,6 +488,39 @@ xtgpu_status build_wide(xtgpu_scene *sc, cudaStream_t s)
     const int max_nodes = std::max(1, n - 1);
     XTG_TRY(dalloc(sc->nodesW, sizeof(uint4) * 5 * (size_t)max_nodes, s));
     XTG_TRY(dalloc(sc->leafW, sizeof(float4) * 3 * (size_t)n, s));
+    const xtgpu_tuning &T = scene_tuning(sc);
+    const int ni = n - 1;
+    HostBuf dpb;
+    if (T.wide_collapse == 1 && ni > 0 && S.root >= 0) {
+        // the cost tables, bottom up
+        HostBuf parb, arrb, errb;
+        XTG_TRY(dalloc(dpb, sizeof(WideDP) * (size_t)ni, s));
+        XTG_TRY(dalloc(parb, sizeof(int32_t) * (size_t)ni, s));
+        XTG_TRY(dalloc(arrb, sizeof(unsigned) * (size_t)ni, s));
+        XTG_TRY(dalloc(errb, sizeof(int), s));
+        XTG_CUDA(cudaMemsetAsync(parb.p, 0xff, sizeof(int32_t) * (size_t)ni, s));
+        XTG_CUDA(cudaMemsetAsync(arrb.p, 0, sizeof(unsigned) * (size_t)ni, s));
+        XTG_CUDA(cudaMemsetAsync(errb.p, 0, sizeof(int), s));
+        k_wide_parents<<<(ni + 255) / 256, 256, 0, s>>>(ni, S.nodes32, (int32_t *)parb.p);
+        const float cprim = T.wide_prim_cost > 0.f ? T.wide_prim_cost : 0.3f;
+        k_wide_dp<<<(ni + 127) / 128, 128, 0, s>>>(ni, S.nodes32, (const int32_t *)parb.p, (unsigned *)arrb.p,
+                                                   (WideDP *)dpb.p, cprim, (int *)errb.p);
+        int err = 0;
+        cudaError_t e = cudaMemcpyAsync(&err, errb.p, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        dfree(parb);
+        dfree(arrb);
+        dfree(errb);
+        if (e != cudaSuccess) {
+            dfree(dpb);
+            return cuda_fail(e, "wide collapse costs", __FILE__, __LINE__);
+        }
+        if (err) {
+            dfree(dpb);
+            set_error("xtgpu_bvh_build: wide collapse costs did not reach the root");
+            return XTGPU_ERR_CUDA;
+        }
+    }
     HostBuf itemsA, itemsB, ctrb;
     XTG_TRY(dalloc(itemsA, sizeof(WideItem) * (size_t)max_nodes, s));
     XTG_TRY(dalloc(itemsB, sizeof(WideItem) * (size_t)max_nodes, s));
@@ -322,8 +539,9 @@ xtgpu_status build_wide(xtgpu_scene *sc, cudaStream_t s)
             st = XTGPU_ERR_CUDA;
             break;
         }
-        k_wide_level<<<(nitems + 127) / 128, 128, 0, s>>>(S.nodes32, S.leaf_prims, cur, nitems, nxt, max_nodes,
-                                                           (uint4 *)sc->nodesW.p, (float4 *)sc->leafW.p, n, ctr);
+        k_wide_level<<<(nitems + 127) / 128, 128, 0, s>>>(S.nodes32, S.leaf_prims, (const WideDP *)dpb.p, cur,
+                                                           nitems, nxt, max_nodes, (uint4 *)sc->nodesW.p,
+                                                           (float4 *)sc->leafW.p, n, ctr);
         int back[4];
         cudaError_t e = cudaMemcpyAsync(back, ctr, sizeof(back), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -350,12 +568,15 @@ xtgpu_status build_wide(xtgpu_scene *sc, cudaStream_t s)
     dfree(itemsA);
     dfree(itemsB);
     dfree(ctrb);
+    dfree(dpb);
     if (st != XTGPU_OK) {
         dfree(sc->nodesW);
         dfree(sc->leafW);
         return st;
     }
     sc->depthW = levels;
+    sc->wide_collapse = T.wide_collapse;
+    sc->wide_prim_cost = T.wide_prim_cost;
     S.nodesW = (const uint4 *)sc->nodesW.p;
     S.leafW = (const float4 *)sc->leafW.p;
     S.rootW = 0;

@@ -125,6 +125,8 @@ struct xtgpu_scene {
     int32_t last_format = XTGPU_NODES_FP32;
     bool built32 = false, built8 = false, builtW = false;
     int32_t depthW = 0;        // levels of the 8-wide BVH
+    int32_t wide_collapse = 1; // how it was collapsed (xtgpu_tuning::wide_collapse)
+    float wide_prim_cost = 0.3f;
     int32_t n_wide = 0;        // its nodes
     int device = 0;
     // host copies used by the service and the tests

@@ -124,7 +124,8 @@ class Tuning(C.Structure):
                 ("tile", C.c_int32), ("wave_paths", C.c_int64), ("leaf_size", C.c_int32),
                 ("node_layout", C.c_int32), ("refill_threshold", C.c_int32), ("extend_min_blocks", C.c_int32),
                 ("stack_entries", C.c_int32), ("steps_per_vote", C.c_int32),
-                ("primary_node_format", C.c_int32), ("primary_variant", C.c_int32), ("bvh_builder", C.c_int32)]
+                ("primary_node_format", C.c_int32), ("primary_variant", C.c_int32), ("bvh_builder", C.c_int32),
+                ("wide_collapse", C.c_int32), ("wide_prim_cost", C.c_float)]
 
 
 def get_tuning() -> "Tuning":
