@@ -278,13 +278,12 @@ __device__ int wide_children_dp(const float4 *__restrict__ bnodes, const WideDP 
         const WideDP &D = dp[ref];
         while (i > 1 && !(D.use & (1u << (i - 1)))) --i;
         if (i == 1) {
-            if (D.use & 0x80u) {
-                int32_t r = ref;
+            int32_t r = ref;
+            if (D.use & 0x80u)
                 for (int g = 0; r >= 0 && g < 64; ++g) r = __float_as_int(bnodes[4 * (size_t)r + 3].x);
-                cref[n] = leaf_ref(leaf_first(r), (uint32_t)D.prims);
-            } else {
-                cref[n] = ref;
-            }
+            // the subtree's primitives start at its leftmost leaf; a walk that
+            // ends on no leaf (a malformed tree) keeps the node internal
+            cref[n] = (D.use & 0x80u) && r < 0 && r != EMPTY_REF ? leaf_ref(leaf_first(r), (uint32_t)D.prims) : ref;
             clo[n] = lo;
             chi[n] = hi;
             ++n;
