@@ -121,11 +121,17 @@ def measured_peaks():
 # ---------------------------------------------------------------------------
 SERVED_FORMAT = 2   # xtgpu.NODES_W8: 8-wide BVH, 8-bit quantised child bounds
 WAVES_IN_FLIGHT = 3   # served form: waves on streams of their own, each filling the earlier ones' tails
-# DRAM bytes (read + write) per ray of the served extend kernel, from one ncu
-# capture of k_extend_pool<W8> on 1,048,576 hairball2m first-bounce rays
-# (python -m xtracer_b200.profile_extend --scene hairball2m); the roofline's
-# traffic is this figure times the rays of an average launch.
-NCU_TRAFFIC_BYTES_PER_RAY = 104.0
+# The served extend kernel (k_extend_pool<W8>) per scene, from one ncu capture
+# each of 1,048,576 first-bounce rays (python -m xtracer_b200.profile_extend
+# --scene <scene> --fmt w8 --rays 1048576 --iters 1): DRAM and L2 bytes per ray,
+# the share of issue slots used, and active lanes per warp instruction.  The
+# roofline's traffic is the DRAM figure of each scene times that scene's rays,
+# per launch; the issue figures name the resource that binds the kernel.
+NCU_EXTEND = {
+    "terrain10k": (35, 477, 0.742, 12.0), "terrain50k": (38, 704, 0.733, 11.1),
+    "terrain200k": (47, 880, 0.714, 10.9), "terrain500k": (61, 980, 0.702, 11.3),
+    "terrain1m": (86, 1247, 0.683, 10.9), "hairball2m": (80, 1901, 0.677, 10.7),
+    "spheres64": (32, 84, 0.687, 16.7), "spheres4096": (33, 120, 0.650, 15.8)}
 
 
 def build_scenes(scale, autotune=False):
@@ -150,11 +156,13 @@ def build_scenes(scale, autotune=False):
     return specs, out, tunes
 
 
-def run_slice(svc, jobs, record=None, per_scene=None, view=False):
+def run_slice(svc, jobs, record=None, per_scene=None, view=False, job_stats=None):
     """Submits the jobs at once, runs the service to completion; returns
     (rays, latencies in s).  per_scene (array) accumulates rays by scene.
     record collects each frame (copied), or with view (host_results services)
-    the last pixel read from the frame's host copy in place."""
+    the last pixel read from the frame's host copy in place.  job_stats, a
+    pair of lists, collects each job's rays and its time from admission to
+    its last wave."""
     from xtracer_b200 import xtgpu
     ids = [svc.submit(j.scene, xtgpu.PATHTRACER, j.width, j.height, j.spp, j.depth, 100.0, j.seed) for j in jobs]
     svc.run()
@@ -167,6 +175,9 @@ def run_slice(svc, jobs, record=None, per_scene=None, view=False):
         if per_scene is not None:
             per_scene[j.scene] += st.rays
         lat.append(st.finish_s - st.submit_s)
+        if job_stats is not None:
+            job_stats[0].append(st.rays)
+            job_stats[1].append(st.render_done_s - st.start_s)
         if record is not None:
             record.append(float(svc.result_view(i)[-1, -1, 0]) if view else svc.result(i))
         svc.release(i)
@@ -212,6 +223,32 @@ def serve_open_loop(svc, jobs, arrivals):
         rays += st.rays
         svc.release(i)
     return lats, rays, wall
+
+
+def full_wave_rates(gscenes, specs):
+    """Mrays/s of every scene at a full wave (one 1024x1024 x 4 spp pathtracer
+    job of 4 Mi paths, depth 4) through xtgpu_render, with binary FP32 nodes
+    (the plain path's) and 8-wide quantised nodes (the served form's); CUDA
+    events, best of 3 after a warm-up."""
+    import torch
+    from xtracer_b200 import xtgpu
+    out = {}
+    for sp, sc in zip(specs, gscenes):
+        row = {}
+        for tag, fmt in (("fp32", xtgpu.NODES_FP32), ("w8", SERVED_FORMAT)):
+            best = None
+            for it in range(4):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                _, rays = sc.render(xtgpu.PATHTRACER, 1024, 1024, spp=4, rdepth=4, seed=99, node_format=fmt)
+                e1.record()
+                torch.cuda.synchronize()
+                if it:
+                    t = e0.elapsed_time(e1) / 1000.0
+                    best = t if best is None else min(best, t)
+            row[tag] = rays / best / 1e6
+        out[sp.name] = row
+    return out
 
 
 def pct(v, q):
@@ -439,7 +476,10 @@ def main():
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / ext_s / 1e9 if ext_s > 0 else None
     rays_per_launch = float(per_scene.sum()) / max(1, rst.extend_launches)
-    traffic = NCU_TRAFFIC_BYTES_PER_RAY * rays_per_launch
+    ncu_rows = [NCU_EXTEND[sp.name] for sp in specs]
+    wsum = max(1.0, float(per_scene.sum()))
+    wavg = lambda k: float(sum(per_scene[i] * ncu_rows[i][k] for i in range(len(specs)))) / wsum
+    traffic = wavg(0) * rays_per_launch
 
     # end to end: same steps, every frame copied to host memory by the service
     e2e_svc = Service(gscenes, node_format=SERVED_FORMAT, use_graphs=True, merge_jobs=True, memory_budget=budget,
@@ -470,8 +510,9 @@ def main():
         run_slice(psvc, slices[0])   # warm-up: allocator pools, modules
         torch.cuda.synchronize()
         p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        psvc_jobs, psvc_times = [], []
         p0.record()
-        pr, pl = run_slice(psvc, timed[0])
+        pr, pl = run_slice(psvc, timed[0], job_stats=(psvc_jobs, psvc_times))
         p1.record()
         torch.cuda.synchronize()
         ps = p0.elapsed_time(p1) / 1000.0
@@ -521,7 +562,24 @@ def main():
             torch.cuda.synchronize()
             other[fname] = fr / (f0.elapsed_time(f1) / 1000.0) / 1e6
             fsvc.close()
-        plain = {"value": pr / ps / 1e6, "unit": "Mrays/s", "step_jobs": len(timed[0]),
+        # where the plain path's time goes: each job of the step at its scene's
+        # full-wave rate would take rays / rate; the rest of its time is the
+        # cost of a job too small to fill the GPU (short waves, launch tails,
+        # per-job set-up).  That bounds what merging jobs can win, and the node
+        # format what the faster traversal can.
+        rates = full_wave_rates(gscenes, specs)
+        jids = psvc_jobs
+        ideal32 = sum(r / (rates[specs[j.scene].name]["fp32"] * 1e6) for j, r in zip(timed[0], jids))
+        ideal8 = sum(r / (rates[specs[j.scene].name]["w8"] * 1e6) for j, r in zip(timed[0], jids))
+        small = [k for k, j in enumerate(timed[0]) if j.width * j.height * j.spp < (1 << 20)]
+        breakdown = {"plain_s": ps, "served_s": ss,
+                     "plain_at_full_wave_rate_s": ideal32, "w8_at_full_wave_rate_s": ideal8,
+                     "bound_merging_only": ps / ideal32, "bound_merging_and_w8": ps / ideal8,
+                     "achieved": ps / ss, "jobs_under_1Mi_paths": len(small),
+                     "their_share_of_plain_s": sum(psvc_times[k] for k in small) / ps,
+                     "their_share_of_rays": sum(jids[k] for k in small) / max(1, sum(jids)),
+                     "full_wave_mrays": rates}
+        plain = {"value": pr / ps / 1e6, "unit": "Mrays/s", "step_jobs": len(timed[0]), "breakdown": breakdown,
                  "p50_ms": 1000 * pct(pl, 50), "p99_ms": 1000 * pct(pl, 99),
                  "served_same_step_mrays": sr / ss / 1e6, "speedup": (sr / ss) / (pr / ps),
                  "served_w8_only_same_step_mrays": w8_only,
@@ -565,11 +623,25 @@ def main():
             psvc = Service(gscenes, node_format=xtgpu.NODES_FP32, use_graphs=False, merge_jobs=False,
                            memory_budget=budget, waves_in_flight=1, stream=stream)
             plats, prays, pwall = serve_open_loop(psvc, jobs, arr)
-            psvc.close()
             plat_all = D.gather(plats)
             latency["plain"] = {"p50_ms": 1000 * pct(plat_all, 50), "p99_ms": 1000 * pct(plat_all, 99),
                                 "max_ms": 1000 * max(plat_all), "wall_s": D.max(pwall),
                                 "mrays_s_wall": D.sum(prays) / D.max(pwall) / 1e6}
+            # both forms at an offered load the plain path can carry (0.8x its
+            # job rate), where the percentiles are those of a stable queue
+            arr8 = arr * (1.5 / 0.8)
+            qsvc = Service(gscenes, node_format=SERVED_FORMAT, use_graphs=True, merge_jobs=True,
+                           memory_budget=budget, waves_in_flight=WAVES_IN_FLIGHT, stream=stream)
+            run_slice(qsvc, slices[0])
+            q8, _, qw = serve_open_loop(qsvc, jobs, arr8)
+            qsvc.close()
+            p8, _, pw8 = serve_open_loop(psvc, jobs, arr8)
+            psvc.close()
+            q8, p8 = D.gather(q8), D.gather(p8)
+            latency["at_0.8x_plain_rate"] = {
+                "jobs_per_s": 0.8 * len(timed[0]) / ps,
+                "served": {"p50_ms": 1000 * pct(q8, 50), "p99_ms": 1000 * pct(q8, 99), "wall_s": D.max(qw)},
+                "plain": {"p50_ms": 1000 * pct(p8, 50), "p99_ms": 1000 * pct(p8, 99), "wall_s": D.max(pw8)}}
 
     cpu = None
     if not args.no_cpu and rank == 0:
@@ -604,9 +676,16 @@ def main():
                     "d2h_bytes_per_step": d2h // max(1, len(timed))},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                         "traffic_source": "ncu DRAM read+write of k_extend_pool<W8> on 1M hairball2m bounce "
-                                           "rays, %.0f B/ray, times %.0f rays per launch" %
-                                           (NCU_TRAFFIC_BYTES_PER_RAY, rays_per_launch),
+                         "traffic_source": "ncu DRAM read+write of k_extend_pool<W8> per scene on 1 Mi "
+                                           "first-bounce rays (%s B/ray), weighted by the timed steps' rays "
+                                           "of each scene, times %.0f rays per launch" %
+                                           ({sp.name: NCU_EXTEND[sp.name][0] for sp in specs}, rays_per_launch),
+                         "binding": {"resource": "instruction issue: the kernel waits on dependent node "
+                                                 "loads and runs a third of its lanes per instruction; DRAM "
+                                                 "and L2 carry a small share of their bandwidth",
+                                     "issue_active_frac": wavg(2), "simt_lanes_of_32": wavg(3),
+                                     "l2_bytes_per_ray": wavg(1), "dram_bytes_per_ray": wavg(0),
+                                     "source": "ncu per scene (profile_extend), weighted by the timed rays"},
                          "algorithmic_bytes_per_launch": alg_bytes / max(1, rst.extend_launches),
                          "kernel": "k_extend_pool<W8> / k_extend_batch<W8> (closest-hit traversal, 8-wide "
                                    "quantised nodes)", "peak_kind": peak_kind,

@@ -429,7 +429,8 @@ typedef struct {
                                       (surface-area costs by dynamic programming, subtrees of
                                       up to 3 primitives as leaves; Ylitie, Karras and Laine
                                       2017), 0 = greedy largest-area opening */
-    float wide_prim_cost;          /* that cost of a primitive test, in node visits (0 = 0.3) */
+    float wide_prim_cost;          /* that cost of a primitive test, in node visits (0 = 1; 1 measured
+                                      best of 0.3, 0.6, 1 and 1.5 over the served scenes) */
 } xtgpu_tuning;
 XTGPU_API xtgpu_status xtgpu_get_tuning(xtgpu_tuning *t);
 XTGPU_API xtgpu_status xtgpu_set_tuning(const xtgpu_tuning *t);

@@ -374,6 +374,9 @@ static xtgpu_status upload_shading(xtgpu_scene *sc, const xtgpu_scene_desc *d, i
     dfree(nm); dfree(no); dfree(npm); dfree(nt); dfree(nx); dfree(nu); dfree(nv);   // the previous buffers
     DevScene &S = sc->dev;
     S.prim_mat = (const int32_t *)sc->prim_mat.p;
+    S.has_lobe = 0;
+    for (const DevMaterial &m : mats)
+        if (m.type == XTGPU_PHONG || m.type == XTGPU_BLINNPHONG) S.has_lobe = 1;
     S.obj_uvs = (const float2 *)sc->obj_uvs.p;
     S.tri_uv = (const float2 *)sc->tri_uv.p;
     S.materials = (const DevMaterial *)sc->materials.p;

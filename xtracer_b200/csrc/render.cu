@@ -1076,7 +1076,10 @@ __global__ void __launch_bounds__(MINB > 0 ? 128 : 256, MINB > 0 ? MINB : 1)
 // 64 registers: four blocks per SM, as before the samplers were added.  A wave
 // of one scene passes it by value (MULTI false): the hit's primitive and
 // material loads then wait only for the hit, not for the job and scene tables.
-template <bool MULTI>
+// LOBE false leaves out the Phong / BlinnPhong specular lobe (FP64, called out
+// of line), whose call costs registers on every path; it is launched for waves
+// whose scenes have no such material.
+template <bool MULTI, bool LOBE>
 __global__ void __launch_bounds__(256, 4)
     k_shade(const __grid_constant__ DevScene S1, const DevJob *__restrict__ jobs,
             const DevScene *__restrict__ scenes, WaveQueues q, int side)
@@ -1193,10 +1196,14 @@ __global__ void __launch_bounds__(256, 4)
                     if (k > M.reflectance) {
                         f = mat_color(S, M, 0, h, o, d);
                         nd3 = s_diffuse(nrm, key, ctr);
-                    } else {
+                    } else if (LOBE) {
                         f = mat_color(S, M, 1, h, o, d);
                         aimed = phong_lobe(S, h, o, d, M.exponent, M.type == XTGPU_BLINNPHONG, key, ctr, nd3,
                                            lobe_raw);
+                    } else {
+                        // not launched for such a scene; never taken
+                        f = make_float3(0.f, 0.f, 0.f);
+                        nd3 = nrm;
                     }
                 } else if (M.type == XTGPU_EMISSIVE) {
                     float3 L = cmul(Pp, cmul(Ii, mat_color(S, M, 2, h, o, d)));
@@ -1472,10 +1479,17 @@ void WaveRunner::enqueue(int njobs, int64_t total, int bounces, int fmt, bool mu
             launch_extend_kernel(T, fmt, multi, single, scenes, jobs, q, side, sms, stack, s);
         if (time_extend && b < MAX_TIMED) rec(ev[2 * b + 1]);
         cudaMemsetAsync(q.ctl + (side ^ 1), 0, sizeof(int32_t), s);
+        bool lobe = single.has_lobe != 0;
         if (multi)
-            k_shade<true><<<gb, 256, 0, s>>>(single, jobs, scenes, q, side);
+            for (const DevScene &h : host_scenes) lobe = lobe || h.has_lobe;
+        if (multi && lobe)
+            k_shade<true, true><<<gb, 256, 0, s>>>(single, jobs, scenes, q, side);
+        else if (multi)
+            k_shade<true, false><<<gb, 256, 0, s>>>(single, jobs, scenes, q, side);
+        else if (lobe)
+            k_shade<false, true><<<gb, 256, 0, s>>>(single, jobs, scenes, q, side);
         else
-            k_shade<false><<<gb, 256, 0, s>>>(single, jobs, scenes, q, side);
+            k_shade<false, false><<<gb, 256, 0, s>>>(single, jobs, scenes, q, side);
         side ^= 1;
     }
     if (!defer_acc) k_accumulate<<<gb, 256, 0, s>>>(jobs, q.ctl, (const int64_t *)prefixbuf.p, q.contrib);
@@ -1600,7 +1614,7 @@ xtgpu_status WaveRunner::read_ctl(int32_t *overflow, unsigned long long *rays, c
 // one primitive per leaf, depth-first node order, 8x8 pixel tiles, 64
 // registers (8 resident 128-thread blocks per SM); camera rays, which are
 // coherent, through binary FP32 nodes with warp-batched fetch.
-static xtgpu_tuning g_tuning = {2, 128, 8, 8, 1ll << 22, 1, 1, 8, 8, 0, 8, XTGPU_NODES_FP32, 0, 0, 1, 0.3f};
+static xtgpu_tuning g_tuning = {2, 128, 8, 8, 1ll << 22, 1, 1, 8, 8, 0, 8, XTGPU_NODES_FP32, 0, 0, 1, 1.0f};
 xtgpu_tuning &tuning() { return g_tuning; }
 
 void launch_extend_kernel(const xtgpu_tuning &T, int fmt, bool multi, const DevScene &single,
@@ -1686,7 +1700,10 @@ void enqueue_wave_raw(const xtgpu_tuning &T, const WaveQueues &q, const DevJob *
         else
             launch_extend_kernel(T, fmt, false, single, scenes, jobs, q, side, sms, stack, s);
         cudaMemsetAsync(q.ctl + (side ^ 1), 0, sizeof(int32_t), s);
-        k_shade<false><<<gb, 256, 0, s>>>(single, jobs, scenes, q, side);
+        if (single.has_lobe)
+            k_shade<false, true><<<gb, 256, 0, s>>>(single, jobs, scenes, q, side);
+        else
+            k_shade<false, false><<<gb, 256, 0, s>>>(single, jobs, scenes, q, side);
         side ^= 1;
     }
     k_accumulate<<<gb, 256, 0, s>>>(jobs, q.ctl, prefix, q.contrib);

@@ -501,7 +501,7 @@ xtgpu_status build_wide(xtgpu_scene *sc, cudaStream_t s)
         XTG_CUDA(cudaMemsetAsync(arrb.p, 0, sizeof(unsigned) * (size_t)ni, s));
         XTG_CUDA(cudaMemsetAsync(errb.p, 0, sizeof(int), s));
         k_wide_parents<<<(ni + 255) / 256, 256, 0, s>>>(ni, S.nodes32, (int32_t *)parb.p);
-        const float cprim = T.wide_prim_cost > 0.f ? T.wide_prim_cost : 0.3f;
+        const float cprim = T.wide_prim_cost > 0.f ? T.wide_prim_cost : 1.0f;
         k_wide_dp<<<(ni + 127) / 128, 128, 0, s>>>(ni, S.nodes32, (const int32_t *)parb.p, (unsigned *)arrb.p,
                                                    (WideDP *)dpb.p, cprim, (int *)errb.p);
         int err = 0;

@@ -82,6 +82,7 @@ struct DevScene {
     const int32_t *prim_obj;   // object of each primitive id (tris, spheres, planes)
     const int32_t *obj_material;
     const int32_t *prim_mat;   // material of each primitive id (obj_material[prim_obj[i]])
+    int32_t has_lobe;          // some material is Phong or BlinnPhong (a specular lobe to sample)
     const DevMaterial *materials;
     const float2 *obj_uvs;     // per object: the surface's (u_scale, v_scale)
     const float2 *tri_uv;      // 3 per triangle, or nullptr (constructor defaults)
@@ -126,7 +127,7 @@ struct xtgpu_scene {
     bool built32 = false, built8 = false, builtW = false;
     int32_t depthW = 0;        // levels of the 8-wide BVH
     int32_t wide_collapse = 1; // how it was collapsed (xtgpu_tuning::wide_collapse)
-    float wide_prim_cost = 0.3f;
+    float wide_prim_cost = 1.0f;
     int32_t n_wide = 0;        // its nodes
     int device = 0;
     // host copies used by the service and the tests
