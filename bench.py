@@ -286,15 +286,19 @@ def roofline_bytes_per_ray(specs, gpu_scenes, node_format):
 # centred crop.  Crop edge and spp per scene keep each render to a few seconds
 # on the host cores; the reference's cost per ray grows with the mesh
 # (Octree::r_intersection tests every triangle of every node a ray's box
-# meets, octree.tml:206-249).  Scene load and octree build are timed apart.
-CPU_SAMPLE = [("terrain10k", 32, 4), ("terrain50k", 20, 4), ("terrain200k", 12, 4), ("terrain500k", 8, 4),
-              ("terrain1m", 6, 4), ("hairball2m", 6, 1), ("spheres64", 64, 16), ("spheres4096", 24, 4)]
+# meets, octree.tml:206-249).  The reference renders tiles in parallel
+# (integrator.cc:40-42), so each crop is handed over as tiles of the given edge,
+# enough of them for every host thread.  Scene load and octree build are timed
+# apart.
+CPU_SAMPLE = [("terrain10k", 32, 4, 2), ("terrain50k", 20, 4, 2), ("terrain200k", 12, 4, 1),
+              ("terrain500k", 8, 4, 1), ("terrain1m", 6, 4, 1), ("hairball2m", 6, 1, 1), ("spheres64", 64, 16, 4),
+              ("spheres4096", 24, 4, 2)]
 CPU_FRAME = 256
 
 
 def cpu_sample_text():
-    return ("pathtracer depth 4, seed 7, on centred crops of %dx%d frames: " % (CPU_FRAME, CPU_FRAME) +
-            ", ".join("%s %dx%d x %d spp" % (n, c, c, spp) for n, c, spp in CPU_SAMPLE) +
+    return ("pathtracer depth 4, seed 7, on centred crops of %dx%d frames in tiles: " % (CPU_FRAME, CPU_FRAME) +
+            ", ".join("%s %dx%d x %d spp (%dx%d tiles)" % (n, c, c, spp, t, t) for n, c, spp, t in CPU_SAMPLE) +
             " (IIntegrator::render timed, rays counted at Scene::intersection; scene load and octree build "
             "timed apart)")
 
@@ -302,6 +306,11 @@ def cpu_sample_text():
 def cpu_crop(c):
     x0 = (CPU_FRAME - c) // 2
     return (x0, x0, x0 + c, x0 + c)
+
+
+def cpu_tiles(c, t):
+    x0, y0, x1, y1 = cpu_crop(c)
+    return [(x, y, min(x + t, x1), min(y + t, y1)) for y in range(y0, y1, t) for x in range(x0, x1, t)]
 
 
 def cpu_reference_runs(scale, threads, repeats):
@@ -314,10 +323,10 @@ def cpu_reference_runs(scale, threads, repeats):
         return None
     work = tempfile.mkdtemp(prefix="xtref")
     out = []
-    for name, crop, spp in CPU_SAMPLE:
+    for name, crop, spp, tile in CPU_SAMPLE:
         spec = scenes.jobstream_scene(name, scale)
         scn = spec.write_scn(work)
-        r = po.ref_bench(scn, "pathtracer", CPU_FRAME, CPU_FRAME, spp, 4, threads, 7, [cpu_crop(crop)], repeats,
+        r = po.ref_bench(scn, "pathtracer", CPU_FRAME, CPU_FRAME, spp, 4, threads, 7, cpu_tiles(crop, tile), repeats,
                          workdir=work)
         r["scene"] = name
         out.append(r)
@@ -347,7 +356,7 @@ def gpu_on_cpu_sample(gscenes, specs):
     from xtracer_b200 import xtgpu
     names = [s.name for s in specs]
     out = {}
-    for name, crop, spp in CPU_SAMPLE:
+    for name, crop, spp, _ in CPU_SAMPLE:
         sc = gscenes[names.index(name)]
         row = {}
         for tag, rect in (("crop", cpu_crop(crop)), ("frame", None)):
