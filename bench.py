@@ -128,10 +128,10 @@ WAVES_IN_FLIGHT = 3   # served form: waves on streams of their own, each filling
 # roofline's traffic is the DRAM figure of each scene times that scene's rays,
 # per launch; the issue figures name the resource that binds the kernel.
 NCU_EXTEND = {
-    "terrain10k": (35, 477, 0.742, 12.0), "terrain50k": (38, 704, 0.733, 11.1),
-    "terrain200k": (47, 880, 0.714, 10.9), "terrain500k": (61, 980, 0.702, 11.3),
-    "terrain1m": (86, 1247, 0.683, 10.9), "hairball2m": (80, 1901, 0.677, 10.7),
-    "spheres64": (32, 84, 0.687, 16.7), "spheres4096": (33, 120, 0.650, 15.8)}
+    "terrain10k": (35, 442, 0.735, 12.8), "terrain50k": (39, 663, 0.726, 11.9),
+    "terrain200k": (48, 846, 0.710, 11.6), "terrain500k": (63, 949, 0.698, 12.0),
+    "terrain1m": (89, 1213, 0.681, 11.6), "hairball2m": (88, 1715, 0.660, 13.5),
+    "spheres64": (32, 86, 0.686, 16.2), "spheres4096": (33, 123, 0.643, 16.4)}
 
 
 def build_scenes(scale, autotune=False):
@@ -225,22 +225,23 @@ def serve_open_loop(svc, jobs, arrivals):
     return lats, rays, wall
 
 
-def full_wave_rates(gscenes, specs):
-    """Mrays/s of every scene at a full wave (one 1024x1024 x 4 spp pathtracer
-    job of 4 Mi paths, depth 4) through xtgpu_render, with binary FP32 nodes
-    (the plain path's) and 8-wide quantised nodes (the served form's); CUDA
-    events, best of 3 after a warm-up."""
+def full_wave_rates(services, specs):
+    """Mrays/s of every scene when one job fills the GPU: a 1024x1024 x 16 spp
+    pathtracer job (16 Mi paths, four full waves, depth 4) submitted alone to
+    each service ({"plain": ..., "served": ...}); CUDA events around the
+    service run, best of 3 after a warm-up."""
     import torch
-    from xtracer_b200 import xtgpu
+    from xtracer_b200 import scenes
     out = {}
-    for sp, sc in zip(specs, gscenes):
+    for k, sp in enumerate(specs):
         row = {}
-        for tag, fmt in (("fp32", xtgpu.NODES_FP32), ("w8", SERVED_FORMAT)):
+        job = [scenes.Job(0, k, 1024, 1024, 16, 4, 0.0, 99)]
+        for tag, svc in services.items():
             best = None
             for it in range(4):
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record()
-                _, rays = sc.render(xtgpu.PATHTRACER, 1024, 1024, spp=4, rdepth=4, seed=99, node_format=fmt)
+                rays, _ = run_slice(svc, job)
                 e1.record()
                 torch.cuda.synchronize()
                 if it:
@@ -531,7 +532,6 @@ def main():
         check_jobs = timed[0][:16]
         pf, sf = [], []
         run_slice(psvc, check_jobs, record=pf)
-        psvc.close()
         run_slice(served, check_jobs, record=sf)
         diff = max(float(np.nanmax(np.abs(a - b))) if a.size else 0.0 for a, b in zip(pf, sf))
         same = all(np.array_equal(a, b, equal_nan=True) for a, b in zip(pf, sf))
@@ -576,18 +576,19 @@ def main():
         # cost of a job too small to fill the GPU (short waves, launch tails,
         # per-job set-up).  That bounds what merging jobs can win, and the node
         # format what the faster traversal can.
-        rates = full_wave_rates(gscenes, specs)
+        rates = full_wave_rates({"plain": psvc, "served": served}, specs)
         jids = psvc_jobs
-        ideal32 = sum(r / (rates[specs[j.scene].name]["fp32"] * 1e6) for j, r in zip(timed[0], jids))
-        ideal8 = sum(r / (rates[specs[j.scene].name]["w8"] * 1e6) for j, r in zip(timed[0], jids))
+        ideal_p = sum(r / (rates[specs[j.scene].name]["plain"] * 1e6) for j, r in zip(timed[0], jids))
+        ideal_s = sum(r / (rates[specs[j.scene].name]["served"] * 1e6) for j, r in zip(timed[0], jids))
         small = [k for k, j in enumerate(timed[0]) if j.width * j.height * j.spp < (1 << 20)]
         breakdown = {"plain_s": ps, "served_s": ss,
-                     "plain_at_full_wave_rate_s": ideal32, "w8_at_full_wave_rate_s": ideal8,
-                     "bound_merging_only": ps / ideal32, "bound_merging_and_w8": ps / ideal8,
+                     "plain_at_full_wave_rate_s": ideal_p, "served_at_full_wave_rate_s": ideal_s,
+                     "bound_merging_only": ps / ideal_p, "bound_merging_and_served_kernels": ps / ideal_s,
                      "achieved": ps / ss, "jobs_under_1Mi_paths": len(small),
                      "their_share_of_plain_s": sum(psvc_times[k] for k in small) / ps,
                      "their_share_of_rays": sum(jids[k] for k in small) / max(1, sum(jids)),
                      "full_wave_mrays": rates}
+        psvc.close()
         plain = {"value": pr / ps / 1e6, "unit": "Mrays/s", "step_jobs": len(timed[0]), "breakdown": breakdown,
                  "p50_ms": 1000 * pct(pl, 50), "p99_ms": 1000 * pct(pl, 99),
                  "served_same_step_mrays": sr / ss / 1e6, "speedup": (sr / ss) / (pr / ps),
