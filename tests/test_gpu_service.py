@@ -225,3 +225,31 @@ def test_run_while_running_is_refused(resident):
     th.join(timeout=60)
     assert not th.is_alive()
     svc.close()
+
+
+def test_live_submission_over_budget_fails_alone(resident):
+    """A job whose frame can never fit the memory budget is marked failed when
+    it reaches the head of the queue; the jobs submitted around it, live, still
+    render to the same bits as alone."""
+    import threading
+    fmt = xtgpu.NODES_W8
+    ok_jobs = [(0, xtgpu.PATHTRACER, 64, 48, 4, 4, 100.0, 31), (1, xtgpu.DEPTH, 40, 30, 2, 1, 100.0, 32)]
+    alone = [resident[s].render(integ, w, h, spp=spp, rdepth=d, ao_max_distance=md, seed=seed, node_format=fmt)[0]
+             for (s, integ, w, h, spp, d, md, seed) in ok_jobs]
+    # a 1024 x 1024 frame is 16 MiB; the budget holds 4 MiB
+    svc = Service(resident, node_format=fmt, wave_paths=1 << 15, merge_jobs=True, memory_budget=4 << 20)
+    svc.open(True)
+    th = threading.Thread(target=lambda: svc.run(max_seconds=60.0))
+    th.start()
+    a = svc.submit(*ok_jobs[0])
+    big = svc.submit(0, xtgpu.PATHTRACER, 1024, 1024, 1, 4, 100.0, 33)
+    b = svc.submit(*ok_jobs[1])
+    svc.open(False)
+    th.join(timeout=60)
+    assert not th.is_alive()
+    assert svc.poll(big).state == 3
+    for jid, ref in zip((a, b), alone):
+        assert svc.poll(jid).state == 2
+        assert np.array_equal(svc.result(jid), ref)
+        svc.release(jid)
+    svc.close()
