@@ -408,20 +408,9 @@ __global__ void k_wide_level(const float4 *__restrict__ bnodes, const float4 *__
     float o[3], sc[3];
     const float alo[3] = {lo.x, lo.y, lo.z}, ahi[3] = {hi.x, hi.y, hi.z};
     for (int a = 0; a < 3; ++a) {
-        // the origin at least one quantum below the lowest child, so that every
-        // stored lower bound keeps its quantum of padding (quant_w); a lower
-        // origin may need a larger quantum, hence the few rounds
         ob[a] = origin_bits_w(alo[a]);
         o[a] = __uint_as_float(ob[a]);
         ex[a] = pick_exp_w(o[a], ahi[a]);
-        for (int round = 0; round < 8; ++round) {
-            const uint32_t b = origin_bits_w(__fsub_rd(alo[a], __uint_as_float(ex[a] << 23)));
-            const uint32_t e = pick_exp_w(__uint_as_float(b), ahi[a]);
-            ob[a] = b;
-            o[a] = __uint_as_float(b);
-            if (e == ex[a]) break;
-            ex[a] = e;
-        }
         sc[a] = __uint_as_float(ex[a] << 23);
     }
     uint32_t qlo[3][8], qhi[3][8], meta[8];

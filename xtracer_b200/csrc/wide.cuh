@@ -1,7 +1,7 @@
 // Closest-hit traversal of the 8-wide quantised BVH built by wide.cu.
 //
-// A node visit tests its 8 child boxes in quantised space (one byte permute and
-// one FMA per bound: t(q) = q * (2^e * inv) + (origin - ray.o) * inv), tests the primitives of
+// A node visit tests its 8 child boxes in quantised space (one FMA per bound:
+// t(q) = q * (2^e * inv) + (origin - ray.o) * inv), tests the primitives of
 // every hit leaf child at once, and goes on with the nearest hit internal
 // child.  The other hit internal children stay behind as one stack entry (node
 // group): the base index, the node's internal-child mask and the hit children
@@ -19,12 +19,7 @@ constexpr int WIDE_MAX_LEAF = 3;
 // far-distance scale of the quantised box test (as for the binary Q8 nodes)
 #define XTG_TFAR_SCALE_W8 1.0000015f
 
-// Byte k of w read as the float 1 + q 2^-15 (one byte permute, no integer
-// conversion): the bits 0x3F80 | q << 8 | 00.
-__device__ __forceinline__ float q8(uint32_t w, int k)
-{
-    return __uint_as_float(__byte_perm(w, 0x3F800000u, 0x7604u | ((uint32_t)k << 4)));
-}
+__device__ __forceinline__ float q8(uint32_t w, int k) { return (float)((w >> (8 * k)) & 0xFFu); }
 
 // Ray sign bits: bit k set if component k of the (clamped) inverse direction
 // is negative; a zero component counts by the sign of its clamped inverse.
@@ -53,19 +48,12 @@ __device__ __forceinline__ bool wide_step(const SceneView &V, const RayPre &r, u
     const uint4 *p = (const uint4 *)V.nodes + 5 * (size_t)node;
     const uint4 w0 = __ldg(p), w1 = __ldg(p + 1);
     ++nv;
-    // t(q) = q s + b per axis, s the quantum over the direction, b the node origin's
-    // entry distance; with q read as 1 + q 2^-15 it is (1 + q 2^-15)(2^15 s) +
-    // (b - 2^15 s).  Folding the bias into the base adds one rounding, at most
-    // D 2^-24 + 2^-9 quanta for a node D quanta from the ray's origin: the far
-    // planes' relative slack (XTG_TFAR_SCALE_W8) covers the first term and the
-    // quantum of padding each bound carries the second.
-    const float sx0 = __uint_as_float((w0.x & 0xFFu) << 23) * r.inv.x;
-    const float sy0 = __uint_as_float((w0.y & 0xFFu) << 23) * r.inv.y;
-    const float sz0 = __uint_as_float((w0.z & 0xFFu) << 23) * r.inv.z;
-    const float sx = sx0 * 32768.0f, sy = sy0 * 32768.0f, sz = sz0 * 32768.0f;
-    const float bx = fmaf(-32768.0f, sx0, fmaf(__uint_as_float(w0.x & ~0xFFu), r.inv.x, -r.oinv.x));
-    const float by = fmaf(-32768.0f, sy0, fmaf(__uint_as_float(w0.y & ~0xFFu), r.inv.y, -r.oinv.y));
-    const float bz = fmaf(-32768.0f, sz0, fmaf(__uint_as_float(w0.z & ~0xFFu), r.inv.z, -r.oinv.z));
+    const float sx = __uint_as_float((w0.x & 0xFFu) << 23) * r.inv.x;
+    const float sy = __uint_as_float((w0.y & 0xFFu) << 23) * r.inv.y;
+    const float sz = __uint_as_float((w0.z & 0xFFu) << 23) * r.inv.z;
+    const float bx = fmaf(__uint_as_float(w0.x & ~0xFFu), r.inv.x, -r.oinv.x);
+    const float by = fmaf(__uint_as_float(w0.y & ~0xFFu), r.inv.y, -r.oinv.y);
+    const float bz = fmaf(__uint_as_float(w0.z & ~0xFFu), r.inv.z, -r.oinv.z);
     const uint32_t imask = w0.w;
     // bound words, 4 slots each: qlo.x at word 8+h, qlo.y 10+h, qlo.z 12+h,
     // qhi.x 14+h, qhi.y 16+h, qhi.z 18+h (h = 0 for slots 0-3, 1 for 4-7);
