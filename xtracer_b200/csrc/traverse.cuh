@@ -252,12 +252,14 @@ __device__ __forceinline__ SceneView scene_view(const DevScene &S)
 }
 
 // Primitive i of the leaf array (3 float4: triangle vertices or sphere centre
-// and radius, the primitive id in the first w).
+// and radius, the primitive id in the first w).  All three words are loaded
+// before the kind is known, so a triangle waits for one round trip, not two
+// (a sphere reads 16 bytes it does not use).
 __device__ __forceinline__ void prim_test(const float4 *leaf, uint32_t i, const RayPre &r, float tmin, float &tmax,
                                           uint32_t &prim, float &bu, float &bv)
 {
     const float4 *lp = leaf + 3 * (size_t)i;
-    float4 a = __ldg(lp), b = __ldg(lp + 1);
+    const float4 a = __ldg(lp), b = __ldg(lp + 1), c = __ldg(lp + 2);
     uint32_t id = __float_as_uint(a.w);
     if (id & SPHERE_BIT) {
         id &= ~SPHERE_BIT;
@@ -266,7 +268,6 @@ __device__ __forceinline__ void prim_test(const float4 *leaf, uint32_t i, const 
             bu = bv = 0.f;
         }
     } else {
-        float4 c = __ldg(lp + 2);
         float u, v;
         if (hit_triangle(r, make_float3(a.x, a.y, a.z), make_float3(b.x, b.y, b.z), make_float3(c.x, c.y, c.z), tmin,
                          tmax, u, v, id, prim)) {
