@@ -128,10 +128,10 @@ WAVES_IN_FLIGHT = 3   # served form: waves on streams of their own, each filling
 # roofline's traffic is the DRAM figure of each scene times that scene's rays,
 # per launch; the issue figures name the resource that binds the kernel.
 NCU_EXTEND = {
-    "terrain10k": (35, 442, 0.735, 12.8), "terrain50k": (39, 663, 0.726, 11.9),
-    "terrain200k": (48, 846, 0.710, 11.6), "terrain500k": (63, 949, 0.698, 12.0),
-    "terrain1m": (89, 1213, 0.681, 11.6), "hairball2m": (88, 1715, 0.660, 13.5),
-    "spheres64": (32, 86, 0.686, 16.2), "spheres4096": (33, 123, 0.643, 16.4)}
+    "terrain10k": (35, 442, 0.745, 12.8), "terrain50k": (39, 661, 0.742, 11.9),
+    "terrain200k": (48, 845, 0.730, 11.6), "terrain500k": (62, 946, 0.721, 12.0),
+    "terrain1m": (89, 1209, 0.705, 11.6), "hairball2m": (88, 1709, 0.680, 13.5),
+    "spheres64": (32, 86, 0.686, 16.2), "spheres4096": (33, 124, 0.645, 16.4)}
 
 
 def build_scenes(scale, autotune=False):
