@@ -56,14 +56,16 @@ __device__ __forceinline__ bool wide_step(const SceneView &V, const RayPre &r, u
     const float bz = fmaf(__uint_as_float(w0.z & ~0xFFu), r.inv.z, -r.oinv.z);
     const uint32_t imask = w0.w;
     // bound words, 4 slots each: qlo.x at word 8+h, qlo.y 10+h, qlo.z 12+h,
-    // qhi.x 14+h, qhi.y 16+h, qhi.z 18+h (h = 0 for slots 0-3, 1 for 4-7);
-    // one half at a time keeps fewer words live.  The near plane of an axis is
-    // its lower bound when the ray goes up that axis, else the upper one, so
-    // each bound takes one FMA and no swap.  An unused slot (qlo 255 > qhi 0)
-    // is behind its own far plane and never hits.
+    // qhi.x 14+h, qhi.y 16+h, qhi.z 18+h (h = 0 for slots 0-3, 1 for 4-7).
+    // Both halves unrolled, so the second half's loads are issued with the
+    // first's instead of after it (a few spilled words, cheaper than the
+    // second wait).  The near plane of an axis is its lower bound when the ray
+    // goes up that axis, else the upper one, so each bound takes one FMA and
+    // no swap.  An unused slot (qlo 255 > qhi 0) is behind its own far plane
+    // and never hits.
     const uint32_t *qw = (const uint32_t *)(p + 2);
     uint32_t hitbits = 0;
-#pragma unroll 1
+#pragma unroll
     for (int h = 0; h < 2; ++h) {
         const uint32_t lx = __ldg(qw + h), ly = __ldg(qw + 2 + h), lz = __ldg(qw + 4 + h);
         const uint32_t hx = __ldg(qw + 6 + h), hy = __ldg(qw + 8 + h), hz = __ldg(qw + 10 + h);
