@@ -47,6 +47,9 @@ __device__ __forceinline__ bool wide_step(const SceneView &V, const RayPre &r, u
 {
     const uint4 *p = (const uint4 *)V.nodes + 5 * (size_t)node;
     const uint4 w0 = __ldg(p), w1 = __ldg(p + 1);
+    // the stack's top entry, read with the node so that a pop at the end of
+    // the step does not wait for local memory (entry 0, unused, when empty)
+    const uint2 top = stack[sp > 0 ? sp - 1 : 0];
     ++nv;
     const float sx = __uint_as_float((w0.x & 0xFFu) << 23) * r.inv.x;
     const float sy = __uint_as_float((w0.y & 0xFFu) << 23) * r.inv.y;
@@ -100,7 +103,8 @@ __device__ __forceinline__ bool wide_step(const SceneView &V, const RayPre &r, u
     if (!hits) {
         // next node group from the stack
         if (sp == 0) return true;
-        const uint2 e = stack[--sp];
+        --sp;
+        const uint2 e = top;
         base = e.x;
         im = e.y & 0xFFu;
         hits = e.y >> 8;
