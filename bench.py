@@ -5,7 +5,7 @@ hairball, 64 and 4096 spheres), 512 seeded jobs with resolution in
 {128,256,512,1024}^2, spp in {1,4,16,64}, pathtracer depth 4.
 
 A step is one slice of 64 jobs of that stream, all submitted at once and run
-to completion through the render service (merged waves, two in flight, 8-bit
+to completion through the render service (merged waves, three in flight, 8-bit
 quantised BVH, CUDA graphs).  Reported beside it, on the same jobs: the plain path (one job per
 launch, FP32 BVH, no graphs), an end-to-end pass with every frame copied back
 to host memory, open-loop p50/p99 latency under Poisson arrivals, the extend
@@ -128,10 +128,10 @@ WAVES_IN_FLIGHT = 3   # served form: waves on streams of their own, each filling
 # roofline's traffic is the DRAM figure of each scene times that scene's rays,
 # per launch; the issue figures name the resource that binds the kernel.
 NCU_EXTEND = {
-    "terrain10k": (35, 442, 0.745, 12.8), "terrain50k": (39, 661, 0.742, 11.9),
-    "terrain200k": (48, 845, 0.730, 11.6), "terrain500k": (62, 946, 0.721, 12.0),
-    "terrain1m": (89, 1209, 0.705, 11.6), "hairball2m": (88, 1709, 0.680, 13.5),
-    "spheres64": (32, 86, 0.686, 16.2), "spheres4096": (33, 124, 0.645, 16.4)}
+    "terrain10k": (37, 482, 0.736, 12.2), "terrain50k": (41, 709, 0.739, 11.3),
+    "terrain200k": (50, 892, 0.731, 11.0), "terrain500k": (65, 990, 0.724, 11.4),
+    "terrain1m": (90, 1254, 0.712, 10.9), "hairball2m": (91, 1760, 0.688, 12.9),
+    "spheres64": (34, 111, 0.638, 16.3), "spheres4096": (35, 153, 0.598, 16.3)}
 
 
 def build_scenes(scale, autotune=False):
