@@ -75,6 +75,8 @@ struct xtgpu_service {
     xtgpu_service_opts o{};
     cudaStream_t s = nullptr;  // admission, frees, results
     bool own_stream = false;   // created here: the legacy default stream cannot be captured
+    cudaStream_t cs = nullptr; // host_results: frame copies to pinned memory, off the
+                               // admission stream that the next waves wait on
     int nslots = 2;
     xtg::WaveSlot slot[XTGPU_MAX_WAVES_IN_FLIGHT];
     cudaEvent_t admitted = nullptr;   // frames of admitted jobs allocated and zeroed
@@ -89,6 +91,7 @@ struct xtgpu_service {
     uint64_t waves = 0;
     // host_results: pinned frames reused by size, events of copies in flight
     std::multimap<uint64_t, float4 *> pinned_free;
+    std::vector<void *> pinned_chunks;   // what cudaMallocHost returned; frames are carved from these
     std::vector<cudaEvent_t> events_free;
     std::vector<int64_t> copying;    // finished on the GPU, host copy in flight
     // the job table and everything above it that submit, poll, result and
@@ -256,7 +259,8 @@ static xtgpu_status retire_wave(xtgpu_service *v, WaveSlot &W)
             // pinned frames come in power-of-two size classes (from 64 KB) and
             // are reused by any job whose frame fits in at most twice its
             // size: pinning memory is slow and may wait for the device, so a
-            // stream of varied frame sizes should reach a steady pool
+            // stream of varied frame sizes should reach a steady pool, and a
+            // class that runs out is pinned 64 MB (up to 16 frames) at a time
             const uint64_t cls = pinned_class(J.frame_bytes);
             auto it = v->pinned_free.lower_bound(J.frame_bytes);
             if (it != v->pinned_free.end() && it->first <= 2 * cls) {
@@ -264,8 +268,13 @@ static xtgpu_status retire_wave(xtgpu_service *v, WaveSlot &W)
                 J.host_bytes = it->first;
                 v->pinned_free.erase(it);
             } else {
-                XTG_CUDA(cudaMallocHost((void **)&J.host, cls));
+                const uint64_t nbuf = std::max<uint64_t>(1, std::min<uint64_t>(16, (64ull << 20) / cls));
+                char *chunk = nullptr;
+                XTG_CUDA(cudaMallocHost((void **)&chunk, nbuf * cls));
+                v->pinned_chunks.push_back(chunk);
+                J.host = (float4 *)chunk;
                 J.host_bytes = cls;
+                for (uint64_t b = 1; b < nbuf; ++b) v->pinned_free.emplace(cls, (float4 *)(chunk + b * cls));
             }
             if (!v->events_free.empty()) {
                 J.copied = v->events_free.back();
@@ -273,9 +282,9 @@ static xtgpu_status retire_wave(xtgpu_service *v, WaveSlot &W)
             } else {
                 XTG_CUDA(cudaEventCreateWithFlags(&J.copied, cudaEventDisableTiming));
             }
-            XTG_CUDA(cudaMemcpyAsync(J.host, J.frame, J.frame_bytes, cudaMemcpyDeviceToHost, v->s));
-            XTG_CUDA(cudaFreeAsync(J.frame, v->s));
-            XTG_CUDA(cudaEventRecord(J.copied, v->s));
+            XTG_CUDA(cudaMemcpyAsync(J.host, J.frame, J.frame_bytes, cudaMemcpyDeviceToHost, v->cs));
+            XTG_CUDA(cudaFreeAsync(J.frame, v->cs));
+            XTG_CUDA(cudaEventRecord(J.copied, v->cs));
             J.frame = nullptr;
             v->mem_used -= J.frame_bytes;
             v->copying.push_back(W.ids[k]);
@@ -317,14 +326,14 @@ static void destroy_service(xtgpu_service *v)
 {
     for (int k = 0; k < v->nslots; ++k)
         if (v->slot[k].s) cudaStreamSynchronize(v->slot[k].s);
+    if (v->cs) cudaStreamSynchronize(v->cs);
     cudaStreamSynchronize(v->s);
     for (auto &kv : v->jobs) {
         if (kv.second.frame) cudaFreeAsync(kv.second.frame, v->s);
-        if (kv.second.host) cudaFreeHost(kv.second.host);
         if (kv.second.copied) cudaEventDestroy(kv.second.copied);
     }
     cudaStreamSynchronize(v->s);
-    for (auto &kv : v->pinned_free) cudaFreeHost(kv.second);
+    for (void *c : v->pinned_chunks) cudaFreeHost(c);
     for (cudaEvent_t e : v->events_free) cudaEventDestroy(e);
     for (int k = 0; k < v->nslots; ++k) {
         WaveSlot &W = v->slot[k];
@@ -334,6 +343,7 @@ static void destroy_service(xtgpu_service *v)
         if (W.s) cudaStreamDestroy(W.s);
     }
     if (v->admitted) cudaEventDestroy(v->admitted);
+    if (v->cs) cudaStreamDestroy(v->cs);
     if (v->own_stream) cudaStreamDestroy(v->s);
     delete v;
 }
@@ -377,7 +387,8 @@ xtgpu_status xtgpu_service_create(const xtgpu_service_opts *opts, void *stream, 
         v->own_stream = true;
     }
     cudaError_t e0 = cudaEventCreateWithFlags(&v->admitted, cudaEventDisableTiming);
-    if (e0 != cudaSuccess) return fail(cuda_fail(e0, "xtgpu_service_create: cudaEventCreate", __FILE__, __LINE__));
+    if (e0 == cudaSuccess) e0 = cudaStreamCreateWithFlags(&v->cs, cudaStreamNonBlocking);
+    if (e0 != cudaSuccess) return fail(cuda_fail(e0, "xtgpu_service_create: event and copy stream", __FILE__, __LINE__));
     for (int k = 0; k < v->nslots; ++k) {
         WaveSlot &W = v->slot[k];
         cudaError_t e = cudaStreamCreateWithFlags(&W.s, cudaStreamNonBlocking);
