@@ -109,6 +109,27 @@ def test_host_results_match(resident, inflight):
     svc.close()
 
 
+def test_host_results_many_frames_of_one_class(resident):
+    """40 finished 64x64 frames held at once: pinned frames of one size class
+    are carved 16 to a pinned chunk, so this takes three chunks; every frame
+    keeps its own buffer and equals its plain render (distinct seeds, so two
+    jobs sharing a buffer would show), and the buffers are reused afterwards."""
+    jobs = [(k % len(resident), xtgpu.PATHTRACER, 64, 64, 1, 2, 100.0, 100 + k) for k in range(40)]
+    alone = [resident[s].render(integ, w, h, spp=spp, rdepth=d, ao_max_distance=md, seed=seed)[0]
+             for (s, integ, w, h, spp, d, md, seed) in jobs]
+    svc = Service(resident, merge_jobs=True, host_results=True)
+    for rep in range(2):
+        ids = [svc.submit(*j) for j in jobs]
+        svc.run()
+        for jid, ref in zip(ids, alone):
+            assert svc.poll(jid).state == 2
+            assert np.array_equal(svc.result_view(jid), ref)
+        assert len({svc.result_view(jid).ctypes.data for jid in ids}) == len(ids)
+        for jid in ids:
+            svc.release(jid)
+    svc.close()
+
+
 def test_arrivals_and_latency_bookkeeping(resident):
     svc = Service(resident, merge_jobs=True)
     ids = [svc.submit(0, xtgpu.PATHTRACER, 32, 32, 4, 4, 100.0, k, submit_s=0.05 * k) for k in range(5)]
