@@ -931,6 +931,7 @@ __global__ void __launch_bounds__(MINB > 0 ? 128 : 256, MINB > 0 ? MINB : 1)
                                 // than held in registers
     int idx = 0, sp = 0;
     uint2 stack[STACK];
+    stack[0] = make_uint2(0u, 0u);   // the 8-wide step reads entry 0 ahead even when the stack is empty
     bool active = false, exhausted = false;
     while (true) {
         const bool want = !active && !exhausted;

@@ -130,6 +130,7 @@ __device__ __forceinline__ void trace_wide(const SceneView &V, const RayPre &r, 
 {
     const uint32_t m = ray_octant(r);
     uint2 stack[STACK];
+    stack[0] = make_uint2(0u, 0u);   // wide_step reads entry 0 ahead even when the stack is empty
     int sp = 0;
     int32_t node = V.root;
     if (node >= 0)
