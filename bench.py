@@ -657,8 +657,10 @@ def main():
                 "served": {"p50_ms": 1000 * pct(q8, 50), "p99_ms": 1000 * pct(q8, 99), "wall_s": D.max(qw)},
                 "plain": {"p50_ms": 1000 * pct(p8, 50), "p99_ms": 1000 * pct(p8, 99), "wall_s": D.max(pw8)}}
 
+    # the reference on the host cores: rank 0 of a one-GPU run only (with
+    # replicas, the host's cores are shared by the ranks' own host work)
     cpu = None
-    if not args.no_cpu and rank == 0:
+    if not args.no_cpu and rank == 0 and world == 1:
         cpu = cpu_reference_sample(args.scale, os.cpu_count() or 1)
         if cpu is not None:
             gpu_same = gpu_on_cpu_sample(gscenes, specs)
