@@ -14,6 +14,12 @@ using namespace xtg;
 
 namespace {
 
+// A candidate replaces the current setting only when its probe is at least 2 %
+// faster: the probe's run-to-run spread is a few per cent, and a pick made on
+// noise (a smaller wave, another builder) can cost more on a served stream
+// than it gained on the probe.
+constexpr float kGain = 0.98f;
+
 struct Probe {
     xtgpu_scene *sc;
     int fmt;
@@ -100,7 +106,7 @@ extern "C" xtgpu_status xtgpu_autotune(xtgpu_scene *sc, int32_t fmt, double budg
             C.bvh_builder = other;
             float t = 0.f;
             if ((st = probe_ms(P, C, &t)) == XTGPU_OK) {
-                if (t < cur) {
+                if (t < cur * kGain) {
                     cur = t;
                     T = C;
                 } else {
@@ -119,7 +125,7 @@ extern "C" xtgpu_status xtgpu_autotune(xtgpu_scene *sc, int32_t fmt, double budg
             C.leaf_size = leaf;
             float t = 0.f;
             if ((st = probe_ms(P, C, &t)) != XTGPU_OK) break;
-            if (t < cur) {
+            if (t < cur * kGain) {
                 cur = t;
                 best_leaf = leaf;
             }
@@ -138,7 +144,7 @@ extern "C" xtgpu_status xtgpu_autotune(xtgpu_scene *sc, int32_t fmt, double budg
             C.*field = v;
             float t = 0.f;
             if ((st = probe_ms(P, C, &t)) != XTGPU_OK) return;
-            if (t < cur) {
+            if (t < cur * kGain) {
                 cur = t;
                 T = C;
             }
@@ -162,7 +168,7 @@ extern "C" xtgpu_status xtgpu_autotune(xtgpu_scene *sc, int32_t fmt, double budg
             C.wave_paths = w;
             float t = 0.f;
             if ((st = probe_ms(P, C, &t)) != XTGPU_OK) break;
-            if (t < cur) {
+            if (t < cur * kGain) {
                 cur = t;
                 T = C;
             }
