@@ -1079,9 +1079,11 @@ __global__ void __launch_bounds__(MINB > 0 ? 128 : 256, MINB > 0 ? MINB : 1)
 // material loads then wait only for the hit, not for the job and scene tables.
 // LOBE false leaves out the Phong / BlinnPhong specular lobe (FP64, called out
 // of line), whose call costs registers on every path; it is launched for waves
-// whose scenes have no such material.
+// whose scenes have no such material.  Launched with exactly the blocks that
+// fit at once (SHADE_BLOCKS_PER_SM per SM), each striding over the paths.
+constexpr int SHADE_BLOCKS_PER_SM = 4;
 template <bool MULTI, bool LOBE>
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256, SHADE_BLOCKS_PER_SM)
     k_shade(const __grid_constant__ DevScene S1, const DevJob *__restrict__ jobs,
             const DevScene *__restrict__ scenes, WaveQueues q, int side)
 {
@@ -1484,13 +1486,13 @@ void WaveRunner::enqueue(int njobs, int64_t total, int bounces, int fmt, bool mu
         if (multi)
             for (const DevScene &h : host_scenes) lobe = lobe || h.has_lobe;
         if (multi && lobe)
-            k_shade<true, true><<<gb, 256, 0, s>>>(single, jobs, scenes, q, side);
+            k_shade<true, true><<<sms * SHADE_BLOCKS_PER_SM, 256, 0, s>>>(single, jobs, scenes, q, side);
         else if (multi)
-            k_shade<true, false><<<gb, 256, 0, s>>>(single, jobs, scenes, q, side);
+            k_shade<true, false><<<sms * SHADE_BLOCKS_PER_SM, 256, 0, s>>>(single, jobs, scenes, q, side);
         else if (lobe)
-            k_shade<false, true><<<gb, 256, 0, s>>>(single, jobs, scenes, q, side);
+            k_shade<false, true><<<sms * SHADE_BLOCKS_PER_SM, 256, 0, s>>>(single, jobs, scenes, q, side);
         else
-            k_shade<false, false><<<gb, 256, 0, s>>>(single, jobs, scenes, q, side);
+            k_shade<false, false><<<sms * SHADE_BLOCKS_PER_SM, 256, 0, s>>>(single, jobs, scenes, q, side);
         side ^= 1;
     }
     if (!defer_acc) k_accumulate<<<gb, 256, 0, s>>>(jobs, q.ctl, (const int64_t *)prefixbuf.p, q.contrib);
@@ -1702,9 +1704,9 @@ void enqueue_wave_raw(const xtgpu_tuning &T, const WaveQueues &q, const DevJob *
             launch_extend_kernel(T, fmt, false, single, scenes, jobs, q, side, sms, stack, s);
         cudaMemsetAsync(q.ctl + (side ^ 1), 0, sizeof(int32_t), s);
         if (single.has_lobe)
-            k_shade<false, true><<<gb, 256, 0, s>>>(single, jobs, scenes, q, side);
+            k_shade<false, true><<<sms * SHADE_BLOCKS_PER_SM, 256, 0, s>>>(single, jobs, scenes, q, side);
         else
-            k_shade<false, false><<<gb, 256, 0, s>>>(single, jobs, scenes, q, side);
+            k_shade<false, false><<<sms * SHADE_BLOCKS_PER_SM, 256, 0, s>>>(single, jobs, scenes, q, side);
         side ^= 1;
     }
     k_accumulate<<<gb, 256, 0, s>>>(jobs, q.ctl, prefix, q.contrib);
